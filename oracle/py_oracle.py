@@ -1,0 +1,176 @@
+"""ctypes binding of the CPU oracle (TEST INFRASTRUCTURE).
+
+Only tests/, ``__graft_entry__.smoke()`` and the CPU-baseline / reference legs of
+bench.py may import this module; the product package never does.  The oracle is
+the C++17 restatement of the reference time step in scopi_oracle.cpp.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle_scopi.so")
+
+NOFRICTION, FRICTION, VISCOUS = 0, 1, 2
+VAP_FIXED, VAP_FPD = 0, 1
+BRUTE_FORCE, KDTREE = 0, 1
+
+
+class OrcParams(C.Structure):
+    _fields_ = [
+        ("dim", C.c_int32), ("problem", C.c_int32), ("vap", C.c_int32), ("contact_method", C.c_int32),
+        ("dmax", C.c_double), ("kd_tree_radius", C.c_double), ("alpha", C.c_double), ("max_ite", C.c_int64),
+        ("tolerance", C.c_double), ("dynamic_descent", C.c_int32), ("mu", C.c_double), ("gamma", C.c_double),
+        ("gamma_min", C.c_double), ("gamma_tol", C.c_double), ("num_threads", C.c_int32),
+    ]
+
+
+class OrcParticles(C.Structure):
+    _fields_ = [
+        ("n", C.c_int64), ("nb_inactive", C.c_int64), ("shape", C.POINTER(C.c_int32)),
+        ("pos", C.POINTER(C.c_double)), ("q", C.POINTER(C.c_double)), ("v", C.POINTER(C.c_double)),
+        ("omega", C.POINTER(C.c_double)), ("vd", C.POINTER(C.c_double)), ("omega_d", C.POINTER(C.c_double)),
+        ("f", C.POINTER(C.c_double)), ("m", C.POINTER(C.c_double)), ("j", C.POINTER(C.c_double)),
+        ("radius", C.POINTER(C.c_double)), ("length", C.POINTER(C.c_double)),
+    ]
+
+
+class OrcStats(C.Structure):
+    _fields_ = [
+        ("contacts", C.c_int64), ("iterations", C.c_int64), ("backtracks", C.c_int64), ("restarts", C.c_int64),
+        ("converged", C.c_int32), ("violation", C.c_double), ("seconds_contacts", C.c_double),
+        ("seconds_solve", C.c_double), ("seconds_other", C.c_double),
+    ]
+
+
+_lib = None
+
+
+def build() -> None:
+    """Compile the oracle with its Makefile (g++, OpenMP, -ffp-contract=off)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        L.orc_create.restype = C.c_void_p
+        L.orc_create.argtypes = [C.POINTER(OrcParams), C.POINTER(OrcParticles)]
+        L.orc_destroy.argtypes = [C.c_void_p]
+        L.orc_run.argtypes = [C.c_void_p, C.c_double, C.c_int64, C.c_int64]
+        L.orc_get_particles.argtypes = [C.c_void_p, C.POINTER(OrcParticles)]
+        L.orc_set_particles.argtypes = [C.c_void_p, C.POINTER(OrcParticles)]
+        L.orc_num_contacts.restype = C.c_int64
+        L.orc_num_contacts.argtypes = [C.c_void_p]
+        P = C.POINTER(C.c_double)
+        L.orc_get_contacts.restype = C.c_int64
+        L.orc_get_contacts.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), P, P, P, P, P, C.c_int64]
+        L.orc_get_lambda.restype = C.c_int64
+        L.orc_get_lambda.argtypes = [C.c_void_p, P, C.c_int64]
+        L.orc_get_stats.argtypes = [C.c_void_p, C.POINTER(OrcStats)]
+        L.orc_detect.restype = C.c_int64
+        L.orc_detect.argtypes = [C.c_void_p]
+        L.orc_amat.argtypes = [C.c_void_p, P, P]
+        L.orc_atmat.argtypes = [C.c_void_p, P, P]
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _particles_struct(pa, keep):
+    keep.append(pa)
+    return OrcParticles(
+        pa.n, pa.nb_inactive, pa.shape.ctypes.data_as(C.POINTER(C.c_int32)), _dp(pa.pos), _dp(pa.q), _dp(pa.v),
+        _dp(pa.omega), _dp(pa.vd), _dp(pa.omega_d), _dp(pa.f), _dp(pa.m), _dp(pa.j), _dp(pa.radius), _dp(pa.length),
+    )
+
+
+class OracleSolver:
+    """Mirror of ``ScopiSolver<dim, problem, OptimGradient<apgd>, contact, vap>`` on the CPU."""
+
+    def __init__(self, particles, problem=NOFRICTION, vap=VAP_FIXED, contact_method=KDTREE, dmax=2.0,
+                 kd_tree_radius=17.0, alpha=0.05, max_ite=10000, tolerance=1e-7, dynamic_descent=True, mu=0.1,
+                 gamma=0.0, gamma_min=-2.0, gamma_tol=1e-6, num_threads=0):
+        self.pa = particles.copy()
+        self.params = OrcParams(particles.dim, problem, vap, contact_method, dmax, kd_tree_radius, alpha, max_ite,
+                                tolerance, 1 if dynamic_descent else 0, mu, gamma, gamma_min, gamma_tol, num_threads)
+        keep = []
+        ps = _particles_struct(self.pa, keep)
+        self.h = lib().orc_create(C.byref(self.params), C.byref(ps))
+        if not self.h:
+            raise RuntimeError("orc_create failed")
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            lib().orc_destroy(h)
+            self.h = None
+
+    def run(self, dt, total_it, initial_iter=0):
+        rc = lib().orc_run(self.h, dt, total_it, initial_iter)
+        if rc != 0:
+            raise RuntimeError("orc_run failed")
+        self.sync()
+        return self
+
+    def sync(self):
+        keep = []
+        ps = _particles_struct(self.pa, keep)
+        lib().orc_get_particles(self.h, C.byref(ps))
+        return self.pa
+
+    def set_particles(self, pa):
+        self.pa = pa.copy()
+        keep = []
+        ps = _particles_struct(self.pa, keep)
+        lib().orc_set_particles(self.h, C.byref(ps))
+
+    def detect(self):
+        lib().orc_detect(self.h)
+        return self.contacts()
+
+    def contacts(self):
+        n = lib().orc_num_contacts(self.h)
+        ci = np.zeros(n, np.int64)
+        cj = np.zeros(n, np.int64)
+        d = np.zeros(n)
+        g = np.zeros(n)
+        nij = np.zeros((n, 3))
+        pi = np.zeros((n, 3))
+        pj = np.zeros((n, 3))
+        lib().orc_get_contacts(self.h, ci.ctypes.data_as(C.POINTER(C.c_int64)), cj.ctypes.data_as(C.POINTER(C.c_int64)),
+                               _dp(d), _dp(nij), _dp(pi), _dp(pj), _dp(g), n)
+        return {"i": ci, "j": cj, "dij": d, "nij": nij, "pi": pi, "pj": pj, "gamma": g}
+
+    def lagrange_multiplier(self):
+        n = lib().orc_get_lambda(self.h, None, 0)
+        out = np.zeros(n)
+        lib().orc_get_lambda(self.h, _dp(out), n)
+        return out
+
+    def stats(self):
+        s = OrcStats()
+        lib().orc_get_stats(self.h, C.byref(s))
+        return {k: getattr(s, k) for k, _ in OrcStats._fields_}
+
+    def amat(self, u):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        out = np.zeros(3 * lib().orc_num_contacts(self.h))
+        lib().orc_amat(self.h, _dp(u), _dp(out))
+        return out
+
+    def atmat(self, f):
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        out = np.zeros(6 * (self.pa.n - self.pa.nb_inactive))
+        lib().orc_atmat(self.h, _dp(f), _dp(out))
+        return out

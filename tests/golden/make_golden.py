@@ -1,0 +1,56 @@
+"""Extract the golden end states of the reference's solver regression tests.
+
+Reads the reference's own golden snapshots (test/references/*.json of
+hpc-maths/scopi, written by ScopiSolver::write_output_files) and keeps only what
+the parity tests compare: per object position, quaternion, velocity and omega
+(the fields test/utils.cpp:14-75 diffs), plus the contact list of the last
+step (i, j, distance, normal, pi, pj).  Writes tests/golden/reference_states.json.
+
+Run once in a checkout that has the reference at REF (default /root/reference):
+    python tests/golden/make_golden.py [REF]
+"""
+import json
+import os
+import sys
+
+FILES = [
+    "3spheres_nofriction",          # test/test_gradient.cpp:377-439
+    "3spheres_viscous",             # test/test_gradient.cpp:441-503
+    "sphere_plane_friction_mu01",   # test/test_gradient.cpp:156-213
+    "two_spheres_asymmetrical",     # test/test_sphere.cpp:341-380
+    "two_spheres_symmetrical",      # test/test_sphere.cpp:382-421
+    "2d_case_spheres",              # test/test_sphere.cpp:423-484
+    "obstacles_sphere_sphere_moving",  # test/test_obstacles.cpp:214-250
+]
+
+
+def main():
+    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    out = {}
+    for name in FILES:
+        with open(os.path.join(ref, "test", "references", name + ".json")) as fh:
+            d = json.load(fh)
+        objs = []
+        for o in d["objects"]:
+            p = o["properties"]
+            om = p["omega"]
+            objs.append({
+                "type": o["type"],
+                "active": p["active"],
+                "position": o["position"],
+                "quaternion": o["quaternion"],
+                "velocity": p["velocity"],
+                "omega": om if isinstance(om, list) else [om],
+            })
+        contacts = []
+        for c in d.get("contacts") or []:
+            contacts.append({k: c[k] for k in ("i", "j", "distance", "normal", "pi", "pj")})
+        out[name] = {"objects": objs, "contacts": contacts}
+    dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_states.json")
+    with open(dst, "w") as fh:
+        json.dump(out, fh, indent=1)
+    print("wrote", dst)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,237 @@
+"""Scenes of the reference's own solver tests, rebuilt with scopi_b200.container.
+
+Each builder returns ``(particles, solver_kwargs, dt, total_it)`` with the
+settings of the cited reference test (hpc-maths/scopi test/*.cpp).  The default
+solver parameters are the reference defaults: dmax 2, kd radius 17
+(contact_kdtree.hpp:229-237), apgd alpha 0.05, max_ite 10000, tol 1e-7, dynamic
+descent (apgd.hpp:120-123), mu 0.1, gamma 0 / -2 / 1e-6 (property.hpp:72,125-127).
+"""
+from __future__ import annotations
+
+import math
+
+from scopi_b200.container import Particles, Property, quaternion
+
+PI = math.pi
+NOFRICTION, FRICTION, VISCOUS = 0, 1, 2
+VAP_FIXED, VAP_FPD = 0, 1
+BRUTE_FORCE, KDTREE = 0, 1
+
+
+class MinstdRand0:
+    """std::minstd_rand0 (a=16807, m=2^31-1) with libstdc++'s uniform_real_distribution<double>.
+
+    libstdc++ generate_canonical<double, 53> draws k=2 values (log2 of the range
+    2^31-2 truncates to 30), accumulates (x-1)*r^i in double and divides by the
+    double-rounded r^2; the distribution returns canonical*(b-a)+a.
+    """
+
+    M = 2147483647
+
+    def __init__(self, seed: int):
+        self.x = seed % self.M or 1
+
+    def __call__(self) -> int:
+        self.x = (16807 * self.x) % self.M
+        return self.x
+
+    def uniform(self, a: float, b: float) -> float:
+        r = self.M - 1  # max - min + 1 = (2^31-2) - 1 + 1
+        s = float(self() - 1) * 1.0
+        s = s + float(self() - 1) * float(r)
+        tmp = float(r * r)  # r*r is exact in long double, rounded once to double
+        ret = s / tmp
+        if ret >= 1.0:
+            ret = math.nextafter(1.0, 0.0)
+        return ret * (b - a) + a
+
+
+def contacts_three_disks():
+    """test/test_contacts_kdtree.cpp:14-73 (kd radius 100) / test_contacts_brute_force.cpp:12-71."""
+    p = Particles(2)
+    p.add_sphere((0.0, 0.0), 0.1)
+    p.add_sphere((1.0, 1.0), 0.2)
+    p.add_sphere((5.0, 10.0), 0.1)
+    return p.finalize(), dict(kd_tree_radius=100.0), 0.0, 0
+
+
+def matrix_a_3d():
+    """test/test_matrices.cpp:17-45: two 3D spheres, brute-force contacts, A/A^T adjointness."""
+    p = Particles(3)
+    p.add_sphere((0.0, 0.0, 0.0), 0.1)
+    p.add_sphere((1.0, 1.0, 0.0), 0.2)
+    return p.finalize(), dict(contact_method=BRUTE_FORCE), 0.0, 0
+
+
+def matrix_a_case2():
+    """test/test_matrices.cpp:47-77: plane at pi/2-pi/4, sphere (2,1) r=0.5; A.u known values."""
+    p = Particles(2)
+    p.add_plane((0.0, 0.0), PI / 2 - PI / 4)
+    p.add_sphere((2.0, 1.0), 0.5, Property(mass=1, moment_inertia=0.1))
+    return p.finalize(), dict(contact_method=BRUTE_FORCE), 0.0, 0
+
+
+def three_spheres(problem=NOFRICTION):
+    """test/test_gradient.cpp:377-503 (NoFriction Tf=6, Viscous Tf=7; dt 0.1, vap_fpd, alpha 0.1)."""
+    p = Particles(2)
+    for (x, y) in ((-1.7, 1.3), (0.5, 1.7), (4.5, 1.3)):
+        p.add_sphere((x, y), 0.5, Property(mass=1, moment_inertia=1, force=(-x, -y)))
+    tf = 6.0 if problem == NOFRICTION else 7.0
+    dt = 0.1
+    kw = dict(problem=problem, vap=VAP_FPD, contact_method=KDTREE, tolerance=1e-7, max_ite=10000, alpha=0.1)
+    return p.finalize(), kw, dt, int(tf / dt)
+
+
+def sphere_plane_friction_mu01():
+    """test/test_gradient.cpp:156-213: Friction mu 0.1, dt 0.1, Tf 20."""
+    p = Particles(2)
+    p.add_plane((0.0, 0.0), PI / 2 - PI / 6)
+    dd, rr = 1.0, 2.0
+    p.add_sphere((0.0, (rr + dd) / math.cos(PI / 6)), rr, Property(mass=1, moment_inertia=0.5 * rr * rr, force=(0, -1)))
+    kw = dict(problem=FRICTION, vap=VAP_FPD, contact_method=KDTREE, tolerance=1e-7, max_ite=10000, alpha=0.1, mu=0.1)
+    dt = 0.1
+    return p.finalize(), kw, dt, int(20 / dt)
+
+
+def two_spheres(symmetric: bool, contact_method=KDTREE):
+    """test/test_sphere.cpp:341-421: vap_fixed, dt 0.005, 1000 steps, default solver."""
+    p = Particles(2)
+    dy = 0.0 if symmetric else 0.05
+    p.add_sphere((-0.2, -dy), 0.1, Property(mass=1.0, moment_inertia=0.1, desired_velocity=(0.25, 0)))
+    p.add_sphere((0.2, dy), 0.1, Property(mass=1.0, moment_inertia=0.1, desired_velocity=(-0.25, 0)))
+    return p.finalize(), dict(vap=VAP_FIXED, contact_method=contact_method), 0.005, 1000
+
+
+def critical_2d_spheres(contact_method=KDTREE):
+    """test/test_sphere.cpp:423-484: 18 disks from std::minstd_rand0(123), dt 0.01, 20 steps."""
+    n = 3
+    g = MinstdRand0(123)
+    p = Particles(2)
+    for i in range(n):
+        for j in range(n):
+            r = g.uniform(0.2, 0.4)
+            x = (i + 0.5) + g.uniform(-0.1, 0.1)
+            y = (j + 0.5) + g.uniform(-0.1, 0.1)
+            vel = g.uniform(2.0, 5.0)
+            p.add_sphere((x, y), r, Property(mass=1.0, moment_inertia=0.1, desired_velocity=(vel, 0.0)))
+            r = g.uniform(0.2, 0.4)
+            x = (n + i + 0.5) + g.uniform(-0.1, 0.1)
+            y = (j + 0.5) + g.uniform(-0.1, 0.1)
+            vel = g.uniform(2.0, 5.0)
+            p.add_sphere((x, y), r, Property(mass=1.0, moment_inertia=0.1, desired_velocity=(-vel, 0.0)))
+    return p.finalize(), dict(vap=VAP_FIXED, contact_method=contact_method), 0.01, 20
+
+
+def obstacle_sphere_plane(variant: str, contact_method=KDTREE):
+    """test/test_obstacles.cpp:43-98: sphere resting on plane(pi/2); variants fixed / velocity / force."""
+    p = Particles(2)
+    p.add_plane((0.0, 0.0), PI / 2.0)
+    prop = Property(mass=1.0, moment_inertia=0.1)
+    vap = VAP_FIXED
+    if variant == "velocity":
+        prop.desired_velocity = (0.0, -1.0)
+    elif variant == "force":
+        prop.force = (0.0, -1.0)
+        vap = VAP_FPD
+    p.add_sphere((0.0, 1.0), 1.0, prop)
+    return p.finalize(), dict(vap=vap, contact_method=contact_method), 0.005, 100
+
+
+def obstacle_sphere_sphere(variant: str, contact_method=KDTREE):
+    """test/test_obstacles.cpp:100-213: sphere on a fixed sphere; fixed / velocity / force / moving."""
+    p = Particles(2)
+    p.add_sphere((0.0, 0.0), 1.0, Property().deactivate())
+    prop = Property(mass=1.0, moment_inertia=0.1)
+    vap = VAP_FIXED
+    pos = (0.0, 2.0)
+    if variant == "velocity":
+        prop.desired_velocity = (0.0, -1.0)
+    elif variant == "force":
+        prop.force = (0.0, -1.0)
+        vap = VAP_FPD
+    elif variant == "moving":
+        pos = (1.0, math.sqrt(3.0))
+        prop.force = (0.0, -10.0)
+        vap = VAP_FPD
+    p.add_sphere(pos, 1.0, prop)
+    return p.finalize(), dict(vap=vap, contact_method=contact_method), 0.005, 100
+
+
+def sphere_inclined_plane(alpha: float, contact_method=KDTREE):
+    """test/test_obstacles.cpp:252-311: plane at pi/2-alpha, g=1, dt 0.01, 1000 steps, vap_fpd."""
+    radius, g, h = 1.0, 1.0, 2.0
+    p = Particles(2)
+    p.add_plane((0.0, 0.0), PI / 2.0 - alpha)
+    p.add_sphere((h * math.sin(alpha), h * math.cos(alpha)), radius,
+                 Property(mass=1.0, moment_inertia=1.0 * radius * radius / 2.0, force=(0.0, -g)))
+    return p.finalize(), dict(vap=VAP_FPD, contact_method=contact_method), 0.01, 1000
+
+
+def sphere_plane_analytic(problem=NOFRICTION):
+    """test/test_gradient.cpp:23-154: sphere on plane(pi/2), tilted gravity g(sin a, -cos a), a=pi/4."""
+    radius, g, h, alpha = 1.0, 1.0, 2.0, PI / 4
+    p = Particles(2)
+    p.add_plane((0.0, 0.0), PI / 2)
+    p.add_sphere((0.0, h), radius, Property(mass=1, moment_inertia=radius * radius / 2.0,
+                                            force=(g * math.sin(alpha), -g * math.cos(alpha))))
+    if problem == NOFRICTION:
+        kw = dict(problem=NOFRICTION, vap=VAP_FPD, tolerance=1e-7, max_ite=10000, alpha=0.01)
+        return p.finalize(), kw, 0.01, 1000
+    kw = dict(problem=VISCOUS, vap=VAP_FPD, tolerance=1e-7, max_ite=10000, alpha=0.1)
+    return p.finalize(), kw, 0.01, 500
+
+
+def analytic_no_friction(alpha, t, r, g, y0):
+    """test/analytical_solution.cpp:6-37."""
+    t_imp = math.sqrt(2 * (y0 - r) / (g * math.cos(alpha)))
+    if t < t_imp:
+        x = (g * t ** 2 * math.sin(alpha) / 2, -g * t ** 2 * math.cos(alpha) / 2 + y0)
+        v = (g * t * math.sin(alpha), -g * t * math.cos(alpha))
+    else:
+        x = (g * t ** 2 * math.sin(alpha) / 2, r)
+        v = (g * t * math.sin(alpha), 0.0)
+    return x, v
+
+
+def analytic_viscous(alpha, t, r, g, y0, gamma_min, t_inv):
+    """test/analytical_solution.cpp:39-124 (position and velocity)."""
+    t_imp = math.sqrt(2 * (y0 - r) / (g * math.cos(alpha)))
+    t_gmin = -gamma_min / (g * math.cos(alpha))
+    gamma_inv = gamma_min if t_inv > t_gmin else -g * t_inv * math.cos(alpha)
+    t_unstick = t_inv - gamma_inv / (g * math.cos(alpha))
+    sa, ca = math.sin(alpha), math.cos(alpha)
+    if t < t_imp:
+        return (g * t ** 2 * sa / 2, -g * t ** 2 * ca / 2 + y0), (g * t * sa, -g * t * ca)
+    if t < t_inv:
+        return (g * t ** 2 * sa / 2, r), (g * t * sa, 0.0)
+    xs = g * t_inv ** 2 * sa / 2 + g * t_inv * sa * (t - t_inv) - g * (t - t_inv) ** 2 * sa / 2
+    vx = g * t_inv * sa - g * (t - t_inv) * sa
+    if t < t_unstick:
+        return (xs, r), (vx, 0.0)
+    return (xs, r + g * (t - t_unstick) ** 2 * ca / 2), (vx, g * (t - t_unstick) * ca)
+
+
+def analytic_inclined(alpha, mu, t, r, g, y0):
+    """test/utils.cpp:77-139 (position, theta) and velocity."""
+    t_imp = math.sqrt(2 * (y0 - r) / (g * math.cos(alpha)))
+    sa, ca = math.sin(alpha), math.cos(alpha)
+    if t > t_imp:
+        vtm = g * t_imp * sa
+        vnm = -g * t_imp * ca
+        t2 = t - t_imp
+        x_imp = g * sa * t_imp * t_imp / 2.0
+        if math.tan(alpha) <= 3 * mu:
+            xn = g * sa * t2 * t2 / 3.0 + 2.0 * vtm * t2 / 3.0 + x_imp
+            theta = -g * sa * t2 * t2 / (3.0 * r) - 2 * vtm * t2 / (3.0 * r)
+            vn = 2.0 * g * sa * t2 / 3.0 + 2.0 * vtm / 3.0
+        else:
+            xn = g * (sa - mu * ca) * t2 * t2 / 2.0 + (vtm + mu * vnm) * t2 + x_imp
+            theta = -mu * g * ca * t2 * t2 / r + 2 * mu * vnm * t2 / r
+            vn = g * (sa - mu * ca) * t2 + (vtm + mu * vnm)
+        x = (xn * ca + r * sa, -xn * sa + r * ca)
+        v = (vn * ca, -vn * sa)
+        return x, theta, v
+    return (y0 * sa, y0 * ca - g * t * t / 2.0), 0.0, (0.0, -g * t)
+
+
+__all__ = ["quaternion"]

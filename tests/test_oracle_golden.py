@@ -1,0 +1,196 @@
+"""Pin the CPU oracle against the reference's own golden files and known answers.
+
+Every case is a reference test (cited per test); tolerances are the reference's
+(test/utils.hpp:16 tolerance=1e-6, test/test_gradient.cpp:19 tol=1e-5,
+doctest::Approx relative 1.2e-5).  These run without a GPU.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import py_oracle as orc
+import scenes as S
+
+APPROX = 1.1920929e-07 * 100  # doctest::Approx default epsilon (FLT_EPSILON * 100)
+
+
+def approx(a, b, eps=APPROX):
+    return abs(a - b) <= eps * (1 + max(abs(a), abs(b)))
+
+
+def run_oracle(scene, steps=None):
+    pa, kw, dt, total = scene
+    s = orc.OracleSolver(pa, **kw)
+    s.run(dt, total if steps is None else steps)
+    return s
+
+
+def compare_objects(state, gold_objs, dim, tol):
+    worst = 0.0
+    for k, o in enumerate(gold_objs):
+        for d in range(dim):
+            worst = max(worst, abs(state.pos[k, d] - o["position"][d]))
+            worst = max(worst, abs(state.v[k, d] - o["velocity"][d]))
+        om = o["omega"]
+        if dim == 2:
+            worst = max(worst, abs(state.omega[k, 2] - om[0]))
+        else:
+            for d in range(3):
+                worst = max(worst, abs(state.omega[k, d] - om[d]))
+        for d in range(4):
+            worst = max(worst, abs(state.q[k, d] - o["quaternion"][d]))
+    assert worst <= tol, f"max abs deviation {worst:.3e} > {tol}"
+    return worst
+
+
+@pytest.mark.parametrize("method", [S.KDTREE, S.BRUTE_FORCE])
+def test_contacts_three_disks(method):
+    """test/test_contacts_kdtree.cpp:14-73, test/test_contacts_brute_force.cpp:12-71."""
+    pa, kw, _, _ = S.contacts_three_disks()
+    kw = dict(kw, contact_method=method)
+    c = orc.OracleSolver(pa, **kw).detect()
+    assert len(c["i"]) == 1 and c["i"][0] == 0 and c["j"][0] == 1
+    assert approx(c["dij"][0], math.sqrt(2.0) - 0.1 - 0.2)
+    assert approx(c["nij"][0, 0], -1 / math.sqrt(2.0)) and approx(c["nij"][0, 1], -1 / math.sqrt(2.0))
+    assert approx(c["pi"][0, 0], 0.1 * math.sqrt(2.0) / 2.0) and approx(c["pi"][0, 1], 0.1 * math.sqrt(2.0) / 2.0)
+    assert approx(c["pj"][0, 0], 1 - 0.2 * math.sqrt(2.0) / 2.0) and approx(c["pj"][0, 1], 1 - 0.2 * math.sqrt(2.0) / 2.0)
+
+
+def test_matrix_a_adjoint():
+    """test/test_matrices.cpp:17-45: dot(A u, f) == dot(u, A^T f)."""
+    pa, kw, _, _ = S.matrix_a_3d()
+    s = orc.OracleSolver(pa, **kw)
+    s.detect()
+    rng = np.random.default_rng(0)
+    u = rng.random(6 * 2)
+    f = rng.random(3 * 1)
+    assert approx(float(np.dot(s.amat(u), f)), float(np.dot(u, s.atmat(f))))
+
+
+def test_matrix_a_case2():
+    """test/test_matrices.cpp:47-77: sphere on a 45-degree plane, known A.u values."""
+    pa, kw, _, _ = S.matrix_a_case2()
+    s = orc.OracleSolver(pa, **kw)
+    c = s.detect()
+    assert len(c["i"]) == 1
+    u = np.array([0.187562190766376, -1.184390935327111, 0., 0., 0., -0.00453709103433])
+    sol = s.amat(u)
+    assert approx(sol[0], -0.18595809) and approx(sol[1], 1.18278683)
+
+
+@pytest.mark.parametrize("name,problem", [("3spheres_nofriction", S.NOFRICTION), ("3spheres_viscous", S.VISCOUS)])
+def test_three_spheres_golden(golden, name, problem):
+    """test/test_gradient.cpp:377-503 against test/references/3spheres_*.json (tol 1e-5)."""
+    s = run_oracle(S.three_spheres(problem))
+    compare_objects(s.pa, golden[name]["objects"], 2, 1e-5)
+
+
+def test_sphere_plane_friction_golden(golden):
+    """test/test_gradient.cpp:156-213 against sphere_plane_friction_mu01.json (tol 1e-5)."""
+    s = run_oracle(S.sphere_plane_friction_mu01())
+    compare_objects(s.pa, golden["sphere_plane_friction_mu01"]["objects"], 2, 1e-5)
+
+
+@pytest.mark.parametrize("method", [S.KDTREE, S.BRUTE_FORCE])
+@pytest.mark.parametrize("sym", [False, True])
+def test_two_spheres_golden(golden, sym, method):
+    """test/test_sphere.cpp:341-421 against two_spheres_*.json (tol 1e-6)."""
+    s = run_oracle(S.two_spheres(sym, method))
+    name = "two_spheres_symmetrical" if sym else "two_spheres_asymmetrical"
+    compare_objects(s.pa, golden[name]["objects"], 2, 1e-6)
+
+
+@pytest.mark.parametrize("method", [S.KDTREE, S.BRUTE_FORCE])
+def test_critical_2d_golden(golden, method):
+    """test/test_sphere.cpp:423-484 against 2d_case_spheres.json (tol 1e-6), with its contact list."""
+    scene = S.critical_2d_spheres(method)
+    s = run_oracle(scene, steps=scene[3] - 1)
+    c = s.detect()  # the snapshot's contacts are those of the last step
+    gold = golden["2d_case_spheres"]
+    gi = [(g["i"], g["j"]) for g in gold["contacts"]]
+    assert list(zip(c["i"].tolist(), c["j"].tolist())) == gi
+    for k, g in enumerate(gold["contacts"]):
+        assert abs(c["dij"][k] - g["distance"]) < 1e-6
+        for d in range(2):
+            assert abs(c["nij"][k, d] - g["normal"][d]) < 1e-6
+            assert abs(c["pi"][k, d] - g["pi"][d]) < 1e-6
+            assert abs(c["pj"][k, d] - g["pj"][d]) < 1e-6
+    s = run_oracle(scene)
+    compare_objects(s.pa, gold["objects"], 2, 1e-6)
+
+
+@pytest.mark.parametrize("method", [S.KDTREE, S.BRUTE_FORCE])
+@pytest.mark.parametrize("variant", ["fixed", "velocity", "force"])
+def test_obstacle_sphere_plane(variant, method):
+    """test/test_obstacles.cpp:14-98: the sphere stays at (0, 1) on plane(pi/2)."""
+    s = run_oracle(S.obstacle_sphere_plane(variant, method))
+    pos, q = s.pa.pos, s.pa.q
+    assert approx(pos[0, 0], 0) and approx(pos[0, 1], 0) and approx(pos[1, 0], 0) and approx(pos[1, 1], 1)
+    assert approx(q[0, 0], math.sqrt(2) / 2) and approx(q[0, 3], math.sqrt(2) / 2)
+    assert approx(q[1, 0], 1) and approx(q[1, 3], 0)
+
+
+@pytest.mark.parametrize("method", [S.KDTREE, S.BRUTE_FORCE])
+@pytest.mark.parametrize("variant", ["fixed", "velocity", "force"])
+def test_obstacle_sphere_sphere(variant, method):
+    """test/test_obstacles.cpp:100-212: the sphere stays at (0, 2) on the fixed sphere."""
+    s = run_oracle(S.obstacle_sphere_sphere(variant, method))
+    pos, q = s.pa.pos, s.pa.q
+    assert approx(pos[0, 0], 0) and approx(pos[0, 1], 0) and approx(pos[1, 0], 0) and approx(pos[1, 1], 2)
+    assert approx(q[1, 0], 1) and approx(q[1, 3], 0)
+
+
+@pytest.mark.parametrize("method", [S.KDTREE, S.BRUTE_FORCE])
+def test_obstacle_sphere_sphere_moving(golden, method):
+    """test/test_obstacles.cpp:214-250 against obstacles_sphere_sphere_moving.json (tol 1e-6)."""
+    s = run_oracle(S.obstacle_sphere_sphere("moving", method))
+    compare_objects(s.pa, golden["obstacles_sphere_sphere_moving"]["objects"], 2, 1e-6)
+
+
+@pytest.mark.parametrize("alpha,e_pos,e_q,e_v", [(math.pi / 6, 0.000998789, 0.0, 0.0010002),
+                                                  (math.pi / 4, 0.00100008, 0.0, 0.00100119),
+                                                  (math.pi / 3, 0.00100105, 0.0, 0.0010027)])
+def test_sphere_inclined_plane(alpha, e_pos, e_q, e_v):
+    """test/test_obstacles.cpp:252-311: pinned relative errors against the analytic solution."""
+    scene = S.sphere_inclined_plane(alpha)
+    s = run_oracle(scene)
+    dt, total = scene[2], scene[3]
+    x, theta, v = S.analytic_inclined(alpha, 0.0, dt * (total + 1), 1.0, 1.0, 2.0)
+    qa = S.quaternion(theta)
+    pos = s.pa.pos[1, :2]
+    err_pos = np.linalg.norm(pos - x) / np.linalg.norm(x)
+    err_q = np.linalg.norm(s.pa.q[1] - qa) / np.linalg.norm(qa)
+    err_v = np.linalg.norm(s.pa.v[1, :2] - v) / np.linalg.norm(v)
+    assert approx(err_pos, e_pos)
+    assert approx(err_q, e_q)
+    assert abs(err_v - e_v) <= 1e-4 * (1 + max(abs(err_v), abs(e_v)))
+    assert approx(s.pa.omega[1, 2], 0.0)
+
+
+def test_sphere_plane_no_friction_analytic():
+    """test/test_gradient.cpp:23-80: errors vs the analytic solution (pos/q 1e-3, v 1e-12)."""
+    scene = S.sphere_plane_analytic(S.NOFRICTION)
+    s = run_oracle(scene)
+    t = scene[2] * scene[3]
+    x, v = S.analytic_no_friction(math.pi / 4, t, 1.0, 1.0, 2.0)
+    assert np.linalg.norm(s.pa.pos[1, :2] - x) / np.linalg.norm(x) <= 1e-3
+    assert np.linalg.norm(s.pa.q[1] - S.quaternion(0.0)) <= 1e-3
+    assert np.linalg.norm(s.pa.v[1, :2] - v) / np.linalg.norm(v) <= 1e-12 * (1 + APPROX)
+    assert approx(s.pa.omega[1, 2], 0.0)
+
+
+def test_sphere_plane_viscous_analytic():
+    """test/test_gradient.cpp:82-154: two runs (force flipped), errors vs analytic (1e-3)."""
+    pa, kw, dt, total = S.sphere_plane_analytic(S.VISCOUS)
+    s = orc.OracleSolver(pa, **kw)
+    s.run(dt, total)
+    g, alpha = 1.0, math.pi / 4
+    p2 = s.pa.copy()
+    p2.f[1, :2] = (-g * math.sin(alpha), g * math.cos(alpha))
+    s.set_particles(p2)
+    s.run(dt, 500)
+    x, v = S.analytic_viscous(alpha, dt * (total + 500), 1.0, g, 2.0, -2.0, dt * total)
+    assert np.linalg.norm(s.pa.pos[1, :2] - x) / np.linalg.norm(x) <= 1e-3
+    assert np.linalg.norm(s.pa.v[1, :2] - v) / np.linalg.norm(v) <= 1e-3
+    assert approx(s.pa.omega[1, 2], 0.0)
