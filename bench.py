@@ -1,0 +1,421 @@
+#!/usr/bin/env python
+"""Time steps/s of the SCoPI time step on B200 at 1M spheres.
+
+Workload (N=1): 1,000,000 spheres on a jittered 100^3 lattice in the unit box with six
+plane walls, inward desired velocity 0.1 (vap_fixed), NoFriction, dmax 0.0018,
+dt 1e-3, APGD tol 1e-6 / max_ite 40000 (scopi_b200.configs.spheres_1m).  A step is one
+full ScopiSolver time step: obstacle motion, contact detection, assembly, APGD,
+velocity and position/quaternion update.  The headline arm is the mixed form (FP32
+APGD iterations + FP64 outer correction to violation <= 1e-6); the plain FP64 form is
+timed on the same steps from the same state and reported beside it.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N>1 runs under torchrun, one independent replica per GPU (the solve has no data-path
+exchange), timed on the device and reduced as the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "time steps/s at 1M spheres (mixed FP32-APGD + FP64 correction, violation <= 1e-6)"
+UNIT = "steps/s"
+WORKLOAD = "spheres_1m"
+
+
+def env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+def roofline_bytes_per_iter(C, N, s, dim=3):
+    """Algorithmic bytes of one APGD iteration (accepted step, no backtracks).
+
+    3D: 3 passes over compressed B (9 values + 2 int32 indices per contact), 6 contact
+    vector streams, 4 particle vector streams of 6N entries.  2D: 4 values, 3N slots.
+    """
+    if dim == 3:
+        return 3 * C * (9 * s + 8) + 6 * C * s + 4 * (6 * N) * s
+    return 3 * C * (4 * s + 8) + 6 * C * s + 4 * (3 * N) * s
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons, power = [], None, set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm), "power_w_max": max(power) if power else None}
+
+
+# ----------------------------------------------------------------------------- ranks
+class Ranks:
+    def __init__(self, n_gpus):
+        self.world = env_int("WORLD_SIZE", 1)
+        self.rank = env_int("RANK", 0)
+        self.local = env_int("LOCAL_RANK", 0)
+        self.n_gpus = n_gpus
+        self.pg = False
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+            if torch.cuda.is_available():
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+            self.pg = True
+
+    def barrier(self):
+        if self.pg:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        import torch.distributed as dist
+        dev = "cuda" if torch.cuda.is_available() else "cpu"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+# ----------------------------------------------------------------------------- GPU arm
+def solver_kwargs():
+    from scopi_b200 import configs
+    st = configs.SETTINGS[WORKLOAD]
+    return dict(dmax=st["dmax"], tolerance=st["tolerance"], max_ite=st["max_ite"], vap=st["vap"]), st["dt"]
+
+
+def time_path(pa, precision, steps, warmup, ranks, sampler=None):
+    import torch
+
+    from scopi_b200 import ScopiSolver
+    kw, dt = solver_kwargs()
+    s = ScopiSolver(pa, precision=precision, mixed_violation_tol=1e-6, device=ranks.local, **kw)
+    s.step(dt, warmup)
+    stream = torch.cuda.ExternalStream(s.stream_handle(), device=ranks.local)
+    torch.cuda.synchronize()
+    ranks.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    l0 = s.kernel_launches()
+    if sampler:
+        sampler.start()
+    per = []
+    e0.record(stream)
+    for _ in range(steps):
+        s.step(dt, 1)
+        per.append(s.stats())
+    e1.record(stream)
+    e1.synchronize()
+    clocks = sampler.stop() if sampler else None
+    torch.cuda.synchronize()
+    ranks.barrier()
+    ms = e0.elapsed_time(e1)
+    launches = s.kernel_launches() - l0
+    s.close()
+    return {"ms": ms, "per_step": per, "launches": launches, "clocks": clocks}
+
+
+def time_e2e(pa, precision, steps, warmup, ranks):
+    """Same steps through the C ABI with host buffers: upload, step, download every step."""
+    import numpy as np
+    import torch
+
+    from scopi_b200 import ScopiSolver
+    kw, dt = solver_kwargs()
+
+    def pinned(a):
+        t = torch.empty(a.shape, dtype=torch.float64 if a.dtype == np.float64 else torch.int32, pin_memory=True)
+        out = t.numpy()
+        out[...] = a
+        return out, t
+
+    keep = []
+    host = pa.copy()
+    for k in ("shape", "pos", "q", "v", "omega", "vd", "omega_d", "f", "m", "j", "radius", "length"):
+        arr, t = pinned(getattr(host, k))
+        keep.append(t)
+        setattr(host, k, arr)
+    s = ScopiSolver(host, precision=precision, mixed_violation_tol=1e-6, device=ranks.local, **kw)
+    s.step(dt, warmup)
+    s.download(host)
+    stream = torch.cuda.ExternalStream(s.stream_handle(), device=ranks.local)
+    torch.cuda.synchronize()
+    ranks.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        s.upload(host)
+        s.step(dt, 1)
+        s.download(host)
+    e1.record(stream)
+    e1.synchronize()
+    ranks.barrier()
+    ms = e0.elapsed_time(e1)
+    n = host.n
+    h2d = 4 * n + 8 * n * (3 + 4 + 3 + 3 + 3 + 3 + 3 + 1 + 3 + 1 + 1)
+    d2h = 8 * n * (3 + 4 + 3 + 3)
+    s.close()
+    return ms, h2d, d2h
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per APGD iteration per contact from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "apgd_dram_traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as fh:
+        return json.load(fh)
+
+
+# ----------------------------------------------------------------------------- CPU legs
+def cpu_sample(pa, iterations_per_step, threads):
+    """Oracle (CPU restatement of the reference path) on the full workload.
+
+    Two time steps from the same state with the APGD loop capped at 1 and at 3
+    iterations: t_per_iteration = (solve_3 - solve_1) / 2; everything else (detection,
+    problem build, velocity recovery, update) is t_fixed; steps/s is rebuilt as
+    1 / (t_fixed + t_per_iteration * iterations_per_step)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import py_oracle as orc
+    kw, dt = solver_kwargs()
+    out = {}
+    t0 = time.perf_counter()
+    for cap in (1, 3):
+        o = orc.OracleSolver(pa, **dict(kw, max_ite=cap, num_threads=threads))
+        o.run(dt, 1)
+        out[cap] = o.stats()
+        del o
+    wall = time.perf_counter() - t0
+    d_it = max(1, out[3]["iterations"] - out[1]["iterations"])
+    t_iter = max(1e-9, (out[3]["seconds_solve"] - out[1]["seconds_solve"]) / d_it)
+    t_fixed = out[1]["seconds_contacts"] + out[1]["seconds_other"] + max(0.0, out[1]["seconds_solve"] - t_iter)
+    est = 1.0 / (t_fixed + t_iter * iterations_per_step)
+    return {"value": est, "t_per_iteration_s": t_iter, "t_outside_apgd_s": t_fixed, "wall_s": wall,
+            "contacts": out[3]["contacts"], "iterations_timed": out[1]["iterations"] + out[3]["iterations"]}
+
+
+def reference_arm(args, ranks):
+    """--impl reference: the CPU restatement of the reference path on the host cores."""
+    if ranks.rank != 0:
+        return 0
+    from scopi_b200 import configs
+    threads = os.cpu_count() or 1
+    pa = configs.spheres_1m()
+    iters = REF_APGD_ITERATIONS_DEFAULT
+    samples = []
+    for k in range(args.warmup + args.steps):
+        r = cpu_sample(pa, iters, threads)
+        if k >= args.warmup:
+            samples.append(r)
+    value = statistics.median(r["value"] for r in samples)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD + ": 1,000,000 spheres, NoFriction, vap_fixed, dmax 0.0018, dt 1e-3, tol 1e-6"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": (f"oracle (C++ restatement of the reference path, OpenMP on the loops the reference "
+                                    f"parallelises, serial APGD) on the full 1M-sphere step, APGD capped at 1 and 3 "
+                                    f"iterations; steps/s = 1/(t_outside_apgd + t_per_iteration * {iters}), "
+                                    f"{iters} = FP64 APGD iterations per step of this workload measured on B200")},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "samples": samples,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# mean FP64 APGD iterations per step of spheres_1m measured on B200 with the FP64 path
+# (the reference's algorithm and tolerance): 505 and 489 on the first two steps
+REF_APGD_ITERATIONS_DEFAULT = 497
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--side", type=int, default=100)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 0)
+    ranks = Ranks(args.gpus)
+    try:
+        if args.impl == "reference":
+            return reference_arm(args, ranks)
+        return ours(args, ranks)
+    finally:
+        ranks.close()
+
+
+def ours(args, ranks):
+    import torch
+    if not torch.cuda.is_available():
+        print(json.dumps({"error": "no CUDA device"}))
+        return 1
+    from scopi_b200 import FP64, MIXED, configs
+    from scopi_b200.build import build
+    build()
+    pa = configs.spheres_1m(side=args.side)
+    n_active = pa.n - pa.nb_inactive
+    sampler = ClockSampler(ranks.local)
+    mixed = time_path(pa, MIXED, args.steps, args.warmup, ranks, sampler)
+    f64 = None if args.no_fp64 else time_path(pa, FP64, args.steps, args.warmup, ranks)
+    e2e_ms, h2d, d2h = time_e2e(pa, MIXED, args.steps, args.warmup, ranks)
+
+    ms = ranks.max(mixed["ms"])
+    value = args.gpus * args.steps * 1000.0 / ms if ranks.world > 1 else args.steps * 1000.0 / ms
+    e2e_ms = ranks.max(e2e_ms)
+    e2e_val = (ranks.world * args.steps * 1000.0 / e2e_ms)
+    f64_val = None
+    if f64:
+        f64_ms = ranks.max(f64["ms"])
+        f64_val = ranks.world * args.steps * 1000.0 / f64_ms
+
+    # roofline of the dominant kernel: the persistent APGD launches (FP32 in the mixed form)
+    per = mixed["per_step"]
+    C = statistics.mean(p["contacts"] for p in per)
+    it32 = sum(p["fp32_iterations"] for p in per)
+    ms_apgd = sum(p["ms_apgd_kernel"] for p in per)
+    b_iter32 = roofline_bytes_per_iter(C, n_active, 4)
+    achieved = (it32 * b_iter32) / (ms_apgd * 1e-3) / 1e9 if ms_apgd > 0 else None
+    peak, peak_kind = measured_peaks()
+    traffic = None
+    prof = profiled_traffic()
+    if prof and it32:
+        traffic = prof.get("dram_bytes_per_iteration_per_contact_fp32", 0) * C * (it32 / max(1, len(per)))
+    f64_roof = None
+    if f64:
+        p64 = f64["per_step"]
+        it64 = sum(p["iterations"] for p in p64)
+        ms64 = sum(p["ms_apgd_kernel"] for p in p64)
+        a64 = (it64 * roofline_bytes_per_iter(C, n_active, 8)) / (ms64 * 1e-3) / 1e9 if ms64 > 0 else None
+        f64_roof = {"achieved": a64, "peak": peak, "unit": "GB/s", "frac": (a64 / peak) if a64 else None,
+                    "iterations_per_step": it64 / len(p64), "ms_apgd_per_step": ms64 / len(p64),
+                    "violation_max": max(p["violation"] for p in p64)}
+
+    cpu = None
+    if not args.no_cpu_baseline and ranks.rank == 0 and args.side == 100:
+        iters = (f64_roof["iterations_per_step"] if f64_roof else REF_APGD_ITERATIONS_DEFAULT)
+        threads = os.cpu_count() or 1
+        r = cpu_sample(pa, iters, threads)
+        cpu = {"value": r["value"], "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": (f"oracle on the full 1M-sphere step, APGD capped at 1 and 3 iterations "
+                          f"({r['wall_s']:.1f} s wall); steps/s = 1/(t_outside_apgd "
+                          f"{r['t_outside_apgd_s']:.2f} s + t_per_iteration {r['t_per_iteration_s']:.3f} s * "
+                          f"{iters:.0f} FP64 iterations per step measured on the GPU)"),
+               "t_per_iteration_s": r["t_per_iteration_s"], "t_outside_apgd_s": r["t_outside_apgd_s"]}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 APGD iterations, f64 correction/geometry/integration",
+        "data": "synthetic",
+        "config": {"workload": (f"{WORKLOAD}: {n_active:,} spheres ({args.side}^3 jittered lattice, spacing 0.0045, "
+                                f"r U[0.9,1.1]*0.002) + 6 plane walls, NoFriction, vap_fixed, dmax 0.0018, dt 1e-3, "
+                                f"APGD tol 1e-6, mixed violation target 1e-6"),
+                   "precision": "mixed", "l2": "inputs larger than L2 (contact arrays > 1 GB per step)",
+                   "parallelism": f"replicas x{ranks.world}" if ranks.world > 1 else "single GPU"},
+        "fp64": {"value": f64_val, "unit": UNIT, "mixed_over_fp64": (value / f64_val) if f64_val else None,
+                 "roofline": f64_roof},
+        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                     "peak_source": f"{peak_kind} hbm_gbs", "kernel": "k_apgd<float,3,NoFriction> (persistent)",
+                     "bytes_per_iteration": b_iter32, "iterations_per_step": it32 / len(per),
+                     "ms_apgd_per_step": ms_apgd / len(per)},
+        "cpu_baseline": cpu,
+        "clocks": mixed["clocks"],
+        "gpu_launches": mixed["launches"],
+        "solver": {"contacts": C, "violation_max": max(p["violation"] for p in per),
+                   "corrections_per_step": sum(p["corrections"] for p in per) / len(per),
+                   "converged_all": all(p["converged"] for p in per)},
+    }
+    if ranks.rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

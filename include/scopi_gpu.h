@@ -1,0 +1,166 @@
+/*
+ * scopi_gpu.h -- C ABI of the B200 (sm_100a) SCoPI time-step engine.
+ *
+ * One handle = one ScopiSolver<dim, problem, OptimGradient<apgd>, contact, vap>
+ * (include/scopi/solver.hpp:91-206 of hpc-maths/scopi v0.1.0) whose particles
+ * live in GPU memory.  A step runs, on the device: obstacle motion, contact
+ * detection (uniform-grid cell list, contact set identical to the reference's
+ * kd-tree / brute force), closest points and contact-Jacobian assembly, the
+ * APGD solve (FP64, or FP32 iterations with an FP64 outer correction), the
+ * velocity update and the position/quaternion integration.
+ *
+ * Conventions: plain C types only, no exceptions across the ABI; every function
+ * returns 0 on success or a negative SCOPI_GPU_E* code, and scopi_gpu_last_error()
+ * gives a message.  The caller owns host buffers; the handle owns device memory
+ * and one CUDA stream.  One host thread per handle.
+ *
+ * Particle layout (host and device): every vector has 3 slots per body.  In 2D the
+ * z slot of pos/v/vd/f is 0 and the scalar rotation quantities (omega, desired
+ * omega, moment of inertia) live in the z slot.  Quaternions are (w, x, y, z).
+ * Obstacles (inactive bodies) come first, as scopi_container requires
+ * (include/scopi/container.hpp:365-373).
+ */
+#ifndef SCOPI_GPU_H
+#define SCOPI_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* error codes */
+#define SCOPI_GPU_OK 0
+#define SCOPI_GPU_EINVAL -1      /* bad argument */
+#define SCOPI_GPU_ECUDA -2       /* CUDA runtime error (message in last_error) */
+#define SCOPI_GPU_ENOMEM -3      /* device allocation failed */
+#define SCOPI_GPU_EUNSUPPORTED -4 /* shape pair / option the reference does not implement */
+#define SCOPI_GPU_ETIMEOUT -5    /* a device-side bounded wait gave up (grid barrier) */
+#define SCOPI_GPU_ENOCONV 1      /* positive: APGD reached max_ite ("APGD didn't converge.") */
+
+/* problem_t (include/scopi/contact/property.hpp:14-36) */
+#define SCOPI_GPU_NOFRICTION 0
+#define SCOPI_GPU_FRICTION 1
+#define SCOPI_GPU_VISCOUS 2
+/* vap policies (include/scopi/vap/vap_fixed.hpp, vap_fpd.hpp) */
+#define SCOPI_GPU_VAP_FIXED 0
+#define SCOPI_GPU_VAP_FPD 1
+/* contact policies (contact/contact_brute_force.hpp, contact/contact_kdtree.hpp) */
+#define SCOPI_GPU_BRUTE_FORCE 0
+#define SCOPI_GPU_KDTREE 1
+/* precision of the APGD iterations */
+#define SCOPI_GPU_FP64 0
+#define SCOPI_GPU_MIXED 1
+/* shapes */
+#define SCOPI_GPU_SPHERE 0
+#define SCOPI_GPU_PLANE 1
+#define SCOPI_GPU_SEGMENT 2
+
+typedef struct scopi_gpu_params {
+    int32_t dim;              /* 2 or 3 */
+    int32_t problem;          /* SCOPI_GPU_NOFRICTION / FRICTION / VISCOUS */
+    int32_t vap;              /* SCOPI_GPU_VAP_FIXED / VAP_FPD */
+    int32_t contact_method;   /* SCOPI_GPU_BRUTE_FORCE / KDTREE */
+    int32_t precision;        /* SCOPI_GPU_FP64 / SCOPI_GPU_MIXED */
+    int32_t dynamic_descent;  /* apgd_params::dynamic_descent (apgd.hpp:123) */
+    int64_t max_ite;          /* apgd_params::max_ite (apgd.hpp:121) */
+    double dmax;              /* ContactsParams::dmax (contact_kdtree.hpp:229) */
+    double kd_tree_radius;    /* ContactsParams::kd_tree_radius, squared (contact_kdtree.hpp:237) */
+    double alpha;             /* apgd_params::alpha (apgd.hpp:120) */
+    double tolerance;         /* apgd_params::tolerance (apgd.hpp:122) */
+    double mu;                /* contact_property<Friction>::mu (property.hpp:72) */
+    double gamma;             /* contact_property<Viscous> (property.hpp:125-127) */
+    double gamma_min;
+    double gamma_tol;
+    double mixed_violation_tol;   /* MIXED: FP64 constraint violation the outer correction must reach */
+    int32_t mixed_max_corrections;/* MIXED: FP32 correction solves after the first one */
+    int32_t device;               /* CUDA device ordinal */
+} scopi_gpu_params;
+
+typedef struct scopi_gpu_particles {
+    int64_t n;           /* bodies */
+    int64_t nb_inactive; /* obstacles first */
+    int32_t* shape;      /* n: SCOPI_GPU_SPHERE / PLANE / SEGMENT */
+    double* pos;         /* n*3 */
+    double* q;           /* n*4 */
+    double* v;           /* n*3 */
+    double* omega;       /* n*3 */
+    double* vd;          /* n*3 */
+    double* omega_d;     /* n*3 */
+    double* f;           /* n*3 */
+    double* m;           /* n */
+    double* j;           /* n*3 */
+    double* radius;      /* n (sphere radius) */
+    double* length;      /* n (segment length) */
+} scopi_gpu_particles;
+
+typedef struct scopi_gpu_stats {
+    int64_t contacts;        /* contacts of the last step */
+    int64_t iterations;      /* APGD iterations of the last step (all solves) */
+    int64_t backtracks;      /* Lipschitz doublings */
+    int64_t restarts;        /* gradient restarts */
+    int64_t fp32_iterations; /* MIXED: iterations run in FP32 */
+    int64_t corrections;     /* MIXED: FP32 correction solves */
+    int32_t converged;       /* 1 if the stopping test was met */
+    int32_t status;          /* SCOPI_GPU_OK / ENOCONV / ETIMEOUT of the last step */
+    double violation;        /* max_c max(0, -(d_c + dt n_c.(A u)_c)) after the solve (FP64) */
+    double ms_step;          /* device time of the last step (CUDA events) */
+    double ms_solve;         /* device time of the APGD part of the last step */
+    double ms_apgd_kernel;   /* device time of the persistent APGD launches of the last step */
+    int64_t steps;           /* steps run by this handle */
+} scopi_gpu_stats;
+
+typedef struct scopi_gpu_handle scopi_gpu_handle;
+
+/* Reference defaults: apgd (0.05, 10000, 1e-7, true), dmax 2, kd radius 17, mu 0.1,
+   gamma (0, -2, 1e-6), NoFriction, vap_fixed, kd-tree, FP64. */
+void scopi_gpu_default_params(scopi_gpu_params* p, int32_t dim);
+
+/* ScopiSolver(particles) constructor, solver.hpp:117-126, with the policies' params
+   (apgd.hpp:105-124, contact_kdtree.hpp:203-238, property.hpp:41-128). */
+int32_t scopi_gpu_create(const scopi_gpu_params* p, scopi_gpu_handle** out);
+int32_t scopi_gpu_destroy(scopi_gpu_handle* h);
+
+/* Upload / download the whole container (scopi_container::push_back, container.hpp:339-384,
+   and the pos()/q()/v()/omega() accessors).  set_particles keeps the previous contacts
+   (and their viscous gamma) so a run can continue after changing forces. */
+int32_t scopi_gpu_set_particles(scopi_gpu_handle* h, const scopi_gpu_particles* parts);
+int32_t scopi_gpu_get_particles(scopi_gpu_handle* h, scopi_gpu_particles* out);
+
+/* ScopiSolver::run(dt, total_it, initial_iter), solver.hpp:267-303 (output disabled). */
+int32_t scopi_gpu_run(scopi_gpu_handle* h, double dt, int64_t total_it, int64_t initial_iter);
+
+/* contact_base::run (contact/base.hpp:71-77) on the current state; returns the count in *n. */
+int32_t scopi_gpu_detect(scopi_gpu_handle* h, int64_t* n);
+
+/* ScopiSolver::current_contacts (solver.hpp:314-317): the last step's contacts, sorted by (i, j).
+   Any pointer may be NULL. nij/pi/pj are cap*3. */
+int32_t scopi_gpu_get_contacts(scopi_gpu_handle* h, int64_t cap, int64_t* n, int64_t* ci, int64_t* cj,
+                               double* dij, double* nij, double* pi, double* pj, double* gamma);
+
+/* OptimGradient::lagrange_multiplier (OptimGradient.hpp:323-326), reference local layout. */
+int32_t scopi_gpu_get_lambda(scopi_gpu_handle* h, int64_t cap, int64_t* n, double* lambda);
+
+int32_t scopi_gpu_get_stats(scopi_gpu_handle* h, scopi_gpu_stats* out);
+
+/* AMatrix::mat_mult / ATMatrix::mat_mult (matrix/velocities.hpp:67-144, 167-254) on the
+   current contact list: u is 6*nb_active, f is 3*contacts. */
+int32_t scopi_gpu_amat(scopi_gpu_handle* h, const double* u, double* out);
+int32_t scopi_gpu_atmat(scopi_gpu_handle* h, const double* f, double* out);
+
+/* Message of the last failing call on this handle (or of the last failing create). */
+const char* scopi_gpu_last_error(scopi_gpu_handle* h);
+
+/* Number of kernels this library launched on the handle's stream so far. */
+int64_t scopi_gpu_kernel_launches(scopi_gpu_handle* h);
+
+/* The handle's CUDA stream (a cudaStream_t), so callers can order their own work and
+   time the engine with CUDA events recorded on the stream its kernels run on.
+   Infrastructure of this library; the reference has no device streams. */
+void* scopi_gpu_get_stream(scopi_gpu_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SCOPI_GPU_H */

@@ -1,0 +1,9 @@
+"""scopi_b200 -- B200 (sm_100a) engine for the SCoPI contact-dynamics time step.
+
+The compute path is libscopi_gpu.so (CUDA, C ABI in include/scopi_gpu.h).  This
+package holds the host-side mirror of the reference's interface (ScopiSolver,
+particle container) and seeded synthetic workloads.
+"""
+from .container import PLANE, SEGMENT, SPHERE, ParticleArrays, Particles, Property, quaternion  # noqa: F401
+from .solver import (BRUTE_FORCE, FP64, FRICTION, KDTREE, MIXED, NOFRICTION, VAP_FIXED, VAP_FPD,  # noqa: F401
+                     VISCOUS, ScopiGPUError, ScopiSolver)

@@ -1,0 +1,152 @@
+"""Seeded synthetic workloads (SplitMix64 -> uniform doubles), shared by tests and bench.
+
+Generator: SplitMix64 with state_k = seed + (k+1) * 0x9E3779B97F4A7C15 (mod 2^64), the
+usual three xor-shift-multiply rounds, uniform = (z >> 11) * 2^-53.  Draw order is
+stated per workload so any implementation can rebuild the same inputs.
+
+Workloads (shapes and distributions of the benchmark configurations):
+  disks_2d        1024 disks, radius U[0.008,0.012], 32x32 grid spacing 0.025, jitter +-0.002,
+                  desired velocity -0.25 (x-c)/|x-c| toward c=(0.4,0.4), m=1, J=0.1.
+  box_3d          spheres on a jittered 47^3 lattice (spacing 0.0115, jitter +-0.0005),
+                  radius U[0.9,1.1]*0.005, m=(r/0.005)^3, J=0.4 m r^2, gravity -9.81 m in z,
+                  six fixed planes bounding the unit box.
+  spheres_1m      100^3 spheres on a jittered lattice (spacing 0.0045, jitter +-0.0002) centred
+                  in the unit box, radius U[0.9,1.1]*0.002, desired velocity 0.1 (c-x)/|c-x|,
+                  m=(r/0.002)^3, J=0.4 m r^2, six plane walls.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .container import PLANE, SPHERE, ParticleArrays, quaternion
+
+_G = np.uint64(0x9E3779B97F4A7C15)
+_M1 = np.uint64(0xBF58476D1CE4E5B9)
+_M2 = np.uint64(0x94D049BB133111EB)
+
+
+def splitmix_uniform(seed: int, n: int) -> np.ndarray:
+    """n uniforms in [0,1) from SplitMix64(seed)."""
+    with np.errstate(over="ignore"):
+        k = np.arange(1, n + 1, dtype=np.uint64)
+        z = np.uint64(seed) + k * _G
+        z = (z ^ (z >> np.uint64(30))) * _M1
+        z = (z ^ (z >> np.uint64(27))) * _M2
+        z = z ^ (z >> np.uint64(31))
+    return (z >> np.uint64(11)).astype(np.float64) * (2.0 ** -53)
+
+
+def _arrays(dim, shape, pos, q, v, omega, vd, omega_d, f, m, j, radius, length, nin):
+    return ParticleArrays(dim=dim, nb_inactive=nin, shape=np.ascontiguousarray(shape, np.int32),
+                          pos=np.ascontiguousarray(pos), q=np.ascontiguousarray(q), v=np.ascontiguousarray(v),
+                          omega=np.ascontiguousarray(omega), vd=np.ascontiguousarray(vd),
+                          omega_d=np.ascontiguousarray(omega_d), f=np.ascontiguousarray(f), m=np.ascontiguousarray(m),
+                          j=np.ascontiguousarray(j), radius=np.ascontiguousarray(radius),
+                          length=np.ascontiguousarray(length))
+
+
+def _box_planes():
+    """Six planes of the unit box; normal = column 0 of R(q) (plane.hpp:143-147)."""
+    zq = quaternion(0.0, (0, 0, 1))
+    yq = quaternion(math.pi / 2, (0, 0, 1))
+    xq = quaternion(math.pi / 2, (0, 1, 0))
+    pos = [(0, 0, 0), (1, 0, 0), (0, 0, 0), (0, 1, 0), (0, 0, 0), (0, 0, 1)]
+    qs = [zq, zq, yq, yq, xq, xq]
+    return np.array(pos, dtype=np.float64), np.array(qs)
+
+
+def _assemble(dim, centers, radius, m, jm, vd=None, f=None, planes=True):
+    n_a = len(radius)
+    if planes:
+        ppos, pq = _box_planes()
+        nin = len(ppos)
+    else:
+        ppos, pq, nin = np.zeros((0, 3)), np.zeros((0, 4)), 0
+    n = nin + n_a
+    shape = np.full(n, SPHERE, np.int32)
+    shape[:nin] = PLANE
+    pos = np.zeros((n, 3))
+    pos[:nin] = ppos
+    pos[nin:, :dim] = centers[:, :dim]
+    q = np.zeros((n, 4))
+    q[:, 0] = 1.0
+    q[:nin] = pq
+    z3 = np.zeros((n, 3))
+    vdd = z3.copy()
+    if vd is not None:
+        vdd[nin:, :dim] = vd[:, :dim]
+    ff = z3.copy()
+    if f is not None:
+        ff[nin:, :dim] = f[:, :dim]
+    mm = np.ones(n)
+    mm[nin:] = m
+    jj = np.ones((n, 3))
+    jj[nin:] = jm
+    rr = np.zeros(n)
+    rr[nin:] = radius
+    return _arrays(dim, shape, pos, q, z3.copy(), z3.copy(), vdd, z3.copy(), ff, mm, jj, rr, np.zeros(n), nin)
+
+
+def disks_2d(seed: int = 1, side: int = 32) -> ParticleArrays:
+    """Draws per disk k = i*side + j: jitter x, jitter y, radius."""
+    n = side * side
+    u = splitmix_uniform(seed, 3 * n).reshape(n, 3)
+    ii, jj = np.meshgrid(np.arange(side), np.arange(side), indexing="ij")
+    cx = 0.0125 + 0.025 * ii.ravel() + (u[:, 0] * 2 - 1) * 0.002
+    cy = 0.0125 + 0.025 * jj.ravel() + (u[:, 1] * 2 - 1) * 0.002
+    r = 0.008 + (0.012 - 0.008) * u[:, 2]
+    c = np.array([0.4, 0.4])
+    x = np.stack([cx, cy], 1)
+    d = x - c
+    nrm = np.sqrt((d * d).sum(1))
+    nrm[nrm == 0] = 1.0
+    vd = -0.25 * d / nrm[:, None]
+    jm = np.zeros((n, 3))
+    jm[:, 2] = 0.1
+    return _assemble(2, x, r, np.ones(n), jm, vd=vd, planes=False)
+
+
+def _lattice(seed, count, side, spacing, origin, jitter, r0):
+    """Draws per sphere k (lexicographic, k fastest): jitter x, y, z, radius."""
+    u = splitmix_uniform(seed, 4 * count).reshape(count, 4)
+    idx = np.arange(count)
+    ix, iy, iz = idx // (side * side), (idx // side) % side, idx % side
+    c = np.stack([origin[0] + spacing * ix, origin[1] + spacing * iy, origin[2] + spacing * iz], 1)
+    c = c + (u[:, :3] * 2 - 1) * jitter
+    r = (0.9 + 0.2 * u[:, 3]) * r0
+    return c, r
+
+
+def box_3d(seed: int = 2, count: int = 100_000, side: int = 47) -> ParticleArrays:
+    sp = 0.0115
+    origin = (0.5 - 23 * sp, 0.5 - 23 * sp, sp)
+    c, r = _lattice(seed, count, side, sp, origin, 0.0005, 0.005)
+    m = (r / 0.005) ** 3
+    jm = np.repeat((0.4 * m * r * r)[:, None], 3, 1)
+    f = np.zeros((count, 3))
+    f[:, 2] = -9.81 * m
+    return _assemble(3, c, r, m, jm, f=f)
+
+
+def spheres_1m(seed: int = 5, side: int = 100) -> ParticleArrays:
+    sp = 0.0045
+    count = side ** 3
+    o = 0.5 - (side - 1) / 2 * sp
+    c, r = _lattice(seed, count, side, sp, (o, o, o), 0.0002, 0.002)
+    m = (r / 0.002) ** 3
+    jm = np.repeat((0.4 * m * r * r)[:, None], 3, 1)
+    d = np.array([0.5, 0.5, 0.5]) - c
+    nrm = np.sqrt((d * d).sum(1))
+    nrm[nrm == 0] = 1.0
+    vd = 0.1 * d / nrm[:, None]
+    return _assemble(3, c, r, m, jm, vd=vd)
+
+
+# solver settings per workload (dmax, dt, tolerance, max_ite, vap)
+SETTINGS = {
+    "disks_2d": dict(dmax=0.01, dt=0.005, tolerance=1e-6, max_ite=40000, vap=0, steps=200),
+    "box_3d": dict(dmax=0.0045, dt=1e-3, tolerance=1e-6, max_ite=40000, vap=1, steps=500),
+    "spheres_1m": dict(dmax=0.0018, dt=1e-3, tolerance=1e-6, max_ite=40000, vap=0, steps=100),
+}

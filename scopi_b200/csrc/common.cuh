@@ -1,0 +1,67 @@
+// common.cuh -- shared device-side types and helpers of the SCoPI B200 engine.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace scopi_gpu {
+
+constexpr int kSMs = 148;          // B200: 2 dies x 74 SMs
+constexpr int kThreads = 256;
+
+// Bodies in device memory (AoS float64, 3 slots per vector, obstacles first).
+struct Bodies {
+    int n;
+    int nin;            // obstacles
+    const int* shape;
+    double* pos;        // n*3
+    double* q;          // n*4
+    double* v;          // n*3
+    double* omega;      // n*3
+    const double* vd;
+    const double* omega_d;
+    const double* f;
+    const double* m;
+    const double* j;    // n*3
+    const double* radius;
+    const double* length;
+};
+
+// Device-resident sizes written by the detection kernels (graph friendly: no host sizes).
+struct Sizes {
+    int C;              // contacts
+    int C_obs;          // obstacle contacts (rows of bodies < nin come first)
+    int n_extra;        // Viscous: second multipliers
+    int overflow;       // capacity exceeded somewhere (host grows and redoes the step)
+    int ncell;          // cells of the uniform grid
+    int pad[3];
+};
+
+struct Grid {
+    double lo[3];
+    double h;           // cell edge
+    int nc[3];
+    int ncell;
+    int ncell1;         // ncell + 1 (length of the cell-start scan)
+    double rmax;
+};
+
+// Contact list (sorted by (i, j)) and the per-contact Jacobian rows.
+struct Contacts {
+    int* ci;
+    int* cj;
+    double* dij;
+    double* nij;     // C*3
+    double* pi;      // C*3
+    double* pj;      // C*3
+    double* gamma;   // Viscous property
+};
+
+enum Problem { kNoFriction = 0, kFriction = 1, kViscous = 2 };
+
+__host__ __device__ inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// grid-stride helper
+#define GRID_STRIDE(i, n) for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (long long)(n); \
+                               i += (long long)gridDim.x * blockDim.x)
+
+}  // namespace scopi_gpu

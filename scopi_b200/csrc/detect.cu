@@ -1,0 +1,876 @@
+// detect.cu -- obstacle motion, a-priori velocity, cell-list contact detection, closest
+// points, contact-Jacobian assembly, particle-major incidence lists, viscous gamma
+// update and the velocity/position/quaternion integration.
+//
+// Built with -fmad=false: the closest-point arithmetic keeps the exact operation
+// order of the reference formulas (no contraction into FMA), so the strict test
+// dij < dmax (include/scopi/contact/base.hpp:118) selects the same pairs, bit for
+// bit, as the CPU restatement of the reference evaluated in the same order.
+#include <math.h>
+
+#include "kernels.cuh"
+
+namespace scopi_gpu {
+
+static long long g_detect_launches = 0;
+long long detect_launches() { return g_detect_launches; }
+#define LAUNCHED(k) (g_detect_launches += (k))
+
+namespace {
+
+constexpr int kSphere = 0, kPlane = 1, kSegment = 2;
+constexpr int kBBoxBlocks = 4 * kSMs;
+
+struct PairGeom {
+    double dij;
+    double nij[3], pi[3], pj[3];
+};
+
+__device__ __forceinline__ double xsign(double x) { return (x > 0.0) ? 1.0 : ((x < 0.0) ? -1.0 : 0.0); }
+
+__device__ __forceinline__ double norm_n(const double* x, int n) {
+    double s = 0.0;
+    for (int k = 0; k < n; ++k) s += x[k] * x[k];
+    return sqrt(s);
+}
+__device__ __forceinline__ double dot_n(const double* a, const double* b, int n) {
+    double s = 0.0;
+    for (int k = 0; k < n; ++k) s += a[k] * b[k];
+    return s;
+}
+
+// column 0 of rotation_matrix<dim>(q): plane::normal / segment::normal
+// (include/scopi/objects/types/plane.hpp:143-147, include/scopi/quaternion.hpp:66-124)
+__device__ __forceinline__ void body_normal(const double* q, int dim, double* nrm) {
+    const double x = q[0], y = q[1], z = q[2], w = q[3];
+    if (dim == 2) {
+        nrm[0] = 1 - 2 * w * w;
+        nrm[1] = 2 * x * w;
+        nrm[2] = 0.0;
+    } else {
+        nrm[0] = 1 - 2 * z * z - 2 * w * w;
+        nrm[1] = 2 * y * z + 2 * x * w;
+        nrm[2] = 2 * y * w - 2 * x * z;
+    }
+}
+
+// rotation_matrix<3>(q), include/scopi/quaternion.hpp:87-124
+__device__ __forceinline__ void rotation3(const double* q, double r[3][3]) {
+    const double x = q[0], y = q[1], z = q[2], w = q[3];
+    r[0][0] = 1 - 2 * z * z - 2 * w * w;
+    r[0][1] = 2 * y * z - 2 * x * w;
+    r[0][2] = 2 * y * w + 2 * x * z;
+    r[1][0] = 2 * y * z + 2 * x * w;
+    r[1][1] = 1 - 2 * y * y - 2 * w * w;
+    r[1][2] = 2 * z * w - 2 * x * y;
+    r[2][0] = 2 * y * w - 2 * x * z;
+    r[2][1] = 2 * z * w + 2 * x * y;
+    r[2][2] = 1 - 2 * y * y - 2 * z * z;
+}
+
+// detail::cross<dim>, include/scopi/matrix/velocities.hpp:26-44
+__device__ __forceinline__ void cross_dim(int dim, const double* x, const double* y, double* o) {
+    if (dim == 2) {
+        o[0] = x[1] * y[2];
+        o[1] = -x[0] * y[2];
+        o[2] = x[0] * y[1] - x[1] * y[0];
+    } else {
+        o[0] = x[1] * y[2] - x[2] * y[1];
+        o[1] = x[2] * y[0] - x[0] * y[2];
+        o[2] = x[0] * y[1] - x[1] * y[0];
+    }
+}
+
+// closest_points(sphere, sphere), include/scopi/objects/methods/closest_points.hpp:36-50
+__device__ __forceinline__ void sphere_sphere(int dim, const double* xa, double ra, const double* xb, double rb,
+                                              PairGeom& g) {
+    double d[3] = {0, 0, 0};
+    for (int k = 0; k < dim; ++k) d[k] = xb[k] - xa[k];
+    const double nrm = norm_n(d, dim);
+    double u[3] = {0, 0, 0};
+    for (int k = 0; k < dim; ++k) u[k] = d[k] / nrm;
+    for (int k = 0; k < 3; ++k) g.pi[k] = g.pj[k] = g.nij[k] = 0.0;
+    for (int k = 0; k < dim; ++k) {
+        g.pi[k] = xa[k] + ra * u[k];
+        g.pj[k] = xb[k] - rb * u[k];
+    }
+    double t[3] = {0, 0, 0};
+    for (int k = 0; k < dim; ++k) t[k] = g.pj[k] - xb[k];
+    const double nt = norm_n(t, dim);
+    for (int k = 0; k < dim; ++k) g.nij[k] = t[k] / nt;
+    double diff[3] = {0, 0, 0};
+    for (int k = 0; k < dim; ++k) diff[k] = g.pi[k] - g.pj[k];
+    g.dij = dot_n(diff, g.nij, dim);
+}
+
+// closest_points(sphere, plane), closest_points.hpp:768-788
+__device__ __forceinline__ void sphere_plane(int dim, const double* xs, double rs, const double* xp, const double* qp,
+                                             PairGeom& g) {
+    double nrm[3];
+    body_normal(qp, dim, nrm);
+    double d[3] = {0, 0, 0};
+    for (int k = 0; k < dim; ++k) d[k] = xs[k] - xp[k];
+    const double p2s = dot_n(d, nrm, dim);
+    const double sg = xsign(p2s);
+    for (int k = 0; k < 3; ++k) g.pi[k] = g.pj[k] = g.nij[k] = 0.0;
+    for (int k = 0; k < dim; ++k) {
+        g.pi[k] = xs[k] - sg * rs * nrm[k];
+        g.pj[k] = xs[k] - p2s * nrm[k];
+        g.nij[k] = sg * nrm[k];
+    }
+    double diff[3] = {0, 0, 0};
+    for (int k = 0; k < dim; ++k) diff[k] = g.pi[k] - g.pj[k];
+    g.dij = dot_n(diff, g.nij, dim);
+}
+
+// closest_points(sphere, segment), closest_points.hpp:824-870; segment.hpp:155-181 (2D)
+__device__ __forceinline__ void sphere_segment(const double* sp, double rs, const double* xg, const double* qg,
+                                               double len, PairGeom& g) {
+    const double x = qg[0], w = qg[3];
+    const double r01 = -2 * x * w, r11 = 1 - 2 * w * w;
+    const double h = 0.5 * len;
+    double e0[2], e1[2];
+    e0[0] = (0.0 * (1 - 2 * w * w) + r01 * (-h)) + xg[0];
+    e0[1] = (0.0 * (2 * x * w) + r11 * (-h)) + xg[1];
+    e1[0] = (0.0 * (1 - 2 * w * w) + r01 * h) + xg[0];
+    e1[1] = (0.0 * (2 * x * w) + r11 * h) + xg[1];
+    double nrm[3];
+    body_normal(qg, 2, nrm);
+    const double tg[2] = {-nrm[1], nrm[0]};
+    const double d0[2] = {sp[0] - e0[0], sp[1] - e0[1]};
+    const double d1[2] = {sp[0] - e1[0], sp[1] - e1[1]};
+    for (int k = 0; k < 3; ++k) g.pi[k] = g.pj[k] = g.nij[k] = 0.0;
+    if (dot_n(d0, tg, 2) < 0 || dot_n(d1, tg, 2) > 0) {
+        const bool first = dot_n(d0, tg, 2) < 0;
+        const double* e = first ? e0 : e1;
+        const double* de = first ? d0 : d1;
+        const double nn = norm_n(de, 2);
+        for (int k = 0; k < 2; ++k) {
+            g.nij[k] = de[k] / nn;
+            g.pi[k] = sp[k] - g.nij[k] * rs;
+            g.pj[k] = e[k];
+        }
+    } else {
+        const double d[2] = {sp[0] - xg[0], sp[1] - xg[1]};
+        const double s2s = dot_n(d, nrm, 2);
+        const double sgn = xsign(s2s);
+        for (int k = 0; k < 2; ++k) {
+            g.pi[k] = sp[k] - sgn * rs * nrm[k];
+            g.pj[k] = sp[k] - s2s * nrm[k];
+            g.nij[k] = sgn * nrm[k];
+        }
+    }
+    const double diff[2] = {g.pi[0] - g.pj[0], g.pi[1] - g.pj[1]};
+    g.dij = dot_n(diff, g.nij, 2);
+}
+
+__device__ __forceinline__ void flip(PairGeom& g) {
+    for (int k = 0; k < 3; ++k) {
+        g.nij[k] *= -1.;
+        const double t = g.pi[k];
+        g.pi[k] = g.pj[k];
+        g.pj[k] = t;
+    }
+}
+
+// closest_points_dispatcher restricted to the pairs of the hot path (a < b).
+__device__ bool exact_pair(const Bodies& B, int dim, int a, int b, PairGeom& g) {
+    const int sa = B.shape[a], sb = B.shape[b];
+    const double* xa = B.pos + 3 * (long long)a;
+    const double* xb = B.pos + 3 * (long long)b;
+    if (sa == kSphere && sb == kSphere) {
+        sphere_sphere(dim, xa, B.radius[a], xb, B.radius[b], g);
+    } else if (sa == kPlane && sb == kSphere) {  // closest_points.hpp:802-809
+        sphere_plane(dim, xb, B.radius[b], xa, B.q + 4 * (long long)a, g);
+        flip(g);
+    } else if (sa == kSphere && sb == kPlane) {
+        sphere_plane(dim, xa, B.radius[a], xb, B.q + 4 * (long long)b, g);
+    } else if (sa == kSegment && sb == kSphere && dim == 2) {  // closest_points.hpp:874-881
+        sphere_segment(xb, B.radius[b], xa, B.q + 4 * (long long)a, B.length[a], g);
+        flip(g);
+    } else if (sa == kSphere && sb == kSegment && dim == 2) {
+        sphere_segment(xa, B.radius[a], xb, B.q + 4 * (long long)b, B.length[b], g);
+    } else {
+        return false;
+    }
+    return true;
+}
+
+// mult_quaternion (src/quaternion.cpp:92-120), normalize (:6-10) and the exp map of
+// solver.hpp:335-351 / 449-479.
+__device__ __forceinline__ void rotate_body(double* q, const double* w, double normw, double dt) {
+    if (normw == 0) normw = 1;
+    double e[4];
+    e[0] = cos(0.5 * normw * dt);
+    const double s = sin(0.5 * normw * dt) / normw;
+    for (int d = 0; d < 3; ++d) e[d + 1] = s * w[d];
+    double r[4];
+    r[0] = q[0] * e[0];
+    for (int d = 0; d < 3; ++d) {
+        r[0] -= q[d + 1] * e[d + 1];
+        r[d + 1] = q[0] * e[d + 1] + e[0] * q[d + 1];
+    }
+    r[1] += (q[2] * e[3] - q[3] * e[2]);
+    r[2] += (q[3] * e[1] - q[1] * e[3]);
+    r[3] += (q[1] * e[2] - q[2] * e[1]);
+    const double nq = norm_n(r, 4);
+    for (int d = 0; d < 4; ++d) q[d] = r[d] / nq;
+}
+
+// ------------------------------------------------------------------ kernels
+
+__global__ void k_obstacles_move(Bodies B, double dt, int dim) {
+    GRID_STRIDE(i, B.nin) {
+        double w[3] = {B.omega_d[3 * i], B.omega_d[3 * i + 1], B.omega_d[3 * i + 2]};
+        if (dim == 2) w[0] = w[1] = 0.0;
+        const double nw = norm_n(w, 3);
+        for (int d = 0; d < dim; ++d) B.pos[3 * i + d] += dt * B.vd[3 * i + d];
+        rotate_body(B.q + 4 * i, w, nw, dt);
+    }
+}
+
+// vap_fixed::set_a_priori_velocity_impl (vap_fixed.hpp:45-55), vap_fpd (vap_fpd.hpp:69-81,
+// src/vap/vap_fpd.cpp:6-26)
+__global__ void k_vap(Bodies B, StepParams p) {
+    GRID_STRIDE(k, B.n - B.nin) {
+        const long long b = B.nin + k;
+        if (p.vap == 0) {
+            for (int d = 0; d < 3; ++d) {
+                B.v[3 * b + d] = B.vd[3 * b + d];
+                B.omega[3 * b + d] = B.omega_d[3 * b + d];
+            }
+        } else {
+            for (int d = 0; d < p.dim; ++d) B.v[3 * b + d] += p.dt * B.f[3 * b + d] / B.m[b];
+            if (p.dim == 3) {
+                const double o1 = B.omega[3 * b], o2 = B.omega[3 * b + 1], o3 = B.omega[3 * b + 2];
+                const double j1 = B.j[3 * b], j2 = B.j[3 * b + 1], j3 = B.j[3 * b + 2];
+                B.omega[3 * b] += o2 * o3 * (j3 - j2);
+                B.omega[3 * b + 1] += o1 * o3 * (j1 - j3);
+                B.omega[3 * b + 2] += o1 * o2 * (j2 - j1);
+            }
+        }
+    }
+}
+
+__global__ void k_bbox_partial(Bodies B, int dim, double* partial) {
+    __shared__ double sh[8][kThreads];
+    double v[7] = {1e300, 1e300, 1e300, -1e300, -1e300, -1e300, 0.0};
+    GRID_STRIDE(k, B.n - B.nin) {
+        const long long b = B.nin + k;
+        for (int d = 0; d < dim; ++d) {
+            v[d] = fmin(v[d], B.pos[3 * b + d]);
+            v[3 + d] = fmax(v[3 + d], B.pos[3 * b + d]);
+        }
+        v[6] = fmax(v[6], B.radius[b]);
+    }
+    for (int k = 0; k < 7; ++k) sh[k][threadIdx.x] = v[k];
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            for (int k = 0; k < 3; ++k) sh[k][threadIdx.x] = fmin(sh[k][threadIdx.x], sh[k][threadIdx.x + s]);
+            for (int k = 3; k < 7; ++k) sh[k][threadIdx.x] = fmax(sh[k][threadIdx.x], sh[k][threadIdx.x + s]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 7; ++k) partial[blockIdx.x * 8 + k] = sh[k][0];
+}
+
+__global__ void k_grid_setup(const double* partial, int nparts, int dim, double dmax, long long cell_cap, int na,
+                             Grid* grid) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300}, rmax = 0.0;
+    for (int b = 0; b < nparts; ++b) {
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = fmin(lo[k], partial[b * 8 + k]);
+            hi[k] = fmax(hi[k], partial[b * 8 + 3 + k]);
+        }
+        rmax = fmax(rmax, partial[b * 8 + 6]);
+    }
+    if (na == 0) {
+        for (int k = 0; k < 3; ++k) lo[k] = hi[k] = 0.0;
+    }
+    for (int k = dim; k < 3; ++k) lo[k] = hi[k] = 0.0;
+    double h = (2 * rmax + dmax) * (1 + 1e-6) + 1e-12;
+    int nc[3] = {1, 1, 1};
+    long long tot = 1;
+    for (int guard = 0; guard < 200; ++guard) {
+        tot = 1;
+        for (int k = 0; k < dim; ++k) {
+            double c = floor((hi[k] - lo[k]) / h) + 1.0;
+            if (!(c >= 1.0)) c = 1.0;  // NaN / inf positions: one cell
+            if (c > 2.0e9) c = 2.0e9;
+            nc[k] = (int)c;
+            tot *= nc[k];
+        }
+        if (tot <= cell_cap) break;
+        h *= 1.5;
+    }
+    for (int k = 0; k < 3; ++k) {
+        grid->lo[k] = lo[k];
+        grid->nc[k] = nc[k];
+    }
+    grid->h = h;
+    grid->ncell = (int)tot;
+    grid->ncell1 = (int)tot + 1;
+    grid->rmax = rmax;
+}
+
+__device__ __forceinline__ int cell_coord(double x, double lo, double h, int nc) {
+    int c = (int)floor((x - lo) / h);
+    return c < 0 ? 0 : (c > nc - 1 ? nc - 1 : c);
+}
+
+__global__ void k_cell_assign(Bodies B, int dim, const Grid* grid, int* cell_of, int* cell_count) {
+    const Grid g = *grid;
+    GRID_STRIDE(k, B.n - B.nin) {
+        const long long b = B.nin + k;
+        int id = 0;
+        for (int d = dim - 1; d >= 0; --d) id = id * g.nc[d] + cell_coord(B.pos[3 * b + d], g.lo[d], g.h, g.nc[d]);
+        cell_of[k] = id;
+        atomicAdd(&cell_count[id], 1);
+    }
+}
+
+__global__ void k_cell_scatter(Bodies B, const int* cell_of, const int* cell_start, int* cell_fill, int* cell_body,
+                               double4* cell_pr) {
+    GRID_STRIDE(k, B.n - B.nin) {
+        const long long b = B.nin + k;
+        const int c = cell_of[k];
+        const int slot = atomicAdd(&cell_fill[c], 1);
+        const int at = cell_start[c] + slot;
+        cell_body[at] = (int)b;
+        cell_pr[at] = make_double4(B.pos[3 * b], B.pos[3 * b + 1], B.pos[3 * b + 2], B.radius[b]);
+    }
+}
+
+// Enumerates the (a, b > a) active pairs of the 3^dim neighbour cells of cell-sorted slot k
+// whose exact closest-point distance is < dmax (and pass the kd-tree candidate filter).
+template <typename F>
+__device__ __forceinline__ void for_each_pair(const Bodies& B, const StepParams& p, const Grid& g, const int* cell_of,
+                                              const int* cell_start, const int* cell_body, const double4* cell_pr,
+                                              int k, F&& emit) {
+    const int a = cell_body[k];
+    const double4 A = cell_pr[k];
+    const double xa[3] = {A.x, A.y, A.z};
+    const int id = cell_of[a - B.nin];
+    int cc[3];
+    cc[0] = id % g.nc[0];
+    cc[1] = (id / g.nc[0]) % g.nc[1];
+    cc[2] = id / (g.nc[0] * g.nc[1]);
+    const int zr = p.dim == 3 ? 1 : 0;
+    for (int dz = -zr; dz <= zr; ++dz) {
+        const int z = cc[2] + dz;
+        if (z < 0 || z >= g.nc[2]) continue;
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int y = cc[1] + dy;
+            if (y < 0 || y >= g.nc[1]) continue;
+            for (int dx = -1; dx <= 1; ++dx) {
+                const int x = cc[0] + dx;
+                if (x < 0 || x >= g.nc[0]) continue;
+                const int cid = (z * g.nc[1] + y) * g.nc[0] + x;
+                const int t1 = cell_start[cid + 1];
+                for (int t = cell_start[cid]; t < t1; ++t) {
+                    const int b = cell_body[t];
+                    if (b <= a) continue;
+                    const double4 Bb = cell_pr[t];
+                    const double xb[3] = {Bb.x, Bb.y, Bb.z};
+                    double s2 = 0.0;
+                    for (int d = 0; d < p.dim; ++d) {
+                        const double dd = xa[d] - xb[d];
+                        s2 += dd * dd;
+                    }
+                    if (p.kd_filter && !(s2 < p.kd_radius)) continue;
+                    const double lim = A.w + Bb.w + p.dmax;
+                    if (!(lim > 0.0) || s2 > lim * lim * (1.0 + 1e-9)) continue;
+                    PairGeom pg;
+                    sphere_sphere(p.dim, xa, A.w, xb, Bb.w, pg);
+                    if (pg.dij < p.dmax) emit(a, b);
+                }
+            }
+        }
+    }
+}
+
+__global__ void k_pair_count(Bodies B, StepParams p, const Grid* grid, const int* cell_of, const int* cell_start,
+                             const int* cell_body, const double4* cell_pr, int* row_count) {
+    const Grid g = *grid;
+    GRID_STRIDE(k, B.n - B.nin) {
+        int cnt = 0;
+        int a0 = cell_body[k];
+        for_each_pair(B, p, g, cell_of, cell_start, cell_body, cell_pr, (int)k, [&](int, int) { ++cnt; });
+        row_count[a0 - B.nin] = cnt;
+    }
+}
+
+__global__ void k_pair_fill(Bodies B, StepParams p, const Grid* grid, const int* cell_of, const int* cell_start,
+                            const int* cell_body, const double4* cell_pr, const int* row_ptr, const Sizes* sizes,
+                            long long cap, int* ci, int* cj) {
+    const Grid g = *grid;
+    const int c_obs = sizes->C_obs;
+    GRID_STRIDE(k, B.n - B.nin) {
+        const int a0 = cell_body[k];
+        long long at = (long long)c_obs + row_ptr[a0 - B.nin];
+        for_each_pair(B, p, g, cell_of, cell_start, cell_body, cell_pr, (int)k, [&](int a, int b) {
+            if (at < cap) {
+                ci[at] = a;
+                cj[at] = b;
+            }
+            ++at;
+        });
+    }
+}
+
+__global__ void k_row_sort(int na, const int* row_ptr, const Sizes* sizes, long long cap, int* cj) {
+    const int c_obs = sizes->C_obs;
+    GRID_STRIDE(r, na) {
+        const long long s = (long long)c_obs + row_ptr[r], e = (long long)c_obs + row_ptr[r + 1];
+        if (e > cap) continue;
+        for (long long x = s + 1; x < e; ++x) {
+            const int key = cj[x];
+            long long y = x - 1;
+            while (y >= s && cj[y] > key) {
+                cj[y + 1] = cj[y];
+                --y;
+            }
+            cj[y + 1] = key;
+        }
+    }
+}
+
+__global__ void k_obs_flags(Bodies B, StepParams p, int* flag) {
+    const long long na = B.n - B.nin;
+    GRID_STRIDE(k, (long long)B.nin * na) {
+        const int o = (int)(k / na);
+        const int b = B.nin + (int)(k % na);
+        PairGeom g;
+        flag[k] = (exact_pair(B, p.dim, o, b, g) && g.dij < p.dmax) ? 1 : 0;
+    }
+}
+
+__global__ void k_obs_fill(Bodies B, const int* flag, const int* pos, long long cap, int* ci, int* cj) {
+    const long long na = B.n - B.nin;
+    GRID_STRIDE(k, (long long)B.nin * na) {
+        if (!flag[k]) continue;
+        const long long at = pos[k];
+        if (at < cap) {
+            ci[at] = (int)(k / na);
+            cj[at] = B.nin + (int)(k % na);
+        }
+    }
+}
+
+__global__ void k_sizes(const int* totals, Sizes* sizes, long long cap) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        const long long c = (long long)totals[0] + totals[1];
+        sizes->C_obs = totals[0];
+        sizes->C = (int)(c < cap ? c : cap);
+        if (c > cap) sizes->overflow = 1;
+    }
+}
+
+__global__ void k_set_cobs(const int* totals, Sizes* sizes) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) sizes->C_obs = totals[0];
+}
+
+// closest points of the listed pairs; viscous gamma carried over from the previous list
+// by (i, j) (transfer, include/scopi/solver.hpp:241-258).
+__global__ void k_geometry(Bodies B, StepParams p, Contacts c, const Sizes* sizes, Contacts old_c, const int* old_C) {
+    const int C = sizes->C;
+    const int oC = old_C ? *old_C : 0;
+    GRID_STRIDE(k, C) {
+        const int a = c.ci[k], b = c.cj[k];
+        PairGeom g;
+        if (!exact_pair(B, p.dim, a, b, g)) {
+            g.dij = 0.0;
+            for (int d = 0; d < 3; ++d) g.nij[d] = g.pi[d] = g.pj[d] = 0.0;
+        }
+        c.dij[k] = g.dij;
+        for (int d = 0; d < 3; ++d) {
+            c.nij[3 * k + d] = g.nij[d];
+            c.pi[3 * k + d] = g.pi[d];
+            c.pj[3 * k + d] = g.pj[d];
+        }
+        double gam = p.gamma0;
+        if (oC > 0 && old_c.ci) {
+            int lo = 0, hi = oC;  // first index with (ci, cj) >= (a, b)
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                const int mi = old_c.ci[mid], mj = old_c.cj[mid];
+                if (mi < a || (mi == a && mj < b))
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            if (lo < oC && old_c.ci[lo] == a && old_c.cj[lo] == b) gam = old_c.gamma[lo];
+        }
+        c.gamma[k] = gam;
+    }
+}
+
+// Per-contact Jacobian rows.  For the normal problems the contact's row of B = n^T A
+// (include/scopi/matrix/velocities.hpp:67-144 projected by global2local) is
+//   B_c u = n.v_i + a_i.w_i - n.v_j + a_j.w_j,  a_i = R_i^T (r_i x n),  a_j = -R_j^T (r_j x n),
+// and c_c = n.(D n + dt A U)_c (CVector, minimization_problem.hpp:34-70).  For friction
+// the three rows of A are kept: P = R^T [r]x so A_c = [I, P_i^T, -I, -P_j^T].
+__global__ void k_assemble(Bodies B, StepParams p, Contacts c, Assembly a, const Sizes* sizes) {
+    const int C = sizes->C;
+    GRID_STRIDE(k, C) {
+        const int bi[2] = {c.ci[k], c.cj[k]};
+        const double* n = c.nij + 3 * k;
+        double AU[3] = {0, 0, 0};
+        double arow[2][3] = {{0, 0, 0}, {0, 0, 0}};
+        double P[2][9];
+        for (int s = 0; s < 2; ++s)
+            for (int e = 0; e < 9; ++e) P[s][e] = 0.0;
+        for (int s = 0; s < 2; ++s) {
+            const int b = bi[s];
+            if (b < B.nin) continue;
+            const double* pt = (s == 0 ? c.pi : c.pj) + 3 * k;
+            double r[3] = {0, 0, 0};
+            for (int d = 0; d < p.dim; ++d) r[d] = pt[d] - B.pos[3 * (long long)b + d];
+            double R[3][3];
+            rotation3(B.q + 4 * (long long)b, R);
+            const double* w = B.omega + 3 * (long long)b;
+            const double* v = B.v + 3 * (long long)b;
+            double Rw[3], cr[3];
+            for (int d = 0; d < 3; ++d) Rw[d] = R[d][0] * w[0] + R[d][1] * w[1] + R[d][2] * w[2];
+            cross_dim(p.dim, r, Rw, cr);
+            const double vz = p.dim == 2 ? 0.0 : v[2];
+            const double vv[3] = {v[0], v[1], vz};
+            for (int d = 0; d < 3; ++d) AU[d] += (s == 0 ? 1.0 : -1.0) * (vv[d] - cr[d]);
+            double rn[3];
+            cross_dim(p.dim, r, n, rn);
+            const double sg = (s == 0) ? 1.0 : -1.0;
+            for (int d = 0; d < 3; ++d) arow[s][d] = sg * (R[0][d] * rn[0] + R[1][d] * rn[1] + R[2][d] * rn[2]);
+            // P = R^T [r]x : P[k][l] = sum_m R[m][k] X[m][l], X = [[0,-r2,r1],[r2,0,-r0],[-r1,r0,0]]
+            const double X[3][3] = {{0.0, -r[2], r[1]}, {r[2], 0.0, -r[0]}, {-r[1], r[0], 0.0}};
+            for (int kk = 0; kk < 3; ++kk)
+                for (int l = 0; l < 3; ++l)
+                    P[s][3 * kk + l] = R[0][kk] * X[0][l] + R[1][kk] * X[1][l] + R[2][kk] * X[2][l];
+        }
+        double Cv[3];
+        for (int d = 0; d < 3; ++d) Cv[d] = (d < p.dim ? c.dij[k] * n[d] : 0.0) + p.dt * AU[d];
+        if (p.problem == kFriction) {
+            for (int d = 0; d < 3; ++d) a.cvec[3 * k + d] = Cv[d];
+            for (int e = 0; e < 9; ++e) {
+                a.bP[18 * (long long)k + e] = P[0][e];
+                a.bP[18 * (long long)k + 9 + e] = P[1][e];
+            }
+        } else {
+            double cc = 0.0;
+            for (int d = 0; d < p.dim; ++d) cc += Cv[d] * n[d];
+            a.cvec[k] = cc;
+        }
+        for (int d = 0; d < 3; ++d) {
+            a.bn[3 * (long long)k + d] = n[d];
+            a.bai[3 * (long long)k + d] = arow[0][d];
+            a.baj[3 * (long long)k + d] = arow[1][d];
+        }
+        if (p.problem == kViscous) a.vflag[k] = (c.gamma[k] < -p.gamma_tol) ? 1 : 0;
+    }
+}
+
+__global__ void k_viscous_slots(const Sizes* sizes, const int* scanned, const int* flag_src, int* slot) {
+    const int C = sizes->C;
+    GRID_STRIDE(k, C) { slot[k] = flag_src[k] ? C + scanned[k] : -1; }
+}
+
+__global__ void k_set_extra(const int* total, Sizes* sizes) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) sizes->n_extra = *total;
+}
+
+__global__ void k_inc_count(int nin, Contacts c, const Sizes* sizes, int* count) {
+    const int C = sizes->C;
+    GRID_STRIDE(k, C) {
+        const int a = c.ci[k], b = c.cj[k];
+        if (a >= nin) atomicAdd(&count[a - nin], 1);
+        if (b >= nin) atomicAdd(&count[b - nin], 1);
+    }
+}
+
+__global__ void k_inc_fill(int nin, Contacts c, const Sizes* sizes, const int* ptr, int* fill, int* idx) {
+    const int C = sizes->C;
+    GRID_STRIDE(k, C) {
+        const int a = c.ci[k], b = c.cj[k];
+        if (a >= nin) {
+            const int s = atomicAdd(&fill[a - nin], 1);
+            idx[ptr[a - nin] + s] = (int)k;
+        }
+        if (b >= nin) {
+            const int s = atomicAdd(&fill[b - nin], 1);
+            idx[ptr[b - nin] + s] = (int)((unsigned)k | 0x80000000u);
+        }
+    }
+}
+
+// sort each particle's incidences by contact index: a deterministic summation order for B^T x
+__global__ void k_inc_sort(int na, const int* ptr, int* idx) {
+    GRID_STRIDE(p, na) {
+        const int s = ptr[p], e = ptr[p + 1];
+        for (int x = s + 1; x < e; ++x) {
+            const int key = idx[x];
+            const unsigned kk = (unsigned)key & 0x7fffffffu;
+            int y = x - 1;
+            while (y >= s && ((unsigned)idx[y] & 0x7fffffffu) > kk) {
+                idx[y + 1] = idx[y];
+                --y;
+            }
+            idx[y + 1] = key;
+        }
+    }
+}
+
+__global__ void k_inc_coef(int na, const int* ptr, const int* idx, Assembly a, double* coef) {
+    const int tot = ptr[na];
+    GRID_STRIDE(k, tot) {
+        const unsigned e = (unsigned)idx[k];
+        const long long c = e & 0x7fffffffu;
+        const bool jside = (e >> 31) != 0;
+        const double sg = jside ? -1.0 : 1.0;
+        const double* ar = (jside ? a.baj : a.bai) + 3 * c;
+        for (int d = 0; d < 3; ++d) {
+            coef[6 * (long long)k + d] = sg * a.bn[3 * c + d];
+            coef[6 * (long long)k + 3 + d] = ar[d];
+        }
+    }
+}
+
+// update_contact_properties_impl<Viscous>, include/scopi/solvers/OptimGradient.hpp:19-35
+__global__ void k_gamma_update(StepParams p, Contacts c, Assembly a, const double* lam, const Sizes* sizes) {
+    const int C = sizes->C;
+    GRID_STRIDE(k, C) {
+        double mu = lam[k];
+        if (a.slot[k] >= 0) mu = lam[k] - lam[a.slot[k]];
+        double dl = 0.0;
+        for (int d = 0; d < p.dim; ++d) dl += c.nij[3 * k + d] * (mu * c.nij[3 * k + d]);
+        c.gamma[k] = fmin(fmax(c.gamma[k] - p.dt * dl, p.gamma_min), 0.);
+    }
+}
+
+// OptimGradient::run velocity recovery (OptimGradient.hpp:265-284), update_velocity
+// (solver.hpp:528-546) and move_active_particles (solver.hpp:441-480).
+__global__ void k_update(Bodies B, StepParams p, const double* u, const Sizes* sizes) {
+    const bool has = (u != nullptr) && (sizes == nullptr || sizes->C > 0);
+    GRID_STRIDE(k, B.n - B.nin) {
+        const long long b = B.nin + k;
+        double* v = B.v + 3 * b;
+        double* w = B.omega + 3 * b;
+        if (has) {
+            for (int d = 0; d < p.dim; ++d) v[d] = v[d] + p.dt * u[6 * k + d];
+            if (p.dim == 3) {
+                for (int d = 0; d < 3; ++d) w[d] = w[d] + p.dt * u[6 * k + 3 + d];
+            } else {
+                w[2] = w[2] + p.dt * u[6 * k + 5];
+            }
+        }
+        double ww[3];
+        double nw;
+        if (p.dim == 2) {
+            ww[0] = 0.0;
+            ww[1] = 0.0;
+            ww[2] = w[2];
+            nw = fabs(w[2]);
+        } else {
+            ww[0] = w[0];
+            ww[1] = w[1];
+            ww[2] = w[2];
+            nw = norm_n(ww, 3);
+        }
+        for (int d = 0; d < p.dim; ++d) B.pos[3 * b + d] += p.dt * v[d];
+        rotate_body(B.q + 4 * b, ww, nw, p.dt);
+    }
+}
+
+// AMatrix::mat_mult (velocities.hpp:67-144) in the reference's 6N layout (test API)
+__global__ void k_amat(Bodies B, StepParams p, Contacts c, const Sizes* sizes, const double* u, double* out) {
+    const int C = sizes->C;
+    const long long na = B.n - B.nin, rot = 3 * na;
+    GRID_STRIDE(k, C) {
+        double row[3] = {0, 0, 0};
+        for (int s = 0; s < 2; ++s) {
+            const int b = s == 0 ? c.ci[k] : c.cj[k];
+            if (b < B.nin) continue;
+            const long long st = 3 * (long long)(b - B.nin);
+            const double vb[3] = {u[st], u[st + 1], u[st + 2]};
+            const double wb[3] = {u[st + rot], u[st + rot + 1], u[st + rot + 2]};
+            const double* pt = (s == 0 ? c.pi : c.pj) + 3 * k;
+            double r[3] = {0, 0, 0};
+            for (int d = 0; d < p.dim; ++d) r[d] = pt[d] - B.pos[3 * (long long)b + d];
+            double R[3][3];
+            rotation3(B.q + 4 * (long long)b, R);
+            double Rw[3], cr[3];
+            for (int d = 0; d < 3; ++d) Rw[d] = R[d][0] * wb[0] + R[d][1] * wb[1] + R[d][2] * wb[2];
+            cross_dim(p.dim, r, Rw, cr);
+            for (int d = 0; d < 3; ++d) {
+                if (s == 0)
+                    row[d] += vb[d] - cr[d];
+                else
+                    row[d] -= vb[d] - cr[d];
+            }
+        }
+        for (int d = 0; d < 3; ++d) out[3 * k + d] = row[d];
+    }
+}
+
+// ATMatrix::mat_mult (velocities.hpp:167-254) in the reference's 6N layout (test API)
+__global__ void k_atmat(Bodies B, StepParams p, Contacts c, const Sizes* sizes, const double* f, double* out) {
+    const int C = sizes->C;
+    const long long na = B.n - B.nin, rot = 3 * na;
+    GRID_STRIDE(k, C) {
+        const double fc[3] = {f[3 * k], f[3 * k + 1], f[3 * k + 2]};
+        for (int s = 0; s < 2; ++s) {
+            const int b = s == 0 ? c.ci[k] : c.cj[k];
+            if (b < B.nin) continue;
+            const long long st = 3 * (long long)(b - B.nin);
+            const double* pt = (s == 0 ? c.pi : c.pj) + 3 * k;
+            double r[3] = {0, 0, 0};
+            for (int d = 0; d < p.dim; ++d) r[d] = pt[d] - B.pos[3 * (long long)b + d];
+            double R[3][3];
+            rotation3(B.q + 4 * (long long)b, R);
+            double cr[3];
+            cross_dim(p.dim, r, fc, cr);
+            const double sg = s == 0 ? 1.0 : -1.0;
+            for (int d = 0; d < 3; ++d) {
+                const double res = R[0][d] * cr[0] + R[1][d] * cr[1] + R[2][d] * cr[2];
+                atomicAdd(&out[st + d], sg * fc[d]);
+                atomicAdd(&out[st + rot + d], sg * res);
+            }
+        }
+    }
+}
+
+int blocks_for(long long n, int per = kThreads) {
+    long long b = (n + per - 1) / per;
+    if (b < 1) b = 1;
+    const long long cap = 16LL * kSMs;
+    return (int)(b < cap ? b : cap);
+}
+
+}  // namespace
+
+void launch_obstacles_move(const Bodies& b, double dt, int dim, cudaStream_t s) {
+    if (b.nin <= 0) return;
+    k_obstacles_move<<<blocks_for(b.nin), kThreads, 0, s>>>(b, dt, dim);
+    LAUNCHED(1);
+}
+
+void launch_vap(const Bodies& b, const StepParams& p, cudaStream_t s) {
+    if (b.n - b.nin <= 0) return;
+    k_vap<<<blocks_for(b.n - b.nin), kThreads, 0, s>>>(b, p);
+    LAUNCHED(1);
+}
+
+void launch_detect(const Bodies& b, const StepParams& p, DetectWork& w, Contacts& out, Sizes* sizes, long long c_cap,
+                   cudaStream_t s) {
+    const int na = b.n - b.nin;
+    cudaMemsetAsync(w.tmp_total, 0, 4 * sizeof(int), s);
+    // uniform grid over the active particles
+    k_bbox_partial<<<kBBoxBlocks, kThreads, 0, s>>>(b, p.dim, w.bbox_partial);
+    k_grid_setup<<<1, 32, 0, s>>>(w.bbox_partial, kBBoxBlocks, p.dim, p.dmax, w.cell_cap, na, w.grid);
+    cudaMemsetAsync(w.cell_count, 0, (w.cell_cap + 1) * sizeof(int), s);
+    cudaMemsetAsync(w.cell_fill, 0, w.cell_cap * sizeof(int), s);
+    LAUNCHED(2);
+    if (na > 0) {
+        k_cell_assign<<<blocks_for(na), kThreads, 0, s>>>(b, p.dim, w.grid, w.cell_of, w.cell_count);
+        scan_exclusive(w.cell_count, w.cell_start, &w.grid->ncell1, 0, w.cell_cap + 1, w.tmp_total + 3, w.scan_work, s,
+                       &g_detect_launches);
+        k_cell_scatter<<<blocks_for(na), kThreads, 0, s>>>(b, w.cell_of, w.cell_start, w.cell_fill, w.cell_body,
+                                                           w.cell_pr);
+        k_pair_count<<<blocks_for(na, 128), 128, 0, s>>>(b, p, w.grid, w.cell_of, w.cell_start, w.cell_body, w.cell_pr,
+                                                         w.row_count);
+        LAUNCHED(3);
+    }
+    // obstacle rows come first in (i, j) order
+    const long long nobs = (long long)b.nin * na;
+    if (nobs > 0) {
+        k_obs_flags<<<blocks_for(nobs), kThreads, 0, s>>>(b, p, w.obs_flag);
+        scan_exclusive(w.obs_flag, w.obs_pos, nullptr, (int)nobs, nobs, w.tmp_total + 0, w.scan_work, s,
+                       &g_detect_launches);
+        LAUNCHED(1);
+    }
+    k_set_cobs<<<1, 1, 0, s>>>(w.tmp_total, sizes);
+    LAUNCHED(1);
+    if (na > 0) {
+        cudaMemsetAsync(w.row_count + na, 0, sizeof(int), s);
+        scan_exclusive(w.row_count, w.row_ptr, nullptr, na + 1, na + 1, w.tmp_total + 1, w.scan_work, s,
+                       &g_detect_launches);
+    }
+    k_sizes<<<1, 1, 0, s>>>(w.tmp_total, sizes, c_cap);
+    LAUNCHED(1);
+    if (nobs > 0) {
+        k_obs_fill<<<blocks_for(nobs), kThreads, 0, s>>>(b, w.obs_flag, w.obs_pos, c_cap, out.ci, out.cj);
+        LAUNCHED(1);
+    }
+    if (na > 0) {
+        k_pair_fill<<<blocks_for(na, 128), 128, 0, s>>>(b, p, w.grid, w.cell_of, w.cell_start, w.cell_body, w.cell_pr,
+                                                        w.row_ptr, sizes, c_cap, out.ci, out.cj);
+        k_row_sort<<<blocks_for(na), kThreads, 0, s>>>(na, w.row_ptr, sizes, c_cap, out.cj);
+        LAUNCHED(2);
+    }
+}
+
+void launch_geometry(const Bodies& b, const StepParams& p, Contacts& c, const Sizes* sizes, long long c_cap,
+                     const Contacts* old_c, const int* old_C, long long, cudaStream_t s) {
+    Contacts oc{};
+    if (old_c) oc = *old_c;
+    k_geometry<<<blocks_for(c_cap), kThreads, 0, s>>>(b, p, c, sizes, oc, old_c ? old_C : nullptr);
+    LAUNCHED(1);
+}
+
+void launch_assemble(const Bodies& b, const StepParams& p, const Contacts& c, Assembly& a, Sizes* sizes,
+                     long long c_cap, int* scan_work, int* tmp_total, cudaStream_t s) {
+    k_assemble<<<blocks_for(c_cap), kThreads, 0, s>>>(b, p, c, a, sizes);
+    LAUNCHED(1);
+    if (p.problem == kViscous) {
+        scan_exclusive(a.vflag, a.slot, &sizes->C, 0, c_cap, tmp_total, scan_work, s, &g_detect_launches);
+        // slot holds the exclusive scan; turn it into C + rank (flagged) or -1
+        k_viscous_slots<<<blocks_for(c_cap), kThreads, 0, s>>>(sizes, a.slot, a.vflag, a.slot);
+        k_set_extra<<<1, 1, 0, s>>>(tmp_total, sizes);
+        LAUNCHED(2);
+    }
+}
+
+void launch_incidence(const Bodies& b, const StepParams& p, const Contacts& c, const Assembly& a, Incidence& inc,
+                      const Sizes* sizes, long long c_cap, int* scan_work, int* tmp_total, cudaStream_t s) {
+    const int na = b.n - b.nin;
+    if (na <= 0) return;
+    cudaMemsetAsync(inc.count, 0, (na + 1) * sizeof(int), s);
+    cudaMemsetAsync(inc.jcount, 0, (na + 1) * sizeof(int), s);
+    k_inc_count<<<blocks_for(c_cap), kThreads, 0, s>>>(b.nin, c, sizes, inc.count);
+    scan_exclusive(inc.count, inc.ptr, nullptr, na + 1, na + 1, tmp_total, scan_work, s, &g_detect_launches);
+    k_inc_fill<<<blocks_for(c_cap), kThreads, 0, s>>>(b.nin, c, sizes, inc.ptr, inc.jcount, inc.idx);
+    k_inc_sort<<<blocks_for(na), kThreads, 0, s>>>(na, inc.ptr, inc.idx);
+    LAUNCHED(3);
+    if (p.problem != kFriction) {
+        k_inc_coef<<<blocks_for(2 * c_cap), kThreads, 0, s>>>(na, inc.ptr, inc.idx, a, inc.coef);
+        LAUNCHED(1);
+    }
+}
+
+void launch_gamma_update(const StepParams& p, Contacts& c, const Assembly& a, const double* lambda, const Sizes* sizes,
+                         long long c_cap, cudaStream_t s) {
+    k_gamma_update<<<blocks_for(c_cap), kThreads, 0, s>>>(p, c, a, lambda, sizes);
+    LAUNCHED(1);
+}
+
+void launch_update(const Bodies& b, const StepParams& p, const double* u, const Sizes* sizes, cudaStream_t s) {
+    if (b.n - b.nin <= 0) return;
+    k_update<<<blocks_for(b.n - b.nin), kThreads, 0, s>>>(b, p, u, sizes);
+    LAUNCHED(1);
+}
+
+void launch_amat(const Bodies& b, const StepParams& p, const Contacts& c, const Sizes* sizes, long long c_cap,
+                 const double* u, double* out, cudaStream_t s) {
+    k_amat<<<blocks_for(c_cap), kThreads, 0, s>>>(b, p, c, sizes, u, out);
+    LAUNCHED(1);
+}
+
+void launch_atmat(const Bodies& b, const StepParams& p, const Contacts& c, const Sizes* sizes, long long c_cap,
+                  const double* f, double* out, cudaStream_t s) {
+    cudaMemsetAsync(out, 0, 6 * (size_t)(b.n - b.nin) * sizeof(double), s);
+    k_atmat<<<blocks_for(c_cap), kThreads, 0, s>>>(b, p, c, sizes, f, out);
+    LAUNCHED(1);
+}
+
+}  // namespace scopi_gpu

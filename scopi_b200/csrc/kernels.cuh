@@ -1,0 +1,147 @@
+// kernels.cuh -- host-side launchers of the SCoPI B200 kernels (one translation unit each).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace scopi_gpu {
+
+// ---------------------------------------------------------------- scan.cu
+size_t scan_work_ints(long long n_max);
+// out[k] = sum_{i<k} in[i] for k < n with n = *n_dev (or n_host when n_dev is null); *total_dev = sum.
+void scan_exclusive(const int* in, int* out, const int* n_dev, int n_host, long long n_max, int* total_dev, int* work,
+                    cudaStream_t s, long long* launches);
+
+// -------------------------------------------------------------- detect.cu
+struct StepParams {
+    int dim;
+    int problem;
+    int vap;
+    int kd_filter;        // contact_kdtree: candidate needs |xi-xj|^2 < kd_tree_radius
+    double dmax;
+    double kd_radius;
+    double dt;
+    double gamma0, gamma_min, gamma_tol, mu;
+};
+
+struct DetectWork {
+    Grid* grid;               // device
+    double* bbox_partial;     // kBBoxBlocks * 8
+    int* cell_count;          // cell_cap + 1
+    int* cell_start;          // cell_cap + 1
+    int* cell_fill;           // cell_cap
+    int* cell_of;             // na
+    int* cell_body;           // na (body index, sorted by cell)
+    double4* cell_pr;         // na (x, y, z, r) sorted by cell
+    int* row_count;           // na + 1
+    int* row_ptr;             // na + 1
+    int* obs_flag;            // nin * na
+    int* obs_pos;             // nin * na
+    int* tmp_total;           // 4 ints
+    int* scan_work;
+    long long cell_cap;
+    long long obs_cap;        // nin * na
+};
+
+struct Assembly {             // FP64 Jacobian rows, K = 1 (normal) problems
+    double* bn;               // C*3  n
+    double* bai;              // C*3  R_i^T (r_i x n)
+    double* baj;              // C*3  -R_j^T (r_j x n)
+    double* bP;               // C*18 friction: P_i = R_i^T [r_i]x, P_j = R_j^T [r_j]x
+    double* cvec;             // C (K=1) or 3C (friction)
+    int* vflag;               // C viscous flag, then scanned -> slot
+    int* slot;                // C viscous second multiplier (-1 = none)
+};
+
+struct Incidence {            // particle-major transpose of the contact list
+    int* count;               // na
+    int* jcount;              // na (j-side incidences)
+    int* ptr;                 // na + 1
+    int* idx;                 // 2C: contact | side<<31
+    double* coef;             // 2C*6 (K=1: sign*n, a_side)
+};
+
+long long detect_launches();
+void launch_obstacles_move(const Bodies& b, double dt, int dim, cudaStream_t s);
+void launch_vap(const Bodies& b, const StepParams& p, cudaStream_t s);
+// Full detection: leaves a sorted (ci, cj) list in `out` and the count in sizes->C.
+void launch_detect(const Bodies& b, const StepParams& p, DetectWork& w, Contacts& out, Sizes* sizes, long long c_cap,
+                   cudaStream_t s);
+// Closest points of the listed pairs + viscous gamma transfer from the previous list.
+void launch_geometry(const Bodies& b, const StepParams& p, Contacts& c, const Sizes* sizes, long long c_cap,
+                     const Contacts* old_c, const int* old_C, long long old_cap, cudaStream_t s);
+void launch_assemble(const Bodies& b, const StepParams& p, const Contacts& c, Assembly& a, Sizes* sizes,
+                     long long c_cap, int* scan_work, int* tmp_total, cudaStream_t s);
+void launch_incidence(const Bodies& b, const StepParams& p, const Contacts& c, const Assembly& a, Incidence& inc,
+                      const Sizes* sizes, long long c_cap, int* scan_work, int* tmp_total, cudaStream_t s);
+void launch_gamma_update(const StepParams& p, Contacts& c, const Assembly& a, const double* lambda, const Sizes* sizes,
+                         long long c_cap, cudaStream_t s);
+// v += dt*u_v, omega += dt*u_w, then pos/q integration (u = M^-1 B^T lambda, may be null).
+void launch_update(const Bodies& b, const StepParams& p, const double* u, const Sizes* sizes, cudaStream_t s);
+void launch_amat(const Bodies& b, const StepParams& p, const Contacts& c, const Sizes* sizes, long long c_cap,
+                 const double* u, double* out, cudaStream_t s);
+void launch_atmat(const Bodies& b, const StepParams& p, const Contacts& c, const Sizes* sizes, long long c_cap,
+                  const double* f, double* out, cudaStream_t s);
+
+// --------------------------------------------------------------- apgd.cu
+struct ApgdSettings {
+    double alpha;
+    double tol;
+    long long max_ite;
+    int dynamic;
+    double dt;
+    double mu;
+};
+
+struct ApgdResult {           // written by block 0 of the persistent kernel
+    long long iterations;
+    long long backtracks;
+    long long restarts;
+    int converged;
+    int lam_buf;              // which of the three lambda buffers holds the result
+    int u_buf;                // which u buffer holds M^-1 B^T lambda of the result
+    int error;                // barrier timeout
+    double last_step;
+    double pad;
+};
+
+template <typename T>
+struct SolveBuffers {
+    const T* bn;
+    const T* bai;
+    const T* baj;
+    const T* bP;
+    const T* cvec;            // linear term (per multiplier)
+    const double* shift;      // correction solves: solution offset lambda0 (null = none)
+    const int* inc_ptr;
+    const int* inc_idx;
+    const T* inc_coef;
+    T* lam[3];
+    T* u[3];                  // per active particle: 6 values
+    T* g;
+    double* partials;         // 2 * max_blocks * kPartials
+    unsigned int* barrier;    // 4 uints (zeroed)
+    ApgdResult* result;
+};
+
+int apgd_max_blocks(int problem, int dim, bool fp32);
+long long apgd_launches();
+// Persistent APGD solve; contacts / multipliers counts come from `sizes`.
+template <typename T>
+cudaError_t launch_apgd_invm(const Bodies& b, const StepParams& p, const ApgdSettings& st, const Contacts& c,
+                             const Assembly& a, SolveBuffers<T>& sb, const T* invm, const Sizes* sizes, int nblocks,
+                             cudaStream_t s);
+// FP64 helpers of the mixed form.
+template <typename Src, typename Dst>
+void launch_convert(const Src* in, Dst* out, long long n_max, const int* n_dev, int mult, cudaStream_t s);
+void launch_particle_pass64(const Bodies& b, const StepParams& p, const Contacts& c, const Assembly& a,
+                            const Incidence& inc, const double* invm, const double* lam, double* u, cudaStream_t s);
+// g = dt^2 B u + c and the violation max(0, -min gap) (bits of a non-negative double in *viol_bits).
+void launch_residual64(const Bodies& b, const StepParams& p, const Contacts& c, const Assembly& a, const double* u,
+                       double* g, unsigned long long* viol_bits, const Sizes* sizes, long long c_cap, cudaStream_t s);
+// lambda64 += delta32 then projection onto the cone / orthant in FP64.
+void launch_accumulate(const StepParams& p, const Contacts& c, const Assembly& a, double* lam64, const float* delta,
+                       const Sizes* sizes, long long c_cap, int first, cudaStream_t s);
+
+}  // namespace scopi_gpu

@@ -1,0 +1,792 @@
+// scopi_gpu.cu -- C ABI (include/scopi_gpu.h): handle, device memory, and the per-step
+// sequence of ScopiSolver::run (include/scopi/solver.hpp:274-302) on one B200.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/scopi_gpu.h"
+#include "kernels.cuh"
+
+using namespace scopi_gpu;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct DevMem {
+    std::vector<void*> ptrs;
+    ~DevMem() { release(); }
+    void release() {
+        for (void* p : ptrs) cudaFree(p);
+        ptrs.clear();
+    }
+};
+
+}  // namespace
+
+struct scopi_gpu_handle {
+    scopi_gpu_params P{};
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    long long launches0 = 0;
+
+    // bodies
+    int n = 0, nin = 0, na = 0;
+    DevMem body_mem;
+    int* d_shape = nullptr;
+    double *d_pos = nullptr, *d_q = nullptr, *d_v = nullptr, *d_omega = nullptr, *d_vd = nullptr, *d_omega_d = nullptr,
+           *d_f = nullptr, *d_m = nullptr, *d_j = nullptr, *d_radius = nullptr, *d_length = nullptr;
+    double* d_invm64 = nullptr;
+    float* d_invm32 = nullptr;
+    // per-particle solve buffers
+    double* d_u64[3] = {nullptr, nullptr, nullptr};
+    double* d_ufin = nullptr;
+    float* d_u32[3] = {nullptr, nullptr, nullptr};
+    DetectWork dw{};
+
+    // contact-capacity buffers
+    long long c_cap = 0;
+    DevMem cap_mem;
+    Contacts cur{}, old{};
+    Sizes* d_sizes_cur = nullptr;
+    Sizes* d_sizes_old = nullptr;
+    bool has_old = false;
+    Assembly as{};
+    Incidence inc{};
+    double* d_lam64[3] = {nullptr, nullptr, nullptr};
+    double* d_g64 = nullptr;
+    double* d_res64 = nullptr;
+    double* d_lamacc = nullptr;
+    float *d_bn32 = nullptr, *d_bai32 = nullptr, *d_baj32 = nullptr, *d_bP32 = nullptr, *d_cvec32 = nullptr,
+          *d_coef32 = nullptr;
+    float* d_lam32[3] = {nullptr, nullptr, nullptr};
+    float* d_g32 = nullptr;
+
+    // fixed small buffers
+    DevMem fixed_mem;
+    double* d_partials = nullptr;
+    unsigned int* d_barrier = nullptr;
+    ApgdResult* d_result = nullptr;
+    unsigned long long* d_viol = nullptr;
+    Sizes* h_sizes = nullptr;          // pinned
+    ApgdResult* h_result = nullptr;    // pinned
+    unsigned long long* h_viol = nullptr;
+    int max_blocks64 = 0, max_blocks32 = 0;
+
+    // results of the last step
+    const double* last_lambda = nullptr;
+    long long last_M = 0;
+    scopi_gpu_stats stats{};
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+
+    int fail(int code, const std::string& msg) {
+        err = msg;
+        return code;
+    }
+    int cuda_fail(cudaError_t e, const char* where) {
+        err = std::string(where) + ": " + cudaGetErrorString(e);
+        return SCOPI_GPU_ECUDA;
+    }
+    int mult_per_contact() const { return P.problem == SCOPI_GPU_FRICTION ? 3 : (P.problem == SCOPI_GPU_VISCOUS ? 2 : 1); }
+    bool mixed() const { return P.precision == SCOPI_GPU_MIXED; }
+
+    Bodies bodies() const {
+        Bodies b;
+        b.n = n;
+        b.nin = nin;
+        b.shape = d_shape;
+        b.pos = d_pos;
+        b.q = d_q;
+        b.v = d_v;
+        b.omega = d_omega;
+        b.vd = d_vd;
+        b.omega_d = d_omega_d;
+        b.f = d_f;
+        b.m = d_m;
+        b.j = d_j;
+        b.radius = d_radius;
+        b.length = d_length;
+        return b;
+    }
+    StepParams step_params(double dt) const {
+        StepParams s;
+        s.dim = P.dim;
+        s.problem = P.problem;
+        s.vap = P.vap;
+        s.kd_filter = P.contact_method == SCOPI_GPU_KDTREE ? 1 : 0;
+        s.dmax = P.dmax;
+        s.kd_radius = P.kd_tree_radius;
+        s.dt = dt;
+        s.gamma0 = P.gamma;
+        s.gamma_min = P.gamma_min;
+        s.gamma_tol = P.gamma_tol;
+        s.mu = P.mu;
+        return s;
+    }
+
+    template <typename T>
+    cudaError_t alloc(DevMem& m, T*& p, size_t count) {
+        void* q = nullptr;
+        cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+        if (e != cudaSuccess) return e;
+        m.ptrs.push_back(q);
+        p = static_cast<T*>(q);
+        return cudaSuccess;
+    }
+
+    int alloc_fixed() {
+        cudaError_t e;
+        max_blocks64 = apgd_max_blocks(P.problem, P.dim, false);
+        max_blocks32 = apgd_max_blocks(P.problem, P.dim, true);
+        const int mb = std::max(std::max(max_blocks64, max_blocks32), 1);
+        if ((e = alloc(fixed_mem, d_partials, 2 * (size_t)mb * 8)) != cudaSuccess) return cuda_fail(e, "alloc");
+        if ((e = alloc(fixed_mem, d_barrier, 4)) != cudaSuccess) return cuda_fail(e, "alloc");
+        if ((e = alloc(fixed_mem, d_result, 1)) != cudaSuccess) return cuda_fail(e, "alloc");
+        if ((e = alloc(fixed_mem, d_viol, 1)) != cudaSuccess) return cuda_fail(e, "alloc");
+        if ((e = alloc(fixed_mem, d_sizes_cur, 1)) != cudaSuccess) return cuda_fail(e, "alloc");
+        if ((e = alloc(fixed_mem, d_sizes_old, 1)) != cudaSuccess) return cuda_fail(e, "alloc");
+        cudaMemset(d_sizes_cur, 0, sizeof(Sizes));
+        cudaMemset(d_sizes_old, 0, sizeof(Sizes));
+        cudaMemset(d_barrier, 0, 4 * sizeof(unsigned int));
+        if ((e = cudaMallocHost(&h_sizes, sizeof(Sizes))) != cudaSuccess) return cuda_fail(e, "cudaMallocHost");
+        if ((e = cudaMallocHost(&h_result, sizeof(ApgdResult))) != cudaSuccess) return cuda_fail(e, "cudaMallocHost");
+        if ((e = cudaMallocHost(&h_viol, sizeof(unsigned long long))) != cudaSuccess)
+            return cuda_fail(e, "cudaMallocHost");
+        for (auto& x : ev)
+            if ((e = cudaEventCreate(&x)) != cudaSuccess) return cuda_fail(e, "cudaEventCreate");
+        return 0;
+    }
+
+    // Buffers whose size follows the number of bodies.
+    int alloc_bodies(int n_, int nin_) {
+        body_mem.release();
+        n = n_;
+        nin = nin_;
+        na = n - nin;
+        cudaError_t e;
+#define A(p, c) \
+    if ((e = alloc(body_mem, p, (c))) != cudaSuccess) return cuda_fail(e, "cudaMalloc(bodies)");
+        A(d_shape, n) A(d_pos, 3 * (size_t)n) A(d_q, 4 * (size_t)n) A(d_v, 3 * (size_t)n) A(d_omega, 3 * (size_t)n)
+        A(d_vd, 3 * (size_t)n) A(d_omega_d, 3 * (size_t)n) A(d_f, 3 * (size_t)n) A(d_m, n) A(d_j, 3 * (size_t)n)
+        A(d_radius, n) A(d_length, n) A(d_invm64, 4 * (size_t)na + 4) A(d_invm32, 4 * (size_t)na + 4)
+        A(d_ufin, 6 * (size_t)na + 6)
+        for (int k = 0; k < 3; ++k) {
+            A(d_u64[k], 6 * (size_t)na + 6)
+            A(d_u32[k], 6 * (size_t)na + 6)
+        }
+        dw.cell_cap = std::max<long long>(4LL * na, 4096);
+        dw.obs_cap = (long long)nin * na;
+        A(dw.grid, 1) A(dw.bbox_partial, 8 * 4 * kSMs) A(dw.cell_count, dw.cell_cap + 1) A(dw.cell_start, dw.cell_cap + 1)
+        A(dw.cell_fill, dw.cell_cap) A(dw.cell_of, na + 1) A(dw.cell_body, na + 1) A(dw.cell_pr, na + 1)
+        A(dw.row_count, na + 1) A(dw.row_ptr, na + 1) A(dw.obs_flag, dw.obs_cap + 1) A(dw.obs_pos, dw.obs_cap + 1)
+        A(dw.tmp_total, 4)
+        const long long scan_max = std::max<long long>(std::max<long long>(dw.cell_cap + 1, dw.obs_cap + 1), na + 1);
+        A(dw.scan_work, scan_work_ints(std::max<long long>(scan_max, 1LL << 26)))
+        A(inc.count, na + 1) A(inc.jcount, na + 1) A(inc.ptr, na + 1)
+#undef A
+        return 0;
+    }
+
+    // Buffers whose size follows the contact capacity.
+    int alloc_contacts(long long cap) {
+        cap_mem.release();
+        c_cap = cap;
+        has_old = false;
+        const long long M = cap * mult_per_contact();
+        cudaError_t e;
+#define A(p, c) \
+    if ((e = alloc(cap_mem, p, (c))) != cudaSuccess) return cuda_fail(e, "cudaMalloc(contacts)");
+        for (Contacts* c : {&cur, &old}) {
+            A(c->ci, cap) A(c->cj, cap) A(c->dij, cap) A(c->nij, 3 * cap) A(c->pi, 3 * cap) A(c->pj, 3 * cap)
+            A(c->gamma, cap)
+        }
+        A(as.bn, 3 * cap) A(as.bai, 3 * cap) A(as.baj, 3 * cap)
+        if (P.problem == SCOPI_GPU_FRICTION) A(as.bP, 18 * cap)
+        A(as.cvec, (P.problem == SCOPI_GPU_FRICTION ? 3 : 1) * cap) A(as.vflag, cap) A(as.slot, cap)
+        A(inc.idx, 2 * cap) A(inc.coef, 12 * cap)
+        for (int k = 0; k < 3; ++k) A(d_lam64[k], M)
+        A(d_g64, M) A(d_res64, M) A(d_lamacc, M)
+        if (mixed()) {
+            A(d_bn32, 3 * cap) A(d_bai32, 3 * cap) A(d_baj32, 3 * cap)
+            if (P.problem == SCOPI_GPU_FRICTION) A(d_bP32, 18 * cap)
+            A(d_cvec32, (P.problem == SCOPI_GPU_FRICTION ? 3 : 1) * cap) A(d_coef32, 12 * cap)
+            for (int k = 0; k < 3; ++k) A(d_lam32[k], M)
+            A(d_g32, M)
+        }
+#undef A
+        cudaMemsetAsync(d_sizes_cur, 0, sizeof(Sizes), stream);
+        cudaMemsetAsync(d_sizes_old, 0, sizeof(Sizes), stream);
+        return 0;
+    }
+
+    long long launches() const { return detect_launches() + apgd_launches(); }
+
+    // contact detection + closest points + assembly + incidence lists into `cur`
+    int detect_and_assemble(double dt, bool assemble) {
+        Bodies b = bodies();
+        StepParams sp = step_params(dt);
+        for (int attempt = 0; attempt < 4; ++attempt) {
+            cudaMemsetAsync(d_sizes_cur, 0, sizeof(Sizes), stream);
+            launch_detect(b, sp, dw, cur, d_sizes_cur, c_cap, stream);
+            cudaMemcpyAsync(h_sizes, d_sizes_cur, sizeof(Sizes), cudaMemcpyDeviceToHost, stream);
+            cudaError_t e = cudaStreamSynchronize(stream);
+            if (e != cudaSuccess) return cuda_fail(e, "detect");
+            if (!h_sizes->overflow) break;
+            // grow: keep the previous contacts (viscous gamma transfer) across the reallocation
+            const long long need = (long long)std::ceil(1.3 * ((double)h_sizes->C + 1.0)) + 1024;
+            long long total = 0;
+            {
+                // the true count is C_obs + active rows; recompute it from the scan totals
+                int tot[2] = {0, 0};
+                cudaMemcpy(tot, dw.tmp_total, 2 * sizeof(int), cudaMemcpyDeviceToHost);
+                total = (long long)tot[0] + tot[1];
+            }
+            const long long newcap = std::max(need, (long long)(1.3 * total) + 1024);
+            int rc = regrow(newcap);
+            if (rc) return rc;
+            if (attempt == 3) return fail(SCOPI_GPU_ENOMEM, "contact capacity could not be grown");
+        }
+        if (!assemble) {
+            launch_geometry(b, sp, cur, d_sizes_cur, c_cap, has_old ? &old : nullptr, has_old ? &d_sizes_old->C : nullptr,
+                            c_cap, stream);
+            return 0;
+        }
+        launch_geometry(b, sp, cur, d_sizes_cur, c_cap, has_old ? &old : nullptr, has_old ? &d_sizes_old->C : nullptr,
+                        c_cap, stream);
+        launch_assemble(b, sp, cur, as, d_sizes_cur, c_cap, dw.scan_work, dw.tmp_total + 2, stream);
+        launch_incidence(b, sp, cur, as, inc, d_sizes_cur, c_cap, dw.scan_work, dw.tmp_total + 2, stream);
+        cudaMemcpyAsync(h_sizes, d_sizes_cur, sizeof(Sizes), cudaMemcpyDeviceToHost, stream);
+        cudaError_t e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cuda_fail(e, "assemble");
+        return 0;
+    }
+
+    int regrow(long long newcap) {
+        // copy the previous contact list (ci, cj, gamma) so the transfer still works
+        std::vector<int> oci, ocj;
+        std::vector<double> ogam;
+        Sizes osz{};
+        if (has_old) {
+            cudaMemcpy(&osz, d_sizes_old, sizeof(Sizes), cudaMemcpyDeviceToHost);
+            oci.resize(osz.C);
+            ocj.resize(osz.C);
+            ogam.resize(osz.C);
+            if (osz.C > 0) {
+                cudaMemcpy(oci.data(), old.ci, osz.C * sizeof(int), cudaMemcpyDeviceToHost);
+                cudaMemcpy(ocj.data(), old.cj, osz.C * sizeof(int), cudaMemcpyDeviceToHost);
+                cudaMemcpy(ogam.data(), old.gamma, osz.C * sizeof(double), cudaMemcpyDeviceToHost);
+            }
+        }
+        const bool had = has_old;
+        int rc = alloc_contacts(newcap);
+        if (rc) return rc;
+        if (had) {
+            if (osz.C > 0) {
+                cudaMemcpy(old.ci, oci.data(), osz.C * sizeof(int), cudaMemcpyHostToDevice);
+                cudaMemcpy(old.cj, ocj.data(), osz.C * sizeof(int), cudaMemcpyHostToDevice);
+                cudaMemcpy(old.gamma, ogam.data(), osz.C * sizeof(double), cudaMemcpyHostToDevice);
+            }
+            Sizes s{};
+            s.C = osz.C;
+            cudaMemcpy(d_sizes_old, &s, sizeof(Sizes), cudaMemcpyHostToDevice);
+            has_old = true;
+        }
+        return 0;
+    }
+
+    int nblocks_for(int maxb, long long work) const {
+        long long b = (work + 255) / 256;
+        b = std::max<long long>(b, 1);
+        return (int)std::min<long long>(b, maxb);
+    }
+
+    template <typename T>
+    int run_apgd(SolveBuffers<T>& sb, const T* invm, int maxb, double dt, double tol, long long max_ite, long long M) {
+        Bodies b = bodies();
+        StepParams sp = step_params(dt);
+        ApgdSettings st;
+        st.alpha = P.alpha;
+        st.tol = tol;
+        st.max_ite = max_ite;
+        st.dynamic = P.dynamic_descent;
+        st.dt = dt;
+        st.mu = P.mu;
+        cudaMemsetAsync(sb.lam[0], 0, M * sizeof(T), stream);
+        cudaMemsetAsync(sb.lam[1], 0, M * sizeof(T), stream);
+        cudaMemsetAsync(sb.u[0], 0, 6 * (size_t)na * sizeof(T), stream);
+        cudaMemsetAsync(sb.u[1], 0, 6 * (size_t)na * sizeof(T), stream);
+        cudaMemsetAsync(d_barrier, 0, 4 * sizeof(unsigned int), stream);
+        const int nb = nblocks_for(maxb, std::max<long long>(h_sizes->C, na));
+        cudaError_t e = launch_apgd_invm<T>(b, sp, st, cur, as, sb, invm, d_sizes_cur, nb, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "APGD launch");
+        cudaMemcpyAsync(h_result, d_result, sizeof(ApgdResult), cudaMemcpyDeviceToHost, stream);
+        e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cuda_fail(e, "APGD");
+        if (h_result->error == 1) return fail(SCOPI_GPU_ETIMEOUT, "APGD grid barrier timed out");
+        return 0;
+    }
+
+    int step(double dt) {
+        Bodies b = bodies();
+        StepParams sp = step_params(dt);
+        cudaEventRecord(ev[0], stream);
+        launch_obstacles_move(b, dt, P.dim, stream);
+        // vap does not read the contacts (vap_fixed.hpp:45-55, vap_fpd.hpp:69-81): run it first
+        launch_vap(b, sp, stream);
+        int rc = detect_and_assemble(dt, true);
+        if (rc) return rc;
+        const int C = h_sizes->C;
+        const long long M = P.problem == SCOPI_GPU_FRICTION ? 3LL * C : (long long)C + h_sizes->n_extra;
+        cudaEventRecord(ev[1], stream);
+        const double* ufin = nullptr;
+        stats.iterations = stats.backtracks = stats.restarts = stats.fp32_iterations = stats.corrections = 0;
+        stats.converged = 1;
+        stats.status = 0;
+        stats.violation = 0.0;
+        float ms_apgd = 0.0f;
+        if (C > 0) {
+            cudaEvent_t a0, a1;
+            cudaEventCreate(&a0);
+            cudaEventCreate(&a1);
+            if (!mixed()) {
+                SolveBuffers<double> sb{};
+                sb.bn = as.bn;
+                sb.bai = as.bai;
+                sb.baj = as.baj;
+                sb.bP = as.bP;
+                sb.cvec = as.cvec;
+                sb.shift = nullptr;
+                sb.inc_ptr = inc.ptr;
+                sb.inc_idx = inc.idx;
+                sb.inc_coef = inc.coef;
+                for (int k = 0; k < 3; ++k) {
+                    sb.lam[k] = d_lam64[k];
+                    sb.u[k] = d_u64[k];
+                }
+                sb.g = d_g64;
+                sb.partials = d_partials;
+                sb.barrier = d_barrier;
+                sb.result = d_result;
+                cudaEventRecord(a0, stream);
+                rc = run_apgd<double>(sb, d_invm64, max_blocks64, dt, P.tolerance, P.max_ite, M);
+                cudaEventRecord(a1, stream);
+                if (rc) return rc;
+                accumulate_stats(false);
+                last_lambda = d_lam64[h_result->lam_buf];
+                ufin = d_u64[h_result->u_buf];
+            } else {
+                rc = mixed_solve(dt, M, a0, a1, ms_apgd);
+                if (rc) return rc;
+                last_lambda = d_lamacc;
+                ufin = d_ufin;
+            }
+            cudaEventSynchronize(a1);
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, a0, a1);
+            if (!mixed()) ms_apgd = ms;
+            cudaEventDestroy(a0);
+            cudaEventDestroy(a1);
+            // violation of the returned multipliers (FP64 residual)
+            cudaMemsetAsync(d_viol, 0, sizeof(unsigned long long), stream);
+            launch_residual64(b, sp, cur, as, ufin, d_res64, d_viol, d_sizes_cur, c_cap, stream);
+            cudaMemcpyAsync(h_viol, d_viol, sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream);
+            if (P.problem == SCOPI_GPU_VISCOUS) launch_gamma_update(sp, cur, as, last_lambda, d_sizes_cur, c_cap, stream);
+        } else {
+            last_lambda = nullptr;
+            *h_viol = 0;
+        }
+        last_M = M;
+        cudaEventRecord(ev[2], stream);
+        launch_update(b, sp, ufin, d_sizes_cur, stream);
+        cudaEventRecord(ev[3], stream);
+        cudaError_t e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cuda_fail(e, "step");
+        double viol;
+        std::memcpy(&viol, h_viol, sizeof(double));
+        stats.violation = viol;
+        stats.contacts = C;
+        float t_step = 0, t_solve = 0;
+        cudaEventElapsedTime(&t_step, ev[0], ev[3]);
+        cudaEventElapsedTime(&t_solve, ev[1], ev[2]);
+        stats.ms_step = t_step;
+        stats.ms_solve = t_solve;
+        stats.ms_apgd_kernel = ms_apgd;
+        stats.steps += 1;
+        // the contacts of this step become the previous ones (std::swap, solver.hpp:301)
+        std::swap(cur, old);
+        std::swap(d_sizes_cur, d_sizes_old);
+        has_old = true;
+        if (!stats.converged) stats.status = SCOPI_GPU_ENOCONV;
+        return 0;
+    }
+
+    void accumulate_stats(bool fp32) {
+        stats.iterations += h_result->iterations;
+        stats.backtracks += h_result->backtracks;
+        stats.restarts += h_result->restarts;
+        if (fp32) stats.fp32_iterations += h_result->iterations;
+        stats.converged = stats.converged && h_result->converged;
+    }
+
+    // FP32 APGD iterations with an FP64 outer correction: after each FP32 solve the
+    // residual g = Q lambda + c and the violation are recomputed in FP64, and APGD is
+    // rerun in FP32 on the correction delta (linear term g, constraint lambda + delta in K).
+    int mixed_solve(double dt, long long M, cudaEvent_t a0, cudaEvent_t a1, float& ms_apgd) {
+        Bodies b = bodies();
+        StepParams sp = step_params(dt);
+        const int C = h_sizes->C;
+        const int per = P.problem == SCOPI_GPU_FRICTION ? 3 : 1;
+        launch_convert<double, float>(as.bn, d_bn32, 3 * c_cap, &d_sizes_cur->C, 3, stream);
+        launch_convert<double, float>(as.bai, d_bai32, 3 * c_cap, &d_sizes_cur->C, 3, stream);
+        launch_convert<double, float>(as.baj, d_baj32, 3 * c_cap, &d_sizes_cur->C, 3, stream);
+        if (P.problem == SCOPI_GPU_FRICTION)
+            launch_convert<double, float>(as.bP, d_bP32, 18 * c_cap, &d_sizes_cur->C, 18, stream);
+        else
+            launch_convert<double, float>(inc.coef, d_coef32, 12 * c_cap, &d_sizes_cur->C, 12, stream);
+        launch_convert<double, float>(as.cvec, d_cvec32, per * c_cap, &d_sizes_cur->C, per, stream);
+        SolveBuffers<float> sb{};
+        sb.bn = d_bn32;
+        sb.bai = d_bai32;
+        sb.baj = d_baj32;
+        sb.bP = d_bP32;
+        sb.cvec = d_cvec32;
+        sb.shift = nullptr;
+        sb.inc_ptr = inc.ptr;
+        sb.inc_idx = inc.idx;
+        sb.inc_coef = d_coef32;
+        for (int k = 0; k < 3; ++k) {
+            sb.lam[k] = d_lam32[k];
+            sb.u[k] = d_u32[k];
+        }
+        sb.g = d_g32;
+        sb.partials = d_partials;
+        sb.barrier = d_barrier;
+        sb.result = d_result;
+        float total = 0.0f;
+        cudaEventRecord(a0, stream);
+        int rc = run_apgd<float>(sb, d_invm32, max_blocks32, dt, P.tolerance, P.max_ite, M);
+        cudaEventRecord(a1, stream);
+        if (rc) return rc;
+        cudaEventSynchronize(a1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a0, a1);
+        total += ms;
+        accumulate_stats(true);
+        launch_accumulate(sp, cur, as, d_lamacc, d_lam32[h_result->lam_buf], d_sizes_cur, c_cap, 1, stream);
+        for (int k = 0;; ++k) {
+            launch_particle_pass64(b, sp, cur, as, inc, d_invm64, d_lamacc, d_ufin, stream);
+            cudaMemsetAsync(d_viol, 0, sizeof(unsigned long long), stream);
+            launch_residual64(b, sp, cur, as, d_ufin, d_res64, d_viol, d_sizes_cur, c_cap, stream);
+            cudaMemcpyAsync(h_viol, d_viol, sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream);
+            cudaError_t e = cudaStreamSynchronize(stream);
+            if (e != cudaSuccess) return cuda_fail(e, "mixed residual");
+            double viol;
+            std::memcpy(&viol, h_viol, sizeof(double));
+            if (viol <= P.mixed_violation_tol || k >= P.mixed_max_corrections) break;
+            // correction solve
+            launch_convert<double, float>(d_res64, d_cvec32, per * c_cap, &d_sizes_cur->C, per, stream);
+            sb.shift = d_lamacc;
+            cudaEventRecord(a0, stream);
+            rc = run_apgd<float>(sb, d_invm32, max_blocks32, dt, P.tolerance, P.max_ite, M);
+            cudaEventRecord(a1, stream);
+            if (rc) return rc;
+            cudaEventSynchronize(a1);
+            cudaEventElapsedTime(&ms, a0, a1);
+            total += ms;
+            accumulate_stats(true);
+            stats.corrections += 1;
+            launch_accumulate(sp, cur, as, d_lamacc, d_lam32[h_result->lam_buf], d_sizes_cur, c_cap, 0, stream);
+        }
+        (void)C;
+        (void)M;
+        ms_apgd = total;
+        return 0;
+    }
+};
+
+extern "C" {
+
+void scopi_gpu_default_params(scopi_gpu_params* p, int32_t dim) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->dim = dim;
+    p->problem = SCOPI_GPU_NOFRICTION;
+    p->vap = SCOPI_GPU_VAP_FIXED;
+    p->contact_method = SCOPI_GPU_KDTREE;
+    p->precision = SCOPI_GPU_FP64;
+    p->dynamic_descent = 1;
+    p->max_ite = 10000;
+    p->dmax = 2.0;
+    p->kd_tree_radius = 17.0;
+    p->alpha = 0.05;
+    p->tolerance = 1e-7;
+    p->mu = 0.1;
+    p->gamma = 0.0;
+    p->gamma_min = -2.0;
+    p->gamma_tol = 1e-6;
+    p->mixed_violation_tol = 1e-6;
+    p->mixed_max_corrections = 3;
+    p->device = 0;
+}
+
+int32_t scopi_gpu_create(const scopi_gpu_params* p, scopi_gpu_handle** out) {
+    if (!p || !out) {
+        g_create_error = "null argument";
+        return SCOPI_GPU_EINVAL;
+    }
+    *out = nullptr;
+    if (p->dim != 2 && p->dim != 3) {
+        g_create_error = "dim must be 2 or 3";
+        return SCOPI_GPU_EINVAL;
+    }
+    if (p->problem < 0 || p->problem > 2 || p->vap < 0 || p->vap > 1 || p->contact_method < 0 ||
+        p->contact_method > 1 || p->precision < 0 || p->precision > 1 || p->alpha <= 0 || p->max_ite < 1) {
+        g_create_error = "invalid parameter";
+        return SCOPI_GPU_EINVAL;
+    }
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev <= p->device) {
+        g_create_error = std::string("no CUDA device: ") + cudaGetErrorString(e);
+        return SCOPI_GPU_ECUDA;
+    }
+    auto* h = new scopi_gpu_handle();
+    h->P = *p;
+    h->dev = p->device;
+    cudaSetDevice(h->dev);
+    if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+        g_create_error = std::string("cudaStreamCreate: ") + cudaGetErrorString(e);
+        delete h;
+        return SCOPI_GPU_ECUDA;
+    }
+    int rc = h->alloc_fixed();
+    if (rc) {
+        g_create_error = h->err;
+        scopi_gpu_destroy(h);
+        return rc;
+    }
+    h->launches0 = h->launches();
+    *out = h;
+    return 0;
+}
+
+int32_t scopi_gpu_destroy(scopi_gpu_handle* h) {
+    if (!h) return SCOPI_GPU_EINVAL;
+    cudaSetDevice(h->dev);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    h->body_mem.release();
+    h->cap_mem.release();
+    h->fixed_mem.release();
+    if (h->h_sizes) cudaFreeHost(h->h_sizes);
+    if (h->h_result) cudaFreeHost(h->h_result);
+    if (h->h_viol) cudaFreeHost(h->h_viol);
+    for (auto& x : h->ev)
+        if (x) cudaEventDestroy(x);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return 0;
+}
+
+int32_t scopi_gpu_set_particles(scopi_gpu_handle* h, const scopi_gpu_particles* p) {
+    if (!h || !p || p->n < 0 || p->nb_inactive < 0 || p->nb_inactive > p->n || p->n >= (1LL << 30))
+        return h ? h->fail(SCOPI_GPU_EINVAL, "invalid particle container") : SCOPI_GPU_EINVAL;
+    if (!p->shape || !p->pos || !p->q || !p->v || !p->omega || !p->vd || !p->omega_d || !p->f || !p->m || !p->j ||
+        !p->radius || !p->length)
+        return h->fail(SCOPI_GPU_EINVAL, "null particle array");
+    const int n = (int)p->n, nin = (int)p->nb_inactive;
+    for (int i = 0; i < n; ++i) {
+        const int s = p->shape[i];
+        if (i >= nin && s != SCOPI_GPU_SPHERE)
+            return h->fail(SCOPI_GPU_EUNSUPPORTED, "active bodies must be spheres");
+        if (s < 0 || s > 2) return h->fail(SCOPI_GPU_EINVAL, "unknown shape");
+        if (s == SCOPI_GPU_SEGMENT && h->P.dim != 2) return h->fail(SCOPI_GPU_EUNSUPPORTED, "segments are 2D only");
+    }
+    cudaSetDevice(h->dev);
+    cudaStreamSynchronize(h->stream);
+    if (n != h->n || nin != h->nin) {
+        int rc = h->alloc_bodies(n, nin);
+        if (rc) return rc;
+        if (h->c_cap == 0) {
+            rc = h->alloc_contacts(std::max<long long>(8192, 6LL * (n - nin) + 2LL * nin * 64));
+            if (rc) return rc;
+        } else {
+            h->has_old = false;
+        }
+    }
+    cudaStream_t s = h->stream;
+    auto up = [&](void* dst, const void* src, size_t bytes) { cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s); };
+    up(h->d_shape, p->shape, n * sizeof(int));
+    up(h->d_pos, p->pos, 3 * (size_t)n * sizeof(double));
+    up(h->d_q, p->q, 4 * (size_t)n * sizeof(double));
+    up(h->d_v, p->v, 3 * (size_t)n * sizeof(double));
+    up(h->d_omega, p->omega, 3 * (size_t)n * sizeof(double));
+    up(h->d_vd, p->vd, 3 * (size_t)n * sizeof(double));
+    up(h->d_omega_d, p->omega_d, 3 * (size_t)n * sizeof(double));
+    up(h->d_f, p->f, 3 * (size_t)n * sizeof(double));
+    up(h->d_m, p->m, (size_t)n * sizeof(double));
+    up(h->d_j, p->j, 3 * (size_t)n * sizeof(double));
+    up(h->d_radius, p->radius, (size_t)n * sizeof(double));
+    up(h->d_length, p->length, (size_t)n * sizeof(double));
+    // M^-1 (minimization_problem.hpp:11-31): 1/m on the translational slots, 1/J on the
+    // rotational ones (2D: z only)
+    std::vector<double> im64(4 * (size_t)(n - nin) + 4, 0.0);
+    std::vector<float> im32(4 * (size_t)(n - nin) + 4, 0.0f);
+    for (int i = nin; i < n; ++i) {
+        const size_t k = 4 * (size_t)(i - nin);
+        im64[k] = 1. / p->m[i];
+        if (h->P.dim == 3) {
+            for (int d = 0; d < 3; ++d) im64[k + 1 + d] = 1. / p->j[3 * (size_t)i + d];
+        } else {
+            im64[k + 3] = 1. / p->j[3 * (size_t)i + 2];
+        }
+        for (int d = 0; d < 4; ++d) im32[k + d] = (float)im64[k + d];
+    }
+    cudaMemcpyAsync(h->d_invm64, im64.data(), im64.size() * sizeof(double), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(h->d_invm32, im32.data(), im32.size() * sizeof(float), cudaMemcpyHostToDevice, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return h->cuda_fail(e, "set_particles");
+    return 0;
+}
+
+int32_t scopi_gpu_get_particles(scopi_gpu_handle* h, scopi_gpu_particles* o) {
+    if (!h || !o) return SCOPI_GPU_EINVAL;
+    cudaSetDevice(h->dev);
+    cudaStream_t s = h->stream;
+    const size_t n = (size_t)h->n;
+    if (o->pos) cudaMemcpyAsync(o->pos, h->d_pos, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (o->q) cudaMemcpyAsync(o->q, h->d_q, 4 * n * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (o->v) cudaMemcpyAsync(o->v, h->d_v, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (o->omega) cudaMemcpyAsync(o->omega, h->d_omega, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return h->cuda_fail(e, "get_particles");
+    return 0;
+}
+
+int32_t scopi_gpu_run(scopi_gpu_handle* h, double dt, int64_t total_it, int64_t initial_iter) {
+    if (!h) return SCOPI_GPU_EINVAL;
+    if (h->n == 0) return h->fail(SCOPI_GPU_EINVAL, "no particles");
+    cudaSetDevice(h->dev);
+    int status = 0;
+    for (int64_t it = initial_iter; it < total_it; ++it) {
+        int rc = h->step(dt);
+        if (rc < 0) return rc;
+        if (h->stats.status == SCOPI_GPU_ENOCONV) status = SCOPI_GPU_ENOCONV;
+    }
+    return status;
+}
+
+int32_t scopi_gpu_detect(scopi_gpu_handle* h, int64_t* nout) {
+    if (!h) return SCOPI_GPU_EINVAL;
+    if (h->n == 0) return h->fail(SCOPI_GPU_EINVAL, "no particles");
+    cudaSetDevice(h->dev);
+    int rc = h->detect_and_assemble(0.0, false);
+    if (rc) return rc;
+    cudaMemcpyAsync(h->h_sizes, h->d_sizes_cur, sizeof(Sizes), cudaMemcpyDeviceToHost, h->stream);
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return h->cuda_fail(e, "detect");
+    std::swap(h->cur, h->old);
+    std::swap(h->d_sizes_cur, h->d_sizes_old);
+    h->has_old = true;
+    if (nout) *nout = h->h_sizes->C;
+    return 0;
+}
+
+int32_t scopi_gpu_get_contacts(scopi_gpu_handle* h, int64_t cap, int64_t* nout, int64_t* ci, int64_t* cj, double* dij,
+                               double* nij, double* pi, double* pj, double* gamma) {
+    if (!h) return SCOPI_GPU_EINVAL;
+    cudaSetDevice(h->dev);
+    Sizes sz{};
+    if (h->has_old) cudaMemcpy(&sz, h->d_sizes_old, sizeof(Sizes), cudaMemcpyDeviceToHost);
+    const long long C = sz.C;
+    if (nout) *nout = C;
+    const long long k = std::min<long long>(C, cap);
+    if (k <= 0) return 0;
+    std::vector<int> tmp(k);
+    if (ci) {
+        cudaMemcpy(tmp.data(), h->old.ci, k * sizeof(int), cudaMemcpyDeviceToHost);
+        for (long long x = 0; x < k; ++x) ci[x] = tmp[x];
+    }
+    if (cj) {
+        cudaMemcpy(tmp.data(), h->old.cj, k * sizeof(int), cudaMemcpyDeviceToHost);
+        for (long long x = 0; x < k; ++x) cj[x] = tmp[x];
+    }
+    if (dij) cudaMemcpy(dij, h->old.dij, k * sizeof(double), cudaMemcpyDeviceToHost);
+    if (nij) cudaMemcpy(nij, h->old.nij, 3 * k * sizeof(double), cudaMemcpyDeviceToHost);
+    if (pi) cudaMemcpy(pi, h->old.pi, 3 * k * sizeof(double), cudaMemcpyDeviceToHost);
+    if (pj) cudaMemcpy(pj, h->old.pj, 3 * k * sizeof(double), cudaMemcpyDeviceToHost);
+    if (gamma) cudaMemcpy(gamma, h->old.gamma, k * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return h->cuda_fail(e, "get_contacts");
+    return 0;
+}
+
+int32_t scopi_gpu_get_lambda(scopi_gpu_handle* h, int64_t cap, int64_t* nout, double* lambda) {
+    if (!h) return SCOPI_GPU_EINVAL;
+    cudaSetDevice(h->dev);
+    const long long M = h->last_lambda ? h->last_M : 0;
+    if (nout) *nout = M;
+    const long long k = std::min<long long>(M, cap);
+    if (k > 0 && lambda) {
+        cudaError_t e = cudaMemcpy(lambda, h->last_lambda, k * sizeof(double), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return h->cuda_fail(e, "get_lambda");
+    }
+    return 0;
+}
+
+int32_t scopi_gpu_get_stats(scopi_gpu_handle* h, scopi_gpu_stats* out) {
+    if (!h || !out) return SCOPI_GPU_EINVAL;
+    *out = h->stats;
+    return 0;
+}
+
+int32_t scopi_gpu_amat(scopi_gpu_handle* h, const double* u, double* out) {
+    if (!h || !u || !out) return SCOPI_GPU_EINVAL;
+    cudaSetDevice(h->dev);
+    Sizes sz{};
+    cudaMemcpy(&sz, h->d_sizes_old, sizeof(Sizes), cudaMemcpyDeviceToHost);
+    double *du = nullptr, *dout = nullptr;
+    cudaMalloc(&du, 6 * (size_t)std::max(h->na, 1) * sizeof(double));
+    cudaMalloc(&dout, 3 * (size_t)std::max(sz.C, 1) * sizeof(double));
+    cudaMemcpy(du, u, 6 * (size_t)h->na * sizeof(double), cudaMemcpyHostToDevice);
+    launch_amat(h->bodies(), h->step_params(0.0), h->old, h->d_sizes_old, h->c_cap, du, dout, h->stream);
+    cudaStreamSynchronize(h->stream);
+    cudaMemcpy(out, dout, 3 * (size_t)sz.C * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(du);
+    cudaFree(dout);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return h->cuda_fail(e, "amat");
+    return 0;
+}
+
+int32_t scopi_gpu_atmat(scopi_gpu_handle* h, const double* f, double* out) {
+    if (!h || !f || !out) return SCOPI_GPU_EINVAL;
+    cudaSetDevice(h->dev);
+    Sizes sz{};
+    cudaMemcpy(&sz, h->d_sizes_old, sizeof(Sizes), cudaMemcpyDeviceToHost);
+    double *df = nullptr, *dout = nullptr;
+    cudaMalloc(&df, 3 * (size_t)std::max(sz.C, 1) * sizeof(double));
+    cudaMalloc(&dout, 6 * (size_t)std::max(h->na, 1) * sizeof(double));
+    cudaMemcpy(df, f, 3 * (size_t)sz.C * sizeof(double), cudaMemcpyHostToDevice);
+    launch_atmat(h->bodies(), h->step_params(0.0), h->old, h->d_sizes_old, h->c_cap, df, dout, h->stream);
+    cudaStreamSynchronize(h->stream);
+    cudaMemcpy(out, dout, 6 * (size_t)h->na * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(df);
+    cudaFree(dout);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return h->cuda_fail(e, "atmat");
+    return 0;
+}
+
+const char* scopi_gpu_last_error(scopi_gpu_handle* h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+int64_t scopi_gpu_kernel_launches(scopi_gpu_handle* h) { return h ? h->launches() - h->launches0 : 0; }
+
+void* scopi_gpu_get_stream(scopi_gpu_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+}  // extern "C"

@@ -1,0 +1,73 @@
+"""C ABI checks that need no GPU: the library builds for sm_100a, loads, and exports
+every function include/scopi_gpu.h declares; the Python mirror exposes the reference
+parameter names."""
+import os
+import re
+import shutil
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    txt = open(os.path.join(ROOT, "include", "scopi_gpu.h")).read()
+    return sorted(set(re.findall(r"\b(scopi_gpu_\w+)\s*\(", txt)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from scopi_b200 import _abi
+    if not os.path.exists(_abi.LIB_PATH):
+        if shutil.which("nvcc") is None and not os.path.exists("/usr/local/cuda/bin/nvcc"):
+            pytest.skip("nvcc unavailable")
+        from scopi_b200 import build
+        build.build()
+    return _abi.load()
+
+
+def test_exports_every_declared_symbol(lib):
+    syms = declared_symbols()
+    assert len(syms) >= 14
+    for s in syms:
+        assert hasattr(lib, s), f"{s} declared in include/scopi_gpu.h but not exported"
+
+
+def test_python_binding_covers_header():
+    from scopi_b200 import _abi
+    assert set(declared_symbols()) == set(_abi.EXPORTED)
+
+
+def test_default_params_match_reference(lib):
+    import ctypes as C
+    from scopi_b200 import _abi
+    p = _abi.Params()
+    lib.scopi_gpu_default_params(C.byref(p), 3)
+    # apgd.hpp:120-123, contact_kdtree.hpp:229-237, property.hpp:72,125-127
+    assert (p.alpha, p.max_ite, p.tolerance, p.dynamic_descent) == (0.05, 10000, 1e-7, 1)
+    assert (p.dmax, p.kd_tree_radius) == (2.0, 17.0)
+    assert (p.mu, p.gamma, p.gamma_min, p.gamma_tol) == (0.1, 0.0, -2.0, 1e-6)
+
+
+def test_create_without_gpu_fails_cleanly(lib):
+    import ctypes as C
+    import torch
+    from scopi_b200 import _abi
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    p = _abi.Params()
+    lib.scopi_gpu_default_params(C.byref(p), 2)
+    h = C.c_void_p()
+    rc = lib.scopi_gpu_create(C.byref(p), C.byref(h))
+    assert rc == _abi.ECUDA and not h.value
+    assert b"CUDA" in lib.scopi_gpu_last_error(None)
+
+
+def test_solver_raises_without_library(tmp_path):
+    from scopi_b200 import _abi
+    with pytest.raises(OSError):
+        _abi._lib, saved = None, _abi._lib
+        try:
+            _abi.load(str(tmp_path / "missing.so"))
+        finally:
+            _abi._lib = saved

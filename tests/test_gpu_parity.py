@@ -1,0 +1,224 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle and the reference goldens.
+
+Bar: contact lists identical and their geometry bit for bit on identical inputs;
+trajectories within the reference's golden tolerances; FP64 multipliers and positions
+within 1e-9 relative of the oracle while both follow the same APGD iterate sequence.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import scenes as S
+from gpu_helpers import gpu_solver, oracle_solver, rel_err, same_contacts, segment_pile
+from scopi_b200 import configs
+from test_oracle_golden import APPROX, approx, compare_objects
+
+pytestmark = pytest.mark.gpu
+
+
+def detect_both(pa, **kw):
+    g = gpu_solver(pa, **kw).detect()
+    o = oracle_solver(pa, **kw).detect()
+    return g, o
+
+
+DETECT_SCENES = {
+    "three_disks": lambda: (S.contacts_three_disks()[0], dict(kd_tree_radius=100.0)),
+    "critical_2d": lambda: (S.critical_2d_spheres()[0], {}),
+    "disks_2d_1024": lambda: (configs.disks_2d(), dict(dmax=0.01)),
+    "box_3d_4000": lambda: (configs.box_3d(count=4000), dict(dmax=0.0045)),
+    "spheres_16cube": lambda: (configs.spheres_1m(side=16), dict(dmax=0.0018)),
+    "inclined_plane": lambda: (S.sphere_inclined_plane(math.pi / 6)[0], {}),
+    "segment_pile": lambda: (segment_pile(), dict(dmax=0.009)),
+    "kd_radius_filter": lambda: (configs.disks_2d(side=12), dict(dmax=0.05, kd_tree_radius=0.03 ** 2)),
+}
+
+
+@pytest.mark.parametrize("name", sorted(DETECT_SCENES))
+@pytest.mark.parametrize("method", [S.KDTREE, S.BRUTE_FORCE])
+def test_contacts_bitexact(name, method):
+    pa, kw = DETECT_SCENES[name]()
+    g, o = detect_both(pa, contact_method=method, **kw)
+    assert len(o["i"]) > 0
+    same_contacts(g, o)
+
+
+def test_contacts_three_disks_known_answer():
+    """test/test_contacts_kdtree.cpp:14-73 on the GPU."""
+    pa, kw, _, _ = S.contacts_three_disks()
+    c = gpu_solver(pa, **kw).detect()
+    assert list(c["i"]) == [0] and list(c["j"]) == [1]
+    assert approx(c["dij"][0], math.sqrt(2.0) - 0.3)
+    assert approx(c["nij"][0, 0], -1 / math.sqrt(2.0))
+
+
+def test_matrix_known_values_and_adjoint():
+    """test/test_matrices.cpp:17-77 on the GPU: A.u values and dot(Au, f) = dot(u, A^T f)."""
+    pa, kw, _, _ = S.matrix_a_case2()
+    s = gpu_solver(pa, **kw)
+    s.detect()
+    u = np.array([0.187562190766376, -1.184390935327111, 0., 0., 0., -0.00453709103433])
+    sol = s.amat(u)
+    assert approx(sol[0], -0.18595809) and approx(sol[1], 1.18278683)
+    pa, kw, _, _ = S.matrix_a_3d()
+    s = gpu_solver(pa, **kw)
+    o = oracle_solver(pa, **kw)
+    s.detect()
+    o.detect()
+    rng = np.random.default_rng(0)
+    u = rng.random(12)
+    f = rng.random(3)
+    assert approx(float(np.dot(s.amat(u), f)), float(np.dot(u, s.atmat(f))))
+    assert np.allclose(s.amat(u), o.amat(u), rtol=1e-14, atol=0)
+    assert np.allclose(s.atmat(f), o.atmat(f), rtol=1e-14, atol=1e-300)
+
+
+GOLDEN_CASES = [
+    ("3spheres_nofriction", lambda: S.three_spheres(S.NOFRICTION), 1e-5),
+    ("3spheres_viscous", lambda: S.three_spheres(S.VISCOUS), 1e-5),
+    ("sphere_plane_friction_mu01", S.sphere_plane_friction_mu01, 1e-5),
+    ("two_spheres_asymmetrical", lambda: S.two_spheres(False), 1e-6),
+    ("two_spheres_symmetrical", lambda: S.two_spheres(True), 1e-6),
+    ("2d_case_spheres", S.critical_2d_spheres, 1e-6),
+    ("obstacles_sphere_sphere_moving", lambda: S.obstacle_sphere_sphere("moving"), 1e-6),
+]
+
+
+@pytest.mark.parametrize("name,builder,tol", GOLDEN_CASES, ids=[c[0] for c in GOLDEN_CASES])
+def test_reference_goldens_on_gpu(golden, name, builder, tol):
+    pa, kw, dt, total = builder()
+    s = gpu_solver(pa, **kw).run(dt, total)
+    compare_objects(s.particles, golden[name]["objects"], 2, tol)
+
+
+def test_critical_2d_contact_list_on_gpu(golden):
+    """The 117-contact list of 2d_case_spheres.json, from the GPU state after 19 steps."""
+    pa, kw, dt, total = S.critical_2d_spheres()
+    s = gpu_solver(pa, **kw).run(dt, total - 1)
+    c = s.detect()
+    gold = golden["2d_case_spheres"]["contacts"]
+    assert list(zip(c["i"].tolist(), c["j"].tolist())) == [(g["i"], g["j"]) for g in gold]
+    for k, g in enumerate(gold):
+        assert abs(c["dij"][k] - g["distance"]) < 1e-6
+
+
+@pytest.mark.parametrize("alpha,e_pos,e_v", [(math.pi / 6, 0.000998789, 0.0010002),
+                                             (math.pi / 4, 0.00100008, 0.00100119),
+                                             (math.pi / 3, 0.00100105, 0.0010027)])
+def test_inclined_plane_pinned_errors_on_gpu(alpha, e_pos, e_v):
+    """test/test_obstacles.cpp:252-311 pinned errors, on the GPU."""
+    pa, kw, dt, total = S.sphere_inclined_plane(alpha)
+    s = gpu_solver(pa, **kw).run(dt, total)
+    x, theta, v = S.analytic_inclined(alpha, 0.0, dt * (total + 1), 1.0, 1.0, 2.0)
+    err_pos = np.linalg.norm(s.particles.pos[1, :2] - x) / np.linalg.norm(x)
+    err_v = np.linalg.norm(s.particles.v[1, :2] - v) / np.linalg.norm(v)
+    assert approx(err_pos, e_pos)
+    assert abs(err_v - e_v) <= 1e-4 * (1 + e_v)
+
+
+def test_viscous_analytic_on_gpu():
+    """test/test_gradient.cpp:82-154 on the GPU (gamma carried across two run() calls)."""
+    pa, kw, dt, total = S.sphere_plane_analytic(S.VISCOUS)
+    s = gpu_solver(pa, **kw)
+    s.run(dt, total)
+    g, alpha = 1.0, math.pi / 4
+    p2 = s.particles.copy()
+    p2.f[1, :2] = (-g * math.sin(alpha), g * math.cos(alpha))
+    s.set_particles(p2)
+    s.run(dt, 500)
+    x, v = S.analytic_viscous(alpha, dt * (total + 500), 1.0, g, 2.0, -2.0, dt * total)
+    assert np.linalg.norm(s.particles.pos[1, :2] - x) / np.linalg.norm(x) <= 1e-3
+    assert np.linalg.norm(s.particles.v[1, :2] - v) / np.linalg.norm(v) <= 1e-3
+
+
+def _trajectory(pa, kw, dt, steps):
+    """Step both engines from the same state and compare after every step.
+
+    The backtracking test of apgd.hpp:174-175 compares two objective values that agree
+    to rounding once the iterates have converged, so which branch it takes there is
+    decided by rounding (the reference's own result depends on its BLAS).  Steps whose
+    branch trace (iterations, backtracks, restarts) is identical must agree to 1e-9 in
+    lambda; the others to the solver tolerance: |dlambda| <= 50 tol and 1e-6 relative.
+    """
+    g = gpu_solver(pa, **kw)
+    o = oracle_solver(pa, **kw)
+    tol = kw.get("tolerance", 1e-7)
+    worst = {"lambda_same_trace": 0.0, "lambda_abs": 0.0, "lambda_rel": 0.0, "pos": 0.0, "v": 0.0, "same_trace": 0}
+    for k in range(steps):
+        g.run(dt, 1)
+        o.run(dt, 1)
+        gc, oc = g.current_contacts(), o.contacts()
+        assert np.array_equal(gc["i"], oc["i"]) and np.array_equal(gc["j"], oc["j"]), f"contact pairs differ at step {k}"
+        lg, lo = g.lagrange_multiplier(), o.lagrange_multiplier()
+        assert len(lg) == len(lo)
+        gs, os_ = g.stats(), o.stats()
+        same = all(gs[x] == os_[x] for x in ("iterations", "backtracks", "restarts"))
+        if len(lo):
+            r = rel_err(lg, lo)
+            if same:
+                worst["same_trace"] += 1
+                worst["lambda_same_trace"] = max(worst["lambda_same_trace"], r)
+            worst["lambda_rel"] = max(worst["lambda_rel"], r)
+            worst["lambda_abs"] = max(worst["lambda_abs"], float(np.linalg.norm(lg - lo)))
+        worst["pos"] = max(worst["pos"], rel_err(g.particles.pos, o.pa.pos))
+        worst["v"] = max(worst["v"], rel_err(g.particles.v, o.pa.v))
+        assert abs(gs["iterations"] - os_["iterations"]) <= max(10, os_["iterations"] // 20)
+    assert worst["lambda_same_trace"] <= 1e-9, worst
+    assert worst["lambda_abs"] <= 50 * tol and worst["lambda_rel"] <= 1e-6, worst
+    return worst
+
+
+@pytest.mark.parametrize("name", ["disks_2d", "box_3d", "spheres", "spheres_viscous"])
+def test_fp64_trajectory_matches_oracle(name):
+    if name == "disks_2d":
+        pa, st, steps = configs.disks_2d(), configs.SETTINGS["disks_2d"], 10
+        kw = dict(dmax=st["dmax"], tolerance=st["tolerance"], max_ite=st["max_ite"], vap=st["vap"])
+    elif name == "box_3d":
+        pa, st, steps = configs.box_3d(count=2000), configs.SETTINGS["box_3d"], 5
+        kw = dict(dmax=st["dmax"], tolerance=st["tolerance"], max_ite=st["max_ite"], vap=st["vap"])
+    else:
+        pa, st, steps = configs.spheres_1m(side=12), configs.SETTINGS["spheres_1m"], 5
+        kw = dict(dmax=st["dmax"], tolerance=st["tolerance"], max_ite=st["max_ite"], vap=st["vap"])
+        if name == "spheres_viscous":
+            kw["problem"] = S.VISCOUS
+    worst = _trajectory(pa, kw, st["dt"], steps)
+    assert worst["pos"] <= 1e-9 and worst["v"] <= 1e-7, worst
+
+
+def test_mixed_precision_reaches_violation_target():
+    pa = configs.spheres_1m(side=16)
+    st = configs.SETTINGS["spheres_1m"]
+    kw = dict(dmax=st["dmax"], tolerance=st["tolerance"], max_ite=st["max_ite"], vap=st["vap"])
+    f64 = gpu_solver(pa, **kw).run(st["dt"], 3)
+    mix = gpu_solver(pa, precision=1, mixed_violation_tol=1e-6, **kw).run(st["dt"], 3)
+    sm = mix.stats()
+    assert sm["violation"] <= 1e-6, sm
+    assert sm["fp32_iterations"] > 0
+    lam_err = rel_err(mix.lagrange_multiplier(), f64.lagrange_multiplier())
+    assert lam_err <= 1e-2, lam_err
+    assert rel_err(mix.particles.pos, f64.particles.pos) <= 1e-7
+
+
+def test_deterministic_bitwise():
+    pa = configs.spheres_1m(side=12)
+    st = configs.SETTINGS["spheres_1m"]
+    kw = dict(dmax=st["dmax"], tolerance=st["tolerance"], max_ite=st["max_ite"], vap=st["vap"])
+    a = gpu_solver(pa, **kw).run(st["dt"], 3)
+    b = gpu_solver(pa, **kw).run(st["dt"], 3)
+    assert np.array_equal(a.particles.pos, b.particles.pos)
+    assert np.array_equal(a.lagrange_multiplier(), b.lagrange_multiplier())
+
+
+def test_kernel_launch_count_reported():
+    pa = configs.disks_2d(side=8)
+    s = gpu_solver(pa, dmax=0.01).run(0.005, 2)
+    assert s.kernel_launches() > 0
+
+
+def test_apgd_max_ite_reports_nonconvergence():
+    pa = configs.disks_2d(side=8)
+    s = gpu_solver(pa, dmax=0.01, max_ite=1, tolerance=1e-30)
+    s.run(0.005, 1)
+    st = s.stats()
+    assert st["iterations"] == 1 and st["converged"] == 0 and st["status"] == 1
