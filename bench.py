@@ -41,12 +41,18 @@ def env_int(k, d):
         return d
 
 
-def roofline_bytes_per_iter(C, N, s, dim=3):
+def roofline_bytes_per_iter(C, N, s, dim=3, torque_free=True):
     """Algorithmic bytes of one APGD iteration (accepted step, no backtracks).
 
-    3D: 3 passes over compressed B (9 values + 2 int32 indices per contact), 6 contact
-    vector streams, 4 particle vector streams of 6N entries.  2D: 4 values, 3N slots.
+    Rows of B: 3 passes over B (values + 2 int32 indices per contact), 6 contact vector
+    streams, 4 particle vector streams.  Full rows carry 9 values per contact in 3D
+    (n, R_i^T(r_i x n), R_j^T(r_j x n)) and 6N particle slots; for normal-only problems
+    on sphere/plane/segment contacts the rotational values are identically zero, so a
+    row is the normal alone (3 values in 3D, 2 in 2D) and the particle vectors have N*dim
+    translational slots.
     """
+    if torque_free:
+        return 3 * C * (dim * s + 8) + 6 * C * s + 4 * (dim * N) * s
     if dim == 3:
         return 3 * C * (9 * s + 8) + 6 * C * s + 4 * (6 * N) * s
     return 3 * C * (4 * s + 8) + 6 * C * s + 4 * (3 * N) * s
@@ -359,6 +365,7 @@ def ours(args, ranks):
     it32 = sum(p["fp32_iterations"] for p in per)
     ms_apgd = sum(p["ms_apgd_kernel"] for p in per)
     b_iter32 = roofline_bytes_per_iter(C, n_active, 4)
+    b_iter32_full = roofline_bytes_per_iter(C, n_active, 4, torque_free=False)
     achieved = (it32 * b_iter32) / (ms_apgd * 1e-3) / 1e9 if ms_apgd > 0 else None
     peak, peak_kind = measured_peaks()
     traffic = None
@@ -402,8 +409,12 @@ def ours(args, ranks):
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                     "peak_source": f"{peak_kind} hbm_gbs", "kernel": "k_apgd<float,3,NoFriction> (persistent)",
-                     "bytes_per_iteration": b_iter32, "iterations_per_step": it32 / len(per),
+                     "peak_source": f"{peak_kind} hbm_gbs",
+                     "kernel": "k_apgd_sph<float,3,NoFriction> (persistent, torque-free rows)",
+                     "bytes_per_iteration": b_iter32,
+                     "achieved_full_row_formula": ((it32 * b_iter32_full) / (ms_apgd * 1e-3) / 1e9
+                                                   if ms_apgd > 0 else None),
+                     "iterations_per_step": it32 / len(per),
                      "ms_apgd_per_step": ms_apgd / len(per)},
         "cpu_baseline": cpu,
         "clocks": mixed["clocks"],

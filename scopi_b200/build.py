@@ -19,6 +19,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
 SOURCES = {
     "detect.cu": ["-fmad=false"],
     "apgd.cu": [],
+    "apgd_sph.cu": [],
     "scan.cu": [],
     "scopi_gpu.cu": [],
 }
@@ -35,7 +36,8 @@ def needs_build() -> bool:
     if not os.path.exists(OUT):
         return True
     t = os.path.getmtime(OUT)
-    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(HERE, "..", "include", "scopi_gpu.h")]
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(HERE, "..", "include", "scopi_gpu.h"),
+                                                                 os.path.abspath(__file__)]
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 

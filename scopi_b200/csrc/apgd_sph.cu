@@ -1,0 +1,544 @@
+// apgd_sph.cu -- persistent APGD for the normal-only problems (NoFriction, Viscous) on
+// contacts whose lever arms are parallel to the normal (sphere-sphere, sphere-plane,
+// sphere-segment: p_i - x_i = -/+ r_i n), where the rotational terms of the contact
+// Jacobian, R^T (r x n), vanish identically.  A contact's row of B is then n^T on the
+// two bodies' translational velocities:
+//     (B u)_c = n_c . (u_i - u_j),     (B^T l)_p = sum_{c ~ p} +-l_c n_c.
+// Same iteration, branch logic and stopping rule as the generic kernel (apgd.cu), i.e.
+// apgd::operator() of include/scopi/solvers/apgd.hpp:148-221, with the data cut to
+// what this row shape needs:
+//   per contact : (ci, cj) int2 + (n, c) packed in one 16/32-byte record, l, l_prev;
+//   per incidence of a body: (+-n, contact index) in one record;
+//   per body    : u(y) gathered once (u(y_next) = u(l+) + beta (u(l+) - u(l)) is formed in
+//                 the particle pass, the restart test being reduced after the first barrier).
+#include "apgd_common.cuh"
+
+namespace scopi_gpu {
+
+static long long g_sph_launches = 0;
+long long apgd_sph_launches() { return g_sph_launches; }
+
+namespace {
+using namespace apgdc;
+
+__device__ __forceinline__ float4 ld4(const float4* p) { return *p; }
+__device__ __forceinline__ dvec4 ld4(const dvec4* p) {
+    const double2* q = reinterpret_cast<const double2*>(p);
+    const double2 a = q[0], b = q[1];
+    return dvec4{a.x, a.y, b.x, b.y};
+}
+__device__ __forceinline__ float4 ld4cg(const float4* p) { return __ldcg(p); }
+__device__ __forceinline__ dvec4 ld4cg(const dvec4* p) {
+    const double2* q = reinterpret_cast<const double2*>(p);
+    const double2 a = __ldcg(q), b = __ldcg(q + 1);
+    return dvec4{a.x, a.y, b.x, b.y};
+}
+__device__ __forceinline__ void st4(float4* p, float x, float y, float z) { *p = make_float4(x, y, z, 0.f); }
+__device__ __forceinline__ void st4(dvec4* p, double x, double y, double z) {
+    double2* q = reinterpret_cast<double2*>(p);
+    q[0] = make_double2(x, y);
+    q[1] = make_double2(z, 0.0);
+}
+__device__ __forceinline__ int idx_of(float w) { return __float_as_int(w); }
+__device__ __forceinline__ int idx_of(double w) { return (int)__double_as_longlong(w); }
+
+template <typename T>
+struct SphArgs {
+    int nin, na;
+    const int2* cij;
+    const V4<T>* nc;
+    const int* slot;
+    const double* shift;
+    const int* inc_ptr;
+    const V4<T>* inc;
+    const double* invm;  // stride 4, component 0 = 1/m
+    T* lam0;
+    T* lam1;
+    T* lam2;
+    V4<T>* u0;
+    V4<T>* u1;
+    V4<T>* u2;
+    V4<T>* u3;
+    double* partials;
+    unsigned int* bar;
+    ApgdResult* result;
+    const Sizes* sizes;
+    double alpha, tol, dt2;
+    long long max_ite;
+    int dynamic;
+};
+
+template <typename T>
+__device__ __forceinline__ T pick(int k, T a, T b, T c) {
+    return k == 0 ? a : (k == 1 ? b : c);
+}
+template <typename T>
+__device__ __forceinline__ T pick4(int k, T a, T b, T c, T d) {
+    return k == 0 ? a : (k == 1 ? b : (k == 2 ? c : d));
+}
+
+// one multiplier of the contact pass
+template <typename T>
+__device__ __forceinline__ void mult_update(const SphArgs<T>& A, long long m, T qy, T cc, const T* lam, const T* lprev,
+                                            T* lnew, T beta, bool use_prev, bool bt, double alpha, double* s) {
+    const T lm = lam[m];
+    const T y = use_prev ? lm + beta * (lm - lprev[m]) : lm;
+    const T gm = qy + cc;
+    T lp;
+    if (A.shift) {
+        const double sh = A.shift[m];
+        double z = sh + ((double)y - alpha * (double)gm);
+        z = z > 0.0 ? z : 0.0;
+        lp = (T)(z - sh);
+    } else {
+        const T z = y - (T)alpha * gm;
+        lp = z > (T)0 ? z : (T)0;
+    }
+    lnew[m] = lp;
+    const double dly = (double)lp - (double)y, dll = (double)lp - (double)lm;
+    s[0] += (double)gm * dly;
+    s[1] += dly * dly;
+    s[2] += (double)cc * (double)lp;
+    if (!bt) s[3] += (double)y * (0.5 * (double)qy + (double)cc);
+    s[4] += dll * dll;
+    s[5] += (double)gm * dll;
+    s[6] += (double)lp * (double)lp;
+}
+
+// Loop-carried scalars of the iteration (block-uniform) live in shared memory and are
+// updated by thread 0, so the registers go to the two passes.
+struct SphState {
+    double alpha, lipsch, theta, beta, beta_n, theta1, Fy, last_step;
+    long long ite, nbt, nrs;
+    int il, ip, in_, jL, jN, jY, jYN, parity, bt, use_prev, restart, done, conv, err;
+};
+
+// FP32: 64 registers (4 blocks/SM, no spills); FP64: 80 registers (3 blocks/SM).
+template <typename T>
+struct SphOcc {
+    static constexpr int blocks = sizeof(T) == 4 ? 4 : 3;
+};
+
+template <typename T, int DIM, int PROB>
+__global__ void __launch_bounds__(kThreadsA, SphOcc<T>::blocks) k_apgd_sph(SphArgs<T> A) {
+    __shared__ SphState S;
+    if (threadIdx.x == 0) {
+        S.alpha = A.alpha;
+        S.lipsch = 1.0 / A.alpha;
+        S.theta = 1.0;
+        S.beta = 0.0;
+        S.beta_n = 0.0;
+        S.theta1 = 1.0;
+        S.Fy = 0.0;
+        S.last_step = 0.0;
+        S.ite = S.nbt = S.nrs = 0;
+        S.il = 0; S.ip = 1; S.in_ = 2;           // lambda buffers: current, previous, candidate
+        S.jL = 0; S.jN = 1; S.jY = 2; S.jYN = 3;  // u buffers: u(l), u(candidate), u(y), u(next y)
+        S.parity = 0;
+        S.bt = 0;
+        S.use_prev = 0;
+        S.restart = 0;
+        S.done = 0;
+        S.conv = 0;
+        S.err = 0;
+    }
+    __syncthreads();
+    const int C = A.sizes->C;
+    const unsigned int nb = gridDim.x;
+    for (;;) {
+        const double alpha = S.alpha;
+        const bool bt = S.bt != 0, use_prev = S.use_prev != 0;
+        const T beta = (T)S.beta;
+        const T* lam = pick(S.il, A.lam0, A.lam1, A.lam2);
+        const T* lprev = pick(S.ip, A.lam0, A.lam1, A.lam2);
+        T* lnew = pick(S.in_, A.lam0, A.lam1, A.lam2);
+        const V4<T>* uY = pick4(S.jY, A.u0, A.u1, A.u2, A.u3);
+        double* part = A.partials + (size_t)S.parity * nb * 8;
+        double* part2 = A.partials + (size_t)(2 + S.parity) * nb * 8;
+        {
+            double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            // ---- contact pass: g = dt^2 n.(u_i(y) - u_j(y)) + c, l+ = P(y - alpha g)
+            GRID_STRIDE(c, C) {
+                const int2 ij = A.cij[c];
+                const V4<T> nc = ld4(A.nc + c);
+                const bool ai = ij.x >= A.nin, aj = ij.y >= A.nin;
+                V4<T> ui, uj;
+                if (ai) ui = ld4cg(uY + (ij.x - A.nin));
+                if (aj) uj = ld4cg(uY + (ij.y - A.nin));
+                T qy = 0;
+                if (ai) qy += nc.x * ui.x + nc.y * ui.y + (DIM == 3 ? nc.z * ui.z : (T)0);
+                if (aj) qy -= nc.x * uj.x + nc.y * uj.y + (DIM == 3 ? nc.z * uj.z : (T)0);
+                qy *= (T)A.dt2;
+                mult_update<T>(A, c, qy, nc.w, lam, lprev, lnew, beta, use_prev, bt, alpha, s);
+                if (PROB == kViscous) {
+                    const int sl = A.slot[c];
+                    if (sl >= 0) mult_update<T>(A, sl, -qy, -nc.w, lam, lprev, lnew, beta, use_prev, bt, alpha, s);
+                }
+            }
+            block_sum<8>(s);
+            if (threadIdx.x == 0)
+                for (int k = 0; k < 8; ++k) part[blockIdx.x * 8 + k] = s[k];
+        }
+        if (!grid_barrier(A.bar, nb)) {
+            if (threadIdx.x == 0) S.err = 1;
+            break;
+        }
+        {
+            double t[8];
+            grid_sum<8>(part, nb, 8, t);
+            if (threadIdx.x == 0) {
+                // momentum for the next y if this candidate is accepted (apgd.hpp:196-206)
+                const double th = S.theta;
+                S.theta1 = 0.5 * (th * sqrt(4 + th * th) - th * th);
+                S.restart = (A.dynamic && t[5] > 0) ? 1 : 0;
+                S.beta_n = S.restart ? 0.0 : th * (1 - th) / (th * th + S.theta1);
+                if (!bt) S.Fy = t[3];
+                // keep the scalars the decision needs after the second pass
+                S.last_step = t[4];
+            }
+            // t[0..2] and |l+|^2 for thread 0, which takes the decision after the second pass
+            __shared__ double tk[4];
+            if (threadIdx.x == 0) {
+                tk[0] = t[0];
+                tk[1] = t[1];
+                tk[2] = t[2];
+                tk[3] = t[6];
+            }
+            __syncthreads();
+            // ---- particle pass: w = B^T l+, u = M^-1 w, u(next y)
+            V4<T>* uL = pick4(S.jL, A.u0, A.u1, A.u2, A.u3);
+            V4<T>* uN = pick4(S.jN, A.u0, A.u1, A.u2, A.u3);
+            V4<T>* uYN = pick4(S.jYN, A.u0, A.u1, A.u2, A.u3);
+            const T bn_ = (T)S.beta_n;
+            double sw = 0.0;
+            // one body per thread; its incidence records, then the l+ gathers they index,
+            // are issued in batches so several loads are in flight per thread
+            constexpr int KB = 4;
+            GRID_STRIDE(p, A.na) {
+                T w0 = 0, w1 = 0, w2 = 0;
+                const int k0 = A.inc_ptr[p], k1 = A.inc_ptr[p + 1];
+                for (int kb = k0; kb < k1; kb += KB) {
+                    T ex[KB], ey[KB], ez[KB], mu[KB];
+                    int ci[KB];
+#pragma unroll
+                    for (int q = 0; q < KB; ++q) {
+                        ex[q] = ey[q] = ez[q] = mu[q] = (T)0;
+                        ci[q] = -1;
+                        if (kb + q < k1) {
+                            const V4<T> e = ld4(A.inc + kb + q);
+                            ex[q] = e.x;
+                            ey[q] = e.y;
+                            ez[q] = e.z;
+                            ci[q] = idx_of(e.w);
+                        }
+                    }
+#pragma unroll
+                    for (int q = 0; q < KB; ++q)
+                        if (ci[q] >= 0) {
+                            mu[q] = __ldcg(lnew + ci[q]);
+                            if (PROB == kViscous) {
+                                const int sl = A.slot[ci[q]];
+                                if (sl >= 0) mu[q] -= __ldcg(lnew + sl);
+                            }
+                        }
+#pragma unroll
+                    for (int q = 0; q < KB; ++q) {
+                        w0 += mu[q] * ex[q];
+                        w1 += mu[q] * ey[q];
+                        if (DIM == 3) w2 += mu[q] * ez[q];
+                    }
+                }
+                const T im = (T)A.invm[4 * (long long)p];
+                const T n0 = im * w0, n1 = im * w1, n2 = im * w2;
+                st4(uN + p, n0, n1, n2);
+                sw += (double)w0 * (double)n0 + (double)w1 * (double)n1 + (double)w2 * (double)n2;
+                if (bn_ != (T)0) {
+                    const V4<T> ul = ld4(uL + p);
+                    st4(uYN + p, n0 + bn_ * (n0 - ul.x), n1 + bn_ * (n1 - ul.y), n2 + bn_ * (n2 - ul.z));
+                } else {
+                    st4(uYN + p, n0, n1, n2);
+                }
+            }
+            double sw8[1] = {sw};
+            block_sum<1>(sw8);
+            if (threadIdx.x == 0) part2[blockIdx.x * 8] = sw8[0];
+            if (!grid_barrier(A.bar, nb)) {
+                if (threadIdx.x == 0) S.err = 1;
+                break;
+            }
+            double t6[1];
+            grid_sum<1>(part2, nb, 8, t6);
+            if (threadIdx.x == 0) {
+                S.parity ^= 1;
+                const double F_lp = 0.5 * A.dt2 * t6[0] + tk[2];
+                bool accept = true;
+                if (A.dynamic && tk[1] == 0.0) {
+                    double lip = S.lipsch, al = S.alpha;
+                    long long nbt = S.nbt;
+                    overflow_cascade(lip, al, nbt);
+                    S.lipsch = lip;
+                    S.alpha = al;
+                    S.nbt = nbt;
+                } else if (A.dynamic && F_lp >= S.Fy + tk[0] + 0.5 * S.lipsch * tk[1]) {
+                    S.lipsch *= 2;  // backtracking, apgd.hpp:172-182
+                    S.alpha = 1. / S.lipsch;
+                    S.bt = 1;
+                    ++S.nbt;
+                    accept = false;
+                }
+                if (accept) {
+                    ++S.ite;
+                    S.bt = 0;
+                    S.last_step = sqrt(S.last_step);
+                    double tol = A.tol;
+                    if (sizeof(T) == 4) {
+                        // FP32 iterations stall at their rounding floor; the FP64 correction recovers the rest
+                        const double floor32 = 4.0 * 1.1920929e-7 * sqrt(tk[3]);
+                        if (floor32 > tol) tol = floor32;
+                    }
+                    int tmp = S.ip; S.ip = S.il; S.il = S.in_; S.in_ = tmp;
+                    tmp = S.jL; S.jL = S.jN; S.jN = tmp;
+                    tmp = S.jY; S.jY = S.jYN; S.jYN = tmp;
+                    if (S.last_step < tol) {
+                        S.conv = 1;
+                        S.done = 1;
+                    } else {
+                        S.beta = S.beta_n;
+                        S.theta = S.restart ? 1.0 : S.theta1;
+                        if (S.restart) ++S.nrs;
+                        if (A.dynamic) {
+                            S.lipsch *= 0.97;
+                            S.alpha = 1. / S.lipsch;
+                        }
+                        S.use_prev = (S.beta != 0.0) ? 1 : 0;
+                        if (S.ite >= A.max_ite) S.done = 1;
+                    }
+                }
+            }
+            __syncthreads();
+            if (S.done) break;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        A.result->iterations = S.ite;
+        A.result->backtracks = S.nbt;
+        A.result->restarts = S.nrs;
+        A.result->converged = S.conv;
+        A.result->lam_buf = S.il;
+        A.result->u_buf = S.jL;
+        A.result->error = S.err;
+        A.result->last_step = S.last_step;
+    }
+}
+
+// ------------------------------------------------------------------ packing
+__global__ void k_pack_cij(const int* ci, const int* cj, int2* cij, const Sizes* sizes) {
+    GRID_STRIDE(c, sizes->C) { cij[c] = make_int2(ci[c], cj[c]); }
+}
+template <typename T>
+__global__ void k_pack_nc(const double* bn, const double* cv, V4<T>* nc, const Sizes* sizes) {
+    GRID_STRIDE(c, sizes->C) {
+        V4<T> r;
+        r.x = (T)bn[3 * c];
+        r.y = (T)bn[3 * c + 1];
+        r.z = (T)bn[3 * c + 2];
+        r.w = (T)cv[c];
+        nc[c] = r;
+    }
+}
+template <typename T>
+__device__ __forceinline__ T idx_bits(int c);
+template <>
+__device__ __forceinline__ float idx_bits<float>(int c) { return __int_as_float(c); }
+template <>
+__device__ __forceinline__ double idx_bits<double>(int c) { return __longlong_as_double((long long)c); }
+
+template <typename T>
+__global__ void k_pack_inc(int na, const int* ptr, const int* idx, const double* bn, V4<T>* inc) {
+    const int tot = ptr[na];
+    GRID_STRIDE(k, tot) {
+        const unsigned e = (unsigned)idx[k];
+        const int c = (int)(e & 0x7fffffffu);
+        const double sg = (e >> 31) ? -1.0 : 1.0;
+        V4<T> r;
+        r.x = (T)(sg * bn[3 * (long long)c]);
+        r.y = (T)(sg * bn[3 * (long long)c + 1]);
+        r.z = (T)(sg * bn[3 * (long long)c + 2]);
+        r.w = idx_bits<T>(c);
+        inc[k] = r;
+    }
+}
+
+// ------------------------------------------------------------------ FP64 helpers (mixed form)
+template <int DIM, int PROB>
+__global__ void k_sph_particle64(int na, const int* ptr, const dvec4* inc, const int* slot, const double* invm,
+                                 const double* lam, dvec4* u) {
+    GRID_STRIDE(p, na) {
+        double w0 = 0, w1 = 0, w2 = 0;
+        for (int k = ptr[p]; k < ptr[p + 1]; ++k) {
+            const dvec4 e = ld4(inc + k);
+            const int c = idx_of(e.w);
+            double mu = lam[c];
+            if (PROB == kViscous && slot[c] >= 0) mu -= lam[slot[c]];
+            w0 += mu * e.x;
+            w1 += mu * e.y;
+            if (DIM == 3) w2 += mu * e.z;
+        }
+        const double im = invm[4 * (long long)p];
+        st4(u + p, im * w0, im * w1, im * w2);
+    }
+}
+
+template <int DIM, int PROB>
+__global__ void k_sph_residual64(int nin, const int2* cij, const dvec4* nc, const int* slot, double dt2, const dvec4* u,
+                                 double* g, unsigned long long* viol_bits, const Sizes* sizes) {
+    double vmax = 0.0;
+    GRID_STRIDE(c, sizes->C) {
+        const int2 ij = cij[c];
+        const dvec4 n = ld4(nc + c);
+        double q = 0.0;
+        if (ij.x >= nin) {
+            const dvec4 a = ld4(u + (ij.x - nin));
+            q += n.x * a.x + n.y * a.y + (DIM == 3 ? n.z * a.z : 0.0);
+        }
+        if (ij.y >= nin) {
+            const dvec4 b = ld4(u + (ij.y - nin));
+            q -= n.x * b.x + n.y * b.y + (DIM == 3 ? n.z * b.z : 0.0);
+        }
+        const double gg = dt2 * q + n.w;
+        g[c] = gg;
+        if (PROB == kViscous && slot[c] >= 0) g[slot[c]] = -gg;
+        vmax = fmax(vmax, -gg);
+    }
+    if (vmax > 0.0) atomicMax(viol_bits, (unsigned long long)__double_as_longlong(vmax));
+}
+
+int blocks(long long n) {
+    long long b = (n + 255) / 256;
+    if (b < 1) b = 1;
+    return (int)(b < 16 * kSMs ? b : 16 * kSMs);
+}
+
+template <typename T, int DIM, int PROB>
+int max_blocks_sph() {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_apgd_sph<T, DIM, PROB>, kThreadsA, 0);
+    int dev = 0, sms = kSMs;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return per_sm * sms;
+}
+
+template <typename T, int DIM, int PROB>
+cudaError_t launch_t(SphArgs<T>& A, int nblocks, cudaStream_t s) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(nblocks);
+    cfg.blockDim = dim3(kThreadsA);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    g_sph_launches += 1;
+    return cudaLaunchKernelEx(&cfg, k_apgd_sph<T, DIM, PROB>, A);
+}
+
+}  // namespace
+
+int apgd_sph_max_blocks(int problem, int dim, bool fp32) {
+#define MB(T, D, P) \
+    if (dim == D && problem == P) return max_blocks_sph<T, D, P>();
+    if (fp32) {
+        MB(float, 2, 0) MB(float, 2, 2) MB(float, 3, 0) MB(float, 3, 2)
+    } else {
+        MB(double, 2, 0) MB(double, 2, 2) MB(double, 3, 0) MB(double, 3, 2)
+    }
+#undef MB
+    return 0;
+}
+
+template <typename T>
+cudaError_t launch_apgd_sph(int nin, int na, int dim, int problem, const ApgdSettings& st, SphSolve<T>& sb,
+                            const Sizes* sizes, int nblocks, cudaStream_t s) {
+    SphArgs<T> A;
+    A.nin = nin;
+    A.na = na;
+    A.cij = sb.cij;
+    A.nc = sb.nc;
+    A.slot = sb.slot;
+    A.shift = sb.shift;
+    A.inc_ptr = sb.inc_ptr;
+    A.inc = sb.inc;
+    A.invm = sb.invm;
+    A.lam0 = sb.lam[0];
+    A.lam1 = sb.lam[1];
+    A.lam2 = sb.lam[2];
+    A.u0 = sb.u[0];
+    A.u1 = sb.u[1];
+    A.u2 = sb.u[2];
+    A.u3 = sb.u[3];
+    A.partials = sb.partials;
+    A.bar = sb.barrier;
+    A.result = sb.result;
+    A.sizes = sizes;
+    A.alpha = st.alpha;
+    A.tol = st.tol;
+    A.dt2 = st.dt * st.dt;
+    A.max_ite = st.max_ite;
+    A.dynamic = st.dynamic;
+#define LA(D, P) \
+    if (dim == D && problem == P) return launch_t<T, D, P>(A, nblocks, s);
+    LA(2, 0) LA(2, 2) LA(3, 0) LA(3, 2)
+#undef LA
+    return cudaErrorInvalidValue;
+}
+template cudaError_t launch_apgd_sph<double>(int, int, int, int, const ApgdSettings&, SphSolve<double>&, const Sizes*,
+                                             int, cudaStream_t);
+template cudaError_t launch_apgd_sph<float>(int, int, int, int, const ApgdSettings&, SphSolve<float>&, const Sizes*,
+                                            int, cudaStream_t);
+
+void launch_pack_cij(const int* ci, const int* cj, int2* cij, const Sizes* sizes, long long c_cap, cudaStream_t s) {
+    k_pack_cij<<<blocks(c_cap), 256, 0, s>>>(ci, cj, cij, sizes);
+    g_sph_launches += 1;
+}
+template <typename T>
+void launch_pack_nc(const double* bn, const double* cvec, V4<T>* nc, const Sizes* sizes, long long c_cap,
+                    cudaStream_t s) {
+    k_pack_nc<T><<<blocks(c_cap), 256, 0, s>>>(bn, cvec, nc, sizes);
+    g_sph_launches += 1;
+}
+template void launch_pack_nc<double>(const double*, const double*, dvec4*, const Sizes*, long long, cudaStream_t);
+template void launch_pack_nc<float>(const double*, const double*, float4*, const Sizes*, long long, cudaStream_t);
+template <typename T>
+void launch_pack_inc(int na, const int* ptr, const int* idx, const double* bn, V4<T>* inc, long long inc_cap,
+                     cudaStream_t s) {
+    if (na <= 0) return;
+    k_pack_inc<T><<<blocks(inc_cap), 256, 0, s>>>(na, ptr, idx, bn, inc);
+    g_sph_launches += 1;
+}
+template void launch_pack_inc<double>(int, const int*, const int*, const double*, dvec4*, long long, cudaStream_t);
+template void launch_pack_inc<float>(int, const int*, const int*, const double*, float4*, long long, cudaStream_t);
+
+void launch_sph_particle64(int na, int dim, int problem, const int* ptr, const dvec4* inc, const int* slot,
+                           const double* invm, const double* lam, dvec4* u, cudaStream_t s) {
+    if (na <= 0) return;
+#define PP(D, P) \
+    if (dim == D && problem == P) k_sph_particle64<D, P><<<blocks(na), 256, 0, s>>>(na, ptr, inc, slot, invm, lam, u);
+    PP(2, 0) PP(2, 2) PP(3, 0) PP(3, 2)
+#undef PP
+    g_sph_launches += 1;
+}
+
+void launch_sph_residual64(int nin, int dim, int problem, const int2* cij, const dvec4* nc, const int* slot, double dt2,
+                           const dvec4* u, double* g, unsigned long long* viol, const Sizes* sizes, long long c_cap,
+                           cudaStream_t s) {
+#define RR(D, P) \
+    if (dim == D && problem == P) \
+        k_sph_residual64<D, P><<<blocks(c_cap), 256, 0, s>>>(nin, cij, nc, slot, dt2, u, g, viol, sizes);
+    RR(2, 0) RR(2, 2) RR(3, 0) RR(3, 2)
+#undef RR
+    g_sph_launches += 1;
+}
+
+}  // namespace scopi_gpu

@@ -278,14 +278,25 @@ __global__ void k_bbox_partial(Bodies B, int dim, double* partial) {
 
 __global__ void k_grid_setup(const double* partial, int nparts, int dim, double dmax, long long cell_cap, int na,
                              Grid* grid) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300}, rmax = 0.0;
-    for (int b = 0; b < nparts; ++b) {
+    __shared__ double sh[7][32];
+    double v[7] = {1e300, 1e300, 1e300, -1e300, -1e300, -1e300, 0.0};
+    for (int b = threadIdx.x; b < nparts; b += blockDim.x) {
         for (int k = 0; k < 3; ++k) {
-            lo[k] = fmin(lo[k], partial[b * 8 + k]);
-            hi[k] = fmax(hi[k], partial[b * 8 + 3 + k]);
+            v[k] = fmin(v[k], partial[b * 8 + k]);
+            v[3 + k] = fmax(v[3 + k], partial[b * 8 + 3 + k]);
         }
-        rmax = fmax(rmax, partial[b * 8 + 6]);
+        v[6] = fmax(v[6], partial[b * 8 + 6]);
+    }
+    for (int k = 0; k < 7; ++k) sh[k][threadIdx.x] = v[k];
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300}, rmax = 0.0;
+    for (int t = 0; t < 32; ++t) {
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = fmin(lo[k], sh[k][t]);
+            hi[k] = fmax(hi[k], sh[3 + k][t]);
+        }
+        rmax = fmax(rmax, sh[6][t]);
     }
     if (na == 0) {
         for (int k = 0; k < 3; ++k) lo[k] = hi[k] = 0.0;
@@ -650,18 +661,21 @@ __global__ void k_gamma_update(StepParams p, Contacts c, Assembly a, const doubl
 
 // OptimGradient::run velocity recovery (OptimGradient.hpp:265-284), update_velocity
 // (solver.hpp:528-546) and move_active_particles (solver.hpp:441-480).
-__global__ void k_update(Bodies B, StepParams p, const double* u, const Sizes* sizes) {
+__global__ void k_update(Bodies B, StepParams p, const double* u, int ustride, int urot, const Sizes* sizes) {
     const bool has = (u != nullptr) && (sizes == nullptr || sizes->C > 0);
     GRID_STRIDE(k, B.n - B.nin) {
         const long long b = B.nin + k;
         double* v = B.v + 3 * b;
         double* w = B.omega + 3 * b;
         if (has) {
-            for (int d = 0; d < p.dim; ++d) v[d] = v[d] + p.dt * u[6 * k + d];
-            if (p.dim == 3) {
-                for (int d = 0; d < 3; ++d) w[d] = w[d] + p.dt * u[6 * k + 3 + d];
-            } else {
-                w[2] = w[2] + p.dt * u[6 * k + 5];
+            const double* uk = u + (long long)ustride * k;
+            for (int d = 0; d < p.dim; ++d) v[d] = v[d] + p.dt * uk[d];
+            if (urot) {
+                if (p.dim == 3) {
+                    for (int d = 0; d < 3; ++d) w[d] = w[d] + p.dt * uk[3 + d];
+                } else {
+                    w[2] = w[2] + p.dt * uk[5];
+                }
             }
         }
         double ww[3];
@@ -854,9 +868,10 @@ void launch_gamma_update(const StepParams& p, Contacts& c, const Assembly& a, co
     LAUNCHED(1);
 }
 
-void launch_update(const Bodies& b, const StepParams& p, const double* u, const Sizes* sizes, cudaStream_t s) {
+void launch_update(const Bodies& b, const StepParams& p, const double* u, int ustride, int urot, const Sizes* sizes,
+                   cudaStream_t s) {
     if (b.n - b.nin <= 0) return;
-    k_update<<<blocks_for(b.n - b.nin), kThreads, 0, s>>>(b, p, u, sizes);
+    k_update<<<blocks_for(b.n - b.nin), kThreads, 0, s>>>(b, p, u, ustride, urot, sizes);
     LAUNCHED(1);
 }
 

@@ -78,7 +78,10 @@ void launch_incidence(const Bodies& b, const StepParams& p, const Contacts& c, c
 void launch_gamma_update(const StepParams& p, Contacts& c, const Assembly& a, const double* lambda, const Sizes* sizes,
                          long long c_cap, cudaStream_t s);
 // v += dt*u_v, omega += dt*u_w, then pos/q integration (u = M^-1 B^T lambda, may be null).
-void launch_update(const Bodies& b, const StepParams& p, const double* u, const Sizes* sizes, cudaStream_t s);
+// u holds `ustride` doubles per active body: translational part first, then (when
+// urot != 0) the rotational part at offset 3.
+void launch_update(const Bodies& b, const StepParams& p, const double* u, int ustride, int urot, const Sizes* sizes,
+                   cudaStream_t s);
 void launch_amat(const Bodies& b, const StepParams& p, const Contacts& c, const Sizes* sizes, long long c_cap,
                  const double* u, double* out, cudaStream_t s);
 void launch_atmat(const Bodies& b, const StepParams& p, const Contacts& c, const Sizes* sizes, long long c_cap,
@@ -143,5 +146,58 @@ void launch_residual64(const Bodies& b, const StepParams& p, const Contacts& c, 
 // lambda64 += delta32 then projection onto the cone / orthant in FP64.
 void launch_accumulate(const StepParams& p, const Contacts& c, const Assembly& a, double* lam64, const float* delta,
                        const Sizes* sizes, long long c_cap, int first, cudaStream_t s);
+
+// ----------------------------------------------------------- apgd_sph.cu
+// Normal-only problems on torque-free contacts (every pair type of the hot path): one
+// record per contact (n, c) and per incidence (+-n, contact index), translational u only.
+struct alignas(32) dvec4 {
+    double x, y, z, w;
+};
+template <typename T>
+struct V4_of;
+template <>
+struct V4_of<float> {
+    using type = float4;
+};
+template <>
+struct V4_of<double> {
+    using type = dvec4;
+};
+template <typename T>
+using V4 = typename V4_of<T>::type;
+
+template <typename T>
+struct SphSolve {
+    const int2* cij;
+    const V4<T>* nc;
+    const int* slot;
+    const double* shift;
+    const int* inc_ptr;
+    const V4<T>* inc;
+    const double* invm;       // stride 4, component 0 = 1/m
+    T* lam[3];
+    V4<T>* u[4];
+    double* partials;         // 4 * max_blocks * 8
+    unsigned int* barrier;
+    ApgdResult* result;
+};
+
+long long apgd_sph_launches();
+int apgd_sph_max_blocks(int problem, int dim, bool fp32);
+template <typename T>
+cudaError_t launch_apgd_sph(int nin, int na, int dim, int problem, const ApgdSettings& st, SphSolve<T>& sb,
+                            const Sizes* sizes, int nblocks, cudaStream_t s);
+void launch_pack_cij(const int* ci, const int* cj, int2* cij, const Sizes* sizes, long long c_cap, cudaStream_t s);
+template <typename T>
+void launch_pack_nc(const double* bn, const double* cvec, V4<T>* nc, const Sizes* sizes, long long c_cap,
+                    cudaStream_t s);
+template <typename T>
+void launch_pack_inc(int na, const int* ptr, const int* idx, const double* bn, V4<T>* inc, long long inc_cap,
+                     cudaStream_t s);
+void launch_sph_particle64(int na, int dim, int problem, const int* ptr, const dvec4* inc, const int* slot,
+                           const double* invm, const double* lam, dvec4* u, cudaStream_t s);
+void launch_sph_residual64(int nin, int dim, int problem, const int2* cij, const dvec4* nc, const int* slot, double dt2,
+                           const dvec4* u, double* g, unsigned long long* viol, const Sizes* sizes, long long c_cap,
+                           cudaStream_t s);
 
 }  // namespace scopi_gpu

@@ -67,6 +67,15 @@ struct scopi_gpu_handle {
           *d_coef32 = nullptr;
     float* d_lam32[3] = {nullptr, nullptr, nullptr};
     float* d_g32 = nullptr;
+    // packed records of the torque-free (sphere) kernels
+    int2* d_cij = nullptr;
+    dvec4* d_nc64 = nullptr;
+    float4* d_nc32 = nullptr;
+    dvec4* d_incv64 = nullptr;
+    float4* d_incv32 = nullptr;
+    dvec4* d_us64[4] = {nullptr, nullptr, nullptr, nullptr};
+    float4* d_us32[4] = {nullptr, nullptr, nullptr, nullptr};
+    dvec4* d_usfin = nullptr;
 
     // fixed small buffers
     DevMem fixed_mem;
@@ -77,13 +86,14 @@ struct scopi_gpu_handle {
     Sizes* h_sizes = nullptr;          // pinned
     ApgdResult* h_result = nullptr;    // pinned
     unsigned long long* h_viol = nullptr;
-    int max_blocks64 = 0, max_blocks32 = 0;
+    int max_blocks64 = 0, max_blocks32 = 0, max_sph64 = 0, max_sph32 = 0;
 
     // results of the last step
     const double* last_lambda = nullptr;
     long long last_M = 0;
     scopi_gpu_stats stats{};
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t ev_a[2] = {nullptr, nullptr};  // around the APGD launches
 
     int fail(int code, const std::string& msg) {
         err = msg;
@@ -95,6 +105,10 @@ struct scopi_gpu_handle {
     }
     int mult_per_contact() const { return P.problem == SCOPI_GPU_FRICTION ? 3 : (P.problem == SCOPI_GPU_VISCOUS ? 2 : 1); }
     bool mixed() const { return P.precision == SCOPI_GPU_MIXED; }
+    // Normal-only problems: every pair type of the hot path (sphere-sphere, sphere-plane,
+    // sphere-segment) has its lever arm along the normal, so the rotational Jacobian terms
+    // vanish and the translational kernels apply.
+    bool sphere_mode() const { return P.problem != SCOPI_GPU_FRICTION; }
 
     Bodies bodies() const {
         Bodies b;
@@ -144,8 +158,12 @@ struct scopi_gpu_handle {
         cudaError_t e;
         max_blocks64 = apgd_max_blocks(P.problem, P.dim, false);
         max_blocks32 = apgd_max_blocks(P.problem, P.dim, true);
-        const int mb = std::max(std::max(max_blocks64, max_blocks32), 1);
-        if ((e = alloc(fixed_mem, d_partials, 2 * (size_t)mb * 8)) != cudaSuccess) return cuda_fail(e, "alloc");
+        if (sphere_mode()) {
+            max_sph64 = apgd_sph_max_blocks(P.problem, P.dim, false);
+            max_sph32 = apgd_sph_max_blocks(P.problem, P.dim, true);
+        }
+        const int mb = std::max({max_blocks64, max_blocks32, max_sph64, max_sph32, 1});
+        if ((e = alloc(fixed_mem, d_partials, 4 * (size_t)mb * 8)) != cudaSuccess) return cuda_fail(e, "alloc");
         if ((e = alloc(fixed_mem, d_barrier, 4)) != cudaSuccess) return cuda_fail(e, "alloc");
         if ((e = alloc(fixed_mem, d_result, 1)) != cudaSuccess) return cuda_fail(e, "alloc");
         if ((e = alloc(fixed_mem, d_viol, 1)) != cudaSuccess) return cuda_fail(e, "alloc");
@@ -159,6 +177,8 @@ struct scopi_gpu_handle {
         if ((e = cudaMallocHost(&h_viol, sizeof(unsigned long long))) != cudaSuccess)
             return cuda_fail(e, "cudaMallocHost");
         for (auto& x : ev)
+            if ((e = cudaEventCreate(&x)) != cudaSuccess) return cuda_fail(e, "cudaEventCreate");
+        for (auto& x : ev_a)
             if ((e = cudaEventCreate(&x)) != cudaSuccess) return cuda_fail(e, "cudaEventCreate");
         return 0;
     }
@@ -176,6 +196,11 @@ struct scopi_gpu_handle {
         A(d_vd, 3 * (size_t)n) A(d_omega_d, 3 * (size_t)n) A(d_f, 3 * (size_t)n) A(d_m, n) A(d_j, 3 * (size_t)n)
         A(d_radius, n) A(d_length, n) A(d_invm64, 4 * (size_t)na + 4) A(d_invm32, 4 * (size_t)na + 4)
         A(d_ufin, 6 * (size_t)na + 6)
+        A(d_usfin, (size_t)na + 1)
+        for (int k = 0; k < 4; ++k) {
+            A(d_us64[k], (size_t)na + 1)
+            A(d_us32[k], (size_t)na + 1)
+        }
         for (int k = 0; k < 3; ++k) {
             A(d_u64[k], 6 * (size_t)na + 6)
             A(d_u32[k], 6 * (size_t)na + 6)
@@ -219,13 +244,17 @@ struct scopi_gpu_handle {
             for (int k = 0; k < 3; ++k) A(d_lam32[k], M)
             A(d_g32, M)
         }
+        A(d_cij, cap) A(d_nc64, cap) A(d_incv64, 2 * cap)
+        if (mixed()) {
+            A(d_nc32, cap) A(d_incv32, 2 * cap)
+        }
 #undef A
         cudaMemsetAsync(d_sizes_cur, 0, sizeof(Sizes), stream);
         cudaMemsetAsync(d_sizes_old, 0, sizeof(Sizes), stream);
         return 0;
     }
 
-    long long launches() const { return detect_launches() + apgd_launches(); }
+    long long launches() const { return detect_launches() + apgd_launches() + apgd_sph_launches(); }
 
     // contact detection + closest points + assembly + incidence lists into `cur`
     int detect_and_assemble(double dt, bool assemble) {
@@ -332,6 +361,49 @@ struct scopi_gpu_handle {
         return 0;
     }
 
+    template <typename T>
+    int run_apgd_sph(SphSolve<T>& sb, int maxb, double dt, double tol, long long max_ite, long long M) {
+        ApgdSettings st;
+        st.alpha = P.alpha;
+        st.tol = tol;
+        st.max_ite = max_ite;
+        st.dynamic = P.dynamic_descent;
+        st.dt = dt;
+        st.mu = P.mu;
+        // lambda = lambda_prev = 0 and u(lambda) = u(y) = 0 (cold start, apgd.hpp:152-159)
+        cudaMemsetAsync(sb.lam[0], 0, M * sizeof(T), stream);
+        cudaMemsetAsync(sb.lam[1], 0, M * sizeof(T), stream);
+        cudaMemsetAsync(sb.u[0], 0, (size_t)na * sizeof(V4<T>), stream);
+        cudaMemsetAsync(sb.u[2], 0, (size_t)na * sizeof(V4<T>), stream);
+        cudaMemsetAsync(d_barrier, 0, 4 * sizeof(unsigned int), stream);
+        const int nb = nblocks_for(maxb, std::max<long long>(h_sizes->C, na));
+        cudaError_t e = launch_apgd_sph<T>(nin, na, P.dim, P.problem, st, sb, d_sizes_cur, nb, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "APGD launch");
+        cudaMemcpyAsync(h_result, d_result, sizeof(ApgdResult), cudaMemcpyDeviceToHost, stream);
+        e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cuda_fail(e, "APGD");
+        if (h_result->error == 1) return fail(SCOPI_GPU_ETIMEOUT, "APGD grid barrier timed out");
+        return 0;
+    }
+
+    template <typename T>
+    SphSolve<T> sph_buffers(const V4<T>* nc, const V4<T>* incv, T* const* lam, V4<T>* const* u) const {
+        SphSolve<T> sb{};
+        sb.cij = d_cij;
+        sb.nc = nc;
+        sb.slot = as.slot;
+        sb.shift = nullptr;
+        sb.inc_ptr = inc.ptr;
+        sb.inc = incv;
+        sb.invm = d_invm64;
+        for (int k = 0; k < 3; ++k) sb.lam[k] = lam[k];
+        for (int k = 0; k < 4; ++k) sb.u[k] = u[k];
+        sb.partials = d_partials;
+        sb.barrier = d_barrier;
+        sb.result = d_result;
+        return sb;
+    }
+
     int step(double dt) {
         Bodies b = bodies();
         StepParams sp = step_params(dt);
@@ -345,56 +417,69 @@ struct scopi_gpu_handle {
         const long long M = P.problem == SCOPI_GPU_FRICTION ? 3LL * C : (long long)C + h_sizes->n_extra;
         cudaEventRecord(ev[1], stream);
         const double* ufin = nullptr;
+        int ustride = 6, urot = 1;
         stats.iterations = stats.backtracks = stats.restarts = stats.fp32_iterations = stats.corrections = 0;
         stats.converged = 1;
         stats.status = 0;
         stats.violation = 0.0;
         float ms_apgd = 0.0f;
         if (C > 0) {
-            cudaEvent_t a0, a1;
-            cudaEventCreate(&a0);
-            cudaEventCreate(&a1);
+            if (sphere_mode()) {
+                launch_pack_cij(cur.ci, cur.cj, d_cij, d_sizes_cur, c_cap, stream);
+                launch_pack_nc<double>(as.bn, as.cvec, d_nc64, d_sizes_cur, c_cap, stream);
+                launch_pack_inc<double>(na, inc.ptr, inc.idx, as.bn, d_incv64, 2 * c_cap, stream);
+                ustride = 4;
+                urot = 0;
+            }
             if (!mixed()) {
-                SolveBuffers<double> sb{};
-                sb.bn = as.bn;
-                sb.bai = as.bai;
-                sb.baj = as.baj;
-                sb.bP = as.bP;
-                sb.cvec = as.cvec;
-                sb.shift = nullptr;
-                sb.inc_ptr = inc.ptr;
-                sb.inc_idx = inc.idx;
-                sb.inc_coef = inc.coef;
-                for (int k = 0; k < 3; ++k) {
-                    sb.lam[k] = d_lam64[k];
-                    sb.u[k] = d_u64[k];
+                cudaEventRecord(ev_a[0], stream);
+                if (sphere_mode()) {
+                    SphSolve<double> sb = sph_buffers<double>(d_nc64, d_incv64, d_lam64, d_us64);
+                    rc = run_apgd_sph<double>(sb, max_sph64, dt, P.tolerance, P.max_ite, M);
+                    if (rc) return rc;
+                    ufin = reinterpret_cast<const double*>(d_us64[h_result->u_buf]);
+                } else {
+                    SolveBuffers<double> sb{};
+                    sb.bn = as.bn;
+                    sb.bai = as.bai;
+                    sb.baj = as.baj;
+                    sb.bP = as.bP;
+                    sb.cvec = as.cvec;
+                    sb.shift = nullptr;
+                    sb.inc_ptr = inc.ptr;
+                    sb.inc_idx = inc.idx;
+                    sb.inc_coef = inc.coef;
+                    for (int k = 0; k < 3; ++k) {
+                        sb.lam[k] = d_lam64[k];
+                        sb.u[k] = d_u64[k];
+                    }
+                    sb.g = d_g64;
+                    sb.partials = d_partials;
+                    sb.barrier = d_barrier;
+                    sb.result = d_result;
+                    rc = run_apgd<double>(sb, d_invm64, max_blocks64, dt, P.tolerance, P.max_ite, M);
+                    if (rc) return rc;
+                    ufin = d_u64[h_result->u_buf];
                 }
-                sb.g = d_g64;
-                sb.partials = d_partials;
-                sb.barrier = d_barrier;
-                sb.result = d_result;
-                cudaEventRecord(a0, stream);
-                rc = run_apgd<double>(sb, d_invm64, max_blocks64, dt, P.tolerance, P.max_ite, M);
-                cudaEventRecord(a1, stream);
-                if (rc) return rc;
+                cudaEventRecord(ev_a[1], stream);
+                cudaEventSynchronize(ev_a[1]);
+                cudaEventElapsedTime(&ms_apgd, ev_a[0], ev_a[1]);
                 accumulate_stats(false);
                 last_lambda = d_lam64[h_result->lam_buf];
-                ufin = d_u64[h_result->u_buf];
             } else {
-                rc = mixed_solve(dt, M, a0, a1, ms_apgd);
+                rc = mixed_solve(dt, M, ms_apgd);
                 if (rc) return rc;
                 last_lambda = d_lamacc;
-                ufin = d_ufin;
+                ufin = sphere_mode() ? reinterpret_cast<const double*>(d_usfin) : d_ufin;
             }
-            cudaEventSynchronize(a1);
-            float ms = 0.0f;
-            cudaEventElapsedTime(&ms, a0, a1);
-            if (!mixed()) ms_apgd = ms;
-            cudaEventDestroy(a0);
-            cudaEventDestroy(a1);
             // violation of the returned multipliers (FP64 residual)
             cudaMemsetAsync(d_viol, 0, sizeof(unsigned long long), stream);
-            launch_residual64(b, sp, cur, as, ufin, d_res64, d_viol, d_sizes_cur, c_cap, stream);
+            if (sphere_mode())
+                launch_sph_residual64(nin, P.dim, P.problem, d_cij, d_nc64, as.slot, dt * dt,
+                                      reinterpret_cast<const dvec4*>(ufin), d_res64, d_viol, d_sizes_cur, c_cap,
+                                      stream);
+            else
+                launch_residual64(b, sp, cur, as, ufin, d_res64, d_viol, d_sizes_cur, c_cap, stream);
             cudaMemcpyAsync(h_viol, d_viol, sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream);
             if (P.problem == SCOPI_GPU_VISCOUS) launch_gamma_update(sp, cur, as, last_lambda, d_sizes_cur, c_cap, stream);
         } else {
@@ -403,7 +488,7 @@ struct scopi_gpu_handle {
         }
         last_M = M;
         cudaEventRecord(ev[2], stream);
-        launch_update(b, sp, ufin, d_sizes_cur, stream);
+        launch_update(b, sp, ufin, ustride, urot, d_sizes_cur, stream);
         cudaEventRecord(ev[3], stream);
         cudaError_t e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) return cuda_fail(e, "step");
@@ -437,74 +522,90 @@ struct scopi_gpu_handle {
     // FP32 APGD iterations with an FP64 outer correction: after each FP32 solve the
     // residual g = Q lambda + c and the violation are recomputed in FP64, and APGD is
     // rerun in FP32 on the correction delta (linear term g, constraint lambda + delta in K).
-    int mixed_solve(double dt, long long M, cudaEvent_t a0, cudaEvent_t a1, float& ms_apgd) {
+    int mixed_solve(double dt, long long M, float& ms_apgd) {
         Bodies b = bodies();
         StepParams sp = step_params(dt);
-        const int C = h_sizes->C;
         const int per = P.problem == SCOPI_GPU_FRICTION ? 3 : 1;
-        launch_convert<double, float>(as.bn, d_bn32, 3 * c_cap, &d_sizes_cur->C, 3, stream);
-        launch_convert<double, float>(as.bai, d_bai32, 3 * c_cap, &d_sizes_cur->C, 3, stream);
-        launch_convert<double, float>(as.baj, d_baj32, 3 * c_cap, &d_sizes_cur->C, 3, stream);
-        if (P.problem == SCOPI_GPU_FRICTION)
-            launch_convert<double, float>(as.bP, d_bP32, 18 * c_cap, &d_sizes_cur->C, 18, stream);
-        else
-            launch_convert<double, float>(inc.coef, d_coef32, 12 * c_cap, &d_sizes_cur->C, 12, stream);
-        launch_convert<double, float>(as.cvec, d_cvec32, per * c_cap, &d_sizes_cur->C, per, stream);
+        SphSolve<float> sbs{};
         SolveBuffers<float> sb{};
-        sb.bn = d_bn32;
-        sb.bai = d_bai32;
-        sb.baj = d_baj32;
-        sb.bP = d_bP32;
-        sb.cvec = d_cvec32;
-        sb.shift = nullptr;
-        sb.inc_ptr = inc.ptr;
-        sb.inc_idx = inc.idx;
-        sb.inc_coef = d_coef32;
-        for (int k = 0; k < 3; ++k) {
-            sb.lam[k] = d_lam32[k];
-            sb.u[k] = d_u32[k];
+        if (sphere_mode()) {
+            launch_pack_nc<float>(as.bn, as.cvec, d_nc32, d_sizes_cur, c_cap, stream);
+            launch_pack_inc<float>(na, inc.ptr, inc.idx, as.bn, d_incv32, 2 * c_cap, stream);
+            sbs = sph_buffers<float>(d_nc32, d_incv32, d_lam32, d_us32);
+        } else {
+            launch_convert<double, float>(as.bn, d_bn32, 3 * c_cap, &d_sizes_cur->C, 3, stream);
+            launch_convert<double, float>(as.bai, d_bai32, 3 * c_cap, &d_sizes_cur->C, 3, stream);
+            launch_convert<double, float>(as.baj, d_baj32, 3 * c_cap, &d_sizes_cur->C, 3, stream);
+            if (P.problem == SCOPI_GPU_FRICTION)
+                launch_convert<double, float>(as.bP, d_bP32, 18 * c_cap, &d_sizes_cur->C, 18, stream);
+            else
+                launch_convert<double, float>(inc.coef, d_coef32, 12 * c_cap, &d_sizes_cur->C, 12, stream);
+            launch_convert<double, float>(as.cvec, d_cvec32, per * c_cap, &d_sizes_cur->C, per, stream);
+            sb.bn = d_bn32;
+            sb.bai = d_bai32;
+            sb.baj = d_baj32;
+            sb.bP = d_bP32;
+            sb.cvec = d_cvec32;
+            sb.shift = nullptr;
+            sb.inc_ptr = inc.ptr;
+            sb.inc_idx = inc.idx;
+            sb.inc_coef = d_coef32;
+            for (int k = 0; k < 3; ++k) {
+                sb.lam[k] = d_lam32[k];
+                sb.u[k] = d_u32[k];
+            }
+            sb.g = d_g32;
+            sb.partials = d_partials;
+            sb.barrier = d_barrier;
+            sb.result = d_result;
         }
-        sb.g = d_g32;
-        sb.partials = d_partials;
-        sb.barrier = d_barrier;
-        sb.result = d_result;
         float total = 0.0f;
-        cudaEventRecord(a0, stream);
-        int rc = run_apgd<float>(sb, d_invm32, max_blocks32, dt, P.tolerance, P.max_ite, M);
-        cudaEventRecord(a1, stream);
+        auto solve32 = [&]() -> int {
+            cudaEventRecord(ev_a[0], stream);
+            int r = sphere_mode() ? run_apgd_sph<float>(sbs, max_sph32, dt, P.tolerance, P.max_ite, M)
+                                  : run_apgd<float>(sb, d_invm32, max_blocks32, dt, P.tolerance, P.max_ite, M);
+            cudaEventRecord(ev_a[1], stream);
+            if (r) return r;
+            cudaEventSynchronize(ev_a[1]);
+            float ms = 0;
+            cudaEventElapsedTime(&ms, ev_a[0], ev_a[1]);
+            total += ms;
+            accumulate_stats(true);
+            return 0;
+        };
+        int rc = solve32();
         if (rc) return rc;
-        cudaEventSynchronize(a1);
-        float ms = 0;
-        cudaEventElapsedTime(&ms, a0, a1);
-        total += ms;
-        accumulate_stats(true);
         launch_accumulate(sp, cur, as, d_lamacc, d_lam32[h_result->lam_buf], d_sizes_cur, c_cap, 1, stream);
         for (int k = 0;; ++k) {
-            launch_particle_pass64(b, sp, cur, as, inc, d_invm64, d_lamacc, d_ufin, stream);
             cudaMemsetAsync(d_viol, 0, sizeof(unsigned long long), stream);
-            launch_residual64(b, sp, cur, as, d_ufin, d_res64, d_viol, d_sizes_cur, c_cap, stream);
+            if (sphere_mode()) {
+                launch_sph_particle64(na, P.dim, P.problem, inc.ptr, d_incv64, as.slot, d_invm64, d_lamacc, d_usfin,
+                                      stream);
+                launch_sph_residual64(nin, P.dim, P.problem, d_cij, d_nc64, as.slot, dt * dt, d_usfin, d_res64, d_viol,
+                                      d_sizes_cur, c_cap, stream);
+            } else {
+                launch_particle_pass64(b, sp, cur, as, inc, d_invm64, d_lamacc, d_ufin, stream);
+                launch_residual64(b, sp, cur, as, d_ufin, d_res64, d_viol, d_sizes_cur, c_cap, stream);
+            }
             cudaMemcpyAsync(h_viol, d_viol, sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream);
             cudaError_t e = cudaStreamSynchronize(stream);
             if (e != cudaSuccess) return cuda_fail(e, "mixed residual");
             double viol;
             std::memcpy(&viol, h_viol, sizeof(double));
             if (viol <= P.mixed_violation_tol || k >= P.mixed_max_corrections) break;
-            // correction solve
-            launch_convert<double, float>(d_res64, d_cvec32, per * c_cap, &d_sizes_cur->C, per, stream);
-            sb.shift = d_lamacc;
-            cudaEventRecord(a0, stream);
-            rc = run_apgd<float>(sb, d_invm32, max_blocks32, dt, P.tolerance, P.max_ite, M);
-            cudaEventRecord(a1, stream);
+            // correction solve: linear term = FP64 residual, solution offset = lambda so far
+            if (sphere_mode()) {
+                launch_pack_nc<float>(as.bn, d_res64, d_nc32, d_sizes_cur, c_cap, stream);
+                sbs.shift = d_lamacc;
+            } else {
+                launch_convert<double, float>(d_res64, d_cvec32, per * c_cap, &d_sizes_cur->C, per, stream);
+                sb.shift = d_lamacc;
+            }
+            rc = solve32();
             if (rc) return rc;
-            cudaEventSynchronize(a1);
-            cudaEventElapsedTime(&ms, a0, a1);
-            total += ms;
-            accumulate_stats(true);
             stats.corrections += 1;
             launch_accumulate(sp, cur, as, d_lamacc, d_lam32[h_result->lam_buf], d_sizes_cur, c_cap, 0, stream);
         }
-        (void)C;
-        (void)M;
         ms_apgd = total;
         return 0;
     }
@@ -587,6 +688,8 @@ int32_t scopi_gpu_destroy(scopi_gpu_handle* h) {
     if (h->h_result) cudaFreeHost(h->h_result);
     if (h->h_viol) cudaFreeHost(h->h_viol);
     for (auto& x : h->ev)
+        if (x) cudaEventDestroy(x);
+    for (auto& x : h->ev_a)
         if (x) cudaEventDestroy(x);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;

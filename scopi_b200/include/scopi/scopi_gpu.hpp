@@ -1,0 +1,549 @@
+// scopi_gpu.hpp -- header-only C++ mirror of the SCoPI API (hpc-maths/scopi v0.1.0) whose
+// time step runs on a B200 through the C ABI of libscopi_gpu.so (include/scopi_gpu.h).
+//
+// Same names, argument meaning and defaults as the reference for the hot path:
+//   scopi_container<dim>::push_back           include/scopi/container.hpp:339-384
+//   property<dim> builder                     include/scopi/property.hpp:16-200
+//   sphere / plane / segment                  include/scopi/objects/types/{sphere,plane,segment}.hpp
+//   quaternion(), mult_quaternion, normalize  src/quaternion.cpp:6-120
+//   NoFriction / Friction / Viscous           include/scopi/contact/property.hpp:14-36
+//   contact_property<...>                     include/scopi/contact/property.hpp:41-128
+//   ContactsParams<contact_kdtree/brute>      include/scopi/contact/contact_kdtree.hpp:203-238,
+//                                             include/scopi/contact/contact_brute_force.hpp:470-495
+//   apgd_params / OptimGradient<apgd>         include/scopi/solvers/apgd.hpp:105-124,
+//                                             include/scopi/solvers/OptimGradient.hpp:56-349
+//   vap_fixed / vap_fpd                       include/scopi/vap/vap_fixed.hpp, vap_fpd.hpp
+//   ScopiSolver<dim, problem, optim, contact, vap>::run / get_params / current_contacts
+//                                             include/scopi/solver.hpp:91-327
+//   Params<solver> (optim_params, default_contact_property, contact_method_params,
+//                   vap_params, solver_params) include/scopi/params.hpp:144-197
+//
+// The policy types are the GPU ones (namespace scopi::gpu); the reference's policy names
+// are aliases of them, so a reference demo compiles against these headers unchanged and a
+// demo written for the reference only swaps its policy types to scopi::gpu::... .
+// Precision of the APGD iterations is a policy: gpu::apgd<gpu::fp64> (the reference's
+// arithmetic) or gpu::apgd<gpu::mixed> (FP32 iterations + FP64 outer correction).
+#pragma once
+
+#include <array>
+#include <cmath>
+#include <cstddef>
+#include <cstdint>
+#include <filesystem>
+#include <initializer_list>
+#include <iostream>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "../../../include/scopi_gpu.h"
+
+namespace scopi {
+
+namespace type {
+template <std::size_t dim>
+using position_t = std::array<double, dim>;
+using quaternion_t = std::array<double, 4>;
+}  // namespace type
+
+// ------------------------------------------------------------------ quaternions
+inline void normalize(type::quaternion_t& q) {
+    const double n = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    for (auto& c : q) c /= n;
+}
+inline type::quaternion_t quaternion(double angle, const std::array<double, 3>& axes) {
+    type::quaternion_t out = {std::cos(angle / 2), std::sin(angle / 2) * axes[0], std::sin(angle / 2) * axes[1],
+                              std::sin(angle / 2) * axes[2]};
+    normalize(out);
+    return out;
+}
+inline type::quaternion_t quaternion(double angle, const std::array<double, 2>& axes) {
+    return quaternion(angle, std::array<double, 3>{axes[0], axes[1], 1.0});
+}
+inline type::quaternion_t quaternion(double angle = 0.0) { return quaternion(angle, std::array<double, 3>{0., 0., 1.}); }
+inline type::quaternion_t mult_quaternion(const type::quaternion_t& a, const type::quaternion_t& b) {
+    type::quaternion_t r;
+    r[0] = a[0] * b[0];
+    for (std::size_t d = 0; d < 3; ++d) {
+        r[0] -= a[d + 1] * b[d + 1];
+        r[d + 1] = a[0] * b[d + 1] + b[0] * a[d + 1];
+    }
+    r[1] += (a[2] * b[3] - a[3] * b[2]);
+    r[2] += (a[3] * b[1] - a[1] * b[3]);
+    r[3] += (a[1] * b[2] - a[2] * b[1]);
+    return r;
+}
+
+// ------------------------------------------------------------------ contact models
+class NoFriction {};
+class Friction {};
+class Viscous {};
+
+template <class problem_t>
+struct contact_property;
+template <>
+struct contact_property<NoFriction> {};
+template <>
+struct contact_property<Friction> {
+    double mu = 0.1;
+};
+template <>
+struct contact_property<Viscous> {
+    double gamma = 0;
+    double gamma_min = -2.;
+    double gamma_tol = 1e-6;
+};
+
+template <class problem_t>
+constexpr int32_t problem_code() {
+    if constexpr (std::is_same_v<problem_t, Friction>) return SCOPI_GPU_FRICTION;
+    if constexpr (std::is_same_v<problem_t, Viscous>) return SCOPI_GPU_VISCOUS;
+    return SCOPI_GPU_NOFRICTION;
+}
+
+// ------------------------------------------------------------------ objects
+template <std::size_t dim>
+struct object_base {
+    type::position_t<dim> position{};
+    type::quaternion_t q = quaternion(0.0);
+    int32_t shape = SCOPI_GPU_SPHERE;
+    double radius_ = 0.0;
+    double length_ = 0.0;
+};
+
+template <std::size_t dim, bool owner = true>
+class sphere : public object_base<dim> {
+  public:
+    sphere(std::initializer_list<type::position_t<dim>> pos, double radius) {
+        this->position = *pos.begin();
+        this->radius_ = radius;
+        this->shape = SCOPI_GPU_SPHERE;
+    }
+    sphere(std::initializer_list<type::position_t<dim>> pos, type::quaternion_t q, double radius)
+        : sphere(pos, radius) {
+        this->q = q;
+    }
+    double radius() const { return this->radius_; }
+};
+
+template <std::size_t dim, bool owner = true>
+class plane : public object_base<dim> {
+  public:
+    plane(std::initializer_list<type::position_t<dim>> pos, double angle = 0) {
+        this->position = *pos.begin();
+        this->q = quaternion(angle);
+        this->shape = SCOPI_GPU_PLANE;
+    }
+    plane(std::initializer_list<type::position_t<dim>> pos, std::initializer_list<type::quaternion_t> q) {
+        this->position = *pos.begin();
+        this->q = *q.begin();
+        this->shape = SCOPI_GPU_PLANE;
+    }
+};
+
+template <std::size_t dim, bool owner = true>
+class segment : public object_base<dim> {
+    static_assert(dim == 2, "segments are 2D objects");
+
+  public:
+    segment(const type::position_t<dim>& p1, const type::position_t<dim>& p2) {
+        for (std::size_t d = 0; d < dim; ++d) this->position[d] = 0.5 * (p1[d] + p2[d]);
+        this->q = quaternion(std::atan2(p1[0] - p2[0], p2[1] - p1[1]));
+        const double dx = p2[0] - p1[0], dy = p2[1] - p1[1];
+        this->length_ = std::sqrt(dx * dx + dy * dy);
+        this->shape = SCOPI_GPU_SEGMENT;
+    }
+};
+
+// ------------------------------------------------------------------ property
+template <std::size_t dim>
+class property {
+  public:
+    using vec = type::position_t<dim>;
+    using rot = std::conditional_t<dim == 2, double, std::array<double, 3>>;
+    property& velocity(const vec& v) { m_v = v; return *this; }
+    property& velocity(std::initializer_list<vec> v) { m_v = *v.begin(); return *this; }
+    property& desired_velocity(const vec& v) { m_dv = v; return *this; }
+    property& desired_velocity(std::initializer_list<vec> v) { m_dv = *v.begin(); return *this; }
+    property& omega(const rot& w) { m_w = w; return *this; }
+    property& desired_omega(const rot& w) { m_dw = w; return *this; }
+    property& force(const vec& f) { m_f = f; return *this; }
+    property& force(std::initializer_list<vec> f) { m_f = *f.begin(); return *this; }
+    property& mass(double m) { m_m = m; return *this; }
+    property& moment_inertia(const rot& j) { m_j = j; return *this; }
+    property& activate() { m_active = true; return *this; }
+    property& deactivate() { m_active = false; return *this; }
+    const vec& velocity() const { return m_v; }
+    const vec& desired_velocity() const { return m_dv; }
+    const rot& omega() const { return m_w; }
+    const rot& desired_omega() const { return m_dw; }
+    const vec& force() const { return m_f; }
+    double mass() const { return m_m; }
+    const rot& moment_inertia() const { return m_j; }
+    bool is_active() const { return m_active; }
+
+  private:
+    vec m_v{}, m_dv{}, m_f{};
+    rot m_w{}, m_dw{}, m_j{};
+    double m_m = 1.0;
+    bool m_active = true;
+};
+
+// ------------------------------------------------------------------ container
+template <std::size_t dim>
+class vec_ref {
+  public:
+    explicit vec_ref(double* p) : m_p(p) {}
+    double& operator()(std::size_t d) const { return m_p[d]; }
+    double& operator[](std::size_t d) const { return m_p[d]; }
+    vec_ref& operator=(const type::position_t<dim>& v) {
+        for (std::size_t d = 0; d < dim; ++d) m_p[d] = v[d];
+        return *this;
+    }
+    vec_ref& operator=(std::initializer_list<double> v) {
+        std::size_t d = 0;
+        for (double x : v) m_p[d++] = x;
+        return *this;
+    }
+    operator type::position_t<dim>() const {
+        type::position_t<dim> o;
+        for (std::size_t d = 0; d < dim; ++d) o[d] = m_p[d];
+        return o;
+    }
+
+  private:
+    double* m_p;
+};
+
+template <std::size_t dim>
+class scopi_container {
+  public:
+    static constexpr std::size_t dim_ = dim;
+    using rot_ref = std::conditional_t<dim == 2, double&, vec_ref<3>>;
+
+    template <class Obj>
+    void push_back(const Obj& s, const property<dim>& p = property<dim>()) {
+        if (!p.is_active()) {
+            if (m_nb_inactive != size())
+                throw std::runtime_error("All the obstacles must be pushed before the active particles.");
+            ++m_nb_inactive;
+        }
+        m_shape.push_back(s.shape);
+        append3(m_pos, s.position);
+        for (double c : s.q) m_q.push_back(c);
+        append3(m_v, p.velocity());
+        append3(m_vd, p.desired_velocity());
+        append3(m_f, p.force());
+        appendrot(m_w, p.omega());
+        appendrot(m_dw, p.desired_omega());
+        appendrot(m_j, p.moment_inertia());
+        m_m.push_back(p.mass());
+        m_radius.push_back(s.radius_);
+        m_length.push_back(s.length_);
+    }
+
+    std::size_t size() const { return m_shape.size(); }
+    std::size_t nb_inactive() const { return m_nb_inactive; }
+    std::size_t nb_active() const { return size() - m_nb_inactive; }
+
+    struct vec_field {
+        std::vector<double>* v;
+        vec_ref<dim> operator()(std::size_t i) const { return vec_ref<dim>(v->data() + 3 * i); }
+        vec_ref<dim> operator[](std::size_t i) const { return (*this)(i); }
+    };
+    struct rot_field {
+        std::vector<double>* v;
+        rot_ref operator()(std::size_t i) const {
+            if constexpr (dim == 2)
+                return (*v)[3 * i + 2];
+            else
+                return vec_ref<3>(v->data() + 3 * i);
+        }
+        rot_ref operator[](std::size_t i) const { return (*this)(i); }
+    };
+    struct quat_field {
+        std::vector<double>* v;
+        vec_ref<4> operator()(std::size_t i) const { return vec_ref<4>(v->data() + 4 * i); }
+        vec_ref<4> operator[](std::size_t i) const { return (*this)(i); }
+    };
+    vec_field pos() { return {&m_pos}; }
+    vec_field v() { return {&m_v}; }
+    vec_field vd() { return {&m_vd}; }
+    vec_field f() { return {&m_f}; }
+    rot_field omega() { return {&m_w}; }
+    rot_field desired_omega() { return {&m_dw}; }
+    rot_field j() { return {&m_j}; }
+    quat_field q() { return {&m_q}; }
+    std::vector<double>& m() { return m_m; }
+
+    // C ABI view (host arrays owned by the container)
+    scopi_gpu_particles abi() {
+        scopi_gpu_particles p;
+        p.n = (int64_t)size();
+        p.nb_inactive = (int64_t)m_nb_inactive;
+        p.shape = m_shape.data();
+        p.pos = m_pos.data();
+        p.q = m_q.data();
+        p.v = m_v.data();
+        p.omega = m_w.data();
+        p.vd = m_vd.data();
+        p.omega_d = m_dw.data();
+        p.f = m_f.data();
+        p.m = m_m.data();
+        p.j = m_j.data();
+        p.radius = m_radius.data();
+        p.length = m_length.data();
+        return p;
+    }
+
+  private:
+    template <class V>
+    static void append3(std::vector<double>& dst, const V& v) {
+        for (std::size_t d = 0; d < 3; ++d) dst.push_back(d < dim ? v[d] : 0.0);
+    }
+    template <class R>
+    static void appendrot(std::vector<double>& dst, const R& r) {
+        if constexpr (dim == 2) {
+            dst.push_back(0.0);
+            dst.push_back(0.0);
+            dst.push_back(r);
+        } else {
+            for (std::size_t d = 0; d < 3; ++d) dst.push_back(r[d]);
+        }
+    }
+    std::vector<int32_t> m_shape;
+    std::vector<double> m_pos, m_q, m_v, m_w, m_vd, m_dw, m_f, m_m, m_j, m_radius, m_length;
+    std::size_t m_nb_inactive = 0;
+};
+
+// ------------------------------------------------------------------ contacts record
+template <std::size_t dim, class problem_t>
+struct neighbor {
+    std::size_t i, j;
+    double dij;
+    type::position_t<dim> nij, pi, pj;
+    contact_property<problem_t> property;
+};
+
+// ------------------------------------------------------------------ GPU policies
+namespace gpu {
+struct fp64 {
+    static constexpr int32_t code = SCOPI_GPU_FP64;
+};
+struct mixed {
+    static constexpr int32_t code = SCOPI_GPU_MIXED;
+};
+
+struct apgd_params {  // apgd.hpp:105-124 (+ the mixed form's correction target)
+    double alpha = 0.05;
+    std::size_t max_ite = 10000;
+    double tolerance = 1e-7;
+    bool dynamic_descent = true;
+    double mixed_violation_tol = 1e-6;
+    int mixed_max_corrections = 3;
+};
+
+template <class precision = fp64>
+struct apgd {
+    using params_t = apgd_params;
+    using precision_t = precision;
+};
+
+template <class Method>
+struct OptimGradient {
+    using method_t = Method;
+    using params_t = typename Method::params_t;
+    params_t m_params;
+    params_t& get_params() { return m_params; }
+};
+
+template <class D>
+struct ContactsParams;
+
+template <class problem_t>
+struct contact_kdtree {
+    static constexpr int32_t code = SCOPI_GPU_KDTREE;
+};
+template <class problem_t>
+struct contact_brute_force {
+    static constexpr int32_t code = SCOPI_GPU_BRUTE_FORCE;
+};
+template <class problem_t>
+struct ContactsParams<contact_kdtree<problem_t>> {  // contact_kdtree.hpp:203-238
+    double dmax{2.};
+    double kd_tree_radius{17.};
+};
+template <class problem_t>
+struct ContactsParams<contact_brute_force<problem_t>> {  // contact_brute_force.hpp:470-495
+    double dmax{2.};
+};
+
+struct VapParams {};
+struct vap_fixed {
+    static constexpr int32_t code = SCOPI_GPU_VAP_FIXED;
+    using params_t = VapParams;
+};
+struct vap_fpd {
+    static constexpr int32_t code = SCOPI_GPU_VAP_FPD;
+    using params_t = VapParams;
+};
+}  // namespace gpu
+
+// reference policy names
+using apgd_params = gpu::apgd_params;
+using apgd = gpu::apgd<gpu::fp64>;
+template <class Method>
+using OptimGradient = gpu::OptimGradient<Method>;
+template <class problem_t>
+using contact_kdtree = gpu::contact_kdtree<problem_t>;
+template <class problem_t>
+using contact_brute_force = gpu::contact_brute_force<problem_t>;
+template <class D>
+using ContactsParams = gpu::ContactsParams<D>;
+using vap_fixed = gpu::vap_fixed;
+using vap_fpd = gpu::vap_fpd;
+
+struct ScopiParams {  // params.hpp:89-134 (output is not produced by the GPU engine)
+    std::size_t output_frequency = std::size_t(-1);
+    std::filesystem::path path = "Results";
+    std::string filename = "scopi_objects";
+    bool write_velocity = false;
+    bool write_lagrange_multiplier = false;
+    bool binary_output = false;
+};
+
+template <class solver_t>
+struct Params {  // params.hpp:144-197
+    typename solver_t::optim_solver_t::params_t& optim_params;
+    contact_property<typename solver_t::problem_t>& default_contact_property;
+    typename solver_t::contact_params_t& contact_method_params;
+    typename solver_t::vap_t::params_t& vap_params;
+    ScopiParams& solver_params;
+};
+
+class gpu_error : public std::runtime_error {
+  public:
+    using std::runtime_error::runtime_error;
+};
+
+// ------------------------------------------------------------------ ScopiSolver
+template <std::size_t dim, class problem_type = NoFriction, class optim_solver_type = OptimGradient<apgd>,
+          template <class> class contact_method_type = contact_kdtree, class vap_type = vap_fixed>
+class ScopiSolver {
+  public:
+    using problem_t = problem_type;
+    using optim_solver_t = optim_solver_type;
+    using contact_method_t = contact_method_type<problem_t>;
+    using contact_params_t = gpu::ContactsParams<contact_method_t>;
+    using vap_t = vap_type;
+    using params_t = Params<ScopiSolver>;
+
+    explicit ScopiSolver(scopi_container<dim>& particles) : m_particles(particles) {}
+    ~ScopiSolver() {
+        if (m_h) scopi_gpu_destroy(m_h);
+    }
+    ScopiSolver(const ScopiSolver&) = delete;
+    ScopiSolver& operator=(const ScopiSolver&) = delete;
+
+    params_t get_params() {
+        return params_t{m_optim.get_params(), m_default_property, m_contact_params, m_vap_params, m_params};
+    }
+
+    // ScopiSolver::run (solver.hpp:267-303): the container is uploaded, the steps run on
+    // the GPU, and positions, quaternions and velocities are copied back.
+    void run(double dt, std::size_t total_it, std::size_t initial_iter = 0) {
+        ensure();
+        scopi_gpu_particles p = m_particles.abi();
+        check(scopi_gpu_set_particles(m_h, &p), "set_particles");
+        const int32_t rc = scopi_gpu_run(m_h, dt, (int64_t)total_it, (int64_t)initial_iter);
+        if (rc < 0) check(rc, "run");
+        if (rc == SCOPI_GPU_ENOCONV) std::cerr << "APGD didn't converge." << std::endl;
+        check(scopi_gpu_get_particles(m_h, &p), "get_particles");
+    }
+
+    // current_contacts (solver.hpp:314-317)
+    const std::vector<neighbor<dim, problem_t>>& current_contacts() {
+        ensure();
+        int64_t n = 0;
+        check(scopi_gpu_get_contacts(m_h, 0, &n, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr),
+              "get_contacts");
+        std::vector<int64_t> ci(n), cj(n);
+        std::vector<double> d(n), nij(3 * n), pi(3 * n), pj(3 * n), g(n);
+        check(scopi_gpu_get_contacts(m_h, n, &n, ci.data(), cj.data(), d.data(), nij.data(), pi.data(), pj.data(),
+                                     g.data()),
+              "get_contacts");
+        m_contacts.resize(n);
+        for (int64_t k = 0; k < n; ++k) {
+            auto& c = m_contacts[k];
+            c.i = (std::size_t)ci[k];
+            c.j = (std::size_t)cj[k];
+            c.dij = d[k];
+            for (std::size_t x = 0; x < dim; ++x) {
+                c.nij[x] = nij[3 * k + x];
+                c.pi[x] = pi[3 * k + x];
+                c.pj[x] = pj[3 * k + x];
+            }
+            if constexpr (std::is_same_v<problem_t, Viscous>) c.property.gamma = g[k];
+        }
+        return m_contacts;
+    }
+
+    std::vector<double> lagrange_multiplier() {
+        ensure();
+        int64_t n = 0;
+        check(scopi_gpu_get_lambda(m_h, 0, &n, nullptr), "get_lambda");
+        std::vector<double> out(n);
+        check(scopi_gpu_get_lambda(m_h, n, &n, out.data()), "get_lambda");
+        return out;
+    }
+
+    scopi_gpu_stats stats() {
+        scopi_gpu_stats s{};
+        if (m_h) scopi_gpu_get_stats(m_h, &s);
+        return s;
+    }
+
+  private:
+    void check(int32_t rc, const char* what) {
+        if (rc < 0) throw gpu_error(std::string("scopi_gpu_") + what + ": " + scopi_gpu_last_error(m_h));
+    }
+    void ensure() {
+        if (m_h) return;
+        scopi_gpu_params p;
+        scopi_gpu_default_params(&p, (int32_t)dim);
+        p.problem = problem_code<problem_t>();
+        p.vap = vap_t::code;
+        p.contact_method = contact_method_t::code;
+        p.precision = optim_solver_t::method_t::precision_t::code;
+        const auto& op = m_optim.get_params();
+        p.alpha = op.alpha;
+        p.max_ite = (int64_t)op.max_ite;
+        p.tolerance = op.tolerance;
+        p.dynamic_descent = op.dynamic_descent ? 1 : 0;
+        p.mixed_violation_tol = op.mixed_violation_tol;
+        p.mixed_max_corrections = op.mixed_max_corrections;
+        p.dmax = m_contact_params.dmax;
+        if constexpr (std::is_same_v<contact_method_t, gpu::contact_kdtree<problem_t>>)
+            p.kd_tree_radius = m_contact_params.kd_tree_radius;
+        if constexpr (std::is_same_v<problem_t, Friction>) p.mu = m_default_property.mu;
+        if constexpr (std::is_same_v<problem_t, Viscous>) {
+            p.gamma = m_default_property.gamma;
+            p.gamma_min = m_default_property.gamma_min;
+            p.gamma_tol = m_default_property.gamma_tol;
+        }
+        const int32_t rc = scopi_gpu_create(&p, &m_h);
+        if (rc < 0) throw gpu_error(std::string("scopi_gpu_create: ") + scopi_gpu_last_error(nullptr));
+    }
+
+    scopi_container<dim>& m_particles;
+    optim_solver_t m_optim;
+    contact_property<problem_t> m_default_property;
+    contact_params_t m_contact_params;
+    typename vap_t::params_t m_vap_params;
+    ScopiParams m_params;
+    std::vector<neighbor<dim, problem_t>> m_contacts;
+    scopi_gpu_handle* m_h = nullptr;
+};
+
+}  // namespace scopi
