@@ -155,6 +155,32 @@ const char* scopi_gpu_last_error(scopi_gpu_handle* h);
 /* Number of kernels this library launched on the handle's stream so far. */
 int64_t scopi_gpu_kernel_launches(scopi_gpu_handle* h);
 
+/* APGD solve of one normal-contact QP (NoFriction, FP64, torque-free rows: sphere, plane
+   and segment contacts) on caller-provided DEVICE arrays, allocating no device memory.
+   No counterpart in the reference (it solves on the host inside OptimGradient::run).
+   For callers that cannot allocate while they solve: a process whose device memory is
+   owned by another allocator, or a latency-critical loop where cudaMalloc/cudaFree would
+   synchronise the device.  Intermediate arrays live in a fixed device array inside this
+   library (about 3.5 MB, held by every GPU that loads the library until exit), so:
+     - limits: at most 16384 contacts and 8192 active bodies; larger sizes return
+       SCOPI_GPU_EINVAL with a message in scopi_gpu_last_error(NULL);
+     - the first call on a device looks up that array's device address (make that first
+       call before any stream capture);
+     - all calls share the array: calls that overlap on the GPU (other streams or host
+       threads) race; run them one after another.
+   Inputs: ci, cj (n_contacts body indices, obstacles < nb_inactive), normal (n_contacts*3,
+   outer normal of j, as scopi_gpu_get_contacts returns it), c (n_contacts linear term
+   n.(d n + dt A U)), inv_mass (n_active, 1/m), inc_ptr/inc_idx (per active body, its
+   contacts sorted by index, entry = contact | (1u<<31) when the body is the contact's j).
+   Outputs: lambda (n_contacts), u (n_active*3, M^-1 B^T lambda; may be NULL).
+   Returns SCOPI_GPU_OK, SCOPI_GPU_ENOCONV (max_ite reached) or an error; the call
+   synchronises `stream` (a cudaStream_t, NULL = legacy default stream). */
+int32_t scopi_gpu_apgd_noalloc(int32_t dim, int64_t n_active, int64_t nb_inactive, int64_t n_contacts,
+                               const int32_t* ci, const int32_t* cj, const double* normal, const double* c,
+                               const double* inv_mass, const int32_t* inc_ptr, const int32_t* inc_idx, double dt,
+                               double alpha, double tolerance, int64_t max_ite, int32_t dynamic_descent,
+                               double* lambda, double* u, int64_t* iterations, void* stream);
+
 /* The handle's CUDA stream (a cudaStream_t), so callers can order their own work and
    time the engine with CUDA events recorded on the stream its kernels run on.
    Infrastructure of this library; the reference has no device streams. */

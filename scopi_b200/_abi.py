@@ -21,7 +21,7 @@ EXPORTED = [
     "scopi_gpu_default_params", "scopi_gpu_create", "scopi_gpu_destroy", "scopi_gpu_set_particles",
     "scopi_gpu_get_particles", "scopi_gpu_run", "scopi_gpu_detect", "scopi_gpu_get_contacts",
     "scopi_gpu_get_lambda", "scopi_gpu_get_stats", "scopi_gpu_amat", "scopi_gpu_atmat",
-    "scopi_gpu_last_error", "scopi_gpu_kernel_launches", "scopi_gpu_get_stream",
+    "scopi_gpu_last_error", "scopi_gpu_kernel_launches", "scopi_gpu_get_stream", "scopi_gpu_apgd_noalloc",
 ]
 
 
@@ -87,6 +87,10 @@ def load(path: str = LIB_PATH):
     L.scopi_gpu_kernel_launches.restype = C.c_int64
     L.scopi_gpu_get_stream.argtypes = [H]
     L.scopi_gpu_get_stream.restype = C.c_void_p
+    P = C.c_void_p  # device pointers
+    L.scopi_gpu_apgd_noalloc.argtypes = [C.c_int32, C.c_int64, C.c_int64, C.c_int64, P, P, P, P, P, P, P, C.c_double,
+                                         C.c_double, C.c_double, C.c_int64, C.c_int32, P, P, I64, C.c_void_p]
+    L.scopi_gpu_apgd_noalloc.restype = C.c_int32
     for name in ("scopi_gpu_create", "scopi_gpu_destroy", "scopi_gpu_set_particles", "scopi_gpu_get_particles",
                  "scopi_gpu_run", "scopi_gpu_detect", "scopi_gpu_get_contacts", "scopi_gpu_get_lambda",
                  "scopi_gpu_get_stats", "scopi_gpu_amat", "scopi_gpu_atmat"):

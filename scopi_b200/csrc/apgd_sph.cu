@@ -11,6 +11,11 @@
 //   per incidence of a body: (+-n, contact index) in one record;
 //   per body    : u(y) gathered once (u(y_next) = u(l+) + beta (u(l+) - u(l)) is formed in
 //                 the particle pass, the restart test being reduced after the first barrier).
+#include <algorithm>
+#include <cstdio>
+#include <mutex>
+
+#include "../../include/scopi_gpu.h"
 #include "apgd_common.cuh"
 
 namespace scopi_gpu {
@@ -541,4 +546,219 @@ void launch_sph_residual64(int nin, int dim, int problem, const int2* cij, const
     g_sph_launches += 1;
 }
 
+// ------------------------------------------------------------------ entry point without allocation
+//
+// scopi_gpu_apgd_noalloc runs the FP64 torque-free APGD solve on caller-provided device
+// arrays and keeps every intermediate array (packed contact and incidence records, the
+// three multiplier buffers, the four per-body velocity buffers, block partials, the grid
+// barrier and the result word) in g_noalloc_scratch below instead of cudaMalloc'd memory.
+// Some callers cannot allocate device memory while they run the solve: a process whose
+// device memory is owned by another allocator (a caching pool that has claimed the
+// memory it will hand out), or a latency-critical loop where cudaMalloc / cudaFree would
+// synchronise the device and stall the other streams.  They pass inputs and outputs only.
+//
+// The array is a file-scope __device__ variable, so every GPU that loads this library
+// holds it (kNoAllocBytes, about 3.5 MB) until the process exits.  Its host-side name is
+// only a stand-in for the device address, so at set-up the device address is fetched once
+// per device with cudaGetSymbolAddress (with that device current) and passed to the
+// kernels.  All calls share the array and it keeps the last call's contents: each call
+// clears what must start at zero, and calls that overlap on the GPU (concurrent streams,
+// or several host threads) race on it.
+namespace {
+
+constexpr long long kNoAllocMaxContacts = 16384;
+constexpr long long kNoAllocMaxBodies = 8192;
+constexpr int kNoAllocMaxBlocks = 4 * kSMs;
+
+constexpr size_t kAlign = 256;
+constexpr size_t align_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
+constexpr size_t kOffCij = 0;
+constexpr size_t kOffNc = align_up(kOffCij + sizeof(int2) * kNoAllocMaxContacts);
+constexpr size_t kOffInc = align_up(kOffNc + sizeof(dvec4) * kNoAllocMaxContacts);
+constexpr size_t kOffInvm = align_up(kOffInc + sizeof(dvec4) * 2 * kNoAllocMaxContacts);
+constexpr size_t kOffLam = align_up(kOffInvm + sizeof(double) * 4 * kNoAllocMaxBodies);
+constexpr size_t kOffU = align_up(kOffLam + sizeof(double) * 3 * kNoAllocMaxContacts);
+constexpr size_t kOffPart = align_up(kOffU + sizeof(dvec4) * 4 * kNoAllocMaxBodies);
+constexpr size_t kOffBar = align_up(kOffPart + sizeof(double) * 4 * kNoAllocMaxBlocks * 8);
+constexpr size_t kOffRes = align_up(kOffBar + 4 * sizeof(unsigned int));
+constexpr size_t kOffSizes = align_up(kOffRes + sizeof(ApgdResult));
+constexpr size_t kNoAllocBytes = align_up(kOffSizes + sizeof(Sizes));
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kMaxDevices = 64;
+unsigned char* g_noalloc_dev[kMaxDevices] = {};
+std::mutex g_noalloc_mutex;
+
+// Device address of g_noalloc_scratch on the current device (set up on first use).
+cudaError_t noalloc_scratch(unsigned char** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_dev[dev]) {
+        void* ptr = nullptr;
+        e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_noalloc_dev[dev] = static_cast<unsigned char*>(ptr);
+    }
+    *out = g_noalloc_dev[dev];
+    return cudaSuccess;
+}
+
+__global__ void k_noalloc_prepare(Sizes* sizes, int C, int na, const double* inv_mass, double* invm4) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        sizes->C = C;
+        sizes->C_obs = 0;
+        sizes->n_extra = 0;
+        sizes->overflow = 0;
+    }
+    GRID_STRIDE(p, na) {
+        invm4[4 * p] = inv_mass[p];
+        invm4[4 * p + 1] = invm4[4 * p + 2] = invm4[4 * p + 3] = 0.0;
+    }
+}
+
+__global__ void k_noalloc_pack_nc(const double* normal, const double* cvec, dvec4* nc, int C) {
+    GRID_STRIDE(c, C) { nc[c] = dvec4{normal[3 * c], normal[3 * c + 1], normal[3 * c + 2], cvec[c]}; }
+}
+
+// copy the result buffers chosen by the solve (recorded in *res) to the caller's outputs
+__global__ void k_noalloc_output(const ApgdResult* res, const double* lam_base, const dvec4* u_base, int C, int na,
+                                 double* lambda, double* u) {
+    const double* lam = lam_base + (size_t)res->lam_buf * kNoAllocMaxContacts;
+    const dvec4* ub = u_base + (size_t)res->u_buf * kNoAllocMaxBodies;
+    GRID_STRIDE(k, C) { lambda[k] = lam[k]; }
+    if (u)
+        GRID_STRIDE(p, na) {
+            const dvec4 v = ld4(ub + p);
+            u[3 * p] = v.x;
+            u[3 * p + 1] = v.y;
+            u[3 * p + 2] = v.z;
+        }
+}
+
+}  // namespace
+
+void set_global_error(const char* msg);
+void set_global_error2(const char* a, const char* b);
+
 }  // namespace scopi_gpu
+
+extern "C" int32_t scopi_gpu_apgd_noalloc(int32_t dim, int64_t n_active, int64_t nb_inactive, int64_t n_contacts,
+                                          const int32_t* ci, const int32_t* cj, const double* normal,
+                                          const double* c, const double* inv_mass, const int32_t* inc_ptr,
+                                          const int32_t* inc_idx, double dt, double alpha, double tolerance,
+                                          int64_t max_ite, int32_t dynamic_descent, double* lambda, double* u,
+                                          int64_t* iterations, void* stream) {
+    using namespace scopi_gpu;
+    if (dim != 2 && dim != 3) {
+        set_global_error("scopi_gpu_apgd_noalloc: dim must be 2 or 3");
+        return SCOPI_GPU_EINVAL;
+    }
+    if (n_contacts < 0 || n_contacts > kNoAllocMaxContacts || n_active < 0 || n_active > kNoAllocMaxBodies ||
+        nb_inactive < 0) {
+        set_global_error("scopi_gpu_apgd_noalloc: size beyond the no-allocation limits (at most 16384 contacts and "
+                         "8192 active bodies)");
+        return SCOPI_GPU_EINVAL;
+    }
+    if (n_contacts > 0 && (!ci || !cj || !normal || !c || !inv_mass || !inc_ptr || !inc_idx || !lambda)) {
+        set_global_error("scopi_gpu_apgd_noalloc: null array");
+        return SCOPI_GPU_EINVAL;
+    }
+    if (!(alpha > 0) || max_ite < 1) {
+        set_global_error("scopi_gpu_apgd_noalloc: alpha must be > 0 and max_ite >= 1");
+        return SCOPI_GPU_EINVAL;
+    }
+    if (iterations) *iterations = 0;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (n_contacts == 0) {
+        if (u && n_active > 0) {
+            cudaError_t e = cudaMemsetAsync(u, 0, 3 * (size_t)n_active * sizeof(double), s);
+            if (e != cudaSuccess) {
+                set_global_error(cudaGetErrorString(e));
+                return SCOPI_GPU_ECUDA;
+            }
+        }
+        return SCOPI_GPU_OK;
+    }
+    unsigned char* base = nullptr;
+    cudaError_t e = noalloc_scratch(&base);
+    if (e != cudaSuccess) {
+        set_global_error2("scopi_gpu_apgd_noalloc: cudaGetSymbolAddress: ", cudaGetErrorString(e));
+        return SCOPI_GPU_ECUDA;
+    }
+    const int C = (int)n_contacts, na = (int)n_active;
+    int2* cij = reinterpret_cast<int2*>(base + kOffCij);
+    dvec4* nc = reinterpret_cast<dvec4*>(base + kOffNc);
+    dvec4* inc = reinterpret_cast<dvec4*>(base + kOffInc);
+    double* invm4 = reinterpret_cast<double*>(base + kOffInvm);
+    double* lam = reinterpret_cast<double*>(base + kOffLam);
+    dvec4* ub = reinterpret_cast<dvec4*>(base + kOffU);
+    double* part = reinterpret_cast<double*>(base + kOffPart);
+    unsigned int* bar = reinterpret_cast<unsigned int*>(base + kOffBar);
+    ApgdResult* res = reinterpret_cast<ApgdResult*>(base + kOffRes);
+    Sizes* sizes = reinterpret_cast<Sizes*>(base + kOffSizes);
+    // the array keeps the previous call's contents: clear what the solve reads before writing
+    cudaMemsetAsync(lam, 0, 2 * sizeof(double) * kNoAllocMaxContacts, s);     // lambda, lambda_prev
+    cudaMemsetAsync(ub, 0, sizeof(dvec4) * kNoAllocMaxBodies, s);             // u(lambda)
+    cudaMemsetAsync(ub + 2 * kNoAllocMaxBodies, 0, sizeof(dvec4) * kNoAllocMaxBodies, s);  // u(y)
+    cudaMemsetAsync(bar, 0, 4 * sizeof(unsigned int), s);
+    cudaMemsetAsync(res, 0, sizeof(ApgdResult), s);
+    k_noalloc_prepare<<<blocks(na), 256, 0, s>>>(sizes, C, na, inv_mass, invm4);
+    launch_pack_cij(ci, cj, cij, sizes, C, s);
+    k_noalloc_pack_nc<<<blocks(C), 256, 0, s>>>(normal, c, nc, C);
+    launch_pack_inc<double>(na, inc_ptr, inc_idx, normal, inc, 2 * (long long)C, s);
+    SphArgs<double> A;
+    A.nin = (int)nb_inactive;
+    A.na = na;
+    A.cij = cij;
+    A.nc = nc;
+    A.slot = nullptr;
+    A.shift = nullptr;
+    A.inc_ptr = inc_ptr;
+    A.inc = inc;
+    A.invm = invm4;
+    A.lam0 = lam;
+    A.lam1 = lam + kNoAllocMaxContacts;
+    A.lam2 = lam + 2 * kNoAllocMaxContacts;
+    A.u0 = ub;
+    A.u1 = ub + kNoAllocMaxBodies;
+    A.u2 = ub + 2 * kNoAllocMaxBodies;
+    A.u3 = ub + 3 * kNoAllocMaxBodies;
+    A.partials = part;
+    A.bar = bar;
+    A.result = res;
+    A.sizes = sizes;
+    A.alpha = alpha;
+    A.tol = tolerance;
+    A.dt2 = dt * dt;
+    A.max_ite = max_ite;
+    A.dynamic = dynamic_descent ? 1 : 0;
+    int maxb = apgd_sph_max_blocks(kNoFriction, dim, false);
+    if (maxb > kNoAllocMaxBlocks) maxb = kNoAllocMaxBlocks;
+    long long nb = (std::max<long long>(C, na) + 255) / 256;
+    if (nb < 1) nb = 1;
+    if (nb > maxb) nb = maxb;
+    e = dim == 3 ? launch_t<double, 3, kNoFriction>(A, (int)nb, s) : launch_t<double, 2, kNoFriction>(A, (int)nb, s);
+    if (e != cudaSuccess) {
+        set_global_error2("scopi_gpu_apgd_noalloc: launch: ", cudaGetErrorString(e));
+        return SCOPI_GPU_ECUDA;
+    }
+    k_noalloc_output<<<blocks(std::max(C, na)), 256, 0, s>>>(res, lam, ub, C, na, lambda, u);
+    ApgdResult host_res;
+    e = cudaMemcpyAsync(&host_res, res, sizeof(ApgdResult), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        set_global_error2("scopi_gpu_apgd_noalloc: ", cudaGetErrorString(e));
+        return SCOPI_GPU_ECUDA;
+    }
+    if (iterations) *iterations = host_res.iterations;
+    if (host_res.error) {
+        set_global_error("scopi_gpu_apgd_noalloc: APGD grid barrier timed out");
+        return SCOPI_GPU_ETIMEOUT;
+    }
+    return host_res.converged ? SCOPI_GPU_OK : SCOPI_GPU_ENOCONV;
+}
+

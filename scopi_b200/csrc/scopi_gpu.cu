@@ -16,7 +16,8 @@ using namespace scopi_gpu;
 
 namespace {
 
-thread_local std::string g_create_error;
+// message of the last failing call that has no handle (fixed buffer: setting it allocates nothing)
+thread_local char g_global_error[512] = "";
 
 struct DevMem {
     std::vector<void*> ptrs;
@@ -28,6 +29,14 @@ struct DevMem {
 };
 
 }  // namespace
+
+namespace scopi_gpu {
+// Message returned by scopi_gpu_last_error(NULL) for calls that have no handle.
+void set_global_error(const char* msg) { std::snprintf(g_global_error, sizeof(g_global_error), "%s", msg ? msg : ""); }
+void set_global_error2(const char* a, const char* b) {
+    std::snprintf(g_global_error, sizeof(g_global_error), "%s%s", a ? a : "", b ? b : "");
+}
+}  // namespace scopi_gpu
 
 struct scopi_gpu_handle {
     scopi_gpu_params P{};
@@ -638,23 +647,23 @@ void scopi_gpu_default_params(scopi_gpu_params* p, int32_t dim) {
 
 int32_t scopi_gpu_create(const scopi_gpu_params* p, scopi_gpu_handle** out) {
     if (!p || !out) {
-        g_create_error = "null argument";
+        scopi_gpu::set_global_error("null argument");
         return SCOPI_GPU_EINVAL;
     }
     *out = nullptr;
     if (p->dim != 2 && p->dim != 3) {
-        g_create_error = "dim must be 2 or 3";
+        scopi_gpu::set_global_error("dim must be 2 or 3");
         return SCOPI_GPU_EINVAL;
     }
     if (p->problem < 0 || p->problem > 2 || p->vap < 0 || p->vap > 1 || p->contact_method < 0 ||
         p->contact_method > 1 || p->precision < 0 || p->precision > 1 || p->alpha <= 0 || p->max_ite < 1) {
-        g_create_error = "invalid parameter";
+        scopi_gpu::set_global_error("invalid parameter");
         return SCOPI_GPU_EINVAL;
     }
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);
     if (e != cudaSuccess || ndev <= p->device) {
-        g_create_error = std::string("no CUDA device: ") + cudaGetErrorString(e);
+        scopi_gpu::set_global_error2("no CUDA device: ", cudaGetErrorString(e));
         return SCOPI_GPU_ECUDA;
     }
     auto* h = new scopi_gpu_handle();
@@ -662,13 +671,13 @@ int32_t scopi_gpu_create(const scopi_gpu_params* p, scopi_gpu_handle** out) {
     h->dev = p->device;
     cudaSetDevice(h->dev);
     if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess) {
-        g_create_error = std::string("cudaStreamCreate: ") + cudaGetErrorString(e);
+        scopi_gpu::set_global_error2("cudaStreamCreate: ", cudaGetErrorString(e));
         delete h;
         return SCOPI_GPU_ECUDA;
     }
     int rc = h->alloc_fixed();
     if (rc) {
-        g_create_error = h->err;
+        scopi_gpu::set_global_error(h->err.c_str());
         scopi_gpu_destroy(h);
         return rc;
     }
@@ -886,7 +895,7 @@ int32_t scopi_gpu_atmat(scopi_gpu_handle* h, const double* f, double* out) {
     return 0;
 }
 
-const char* scopi_gpu_last_error(scopi_gpu_handle* h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+const char* scopi_gpu_last_error(scopi_gpu_handle* h) { return h ? h->err.c_str() : g_global_error; }
 
 int64_t scopi_gpu_kernel_launches(scopi_gpu_handle* h) { return h ? h->launches() - h->launches0 : 0; }
 
