@@ -53,12 +53,13 @@ __device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int nbl
     return s_ok != 0;
 }
 
-// Fixed-order sum of NP doubles over the block; the result is returned in every thread.
+// Fixed-order sum of NP doubles over the block (up to 1024 threads); the result is
+// returned in every thread.
 template <int NP>
 __device__ __forceinline__ void block_sum(double* v) {
-    __shared__ double sh[kThreadsA / 32][NP];
+    __shared__ double sh[32][NP];
     __shared__ double tot[NP];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
     for (int k = 0; k < NP; ++k) {
         double x = v[k];
@@ -69,7 +70,7 @@ __device__ __forceinline__ void block_sum(double* v) {
     __syncthreads();
     if (threadIdx.x < NP) {
         double s = 0.0;
-        for (int w = 0; w < kThreadsA / 32; ++w) s += sh[w][threadIdx.x];
+        for (int w = 0; w < nw; ++w) s += sh[w][threadIdx.x];
         tot[threadIdx.x] = s;
     }
     __syncthreads();

@@ -118,14 +118,16 @@ struct SphState {
     int il, ip, in_, jL, jN, jY, jYN, parity, bt, use_prev, restart, done, conv, err;
 };
 
-// FP32: 64 registers (4 blocks/SM, no spills); FP64: 80 registers (3 blocks/SM).
+// One block per SM: 1024 threads at 64 registers (FP32), 768 at 80 (FP64).  Fewer,
+// larger blocks cut the grid-barrier arrivals and the per-block partials that every
+// block re-reads after each barrier (148 instead of 592).
 template <typename T>
 struct SphOcc {
-    static constexpr int blocks = sizeof(T) == 4 ? 4 : 3;
+    static constexpr int threads = sizeof(T) == 4 ? 1024 : 768;
 };
 
 template <typename T, int DIM, int PROB>
-__global__ void __launch_bounds__(kThreadsA, SphOcc<T>::blocks) k_apgd_sph(SphArgs<T> A) {
+__global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A) {
     __shared__ SphState S;
     if (threadIdx.x == 0) {
         S.alpha = A.alpha;
@@ -427,7 +429,7 @@ int blocks(long long n) {
 template <typename T, int DIM, int PROB>
 int max_blocks_sph() {
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_apgd_sph<T, DIM, PROB>, kThreadsA, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_apgd_sph<T, DIM, PROB>, SphOcc<T>::threads, 0);
     int dev = 0, sms = kSMs;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -438,7 +440,7 @@ template <typename T, int DIM, int PROB>
 cudaError_t launch_t(SphArgs<T>& A, int nblocks, cudaStream_t s) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(nblocks);
-    cfg.blockDim = dim3(kThreadsA);
+    cfg.blockDim = dim3(SphOcc<T>::threads);
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;
@@ -450,6 +452,8 @@ cudaError_t launch_t(SphArgs<T>& A, int nblocks, cudaStream_t s) {
 }
 
 }  // namespace
+
+int apgd_sph_threads(bool fp32) { return fp32 ? SphOcc<float>::threads : SphOcc<double>::threads; }
 
 int apgd_sph_max_blocks(int problem, int dim, bool fp32) {
 #define MB(T, D, P) \
@@ -738,7 +742,8 @@ extern "C" int32_t scopi_gpu_apgd_noalloc(int32_t dim, int64_t n_active, int64_t
     A.dynamic = dynamic_descent ? 1 : 0;
     int maxb = apgd_sph_max_blocks(kNoFriction, dim, false);
     if (maxb > kNoAllocMaxBlocks) maxb = kNoAllocMaxBlocks;
-    long long nb = (std::max<long long>(C, na) + 255) / 256;
+    const int thr = SphOcc<double>::threads;
+    long long nb = (std::max<long long>(C, na) + thr - 1) / thr;
     if (nb < 1) nb = 1;
     if (nb > maxb) nb = maxb;
     e = dim == 3 ? launch_t<double, 3, kNoFriction>(A, (int)nb, s) : launch_t<double, 2, kNoFriction>(A, (int)nb, s);

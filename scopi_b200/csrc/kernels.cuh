@@ -184,6 +184,7 @@ struct SphSolve {
 
 long long apgd_sph_launches();
 int apgd_sph_max_blocks(int problem, int dim, bool fp32);
+int apgd_sph_threads(bool fp32);  // threads per block of the torque-free kernel
 template <typename T>
 cudaError_t launch_apgd_sph(int nin, int na, int dim, int problem, const ApgdSettings& st, SphSolve<T>& sb,
                             const Sizes* sizes, int nblocks, cudaStream_t s);

@@ -338,8 +338,8 @@ struct scopi_gpu_handle {
         return 0;
     }
 
-    int nblocks_for(int maxb, long long work) const {
-        long long b = (work + 255) / 256;
+    int nblocks_for(int maxb, long long work, int threads = 256) const {
+        long long b = (work + threads - 1) / threads;
         b = std::max<long long>(b, 1);
         return (int)std::min<long long>(b, maxb);
     }
@@ -385,7 +385,7 @@ struct scopi_gpu_handle {
         cudaMemsetAsync(sb.u[0], 0, (size_t)na * sizeof(V4<T>), stream);
         cudaMemsetAsync(sb.u[2], 0, (size_t)na * sizeof(V4<T>), stream);
         cudaMemsetAsync(d_barrier, 0, 4 * sizeof(unsigned int), stream);
-        const int nb = nblocks_for(maxb, std::max<long long>(h_sizes->C, na));
+        const int nb = nblocks_for(maxb, std::max<long long>(h_sizes->C, na), apgd_sph_threads(sizeof(T) == 4));
         cudaError_t e = launch_apgd_sph<T>(nin, na, P.dim, P.problem, st, sb, d_sizes_cur, nb, stream);
         if (e != cudaSuccess) return cuda_fail(e, "APGD launch");
         cudaMemcpyAsync(h_result, d_result, sizeof(ApgdResult), cudaMemcpyDeviceToHost, stream);
