@@ -155,6 +155,37 @@ const char* scopi_gpu_last_error(scopi_gpu_handle* h);
 /* Number of kernels this library launched on the handle's stream so far. */
 int64_t scopi_gpu_kernel_launches(scopi_gpu_handle* h);
 
+/* ---- batches of independent scenes (one ScopiSolver per scene in the reference) ----
+   scopi_gpu_batch_create concatenates n_scenes containers (each obstacles first) into one
+   handle; scopi_gpu_run(h, dt, k, 0) then advances every scene k steps, one CUDA graph
+   replay per step: contact detection keeps scenes apart, and one persistent launch solves
+   all scenes (one CTA per scene, each iterating until its own stopping test holds; the
+   mixed precision form corrects each scene in FP64 inside the same launch).  The block
+   size of that launch is chosen on the first step by timing 256, 512 and 1024 threads.
+   NoFriction only.  scopi_gpu_get_stats reports the worst scene (iterations, violation). */
+typedef struct scopi_gpu_scene_stats {
+    int64_t contacts;
+    int64_t iterations;
+    int64_t fp32_iterations;
+    int64_t backtracks;
+    int64_t restarts;
+    int32_t corrections;
+    int32_t converged;
+    double violation;
+} scopi_gpu_scene_stats;
+
+int32_t scopi_gpu_batch_create(const scopi_gpu_params* p, int32_t n_scenes, const scopi_gpu_particles* scenes,
+                               scopi_gpu_handle** out);
+/* pos/q/v/omega of one scene, in that scene's own body order (obstacles first). */
+int32_t scopi_gpu_batch_get_scene(scopi_gpu_handle* h, int32_t scene, scopi_gpu_particles* out);
+/* statistics of one scene for the last step */
+int32_t scopi_gpu_batch_get_scene_stats(scopi_gpu_handle* h, int32_t scene, scopi_gpu_scene_stats* out);
+/* block size chosen by the autotuner (0 before the first step) */
+int32_t scopi_gpu_batch_block_threads(scopi_gpu_handle* h);
+/* pin the block size per scene (256, 512 or 1024) instead of autotuning it on the first
+   step; 0 restores autotuning.  Only before the first step (else SCOPI_GPU_EINVAL). */
+int32_t scopi_gpu_batch_set_block_threads(scopi_gpu_handle* h, int32_t threads);
+
 /* APGD solve of one normal-contact QP (NoFriction, FP64, torque-free rows: sphere, plane
    and segment contacts) on caller-provided DEVICE arrays, allocating no device memory.
    No counterpart in the reference (it solves on the host inside OptimGradient::run).

@@ -6,4 +6,4 @@ particle container) and seeded synthetic workloads.
 """
 from .container import PLANE, SEGMENT, SPHERE, ParticleArrays, Particles, Property, quaternion  # noqa: F401
 from .solver import (BRUTE_FORCE, FP64, FRICTION, KDTREE, MIXED, NOFRICTION, VAP_FIXED, VAP_FPD,  # noqa: F401
-                     VISCOUS, ScopiGPUError, ScopiSolver)
+                     VISCOUS, ScopiBatch, ScopiGPUError, ScopiSolver)

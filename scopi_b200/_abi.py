@@ -22,6 +22,8 @@ EXPORTED = [
     "scopi_gpu_get_particles", "scopi_gpu_run", "scopi_gpu_detect", "scopi_gpu_get_contacts",
     "scopi_gpu_get_lambda", "scopi_gpu_get_stats", "scopi_gpu_amat", "scopi_gpu_atmat",
     "scopi_gpu_last_error", "scopi_gpu_kernel_launches", "scopi_gpu_get_stream", "scopi_gpu_apgd_noalloc",
+    "scopi_gpu_batch_create", "scopi_gpu_batch_get_scene", "scopi_gpu_batch_get_scene_stats",
+    "scopi_gpu_batch_block_threads", "scopi_gpu_batch_set_block_threads",
 ]
 
 
@@ -51,6 +53,13 @@ class Stats(C.Structure):
         ("fp32_iterations", C.c_int64), ("corrections", C.c_int64), ("converged", C.c_int32),
         ("status", C.c_int32), ("violation", C.c_double), ("ms_step", C.c_double), ("ms_solve", C.c_double),
         ("ms_apgd_kernel", C.c_double), ("steps", C.c_int64),
+    ]
+
+
+class SceneStats(C.Structure):
+    _fields_ = [
+        ("contacts", C.c_int64), ("iterations", C.c_int64), ("fp32_iterations", C.c_int64), ("backtracks", C.c_int64),
+        ("restarts", C.c_int64), ("corrections", C.c_int32), ("converged", C.c_int32), ("violation", C.c_double),
     ]
 
 
@@ -91,6 +100,16 @@ def load(path: str = LIB_PATH):
     L.scopi_gpu_apgd_noalloc.argtypes = [C.c_int32, C.c_int64, C.c_int64, C.c_int64, P, P, P, P, P, P, P, C.c_double,
                                          C.c_double, C.c_double, C.c_int64, C.c_int32, P, P, I64, C.c_void_p]
     L.scopi_gpu_apgd_noalloc.restype = C.c_int32
+    L.scopi_gpu_batch_create.argtypes = [C.POINTER(Params), C.c_int32, C.POINTER(ParticlesC), C.POINTER(H)]
+    L.scopi_gpu_batch_create.restype = C.c_int32
+    L.scopi_gpu_batch_get_scene.argtypes = [H, C.c_int32, C.POINTER(ParticlesC)]
+    L.scopi_gpu_batch_get_scene.restype = C.c_int32
+    L.scopi_gpu_batch_get_scene_stats.argtypes = [H, C.c_int32, C.POINTER(SceneStats)]
+    L.scopi_gpu_batch_get_scene_stats.restype = C.c_int32
+    L.scopi_gpu_batch_block_threads.argtypes = [H]
+    L.scopi_gpu_batch_block_threads.restype = C.c_int32
+    L.scopi_gpu_batch_set_block_threads.argtypes = [H, C.c_int32]
+    L.scopi_gpu_batch_set_block_threads.restype = C.c_int32
     for name in ("scopi_gpu_create", "scopi_gpu_destroy", "scopi_gpu_set_particles", "scopi_gpu_get_particles",
                  "scopi_gpu_run", "scopi_gpu_detect", "scopi_gpu_get_contacts", "scopi_gpu_get_lambda",
                  "scopi_gpu_get_stats", "scopi_gpu_amat", "scopi_gpu_atmat"):

@@ -20,6 +20,7 @@ SOURCES = {
     "detect.cu": ["-fmad=false"],
     "apgd.cu": [],
     "apgd_sph.cu": [],
+    "apgd_batch.cu": [],
     "scan.cu": [],
     "scopi_gpu.cu": [],
 }

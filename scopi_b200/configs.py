@@ -10,6 +10,10 @@ Workloads (shapes and distributions of the benchmark configurations):
   box_3d          spheres on a jittered 47^3 lattice (spacing 0.0115, jitter +-0.0005),
                   radius U[0.9,1.1]*0.005, m=(r/0.005)^3, J=0.4 m r^2, gravity -9.81 m in z,
                   six fixed planes bounding the unit box.
+  pile_scenes     independent 2D scenes for the batched solve: N_s = round(exp(U[ln 200, ln 5000]))
+                  disks, radius U[0.008,0.012], random sequential non-overlapping placement in
+                  [0,W] x [0.02, 0.02+H], W = H = 0.04 sqrt(N_s), a fixed segment (0,0)-(W,0)
+                  below, m = (r/0.01)^2, J = m r^2 / 2, gravity -9.81 m.
   spheres_1m      100^3 spheres on a jittered lattice (spacing 0.0045, jitter +-0.0002) centred
                   in the unit box, radius U[0.9,1.1]*0.002, desired velocity 0.1 (c-x)/|c-x|,
                   m=(r/0.002)^3, J=0.4 m r^2, six plane walls.
@@ -144,9 +148,58 @@ def spheres_1m(seed: int = 5, side: int = 100) -> ParticleArrays:
     return _assemble(3, c, r, m, jm, vd=vd)
 
 
+def pile_scene(seed: int, nmin: int = 200, nmax: int = 5000) -> ParticleArrays:
+    """One pile scene.  Draws: u[0] -> N_s; candidate k uses (x, y, r) = u[1+3k], u[2+3k], u[3+3k]."""
+    from .container import Particles, Property
+    n_draw = 1 + 3 * 16 * nmax
+    u = splitmix_uniform(seed, n_draw)
+    n = int(round(math.exp(math.log(nmin) + u[0] * (math.log(nmax) - math.log(nmin)))))
+    W = H = 0.04 * math.sqrt(n)
+    cell = 0.025
+    grid = {}
+    placed = []
+    k = 0
+    while len(placed) < n:
+        if 3 + 3 * k >= len(u):
+            u = splitmix_uniform(seed, 2 * len(u))
+            if k > 400 * n:
+                break
+        x = u[1 + 3 * k] * W
+        y = 0.02 + u[2 + 3 * k] * H
+        r = 0.008 + 0.004 * u[3 + 3 * k]
+        k += 1
+        ci, cj = int(x // cell), int(y // cell)
+        ok = True
+        for a in (ci - 1, ci, ci + 1):
+            for b in (cj - 1, cj, cj + 1):
+                for (px, py, pr) in grid.get((a, b), ()):
+                    if (px - x) ** 2 + (py - y) ** 2 < (pr + r) ** 2:
+                        ok = False
+                        break
+                if not ok:
+                    break
+            if not ok:
+                break
+        if ok:
+            placed.append((x, y, r))
+            grid.setdefault((ci, cj), []).append((x, y, r))
+    p = Particles(2)
+    p.add_segment((0.0, 0.0), (W, 0.0))
+    for x, y, r in placed:
+        m = (r / 0.01) ** 2
+        p.add_sphere((x, y), r, Property(mass=m, moment_inertia=0.5 * m * r * r, force=(0.0, -9.81 * m)))
+    return p.finalize()
+
+
+def pile_scenes(n_scenes: int = 256, seed: int = 4, nmin: int = 200, nmax: int = 5000):
+    """The batched workload: scene s is pile_scene(seed * 1000 + s)."""
+    return [pile_scene(seed * 1000 + s, nmin, nmax) for s in range(n_scenes)]
+
+
 # solver settings per workload (dmax, dt, tolerance, max_ite, vap)
 SETTINGS = {
     "disks_2d": dict(dmax=0.01, dt=0.005, tolerance=1e-6, max_ite=40000, vap=0, steps=200),
     "box_3d": dict(dmax=0.0045, dt=1e-3, tolerance=1e-6, max_ite=40000, vap=1, steps=500),
     "spheres_1m": dict(dmax=0.0018, dt=1e-3, tolerance=1e-6, max_ite=40000, vap=0, steps=100),
+    "pile_scenes": dict(dmax=0.009, dt=1e-3, tolerance=1e-6, max_ite=40000, vap=1, steps=1000),
 }

@@ -24,7 +24,19 @@ struct Bodies {
     const double* j;    // n*3
     const double* radius;
     const double* length;
+    // Batches of independent scenes (null for one scene): scene of each body, an x shift
+    // per scene applied to the cell keys only (scenes occupy disjoint cell ranges), and
+    // per obstacle the active range it can touch (obs_a0: first active index, obs_off:
+    // prefix offsets of the per-obstacle ranges, nin + 1 entries).
+    const int* scene = nullptr;
+    const double* scene_shift = nullptr;
+    const int* obs_a0 = nullptr;
+    const int* obs_off = nullptr;
 };
+
+__host__ __device__ inline double key_x(const Bodies& B, long long b, double x) {
+    return B.scene_shift ? x + B.scene_shift[B.scene[b]] : x;
+}
 
 // Device-resident sizes written by the detection kernels (graph friendly: no host sizes).
 struct Sizes {

@@ -231,7 +231,8 @@ __global__ void k_obstacles_move(Bodies B, double dt, int dim) {
 
 // vap_fixed::set_a_priori_velocity_impl (vap_fixed.hpp:45-55), vap_fpd (vap_fpd.hpp:69-81,
 // src/vap/vap_fpd.cpp:6-26)
-__global__ void k_vap(Bodies B, StepParams p) {
+__global__ void k_vap(Bodies B, StepParams p, const Sizes* sizes) {
+    if (sizes && sizes->overflow) return;  // the step is redone after the buffers grow
     GRID_STRIDE(k, B.n - B.nin) {
         const long long b = B.nin + k;
         if (p.vap == 0) {
@@ -258,8 +259,9 @@ __global__ void k_bbox_partial(Bodies B, int dim, double* partial) {
     GRID_STRIDE(k, B.n - B.nin) {
         const long long b = B.nin + k;
         for (int d = 0; d < dim; ++d) {
-            v[d] = fmin(v[d], B.pos[3 * b + d]);
-            v[3 + d] = fmax(v[3 + d], B.pos[3 * b + d]);
+            const double x = d == 0 ? key_x(B, b, B.pos[3 * b]) : B.pos[3 * b + d];
+            v[d] = fmin(v[d], x);
+            v[3 + d] = fmax(v[3 + d], x);
         }
         v[6] = fmax(v[6], B.radius[b]);
     }
@@ -337,7 +339,10 @@ __global__ void k_cell_assign(Bodies B, int dim, const Grid* grid, int* cell_of,
     GRID_STRIDE(k, B.n - B.nin) {
         const long long b = B.nin + k;
         int id = 0;
-        for (int d = dim - 1; d >= 0; --d) id = id * g.nc[d] + cell_coord(B.pos[3 * b + d], g.lo[d], g.h, g.nc[d]);
+        for (int d = dim - 1; d >= 0; --d) {
+            const double x = d == 0 ? key_x(B, b, B.pos[3 * b]) : B.pos[3 * b + d];
+            id = id * g.nc[d] + cell_coord(x, g.lo[d], g.h, g.nc[d]);
+        }
         cell_of[k] = id;
         atomicAdd(&cell_count[id], 1);
     }
@@ -384,6 +389,7 @@ __device__ __forceinline__ void for_each_pair(const Bodies& B, const StepParams&
                 for (int t = cell_start[cid]; t < t1; ++t) {
                     const int b = cell_body[t];
                     if (b <= a) continue;
+                    if (B.scene && B.scene[a] != B.scene[b]) continue;
                     const double4 Bb = cell_pr[t];
                     const double xb[3] = {Bb.x, Bb.y, Bb.z};
                     double s2 = 0.0;
@@ -449,24 +455,45 @@ __global__ void k_row_sort(int na, const int* row_ptr, const Sizes* sizes, long 
     }
 }
 
-__global__ void k_obs_flags(Bodies B, StepParams p, int* flag) {
-    const long long na = B.n - B.nin;
-    GRID_STRIDE(k, (long long)B.nin * na) {
-        const int o = (int)(k / na);
-        const int b = B.nin + (int)(k % na);
+// (obstacle, active) pair of flag slot k: every active for one scene, the obstacle's own
+// scene's actives in a batch (rows stay sorted by (obstacle, active))
+__device__ __forceinline__ void obs_pair(const Bodies& B, long long k, int& o, int& b) {
+    if (!B.obs_off) {
+        const long long na = B.n - B.nin;
+        o = (int)(k / na);
+        b = B.nin + (int)(k % na);
+        return;
+    }
+    int lo = 0, hi = B.nin;  // last o with obs_off[o] <= k
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (B.obs_off[mid] <= k)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    o = lo;
+    b = B.nin + B.obs_a0[o] + (int)(k - B.obs_off[o]);
+}
+
+__global__ void k_obs_flags(Bodies B, StepParams p, long long nobs, int* flag) {
+    GRID_STRIDE(k, nobs) {
+        int o, b;
+        obs_pair(B, k, o, b);
         PairGeom g;
         flag[k] = (exact_pair(B, p.dim, o, b, g) && g.dij < p.dmax) ? 1 : 0;
     }
 }
 
-__global__ void k_obs_fill(Bodies B, const int* flag, const int* pos, long long cap, int* ci, int* cj) {
-    const long long na = B.n - B.nin;
-    GRID_STRIDE(k, (long long)B.nin * na) {
+__global__ void k_obs_fill(Bodies B, long long nobs, const int* flag, const int* pos, long long cap, int* ci, int* cj) {
+    GRID_STRIDE(k, nobs) {
         if (!flag[k]) continue;
         const long long at = pos[k];
         if (at < cap) {
-            ci[at] = (int)(k / na);
-            cj[at] = B.nin + (int)(k % na);
+            int o, b;
+            obs_pair(B, k, o, b);
+            ci[at] = o;
+            cj[at] = b;
         }
     }
 }
@@ -662,6 +689,7 @@ __global__ void k_gamma_update(StepParams p, Contacts c, Assembly a, const doubl
 // OptimGradient::run velocity recovery (OptimGradient.hpp:265-284), update_velocity
 // (solver.hpp:528-546) and move_active_particles (solver.hpp:441-480).
 __global__ void k_update(Bodies B, StepParams p, const double* u, int ustride, int urot, const Sizes* sizes) {
+    if (sizes && sizes->overflow) return;  // the step is redone after the buffers grow
     const bool has = (u != nullptr) && (sizes == nullptr || sizes->C > 0);
     GRID_STRIDE(k, B.n - B.nin) {
         const long long b = B.nin + k;
@@ -769,9 +797,9 @@ void launch_obstacles_move(const Bodies& b, double dt, int dim, cudaStream_t s) 
     LAUNCHED(1);
 }
 
-void launch_vap(const Bodies& b, const StepParams& p, cudaStream_t s) {
+void launch_vap(const Bodies& b, const StepParams& p, cudaStream_t s, const Sizes* sizes) {
     if (b.n - b.nin <= 0) return;
-    k_vap<<<blocks_for(b.n - b.nin), kThreads, 0, s>>>(b, p);
+    k_vap<<<blocks_for(b.n - b.nin), kThreads, 0, s>>>(b, p, sizes);
     LAUNCHED(1);
 }
 
@@ -796,9 +824,9 @@ void launch_detect(const Bodies& b, const StepParams& p, DetectWork& w, Contacts
         LAUNCHED(3);
     }
     // obstacle rows come first in (i, j) order
-    const long long nobs = (long long)b.nin * na;
+    const long long nobs = w.obs_cap;  // nin * na, or the sum of the per-obstacle ranges of a batch
     if (nobs > 0) {
-        k_obs_flags<<<blocks_for(nobs), kThreads, 0, s>>>(b, p, w.obs_flag);
+        k_obs_flags<<<blocks_for(nobs), kThreads, 0, s>>>(b, p, nobs, w.obs_flag);
         scan_exclusive(w.obs_flag, w.obs_pos, nullptr, (int)nobs, nobs, w.tmp_total + 0, w.scan_work, s,
                        &g_detect_launches);
         LAUNCHED(1);
@@ -813,7 +841,7 @@ void launch_detect(const Bodies& b, const StepParams& p, DetectWork& w, Contacts
     k_sizes<<<1, 1, 0, s>>>(w.tmp_total, sizes, c_cap);
     LAUNCHED(1);
     if (nobs > 0) {
-        k_obs_fill<<<blocks_for(nobs), kThreads, 0, s>>>(b, w.obs_flag, w.obs_pos, c_cap, out.ci, out.cj);
+        k_obs_fill<<<blocks_for(nobs), kThreads, 0, s>>>(b, nobs, w.obs_flag, w.obs_pos, c_cap, out.ci, out.cj);
         LAUNCHED(1);
     }
     if (na > 0) {

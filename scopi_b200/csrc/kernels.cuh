@@ -64,7 +64,7 @@ struct Incidence {            // particle-major transpose of the contact list
 
 long long detect_launches();
 void launch_obstacles_move(const Bodies& b, double dt, int dim, cudaStream_t s);
-void launch_vap(const Bodies& b, const StepParams& p, cudaStream_t s);
+void launch_vap(const Bodies& b, const StepParams& p, cudaStream_t s, const Sizes* sizes = nullptr);
 // Full detection: leaves a sorted (ci, cj) list in `out` and the count in sizes->C.
 void launch_detect(const Bodies& b, const StepParams& p, DetectWork& w, Contacts& out, Sizes* sizes, long long c_cap,
                    cudaStream_t s);
@@ -200,5 +200,49 @@ void launch_sph_particle64(int na, int dim, int problem, const int* ptr, const d
 void launch_sph_residual64(int nin, int dim, int problem, const int2* cij, const dvec4* nc, const int* slot, double dt2,
                            const dvec4* u, double* g, unsigned long long* viol, const Sizes* sizes, long long c_cap,
                            cudaStream_t s);
+
+// --------------------------------------------------------- apgd_batch.cu
+struct BatchSceneStats {
+    long long contacts;
+    long long iterations;
+    long long fp32_iterations;
+    long long backtracks;
+    long long restarts;
+    int corrections;
+    int converged;
+    double violation;
+};
+
+template <typename T>
+struct BatchSolve {
+    int nin;
+    const int* order;
+    const int *sc_p0, *sc_p1, *sc_o0, *sc_o1, *sc_a0, *sc_a1;
+    const int2* cij;
+    V4<T>* nc;
+    const dvec4* nc64;
+    const int* inc_ptr;
+    const V4<T>* inc;
+    const dvec4* inc64;
+    const double* invm;
+    T* lam[3];
+    V4<T>* u[4];
+    double* lam64;
+    dvec4* ufin;
+    BatchSceneStats* stats;
+    const Sizes* sizes;
+    double alpha, tol, dt, viol_tol;
+    long long max_ite;
+    int dynamic;
+    int max_corrections;
+};
+
+long long apgd_batch_launches();
+void launch_batch_ranges(int n_scenes, int nin, const int* sc_obs0, const int* sc_obs1, const int* sc_p0,
+                         const int* sc_p1, const int* obs_off, const int* obs_pos, const int* row_ptr,
+                         const Sizes* sizes, int* o0, int* o1, int* a0, int* a1, cudaStream_t s);
+// one CTA per scene (block_threads = 256, 512 or 1024)
+template <typename T>
+cudaError_t launch_apgd_batch(int dim, int block_threads, const BatchSolve<T>& b, int n_scenes, cudaStream_t s);
 
 }  // namespace scopi_gpu

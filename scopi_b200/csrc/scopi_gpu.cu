@@ -135,7 +135,250 @@ struct scopi_gpu_handle {
         b.j = d_j;
         b.radius = d_radius;
         b.length = d_length;
+        if (batch) {
+            b.scene = d_scene;
+            b.scene_shift = d_shift;
+            b.obs_a0 = d_obs_a0;
+            b.obs_off = d_obs_off;
+        }
         return b;
+    }
+
+    // ---- batch of independent scenes (scopi_gpu_batch_create): all obstacles first (scene
+    // by scene), then the active bodies of scene 0, 1, ...
+    bool batch = false;
+    int n_scenes = 0;
+    std::vector<int> sc_n, sc_nin;                     // bodies / obstacles per scene
+    std::vector<long long> sc_obs_start, sc_act_start;  // global index of its first obstacle / active
+    DevMem batch_mem;
+    int* d_scene = nullptr;
+    double* d_shift = nullptr;
+    int* d_obs_a0 = nullptr;
+    int* d_obs_off = nullptr;
+    int *d_sc_obs0 = nullptr, *d_sc_obs1 = nullptr, *d_sc_p0 = nullptr, *d_sc_p1 = nullptr, *d_order = nullptr;
+    int *d_sc_o0 = nullptr, *d_sc_o1 = nullptr, *d_sc_a0 = nullptr, *d_sc_a1 = nullptr;
+    BatchSceneStats* d_bstats = nullptr;
+    std::vector<BatchSceneStats> h_bstats;
+    double* d_obs_snap = nullptr;  // obstacle pos (3) and q (4) before the step, restored on overflow
+    int batch_threads = 0;         // block size chosen by the autotuner
+    float batch_tune_ms[3] = {0, 0, 0};
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    double graph_dt = 0.0;
+    long long graph_cap = -1;
+    long long graph_kernels = 0;   // kernels one replay of `graph_exec` launches
+    long long replayed = 0;        // kernels launched by graph replays so far
+    long long cell_cap_hint = 0;   // cell-list capacity wanted by the batch layout
+
+    void drop_graph() {
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        if (graph) cudaGraphDestroy(graph);
+        graph_exec = nullptr;
+        graph = nullptr;
+    }
+
+    // Every kernel of one batch step, enqueued on `stream` with no host synchronisation
+    // (captured once into a CUDA graph and replayed every step).
+    void enqueue_batch_step(double dt, int bt) {
+        Bodies b = bodies();
+        StepParams sp = step_params(dt);
+        if (nin > 0) {
+            cudaMemcpyAsync(d_obs_snap, d_pos, 3 * (size_t)nin * sizeof(double), cudaMemcpyDeviceToDevice, stream);
+            cudaMemcpyAsync(d_obs_snap + 3 * (size_t)nin, d_q, 4 * (size_t)nin * sizeof(double),
+                            cudaMemcpyDeviceToDevice, stream);
+        }
+        launch_obstacles_move(b, dt, P.dim, stream);
+        cudaMemsetAsync(d_sizes_cur, 0, sizeof(Sizes), stream);
+        launch_detect(b, sp, dw, cur, d_sizes_cur, c_cap, stream);
+        launch_vap(b, sp, stream, d_sizes_cur);
+        launch_geometry(b, sp, cur, d_sizes_cur, c_cap, nullptr, nullptr, c_cap, stream);
+        launch_assemble(b, sp, cur, as, d_sizes_cur, c_cap, dw.scan_work, dw.tmp_total + 2, stream);
+        launch_incidence(b, sp, cur, as, inc, d_sizes_cur, c_cap, dw.scan_work, dw.tmp_total + 2, stream);
+        launch_pack_cij(cur.ci, cur.cj, d_cij, d_sizes_cur, c_cap, stream);
+        launch_pack_nc<double>(as.bn, as.cvec, d_nc64, d_sizes_cur, c_cap, stream);
+        launch_pack_inc<double>(na, inc.ptr, inc.idx, as.bn, d_incv64, 2 * c_cap, stream);
+        if (mixed()) {
+            launch_pack_nc<float>(as.bn, as.cvec, d_nc32, d_sizes_cur, c_cap, stream);
+            launch_pack_inc<float>(na, inc.ptr, inc.idx, as.bn, d_incv32, 2 * c_cap, stream);
+        }
+        launch_batch_ranges(n_scenes, nin, d_sc_obs0, d_sc_obs1, d_sc_p0, d_sc_p1, d_obs_off, dw.obs_pos, dw.row_ptr,
+                            d_sizes_cur, d_sc_o0, d_sc_o1, d_sc_a0, d_sc_a1, stream);
+        enqueue_batch_solve(dt, bt);
+        launch_update(b, sp, reinterpret_cast<const double*>(d_usfin), 4, 0, d_sizes_cur, stream);
+    }
+
+    void enqueue_batch_solve(double dt, int bt) {
+        auto fill = [&](auto& bs) {
+            bs.nin = nin;
+            bs.order = d_order;
+            bs.sc_p0 = d_sc_p0;
+            bs.sc_p1 = d_sc_p1;
+            bs.sc_o0 = d_sc_o0;
+            bs.sc_o1 = d_sc_o1;
+            bs.sc_a0 = d_sc_a0;
+            bs.sc_a1 = d_sc_a1;
+            bs.cij = d_cij;
+            bs.nc64 = d_nc64;
+            bs.inc_ptr = inc.ptr;
+            bs.inc64 = d_incv64;
+            bs.invm = d_invm64;
+            bs.lam64 = d_lamacc;
+            bs.ufin = d_usfin;
+            bs.stats = d_bstats;
+            bs.sizes = d_sizes_cur;
+            bs.alpha = P.alpha;
+            bs.tol = P.tolerance;
+            bs.dt = dt;
+            bs.viol_tol = P.mixed_violation_tol;
+            bs.max_ite = P.max_ite;
+            bs.dynamic = P.dynamic_descent;
+            bs.max_corrections = P.mixed_max_corrections;
+        };
+        if (mixed()) {
+            BatchSolve<float> bs{};
+            fill(bs);
+            bs.nc = d_nc32;
+            bs.inc = d_incv32;
+            for (int k = 0; k < 3; ++k) bs.lam[k] = d_lam32[k];
+            for (int k = 0; k < 4; ++k) bs.u[k] = d_us32[k];
+            launch_apgd_batch<float>(P.dim, bt, bs, n_scenes, stream);
+        } else {
+            BatchSolve<double> bs{};
+            fill(bs);
+            bs.nc = d_nc64;
+            bs.inc = d_incv64;
+            for (int k = 0; k < 3; ++k) bs.lam[k] = d_lam64[k];
+            for (int k = 0; k < 4; ++k) bs.u[k] = d_us64[k];
+            launch_apgd_batch<double>(P.dim, bt, bs, n_scenes, stream);
+        }
+    }
+
+    int read_batch_sizes() {
+        cudaMemcpyAsync(h_sizes, d_sizes_cur, sizeof(Sizes), cudaMemcpyDeviceToHost, stream);
+        cudaError_t e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cuda_fail(e, "batch step");
+        return 0;
+    }
+
+    // undo the obstacle motion of a step that overflowed and grow the contact buffers
+    int batch_overflow_recover() {
+        if (nin > 0) {
+            cudaMemcpyAsync(d_pos, d_obs_snap, 3 * (size_t)nin * sizeof(double), cudaMemcpyDeviceToDevice, stream);
+            cudaMemcpyAsync(d_q, d_obs_snap + 3 * (size_t)nin, 4 * (size_t)nin * sizeof(double),
+                            cudaMemcpyDeviceToDevice, stream);
+        }
+        int tot[2] = {0, 0};
+        cudaMemcpy(tot, dw.tmp_total, 2 * sizeof(int), cudaMemcpyDeviceToHost);
+        const long long need = (long long)(1.3 * ((double)tot[0] + tot[1])) + 4096;
+        drop_graph();
+        int rc = alloc_contacts(std::max(need, 2 * c_cap));
+        has_old = false;
+        return rc;
+    }
+
+    void collect_batch_stats() {
+        h_bstats.resize(n_scenes);
+        cudaMemcpy(h_bstats.data(), d_bstats, n_scenes * sizeof(BatchSceneStats), cudaMemcpyDeviceToHost);
+        stats.contacts = 0;
+        stats.iterations = stats.fp32_iterations = stats.backtracks = stats.restarts = stats.corrections = 0;
+        stats.converged = 1;
+        stats.violation = 0.0;
+        for (const auto& s : h_bstats) {
+            stats.contacts += s.contacts;
+            stats.iterations = std::max<int64_t>(stats.iterations, s.iterations);  // the longest scene
+            stats.fp32_iterations = std::max<int64_t>(stats.fp32_iterations, s.fp32_iterations);
+            stats.backtracks += s.backtracks;
+            stats.restarts += s.restarts;
+            stats.corrections += s.corrections;
+            stats.converged = stats.converged && s.converged;
+            stats.violation = std::max(stats.violation, s.violation);
+        }
+        stats.status = stats.converged ? 0 : SCOPI_GPU_ENOCONV;
+    }
+
+    // One time step of every scene: eager with block-size autotuning the first time, then
+    // one CUDA graph replay per step.
+    int step_batch(double dt) {
+        for (int attempt = 0; attempt < 4; ++attempt) {
+            cudaEventRecord(ev[0], stream);
+            if (!batch_threads) {
+                // autotune: time the batched solve at 256, 512 and 1024 threads per scene on
+                // this step's problem (each run is a full cold-start solve), keep the fastest
+                const int cand[3] = {256, 512, 1024};
+                enqueue_batch_step(dt, 256);  // the first step itself runs with 256 threads
+                int rc = read_batch_sizes();
+                if (rc) return rc;
+                if (h_sizes->overflow) {
+                    // nothing after detection ran (overflow guards): restore, grow, redo
+                    rc = batch_overflow_recover();
+                    if (rc) return rc;
+                    continue;
+                }
+                // timing only: re-solve this step's contact problem (its packed records are
+                // still in place) with each block size; the update already used the first solve
+                float best = 1e30f;
+                int best_bt = 256;
+                for (int k = 0; k < 3; ++k) {
+                    cudaEventRecord(ev_a[0], stream);
+                    enqueue_batch_solve(dt, cand[k]);
+                    cudaEventRecord(ev_a[1], stream);
+                    cudaEventSynchronize(ev_a[1]);
+                    float ms = 0;
+                    cudaEventElapsedTime(&ms, ev_a[0], ev_a[1]);
+                    batch_tune_ms[k] = ms;
+                    if (ms < best) {
+                        best = ms;
+                        best_bt = cand[k];
+                    }
+                }
+                batch_threads = best_bt;
+                cudaEventRecord(ev[3], stream);
+                collect_batch_stats();
+                finish_batch_step_timing();
+                return 0;
+            }
+            if (!graph_exec || graph_dt != dt || graph_cap != c_cap) {
+                drop_graph();
+                cudaError_t e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
+                if (e != cudaSuccess) return cuda_fail(e, "cudaStreamBeginCapture");
+                const long long l0 = launches();
+                enqueue_batch_step(dt, batch_threads);
+                graph_kernels = launches() - l0;
+                replayed -= graph_kernels;  // the capture itself launched nothing
+                e = cudaStreamEndCapture(stream, &graph);
+                if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+                e = cudaGraphInstantiate(&graph_exec, graph, 0);
+                if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+                graph_dt = dt;
+                graph_cap = c_cap;
+                cudaEventRecord(ev[0], stream);
+            }
+            cudaError_t e = cudaGraphLaunch(graph_exec, stream);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaGraphLaunch");
+            replayed += graph_kernels;
+            int rc = read_batch_sizes();
+            if (rc) return rc;
+            if (h_sizes->overflow) {
+                rc = batch_overflow_recover();
+                if (rc) return rc;
+                continue;
+            }
+            cudaEventRecord(ev[3], stream);
+            collect_batch_stats();
+            finish_batch_step_timing();
+            return 0;
+        }
+        return fail(SCOPI_GPU_ENOMEM, "contact capacity could not be grown");
+    }
+
+    void finish_batch_step_timing() {
+        cudaEventSynchronize(ev[3]);
+        float t = 0;
+        cudaEventElapsedTime(&t, ev[0], ev[3]);
+        stats.ms_step = t;
+        stats.ms_solve = t;
+        stats.ms_apgd_kernel = 0;
+        stats.steps += 1;
     }
     StepParams step_params(double dt) const {
         StepParams s;
@@ -193,7 +436,7 @@ struct scopi_gpu_handle {
     }
 
     // Buffers whose size follows the number of bodies.
-    int alloc_bodies(int n_, int nin_) {
+    int alloc_bodies(int n_, int nin_, long long obs_cap = -1) {
         body_mem.release();
         n = n_;
         nin = nin_;
@@ -214,8 +457,8 @@ struct scopi_gpu_handle {
             A(d_u64[k], 6 * (size_t)na + 6)
             A(d_u32[k], 6 * (size_t)na + 6)
         }
-        dw.cell_cap = std::max<long long>(4LL * na, 4096);
-        dw.obs_cap = (long long)nin * na;
+        dw.cell_cap = std::max<long long>({4LL * na, 4096LL, cell_cap_hint});
+        dw.obs_cap = obs_cap >= 0 ? obs_cap : (long long)nin * na;
         A(dw.grid, 1) A(dw.bbox_partial, 8 * 4 * kSMs) A(dw.cell_count, dw.cell_cap + 1) A(dw.cell_start, dw.cell_cap + 1)
         A(dw.cell_fill, dw.cell_cap) A(dw.cell_of, na + 1) A(dw.cell_body, na + 1) A(dw.cell_pr, na + 1)
         A(dw.row_count, na + 1) A(dw.row_ptr, na + 1) A(dw.obs_flag, dw.obs_cap + 1) A(dw.obs_pos, dw.obs_cap + 1)
@@ -263,7 +506,9 @@ struct scopi_gpu_handle {
         return 0;
     }
 
-    long long launches() const { return detect_launches() + apgd_launches() + apgd_sph_launches(); }
+    long long launches() const {
+        return detect_launches() + apgd_launches() + apgd_sph_launches() + apgd_batch_launches() + replayed;
+    }
 
     // contact detection + closest points + assembly + incidence lists into `cur`
     int detect_and_assemble(double dt, bool assemble) {
@@ -690,6 +935,8 @@ int32_t scopi_gpu_destroy(scopi_gpu_handle* h) {
     if (!h) return SCOPI_GPU_EINVAL;
     cudaSetDevice(h->dev);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    h->drop_graph();
+    h->batch_mem.release();
     h->body_mem.release();
     h->cap_mem.release();
     h->fixed_mem.release();
@@ -705,7 +952,14 @@ int32_t scopi_gpu_destroy(scopi_gpu_handle* h) {
     return 0;
 }
 
+static int32_t upload_particles(scopi_gpu_handle* h, const scopi_gpu_particles* p, long long obs_cap);
+
 int32_t scopi_gpu_set_particles(scopi_gpu_handle* h, const scopi_gpu_particles* p) {
+    if (h && h->batch) return h->fail(SCOPI_GPU_EINVAL, "batch handles take their scenes at creation");
+    return upload_particles(h, p, -1);
+}
+
+static int32_t upload_particles(scopi_gpu_handle* h, const scopi_gpu_particles* p, long long obs_cap) {
     if (!h || !p || p->n < 0 || p->nb_inactive < 0 || p->nb_inactive > p->n || p->n >= (1LL << 30))
         return h ? h->fail(SCOPI_GPU_EINVAL, "invalid particle container") : SCOPI_GPU_EINVAL;
     if (!p->shape || !p->pos || !p->q || !p->v || !p->omega || !p->vd || !p->omega_d || !p->f || !p->m || !p->j ||
@@ -721,8 +975,8 @@ int32_t scopi_gpu_set_particles(scopi_gpu_handle* h, const scopi_gpu_particles* 
     }
     cudaSetDevice(h->dev);
     cudaStreamSynchronize(h->stream);
-    if (n != h->n || nin != h->nin) {
-        int rc = h->alloc_bodies(n, nin);
+    if (n != h->n || nin != h->nin || h->batch) {
+        int rc = h->alloc_bodies(n, nin, obs_cap);
         if (rc) return rc;
         if (h->c_cap == 0) {
             rc = h->alloc_contacts(std::max<long long>(8192, 6LL * (n - nin) + 2LL * nin * 64));
@@ -786,7 +1040,7 @@ int32_t scopi_gpu_run(scopi_gpu_handle* h, double dt, int64_t total_it, int64_t 
     cudaSetDevice(h->dev);
     int status = 0;
     for (int64_t it = initial_iter; it < total_it; ++it) {
-        int rc = h->step(dt);
+        int rc = h->batch ? h->step_batch(dt) : h->step(dt);
         if (rc < 0) return rc;
         if (h->stats.status == SCOPI_GPU_ENOCONV) status = SCOPI_GPU_ENOCONV;
     }
@@ -900,5 +1154,199 @@ const char* scopi_gpu_last_error(scopi_gpu_handle* h) { return h ? h->err.c_str(
 int64_t scopi_gpu_kernel_launches(scopi_gpu_handle* h) { return h ? h->launches() - h->launches0 : 0; }
 
 void* scopi_gpu_get_stream(scopi_gpu_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+int32_t scopi_gpu_batch_create(const scopi_gpu_params* p, int32_t n_scenes, const scopi_gpu_particles* scenes,
+                               scopi_gpu_handle** out) {
+    if (!p || !scenes || !out || n_scenes <= 0) {
+        scopi_gpu::set_global_error("scopi_gpu_batch_create: invalid argument");
+        return SCOPI_GPU_EINVAL;
+    }
+    *out = nullptr;
+    if (p->problem != SCOPI_GPU_NOFRICTION) {
+        scopi_gpu::set_global_error("scopi_gpu_batch_create: batches solve NoFriction scenes");
+        return SCOPI_GPU_EUNSUPPORTED;
+    }
+    long long ntot = 0, nin_tot = 0;
+    for (int s = 0; s < n_scenes; ++s) {
+        const scopi_gpu_particles& sc = scenes[s];
+        if (sc.n < 0 || sc.nb_inactive < 0 || sc.nb_inactive > sc.n || !sc.shape || !sc.pos || !sc.q || !sc.v ||
+            !sc.omega || !sc.vd || !sc.omega_d || !sc.f || !sc.m || !sc.j || !sc.radius || !sc.length) {
+            scopi_gpu::set_global_error("scopi_gpu_batch_create: invalid scene container");
+            return SCOPI_GPU_EINVAL;
+        }
+        ntot += sc.n;
+        nin_tot += sc.nb_inactive;
+    }
+    if (ntot >= (1LL << 30)) {
+        scopi_gpu::set_global_error("scopi_gpu_batch_create: too many bodies");
+        return SCOPI_GPU_EINVAL;
+    }
+    int rc = scopi_gpu_create(p, out);
+    if (rc) return rc;
+    scopi_gpu_handle* h = *out;
+    h->batch = true;
+    h->n_scenes = n_scenes;
+    h->sc_n.resize(n_scenes);
+    h->sc_nin.resize(n_scenes);
+    h->sc_obs_start.resize(n_scenes);
+    h->sc_act_start.resize(n_scenes);
+    // concatenation: every scene's obstacles first, then every scene's active bodies
+    std::vector<int32_t> shape(ntot), scene_of(ntot);
+    std::vector<double> pos(3 * ntot), q(4 * ntot), v(3 * ntot), om(3 * ntot), vd(3 * ntot), od(3 * ntot), f(3 * ntot),
+        m(ntot), jj(3 * ntot), rad(ntot), len(ntot);
+    auto copy_body = [&](const scopi_gpu_particles& sc, long long src, long long dst, int s) {
+        shape[dst] = sc.shape[src];
+        scene_of[dst] = s;
+        for (int d = 0; d < 3; ++d) {
+            pos[3 * dst + d] = sc.pos[3 * src + d];
+            v[3 * dst + d] = sc.v[3 * src + d];
+            om[3 * dst + d] = sc.omega[3 * src + d];
+            vd[3 * dst + d] = sc.vd[3 * src + d];
+            od[3 * dst + d] = sc.omega_d[3 * src + d];
+            f[3 * dst + d] = sc.f[3 * src + d];
+            jj[3 * dst + d] = sc.j[3 * src + d];
+        }
+        for (int d = 0; d < 4; ++d) q[4 * dst + d] = sc.q[4 * src + d];
+        m[dst] = sc.m[src];
+        rad[dst] = sc.radius[src];
+        len[dst] = sc.length[src];
+    };
+    long long ob = 0, ac = nin_tot;
+    std::vector<int> obs_a0(nin_tot + 1), obs_off(nin_tot + 1, 0), sc_obs0(n_scenes), sc_obs1(n_scenes),
+        sc_p0(n_scenes), sc_p1(n_scenes);
+    for (int s = 0; s < n_scenes; ++s) {
+        const scopi_gpu_particles& sc = scenes[s];
+        h->sc_n[s] = (int)sc.n;
+        h->sc_nin[s] = (int)sc.nb_inactive;
+        h->sc_obs_start[s] = ob;
+        h->sc_act_start[s] = ac;
+        sc_obs0[s] = (int)ob;
+        sc_p0[s] = (int)(ac - nin_tot);
+        for (long long k = 0; k < sc.nb_inactive; ++k) {
+            obs_a0[ob] = (int)(ac - nin_tot);
+            obs_off[ob + 1] = obs_off[ob] + (int)(sc.n - sc.nb_inactive);
+            copy_body(sc, k, ob++, s);
+        }
+        for (long long k = sc.nb_inactive; k < sc.n; ++k) copy_body(sc, k, ac++, s);
+        sc_obs1[s] = (int)ob;
+        sc_p1[s] = (int)(ac - nin_tot);
+    }
+    // cell-key shift: scene s is moved to x = s * pitch so the scenes occupy disjoint cells
+    double wmax = 0.0, rmax = 0.0;
+    std::vector<double> xmin(n_scenes, 1e300);
+    for (long long b = 0; b < ntot; ++b) {
+        const int s = scene_of[b];
+        xmin[s] = std::min(xmin[s], pos[3 * b] - len[b] - rad[b]);
+        rmax = std::max(rmax, rad[b]);
+    }
+    for (long long b = 0; b < ntot; ++b) {
+        const int s = scene_of[b];
+        wmax = std::max(wmax, pos[3 * b] + len[b] + rad[b] - xmin[s]);
+    }
+    // pairs of different scenes are rejected explicitly, so the gap between scenes only
+    // keeps them out of each other's cells (efficiency, not correctness)
+    const double hcell = 2.0 * rmax + p->dmax;
+    const double pitch = wmax + 2.0 * hcell + 1e-9;
+    std::vector<double> shift(n_scenes);
+    for (int s = 0; s < n_scenes; ++s) shift[s] = s * pitch - (xmin[s] < 1e299 ? xmin[s] : 0.0);
+    // cell-list capacity for the shifted layout at the initial extent in y (z), twice over
+    // for bodies that spread while falling; coarser cells are used past this capacity
+    {
+        double cells = std::ceil(n_scenes * pitch / std::max(hcell, 1e-12)) + 1.0;
+        for (int d = 1; d < p->dim; ++d) {
+            double lo = 1e300, hi = -1e300;
+            for (long long b = nin_tot; b < ntot; ++b) {
+                lo = std::min(lo, pos[3 * b + d]);
+                hi = std::max(hi, pos[3 * b + d]);
+            }
+            cells *= (hi >= lo ? std::ceil((hi - lo) / std::max(hcell, 1e-12)) : 0.0) + 1.0;
+        }
+        h->cell_cap_hint = (long long)std::min(2.0 * cells, 64.0e6);
+    }
+    std::vector<int> order(n_scenes);
+    for (int s = 0; s < n_scenes; ++s) order[s] = s;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return (sc_p1[a] - sc_p0[a]) > (sc_p1[b] - sc_p0[b]); });
+    scopi_gpu_particles cat{ntot, nin_tot, shape.data(), pos.data(), q.data(), v.data(), om.data(), vd.data(),
+                            od.data(), f.data(), m.data(), jj.data(), rad.data(), len.data()};
+    rc = upload_particles(h, &cat, obs_off[nin_tot]);
+    if (rc) {
+        scopi_gpu::set_global_error(h->err.c_str());
+        scopi_gpu_destroy(h);
+        *out = nullptr;
+        return rc;
+    }
+    cudaError_t e;
+#define BA(ptr, cnt) \
+    if ((e = h->alloc(h->batch_mem, ptr, (cnt))) != cudaSuccess) return h->cuda_fail(e, "cudaMalloc(batch)");
+    BA(h->d_scene, ntot) BA(h->d_shift, n_scenes) BA(h->d_obs_a0, nin_tot + 1) BA(h->d_obs_off, nin_tot + 1)
+    BA(h->d_sc_obs0, n_scenes) BA(h->d_sc_obs1, n_scenes) BA(h->d_sc_p0, n_scenes) BA(h->d_sc_p1, n_scenes)
+    BA(h->d_order, n_scenes) BA(h->d_sc_o0, n_scenes) BA(h->d_sc_o1, n_scenes) BA(h->d_sc_a0, n_scenes)
+    BA(h->d_sc_a1, n_scenes) BA(h->d_bstats, n_scenes) BA(h->d_obs_snap, 7 * nin_tot + 7)
+#undef BA
+    cudaMemcpy(h->d_scene, scene_of.data(), ntot * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(h->d_shift, shift.data(), n_scenes * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpy(h->d_obs_a0, obs_a0.data(), (nin_tot + 1) * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(h->d_obs_off, obs_off.data(), (nin_tot + 1) * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(h->d_sc_obs0, sc_obs0.data(), n_scenes * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(h->d_sc_obs1, sc_obs1.data(), n_scenes * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(h->d_sc_p0, sc_p0.data(), n_scenes * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(h->d_sc_p1, sc_p1.data(), n_scenes * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(h->d_order, order.data(), n_scenes * sizeof(int), cudaMemcpyHostToDevice);
+    e = cudaMemset(h->d_bstats, 0, n_scenes * sizeof(BatchSceneStats));
+    if (e != cudaSuccess) return h->cuda_fail(e, "batch set-up");
+    return 0;
+}
+
+int32_t scopi_gpu_batch_get_scene(scopi_gpu_handle* h, int32_t scene, scopi_gpu_particles* o) {
+    if (!h || !o || !h->batch || scene < 0 || scene >= h->n_scenes) return SCOPI_GPU_EINVAL;
+    cudaSetDevice(h->dev);
+    const long long nin_s = h->sc_nin[scene], na_s = h->sc_n[scene] - nin_s;
+    struct Seg {
+        long long src, dst, cnt;
+    } segs[2] = {{h->sc_obs_start[scene], 0, nin_s}, {h->sc_act_start[scene], nin_s, na_s}};
+    for (const Seg& g : segs) {
+        if (g.cnt <= 0) continue;
+        if (o->pos)
+            cudaMemcpy(o->pos + 3 * g.dst, h->d_pos + 3 * g.src, 3 * g.cnt * sizeof(double), cudaMemcpyDeviceToHost);
+        if (o->q) cudaMemcpy(o->q + 4 * g.dst, h->d_q + 4 * g.src, 4 * g.cnt * sizeof(double), cudaMemcpyDeviceToHost);
+        if (o->v) cudaMemcpy(o->v + 3 * g.dst, h->d_v + 3 * g.src, 3 * g.cnt * sizeof(double), cudaMemcpyDeviceToHost);
+        if (o->omega)
+            cudaMemcpy(o->omega + 3 * g.dst, h->d_omega + 3 * g.src, 3 * g.cnt * sizeof(double),
+                       cudaMemcpyDeviceToHost);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return h->cuda_fail(e, "batch_get_scene");
+    return 0;
+}
+
+int32_t scopi_gpu_batch_get_scene_stats(scopi_gpu_handle* h, int32_t scene, scopi_gpu_scene_stats* out) {
+    if (!h || !out || !h->batch || scene < 0 || scene >= h->n_scenes) return SCOPI_GPU_EINVAL;
+    if ((int)h->h_bstats.size() != h->n_scenes) {
+        std::memset(out, 0, sizeof(*out));
+        return 0;
+    }
+    const BatchSceneStats& s = h->h_bstats[scene];
+    out->contacts = s.contacts;
+    out->iterations = s.iterations;
+    out->fp32_iterations = s.fp32_iterations;
+    out->backtracks = s.backtracks;
+    out->restarts = s.restarts;
+    out->corrections = s.corrections;
+    out->converged = s.converged;
+    out->violation = s.violation;
+    return 0;
+}
+
+int32_t scopi_gpu_batch_block_threads(scopi_gpu_handle* h) { return h ? h->batch_threads : 0; }
+
+int32_t scopi_gpu_batch_set_block_threads(scopi_gpu_handle* h, int32_t threads) {
+    if (!h || !h->batch) return SCOPI_GPU_EINVAL;
+    if (h->stats.steps > 0) return h->fail(SCOPI_GPU_EINVAL, "the block size is fixed once the batch has stepped");
+    if (threads != 0 && threads != 256 && threads != 512 && threads != 1024)
+        return h->fail(SCOPI_GPU_EINVAL, "block size must be 256, 512 or 1024 (0 = autotune)");
+    h->batch_threads = threads;
+    return 0;
+}
 
 }  // extern "C"

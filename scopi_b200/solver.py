@@ -205,3 +205,90 @@ class ScopiSolver:
         out = np.zeros(6 * (self.particles.n - self.particles.nb_inactive))
         self._check(self._lib.scopi_gpu_atmat(self._h, _dp(f), _dp(out)), "scopi_gpu_atmat")
         return out
+
+
+class ScopiBatch:
+    """Many independent scenes stepped together (one ScopiSolver per scene in the reference).
+
+    ``scenes`` is a list of ``ParticleArrays`` (each obstacles first).  ``run(dt, k)`` advances
+    every scene k steps (one CUDA graph replay per step, one persistent launch solving every
+    scene); ``scene(s)`` returns scene s's particles and ``scene_stats(s)`` its solver
+    statistics of the last step.  NoFriction only.  ``block_threads`` pins the threads per
+    scene (256, 512 or 1024); 0 lets the first step autotune it.
+    """
+
+    def __init__(self, scenes, vap=VAP_FPD, contact_method=KDTREE, precision=FP64, device=0, block_threads=0,
+                 **overrides):
+        self._lib = _abi.load()
+        p = _abi.Params()
+        self._lib.scopi_gpu_default_params(C.byref(p), scenes[0].dim)
+        p.problem, p.vap, p.contact_method, p.precision, p.device = NOFRICTION, vap, contact_method, precision, device
+        for k, v in overrides.items():
+            if k == "dynamic_descent":
+                v = 1 if v else 0
+            setattr(p, k, v)
+        self._params = p
+        self.scenes = [s.copy() for s in scenes]
+        arr = (_abi.ParticlesC * len(self.scenes))()
+        self._keep = []
+        for k, pa in enumerate(self.scenes):
+            arr[k] = _abi.ParticlesC(pa.n, pa.nb_inactive, pa.shape.ctypes.data_as(C.POINTER(C.c_int32)), _dp(pa.pos),
+                                     _dp(pa.q), _dp(pa.v), _dp(pa.omega), _dp(pa.vd), _dp(pa.omega_d), _dp(pa.f),
+                                     _dp(pa.m), _dp(pa.j), _dp(pa.radius), _dp(pa.length))
+        h = C.c_void_p()
+        rc = self._lib.scopi_gpu_batch_create(C.byref(p), len(self.scenes), arr, C.byref(h))
+        if rc < 0:
+            raise ScopiGPUError(f"scopi_gpu_batch_create failed ({rc}): {self._lib.scopi_gpu_last_error(None).decode()}")
+        self._h = h
+        if block_threads:
+            self._check(self._lib.scopi_gpu_batch_set_block_threads(h, int(block_threads)),
+                        "scopi_gpu_batch_set_block_threads")
+
+    def _check(self, rc, what):
+        if rc < 0:
+            raise ScopiGPUError(f"{what} failed ({rc}): {self._lib.scopi_gpu_last_error(self._h).decode()}")
+        return rc
+
+    def run(self, dt: float, steps: int):
+        rc = self._check(self._lib.scopi_gpu_run(self._h, dt, steps, 0), "scopi_gpu_run")
+        if rc == _abi.ENOCONV:
+            print("APGD didn't converge.", file=sys.stderr)
+        return self
+
+    def scene(self, s: int) -> ParticleArrays:
+        pa = self.scenes[s]
+        st = _abi.ParticlesC(pa.n, pa.nb_inactive, pa.shape.ctypes.data_as(C.POINTER(C.c_int32)), _dp(pa.pos), _dp(pa.q),
+                             _dp(pa.v), _dp(pa.omega), _dp(pa.vd), _dp(pa.omega_d), _dp(pa.f), _dp(pa.m), _dp(pa.j),
+                             _dp(pa.radius), _dp(pa.length))
+        self._check(self._lib.scopi_gpu_batch_get_scene(self._h, s, C.byref(st)), "scopi_gpu_batch_get_scene")
+        return pa
+
+    def scene_stats(self, s: int):
+        st = _abi.SceneStats()
+        self._check(self._lib.scopi_gpu_batch_get_scene_stats(self._h, s, C.byref(st)), "scopi_gpu_batch_get_scene_stats")
+        return {k: getattr(st, k) for k, _ in _abi.SceneStats._fields_}
+
+    def stats(self):
+        s = _abi.Stats()
+        self._check(self._lib.scopi_gpu_get_stats(self._h, C.byref(s)), "scopi_gpu_get_stats")
+        return {k: getattr(s, k) for k, _ in _abi.Stats._fields_}
+
+    def block_threads(self) -> int:
+        return int(self._lib.scopi_gpu_batch_block_threads(self._h))
+
+    def stream_handle(self) -> int:
+        return int(self._lib.scopi_gpu_get_stream(self._h) or 0)
+
+    def kernel_launches(self) -> int:
+        return int(self._lib.scopi_gpu_kernel_launches(self._h))
+
+    def close(self):
+        if self._h:
+            self._lib.scopi_gpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

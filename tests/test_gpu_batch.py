@@ -1,0 +1,143 @@
+"""Batched ensemble (many independent 2D pile scenes, one persistent solve launch per step,
+one CUDA graph replay per step) against each scene stepped alone: by the oracle (CPU
+restatement of ScopiSolver, include/scopi/solver.hpp:153-178) and by the single-scene GPU
+solver."""
+import numpy as np
+import pytest
+
+from gpu_helpers import oracle_solver, rel_err
+from scopi_b200 import FP64, MIXED, ScopiBatch, ScopiGPUError, ScopiSolver, configs
+from scopi_b200.container import Particles, Property
+
+pytestmark = pytest.mark.gpu
+
+ST = configs.SETTINGS["pile_scenes"]
+KW = dict(dmax=ST["dmax"], tolerance=ST["tolerance"], max_ite=ST["max_ite"])
+
+
+def small_piles(n, nmin=30, nmax=300, seed=7, vmax=0.6):
+    """Pile scenes whose disks get random velocities in [-vmax, vmax]^2, so neighbours
+    approach each other and the first steps already have active constraints."""
+    out = []
+    for s in range(n):
+        pa = configs.pile_scene(seed * 1000 + s, nmin, nmax)
+        u = configs.splitmix_uniform(seed * 7919 + s, 2 * pa.n).reshape(pa.n, 2)
+        pa.v[pa.nb_inactive:, :2] = (2 * u[pa.nb_inactive:] - 1) * vmax
+        out.append(pa)
+    return out
+
+
+def lone_disk():
+    """A scene without contacts: one disk far above its segment (free fall)."""
+    p = Particles(2)
+    p.add_segment((0.0, 0.0), (0.5, 0.0))
+    m = 1.3
+    p.add_sphere((0.25, 0.8), 0.01, Property(mass=m, moment_inertia=0.5 * m * 1e-4, force=(0.0, -9.81 * m)))
+    return p.finalize()
+
+
+def test_batch_fp64_matches_oracle_per_scene():
+    scenes = small_piles(4)
+    steps = 8
+    b = ScopiBatch(scenes, vap=ST["vap"], precision=FP64, **KW)
+    oracles = [oracle_solver(s, vap=ST["vap"], **KW) for s in scenes]
+    for k in range(steps):
+        b.run(ST["dt"], 1)
+        for s, o in enumerate(oracles):
+            o.run(ST["dt"], 1)
+            assert b.scene_stats(s)["contacts"] == len(o.contacts()["i"]), f"scene {s} step {k}"
+    iters = 0
+    for s, o in enumerate(oracles):
+        g = b.scene(s)
+        assert rel_err(g.pos, o.pa.pos) <= 1e-9, s
+        assert rel_err(g.v, o.pa.v) <= 1e-7, s
+        assert b.scene_stats(s)["converged"] == 1
+        iters = max(iters, b.scene_stats(s)["iterations"])
+    assert iters > 10  # the solves did work
+
+
+def test_batch_fp64_matches_single_scene_gpu():
+    scenes = small_piles(6, 100, 1500, seed=8) + [lone_disk()]
+    steps = 6
+    b = ScopiBatch(scenes, vap=ST["vap"], precision=FP64, **KW).run(ST["dt"], steps)
+    for s, pa in enumerate(scenes):
+        one = ScopiSolver(pa, vap=ST["vap"], precision=FP64, **KW).run(ST["dt"], steps)
+        g = b.scene(s)
+        assert b.scene_stats(s)["contacts"] == one.stats()["contacts"], s
+        assert rel_err(g.pos, one.particles.pos) <= 1e-9, s
+        assert rel_err(g.v, one.particles.v) <= 1e-7, s
+
+
+def test_batch_scene_without_contacts_falls_freely():
+    scenes = small_piles(2) + [lone_disk()]
+    b = ScopiBatch(scenes, vap=ST["vap"], precision=FP64, **KW).run(ST["dt"], 5)
+    st = b.scene_stats(2)
+    assert st["contacts"] == 0 and st["iterations"] == 0
+    g = b.scene(2)
+    # vap_fpd: v_{k+1} = v_k + dt f/m, then x += dt v (solver.hpp:138-148, vap_fpd.hpp:26-38)
+    v, y = 0.0, 0.8
+    for _ in range(5):
+        v += ST["dt"] * -9.81
+        y += ST["dt"] * v
+    assert abs(g.v[1, 1] - v) <= 1e-12 and abs(g.pos[1, 1] - y) <= 1e-12
+
+
+def test_batch_mixed_reaches_violation_target():
+    scenes = small_piles(6, 100, 1500, seed=9)
+    f64 = ScopiBatch(scenes, vap=ST["vap"], precision=FP64, **KW).run(ST["dt"], 3)
+    mix = ScopiBatch(scenes, vap=ST["vap"], precision=MIXED, mixed_violation_tol=1e-6, **KW).run(ST["dt"], 3)
+    for s in range(len(scenes)):
+        st = mix.scene_stats(s)
+        assert st["violation"] <= 1e-6, (s, st)
+        if st["contacts"]:
+            assert st["fp32_iterations"] > 0
+        assert rel_err(mix.scene(s).pos, f64.scene(s).pos) <= 1e-7, s
+
+
+def test_batch_block_sizes_agree_and_are_deterministic():
+    scenes = small_piles(5, 100, 1500, seed=10)
+    runs = {}
+    for bt in (256, 1024, 256):
+        b = ScopiBatch(scenes, vap=ST["vap"], precision=FP64, block_threads=bt, **KW).run(ST["dt"], 4)
+        assert b.block_threads() == bt
+        pos = [b.scene(s).pos.copy() for s in range(len(scenes))]
+        if bt in runs:
+            for a, c in zip(runs[bt], pos):
+                assert np.array_equal(a, c), "same block size, different result"
+        runs[bt] = pos
+    for a, c in zip(runs[256], runs[1024]):
+        assert rel_err(a, c) <= 1e-9
+
+
+def test_batch_autotune_graph_replay_and_launch_count():
+    scenes = small_piles(8, 100, 1500, seed=11)
+    b = ScopiBatch(scenes, vap=ST["vap"], precision=MIXED, **KW)
+    b.run(ST["dt"], 1)
+    assert b.block_threads() in (256, 512, 1024)
+    b.run(ST["dt"], 1)  # captures the graph, replays it once
+    l1 = b.kernel_launches()
+    b.run(ST["dt"], 1)
+    l2 = b.kernel_launches()
+    b.run(ST["dt"], 3)
+    l3 = b.kernel_launches()
+    per_step = l2 - l1
+    assert per_step > 0 and l3 - l2 == 3 * per_step
+    assert b.stats()["steps"] == 6
+    with pytest.raises(ScopiGPUError):
+        b._check(b._lib.scopi_gpu_batch_set_block_threads(b._h, 512), "set_block_threads")
+
+
+def test_batch_rejects_bad_block_size_and_friction():
+    scenes = small_piles(2)
+    with pytest.raises(ScopiGPUError):
+        ScopiBatch(scenes, block_threads=300, **KW)
+    b = ScopiBatch(scenes, **KW)
+    assert b._lib.scopi_gpu_batch_set_block_threads(b._h, 512) == 0
+    from scopi_b200 import _abi
+    import ctypes as C
+    p = _abi.Params()
+    b._lib.scopi_gpu_default_params(C.byref(p), 2)
+    p.problem = 1  # Friction
+    arr = (_abi.ParticlesC * 1)()
+    h = C.c_void_p()
+    assert b._lib.scopi_gpu_batch_create(C.byref(p), 0, arr, C.byref(h)) < 0
