@@ -41,15 +41,16 @@ def env_int(k, d):
         return d
 
 
-def roofline_bytes_per_iter(C, N, s, dim=3, torque_free=True):
+def roofline_bytes_per_iter(C, N, s, dim=3, torque_free=False):
     """Algorithmic bytes of one APGD iteration (accepted step, no backtracks).
 
     Rows of B: 3 passes over B (values + 2 int32 indices per contact), 6 contact vector
     streams, 4 particle vector streams.  Full rows carry 9 values per contact in 3D
-    (n, R_i^T(r_i x n), R_j^T(r_j x n)) and 6N particle slots; for normal-only problems
-    on sphere/plane/segment contacts the rotational values are identically zero, so a
-    row is the normal alone (3 values in 3D, 2 in 2D) and the particle vectors have N*dim
-    translational slots.
+    (n, R_i^T(r_i x n), R_j^T(r_j x n)) and 6N particle slots (4 values and 3N slots in
+    2D): this is the figure `roofline.achieved` uses.  For normal-only problems on
+    sphere/plane/segment contacts the rotational values are identically zero, so the
+    torque-free kernel streams a row as the normal alone (3 values in 3D, 2 in 2D) with
+    N*dim translational particle slots (`torque_free=True`, reported beside it).
     """
     if torque_free:
         return 3 * C * (dim * s + 8) + 6 * C * s + 4 * (dim * N) * s
@@ -158,12 +159,12 @@ def solver_kwargs():
     return dict(dmax=st["dmax"], tolerance=st["tolerance"], max_ite=st["max_ite"], vap=st["vap"]), st["dt"]
 
 
-def time_path(pa, precision, steps, warmup, ranks, sampler=None):
+def time_path(pa, precision, steps, warmup, ranks, sampler=None, **extra):
     import torch
 
     from scopi_b200 import ScopiSolver
     kw, dt = solver_kwargs()
-    s = ScopiSolver(pa, precision=precision, mixed_violation_tol=1e-6, device=ranks.local, **kw)
+    s = ScopiSolver(pa, precision=precision, mixed_violation_tol=1e-6, device=ranks.local, **kw, **extra)
     s.step(dt, warmup)
     stream = torch.cuda.ExternalStream(s.stream_handle(), device=ranks.local)
     torch.cuda.synchronize()
@@ -243,13 +244,10 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per APGD iteration per contact from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "apgd_dram_traffic.json")
-    if not os.path.exists(p):
-        return None
-    with open(p) as fh:
-        return json.load(fh)
+# DRAM bytes (read + write) per FP32 APGD iteration per contact of k_apgd_sph on the
+# 1M-sphere workload, from one ncu capture (profiles/apgd_sph_spheres_1m_traffic.md);
+# None until measured
+TRAFFIC_FP32_PER_CONTACT_ITERATION = None
 
 
 # ----------------------------------------------------------------------------- CPU legs
@@ -318,21 +316,110 @@ REF_APGD_ITERATIONS_DEFAULT = 497
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--side", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--workload", default="spheres_1m", choices=["spheres_1m", "piles"],
+                    help="spheres_1m: the headline line; piles: 256 pile scenes stepped as one batch")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 0)
+    if args.steps is None:
+        args.steps = 5 if args.workload == "spheres_1m" else 1000 - args.warmup
     ranks = Ranks(args.gpus)
     try:
         if args.impl == "reference":
             return reference_arm(args, ranks)
+        if args.workload == "piles":
+            return piles(args, ranks)
         return ours(args, ranks)
     finally:
         ranks.close()
+
+
+def piles(args, ranks):
+    """256 independent 2D pile scenes (200-5000 disks each, log-uniform) on a segment, all
+    stepped by one batch handle: one CUDA graph replay and one persistent APGD launch per
+    time step.  Steps 1..W warm up (graph capture), the next K are timed; with the
+    defaults that is the whole 1000-step run."""
+    import torch
+    from scopi_b200 import FP64, MIXED, ScopiBatch, configs
+    from scopi_b200.build import build
+    build()
+    st = configs.SETTINGS["pile_scenes"]
+    scenes = configs.pile_scenes(256)
+    kw = dict(dmax=st["dmax"], tolerance=st["tolerance"], max_ite=st["max_ite"])
+    n_disks = sum(s.n - s.nb_inactive for s in scenes)
+
+    def run(precision, sampler=None, **extra):
+        b = ScopiBatch(scenes, vap=st["vap"], precision=precision, device=ranks.local, mixed_violation_tol=1e-6,
+                       **kw, **extra)
+        b.run(st["dt"], args.warmup)
+        stream = torch.cuda.ExternalStream(b.stream_handle(), device=ranks.local)
+        torch.cuda.synchronize()
+        ranks.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        l0 = b.kernel_launches()
+        if sampler:
+            sampler.start()
+        viol, iters, contacts, conv = 0.0, [], [], True
+        e0.record(stream)
+        for _ in range(args.steps):
+            b.run(st["dt"], 1)
+            s = b.stats()
+            viol = max(viol, s["violation"])
+            iters.append(s["iterations"])
+            contacts.append(s["contacts"])
+            conv = conv and bool(s["converged"])
+        e1.record(stream)
+        e1.synchronize()
+        clocks = sampler.stop() if sampler else None
+        torch.cuda.synchronize()
+        ranks.barrier()
+        out = {"ms": ranks.max(e0.elapsed_time(e1)), "launches": b.kernel_launches() - l0, "clocks": clocks,
+               "violation_max": viol, "longest_scene_iterations_mean": statistics.mean(iters),
+               "contacts_mean": statistics.mean(contacts), "converged_all": conv, "block_threads": b.block_threads()}
+        b.close()
+        return out
+
+    sampler = ClockSampler(ranks.local)
+    mixed = run(MIXED, sampler)
+    f64 = None if args.no_fp64 else run(FP64)
+    abl = {}
+    if not args.no_fp64:
+        for name, prec, init in (("mixed_reference_start", MIXED, 0), ("fp64_curvature_start", FP64, 1)):
+            r = run(prec, initial_step=init)
+            abl[name] = {"value": ranks.world * args.steps * 1000.0 / r["ms"], "unit": UNIT,
+                         "violation_max": r["violation_max"],
+                         "longest_scene_iterations_mean": r["longest_scene_iterations_mean"]}
+    value = ranks.world * args.steps * 1000.0 / mixed["ms"]
+    line = {
+        "metric": "time steps/s of 256 independent 2D pile scenes (one batch, violation <= 1e-6)",
+        "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": mixed["ms"] / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 APGD iterations, f64 correction/geometry/integration", "data": "synthetic",
+        "config": {"workload": (f"pile_scenes: 256 scenes, {n_disks:,} disks in all (N_s = round(exp(U[ln 200, "
+                                f"ln 5000]))), r U[0.008,0.012], segment floor, gravity, NoFriction, vap_fpd, dmax "
+                                f"0.009, dt 1e-3, per-scene APGD tol 1e-6, steps {args.warmup + 1}.."
+                                f"{args.warmup + args.steps} of the run timed"),
+                   "precision": "mixed", "l2": "working set L2-resident; latency-bound (one CTA per scene)",
+                   "parallelism": f"replicas x{ranks.world}" if ranks.world > 1 else "single GPU"},
+        "fp64": ({"value": ranks.world * args.steps * 1000.0 / f64["ms"], "unit": UNIT,
+                  "mixed_over_fp64": f64["ms"] / mixed["ms"], "violation_max": f64["violation_max"],
+                  "longest_scene_iterations_mean": f64["longest_scene_iterations_mean"],
+                  "block_threads": f64["block_threads"]} if f64 else None),
+        "ablation": abl or None,
+        "solver": {k: mixed[k] for k in ("violation_max", "longest_scene_iterations_mean", "contacts_mean",
+                                        "converged_all", "block_threads")},
+        "clocks": mixed["clocks"], "gpu_launches": mixed["launches"],
+    }
+    if ranks.rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
 
 
 def ours(args, ranks):
@@ -348,6 +435,16 @@ def ours(args, ranks):
     sampler = ClockSampler(ranks.local)
     mixed = time_path(pa, MIXED, args.steps, args.warmup, ranks, sampler)
     f64 = None if args.no_fp64 else time_path(pa, FP64, args.steps, args.warmup, ranks)
+    # ablation: the two changes of the mixed form taken one at a time (FP32 iterations with
+    # the reference's first step; the curvature first step alone in FP64)
+    abl = {}
+    if not args.no_fp64:
+        for name, prec, init in (("mixed_reference_start", MIXED, 0), ("fp64_curvature_start", FP64, 1)):
+            r = time_path(pa, prec, args.steps, args.warmup, ranks, initial_step=init)
+            its = [p["fp32_iterations"] if prec == MIXED else p["iterations"] for p in r["per_step"]]
+            abl[name] = {"value": ranks.world * args.steps * 1000.0 / ranks.max(r["ms"]), "unit": UNIT,
+                         "iterations_per_step": statistics.mean(its),
+                         "violation_max": max(p["violation"] for p in r["per_step"])}
     e2e_ms, h2d, d2h = time_e2e(pa, MIXED, args.steps, args.warmup, ranks)
 
     ms = ranks.max(mixed["ms"])
@@ -365,20 +462,25 @@ def ours(args, ranks):
     it32 = sum(p["fp32_iterations"] for p in per)
     ms_apgd = sum(p["ms_apgd_kernel"] for p in per)
     b_iter32 = roofline_bytes_per_iter(C, n_active, 4)
-    b_iter32_full = roofline_bytes_per_iter(C, n_active, 4, torque_free=False)
+    b_iter32_tf = roofline_bytes_per_iter(C, n_active, 4, torque_free=True)
     achieved = (it32 * b_iter32) / (ms_apgd * 1e-3) / 1e9 if ms_apgd > 0 else None
+    achieved_tf = (it32 * b_iter32_tf) / (ms_apgd * 1e-3) / 1e9 if ms_apgd > 0 else None
     peak, peak_kind = measured_peaks()
-    traffic = None
-    prof = profiled_traffic()
-    if prof and it32:
-        traffic = prof.get("dram_bytes_per_iteration_per_contact_fp32", 0) * C * (it32 / max(1, len(per)))
+    # DRAM bytes of one APGD launch (one whole solve): ncu dram__bytes_read.sum +
+    # dram__bytes_write.sum per FP32 iteration per contact, times this run's contacts and
+    # iterations per launch
+    traffic = (TRAFFIC_FP32_PER_CONTACT_ITERATION * C * it32 / max(1, len(per))
+               if it32 and TRAFFIC_FP32_PER_CONTACT_ITERATION else None)
     f64_roof = None
     if f64:
         p64 = f64["per_step"]
         it64 = sum(p["iterations"] for p in p64)
         ms64 = sum(p["ms_apgd_kernel"] for p in p64)
         a64 = (it64 * roofline_bytes_per_iter(C, n_active, 8)) / (ms64 * 1e-3) / 1e9 if ms64 > 0 else None
+        a64_tf = ((it64 * roofline_bytes_per_iter(C, n_active, 8, torque_free=True)) / (ms64 * 1e-3) / 1e9
+                  if ms64 > 0 else None)
         f64_roof = {"achieved": a64, "peak": peak, "unit": "GB/s", "frac": (a64 / peak) if a64 else None,
+                    "achieved_streamed": a64_tf, "frac_streamed": (a64_tf / peak) if a64_tf else None,
                     "iterations_per_step": it64 / len(p64), "ms_apgd_per_step": ms64 / len(p64),
                     "violation_max": max(p["violation"] for p in p64)}
 
@@ -406,14 +508,17 @@ def ours(args, ranks):
                    "parallelism": f"replicas x{ranks.world}" if ranks.world > 1 else "single GPU"},
         "fp64": {"value": f64_val, "unit": UNIT, "mixed_over_fp64": (value / f64_val) if f64_val else None,
                  "roofline": f64_roof},
+        "ablation": abl or None,
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                      "peak_source": f"{peak_kind} hbm_gbs",
                      "kernel": "k_apgd_sph<float,3,NoFriction> (persistent, torque-free rows)",
                      "bytes_per_iteration": b_iter32,
-                     "achieved_full_row_formula": ((it32 * b_iter32_full) / (ms_apgd * 1e-3) / 1e9
-                                                   if ms_apgd > 0 else None),
+                     "achieved_streamed": achieved_tf,
+                     "frac_streamed": (achieved_tf / peak) if achieved_tf else None,
+                     "bytes_per_iteration_streamed": b_iter32_tf,
+                     "traffic_per_iteration": (traffic / (it32 / len(per))) if traffic else None,
                      "iterations_per_step": it32 / len(per),
                      "ms_apgd_per_step": ms_apgd / len(per)},
         "cpu_baseline": cpu,

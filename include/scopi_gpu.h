@@ -76,7 +76,18 @@ typedef struct scopi_gpu_params {
     double mixed_violation_tol;   /* MIXED: FP64 constraint violation the outer correction must reach */
     int32_t mixed_max_corrections;/* MIXED: FP32 correction solves after the first one */
     int32_t device;               /* CUDA device ordinal */
+    int32_t initial_step;         /* SCOPI_GPU_STEP_AUTO / _REFERENCE / _CURVATURE (below) */
 } scopi_gpu_params;
+
+/* First APGD step of every solve.  REFERENCE: alpha as given (apgd.hpp:120, the
+   reference's fixed 0.05), grown by 1/0.97 per accepted iteration.  CURVATURE: 1/L with
+   L = 1.5 x the Rayleigh quotient d^T Q d / |d|^2 along the first projected-gradient
+   direction d (one extra particle pass per solve); torque-free and batched kernels only,
+   the 6-dof kernel (Friction) keeps alpha.  AUTO: REFERENCE for FP64 (the drop-in, same
+   iterates as the reference), CURVATURE for MIXED. */
+#define SCOPI_GPU_STEP_AUTO (-1)
+#define SCOPI_GPU_STEP_REFERENCE 0
+#define SCOPI_GPU_STEP_CURVATURE 1
 
 typedef struct scopi_gpu_particles {
     int64_t n;           /* bodies */

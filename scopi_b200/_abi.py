@@ -34,6 +34,7 @@ class Params(C.Structure):
         ("kd_tree_radius", C.c_double), ("alpha", C.c_double), ("tolerance", C.c_double), ("mu", C.c_double),
         ("gamma", C.c_double), ("gamma_min", C.c_double), ("gamma_tol", C.c_double),
         ("mixed_violation_tol", C.c_double), ("mixed_max_corrections", C.c_int32), ("device", C.c_int32),
+        ("initial_step", C.c_int32),
     ]
 
 

@@ -148,8 +148,12 @@ def spheres_1m(seed: int = 5, side: int = 100) -> ParticleArrays:
     return _assemble(3, c, r, m, jm, vd=vd)
 
 
-def pile_scene(seed: int, nmin: int = 200, nmax: int = 5000) -> ParticleArrays:
-    """One pile scene.  Draws: u[0] -> N_s; candidate k uses (x, y, r) = u[1+3k], u[2+3k], u[3+3k]."""
+def pile_scene(seed: int, nmin: int = 200, nmax: int = 5000, vmax: float = 0.0) -> ParticleArrays:
+    """One pile scene.  Draws: u[0] -> N_s; candidate k uses (x, y, r) = u[1+3k], u[2+3k], u[3+3k].
+
+    vmax > 0 gives the disks initial velocities U[-vmax, vmax]^2 (draws 2k, 2k+1 of
+    SplitMix64(seed + 0x5851F42D), disk k in placement order), so that neighbours approach
+    each other and the first steps already have active constraints (tests, profiles)."""
     from .container import Particles, Property
     n_draw = 1 + 3 * 16 * nmax
     u = splitmix_uniform(seed, n_draw)
@@ -185,15 +189,19 @@ def pile_scene(seed: int, nmin: int = 200, nmax: int = 5000) -> ParticleArrays:
             grid.setdefault((ci, cj), []).append((x, y, r))
     p = Particles(2)
     p.add_segment((0.0, 0.0), (W, 0.0))
-    for x, y, r in placed:
+    vel = (2.0 * splitmix_uniform(seed + 0x5851F42D, 2 * len(placed)).reshape(-1, 2) - 1.0) * vmax
+    for k, (x, y, r) in enumerate(placed):
         m = (r / 0.01) ** 2
-        p.add_sphere((x, y), r, Property(mass=m, moment_inertia=0.5 * m * r * r, force=(0.0, -9.81 * m)))
+        prop = Property(mass=m, moment_inertia=0.5 * m * r * r, force=(0.0, -9.81 * m))
+        if vmax > 0.0:
+            prop.velocity = (float(vel[k, 0]), float(vel[k, 1]))
+        p.add_sphere((x, y), r, prop)
     return p.finalize()
 
 
-def pile_scenes(n_scenes: int = 256, seed: int = 4, nmin: int = 200, nmax: int = 5000):
+def pile_scenes(n_scenes: int = 256, seed: int = 4, nmin: int = 200, nmax: int = 5000, vmax: float = 0.0):
     """The batched workload: scene s is pile_scene(seed * 1000 + s)."""
-    return [pile_scene(seed * 1000 + s, nmin, nmax) for s in range(n_scenes)]
+    return [pile_scene(seed * 1000 + s, nmin, nmax, vmax) for s in range(n_scenes)]
 
 
 # solver settings per workload (dmax, dt, tolerance, max_ite, vap)

@@ -391,6 +391,7 @@ __global__ void __launch_bounds__(kApgdThreads) k_apgd(ApgdArgs<T> A) {
     int jl = 0, jp = 1, jn = 2;    // u of the same three
     double alpha = A.alpha;
     double lipsch = 1.0 / alpha;
+    double lgood = lipsch;         // last finite estimate of an accepted iteration
     double theta = 1.0;
     double beta = 0.0;
     bool use_prev = false;         // beta != 0
@@ -437,6 +438,7 @@ __global__ void __launch_bounds__(kApgdThreads) k_apgd(ApgdArgs<T> A) {
         }
         ++ite;
         bt = false;
+        if (isfinite(lipsch)) lgood = lipsch;
         last_step = sqrt(t[4]);
         double tol = A.tol;
         if (sizeof(T) == 4) {
@@ -472,6 +474,7 @@ __global__ void __launch_bounds__(kApgdThreads) k_apgd(ApgdArgs<T> A) {
         A.result->u_buf = jl;
         A.result->error = err;
         A.result->last_step = last_step;
+        A.result->lipsch = lgood;
     }
 }
 

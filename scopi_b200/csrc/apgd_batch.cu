@@ -61,10 +61,11 @@ struct BatchArgs {
     long long max_ite;
     int dynamic;
     int max_corrections;
+    int curvature_start;
 };
 
 struct BState {
-    double alpha, lipsch, theta, beta, beta_n, theta1, Fy, last_step;
+    double alpha, lipsch, theta, beta, beta_n, theta1, Fy, last_step, lgood;
     double tk[4];
     long long ite, nbt, nrs;
     int il, ip, in_, jL, jN, jY, jYN, bt, use_prev, restart, done, conv;
@@ -80,12 +81,15 @@ __device__ __forceinline__ int scene_contact(int k, int o0, int n0, int a0) { re
 
 // One APGD solve of the scene on the T data; `shift` (FP64 lambda so far) turns it into the
 // correction problem.  Returns in S the iteration counts; the result is lam[S.il], u[S.jL].
-template <typename T, int DIM>
+// KB independent contacts / incidence records per thread are in flight: the passes are
+// bound by the latency of dependent L2 gathers, not by bandwidth.
+template <typename T, int DIM, int KB>
 __device__ void solve_scene(const BatchArgs<T>& A, BState& S, int o0, int n0, int a0, int nct, int p0, int p1,
-                            const double* shift) {
+                            const double* shift, double alpha0) {
     if (threadIdx.x == 0) {
-        S.alpha = A.alpha;
-        S.lipsch = 1.0 / A.alpha;
+        S.alpha = alpha0;
+        S.lipsch = 1.0 / alpha0;
+        S.lgood = S.lipsch;
         S.theta = 1.0;
         S.beta = 0.0;
         S.beta_n = 0.0;
@@ -112,6 +116,41 @@ __device__ void solve_scene(const BatchArgs<T>& A, BState& S, int o0, int n0, in
         bst4(A.u[2] + p, (T)0, (T)0, (T)0);
     }
     __syncthreads();
+    const int nt = blockDim.x;
+    if (A.curvature_start) {
+        // initial step from the curvature along the first descent direction d (kept in the
+        // candidate buffer, which the first contact pass overwrites)
+        T* dbuf = A.lam[2];
+        double r2[2] = {0.0, 0.0};
+        for (int k = threadIdx.x; k < nct; k += nt) {
+            const int c = scene_contact(k, o0, n0, a0);
+            const T d = first_descent<T>(bld4(A.nc + c).w, shift, c);
+            dbuf[c] = d;
+            r2[0] += (double)d * (double)d;
+        }
+        __syncthreads();
+        for (int p = p0 + threadIdx.x; p < p1; p += nt) {
+            T w0 = 0, w1 = 0, w2 = 0;
+            for (int k = A.inc_ptr[p]; k < A.inc_ptr[p + 1]; ++k) {
+                const V4<T> e = bld4(A.inc + k);
+                const T mu = dbuf[bidx(e.w)];
+                w0 += mu * e.x;
+                w1 += mu * e.y;
+                if (DIM == 3) w2 += mu * e.z;
+            }
+            r2[1] += A.invm[4 * (long long)p] * ((double)w0 * w0 + (double)w1 * w1 + (double)w2 * w2);
+        }
+        block_reduce_t0<2>(r2);
+        if (threadIdx.x == 0) {
+            double l;
+            if (initial_lipschitz(r2[0], r2[1], A.dt2, l)) {
+                S.lipsch = l;
+                S.alpha = 1.0 / l;
+                S.lgood = l;
+            }
+        }
+        __syncthreads();
+    }
     for (;;) {
         const double alpha = S.alpha;
         const bool bt = S.bt != 0, use_prev = S.use_prev != 0;
@@ -121,44 +160,64 @@ __device__ void solve_scene(const BatchArgs<T>& A, BState& S, int o0, int n0, in
         T* lnew = A.lam[S.in_];
         const V4<T>* uY = A.u[S.jY];
         double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        for (int k = threadIdx.x; k < nct; k += blockDim.x) {
-            const int c = scene_contact(k, o0, n0, a0);
-            const int2 ij = A.cij[c];
-            const V4<T> n = bld4(A.nc + c);
-            T qy = 0;
-            if (ij.x >= A.nin) {
-                const V4<T> ui = bld4(uY + (ij.x - A.nin));
-                qy += n.x * ui.x + n.y * ui.y + (DIM == 3 ? n.z * ui.z : (T)0);
+        for (int kb = threadIdx.x; kb < nct; kb += KB * nt) {
+            int c[KB];
+            int2 ij[KB];
+            V4<T> n[KB];
+            T lm[KB], lq[KB], qy[KB];
+#pragma unroll
+            for (int q = 0; q < KB; ++q) {
+                const int k = kb + q * nt;
+                c[q] = k < nct ? scene_contact(k, o0, n0, a0) : -1;
+                ij[q] = make_int2(-1, -1);
+                if (c[q] >= 0) {
+                    ij[q] = A.cij[c[q]];
+                    n[q] = bld4(A.nc + c[q]);
+                    lm[q] = lam[c[q]];
+                    lq[q] = use_prev ? lprev[c[q]] : (T)0;
+                }
             }
-            if (ij.y >= A.nin) {
-                const V4<T> uj = bld4(uY + (ij.y - A.nin));
-                qy -= n.x * uj.x + n.y * uj.y + (DIM == 3 ? n.z * uj.z : (T)0);
+#pragma unroll
+            for (int q = 0; q < KB; ++q) {
+                qy[q] = (T)0;
+                if (c[q] < 0) continue;
+                if (ij[q].x >= A.nin) {
+                    const V4<T> ui = bld4(uY + (ij[q].x - A.nin));
+                    qy[q] += n[q].x * ui.x + n[q].y * ui.y + (DIM == 3 ? n[q].z * ui.z : (T)0);
+                }
+                if (ij[q].y >= A.nin) {
+                    const V4<T> uj = bld4(uY + (ij[q].y - A.nin));
+                    qy[q] -= n[q].x * uj.x + n[q].y * uj.y + (DIM == 3 ? n[q].z * uj.z : (T)0);
+                }
             }
-            qy *= (T)A.dt2;
-            const T lm = lam[c];
-            const T y = use_prev ? lm + beta * (lm - lprev[c]) : lm;
-            const T gm = qy + n.w;
-            T lp;
-            if (shift) {
-                const double sh = shift[c];
-                double z = sh + ((double)y - alpha * (double)gm);
-                z = z > 0.0 ? z : 0.0;
-                lp = (T)(z - sh);
-            } else {
-                const T z = y - (T)alpha * gm;
-                lp = z > (T)0 ? z : (T)0;
+#pragma unroll
+            for (int q = 0; q < KB; ++q) {
+                if (c[q] < 0) continue;
+                const T qq = qy[q] * (T)A.dt2;
+                const T y = use_prev ? lm[q] + beta * (lm[q] - lq[q]) : lm[q];
+                const T gm = qq + n[q].w;
+                T lp;
+                if (shift) {
+                    const double sh = shift[c[q]];
+                    double z = sh + ((double)y - alpha * (double)gm);
+                    z = z > 0.0 ? z : 0.0;
+                    lp = (T)(z - sh);
+                } else {
+                    const T z = y - (T)alpha * gm;
+                    lp = z > (T)0 ? z : (T)0;
+                }
+                lnew[c[q]] = lp;
+                const double dly = (double)lp - (double)y, dll = (double)lp - (double)lm[q];
+                s[0] += (double)gm * dly;
+                s[1] += dly * dly;
+                s[2] += (double)n[q].w * (double)lp;
+                if (!bt) s[3] += (double)y * (0.5 * (double)qq + (double)n[q].w);
+                s[4] += dll * dll;
+                s[5] += (double)gm * dll;
+                s[6] += (double)lp * (double)lp;
             }
-            lnew[c] = lp;
-            const double dly = (double)lp - (double)y, dll = (double)lp - (double)lm;
-            s[0] += (double)gm * dly;
-            s[1] += dly * dly;
-            s[2] += (double)n.w * (double)lp;
-            if (!bt) s[3] += (double)y * (0.5 * (double)qy + (double)n.w);
-            s[4] += dll * dll;
-            s[5] += (double)gm * dll;
-            s[6] += (double)lp * (double)lp;
         }
-        block_sum<8>(s);
+        block_reduce_t0<8>(s);
         if (threadIdx.x == 0) {
             const double th = S.theta;
             S.theta1 = 0.5 * (th * sqrt(4 + th * th) - th * th);
@@ -176,30 +235,47 @@ __device__ void solve_scene(const BatchArgs<T>& A, BState& S, int o0, int n0, in
         V4<T>* uN = A.u[S.jN];
         V4<T>* uYN = A.u[S.jYN];
         const T bn_ = (T)S.beta_n;
-        double sw = 0.0;
-        for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+        double sw = 0.0, sq = 0.0;
+        for (int p = p0 + threadIdx.x; p < p1; p += nt) {
+            V4<T> ul, uy;
+            if (bn_ != (T)0) ul = bld4(uL + p);
+            if (sizeof(T) == 4) uy = bld4(uY + p);
             T w0 = 0, w1 = 0, w2 = 0;
-            const int k1 = A.inc_ptr[p + 1];
-            for (int k = A.inc_ptr[p]; k < k1; ++k) {
-                const V4<T> e = bld4(A.inc + k);
-                const T mu = lnew[bidx(e.w)];
-                w0 += mu * e.x;
-                w1 += mu * e.y;
-                if (DIM == 3) w2 += mu * e.z;
+            const int k0 = A.inc_ptr[p], k1 = A.inc_ptr[p + 1];
+            for (int kb = k0; kb < k1; kb += KB) {
+                V4<T> e[KB];
+                T mu[KB];
+#pragma unroll
+                for (int q = 0; q < KB; ++q)
+                    if (kb + q < k1) e[q] = bld4(A.inc + kb + q);
+#pragma unroll
+                for (int q = 0; q < KB; ++q) mu[q] = kb + q < k1 ? lnew[bidx(e[q].w)] : (T)0;
+#pragma unroll
+                for (int q = 0; q < KB; ++q) {
+                    if (kb + q >= k1) continue;
+                    w0 += mu[q] * e[q].x;
+                    w1 += mu[q] * e[q].y;
+                    if (DIM == 3) w2 += mu[q] * e[q].z;
+                }
             }
             const T im = (T)A.invm[4 * (long long)p];
             const T v0 = im * w0, v1 = im * w1, v2 = im * w2;
             bst4(uN + p, v0, v1, v2);
             sw += (double)w0 * (double)v0 + (double)w1 * (double)v1 + (double)w2 * (double)v2;
+            if (sizeof(T) == 4) {
+                // m |u(l+) - u(y)|^2: the curvature d^T Q d / dt^2 along d = l+ - y
+                const double d0 = (double)v0 - (double)uy.x, d1 = (double)v1 - (double)uy.y,
+                             d2 = (double)v2 - (double)uy.z;
+                sq += (d0 * d0 + d1 * d1 + d2 * d2) / (double)im;
+            }
             if (bn_ != (T)0) {
-                const V4<T> ul = bld4(uL + p);
                 bst4(uYN + p, v0 + bn_ * (v0 - ul.x), v1 + bn_ * (v1 - ul.y), v2 + bn_ * (v2 - ul.z));
             } else {
                 bst4(uYN + p, v0, v1, v2);
             }
         }
-        double sw1[1] = {sw};
-        block_sum<1>(sw1);
+        double sw1[2] = {sw, sq};
+        block_reduce_t0<2>(sw1);
         if (threadIdx.x == 0) {
             const double F_lp = 0.5 * A.dt2 * sw1[0] + S.tk[2];
             bool accept = true;
@@ -210,7 +286,8 @@ __device__ void solve_scene(const BatchArgs<T>& A, BState& S, int o0, int n0, in
                 S.lipsch = lip;
                 S.alpha = al;
                 S.nbt = nbt;
-            } else if (A.dynamic && F_lp >= S.Fy + S.tk[0] + 0.5 * S.lipsch * S.tk[1]) {
+            } else if (A.dynamic &&
+                       sufficient_decrease_fails<T>(F_lp, S.Fy, S.tk[0], S.tk[1], A.dt2 * sw1[1], S.lipsch)) {
                 S.lipsch *= 2;
                 S.alpha = 1. / S.lipsch;
                 S.bt = 1;
@@ -220,6 +297,7 @@ __device__ void solve_scene(const BatchArgs<T>& A, BState& S, int o0, int n0, in
             if (accept) {
                 ++S.ite;
                 S.bt = 0;
+                if (isfinite(S.lipsch)) S.lgood = S.lipsch;
                 S.last_step = sqrt(S.last_step);
                 double tol = A.tol;
                 if (sizeof(T) == 4) {
@@ -299,8 +377,16 @@ __device__ double residual_scene(const BatchArgs<T>& A, int o0, int n0, int a0, 
     return m;
 }
 
+// Two CTAs per SM at 256 and 512 threads (all 256 scenes of the benchmark batch resident
+// at once on 148 SMs), one at 1024; loads in flight per thread chosen to fit the registers.
+template <int BT>
+struct BatchKB {
+    static constexpr int value = BT <= 256 ? 4 : 1;
+    static constexpr int min_blocks = BT <= 512 ? 2 : 1;
+};
+
 template <typename T, int DIM, int BT>
-__global__ void __launch_bounds__(BT) k_apgd_batch(BatchArgs<T> A) {
+__global__ void __launch_bounds__(BT, BatchKB<BT>::min_blocks) k_apgd_batch(BatchArgs<T> A) {
     if (A.sizes->overflow) return;  // the step is redone after the buffers grow
     __shared__ BState S;
     const int scene = A.order[blockIdx.x];
@@ -311,7 +397,7 @@ __global__ void __launch_bounds__(BT) k_apgd_batch(BatchArgs<T> A) {
     int corr = 0, conv = 1;
     double viol = 0.0;
     if (nct > 0) {
-        solve_scene<T, DIM>(A, S, o0, n0, a0, nct, p0, p1, nullptr);
+        solve_scene<T, DIM, BatchKB<BT>::value>(A, S, o0, n0, a0, nct, p0, p1, nullptr, A.alpha);
         iters += S.ite;
         nbt += S.nbt;
         nrs += S.nrs;
@@ -331,8 +417,10 @@ __global__ void __launch_bounds__(BT) k_apgd_batch(BatchArgs<T> A) {
             for (;;) {
                 viol = residual_scene<T, DIM>(A, o0, n0, a0, nct, p0, p1, true);
                 if (viol <= A.viol_tol || corr >= A.max_corrections) break;
+                // the correction starts from the step size the previous solve ended with
+                const double a_next = 1.0 / S.lgood;
                 __syncthreads();
-                solve_scene<T, DIM>(A, S, o0, n0, a0, nct, p0, p1, A.lam64);
+                solve_scene<T, DIM, BatchKB<BT>::value>(A, S, o0, n0, a0, nct, p0, p1, A.lam64, a_next);
                 iters += S.ite;
                 f32 += S.ite;
                 nbt += S.nbt;
@@ -433,6 +521,7 @@ cudaError_t launch_apgd_batch(int dim, int block_threads, const BatchSolve<T>& b
     A.max_ite = b.max_ite;
     A.dynamic = b.dynamic;
     A.max_corrections = b.max_corrections;
+    A.curvature_start = b.curvature_start;
 #define LB(D, B) \
     if (dim == D && block_threads == B) return launch_bt<T, D, B>(A, n_scenes, s);
     LB(2, 256) LB(2, 512) LB(2, 1024) LB(3, 256) LB(3, 512) LB(3, 1024)

@@ -79,6 +79,32 @@ __device__ __forceinline__ void block_sum(double* v) {
     __syncthreads();
 }
 
+// Block sum whose result only thread 0 needs (it is in thread 0's v[] on return): one
+// block barrier.  The caller synchronises the block before the next call, which reuses
+// the staging array.  Fixed summation order (deterministic).
+template <int NP>
+__device__ __forceinline__ void block_reduce_t0(double* v) {
+    __shared__ double sh[NP][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+        double x = v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) sh[k][warp] = x;
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+            double x = lane < nw ? sh[k][lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            v[k] = x;
+        }
+    }
+}
+
 // Every block sums the per-block partials part[b*stride + k] (b < nb) in the same order.
 template <int NP>
 __device__ __forceinline__ void grid_sum(const double* part, unsigned int nb, int stride, double* t) {
@@ -109,6 +135,40 @@ __device__ __forceinline__ void cone_project(double* l, const double* n, double 
             for (int d = 0; d < DIM; ++d) l[d] = nn * (lt[d] / nrm) + nln * n[d];
         }
     }
+}
+
+// Backtracking test of apgd.hpp:172-182, F(l+) >= F(y) + g(y).d + L/2 |d|^2 with d = l+ - y.
+// FP64 evaluates it as the reference does.  For a quadratic F the test is exactly
+// d^T Q d >= L |d|^2; FP32 iterations use that form (dQd = dt^2 sum_p m |u(l+) - u(y)|^2),
+// since F(l+) - F(y) in FP32 carries round-off of the size of F itself and fails the
+// test spuriously once the steps are small, which collapses alpha and stalls the solve.
+template <typename T>
+__device__ __forceinline__ bool sufficient_decrease_fails(double F_lp, double Fy, double gd, double dd, double dQd,
+                                                          double lipsch) {
+    if (sizeof(T) == 4) return dQd >= lipsch * dd;
+    return F_lp >= Fy + gd + 0.5 * lipsch * dd;
+}
+
+// First projected-gradient direction of a solve at its cold start (lambda = 0, or delta = 0
+// for a correction with offset `shift`): d = -g where the bound lets it move.  The
+// Rayleigh quotient d^T Q d / |d|^2 then sets the initial step (see the kernels).
+template <typename T>
+__device__ __forceinline__ T first_descent(T g, const double* shift, long long m) {
+    if (shift) return (shift[m] > 0.0 || g < (T)0) ? -g : (T)0;
+    return g < (T)0 ? -g : (T)0;
+}
+// Initial Lipschitz estimate: 1.5 x the curvature along d (d^T Q d = dt^2 sum_p
+// w_p . M^-1 w_p with w = B^T d).  The reference starts every solve from the fixed
+// alpha = 0.05 (apgd.hpp:120) and grows it by 1/0.97 per accepted iteration; for the
+// problems here 1/L is many orders of magnitude larger, so most of its iterations are
+// that ramp, and its first step alpha*|g| can fall below the tolerance so that the solve
+// stops at once with a resting contact still open by ~ g dt^2.
+__device__ __forceinline__ bool initial_lipschitz(double dd, double wmw, double dt2, double& lipsch) {
+    if (!(dd > 0.0) || !(wmw > 0.0)) return false;
+    const double l = 1.5 * dt2 * wmw / dd;
+    if (!isfinite(l) || !(l > 0.0)) return false;
+    lipsch = l;
+    return true;
 }
 
 // l+ == y bit for bit: the reference compares F(l+) >= F(y) on identical vectors, doubles

@@ -71,6 +71,7 @@ struct SphArgs {
     double alpha, tol, dt2;
     long long max_ite;
     int dynamic;
+    int curvature_start;
 };
 
 template <typename T>
@@ -113,7 +114,7 @@ __device__ __forceinline__ void mult_update(const SphArgs<T>& A, long long m, T 
 // Loop-carried scalars of the iteration (block-uniform) live in shared memory and are
 // updated by thread 0, so the registers go to the two passes.
 struct SphState {
-    double alpha, lipsch, theta, beta, beta_n, theta1, Fy, last_step;
+    double alpha, lipsch, theta, beta, beta_n, theta1, Fy, last_step, lgood;
     long long ite, nbt, nrs;
     int il, ip, in_, jL, jN, jY, jYN, parity, bt, use_prev, restart, done, conv, err;
 };
@@ -132,6 +133,7 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
     if (threadIdx.x == 0) {
         S.alpha = A.alpha;
         S.lipsch = 1.0 / A.alpha;
+        S.lgood = S.lipsch;
         S.theta = 1.0;
         S.beta = 0.0;
         S.beta_n = 0.0;
@@ -152,7 +154,71 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
     __syncthreads();
     const int C = A.sizes->C;
     const unsigned int nb = gridDim.x;
+    if (A.curvature_start) {
+        // initial step from the curvature along the first descent direction d (stored in
+        // the candidate buffer, which the first contact pass overwrites); partial-sum
+        // regions 1 and 3 are first reused by the second iteration, after two barriers
+        T* dbuf = A.lam2;
+        double a2[2] = {0.0, 0.0};
+        GRID_STRIDE(c, C) {
+            const T cc = ld4(A.nc + c).w;
+            const T d = first_descent<T>(cc, A.shift, c);
+            dbuf[c] = d;
+            a2[0] += (double)d * (double)d;
+            if (PROB == kViscous) {
+                const int sl = A.slot[c];
+                if (sl >= 0) {
+                    const T d2 = first_descent<T>(-cc, A.shift, sl);
+                    dbuf[sl] = d2;
+                    a2[0] += (double)d2 * (double)d2;
+                }
+            }
+        }
+        block_sum<2>(a2);
+        if (threadIdx.x == 0) A.partials[(size_t)1 * nb * 8 + blockIdx.x * 8] = a2[0];
+        bool ok = grid_barrier(A.bar, nb);
+        double wm[2] = {0.0, 0.0};
+        if (ok) GRID_STRIDE(p, A.na) {
+            T w0 = 0, w1 = 0, w2 = 0;
+            for (int k = A.inc_ptr[p]; k < A.inc_ptr[p + 1]; ++k) {
+                const V4<T> e = ld4(A.inc + k);
+                const int ci = idx_of(e.w);
+                T mu = __ldcg(dbuf + ci);
+                if (PROB == kViscous) {
+                    const int sl = A.slot[ci];
+                    if (sl >= 0) mu -= __ldcg(dbuf + sl);
+                }
+                w0 += mu * e.x;
+                w1 += mu * e.y;
+                if (DIM == 3) w2 += mu * e.z;
+            }
+            const double im = A.invm[4 * (long long)p];
+            wm[0] += im * ((double)w0 * w0 + (double)w1 * w1 + (double)w2 * w2);
+        }
+        block_sum<2>(wm);
+        if (threadIdx.x == 0) A.partials[(size_t)3 * nb * 8 + blockIdx.x * 8] = wm[0];
+        if (ok) ok = grid_barrier(A.bar, nb);
+        double t1[1] = {0.0}, t3[1] = {0.0};
+        if (ok) {
+            grid_sum<1>(A.partials + (size_t)1 * nb * 8, nb, 8, t1);
+            grid_sum<1>(A.partials + (size_t)3 * nb * 8, nb, 8, t3);
+        }
+        if (threadIdx.x == 0) {
+            double l;
+            if (ok && initial_lipschitz(t1[0], t3[0], A.dt2, l)) {
+                S.lipsch = l;
+                S.alpha = 1.0 / l;
+                S.lgood = l;
+            }
+            if (!ok) {
+                S.err = 1;
+                S.done = 1;
+            }
+        }
+        __syncthreads();
+    }
     for (;;) {
+        if (S.done) break;
         const double alpha = S.alpha;
         const bool bt = S.bt != 0, use_prev = S.use_prev != 0;
         const T beta = (T)S.beta;
@@ -217,7 +283,7 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
             V4<T>* uN = pick4(S.jN, A.u0, A.u1, A.u2, A.u3);
             V4<T>* uYN = pick4(S.jYN, A.u0, A.u1, A.u2, A.u3);
             const T bn_ = (T)S.beta_n;
-            double sw = 0.0;
+            double sw = 0.0, sq = 0.0;
             // one body per thread; its incidence records, then the l+ gathers they index,
             // are issued in batches so several loads are in flight per thread
             constexpr int KB = 4;
@@ -259,6 +325,13 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
                 const T n0 = im * w0, n1 = im * w1, n2 = im * w2;
                 st4(uN + p, n0, n1, n2);
                 sw += (double)w0 * (double)n0 + (double)w1 * (double)n1 + (double)w2 * (double)n2;
+                if (sizeof(T) == 4) {
+                    // m |u(l+) - u(y)|^2: the curvature d^T Q d / dt^2 along d = l+ - y
+                    const V4<T> uy = ld4cg(uY + p);
+                    const double d0 = (double)n0 - (double)uy.x, d1 = (double)n1 - (double)uy.y,
+                                 d2 = (double)n2 - (double)uy.z;
+                    sq += (d0 * d0 + d1 * d1 + d2 * d2) / (double)im;
+                }
                 if (bn_ != (T)0) {
                     const V4<T> ul = ld4(uL + p);
                     st4(uYN + p, n0 + bn_ * (n0 - ul.x), n1 + bn_ * (n1 - ul.y), n2 + bn_ * (n2 - ul.z));
@@ -266,15 +339,18 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
                     st4(uYN + p, n0, n1, n2);
                 }
             }
-            double sw8[1] = {sw};
-            block_sum<1>(sw8);
-            if (threadIdx.x == 0) part2[blockIdx.x * 8] = sw8[0];
+            double sw8[2] = {sw, sq};
+            block_sum<2>(sw8);
+            if (threadIdx.x == 0) {
+                part2[blockIdx.x * 8] = sw8[0];
+                part2[blockIdx.x * 8 + 1] = sw8[1];
+            }
             if (!grid_barrier(A.bar, nb)) {
                 if (threadIdx.x == 0) S.err = 1;
                 break;
             }
-            double t6[1];
-            grid_sum<1>(part2, nb, 8, t6);
+            double t6[2];
+            grid_sum<2>(part2, nb, 8, t6);
             if (threadIdx.x == 0) {
                 S.parity ^= 1;
                 const double F_lp = 0.5 * A.dt2 * t6[0] + tk[2];
@@ -286,7 +362,8 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
                     S.lipsch = lip;
                     S.alpha = al;
                     S.nbt = nbt;
-                } else if (A.dynamic && F_lp >= S.Fy + tk[0] + 0.5 * S.lipsch * tk[1]) {
+                } else if (A.dynamic && sufficient_decrease_fails<T>(F_lp, S.Fy, tk[0], tk[1], A.dt2 * t6[1],
+                                                                      S.lipsch)) {
                     S.lipsch *= 2;  // backtracking, apgd.hpp:172-182
                     S.alpha = 1. / S.lipsch;
                     S.bt = 1;
@@ -296,6 +373,7 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
                 if (accept) {
                     ++S.ite;
                     S.bt = 0;
+                    if (isfinite(S.lipsch)) S.lgood = S.lipsch;
                     S.last_step = sqrt(S.last_step);
                     double tol = A.tol;
                     if (sizeof(T) == 4) {
@@ -335,6 +413,7 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
         A.result->u_buf = S.jL;
         A.result->error = S.err;
         A.result->last_step = S.last_step;
+        A.result->lipsch = S.lgood;
     }
 }
 
@@ -496,6 +575,7 @@ cudaError_t launch_apgd_sph(int nin, int na, int dim, int problem, const ApgdSet
     A.dt2 = st.dt * st.dt;
     A.max_ite = st.max_ite;
     A.dynamic = st.dynamic;
+    A.curvature_start = st.curvature_start;
 #define LA(D, P) \
     if (dim == D && problem == P) return launch_t<T, D, P>(A, nblocks, s);
     LA(2, 0) LA(2, 2) LA(3, 0) LA(3, 2)
@@ -740,6 +820,7 @@ extern "C" int32_t scopi_gpu_apgd_noalloc(int32_t dim, int64_t n_active, int64_t
     A.dt2 = dt * dt;
     A.max_ite = max_ite;
     A.dynamic = dynamic_descent ? 1 : 0;
+    A.curvature_start = 0;
     int maxb = apgd_sph_max_blocks(kNoFriction, dim, false);
     if (maxb > kNoAllocMaxBlocks) maxb = kNoAllocMaxBlocks;
     const int thr = SphOcc<double>::threads;

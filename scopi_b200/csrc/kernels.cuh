@@ -95,6 +95,7 @@ struct ApgdSettings {
     int dynamic;
     double dt;
     double mu;
+    int curvature_start;      // first step from the curvature estimate instead of alpha
 };
 
 struct ApgdResult {           // written by block 0 of the persistent kernel
@@ -106,7 +107,7 @@ struct ApgdResult {           // written by block 0 of the persistent kernel
     int u_buf;                // which u buffer holds M^-1 B^T lambda of the result
     int error;                // barrier timeout
     double last_step;
-    double pad;
+    double lipsch;            // Lipschitz estimate of the last accepted iteration (finite)
 };
 
 template <typename T>
@@ -235,6 +236,7 @@ struct BatchSolve {
     long long max_ite;
     int dynamic;
     int max_corrections;
+    int curvature_start;
 };
 
 long long apgd_batch_launches();

@@ -19,6 +19,11 @@ namespace {
 // message of the last failing call that has no handle (fixed buffer: setting it allocates nothing)
 thread_local char g_global_error[512] = "";
 
+// batched scenes: threads per scene until the autotuner has run, and the longest scene
+// solve (APGD iterations) of the step whose problem it is tuned on
+constexpr int kBatchDefaultThreads = 512;
+constexpr long long kBatchTuneIterations = 64;
+
 struct DevMem {
     std::vector<void*> ptrs;
     ~DevMem() { release(); }
@@ -160,12 +165,14 @@ struct scopi_gpu_handle {
     BatchSceneStats* d_bstats = nullptr;
     std::vector<BatchSceneStats> h_bstats;
     double* d_obs_snap = nullptr;  // obstacle pos (3) and q (4) before the step, restored on overflow
-    int batch_threads = 0;         // block size chosen by the autotuner
+    int batch_threads = 0;         // block size chosen by the autotuner or pinned (0 = not yet)
+    int batch_bt_used = 0;         // block size of the last step
     float batch_tune_ms[3] = {0, 0, 0};
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     double graph_dt = 0.0;
     long long graph_cap = -1;
+    int graph_bt = 0;
     long long graph_kernels = 0;   // kernels one replay of `graph_exec` launches
     long long replayed = 0;        // kernels launched by graph replays so far
     long long cell_cap_hint = 0;   // cell-list capacity wanted by the batch layout
@@ -233,6 +240,7 @@ struct scopi_gpu_handle {
             bs.max_ite = P.max_ite;
             bs.dynamic = P.dynamic_descent;
             bs.max_corrections = P.mixed_max_corrections;
+            bs.curvature_start = curvature_start();
         };
         if (mixed()) {
             BatchSolve<float> bs{};
@@ -296,53 +304,22 @@ struct scopi_gpu_handle {
         stats.status = stats.converged ? 0 : SCOPI_GPU_ENOCONV;
     }
 
-    // One time step of every scene: eager with block-size autotuning the first time, then
-    // one CUDA graph replay per step.
+    // One time step of every scene: one CUDA graph replay (captured on the first step and
+    // again whenever dt, the contact capacity or the block size changes).  Autotuning: the
+    // steps run with 512 threads per scene until the first step whose longest scene solve
+    // takes >= 64 iterations (the first steps of a falling pile converge in one); that
+    // step's contact problem is then re-solved with 256, 512 and 1024 threads per scene
+    // and the fastest is kept for the rest of the run.
     int step_batch(double dt) {
         for (int attempt = 0; attempt < 4; ++attempt) {
+            const int bt = batch_threads ? batch_threads : kBatchDefaultThreads;
             cudaEventRecord(ev[0], stream);
-            if (!batch_threads) {
-                // autotune: time the batched solve at 256, 512 and 1024 threads per scene on
-                // this step's problem (each run is a full cold-start solve), keep the fastest
-                const int cand[3] = {256, 512, 1024};
-                enqueue_batch_step(dt, 256);  // the first step itself runs with 256 threads
-                int rc = read_batch_sizes();
-                if (rc) return rc;
-                if (h_sizes->overflow) {
-                    // nothing after detection ran (overflow guards): restore, grow, redo
-                    rc = batch_overflow_recover();
-                    if (rc) return rc;
-                    continue;
-                }
-                // timing only: re-solve this step's contact problem (its packed records are
-                // still in place) with each block size; the update already used the first solve
-                float best = 1e30f;
-                int best_bt = 256;
-                for (int k = 0; k < 3; ++k) {
-                    cudaEventRecord(ev_a[0], stream);
-                    enqueue_batch_solve(dt, cand[k]);
-                    cudaEventRecord(ev_a[1], stream);
-                    cudaEventSynchronize(ev_a[1]);
-                    float ms = 0;
-                    cudaEventElapsedTime(&ms, ev_a[0], ev_a[1]);
-                    batch_tune_ms[k] = ms;
-                    if (ms < best) {
-                        best = ms;
-                        best_bt = cand[k];
-                    }
-                }
-                batch_threads = best_bt;
-                cudaEventRecord(ev[3], stream);
-                collect_batch_stats();
-                finish_batch_step_timing();
-                return 0;
-            }
-            if (!graph_exec || graph_dt != dt || graph_cap != c_cap) {
+            if (!graph_exec || graph_dt != dt || graph_cap != c_cap || graph_bt != bt) {
                 drop_graph();
                 cudaError_t e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
                 if (e != cudaSuccess) return cuda_fail(e, "cudaStreamBeginCapture");
                 const long long l0 = launches();
-                enqueue_batch_step(dt, batch_threads);
+                enqueue_batch_step(dt, bt);
                 graph_kernels = launches() - l0;
                 replayed -= graph_kernels;  // the capture itself launched nothing
                 e = cudaStreamEndCapture(stream, &graph);
@@ -351,6 +328,7 @@ struct scopi_gpu_handle {
                 if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
                 graph_dt = dt;
                 graph_cap = c_cap;
+                graph_bt = bt;
                 cudaEventRecord(ev[0], stream);
             }
             cudaError_t e = cudaGraphLaunch(graph_exec, stream);
@@ -359,6 +337,7 @@ struct scopi_gpu_handle {
             int rc = read_batch_sizes();
             if (rc) return rc;
             if (h_sizes->overflow) {
+                // nothing after detection ran (overflow guards): restore, grow, redo
                 rc = batch_overflow_recover();
                 if (rc) return rc;
                 continue;
@@ -366,9 +345,35 @@ struct scopi_gpu_handle {
             cudaEventRecord(ev[3], stream);
             collect_batch_stats();
             finish_batch_step_timing();
+            batch_bt_used = bt;
+            if (!batch_threads && stats.iterations >= kBatchTuneIterations) return autotune_batch(dt);
             return 0;
         }
         return fail(SCOPI_GPU_ENOMEM, "contact capacity could not be grown");
+    }
+
+    // timing only: re-solve the last step's contact problem (its packed records are still in
+    // place; the update already used the step's own solve) with each block size
+    int autotune_batch(double dt) {
+        const int cand[3] = {256, 512, 1024};
+        float best = 1e30f;
+        int best_bt = kBatchDefaultThreads;
+        for (int k = 0; k < 3; ++k) {
+            cudaEventRecord(ev_a[0], stream);
+            enqueue_batch_solve(dt, cand[k]);
+            cudaEventRecord(ev_a[1], stream);
+            cudaError_t e = cudaEventSynchronize(ev_a[1]);
+            if (e != cudaSuccess) return cuda_fail(e, "batch autotune");
+            float ms = 0;
+            cudaEventElapsedTime(&ms, ev_a[0], ev_a[1]);
+            batch_tune_ms[k] = ms;
+            if (ms < best) {
+                best = ms;
+                best_bt = cand[k];
+            }
+        }
+        batch_threads = best_bt;
+        return 0;
     }
 
     void finish_batch_step_timing() {
@@ -506,6 +511,12 @@ struct scopi_gpu_handle {
         return 0;
     }
 
+    // first APGD step: the reference's alpha, or the curvature estimate (AUTO: MIXED only)
+    int curvature_start() const {
+        if (P.initial_step == SCOPI_GPU_STEP_AUTO) return mixed() ? 1 : 0;
+        return P.initial_step == SCOPI_GPU_STEP_CURVATURE ? 1 : 0;
+    }
+
     long long launches() const {
         return detect_launches() + apgd_launches() + apgd_sph_launches() + apgd_batch_launches() + replayed;
     }
@@ -590,16 +601,18 @@ struct scopi_gpu_handle {
     }
 
     template <typename T>
-    int run_apgd(SolveBuffers<T>& sb, const T* invm, int maxb, double dt, double tol, long long max_ite, long long M) {
+    int run_apgd(SolveBuffers<T>& sb, const T* invm, int maxb, double dt, double tol, long long max_ite, long long M,
+                 double alpha0 = 0.0) {
         Bodies b = bodies();
         StepParams sp = step_params(dt);
         ApgdSettings st;
-        st.alpha = P.alpha;
+        st.alpha = alpha0 > 0.0 ? alpha0 : P.alpha;
         st.tol = tol;
         st.max_ite = max_ite;
         st.dynamic = P.dynamic_descent;
         st.dt = dt;
         st.mu = P.mu;
+        st.curvature_start = 0;  // the 6-dof kernel starts from alpha
         cudaMemsetAsync(sb.lam[0], 0, M * sizeof(T), stream);
         cudaMemsetAsync(sb.lam[1], 0, M * sizeof(T), stream);
         cudaMemsetAsync(sb.u[0], 0, 6 * (size_t)na * sizeof(T), stream);
@@ -616,14 +629,16 @@ struct scopi_gpu_handle {
     }
 
     template <typename T>
-    int run_apgd_sph(SphSolve<T>& sb, int maxb, double dt, double tol, long long max_ite, long long M) {
+    int run_apgd_sph(SphSolve<T>& sb, int maxb, double dt, double tol, long long max_ite, long long M,
+                     double alpha0 = 0.0) {
         ApgdSettings st;
-        st.alpha = P.alpha;
+        st.alpha = alpha0 > 0.0 ? alpha0 : P.alpha;
         st.tol = tol;
         st.max_ite = max_ite;
         st.dynamic = P.dynamic_descent;
         st.dt = dt;
         st.mu = P.mu;
+        st.curvature_start = curvature_start();
         // lambda = lambda_prev = 0 and u(lambda) = u(y) = 0 (cold start, apgd.hpp:152-159)
         cudaMemsetAsync(sb.lam[0], 0, M * sizeof(T), stream);
         cudaMemsetAsync(sb.lam[1], 0, M * sizeof(T), stream);
@@ -814,12 +829,17 @@ struct scopi_gpu_handle {
             sb.result = d_result;
         }
         float total = 0.0f;
+        // correction solves start from the step size the previous solve ended with (same Q):
+        // from the default alpha their first steps alpha * g can be below the tolerance and
+        // the solve stops at once, leaving the violation where it was
+        double alpha0 = 0.0;
         auto solve32 = [&]() -> int {
             cudaEventRecord(ev_a[0], stream);
-            int r = sphere_mode() ? run_apgd_sph<float>(sbs, max_sph32, dt, P.tolerance, P.max_ite, M)
-                                  : run_apgd<float>(sb, d_invm32, max_blocks32, dt, P.tolerance, P.max_ite, M);
+            int r = sphere_mode() ? run_apgd_sph<float>(sbs, max_sph32, dt, P.tolerance, P.max_ite, M, alpha0)
+                                  : run_apgd<float>(sb, d_invm32, max_blocks32, dt, P.tolerance, P.max_ite, M, alpha0);
             cudaEventRecord(ev_a[1], stream);
             if (r) return r;
+            if (std::isfinite(h_result->lipsch) && h_result->lipsch > 0.0) alpha0 = 1.0 / h_result->lipsch;
             cudaEventSynchronize(ev_a[1]);
             float ms = 0;
             cudaEventElapsedTime(&ms, ev_a[0], ev_a[1]);
@@ -888,6 +908,7 @@ void scopi_gpu_default_params(scopi_gpu_params* p, int32_t dim) {
     p->mixed_violation_tol = 1e-6;
     p->mixed_max_corrections = 3;
     p->device = 0;
+    p->initial_step = SCOPI_GPU_STEP_AUTO;
 }
 
 int32_t scopi_gpu_create(const scopi_gpu_params* p, scopi_gpu_handle** out) {
@@ -1338,7 +1359,10 @@ int32_t scopi_gpu_batch_get_scene_stats(scopi_gpu_handle* h, int32_t scene, scop
     return 0;
 }
 
-int32_t scopi_gpu_batch_block_threads(scopi_gpu_handle* h) { return h ? h->batch_threads : 0; }
+int32_t scopi_gpu_batch_block_threads(scopi_gpu_handle* h) {
+    if (!h) return 0;
+    return h->batch_threads ? h->batch_threads : h->batch_bt_used;
+}
 
 int32_t scopi_gpu_batch_set_block_threads(scopi_gpu_handle* h, int32_t threads) {
     if (!h || !h->batch) return SCOPI_GPU_EINVAL;

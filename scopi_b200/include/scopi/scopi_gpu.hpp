@@ -342,6 +342,7 @@ struct apgd_params {  // apgd.hpp:105-124 (+ the mixed form's correction target)
     bool dynamic_descent = true;
     double mixed_violation_tol = 1e-6;
     int mixed_max_corrections = 3;
+    int initial_step = SCOPI_GPU_STEP_AUTO;  // first step: reference alpha or curvature estimate
 };
 
 template <class precision = fp64>
@@ -523,6 +524,7 @@ class ScopiSolver {
         p.dynamic_descent = op.dynamic_descent ? 1 : 0;
         p.mixed_violation_tol = op.mixed_violation_tol;
         p.mixed_max_corrections = op.mixed_max_corrections;
+        p.initial_step = op.initial_step;
         p.dmax = m_contact_params.dmax;
         if constexpr (std::is_same_v<contact_method_t, gpu::contact_kdtree<problem_t>>)
             p.kd_tree_radius = m_contact_params.kd_tree_radius;

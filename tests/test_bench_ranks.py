@@ -46,7 +46,12 @@ def test_max_over_ranks_gloo():
 def test_roofline_formula_matches_design():
     import bench
     C, N = 3_000_000, 1_000_000
-    # full 6-dof rows, FP64: the 1.06 GB per iteration example of the blueprint
-    assert abs(bench.roofline_bytes_per_iter(C, N, 8, torque_free=False) - 1.056e9) < 1e6
-    # torque-free rows (normal only), FP32
-    assert bench.roofline_bytes_per_iter(C, N, 4) == 3 * C * (3 * 4 + 8) + 6 * C * 4 + 4 * (3 * N) * 4
+    # full 6-dof rows (the figure roofline.achieved uses), FP64: 1.06 GB per iteration at
+    # 1M spheres / 3M contacts, and 0.56 GB in FP32
+    assert abs(bench.roofline_bytes_per_iter(C, N, 8) - 1.056e9) < 1e6
+    assert abs(bench.roofline_bytes_per_iter(C, N, 4) - 0.564e9) < 1e6
+    # 2D: 4 values per contact, 3N particle slots
+    assert bench.roofline_bytes_per_iter(C, N, 8, dim=2) == 3 * C * (4 * 8 + 8) + 6 * C * 8 + 4 * (3 * N) * 8
+    # torque-free rows (normal only), FP32: what the kernel streams
+    assert (bench.roofline_bytes_per_iter(C, N, 4, torque_free=True)
+            == 3 * C * (3 * 4 + 8) + 6 * C * 4 + 4 * (3 * N) * 4)

@@ -16,15 +16,9 @@ KW = dict(dmax=ST["dmax"], tolerance=ST["tolerance"], max_ite=ST["max_ite"])
 
 
 def small_piles(n, nmin=30, nmax=300, seed=7, vmax=0.6):
-    """Pile scenes whose disks get random velocities in [-vmax, vmax]^2, so neighbours
-    approach each other and the first steps already have active constraints."""
-    out = []
-    for s in range(n):
-        pa = configs.pile_scene(seed * 1000 + s, nmin, nmax)
-        u = configs.splitmix_uniform(seed * 7919 + s, 2 * pa.n).reshape(pa.n, 2)
-        pa.v[pa.nb_inactive:, :2] = (2 * u[pa.nb_inactive:] - 1) * vmax
-        out.append(pa)
-    return out
+    """Pile scenes whose disks start with random velocities in [-vmax, vmax]^2, so the
+    first steps already have active constraints."""
+    return configs.pile_scenes(n, seed, nmin, nmax, vmax)
 
 
 def lone_disk():
@@ -141,3 +135,24 @@ def test_batch_rejects_bad_block_size_and_friction():
     arr = (_abi.ParticlesC * 1)()
     h = C.c_void_p()
     assert b._lib.scopi_gpu_batch_create(C.byref(p), 0, arr, C.byref(h)) < 0
+
+
+def test_batch_autotune_waits_for_a_nontrivial_step():
+    """Falling piles converge in one iteration for their first steps: no tuning on those."""
+    scenes = configs.pile_scenes(4, seed=12, nmin=50, nmax=200)
+    b = ScopiBatch(scenes, vap=ST["vap"], precision=MIXED, **KW).run(ST["dt"], 2)
+    assert max(b.scene_stats(s)["iterations"] for s in range(4)) < 64
+    assert b.block_threads() == 512
+
+
+def test_batch_mixed_keeps_violation_target_through_landing():
+    """Disks landing on the segment: the reference's fixed first step alpha = 0.05 can stop
+    a solve after one iteration with a resting contact still open by ~ g dt^2 (the FP64
+    drop-in reproduces that); the mixed form's curvature start keeps every step <= 1e-6."""
+    scenes = configs.pile_scenes(12, seed=13, nmin=200, nmax=1000)
+    b = ScopiBatch(scenes, vap=ST["vap"], precision=MIXED, mixed_violation_tol=1e-6, **KW)
+    worst = 0.0
+    for _ in range(70):
+        b.run(ST["dt"], 1)
+        worst = max(worst, b.stats()["violation"])
+    assert worst <= 1e-6

@@ -225,3 +225,19 @@ def test_apgd_max_ite_reports_nonconvergence():
     s.run(0.005, 1)
     st = s.stats()
     assert st["iterations"] == 1 and st["converged"] == 0 and st["status"] == 1
+
+
+@pytest.mark.parametrize("precision,init", [(0, 1), (1, 0)])
+def test_initial_step_choices(precision, init):
+    """The first-step rule taken apart from the precision: FP64 with the curvature start and
+    MIXED with the reference's alpha both reach the same state as the FP64 drop-in."""
+    pa = configs.spheres_1m(side=16)
+    st = configs.SETTINGS["spheres_1m"]
+    kw = dict(dmax=st["dmax"], tolerance=st["tolerance"], max_ite=st["max_ite"], vap=st["vap"])
+    ref = gpu_solver(pa, **kw).run(st["dt"], 3)
+    alt = gpu_solver(pa, precision=precision, initial_step=init, mixed_violation_tol=1e-6, **kw).run(st["dt"], 3)
+    sa, sr = alt.stats(), ref.stats()
+    assert sa["converged"] == 1 and sa["violation"] <= 1e-6, sa
+    if init == 1:
+        assert sa["iterations"] < sr["iterations"] / 4, (sa, sr)
+    assert rel_err(alt.particles.pos, ref.particles.pos) <= 1e-7
