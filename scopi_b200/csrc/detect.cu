@@ -174,7 +174,7 @@ __device__ __forceinline__ void flip(PairGeom& g) {
 }
 
 // closest_points_dispatcher restricted to the pairs of the hot path (a < b).
-__device__ bool exact_pair(const Bodies& B, int dim, int a, int b, PairGeom& g) {
+__device__ __forceinline__ bool exact_pair(const Bodies& B, int dim, int a, int b, PairGeom& g) {
     const int sa = B.shape[a], sb = B.shape[b];
     const double* xa = B.pos + 3 * (long long)a;
     const double* xb = B.pos + 3 * (long long)b;
@@ -360,21 +360,44 @@ __global__ void k_cell_scatter(Bodies B, const int* cell_of, const int* cell_sta
     }
 }
 
-// Enumerates the (a, b > a) active pairs of the 3^dim neighbour cells of cell-sorted slot k
-// whose exact closest-point distance is < dmax (and pass the kd-tree candidate filter).
-template <typename F>
-__device__ __forceinline__ void for_each_pair(const Bodies& B, const StepParams& p, const Grid& g, const int* cell_of,
-                                              const int* cell_start, const int* cell_body, const double4* cell_pr,
-                                              int k, F&& emit) {
-    const int a = cell_body[k];
-    const double4 A = cell_pr[k];
-    const double xa[3] = {A.x, A.y, A.z};
-    const int id = cell_of[a - B.nin];
-    int cc[3];
+// Pair test of the contact list: kd-tree candidate filter, sphere bound, then the exact
+// closest-point distance < dmax (contact_kdtree.hpp:240-262, base.hpp:104-141).  Always
+// evaluated with the lower body index first, as the reference does for its (i < j) pairs,
+// so that the decision is bitwise the same whichever body finds the pair.
+// DIM is a template argument so that the coordinate loops unroll and the small arrays of
+// the geometry stay in registers (a runtime dimension puts them in local memory).
+template <int DIM>
+__device__ __forceinline__ bool pair_in_contact(const StepParams& p, const double4& L, const double4& H) {
+    const double xl[3] = {L.x, L.y, L.z}, xh[3] = {H.x, H.y, H.z};
+    double s2 = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        const double dd = xl[d] - xh[d];
+        s2 += dd * dd;
+    }
+    if (p.kd_filter && !(s2 < p.kd_radius)) return false;
+    const double lim = L.w + H.w + p.dmax;
+    if (!(lim > 0.0) || s2 > lim * lim * (1.0 + 1e-9)) return false;
+    PairGeom pg;
+    sphere_sphere(DIM, xl, L.w, xh, H.w, pg);
+    return pg.dij < p.dmax;
+}
+
+__device__ __forceinline__ void cell_coords(const Grid& g, int id, int* cc) {
     cc[0] = id % g.nc[0];
     cc[1] = (id / g.nc[0]) % g.nc[1];
     cc[2] = id / (g.nc[0] * g.nc[1]);
-    const int zr = p.dim == 3 ? 1 : 0;
+}
+
+// Enumerates the (a, b > a) active pairs in contact of body a (position and radius A) over
+// the 3^dim neighbour cells of its cell.
+template <int DIM, typename F>
+__device__ __forceinline__ void for_each_pair_of(const Bodies& B, const StepParams& p, const Grid& g,
+                                                 const int* cell_of, const int* cell_start, const int* cell_body,
+                                                 const double4* cell_pr, int a, const double4& A, F&& emit) {
+    int cc[3];
+    cell_coords(g, cell_of[a - B.nin], cc);
+    const int zr = DIM == 3 ? 1 : 0;
     for (int dz = -zr; dz <= zr; ++dz) {
         const int z = cc[2] + dz;
         if (z < 0 || z >= g.nc[2]) continue;
@@ -390,51 +413,103 @@ __device__ __forceinline__ void for_each_pair(const Bodies& B, const StepParams&
                     const int b = cell_body[t];
                     if (b <= a) continue;
                     if (B.scene && B.scene[a] != B.scene[b]) continue;
-                    const double4 Bb = cell_pr[t];
-                    const double xb[3] = {Bb.x, Bb.y, Bb.z};
-                    double s2 = 0.0;
-                    for (int d = 0; d < p.dim; ++d) {
-                        const double dd = xa[d] - xb[d];
-                        s2 += dd * dd;
-                    }
-                    if (p.kd_filter && !(s2 < p.kd_radius)) continue;
-                    const double lim = A.w + Bb.w + p.dmax;
-                    if (!(lim > 0.0) || s2 > lim * lim * (1.0 + 1e-9)) continue;
-                    PairGeom pg;
-                    sphere_sphere(p.dim, xa, A.w, xb, Bb.w, pg);
-                    if (pg.dij < p.dmax) emit(a, b);
+                    if (pair_in_contact<DIM>(p, A, cell_pr[t])) emit(a, b);
                 }
             }
         }
     }
 }
 
-__global__ void k_pair_count(Bodies B, StepParams p, const Grid* grid, const int* cell_of, const int* cell_start,
-                             const int* cell_body, const double4* cell_pr, int* row_count) {
+// One pass over the half stencil: body k (cell-sorted slot) meets the bodies after it in its
+// own cell and those of the 13 (3D) / 4 (2D) neighbour cells that follow its cell in
+// (z, y, x) order, so every unordered pair of neighbouring cells is visited once.  A pair in
+// contact is counted in the row of its lower index (atomic slot) and its partner kept in
+// that row's scratch while the row has room; the row sort makes the order deterministic.
+template <int DIM>
+__global__ void k_pair_search(Bodies B, StepParams p, const Grid* grid, const int* cell_of, const int* cell_start,
+                              const int* cell_body, const double4* cell_pr, int* row_count, int* row_tmp) {
     const Grid g = *grid;
+    constexpr int nst = DIM == 3 ? 14 : 5;
     GRID_STRIDE(k, B.n - B.nin) {
-        int cnt = 0;
-        int a0 = cell_body[k];
-        for_each_pair(B, p, g, cell_of, cell_start, cell_body, cell_pr, (int)k, [&](int, int) { ++cnt; });
-        row_count[a0 - B.nin] = cnt;
+        const int a = cell_body[k];
+        const double4 A = cell_pr[k];
+        int cc[3];
+        cell_coords(g, cell_of[a - B.nin], cc);
+        for (int o = 0; o < nst; ++o) {
+            // o = 0: own cell; then the offsets with (dz, dy, dx) > (0, 0, 0) lexicographically
+            int dx = 0, dy = 0, dz = 0;
+            if (o > 0) {
+                const int q = o - 1;
+                if (DIM == 3) {
+                    if (q == 0) {
+                        dx = 1;
+                    } else if (q < 4) {
+                        dy = 1;
+                        dx = q - 2;
+                    } else {
+                        dz = 1;
+                        dy = (q - 4) / 3 - 1;
+                        dx = (q - 4) % 3 - 1;
+                    }
+                } else {
+                    if (q == 0) {
+                        dx = 1;
+                    } else {
+                        dy = 1;
+                        dx = q - 2;
+                    }
+                }
+            }
+            const int x = cc[0] + dx, y = cc[1] + dy, z = cc[2] + dz;
+            if (x < 0 || x >= g.nc[0] || y < 0 || y >= g.nc[1] || z >= g.nc[2]) continue;
+            const int cid = (z * g.nc[1] + y) * g.nc[0] + x;
+            const int t1 = cell_start[cid + 1];
+            for (int t = o == 0 ? (int)k + 1 : cell_start[cid]; t < t1; ++t) {
+                const int b = cell_body[t];
+                if (B.scene && B.scene[a] != B.scene[b]) continue;
+                const double4 Bb = cell_pr[t];
+                const bool a_lo = a < b;
+                if (!pair_in_contact<DIM>(p, a_lo ? A : Bb, a_lo ? Bb : A)) continue;
+                const int lo = a_lo ? a : b, hi = a_lo ? b : a;
+                const int r = lo - B.nin;
+                const int slot = atomicAdd(&row_count[r], 1);
+                if (slot < kRowCap) row_tmp[(long long)r * kRowCap + slot] = hi;
+            }
+        }
     }
 }
 
-__global__ void k_pair_fill(Bodies B, StepParams p, const Grid* grid, const int* cell_of, const int* cell_start,
-                            const int* cell_body, const double4* cell_pr, const int* row_ptr, const Sizes* sizes,
-                            long long cap, int* ci, int* cj) {
+// Rows in place: (ci, cj) of row r at c_obs + row_ptr[r]; a row whose partners did not fit
+// its scratch is enumerated again over the full stencil by its thread.
+template <int DIM>
+__global__ void k_pair_compact(Bodies B, StepParams p, const Grid* grid, const int* cell_of, const int* cell_start,
+                               const int* cell_body, const double4* cell_pr, const int* row_count, const int* row_tmp,
+                               const int* row_ptr, const Sizes* sizes, long long cap, int* ci, int* cj) {
     const Grid g = *grid;
     const int c_obs = sizes->C_obs;
-    GRID_STRIDE(k, B.n - B.nin) {
-        const int a0 = cell_body[k];
-        long long at = (long long)c_obs + row_ptr[a0 - B.nin];
-        for_each_pair(B, p, g, cell_of, cell_start, cell_body, cell_pr, (int)k, [&](int a, int b) {
-            if (at < cap) {
-                ci[at] = a;
-                cj[at] = b;
+    GRID_STRIDE(r, B.n - B.nin) {
+        const int cnt = row_count[r];
+        if (cnt == 0) continue;
+        const int a = B.nin + (int)r;
+        long long at = (long long)c_obs + row_ptr[r];
+        if (at + cnt > cap) continue;  // contact buffers too small: the step is redone
+        if (cnt <= kRowCap) {
+            for (int q = 0; q < cnt; ++q) {
+                ci[at + q] = a;
+                cj[at + q] = row_tmp[(long long)r * kRowCap + q];
             }
-            ++at;
-        });
+        } else {
+            const double4 A = make_double4(B.pos[3 * (long long)a], B.pos[3 * (long long)a + 1],
+                                           B.pos[3 * (long long)a + 2], B.radius[a]);
+            const long long end = at + cnt;  // the same test finds the same cnt partners
+            for_each_pair_of<DIM>(B, p, g, cell_of, cell_start, cell_body, cell_pr, a, A, [&](int i, int j) {
+                if (at < end) {
+                    ci[at] = i;
+                    cj[at] = j;
+                }
+                ++at;
+            });
+        }
     }
 }
 
@@ -459,9 +534,11 @@ __global__ void k_row_sort(int na, const int* row_ptr, const Sizes* sizes, long 
 // scene's actives in a batch (rows stay sorted by (obstacle, active))
 __device__ __forceinline__ void obs_pair(const Bodies& B, long long k, int& o, int& b) {
     if (!B.obs_off) {
-        const long long na = B.n - B.nin;
-        o = (int)(k / na);
-        b = B.nin + (int)(k % na);
+        // nin * na < 2^31 here (the flag arrays are int-indexed): 32-bit division, not
+        // the 64-bit one, which the GPU emulates in software
+        const unsigned na = (unsigned)(B.n - B.nin), kk = (unsigned)k;
+        o = (int)(kk / na);
+        b = B.nin + (int)(kk - (unsigned)o * na);
         return;
     }
     int lo = 0, hi = B.nin;  // last o with obs_off[o] <= k
@@ -476,12 +553,13 @@ __device__ __forceinline__ void obs_pair(const Bodies& B, long long k, int& o, i
     b = B.nin + B.obs_a0[o] + (int)(k - B.obs_off[o]);
 }
 
+template <int DIM>
 __global__ void k_obs_flags(Bodies B, StepParams p, long long nobs, int* flag) {
     GRID_STRIDE(k, nobs) {
         int o, b;
         obs_pair(B, k, o, b);
         PairGeom g;
-        flag[k] = (exact_pair(B, p.dim, o, b, g) && g.dij < p.dmax) ? 1 : 0;
+        flag[k] = (exact_pair(B, DIM, o, b, g) && g.dij < p.dmax) ? 1 : 0;
     }
 }
 
@@ -513,13 +591,14 @@ __global__ void k_set_cobs(const int* totals, Sizes* sizes) {
 
 // closest points of the listed pairs; viscous gamma carried over from the previous list
 // by (i, j) (transfer, include/scopi/solver.hpp:241-258).
+template <int DIM>
 __global__ void k_geometry(Bodies B, StepParams p, Contacts c, const Sizes* sizes, Contacts old_c, const int* old_C) {
     const int C = sizes->C;
     const int oC = old_C ? *old_C : 0;
     GRID_STRIDE(k, C) {
         const int a = c.ci[k], b = c.cj[k];
         PairGeom g;
-        if (!exact_pair(B, p.dim, a, b, g)) {
+        if (!exact_pair(B, DIM, a, b, g)) {
             g.dij = 0.0;
             for (int d = 0; d < 3; ++d) g.nij[d] = g.pi[d] = g.pj[d] = 0.0;
         }
@@ -551,6 +630,7 @@ __global__ void k_geometry(Bodies B, StepParams p, Contacts c, const Sizes* size
 //   B_c u = n.v_i + a_i.w_i - n.v_j + a_j.w_j,  a_i = R_i^T (r_i x n),  a_j = -R_j^T (r_j x n),
 // and c_c = n.(D n + dt A U)_c (CVector, minimization_problem.hpp:34-70).  For friction
 // the three rows of A are kept: P = R^T [r]x so A_c = [I, P_i^T, -I, -P_j^T].
+template <int DIM>
 __global__ void k_assemble(Bodies B, StepParams p, Contacts c, Assembly a, const Sizes* sizes) {
     const int C = sizes->C;
     GRID_STRIDE(k, C) {
@@ -566,19 +646,19 @@ __global__ void k_assemble(Bodies B, StepParams p, Contacts c, Assembly a, const
             if (b < B.nin) continue;
             const double* pt = (s == 0 ? c.pi : c.pj) + 3 * k;
             double r[3] = {0, 0, 0};
-            for (int d = 0; d < p.dim; ++d) r[d] = pt[d] - B.pos[3 * (long long)b + d];
+            for (int d = 0; d < DIM; ++d) r[d] = pt[d] - B.pos[3 * (long long)b + d];
             double R[3][3];
             rotation3(B.q + 4 * (long long)b, R);
             const double* w = B.omega + 3 * (long long)b;
             const double* v = B.v + 3 * (long long)b;
             double Rw[3], cr[3];
             for (int d = 0; d < 3; ++d) Rw[d] = R[d][0] * w[0] + R[d][1] * w[1] + R[d][2] * w[2];
-            cross_dim(p.dim, r, Rw, cr);
-            const double vz = p.dim == 2 ? 0.0 : v[2];
+            cross_dim(DIM, r, Rw, cr);
+            const double vz = DIM == 2 ? 0.0 : v[2];
             const double vv[3] = {v[0], v[1], vz};
             for (int d = 0; d < 3; ++d) AU[d] += (s == 0 ? 1.0 : -1.0) * (vv[d] - cr[d]);
             double rn[3];
-            cross_dim(p.dim, r, n, rn);
+            cross_dim(DIM, r, n, rn);
             const double sg = (s == 0) ? 1.0 : -1.0;
             for (int d = 0; d < 3; ++d) arow[s][d] = sg * (R[0][d] * rn[0] + R[1][d] * rn[1] + R[2][d] * rn[2]);
             // P = R^T [r]x : P[k][l] = sum_m R[m][k] X[m][l], X = [[0,-r2,r1],[r2,0,-r0],[-r1,r0,0]]
@@ -588,7 +668,7 @@ __global__ void k_assemble(Bodies B, StepParams p, Contacts c, Assembly a, const
                     P[s][3 * kk + l] = R[0][kk] * X[0][l] + R[1][kk] * X[1][l] + R[2][kk] * X[2][l];
         }
         double Cv[3];
-        for (int d = 0; d < 3; ++d) Cv[d] = (d < p.dim ? c.dij[k] * n[d] : 0.0) + p.dt * AU[d];
+        for (int d = 0; d < 3; ++d) Cv[d] = (d < DIM ? c.dij[k] * n[d] : 0.0) + p.dt * AU[d];
         if (p.problem == kFriction) {
             for (int d = 0; d < 3; ++d) a.cvec[3 * k + d] = Cv[d];
             for (int e = 0; e < 9; ++e) {
@@ -597,7 +677,7 @@ __global__ void k_assemble(Bodies B, StepParams p, Contacts c, Assembly a, const
             }
         } else {
             double cc = 0.0;
-            for (int d = 0; d < p.dim; ++d) cc += Cv[d] * n[d];
+            for (int d = 0; d < DIM; ++d) cc += Cv[d] * n[d];
             a.cvec[k] = cc;
         }
         for (int d = 0; d < 3; ++d) {
@@ -819,14 +899,22 @@ void launch_detect(const Bodies& b, const StepParams& p, DetectWork& w, Contacts
                        &g_detect_launches);
         k_cell_scatter<<<blocks_for(na), kThreads, 0, s>>>(b, w.cell_of, w.cell_start, w.cell_fill, w.cell_body,
                                                            w.cell_pr);
-        k_pair_count<<<blocks_for(na, 128), 128, 0, s>>>(b, p, w.grid, w.cell_of, w.cell_start, w.cell_body, w.cell_pr,
-                                                         w.row_count);
+        cudaMemsetAsync(w.row_count, 0, (na + 1) * sizeof(int), s);
+        if (p.dim == 3)
+            k_pair_search<3><<<blocks_for(na, 128), 128, 0, s>>>(b, p, w.grid, w.cell_of, w.cell_start, w.cell_body,
+                                                                 w.cell_pr, w.row_count, w.row_tmp);
+        else
+            k_pair_search<2><<<blocks_for(na, 128), 128, 0, s>>>(b, p, w.grid, w.cell_of, w.cell_start, w.cell_body,
+                                                                 w.cell_pr, w.row_count, w.row_tmp);
         LAUNCHED(3);
     }
     // obstacle rows come first in (i, j) order
     const long long nobs = w.obs_cap;  // nin * na, or the sum of the per-obstacle ranges of a batch
     if (nobs > 0) {
-        k_obs_flags<<<blocks_for(nobs), kThreads, 0, s>>>(b, p, nobs, w.obs_flag);
+        if (p.dim == 3)
+            k_obs_flags<3><<<blocks_for(nobs), kThreads, 0, s>>>(b, p, nobs, w.obs_flag);
+        else
+            k_obs_flags<2><<<blocks_for(nobs), kThreads, 0, s>>>(b, p, nobs, w.obs_flag);
         scan_exclusive(w.obs_flag, w.obs_pos, nullptr, (int)nobs, nobs, w.tmp_total + 0, w.scan_work, s,
                        &g_detect_launches);
         LAUNCHED(1);
@@ -834,7 +922,6 @@ void launch_detect(const Bodies& b, const StepParams& p, DetectWork& w, Contacts
     k_set_cobs<<<1, 1, 0, s>>>(w.tmp_total, sizes);
     LAUNCHED(1);
     if (na > 0) {
-        cudaMemsetAsync(w.row_count + na, 0, sizeof(int), s);
         scan_exclusive(w.row_count, w.row_ptr, nullptr, na + 1, na + 1, w.tmp_total + 1, w.scan_work, s,
                        &g_detect_launches);
     }
@@ -845,8 +932,14 @@ void launch_detect(const Bodies& b, const StepParams& p, DetectWork& w, Contacts
         LAUNCHED(1);
     }
     if (na > 0) {
-        k_pair_fill<<<blocks_for(na, 128), 128, 0, s>>>(b, p, w.grid, w.cell_of, w.cell_start, w.cell_body, w.cell_pr,
-                                                        w.row_ptr, sizes, c_cap, out.ci, out.cj);
+        if (p.dim == 3)
+            k_pair_compact<3><<<blocks_for(na), kThreads, 0, s>>>(b, p, w.grid, w.cell_of, w.cell_start, w.cell_body,
+                                                                  w.cell_pr, w.row_count, w.row_tmp, w.row_ptr, sizes,
+                                                                  c_cap, out.ci, out.cj);
+        else
+            k_pair_compact<2><<<blocks_for(na), kThreads, 0, s>>>(b, p, w.grid, w.cell_of, w.cell_start, w.cell_body,
+                                                                  w.cell_pr, w.row_count, w.row_tmp, w.row_ptr, sizes,
+                                                                  c_cap, out.ci, out.cj);
         k_row_sort<<<blocks_for(na), kThreads, 0, s>>>(na, w.row_ptr, sizes, c_cap, out.cj);
         LAUNCHED(2);
     }
@@ -856,13 +949,19 @@ void launch_geometry(const Bodies& b, const StepParams& p, Contacts& c, const Si
                      const Contacts* old_c, const int* old_C, long long, cudaStream_t s) {
     Contacts oc{};
     if (old_c) oc = *old_c;
-    k_geometry<<<blocks_for(c_cap), kThreads, 0, s>>>(b, p, c, sizes, oc, old_c ? old_C : nullptr);
+    if (p.dim == 3)
+        k_geometry<3><<<blocks_for(c_cap), kThreads, 0, s>>>(b, p, c, sizes, oc, old_c ? old_C : nullptr);
+    else
+        k_geometry<2><<<blocks_for(c_cap), kThreads, 0, s>>>(b, p, c, sizes, oc, old_c ? old_C : nullptr);
     LAUNCHED(1);
 }
 
 void launch_assemble(const Bodies& b, const StepParams& p, const Contacts& c, Assembly& a, Sizes* sizes,
                      long long c_cap, int* scan_work, int* tmp_total, cudaStream_t s) {
-    k_assemble<<<blocks_for(c_cap), kThreads, 0, s>>>(b, p, c, a, sizes);
+    if (p.dim == 3)
+        k_assemble<3><<<blocks_for(c_cap), kThreads, 0, s>>>(b, p, c, a, sizes);
+    else
+        k_assemble<2><<<blocks_for(c_cap), kThreads, 0, s>>>(b, p, c, a, sizes);
     LAUNCHED(1);
     if (p.problem == kViscous) {
         scan_exclusive(a.vflag, a.slot, &sizes->C, 0, c_cap, tmp_total, scan_work, s, &g_detect_launches);
@@ -874,7 +973,8 @@ void launch_assemble(const Bodies& b, const StepParams& p, const Contacts& c, As
 }
 
 void launch_incidence(const Bodies& b, const StepParams& p, const Contacts& c, const Assembly& a, Incidence& inc,
-                      const Sizes* sizes, long long c_cap, int* scan_work, int* tmp_total, cudaStream_t s) {
+                      const Sizes* sizes, long long c_cap, int* scan_work, int* tmp_total, cudaStream_t s,
+                      bool with_coef) {
     const int na = b.n - b.nin;
     if (na <= 0) return;
     cudaMemsetAsync(inc.count, 0, (na + 1) * sizeof(int), s);
@@ -884,7 +984,7 @@ void launch_incidence(const Bodies& b, const StepParams& p, const Contacts& c, c
     k_inc_fill<<<blocks_for(c_cap), kThreads, 0, s>>>(b.nin, c, sizes, inc.ptr, inc.jcount, inc.idx);
     k_inc_sort<<<blocks_for(na), kThreads, 0, s>>>(na, inc.ptr, inc.idx);
     LAUNCHED(3);
-    if (p.problem != kFriction) {
+    if (with_coef && p.problem != kFriction) {
         k_inc_coef<<<blocks_for(2 * c_cap), kThreads, 0, s>>>(na, inc.ptr, inc.idx, a, inc.coef);
         LAUNCHED(1);
     }

@@ -25,6 +25,10 @@ struct StepParams {
     double gamma0, gamma_min, gamma_tol, mu;
 };
 
+// partners per contact row kept by the one-pass pair search; a row with more is
+// re-enumerated by its compaction thread
+constexpr int kRowCap = 24;
+
 struct DetectWork {
     Grid* grid;               // device
     double* bbox_partial;     // kBBoxBlocks * 8
@@ -36,6 +40,7 @@ struct DetectWork {
     double4* cell_pr;         // na (x, y, z, r) sorted by cell
     int* row_count;           // na + 1
     int* row_ptr;             // na + 1
+    int* row_tmp;             // na * kRowCap: partners found by the search pass, unordered
     int* obs_flag;            // nin * na
     int* obs_pos;             // nin * na
     int* tmp_total;           // 4 ints
@@ -73,8 +78,11 @@ void launch_geometry(const Bodies& b, const StepParams& p, Contacts& c, const Si
                      const Contacts* old_c, const int* old_C, long long old_cap, cudaStream_t s);
 void launch_assemble(const Bodies& b, const StepParams& p, const Contacts& c, Assembly& a, Sizes* sizes,
                      long long c_cap, int* scan_work, int* tmp_total, cudaStream_t s);
+// with_coef: also the 6 FP64 coefficients per incidence (inc.coef) that the 6-dof
+// normal-row kernels read; the torque-free kernels pack their own records instead
 void launch_incidence(const Bodies& b, const StepParams& p, const Contacts& c, const Assembly& a, Incidence& inc,
-                      const Sizes* sizes, long long c_cap, int* scan_work, int* tmp_total, cudaStream_t s);
+                      const Sizes* sizes, long long c_cap, int* scan_work, int* tmp_total, cudaStream_t s,
+                      bool with_coef);
 void launch_gamma_update(const StepParams& p, Contacts& c, const Assembly& a, const double* lambda, const Sizes* sizes,
                          long long c_cap, cudaStream_t s);
 // v += dt*u_v, omega += dt*u_w, then pos/q integration (u = M^-1 B^T lambda, may be null).

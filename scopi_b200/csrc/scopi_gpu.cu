@@ -200,7 +200,7 @@ struct scopi_gpu_handle {
         launch_vap(b, sp, stream, d_sizes_cur);
         launch_geometry(b, sp, cur, d_sizes_cur, c_cap, nullptr, nullptr, c_cap, stream);
         launch_assemble(b, sp, cur, as, d_sizes_cur, c_cap, dw.scan_work, dw.tmp_total + 2, stream);
-        launch_incidence(b, sp, cur, as, inc, d_sizes_cur, c_cap, dw.scan_work, dw.tmp_total + 2, stream);
+        launch_incidence(b, sp, cur, as, inc, d_sizes_cur, c_cap, dw.scan_work, dw.tmp_total + 2, stream, false);
         launch_pack_cij(cur.ci, cur.cj, d_cij, d_sizes_cur, c_cap, stream);
         launch_pack_nc<double>(as.bn, as.cvec, d_nc64, d_sizes_cur, c_cap, stream);
         launch_pack_inc<double>(na, inc.ptr, inc.idx, as.bn, d_incv64, 2 * c_cap, stream);
@@ -466,7 +466,7 @@ struct scopi_gpu_handle {
         dw.obs_cap = obs_cap >= 0 ? obs_cap : (long long)nin * na;
         A(dw.grid, 1) A(dw.bbox_partial, 8 * 4 * kSMs) A(dw.cell_count, dw.cell_cap + 1) A(dw.cell_start, dw.cell_cap + 1)
         A(dw.cell_fill, dw.cell_cap) A(dw.cell_of, na + 1) A(dw.cell_body, na + 1) A(dw.cell_pr, na + 1)
-        A(dw.row_count, na + 1) A(dw.row_ptr, na + 1) A(dw.obs_flag, dw.obs_cap + 1) A(dw.obs_pos, dw.obs_cap + 1)
+        A(dw.row_count, na + 1) A(dw.row_ptr, na + 1) A(dw.row_tmp, (size_t)na * kRowCap + 1) A(dw.obs_flag, dw.obs_cap + 1) A(dw.obs_pos, dw.obs_cap + 1)
         A(dw.tmp_total, 4)
         const long long scan_max = std::max<long long>(std::max<long long>(dw.cell_cap + 1, dw.obs_cap + 1), na + 1);
         A(dw.scan_work, scan_work_ints(std::max<long long>(scan_max, 1LL << 26)))
@@ -554,7 +554,8 @@ struct scopi_gpu_handle {
         launch_geometry(b, sp, cur, d_sizes_cur, c_cap, has_old ? &old : nullptr, has_old ? &d_sizes_old->C : nullptr,
                         c_cap, stream);
         launch_assemble(b, sp, cur, as, d_sizes_cur, c_cap, dw.scan_work, dw.tmp_total + 2, stream);
-        launch_incidence(b, sp, cur, as, inc, d_sizes_cur, c_cap, dw.scan_work, dw.tmp_total + 2, stream);
+        launch_incidence(b, sp, cur, as, inc, d_sizes_cur, c_cap, dw.scan_work, dw.tmp_total + 2, stream,
+                         !sphere_mode());
         cudaMemcpyAsync(h_sizes, d_sizes_cur, sizeof(Sizes), cudaMemcpyDeviceToHost, stream);
         cudaError_t e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) return cuda_fail(e, "assemble");
@@ -987,6 +988,8 @@ static int32_t upload_particles(scopi_gpu_handle* h, const scopi_gpu_particles* 
         !p->radius || !p->length)
         return h->fail(SCOPI_GPU_EINVAL, "null particle array");
     const int n = (int)p->n, nin = (int)p->nb_inactive;
+    if ((long long)nin * (n - nin) >= (1LL << 31) && obs_cap < 0)
+        return h->fail(SCOPI_GPU_EUNSUPPORTED, "obstacles x active bodies must stay below 2^31");
     for (int i = 0; i < n; ++i) {
         const int s = p->shape[i];
         if (i >= nin && s != SCOPI_GPU_SPHERE)

@@ -33,6 +33,8 @@ DETECT_SCENES = {
     "inclined_plane": lambda: (S.sphere_inclined_plane(math.pi / 6)[0], {}),
     "segment_pile": lambda: (segment_pile(), dict(dmax=0.009)),
     "kd_radius_filter": lambda: (configs.disks_2d(side=12), dict(dmax=0.05, kd_tree_radius=0.03 ** 2)),
+    # rows of up to ~90 partners: past the search pass's per-row scratch (re-enumerated rows)
+    "dense_rows": lambda: (configs.disks_2d(side=10), dict(dmax=0.2)),
 }
 
 
