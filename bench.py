@@ -245,9 +245,9 @@ def measured_peaks():
 
 
 # DRAM bytes (read + write) per FP32 APGD iteration per contact of k_apgd_sph on the
-# 1M-sphere workload, from one ncu capture (profiles/apgd_sph_spheres_1m_traffic.md);
-# None until measured
-TRAFFIC_FP32_PER_CONTACT_ITERATION = None
+# 1M-sphere workload, from one ncu capture of a whole launch (19 iterations, the curvature
+# pre-pass included): 7.015 GB / (19 x 3,000,279) (profiles/apgd_sph_spheres_1m_traffic.md)
+TRAFFIC_FP32_PER_CONTACT_ITERATION = 123.06
 
 
 # ----------------------------------------------------------------------------- CPU legs
@@ -327,7 +327,8 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 0)
     if args.steps is None:
-        args.steps = 5 if args.workload == "spheres_1m" else 1000 - args.warmup
+        # the workloads' own run lengths: 100 steps (1M spheres), 1000 steps (piles)
+        args.steps = (100 if args.workload == "spheres_1m" else 1000) - args.warmup
     ranks = Ranks(args.gpus)
     try:
         if args.impl == "reference":
