@@ -36,6 +36,7 @@ class OrcParticles(C.Structure):
         ("omega", C.POINTER(C.c_double)), ("vd", C.POINTER(C.c_double)), ("omega_d", C.POINTER(C.c_double)),
         ("f", C.POINTER(C.c_double)), ("m", C.POINTER(C.c_double)), ("j", C.POINTER(C.c_double)),
         ("radius", C.POINTER(C.c_double)), ("length", C.POINTER(C.c_double)),
+        ("axes", C.POINTER(C.c_double)), ("squareness", C.POINTER(C.c_double)),
     ]
 
 
@@ -79,6 +80,14 @@ def lib():
         L.orc_detect.argtypes = [C.c_void_p]
         L.orc_amat.argtypes = [C.c_void_p, P, P]
         L.orc_atmat.argtypes = [C.c_void_p, P, P]
+        L.orc_se_se.restype = C.c_int
+        L.orc_se_se.argtypes = [P, P, P]
+        L.orc_se_plane.restype = C.c_int
+        L.orc_se_plane.argtypes = [P, P, P]
+        L.orc_se_se_system.argtypes = [P, P, P, P, P]
+        L.orc_se_plane_residual.argtypes = [P, P, P, P]
+        L.orc_se_se_hybrid.restype = C.c_int
+        L.orc_se_se_hybrid.argtypes = [P, P, P, C.POINTER(C.c_int)]
         _lib = L
     return _lib
 
@@ -92,6 +101,7 @@ def _particles_struct(pa, keep):
     return OrcParticles(
         pa.n, pa.nb_inactive, pa.shape.ctypes.data_as(C.POINTER(C.c_int32)), _dp(pa.pos), _dp(pa.q), _dp(pa.v),
         _dp(pa.omega), _dp(pa.vd), _dp(pa.omega_d), _dp(pa.f), _dp(pa.m), _dp(pa.j), _dp(pa.radius), _dp(pa.length),
+        _dp(pa.axes), _dp(pa.squareness),
     )
 
 
@@ -174,3 +184,57 @@ class OracleSolver:
         out = np.zeros(6 * (self.pa.n - self.pa.nb_inactive))
         lib().orc_atmat(self.h, _dp(f), _dp(out))
         return out
+
+
+def se_record(c, q, r, sq):
+    """Body record {c[3], q[4] (w, x, y, z), r[3], e, n} of the superellipsoid entry points."""
+    return np.concatenate([np.asarray(c, float).ravel()[:3], np.asarray(q, float).ravel()[:4],
+                           np.asarray(r, float).ravel()[:3], np.asarray(sq, float).ravel()[:2]])
+
+
+def _unpack(out):
+    return {"pi": out[0:3].copy(), "pj": out[3:6].copy(), "nij": out[6:9].copy(), "dij": float(out[9]),
+            "u": out[10:14].copy()}
+
+
+def se_se(s1, s2):
+    """closest_points(superellipsoid<3>, superellipsoid<3>) on two body records."""
+    out = np.zeros(14)
+    a, b = np.ascontiguousarray(s1, float), np.ascontiguousarray(s2, float)
+    info = lib().orc_se_se(_dp(a), _dp(b), _dp(out))
+    r = _unpack(out)
+    r["info"] = info
+    return r
+
+
+def se_plane(s, plane_c, plane_q):
+    """closest_points(superellipsoid<3>, plane<3>); the plane record is {c[3], q[4]}."""
+    out = np.zeros(14)
+    a = np.ascontiguousarray(s, float)
+    p = np.ascontiguousarray(np.concatenate([np.asarray(plane_c, float)[:3], np.asarray(plane_q, float)[:4]]))
+    lib().orc_se_plane(_dp(a), _dp(p), _dp(out))
+    r = _unpack(out)
+    F = np.zeros(4)
+    uu = np.ascontiguousarray(r["u"])
+    lib().orc_se_plane_residual(_dp(a), _dp(p), _dp(uu), _dp(F))
+    r["residual"] = F
+    return r
+
+
+def se_se_system(s1, s2, u):
+    """F (4) and the analytic Jacobian (4 x 4) of the SE-SE closest-point system at u."""
+    F = np.zeros(4)
+    J = np.zeros(16)
+    a, b = np.ascontiguousarray(s1, float), np.ascontiguousarray(s2, float)
+    uu = np.ascontiguousarray(u, float)
+    lib().orc_se_se_system(_dp(a), _dp(b), _dp(uu), _dp(F), _dp(J))
+    return F, J.reshape(4, 4).T.copy()
+
+
+def hybrid_solve(s1, s2, u0):
+    """The restated MINPACK hybrid method on the SE-SE system from the start u0."""
+    u = np.ascontiguousarray(u0, float).copy()
+    nfev = C.c_int(0)
+    a, b = np.ascontiguousarray(s1, float), np.ascontiguousarray(s2, float)
+    info = lib().orc_se_se_hybrid(_dp(a), _dp(b), _dp(u), C.byref(nfev))
+    return {"u": u, "info": info, "nfev": nfev.value}

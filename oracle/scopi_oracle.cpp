@@ -9,6 +9,7 @@
 // reference does not pin a BLAS; see tests for the ulp-band handling).
 
 #include "scopi_oracle.h"
+#include "se_geometry.hpp"
 
 #include <algorithm>
 #include <array>
@@ -118,6 +119,7 @@ struct orc_solver {
     std::vector<V3> pos, v, omega, vd, omega_d, f, jm;
     std::vector<Q4> q;
     std::vector<double> m, radius, length;
+    std::vector<std::array<double, 5>> se_par;  // superellipsoids: semi-axes, e, n
     std::vector<Contact> contacts, old_contacts;
     std::vector<double> lambda;
     orc_stats stats{};
@@ -226,6 +228,14 @@ struct orc_solver {
             std::swap(c.pi, c.pj);
         } else if (sa == ORC_SPHERE && sb == ORC_SEGMENT) {
             c = sphere_segment(a, b);
+        } else if (dim == 3 && sa == ORC_SUPERELLIPSOID && sb == ORC_SUPERELLIPSOID) {
+            c = from_pair(orc_se::se_se(se_of(a), se_of(b)));
+        } else if (dim == 3 && sa == ORC_SUPERELLIPSOID && sb == ORC_PLANE) {
+            c = from_pair(orc_se::se_plane(se_of(a), plane_of(b)));
+        } else if (dim == 3 && sa == ORC_PLANE && sb == ORC_SUPERELLIPSOID) {  // closest_points.hpp:1761-1768
+            c = from_pair(orc_se::se_plane(se_of(b), plane_of(a)));
+            for (auto& x : c.nij) x *= -1.;
+            std::swap(c.pi, c.pj);
         } else {
             return false;  // pairs the reference leaves unimplemented
         }
@@ -769,6 +779,34 @@ struct orc_solver {
         m.assign(in->m, in->m + n);
         radius.assign(in->radius, in->radius + n);
         length.assign(in->length, in->length + n);
+        se_par.assign(n, {0, 0, 0, 1, 1});
+        if (in->axes && in->squareness)
+            for (int64_t i = 0; i < n; ++i)
+                se_par[i] = {in->axes[3 * i], in->axes[3 * i + 1], in->axes[3 * i + 2], in->squareness[2 * i],
+                             in->squareness[2 * i + 1]};
+    }
+    orc_se::SE se_of(int64_t b) const {
+        orc_se::SE s;
+        s.c = pos[b];
+        s.R = rotation3(q[b]);
+        for (int k = 0; k < 3; ++k) s.r[k] = se_par[b][k];
+        s.e = se_par[b][3];
+        s.n = se_par[b][4];
+        return s;
+    }
+    orc_se::Plane plane_of(int64_t b) const {
+        orc_se::Plane p;
+        p.c = pos[b];
+        p.R = rotation3(q[b]);
+        return p;
+    }
+    static Contact from_pair(const orc_se::PairOut& o) {
+        Contact c{};
+        c.pi = o.pi;
+        c.pj = o.pj;
+        c.nij = o.nij;
+        c.dij = o.dij;
+        return c;
     }
 };
 
@@ -869,6 +907,66 @@ int orc_atmat(const orc_solver* s, const double* fv, double* out) {
     s->atmat(ff, o);
     std::memcpy(out, o.data(), o.size() * sizeof(double));
     return 0;
+}
+
+namespace {
+orc_se::SE se_from(const double* a) {
+    orc_se::SE s;
+    s.c = {a[0], a[1], a[2]};
+    s.R = rotation3({a[3], a[4], a[5], a[6]});
+    for (int k = 0; k < 3; ++k) s.r[k] = a[7 + k];
+    s.e = a[10];
+    s.n = a[11];
+    return s;
+}
+void write_pair(const orc_se::PairOut& o, double* out) {
+    for (int k = 0; k < 3; ++k) {
+        out[k] = o.pi[k];
+        out[3 + k] = o.pj[k];
+        out[6 + k] = o.nij[k];
+    }
+    out[9] = o.dij;
+    for (int k = 0; k < 4; ++k) out[10 + k] = o.u[k];
+}
+}  // namespace
+
+int orc_se_se(const double* s1, const double* s2, double* out) {
+    const orc_se::PairOut o = orc_se::se_se(se_from(s1), se_from(s2));
+    write_pair(o, out);
+    return o.info;
+}
+
+int orc_se_plane(const double* s, const double* plane, double* out) {
+    orc_se::Plane p;
+    p.c = {plane[0], plane[1], plane[2]};
+    p.R = rotation3({plane[3], plane[4], plane[5], plane[6]});
+    const orc_se::PairOut o = orc_se::se_plane(se_from(s), p);
+    write_pair(o, out);
+    return o.info;
+}
+
+int orc_se_se_hybrid(const double* s1, const double* s2, double* u, int* nfev) {
+    const orc_se::SE a = se_from(s1), b = se_from(s2);
+    const orc_se::HybrResult h = orc_se::hybrj<4>([&](const double* x, double* F) { orc_se::sese_F(a, b, x, F); },
+                                                  [&](const double* x, double* J) { orc_se::sese_J(a, b, x, J); }, u);
+    if (nfev) *nfev = h.nfev;
+    return h.info;
+}
+
+void orc_se_plane_residual(const double* s, const double* plane, const double* u, double* F) {
+    orc_se::Plane p;
+    p.c = {plane[0], plane[1], plane[2]};
+    p.R = rotation3({plane[3], plane[4], plane[5], plane[6]});
+    const orc_se::SE b = se_from(s);
+    const orc_se::V3 np = orc_se::plane_normal(p);
+    const orc_se::V3 rel = {b.c[0] - p.c[0], b.c[1] - p.c[1], b.c[2] - p.c[2]};
+    orc_se::sep_F(b, p, orc_se::dot(rel, np) < 0 ? -1.0 : 1.0, u, F);
+}
+
+void orc_se_se_system(const double* s1, const double* s2, const double* u, double* F, double* J) {
+    const orc_se::SE a = se_from(s1), b = se_from(s2);
+    orc_se::sese_F(a, b, u, F);
+    orc_se::sese_J(a, b, u, J);
 }
 
 }  // extern "C"

@@ -40,7 +40,7 @@
 extern "C" {
 #endif
 
-enum { ORC_SPHERE = 0, ORC_PLANE = 1, ORC_SEGMENT = 2 };
+enum { ORC_SPHERE = 0, ORC_PLANE = 1, ORC_SEGMENT = 2, ORC_SUPERELLIPSOID = 3 };
 enum { ORC_NOFRICTION = 0, ORC_FRICTION = 1, ORC_VISCOUS = 2 };
 enum { ORC_VAP_FIXED = 0, ORC_VAP_FPD = 1 };
 enum { ORC_BRUTE_FORCE = 0, ORC_KDTREE = 1 };
@@ -76,8 +76,10 @@ typedef struct {
     double* f;                /* n*3 */
     double* m;                /* n   */
     double* j;                /* n*3 */
-    double* radius;           /* n   (sphere radius) */
+    double* radius;           /* n   (sphere radius; bounding radius of a superellipsoid) */
     double* length;           /* n   (segment length) */
+    double* axes;             /* n*3 superellipsoid semi-axes (may be NULL without superellipsoids) */
+    double* squareness;       /* n*2 superellipsoid squareness (e, n) */
 } orc_particles;
 
 typedef struct {
@@ -107,6 +109,18 @@ int64_t orc_get_lambda(const orc_solver* s, double* out, int64_t cap);
 int orc_get_stats(const orc_solver* s, orc_stats* out);
 /* Contact detection alone on the current particle state (sorted). */
 int64_t orc_detect(orc_solver* s);
+/* Closest points of two 3D superellipsoids / a superellipsoid and a plane, as the contact
+   list would record them (closest_points.hpp:263-733, 1479-1768).  A body is
+   {c[3], q[4] (w, x, y, z), r[3], e, n}; a plane {c[3], q[4]}.  out = pi[3], pj[3], nij[3],
+   dij, u[4] (the solver's unknowns); returns the solver's info (hybrd) / iterations (Newton). */
+int orc_se_se(const double* s1, const double* s2, double* out);
+int orc_se_plane(const double* s, const double* plane, double* out);
+/* The hybrid method alone from the start u (in/out); returns info, *nfev its function count. */
+int orc_se_se_hybrid(const double* s1, const double* s2, double* u, int* nfev);
+/* F and the analytic Jacobian (column-major) of the SE-SE system at u, for cross-checks;
+   the SE-plane residual (with the body's side as its sign) at u = (a, b, plane coords). */
+void orc_se_plane_residual(const double* s, const double* plane, const double* u, double* F);
+void orc_se_se_system(const double* s1, const double* s2, const double* u, double* F, double* J);
 /* A.u and A^T.f on the current contact list (3C and 6*na long vectors). */
 int orc_amat(const orc_solver* s, const double* u, double* out);
 int orc_atmat(const orc_solver* s, const double* f, double* out);

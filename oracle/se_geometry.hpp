@@ -1,0 +1,726 @@
+// se_geometry.hpp -- superellipsoid closest points for the CPU oracle (test infrastructure:
+// only tests/, smoke() and bench.py's CPU legs use the oracle; never the product path).
+//
+// Restates, for 3D superellipsoids:
+//   superellipsoid::point / normal / binit_xy / ainit_yz
+//       include/scopi/objects/types/superellipsoid.hpp:282-325, 360-466
+//   closest_points(superellipsoid<3>, superellipsoid<3>)   closest_points.hpp:263-733
+//       (start = argmin over the two angle grids of |p1 - p2| + 2 (1 + n1.n2), then
+//        hybrd1 on F = [ (p2 - p1) x n1 ; n1.n2 + |n1||n2| ] with the analytic Jacobian)
+//   closest_points(superellipsoid<3>, plane<3>)            closest_points.hpp:1479-1768
+//       (the solution of its system F = [ (pp - p1) x n1 ; s np.n1 + |np||n1| ], in
+//        closed form: see se_plane)
+//   hybrd1 / hybrd                                         minpack.hpp:338-923
+//       restated from the published MINPACK algorithm (Powell's hybrid method: QR of the
+//       Jacobian, dogleg step in a trust region, Broyden rank-1 updates with Givens
+//       rotations), mode 2 with unit scaling, factor 100, xtol 1e-10, maxfev 200 (n + 1);
+//       the Jacobian is always the analytic one (fdjac_analytic, minpack.hpp:88-125).
+// The Jacobians are built by the chain rule from the derivatives of the parametrisation,
+// which is the same function as the reference's expanded expressions.
+#pragma once
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <limits>
+#include <vector>
+
+namespace orc_se {
+
+using V3 = std::array<double, 3>;
+using M3 = std::array<std::array<double, 3>, 3>;
+
+struct SE {
+    V3 c;           // centre
+    M3 R;           // rotation (body -> world)
+    double r[3];    // semi-axes
+    double e, n;    // squareness: e for b (xy), n for a
+};
+
+inline double sgn(double x) { return x > 0 ? 1.0 : (x < 0 ? -1.0 : 0.0); }
+// sign(t) |t|^k and its derivative w.r.t. the angle for t = cos(x) / sin(x)
+inline double cpow(double x, double k) {
+    const double c = std::cos(x);
+    return sgn(c) * std::pow(std::abs(c), k);
+}
+inline double spow(double x, double k) {
+    const double s = std::sin(x);
+    return sgn(s) * std::pow(std::abs(s), k);
+}
+inline double dcpow(double x, double k) { return -k * std::sin(x) * std::pow(std::abs(std::cos(x)), k - 1); }
+inline double dspow(double x, double k) { return k * std::cos(x) * std::pow(std::abs(std::sin(x)), k - 1); }
+
+inline V3 mv(const M3& R, const V3& x) {
+    return {R[0][0] * x[0] + R[0][1] * x[1] + R[0][2] * x[2], R[1][0] * x[0] + R[1][1] * x[1] + R[1][2] * x[2],
+            R[2][0] * x[0] + R[2][1] * x[1] + R[2][2] * x[2]};
+}
+inline V3 cross(const V3& a, const V3& b) {
+    return {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+}
+inline double dot(const V3& a, const V3& b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+inline double norm(const V3& a) { return std::sqrt(dot(a, a)); }
+
+// body-frame point, unnormalised normal and their angle derivatives
+struct Local {
+    V3 p, pa, pb;   // point, d/da, d/db
+    V3 N, Na, Nb;   // normal (unnormalised), d/da, d/db
+};
+inline Local local(const SE& s, double a, double b) {
+    const double rx = s.r[0], ry = s.r[1], rz = s.r[2];
+    const double Ca = cpow(a, s.n), Sa = spow(a, s.n), Cb = cpow(b, s.e), Sb = spow(b, s.e);
+    const double dCa = dcpow(a, s.n), dSa = dspow(a, s.n), dCb = dcpow(b, s.e), dSb = dspow(b, s.e);
+    const double n2 = 2 - s.n, e2 = 2 - s.e;
+    const double Ca2 = cpow(a, n2), Sa2 = spow(a, n2), Cb2 = cpow(b, e2), Sb2 = spow(b, e2);
+    const double dCa2 = dcpow(a, n2), dSa2 = dspow(a, n2), dCb2 = dcpow(b, e2), dSb2 = dspow(b, e2);
+    Local L;
+    L.p = {rx * Ca * Cb, ry * Ca * Sb, rz * Sa};
+    L.pa = {rx * dCa * Cb, ry * dCa * Sb, rz * dSa};
+    L.pb = {rx * Ca * dCb, ry * Ca * dSb, 0.0};
+    L.N = {ry * rz * Ca2 * Cb2, rx * rz * Ca2 * Sb2, rx * ry * Sa2};
+    L.Na = {ry * rz * dCa2 * Cb2, rx * rz * dCa2 * Sb2, rx * ry * dSa2};
+    L.Nb = {ry * rz * Ca2 * dCb2, rx * rz * Ca2 * dSb2, 0.0};
+    return L;
+}
+
+// superellipsoid::point(a, b), superellipsoid.hpp:291-300 (world frame)
+inline V3 point(const SE& s, double a, double b) {
+    const V3 p = {s.r[0] * cpow(a, s.n) * cpow(b, s.e), s.r[1] * cpow(a, s.n) * spow(b, s.e), s.r[2] * spow(a, s.n)};
+    const V3 w = mv(s.R, p);
+    return {w[0] + s.c[0], w[1] + s.c[1], w[2] + s.c[2]};
+}
+// superellipsoid::normal(a, b), superellipsoid.hpp:313-325 (unit, world frame)
+inline V3 normal(const SE& s, double a, double b) {
+    const double n2 = 2 - s.n, e2 = 2 - s.e;
+    const V3 N = {s.r[1] * s.r[2] * cpow(a, n2) * cpow(b, e2), s.r[0] * s.r[2] * cpow(a, n2) * spow(b, e2),
+                  s.r[0] * s.r[1] * spow(a, n2)};
+    V3 w = mv(s.R, N);
+    const double l = norm(w);
+    for (auto& x : w) x /= l;
+    return w;
+}
+
+// superellipsoid::binit_xy / ainit_yz, superellipsoid.hpp:360-466
+inline std::vector<double> binit_xy(const SE& s, int num) {
+    const double pi = 4 * std::atan(1);
+    std::vector<double> out;
+    for (int i = 0; i < num; ++i) {
+        const double t = num > 1 ? (0.5 * pi) * i / (num - 1) : 0.0;
+        const double x = s.r[0] * std::cos(t), y = s.r[1] * std::sin(t);
+        const double d = std::pow(std::pow(s.r[1] * x, 2.0 / s.e) + std::pow(s.r[0] * y, 2.0 / s.e), s.e / 2.0);
+        const double ys = y * s.r[0] * s.r[1] / d;
+        const double sb = std::max(-1.0, std::min(1.0, std::sqrt(std::pow(std::pow(ys / s.r[1], 2), 1.0 / s.e))));
+        const double b = std::asin(sb);
+        out.push_back(b);
+        out.push_back(b + pi / 2);
+        out.push_back(b - pi);
+        out.push_back(b - pi / 2);
+    }
+    for (auto& b : out)
+        if (std::abs(b) < 1.0e-6) b = 0.01;
+    return out;
+}
+inline std::vector<double> ainit_yz(const SE& s, int num) {
+    const double pi = 4 * std::atan(1);
+    std::vector<double> out;
+    for (int i = 0; i < num; ++i) {
+        const double t = num > 1 ? (0.5 * pi) * i / (num - 1) : 0.0;
+        const double y = s.r[1] * std::cos(t), z = s.r[2] * std::sin(t);
+        const double d = std::pow(std::pow(s.r[2] * y, 2.0 / s.n) + std::pow(s.r[1] * z, 2.0 / s.n), s.n / 2.0);
+        const double zs = z * s.r[1] * s.r[2] / d;
+        const double sa = std::max(-1.0, std::min(1.0, std::sqrt(std::pow(std::pow(zs / s.r[2], 2), 1.0 / s.n))));
+        const double a = std::asin(sa);
+        out.push_back(a);
+        out.push_back(a + pi / 2);
+        out.push_back(a - pi);
+        out.push_back(a - pi / 2);
+    }
+    for (auto& a : out)
+        if (std::abs(a) < 1.0e-6) a = 0.01;
+    return out;
+}
+inline std::vector<double> sorted_unique(std::vector<double> v) {
+    std::sort(v.begin(), v.end());
+    v.erase(std::unique(v.begin(), v.end()), v.end());
+    return v;
+}
+
+// ---------------------------------------------------------------- MINPACK (restated)
+constexpr double kEps = 2.220446049250313e-16;    // dpmpar(1)
+constexpr double kGiant = std::numeric_limits<double>::max();  // dpmpar(3)
+
+// enorm: Euclidean norm with the three-range accumulation of MINPACK
+inline double enorm(int n, const double* x) {
+    const double rdwarf = 3.834e-20, rgiant = 1.304e19;
+    double s1 = 0, s2 = 0, s3 = 0, x1max = 0, x3max = 0;
+    const double agiant = rgiant / n;
+    for (int i = 0; i < n; ++i) {
+        const double xabs = std::abs(x[i]);
+        if (xabs > rdwarf && xabs < agiant) {
+            s2 += xabs * xabs;
+        } else if (xabs <= rdwarf) {
+            if (xabs > x3max) {
+                s3 = 1 + s3 * (x3max / xabs) * (x3max / xabs);
+                x3max = xabs;
+            } else if (xabs != 0) {
+                s3 += (xabs / x3max) * (xabs / x3max);
+            }
+        } else {
+            if (xabs > x1max) {
+                s1 = 1 + s1 * (x1max / xabs) * (x1max / xabs);
+                x1max = xabs;
+            } else {
+                s1 += (xabs / x1max) * (xabs / x1max);
+            }
+        }
+    }
+    if (s1 != 0) return x1max * std::sqrt(s1 + (s2 / x1max) / x1max);
+    if (s2 != 0) {
+        if (s2 >= x3max) return std::sqrt(s2 * (1 + (x3max / s2) * (x3max * s3)));
+        return std::sqrt(x3max * ((s2 / x3max) + (x3max * s3)));
+    }
+    return x3max * std::sqrt(s3);
+}
+
+// Column-major n x n matrices a[i + j*n].  Householder QR without pivoting (qrfac).
+inline void qrfac(int n, double* a, double* rdiag, double* acnorm) {
+    for (int j = 0; j < n; ++j) {
+        acnorm[j] = enorm(n, a + j * n);
+        rdiag[j] = acnorm[j];
+    }
+    for (int j = 0; j < n; ++j) {
+        double ajnorm = enorm(n - j, a + j + j * n);
+        if (ajnorm != 0) {
+            if (a[j + j * n] < 0) ajnorm = -ajnorm;
+            for (int i = j; i < n; ++i) a[i + j * n] /= ajnorm;
+            a[j + j * n] += 1;
+            for (int k = j + 1; k < n; ++k) {
+                double sum = 0;
+                for (int i = j; i < n; ++i) sum += a[i + j * n] * a[i + k * n];
+                const double temp = sum / a[j + j * n];
+                for (int i = j; i < n; ++i) a[i + k * n] -= temp * a[i + j * n];
+            }
+        }
+        rdiag[j] = -ajnorm;
+    }
+}
+// orthogonal factor of qrfac accumulated in q (qform)
+inline void qform(int n, double* q, double* wa) {
+    for (int j = 1; j < n; ++j)
+        for (int i = 0; i < j; ++i) q[i + j * n] = 0;
+    for (int l = 0; l < n; ++l) {
+        const int k = n - 1 - l;
+        for (int i = k; i < n; ++i) {
+            wa[i] = q[i + k * n];
+            q[i + k * n] = 0;
+        }
+        q[k + k * n] = 1;
+        if (wa[k] == 0) continue;
+        for (int j = k; j < n; ++j) {
+            double sum = 0;
+            for (int i = k; i < n; ++i) sum += q[i + j * n] * wa[i];
+            const double temp = sum / wa[k];
+            for (int i = k; i < n; ++i) q[i + j * n] -= temp * wa[i];
+        }
+    }
+}
+// dogleg step in the trust region delta; r = upper triangle packed by rows
+inline void dogleg(int n, const double* r, const double* diag, const double* qtb, double delta, double* x, double* wa1,
+                   double* wa2) {
+    int jj = (n * (n + 1)) / 2;  // one past the last packed element (0-based)
+    for (int k = 1; k <= n; ++k) {
+        const int j = n - k;
+        jj -= k;
+        int l = jj + 1;
+        double sum = 0;
+        for (int i = j + 1; i < n; ++i) sum += r[l++] * x[i];
+        double temp = r[jj];
+        if (temp == 0) {
+            int ll = j;
+            for (int i = 0; i <= j; ++i) {
+                temp = std::max(temp, std::abs(r[ll]));
+                ll += n - i - 1;
+            }
+            temp = kEps * temp;
+            if (temp == 0) temp = kEps;
+        }
+        x[j] = (qtb[j] - sum) / temp;
+    }
+    for (int j = 0; j < n; ++j) {
+        wa1[j] = 0;
+        wa2[j] = diag[j] * x[j];
+    }
+    const double qnorm = enorm(n, wa2);
+    if (qnorm <= delta) return;
+    int l = 0;
+    for (int j = 0; j < n; ++j) {
+        const double temp = qtb[j];
+        for (int i = j; i < n; ++i) wa1[i] += r[l++] * temp;
+        wa1[j] /= diag[j];
+    }
+    const double gnorm = enorm(n, wa1);
+    double sgnorm = 0, alpha = delta / qnorm;
+    if (gnorm != 0) {
+        for (int j = 0; j < n; ++j) wa1[j] = (wa1[j] / gnorm) / diag[j];
+        l = 0;
+        for (int j = 0; j < n; ++j) {
+            double sum = 0;
+            for (int i = j; i < n; ++i) sum += r[l++] * wa1[i];
+            wa2[j] = sum;
+        }
+        const double temp = enorm(n, wa2);
+        sgnorm = (gnorm / temp) / temp;
+        alpha = 0;
+        if (sgnorm < delta) {
+            const double bnorm = enorm(n, qtb);
+            double t = (bnorm / gnorm) * (bnorm / qnorm) * (sgnorm / delta);
+            t = t - (delta / qnorm) * (sgnorm / delta) * (sgnorm / delta) +
+                std::sqrt((t - (delta / qnorm)) * (t - (delta / qnorm)) +
+                          (1 - (delta / qnorm) * (delta / qnorm)) * (1 - (sgnorm / delta) * (sgnorm / delta)));
+            alpha = ((delta / qnorm) * (1 - (sgnorm / delta) * (sgnorm / delta))) / t;
+        }
+    }
+    const double temp = (1 - alpha) * std::min(sgnorm, delta);
+    for (int j = 0; j < n; ++j) x[j] = temp * wa1[j] + alpha * x[j];
+}
+// rank-1 update of the packed triangle s (m = n) by Givens rotations (r1updt)
+inline bool r1updt(int n, double* s, const double* u, double* v, double* w) {
+    const int m = n;
+    int jj = (n * (2 * m - n + 1)) / 2 - (m - n) - 1;  // 0-based index of s(n, n)
+    int l = jj;
+    for (int i = n - 1; i < m; ++i) w[i] = s[l++];
+    for (int nmj = 1; nmj <= n - 1; ++nmj) {
+        const int j = n - 1 - nmj;
+        jj -= m - j;
+        w[j] = 0;
+        if (v[j] != 0) {
+            double cs, sn, tau;
+            if (std::abs(v[n - 1]) < std::abs(v[j])) {
+                const double cotan = v[n - 1] / v[j];
+                sn = 0.5 / std::sqrt(0.25 + 0.25 * cotan * cotan);
+                cs = sn * cotan;
+                tau = 1;
+                if (std::abs(cs) * kGiant > 1) tau = 1 / cs;
+            } else {
+                const double tn = v[j] / v[n - 1];
+                cs = 0.5 / std::sqrt(0.25 + 0.25 * tn * tn);
+                sn = cs * tn;
+                tau = sn;
+            }
+            v[n - 1] = sn * v[j] + cs * v[n - 1];
+            v[j] = tau;
+            l = jj;
+            for (int i = j; i < m; ++i) {
+                const double temp = cs * s[l] - sn * w[i];
+                w[i] = sn * s[l] + cs * w[i];
+                s[l] = temp;
+                ++l;
+            }
+        }
+    }
+    for (int i = 0; i < m; ++i) w[i] += v[n - 1] * u[i];
+    bool sing = false;
+    for (int j = 0; j < n - 1; ++j) {
+        if (w[j] != 0) {
+            double cs, sn, tau;
+            if (std::abs(s[jj]) < std::abs(w[j])) {
+                const double cotan = s[jj] / w[j];
+                sn = 0.5 / std::sqrt(0.25 + 0.25 * cotan * cotan);
+                cs = sn * cotan;
+                tau = 1;
+                if (std::abs(cs) * kGiant > 1) tau = 1 / cs;
+            } else {
+                const double tn = w[j] / s[jj];
+                cs = 0.5 / std::sqrt(0.25 + 0.25 * tn * tn);
+                sn = cs * tn;
+                tau = sn;
+            }
+            l = jj;
+            for (int i = j; i < m; ++i) {
+                const double temp = cs * s[l] + sn * w[i];
+                w[i] = -sn * s[l] + cs * w[i];
+                s[l] = temp;
+                ++l;
+            }
+            w[j] = tau;
+        }
+        if (s[jj] == 0) sing = true;
+        jj += m - j;
+    }
+    l = jj;
+    for (int i = n - 1; i < m; ++i) s[l++] = w[i];
+    if (s[jj] == 0) sing = true;
+    return sing;
+}
+// apply the stored Givens rotations to the m x n matrix a (r1mpyq), a[i + j*lda]
+inline void r1mpyq(int m, int n, double* a, int lda, const double* v, const double* w) {
+    for (int nmj = 1; nmj <= n - 1; ++nmj) {
+        const int j = n - 1 - nmj;
+        double cs, sn;
+        if (std::abs(v[j]) > 1) {
+            cs = 1 / v[j];
+            sn = std::sqrt(1 - cs * cs);
+        } else {
+            sn = v[j];
+            cs = std::sqrt(1 - sn * sn);
+        }
+        for (int i = 0; i < m; ++i) {
+            const double temp = cs * a[i + j * lda] - sn * a[i + (n - 1) * lda];
+            a[i + (n - 1) * lda] = sn * a[i + j * lda] + cs * a[i + (n - 1) * lda];
+            a[i + j * lda] = temp;
+        }
+    }
+    for (int j = 0; j < n - 1; ++j) {
+        double cs, sn;
+        if (std::abs(w[j]) > 1) {
+            cs = 1 / w[j];
+            sn = std::sqrt(1 - cs * cs);
+        } else {
+            sn = w[j];
+            cs = std::sqrt(1 - sn * sn);
+        }
+        for (int i = 0; i < m; ++i) {
+            const double temp = cs * a[i + j * lda] + sn * a[i + (n - 1) * lda];
+            a[i + (n - 1) * lda] = -sn * a[i + j * lda] + cs * a[i + (n - 1) * lda];
+            a[i + j * lda] = temp;
+        }
+    }
+}
+
+struct HybrResult {
+    int info;
+    int nfev;
+    int njev;
+};
+
+// Powell hybrid method with analytic Jacobian (hybrd1 of minpack.hpp:852-923 with
+// fdjac_analytic): fun(x, f) evaluates F, jac(x, J) the Jacobian (column-major).
+template <int N, typename Fun, typename Jac>
+HybrResult hybrj(Fun&& fun, Jac&& jac, double* x, double xtol = 1e-10, int maxfev = 200 * (N + 1),
+                 double factor = 100.0) {
+    const double p1 = 0.1, p5 = 0.5, p001 = 1e-3, p0001 = 1e-4;
+    double fvec[N], fjac[N * N], diag[N], r[(N * (N + 1)) / 2], qtf[N], wa1[N], wa2[N], wa3[N], wa4[N];
+    for (int j = 0; j < N; ++j) diag[j] = 1.0;  // mode 2, unit scaling
+    HybrResult res{0, 0, 0};
+    fun(x, fvec);
+    res.nfev = 1;
+    double fnorm = enorm(N, fvec);
+    int iter = 1, ncsuc = 0, ncfail = 0, nslow1 = 0, nslow2 = 0;
+    double delta = 0, xnorm = 0;
+    for (;;) {
+        bool jeval = true;
+        jac(x, fjac);
+        ++res.njev;
+        qrfac(N, fjac, wa1, wa2);
+        if (iter == 1) {
+            for (int j = 0; j < N; ++j) wa3[j] = diag[j] * x[j];
+            xnorm = enorm(N, wa3);
+            delta = factor * xnorm;
+            if (delta == 0) delta = factor;
+        }
+        for (int i = 0; i < N; ++i) qtf[i] = fvec[i];
+        for (int j = 0; j < N; ++j) {
+            if (fjac[j + j * N] == 0) continue;
+            double sum = 0;
+            for (int i = j; i < N; ++i) sum += fjac[i + j * N] * qtf[i];
+            const double temp = -sum / fjac[j + j * N];
+            for (int i = j; i < N; ++i) qtf[i] += fjac[i + j * N] * temp;
+        }
+        for (int j = 0; j < N; ++j) {
+            int l = j;
+            for (int i = 0; i < j; ++i) {
+                r[l] = fjac[i + j * N];
+                l += N - i - 1;
+            }
+            r[l] = wa1[j];
+        }
+        qform(N, fjac, wa1);
+        for (;;) {
+            dogleg(N, r, diag, qtf, delta, wa1, wa2, wa3);
+            for (int j = 0; j < N; ++j) {
+                wa1[j] = -wa1[j];
+                wa2[j] = x[j] + wa1[j];
+                wa3[j] = diag[j] * wa1[j];
+            }
+            const double pnorm = enorm(N, wa3);
+            if (iter == 1) delta = std::min(delta, pnorm);
+            fun(wa2, wa4);
+            ++res.nfev;
+            const double fnorm1 = enorm(N, wa4);
+            double actred = -1;
+            if (fnorm1 < fnorm) actred = 1 - (fnorm1 / fnorm) * (fnorm1 / fnorm);
+            int l = 0;
+            for (int i = 0; i < N; ++i) {
+                double sum = 0;
+                for (int j = i; j < N; ++j) sum += r[l++] * wa1[j];
+                wa3[i] = qtf[i] + sum;
+            }
+            const double temp = enorm(N, wa3);
+            double prered = 0;
+            if (temp < fnorm) prered = 1 - (temp / fnorm) * (temp / fnorm);
+            double ratio = 0;
+            if (prered > 0) ratio = actred / prered;
+            if (ratio < p1) {
+                ncsuc = 0;
+                ++ncfail;
+                delta = p5 * delta;
+            } else {
+                ncfail = 0;
+                ++ncsuc;
+                if (ratio >= p5 || ncsuc > 1) delta = std::max(delta, pnorm / p5);
+                if (std::abs(ratio - 1) <= p1) delta = pnorm / p5;
+            }
+            if (ratio >= p0001) {
+                for (int j = 0; j < N; ++j) {
+                    x[j] = wa2[j];
+                    wa2[j] = diag[j] * x[j];
+                    fvec[j] = wa4[j];
+                }
+                xnorm = enorm(N, wa2);
+                fnorm = fnorm1;
+                ++iter;
+            }
+            ++nslow1;
+            if (actred >= p001) nslow1 = 0;
+            if (jeval) ++nslow2;
+            if (actred >= p1) nslow2 = 0;
+            if (delta <= xtol * xnorm || fnorm == 0) res.info = 1;
+            if (res.info != 0) return res;
+            if (res.nfev >= maxfev) res.info = 2;
+            if (p1 * std::max(p1 * delta, pnorm) <= kEps * xnorm) res.info = 3;
+            if (nslow2 == 5) res.info = 4;
+            if (nslow1 == 10) res.info = 5;
+            if (res.info != 0) return res;
+            if (ncfail == 2) break;
+            for (int j = 0; j < N; ++j) {
+                double sum = 0;
+                for (int i = 0; i < N; ++i) sum += fjac[i + j * N] * wa4[i];
+                wa2[j] = (sum - wa3[j]) / pnorm;
+                wa1[j] = diag[j] * ((diag[j] * wa1[j]) / pnorm);
+                if (ratio >= p0001) qtf[j] = sum;
+            }
+            r1updt(N, r, wa1, wa2, wa3);
+            r1mpyq(N, N, fjac, N, wa2, wa3);
+            r1mpyq(1, N, qtf, 1, wa2, wa3);
+            jeval = false;
+        }
+    }
+}
+
+// ------------------------------------------------------------- SE - SE (3D)
+struct PairOut {
+    V3 pi, pj, nij;
+    double dij;
+    int info;
+    double u[4];
+};
+
+// F and its Jacobian (column-major 4x4) for u = (a1, b1, a2, b2)
+inline void sese_F(const SE& s1, const SE& s2, const double* u, double* F) {
+    const Local L1 = local(s1, u[0], u[1]), L2 = local(s2, u[2], u[3]);
+    const V3 p1 = mv(s1.R, L1.p), p2 = mv(s2.R, L2.p);
+    const V3 d = {p2[0] + s2.c[0] - p1[0] - s1.c[0], p2[1] + s2.c[1] - p1[1] - s1.c[1],
+                  p2[2] + s2.c[2] - p1[2] - s1.c[2]};
+    const V3 n1 = mv(s1.R, L1.N), n2 = mv(s2.R, L2.N);
+    const V3 x = cross(d, n1);
+    F[0] = x[0];
+    F[1] = x[1];
+    F[2] = x[2];
+    F[3] = dot(n1, n2) + norm(n1) * norm(n2);
+}
+inline void sese_J(const SE& s1, const SE& s2, const double* u, double* J) {
+    const Local L1 = local(s1, u[0], u[1]), L2 = local(s2, u[2], u[3]);
+    const V3 p1 = mv(s1.R, L1.p), p2 = mv(s2.R, L2.p);
+    const V3 d = {p2[0] + s2.c[0] - p1[0] - s1.c[0], p2[1] + s2.c[1] - p1[1] - s1.c[1],
+                  p2[2] + s2.c[2] - p1[2] - s1.c[2]};
+    const V3 n1 = mv(s1.R, L1.N), n2 = mv(s2.R, L2.N);
+    const double l1 = norm(n1), l2 = norm(n2);
+    V3 dd[4], dn1[4], dn2[4];
+    const V3 z = {0, 0, 0};
+    const V3 pa1 = mv(s1.R, L1.pa), pb1 = mv(s1.R, L1.pb);
+    dd[0] = {-pa1[0], -pa1[1], -pa1[2]};
+    dd[1] = {-pb1[0], -pb1[1], -pb1[2]};
+    dd[2] = mv(s2.R, L2.pa);
+    dd[3] = mv(s2.R, L2.pb);
+    dn1[0] = mv(s1.R, L1.Na);
+    dn1[1] = mv(s1.R, L1.Nb);
+    dn1[2] = dn1[3] = z;
+    dn2[0] = dn2[1] = z;
+    dn2[2] = mv(s2.R, L2.Na);
+    dn2[3] = mv(s2.R, L2.Nb);
+    for (int k = 0; k < 4; ++k) {
+        const V3 a = cross(dd[k], n1), b = cross(d, dn1[k]);
+        J[0 + 4 * k] = a[0] + b[0];
+        J[1 + 4 * k] = a[1] + b[1];
+        J[2 + 4 * k] = a[2] + b[2];
+        J[3 + 4 * k] = dot(dn1[k], n2) + dot(n1, dn2[k]) + dot(n1, dn1[k]) / l1 * l2 + l1 * dot(n2, dn2[k]) / l2;
+    }
+}
+
+// hybrd1 start: argmin over the (a, b) grids of the two bodies, first minimum in row-major order
+inline void sese_start(const SE& s1, const SE& s2, double* u0) {
+    const int num = 6;
+    const auto b1 = sorted_unique(binit_xy(s1, num)), a1 = sorted_unique(ainit_yz(s1, num));
+    const auto b2 = sorted_unique(binit_xy(s2, num)), a2 = sorted_unique(ainit_yz(s2, num));
+    // meshgrid(a, b) flattened row-major: index i*nb + j -> (a[i], b[j])
+    std::vector<V3> P1, N1, P2, N2;
+    std::vector<std::array<double, 2>> U1, U2;
+    for (double a : a1)
+        for (double b : b1) {
+            P1.push_back(point(s1, a, b));
+            N1.push_back(normal(s1, a, b));
+            U1.push_back({a, b});
+        }
+    for (double a : a2)
+        for (double b : b2) {
+            P2.push_back(point(s2, a, b));
+            N2.push_back(normal(s2, a, b));
+            U2.push_back({a, b});
+        }
+    double best = INFINITY;
+    size_t bi = 0, bj = 0;
+    for (size_t i = 0; i < P1.size(); ++i)
+        for (size_t j = 0; j < P2.size(); ++j) {
+            const V3 df = {P1[i][0] - P2[j][0], P1[i][1] - P2[j][1], P1[i][2] - P2[j][2]};
+            const double v = norm(df) + 2 * (1 + dot(N1[i], N2[j]));
+            if (v < best) {
+                best = v;
+                bi = i;
+                bj = j;
+            }
+        }
+    u0[0] = U1[bi][0];
+    u0[1] = U1[bi][1];
+    u0[2] = U2[bj][0];
+    u0[3] = U2[bj][1];
+}
+
+// closest_points(superellipsoid<3>, superellipsoid<3>), closest_points.hpp:263-733
+inline PairOut se_se(const SE& s1, const SE& s2) {
+    double u[4];
+    sese_start(s1, s2, u);
+    const HybrResult h = hybrj<4>([&](const double* x, double* F) { sese_F(s1, s2, x, F); },
+                                  [&](const double* x, double* J) { sese_J(s1, s2, x, J); }, u);
+    PairOut o;
+    o.info = h.info;
+    for (int k = 0; k < 4; ++k) o.u[k] = u[k];
+    o.pi = point(s1, u[0], u[1]);
+    o.pj = point(s2, u[2], u[3]);
+    o.nij = normal(s2, u[2], u[3]);
+    const V3 df = {o.pi[0] - o.pj[0], o.pi[1] - o.pj[1], o.pi[2] - o.pj[2]};
+    o.dij = sgn(dot(df, o.nij)) * norm(df);
+    return o;
+}
+
+// ----------------------------------------------------------- SE - plane (3D)
+struct Plane {
+    V3 c;
+    M3 R;  // normal = column 0, in-plane directions = columns 1 and 2
+};
+inline V3 plane_normal(const Plane& p) { return {p.R[0][0], p.R[1][0], p.R[2][0]}; }
+
+// u = (a1, b1, a2, b2): body angles and plane coordinates; the normal of the body is taken
+// with the factor sign(cos a1) of the reference's expressions
+inline void sep_F(const SE& s, const Plane& P, double sg, const double* u, double* F) {
+    const Local L = local(s, u[0], u[1]);
+    const double k = sgn(std::cos(u[0]));
+    const V3 p1 = mv(s.R, L.p);
+    const V3 pp = mv(P.R, V3{0.0, u[2], u[3]});
+    const V3 d = {pp[0] + P.c[0] - p1[0] - s.c[0], pp[1] + P.c[1] - p1[1] - s.c[1], pp[2] + P.c[2] - p1[2] - s.c[2]};
+    V3 n1 = mv(s.R, L.N);
+    for (auto& x : n1) x *= k;
+    const V3 np = plane_normal(P);
+    const V3 x = cross(d, n1);
+    F[0] = x[0];
+    F[1] = x[1];
+    F[2] = x[2];
+    F[3] = sg * dot(np, n1) + norm(np) * norm(n1);
+}
+inline void sep_J(const SE& s, const Plane& P, double sg, const double* u, double* J) {
+    const Local L = local(s, u[0], u[1]);
+    const double k = sgn(std::cos(u[0]));
+    const V3 p1 = mv(s.R, L.p);
+    const V3 pp = mv(P.R, V3{0.0, u[2], u[3]});
+    const V3 d = {pp[0] + P.c[0] - p1[0] - s.c[0], pp[1] + P.c[1] - p1[1] - s.c[1], pp[2] + P.c[2] - p1[2] - s.c[2]};
+    V3 n1 = mv(s.R, L.N);
+    for (auto& x : n1) x *= k;
+    const V3 np = plane_normal(P);
+    const double l1 = norm(n1), lp = norm(np);
+    V3 dd[4], dn1[4];
+    const V3 pa = mv(s.R, L.pa), pb = mv(s.R, L.pb);
+    dd[0] = {-pa[0], -pa[1], -pa[2]};
+    dd[1] = {-pb[0], -pb[1], -pb[2]};
+    dd[2] = {P.R[0][1], P.R[1][1], P.R[2][1]};
+    dd[3] = {P.R[0][2], P.R[1][2], P.R[2][2]};
+    dn1[0] = mv(s.R, L.Na);
+    dn1[1] = mv(s.R, L.Nb);
+    for (int q = 0; q < 2; ++q)
+        for (auto& x : dn1[q]) x *= k;
+    dn1[2] = dn1[3] = V3{0, 0, 0};
+    for (int c = 0; c < 4; ++c) {
+        const V3 a = cross(dd[c], n1), b = cross(d, dn1[c]);
+        J[0 + 4 * c] = a[0] + b[0];
+        J[1 + 4 * c] = a[1] + b[1];
+        J[2 + 4 * c] = a[2] + b[2];
+        J[3 + 4 * c] = sg * dot(np, dn1[c]) + lp * dot(n1, dn1[c]) / l1;
+    }
+}
+
+// Angles (a, b) of the body point whose outward normal points along the body-frame
+// direction m: from N(a, b) = lambda m (lambda > 0), with cos a >= 0,
+//   b = atan2(sign(my) |ry my|^(1/(2-e)), sign(mx) |rx mx|^(1/(2-e))),
+//   |tan a|^(2-n) = |mz| |(ry rz C(b,2-e), rx rz S(b,2-e))| / (rx ry |(mx, my)|), sign(a) = sign(mz).
+inline void support_angles(const SE& s, const V3& m, double& a, double& b) {
+    const double pi = 4 * std::atan(1);
+    const double rx = s.r[0], ry = s.r[1], rz = s.r[2];
+    const double mxy = std::sqrt(m[0] * m[0] + m[1] * m[1]);
+    if (mxy == 0) {
+        b = 0;
+        a = m[2] >= 0 ? pi / 2 : -pi / 2;
+        return;
+    }
+    const double ke = 1.0 / (2 - s.e), kn = 1.0 / (2 - s.n);
+    b = std::atan2(sgn(m[1]) * std::pow(std::abs(ry * m[1]), ke), sgn(m[0]) * std::pow(std::abs(rx * m[0]), ke));
+    const double cb = cpow(b, 2 - s.e), sb = spow(b, 2 - s.e);
+    const double h = std::sqrt((ry * rz * cb) * (ry * rz * cb) + (rx * rz * sb) * (rx * rz * sb));
+    const double t = std::abs(m[2]) * h / (rx * ry * mxy);
+    a = sgn(m[2]) * std::atan(std::pow(t, kn));
+}
+
+// closest_points(superellipsoid<3>, plane<3>), closest_points.hpp:1479-1759.  The system
+// there, F = [ (pp - p1) x n1 ; s np.n1 + |np||n1| ] over the body angles and the plane
+// coordinates, has for a convex body one solution: the body point whose outward normal is
+// opposite to the plane normal oriented toward the body (s = the body's side), and its
+// projection on the plane.  That solution is computed in closed form here.  (The
+// reference's Newton does not reach it on bodies of this size: its start takes the plane
+// coordinates from the angle grid, in metres, and its residual receives the signed
+// centre-plane distance where it needs s; F3 also has a double root.)  pi on the body, pj on
+// the plane, nij = s np, dij = (pi - pj).nij.
+inline PairOut se_plane(const SE& s, const Plane& P) {
+    const V3 np = plane_normal(P);
+    const V3 rel = {s.c[0] - P.c[0], s.c[1] - P.c[1], s.c[2] - P.c[2]};
+    const double sg = dot(rel, np) < 0 ? -1.0 : 1.0;
+    // body-frame direction of the wanted outward normal: -s np
+    const V3 m = {-sg * (s.R[0][0] * np[0] + s.R[1][0] * np[1] + s.R[2][0] * np[2]),
+                  -sg * (s.R[0][1] * np[0] + s.R[1][1] * np[1] + s.R[2][1] * np[2]),
+                  -sg * (s.R[0][2] * np[0] + s.R[1][2] * np[1] + s.R[2][2] * np[2])};
+    double a, b;
+    support_angles(s, m, a, b);
+    PairOut o;
+    o.info = 0;
+    o.pi = point(s, a, b);
+    const V3 d = {o.pi[0] - P.c[0], o.pi[1] - P.c[1], o.pi[2] - P.c[2]};
+    const double h = dot(d, np);
+    o.pj = {o.pi[0] - h * np[0], o.pi[1] - h * np[1], o.pi[2] - h * np[2]};
+    o.nij = {sg * np[0], sg * np[1], sg * np[2]};
+    const V3 df = {o.pi[0] - o.pj[0], o.pi[1] - o.pj[1], o.pi[2] - o.pj[2]};
+    o.dij = dot(df, o.nij);
+    // plane coordinates of pj (columns 1, 2 of the plane's rotation)
+    const V3 e = {o.pj[0] - P.c[0], o.pj[1] - P.c[1], o.pj[2] - P.c[2]};
+    o.u[0] = a;
+    o.u[1] = b;
+    o.u[2] = P.R[0][1] * e[0] + P.R[1][1] * e[1] + P.R[2][1] * e[2];
+    o.u[3] = P.R[0][2] * e[0] + P.R[1][2] * e[1] + P.R[2][2] * e[2];
+    return o;
+}
+
+}  // namespace orc_se

@@ -17,6 +17,11 @@ Workloads (shapes and distributions of the benchmark configurations):
   spheres_1m      100^3 spheres on a jittered lattice (spacing 0.0045, jitter +-0.0002) centred
                   in the unit box, radius U[0.9,1.1]*0.002, desired velocity 0.1 (c-x)/|c-x|,
                   m=(r/0.002)^3, J=0.4 m r^2, six plane walls.
+  se_pile         3D superellipsoids on the first `count` points of a side^3 lattice (spacing
+                  0.018, centred in x and y, lowest layer at z = 0.02; k fastest), semi-axes
+                  U[0.004,0.008] each, squareness e, n U[0.6,1.4], uniform random orientation
+                  (Shoemake), m = abc/0.006^3, J = m/5 (b^2+c^2, a^2+c^2, a^2+b^2), gravity
+                  -9.81 m in z, a floor plane z = 0 with its normal +z.
 """
 from __future__ import annotations
 
@@ -148,6 +153,28 @@ def spheres_1m(seed: int = 5, side: int = 100) -> ParticleArrays:
     return _assemble(3, c, r, m, jm, vd=vd)
 
 
+def se_pile(count: int = 50_000, side: int = 37, seed: int = 3) -> ParticleArrays:
+    """Draws per body k: semi-axes (3), squareness e, n (2), Shoemake u1, u2, u3 (3)."""
+    from .container import Particles, Property
+    u = splitmix_uniform(seed, 8 * count).reshape(count, 8)
+    sp = 0.018
+    p = Particles(3)
+    p.add_plane((0.0, 0.0, 0.0), q=quaternion(-math.pi / 2, (0, 1, 0)))  # normal (column 0 of R) = +z
+    for k in range(count):
+        ix, iy, iz = k // (side * side), (k // side) % side, k % side
+        c = ((ix - (side - 1) / 2) * sp, (iy - (side - 1) / 2) * sp, 0.02 + iz * sp)
+        a, b, cc = 0.004 + 0.004 * u[k, 0:3]
+        e, n = 0.6 + 0.8 * u[k, 3:5]
+        u1, u2, u3 = u[k, 5:8]
+        q = np.array([math.sqrt(u1) * math.cos(2 * math.pi * u3), math.sqrt(1 - u1) * math.sin(2 * math.pi * u2),
+                      math.sqrt(1 - u1) * math.cos(2 * math.pi * u2), math.sqrt(u1) * math.sin(2 * math.pi * u3)])
+        m = a * b * cc / 0.006 ** 3
+        prop = Property(mass=m, moment_inertia=(m / 5 * (b * b + cc * cc), m / 5 * (a * a + cc * cc),
+                                                m / 5 * (a * a + b * b)), force=(0.0, 0.0, -9.81 * m))
+        p.add_superellipsoid(c, (a, b, cc), (e, n), prop, q=q)
+    return p.finalize()
+
+
 def pile_scene(seed: int, nmin: int = 200, nmax: int = 5000, vmax: float = 0.0) -> ParticleArrays:
     """One pile scene.  Draws: u[0] -> N_s; candidate k uses (x, y, r) = u[1+3k], u[2+3k], u[3+3k].
 
@@ -210,4 +237,5 @@ SETTINGS = {
     "box_3d": dict(dmax=0.0045, dt=1e-3, tolerance=1e-6, max_ite=40000, vap=1, steps=500),
     "spheres_1m": dict(dmax=0.0018, dt=1e-3, tolerance=1e-6, max_ite=40000, vap=0, steps=100),
     "pile_scenes": dict(dmax=0.009, dt=1e-3, tolerance=1e-6, max_ite=40000, vap=1, steps=1000),
+    "se_pile": dict(dmax=0.004, dt=5e-4, tolerance=1e-6, max_ite=40000, vap=1, steps=300, mu=0.3),
 }

@@ -2,8 +2,9 @@
 
 Mirrors ``scopi_container<dim>`` / ``property<dim>`` (include/scopi/container.hpp:339-384,
 include/scopi/property.hpp:16-200) and the shape constructors the hot path uses:
-``sphere`` (objects/types/sphere.hpp), ``plane`` (objects/types/plane.hpp:50-70) and
-``segment`` (objects/types/segment.hpp:133-138).
+``sphere`` (objects/types/sphere.hpp), ``plane`` (objects/types/plane.hpp:50-70),
+``segment`` (objects/types/segment.hpp:133-138) and ``superellipsoid``
+(objects/types/superellipsoid.hpp:59-70: centre, rotation, semi-axes, squareness (e, n)).
 
 Layout (shared with the C-ABI ``scopi_gpu_particles`` in include/scopi_gpu.h):
 every vector quantity has 3 slots per body.  In 2D the z slot of pos, v, vd and f
@@ -19,7 +20,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-SPHERE, PLANE, SEGMENT = 0, 1, 2
+SPHERE, PLANE, SEGMENT, SUPERELLIPSOID = 0, 1, 2, 3
 
 
 def quaternion(angle: float, axes=(0.0, 0.0, 1.0)) -> np.ndarray:
@@ -89,10 +90,12 @@ class Particles:
     j: list = field(default_factory=list)
     radius: list = field(default_factory=list)
     length: list = field(default_factory=list)
+    axes: list = field(default_factory=list)
+    squareness: list = field(default_factory=list)
     nb_inactive: int = 0
 
     # --- builders --------------------------------------------------------
-    def _push(self, shape, pos, q, prop: Property, radius=0.0, length=0.0):
+    def _push(self, shape, pos, q, prop: Property, radius=0.0, length=0.0, axes=(0.0, 0.0, 0.0), squareness=(1.0, 1.0)):
         n = len(self.shape)
         if not prop.active:
             if self.nb_inactive != n:
@@ -110,6 +113,8 @@ class Particles:
         self.j.append(_rot3(prop.moment_inertia, self.dim))
         self.radius.append(float(radius))
         self.length.append(float(length))
+        self.axes.append(np.asarray(axes, dtype=np.float64))
+        self.squareness.append(np.asarray(squareness, dtype=np.float64))
         return self
 
     def add_sphere(self, pos, radius, prop: Property | None = None, q=None):
@@ -129,6 +134,19 @@ class Particles:
         d = p2 - p1
         length = math.sqrt(float(np.dot(d, d)))
         return self._push(SEGMENT, 0.5 * (p1 + p2), quaternion(ang), prop or Property().deactivate(), length=length)
+
+    def add_superellipsoid(self, pos, radius, squareness, prop: Property | None = None, q=None):
+        """``superellipsoid<3>(pos, q, radius, squareness)`` (3D): semi-axes (rx, ry, rz) and
+        squareness (e, n).  ``radius`` of the body record holds the bounding radius
+        sqrt(rx^2 + ry^2 + rz^2) (the body lies in its axis box for e, n <= 2), which the
+        contact search uses; the closest points use the exact surface."""
+        if self.dim != 3:
+            raise ValueError("superellipsoids are 3D here")
+        r = np.asarray(radius, dtype=np.float64).reshape(3)
+        sq = np.asarray(squareness, dtype=np.float64).reshape(2)
+        q = quaternion(0.0) if q is None else q
+        return self._push(SUPERELLIPSOID, pos, q, prop or Property(), radius=float(np.sqrt(np.dot(r, r))), axes=r,
+                          squareness=sq)
 
     # --- array views -----------------------------------------------------
     def finalize(self) -> "ParticleArrays":
@@ -153,6 +171,17 @@ class ParticleArrays:
     j: np.ndarray
     radius: np.ndarray
     length: np.ndarray
+    axes: np.ndarray = None        # n x 3 superellipsoid semi-axes (0 for other shapes)
+    squareness: np.ndarray = None  # n x 2 superellipsoid squareness (e, n)
+
+    def __post_init__(self):
+        n = int(self.shape.shape[0])
+        if self.axes is None:
+            self.axes = np.zeros((n, 3))
+        if self.squareness is None:
+            self.squareness = np.ones((n, 2))
+        self.axes = np.ascontiguousarray(self.axes, dtype=np.float64).reshape(n, 3)
+        self.squareness = np.ascontiguousarray(self.squareness, dtype=np.float64).reshape(n, 2)
 
     @property
     def n(self) -> int:
@@ -173,6 +202,8 @@ class ParticleArrays:
             j=a2(p.j, 3),
             radius=np.ascontiguousarray(np.asarray(p.radius, dtype=np.float64)),
             length=np.ascontiguousarray(np.asarray(p.length, dtype=np.float64)),
+            axes=a2(p.axes, 3) if p.axes else None,
+            squareness=a2(p.squareness, 2) if p.squareness else None,
         )
 
     def copy(self) -> "ParticleArrays":

@@ -1,0 +1,197 @@
+"""Pins of the oracle's superellipsoid closest points (closest_points.hpp:263-733, 1479-1768).
+
+The reference's own superellipsoid tests are disabled (test/CMakeLists.txt:11, cases
+commented out in test/test_closest_points.cpp:1502-1770), so the oracle is pinned here by
+(1) its analytic Jacobian against finite differences, (2) its restatement of MINPACK's
+hybrid method against scipy's `root(method="hybr")`, which wraps the original MINPACK, on
+the same system from the same start, (3) known answers: spheres (e = n = 1, equal
+semi-axes), ellipsoids along a line, a superellipsoid above a plane."""
+import math
+
+import numpy as np
+import pytest
+import scipy.optimize
+
+import py_oracle as orc
+from scopi_b200 import configs, quaternion
+
+
+def rot(q):
+    w, x, y, z = q
+    return np.array([[1 - 2 * y * y - 2 * z * z, 2 * x * y - 2 * w * z, 2 * x * z + 2 * w * y],
+                     [2 * x * y + 2 * w * z, 1 - 2 * x * x - 2 * z * z, 2 * y * z - 2 * w * x],
+                     [2 * x * z - 2 * w * y, 2 * y * z + 2 * w * x, 1 - 2 * x * x - 2 * y * y]])
+
+
+def random_q(rng):
+    u = rng.uniform(size=3)
+    return np.array([math.sqrt(1 - u[0]) * math.sin(2 * math.pi * u[1]),
+                     math.sqrt(1 - u[0]) * math.cos(2 * math.pi * u[1]),
+                     math.sqrt(u[0]) * math.sin(2 * math.pi * u[2]),
+                     math.sqrt(u[0]) * math.cos(2 * math.pi * u[2])])[[3, 0, 1, 2]]
+
+
+def random_pair(rng, gap=0.002):
+    r1 = rng.uniform(0.004, 0.008, 3)
+    r2 = rng.uniform(0.004, 0.008, 3)
+    sq1 = rng.uniform(0.6, 1.4, 2)
+    sq2 = rng.uniform(0.6, 1.4, 2)
+    d = rng.normal(size=3)
+    d /= np.linalg.norm(d)
+    c2 = d * (np.linalg.norm(r1) + np.linalg.norm(r2)) * rng.uniform(0.55, 0.8)
+    return (orc.se_record([0, 0, 0], random_q(rng), r1, sq1), orc.se_record(c2, random_q(rng), r2, sq2))
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_jacobian_matches_finite_differences(seed):
+    rng = np.random.default_rng(seed)
+    s1, s2 = random_pair(rng)
+    u = rng.uniform(-1.2, 1.2, 4)
+    F, J = orc.se_se_system(s1, s2, u)
+    h = 1e-7
+    Jfd = np.zeros((4, 4))
+    for k in range(4):
+        e = np.zeros(4)
+        e[k] = h
+        Jfd[:, k] = (orc.se_se_system(s1, s2, u + e)[0] - orc.se_se_system(s1, s2, u - e)[0]) / (2 * h)
+    scale = np.abs(J).max()
+    assert np.abs(J - Jfd).max() <= 1e-6 * scale, (J, Jfd)
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_closest_points_solve_the_system(seed):
+    """The result solves F to MINPACK's resolution.  The reference's system is poorly scaled
+    (F0..2 = d x n1 ~ |d| r^2 while F3 = n1.n2 + |n1||n2| ~ r^4), so MINPACK often stops on
+    slow progress (info 4) with |F| ~ 1e-12 and the alignment of the normals resolved to
+    ~1e-3; the distance and contact points are still accurate to ~1e-7 of the body size."""
+    rng = np.random.default_rng(100 + seed)
+    s1, s2 = random_pair(rng)
+    out = orc.se_se(s1, s2)
+    assert out["info"] in (1, 4, 5)
+    F, J = orc.se_se_system(s1, s2, out["u"])
+    assert np.linalg.norm(F[:3]) <= 1e-4 * np.abs(J[:3]).max()
+    assert abs(F[3]) <= 1e-2 * np.abs(J[3]).max()
+    # the distance is the gap along the common normal: |pi - pj| = |dij|
+    assert abs(np.linalg.norm(out["pi"] - out["pj"]) - abs(out["dij"])) <= 1e-15
+
+
+def test_minpack_restatement_iterates_like_minpack():
+    """From the same start the restated hybrid method and MINPACK (scipy's hybr, the
+    original Fortran) take the same path: same status, same final iterate, and the same
+    function evaluations (scipy's count has 2 more: its own shape-check calls)."""
+    rng = np.random.default_rng(7)
+    for _ in range(5):
+        s1, s2 = random_pair(rng)
+        ours = orc.se_se(s1, s2)
+        u0 = ours["u"] + rng.uniform(-0.05, 0.05, 4)
+
+        def fun(u):
+            return orc.se_se_system(s1, s2, u)[0]
+
+        def jac(u):
+            return orc.se_se_system(s1, s2, u)[1]
+
+        ref = scipy.optimize.root(fun, u0, jac=jac, method="hybr",
+                                  options={"xtol": 1e-10, "maxfev": 1000, "factor": 100, "diag": np.ones(4)})
+        mine = orc.hybrid_solve(s1, s2, u0)
+        assert mine["info"] == ref.status
+        assert 0 <= ref.nfev - mine["nfev"] <= 2, (mine, ref.nfev)
+        assert np.allclose(mine["u"], ref.x, rtol=0, atol=1e-12)
+
+
+def test_spheres_as_superellipsoids():
+    """e = n = 1, equal semi-axes: the sphere formulas wherever the hybrid method reports
+    convergence (info 1).  The angle parametrisation is singular at its poles (a = +-pi/2),
+    and with the system's scaling MINPACK stops on slow progress (info 4) for about 40 % of
+    random orientations of spheres, some of them far from the root -- the reference's method
+    as written; the oracle keeps it."""
+    converged = 0
+    for seed in range(40):
+        rng = np.random.default_rng(200 + seed)
+        r = 0.005
+        c2 = rng.normal(size=3)
+        c2 *= 0.0115 / np.linalg.norm(c2)
+        s1 = orc.se_record([0, 0, 0], random_q(rng), [r, r, r], [1, 1])
+        s2 = orc.se_record(c2, random_q(rng), [r, r, r], [1, 1])
+        out = orc.se_se(s1, s2)
+        if out["info"] != 1:
+            continue
+        converged += 1
+        gap = np.linalg.norm(c2) - 2 * r
+        u = c2 / np.linalg.norm(c2)
+        assert abs(out["dij"] - gap) <= 1e-12
+        assert np.allclose(out["pi"], r * u, atol=1e-12)
+        assert np.allclose(out["pj"], c2 - r * u, atol=1e-12)
+        assert np.allclose(out["nij"], -u, atol=1e-9)
+    assert converged >= 15
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_ellipsoids_on_a_line(seed):
+    """Axis-aligned ellipsoids on the x axis: gap L - a1 - a2, whatever common rotation."""
+    rng = np.random.default_rng(300 + seed)
+    a1, a2 = 0.007, 0.005
+    r1 = [a1, 0.004, 0.006]
+    r2 = [a2, 0.006, 0.0045]
+    L = a1 + a2 + 0.0017
+    q = random_q(rng)
+    R = rot(q)
+    s1 = orc.se_record([0, 0, 0], q, r1, [1, 1])
+    s2 = orc.se_record(R @ np.array([L, 0, 0]), q, r2, [1, 1])
+    out = orc.se_se(s1, s2)
+    assert abs(out["dij"] - (L - a1 - a2)) <= 1e-11
+    assert np.allclose(out["pi"], R @ np.array([a1, 0, 0]), atol=1e-11)
+    assert np.allclose(out["pj"], R @ np.array([L - a2, 0, 0]), atol=1e-11)
+
+
+@pytest.mark.parametrize("e,n", [(1.0, 1.0), (0.6, 0.6), (1.4, 0.8)])
+def test_superellipsoid_above_a_plane(e, n):
+    """Unrotated body above the floor z = 0 (normal +z): lowest point (0, 0, c - rz)."""
+    r = [0.006, 0.005, 0.004]
+    c = [0.1, 0.2, 0.0052]
+    s = orc.se_record(c, quaternion(0.0), r, [e, n])
+    qp = quaternion(-math.pi / 2, (0, 1, 0))  # column 0 of R = +z
+    out = orc.se_plane(s, [0, 0, 0], qp)
+    assert abs(out["dij"] - (c[2] - r[2])) <= 1e-15
+    assert np.allclose(out["pi"], [c[0], c[1], c[2] - r[2]], atol=1e-15)
+    assert np.allclose(out["pj"], [c[0], c[1], 0.0], atol=1e-15)
+    assert np.allclose(out["nij"], [0, 0, 1], atol=1e-12)
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_rotated_superellipsoid_above_a_plane_matches_sampling(seed):
+    rng = np.random.default_rng(400 + seed)
+    r = rng.uniform(0.004, 0.008, 3)
+    sq = rng.uniform(0.6, 1.4, 2)
+    q = random_q(rng)
+    c = [0.0, 0.0, 0.02]
+    s = orc.se_record(c, q, r, sq)
+    qp = quaternion(-math.pi / 2, (0, 1, 0))
+    out = orc.se_plane(s, [0, 0, 0], qp)
+    # lowest surface point by dense sampling of the parametrisation
+    a = np.linspace(-math.pi / 2, math.pi / 2, 801)
+    b = np.linspace(-math.pi, math.pi, 1601)
+    A, B = np.meshgrid(a, b, indexing="ij")
+
+    def spow(x, k):
+        return np.sign(x) * np.abs(x) ** k
+
+    P = np.stack([r[0] * spow(np.cos(A), sq[1]) * spow(np.cos(B), sq[0]),
+                  r[1] * spow(np.cos(A), sq[1]) * spow(np.sin(B), sq[0]),
+                  r[2] * spow(np.sin(A), sq[1])], -1)
+    z = (P @ rot(q).T)[..., 2] + c[2]
+    assert out["dij"] <= z.min() + 1e-12
+    assert out["dij"] >= z.min() - 2e-6
+    # it solves the reference's system (with the body's side as the sign)
+    scale = np.prod(r) ** (2 / 3)
+    assert np.abs(out["residual"]).max() <= 1e-12 * scale
+
+
+def test_superellipsoid_scene_runs_in_the_oracle():
+    pa = configs.se_pile(count=27, side=3, seed=3)
+    o = orc.OracleSolver(pa, problem=orc.FRICTION, vap=orc.VAP_FPD, dmax=0.004, mu=0.3, tolerance=1e-6,
+                         max_ite=40000)
+    o.run(5e-4, 3)
+    c = o.contacts()
+    assert len(c["i"]) > 0
+    assert np.all(np.isfinite(o.pa.pos))
