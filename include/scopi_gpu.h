@@ -56,6 +56,7 @@ extern "C" {
 #define SCOPI_GPU_SPHERE 0
 #define SCOPI_GPU_PLANE 1
 #define SCOPI_GPU_SEGMENT 2
+#define SCOPI_GPU_SUPERELLIPSOID 3  /* 3D, superellipsoid<3> (superellipsoid.hpp:59-70) */
 
 typedef struct scopi_gpu_params {
     int32_t dim;              /* 2 or 3 */
@@ -92,7 +93,7 @@ typedef struct scopi_gpu_params {
 typedef struct scopi_gpu_particles {
     int64_t n;           /* bodies */
     int64_t nb_inactive; /* obstacles first */
-    int32_t* shape;      /* n: SCOPI_GPU_SPHERE / PLANE / SEGMENT */
+    int32_t* shape;      /* n: SCOPI_GPU_SPHERE / PLANE / SEGMENT / SUPERELLIPSOID */
     double* pos;         /* n*3 */
     double* q;           /* n*4 */
     double* v;           /* n*3 */
@@ -102,8 +103,10 @@ typedef struct scopi_gpu_particles {
     double* f;           /* n*3 */
     double* m;           /* n */
     double* j;           /* n*3 */
-    double* radius;      /* n (sphere radius) */
+    double* radius;      /* n (sphere radius; superellipsoid: bounding radius |(rx, ry, rz)|) */
     double* length;      /* n (segment length) */
+    double* axes;        /* n*3 superellipsoid semi-axes (rx, ry, rz); NULL when there are none */
+    double* squareness;  /* n*2 superellipsoid squareness (e, n); NULL when there are none */
 } scopi_gpu_particles;
 
 typedef struct scopi_gpu_stats {

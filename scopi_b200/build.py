@@ -21,6 +21,7 @@ SOURCES = {
     "apgd.cu": [],
     "apgd_sph.cu": [],
     "apgd_batch.cu": [],
+    "se.cu": ["-fmad=false"],
     "scan.cu": [],
     "scopi_gpu.cu": [],
 }

@@ -175,6 +175,12 @@ def se_pile(count: int = 50_000, side: int = 37, seed: int = 3) -> ParticleArray
     return p.finalize()
 
 
+def se_kd_radius(pa: ParticleArrays, dmax: float) -> float:
+    """Squared kd-tree candidate radius (2 r_max + dmax)^2 with r_max the largest bounding
+    radius of the active bodies (the search radius of the reference's contact_kdtree)."""
+    return float((2 * pa.radius[pa.nb_inactive:].max() + dmax) ** 2)
+
+
 def pile_scene(seed: int, nmin: int = 200, nmax: int = 5000, vmax: float = 0.0) -> ParticleArrays:
     """One pile scene.  Draws: u[0] -> N_s; candidate k uses (x, y, r) = u[1+3k], u[2+3k], u[3+3k].
 

@@ -24,6 +24,8 @@ struct Bodies {
     const double* j;    // n*3
     const double* radius;
     const double* length;
+    const double* axes = nullptr;      // n*3 superellipsoid semi-axes
+    const double* sq = nullptr;        // n*2 superellipsoid squareness (e, n)
     // Batches of independent scenes (null for one scene): scene of each body, an x shift
     // per scene applied to the cell keys only (scenes occupy disjoint cell ranges), and
     // per obstacle the active range it can touch (obs_a0: first active index, obs_off:

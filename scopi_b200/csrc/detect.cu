@@ -9,6 +9,7 @@
 #include <math.h>
 
 #include "kernels.cuh"
+#include "se_geom.cuh"
 
 namespace scopi_gpu {
 
@@ -18,7 +19,7 @@ long long detect_launches() { return g_detect_launches; }
 
 namespace {
 
-constexpr int kSphere = 0, kPlane = 1, kSegment = 2;
+constexpr int kSphere = 0, kPlane = 1, kSegment = 2, kSuperellipsoid = 3;
 constexpr int kBBoxBlocks = 4 * kSMs;
 
 struct PairGeom {
@@ -190,8 +191,15 @@ __device__ __forceinline__ bool exact_pair(const Bodies& B, int dim, int a, int 
         flip(g);
     } else if (sa == kSphere && sb == kSegment && dim == 2) {
         sphere_segment(xa, B.radius[a], xb, B.q + 4 * (long long)b, B.length[b], g);
+    } else if (sa == kPlane && sb == kSuperellipsoid && dim == 3) {  // closest_points.hpp:1761-1768
+        const se::Body s = se::load(B, b);
+        se::body_plane(s, xa, B.q + 4 * (long long)a, g.pi, g.pj, g.nij, g.dij);
+        flip(g);
+    } else if (sa == kSuperellipsoid && sb == kPlane && dim == 3) {
+        const se::Body s = se::load(B, a);
+        se::body_plane(s, xb, B.q + 4 * (long long)b, g.pi, g.pj, g.nij, g.dij);
     } else {
-        return false;
+        return false;  // superellipsoid pairs: se.cu
     }
     return true;
 }
@@ -376,8 +384,13 @@ __device__ __forceinline__ bool pair_in_contact(const StepParams& p, const doubl
         s2 += dd * dd;
     }
     if (p.kd_filter && !(s2 < p.kd_radius)) return false;
+    // superellipsoids: the candidates of the reference's kd-tree radius search (the exact
+    // solve of se.cu decides; contact_kdtree.hpp:240-262), or without that search the pairs
+    // whose bounding spheres (w = bounding radius) come within dmax
+    if (p.se_mode && p.kd_filter) return true;
     const double lim = L.w + H.w + p.dmax;
     if (!(lim > 0.0) || s2 > lim * lim * (1.0 + 1e-9)) return false;
+    if (p.se_mode) return true;
     PairGeom pg;
     sphere_sphere(DIM, xl, L.w, xh, H.w, pg);
     return pg.dij < p.dmax;

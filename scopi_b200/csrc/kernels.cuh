@@ -19,6 +19,7 @@ struct StepParams {
     int problem;
     int vap;
     int kd_filter;        // contact_kdtree: candidate needs |xi-xj|^2 < kd_tree_radius
+    int se_mode;          // superellipsoids: the search keeps the bounding-sphere candidates (se.cu decides)
     double dmax;
     double kd_radius;
     double dt;
@@ -94,6 +95,14 @@ void launch_amat(const Bodies& b, const StepParams& p, const Contacts& c, const 
                  const double* u, double* out, cudaStream_t s);
 void launch_atmat(const Bodies& b, const StepParams& p, const Contacts& c, const Sizes* sizes, long long c_cap,
                   const double* f, double* out, cudaStream_t s);
+
+// ----------------------------------------------------------------- se.cu
+long long se_launches();
+// closest points of the superellipsoid rows [C_obs, C) of c (one block per row)
+void launch_se_pairs(const Bodies& b, Contacts& c, const Sizes* sizes, int grid, cudaStream_t s);
+// rows of src with dij < dmax (obstacle rows all kept) into dst, (i, j) order kept; sizes->C updated
+void launch_se_filter(const Contacts& src, Contacts& dst, Sizes* sizes, double dmax, long long c_cap, int* keep,
+                      int* pos, int* scan_work, int* total, cudaStream_t s);
 
 // --------------------------------------------------------------- apgd.cu
 struct ApgdSettings {

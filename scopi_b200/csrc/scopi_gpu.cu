@@ -56,6 +56,9 @@ struct scopi_gpu_handle {
     int* d_shape = nullptr;
     double *d_pos = nullptr, *d_q = nullptr, *d_v = nullptr, *d_omega = nullptr, *d_vd = nullptr, *d_omega_d = nullptr,
            *d_f = nullptr, *d_m = nullptr, *d_j = nullptr, *d_radius = nullptr, *d_length = nullptr;
+    double *d_axes = nullptr, *d_sq = nullptr;  // superellipsoids
+    int *d_se_keep = nullptr, *d_se_pos = nullptr;  // contact filter of superellipsoid candidates
+    bool has_se = false;                        // some active body is a superellipsoid
     double* d_invm64 = nullptr;
     float* d_invm32 = nullptr;
     // per-particle solve buffers
@@ -122,7 +125,9 @@ struct scopi_gpu_handle {
     // Normal-only problems: every pair type of the hot path (sphere-sphere, sphere-plane,
     // sphere-segment) has its lever arm along the normal, so the rotational Jacobian terms
     // vanish and the translational kernels apply.
-    bool sphere_mode() const { return P.problem != SCOPI_GPU_FRICTION; }
+    // torque-free rows: every contact's lever arms are parallel to its normal (spheres,
+    // planes, segments); superellipsoid contacts need the 6-dof rows
+    bool sphere_mode() const { return P.problem != SCOPI_GPU_FRICTION && !has_se; }
 
     Bodies bodies() const {
         Bodies b;
@@ -140,6 +145,10 @@ struct scopi_gpu_handle {
         b.j = d_j;
         b.radius = d_radius;
         b.length = d_length;
+        if (has_se) {
+            b.axes = d_axes;
+            b.sq = d_sq;
+        }
         if (batch) {
             b.scene = d_scene;
             b.scene_shift = d_shift;
@@ -391,6 +400,7 @@ struct scopi_gpu_handle {
         s.problem = P.problem;
         s.vap = P.vap;
         s.kd_filter = P.contact_method == SCOPI_GPU_KDTREE ? 1 : 0;
+        s.se_mode = has_se ? 1 : 0;
         s.dmax = P.dmax;
         s.kd_radius = P.kd_tree_radius;
         s.dt = dt;
@@ -451,7 +461,7 @@ struct scopi_gpu_handle {
     if ((e = alloc(body_mem, p, (c))) != cudaSuccess) return cuda_fail(e, "cudaMalloc(bodies)");
         A(d_shape, n) A(d_pos, 3 * (size_t)n) A(d_q, 4 * (size_t)n) A(d_v, 3 * (size_t)n) A(d_omega, 3 * (size_t)n)
         A(d_vd, 3 * (size_t)n) A(d_omega_d, 3 * (size_t)n) A(d_f, 3 * (size_t)n) A(d_m, n) A(d_j, 3 * (size_t)n)
-        A(d_radius, n) A(d_length, n) A(d_invm64, 4 * (size_t)na + 4) A(d_invm32, 4 * (size_t)na + 4)
+        A(d_radius, n) A(d_length, n) A(d_axes, 3 * (size_t)n) A(d_sq, 2 * (size_t)n) A(d_invm64, 4 * (size_t)na + 4) A(d_invm32, 4 * (size_t)na + 4)
         A(d_ufin, 6 * (size_t)na + 6)
         A(d_usfin, (size_t)na + 1)
         for (int k = 0; k < 4; ++k) {
@@ -501,7 +511,7 @@ struct scopi_gpu_handle {
             for (int k = 0; k < 3; ++k) A(d_lam32[k], M)
             A(d_g32, M)
         }
-        A(d_cij, cap) A(d_nc64, cap) A(d_incv64, 2 * cap)
+        A(d_cij, cap) A(d_nc64, cap) A(d_incv64, 2 * cap) A(d_se_keep, cap + 1) A(d_se_pos, cap + 1)
         if (mixed()) {
             A(d_nc32, cap) A(d_incv32, 2 * cap)
         }
@@ -518,7 +528,8 @@ struct scopi_gpu_handle {
     }
 
     long long launches() const {
-        return detect_launches() + apgd_launches() + apgd_sph_launches() + apgd_batch_launches() + replayed;
+        return detect_launches() + apgd_launches() + apgd_sph_launches() + apgd_batch_launches() + se_launches() +
+               replayed;
     }
 
     // contact detection + closest points + assembly + incidence lists into `cur`
@@ -546,13 +557,18 @@ struct scopi_gpu_handle {
             if (rc) return rc;
             if (attempt == 3) return fail(SCOPI_GPU_ENOMEM, "contact capacity could not be grown");
         }
-        if (!assemble) {
-            launch_geometry(b, sp, cur, d_sizes_cur, c_cap, has_old ? &old : nullptr, has_old ? &d_sizes_old->C : nullptr,
-                            c_cap, stream);
-            return 0;
-        }
         launch_geometry(b, sp, cur, d_sizes_cur, c_cap, has_old ? &old : nullptr, has_old ? &d_sizes_old->C : nullptr,
                         c_cap, stream);
+        if (has_se) {
+            // the search kept bounding-sphere candidates: closest points of the superellipsoid
+            // pairs, then the rows with dij < dmax into the other list (no viscous gamma to
+            // carry here), which becomes the current one
+            launch_se_pairs(b, cur, d_sizes_cur, 3 * kSMs, stream);
+            launch_se_filter(cur, old, d_sizes_cur, P.dmax, c_cap, d_se_keep, d_se_pos, dw.scan_work,
+                             dw.tmp_total + 2, stream);
+            std::swap(cur, old);
+        }
+        if (!assemble) return 0;
         launch_assemble(b, sp, cur, as, d_sizes_cur, c_cap, dw.scan_work, dw.tmp_total + 2, stream);
         launch_incidence(b, sp, cur, as, inc, d_sizes_cur, c_cap, dw.scan_work, dw.tmp_total + 2, stream,
                          !sphere_mode());
@@ -990,13 +1006,32 @@ static int32_t upload_particles(scopi_gpu_handle* h, const scopi_gpu_particles* 
     const int n = (int)p->n, nin = (int)p->nb_inactive;
     if ((long long)nin * (n - nin) >= (1LL << 31) && obs_cap < 0)
         return h->fail(SCOPI_GPU_EUNSUPPORTED, "obstacles x active bodies must stay below 2^31");
+    int n_se = 0, n_sph = 0;
     for (int i = 0; i < n; ++i) {
         const int s = p->shape[i];
-        if (i >= nin && s != SCOPI_GPU_SPHERE)
-            return h->fail(SCOPI_GPU_EUNSUPPORTED, "active bodies must be spheres");
-        if (s < 0 || s > 2) return h->fail(SCOPI_GPU_EINVAL, "unknown shape");
+        if (s < 0 || s > 3) return h->fail(SCOPI_GPU_EINVAL, "unknown shape");
+        if (i >= nin && s != SCOPI_GPU_SPHERE && s != SCOPI_GPU_SUPERELLIPSOID)
+            return h->fail(SCOPI_GPU_EUNSUPPORTED, "active bodies must be spheres or superellipsoids");
+        if (i < nin && s == SCOPI_GPU_SUPERELLIPSOID)
+            return h->fail(SCOPI_GPU_EUNSUPPORTED, "superellipsoid obstacles are not supported");
         if (s == SCOPI_GPU_SEGMENT && h->P.dim != 2) return h->fail(SCOPI_GPU_EUNSUPPORTED, "segments are 2D only");
+        if (i >= nin) (s == SCOPI_GPU_SUPERELLIPSOID ? n_se : n_sph)++;
     }
+    if (n_se > 0) {
+        if (h->P.dim != 3) return h->fail(SCOPI_GPU_EUNSUPPORTED, "superellipsoids are 3D only");
+        if (n_sph > 0) return h->fail(SCOPI_GPU_EUNSUPPORTED, "spheres and superellipsoids cannot be mixed");
+        if (!p->axes || !p->squareness) return h->fail(SCOPI_GPU_EINVAL, "superellipsoid axes / squareness missing");
+        if (h->P.problem == SCOPI_GPU_VISCOUS)
+            return h->fail(SCOPI_GPU_EUNSUPPORTED, "superellipsoids: NoFriction and Friction problems");
+        if (h->batch) return h->fail(SCOPI_GPU_EUNSUPPORTED, "batches hold sphere scenes");
+        for (int i = nin; i < n; ++i) {
+            const double* r = p->axes + 3 * (size_t)i;
+            const double* q = p->squareness + 2 * (size_t)i;
+            if (!(r[0] > 0 && r[1] > 0 && r[2] > 0) || !(q[0] > 0 && q[0] < 2 && q[1] > 0 && q[1] < 2))
+                return h->fail(SCOPI_GPU_EINVAL, "superellipsoid: semi-axes > 0 and squareness in (0, 2)");
+        }
+    }
+    h->has_se = n_se > 0;
     cudaSetDevice(h->dev);
     cudaStreamSynchronize(h->stream);
     if (n != h->n || nin != h->nin || h->batch) {
@@ -1023,6 +1058,8 @@ static int32_t upload_particles(scopi_gpu_handle* h, const scopi_gpu_particles* 
     up(h->d_j, p->j, 3 * (size_t)n * sizeof(double));
     up(h->d_radius, p->radius, (size_t)n * sizeof(double));
     up(h->d_length, p->length, (size_t)n * sizeof(double));
+    if (p->axes) up(h->d_axes, p->axes, 3 * (size_t)n * sizeof(double));
+    if (p->squareness) up(h->d_sq, p->squareness, 2 * (size_t)n * sizeof(double));
     // M^-1 (minimization_problem.hpp:11-31): 1/m on the translational slots, 1/J on the
     // rotational ones (2D: z only)
     std::vector<double> im64(4 * (size_t)(n - nin) + 4, 0.0);

@@ -1,0 +1,621 @@
+// se.cu -- closest points of pairs of 3D superellipsoids, one block per pair.
+//
+// closest_points(superellipsoid<3>, superellipsoid<3>), closest_points.hpp:263-733:
+//   start: the angle grids of both bodies (sorted unique binit_xy(6), ainit_yz(6) of
+//          superellipsoid.hpp:360-466, ~21 x 21 points each), argmin over all point pairs
+//          of |p1 - p2| + 2 (1 + n1.n2), first minimum in row-major order;
+//   solve: hybrd1 (minpack.hpp:852-923: Powell's hybrid method, xtol 1e-10, maxfev 1000,
+//          unit scaling, factor 100) on F = [ (p2 - p1) x n1 ; n1.n2 + |n1||n2| ] with its
+//          analytic Jacobian (n1, n2 unnormalised normals);
+//   result: pi = p1(u), pj = p2(u), nij = unit normal of body 2 at pj,
+//          dij = sign((pi - pj).nij) |pi - pj|.
+// The block computes the surface samples of both bodies into shared memory, every thread
+// scans a slice of the sample pairs, a block reduction finds the first minimum, and thread
+// 0 runs the hybrid method (4 unknowns, a few dozen function evaluations, bounded by
+// maxfev).  Built with -fmad=false like detect.cu.
+#include <math.h>
+
+#include <algorithm>
+
+#include "kernels.cuh"
+#include "se_geom.cuh"
+
+namespace scopi_gpu {
+
+static long long g_se_launches = 0;
+long long se_launches() { return g_se_launches; }
+
+namespace {
+using namespace se;
+
+constexpr int kSeThreads = 256;
+constexpr int kSeGrid = 24;       // unique angles per grid axis at most (4 * 6)
+constexpr int kSeSamples = kSeGrid * kSeGrid;
+
+// --------------------------------------------------------------- F and Jacobian
+__device__ void sese_F(const Body& s1, const Body& s2, const double* u, double* F) {
+    Local L1, L2;
+    local(s1, u[0], u[1], L1);
+    local(s2, u[2], u[3], L2);
+    double p1[3], p2[3], n1[3], n2[3];
+    mv(s1.R, L1.p, p1);
+    mv(s2.R, L2.p, p2);
+    mv(s1.R, L1.N, n1);
+    mv(s2.R, L2.N, n2);
+    const double d[3] = {p2[0] + s2.c[0] - p1[0] - s1.c[0], p2[1] + s2.c[1] - p1[1] - s1.c[1],
+                         p2[2] + s2.c[2] - p1[2] - s1.c[2]};
+    cross(d, n1, F);
+    F[3] = dot3(n1, n2) + norm3(n1) * norm3(n2);
+}
+
+__device__ void sese_J(const Body& s1, const Body& s2, const double* u, double* J) {  // column-major
+    Local L1, L2;
+    local(s1, u[0], u[1], L1);
+    local(s2, u[2], u[3], L2);
+    double p1[3], p2[3], n1[3], n2[3];
+    mv(s1.R, L1.p, p1);
+    mv(s2.R, L2.p, p2);
+    mv(s1.R, L1.N, n1);
+    mv(s2.R, L2.N, n2);
+    const double d[3] = {p2[0] + s2.c[0] - p1[0] - s1.c[0], p2[1] + s2.c[1] - p1[1] - s1.c[1],
+                         p2[2] + s2.c[2] - p1[2] - s1.c[2]};
+    const double l1 = norm3(n1), l2 = norm3(n2);
+    for (int k = 0; k < 4; ++k) {
+        double dd[3], dn1[3] = {0, 0, 0}, dn2[3] = {0, 0, 0};
+        if (k < 2) {
+            double t[3];
+            mv(s1.R, k == 0 ? L1.pa : L1.pb, t);
+            for (int c = 0; c < 3; ++c) dd[c] = -t[c];
+            mv(s1.R, k == 0 ? L1.Na : L1.Nb, dn1);
+        } else {
+            mv(s2.R, k == 2 ? L2.pa : L2.pb, dd);
+            mv(s2.R, k == 2 ? L2.Na : L2.Nb, dn2);
+        }
+        double a[3], b[3];
+        cross(dd, n1, a);
+        cross(d, dn1, b);
+        J[0 + 4 * k] = a[0] + b[0];
+        J[1 + 4 * k] = a[1] + b[1];
+        J[2 + 4 * k] = a[2] + b[2];
+        J[3 + 4 * k] = dot3(dn1, n2) + dot3(n1, dn2) + dot3(n1, dn1) / l1 * l2 + l1 * dot3(n2, dn2) / l2;
+    }
+}
+
+// ------------------------------------------------------- MINPACK pieces (n = 4)
+constexpr int N = 4;
+constexpr double kEps = 2.220446049250313e-16;
+constexpr double kGiant = 1.7976931348623157e308;
+
+__device__ double enorm(int n, const double* x) {
+    const double rdwarf = 3.834e-20, rgiant = 1.304e19;
+    double s1 = 0, s2 = 0, s3 = 0, x1max = 0, x3max = 0;
+    const double agiant = rgiant / n;
+    for (int i = 0; i < n; ++i) {
+        const double xabs = fabs(x[i]);
+        if (xabs > rdwarf && xabs < agiant) {
+            s2 += xabs * xabs;
+        } else if (xabs <= rdwarf) {
+            if (xabs > x3max) {
+                s3 = 1 + s3 * (x3max / xabs) * (x3max / xabs);
+                x3max = xabs;
+            } else if (xabs != 0) {
+                s3 += (xabs / x3max) * (xabs / x3max);
+            }
+        } else {
+            if (xabs > x1max) {
+                s1 = 1 + s1 * (x1max / xabs) * (x1max / xabs);
+                x1max = xabs;
+            } else {
+                s1 += (xabs / x1max) * (xabs / x1max);
+            }
+        }
+    }
+    if (s1 != 0) return x1max * sqrt(s1 + (s2 / x1max) / x1max);
+    if (s2 != 0) {
+        if (s2 >= x3max) return sqrt(s2 * (1 + (x3max / s2) * (x3max * s3)));
+        return sqrt(x3max * ((s2 / x3max) + (x3max * s3)));
+    }
+    return x3max * sqrt(s3);
+}
+
+__device__ void qrfac(double* a, double* rdiag, double* acnorm) {
+    for (int j = 0; j < N; ++j) {
+        acnorm[j] = enorm(N, a + j * N);
+        rdiag[j] = acnorm[j];
+    }
+    for (int j = 0; j < N; ++j) {
+        double ajnorm = enorm(N - j, a + j + j * N);
+        if (ajnorm != 0) {
+            if (a[j + j * N] < 0) ajnorm = -ajnorm;
+            for (int i = j; i < N; ++i) a[i + j * N] /= ajnorm;
+            a[j + j * N] += 1;
+            for (int k = j + 1; k < N; ++k) {
+                double sum = 0;
+                for (int i = j; i < N; ++i) sum += a[i + j * N] * a[i + k * N];
+                const double temp = sum / a[j + j * N];
+                for (int i = j; i < N; ++i) a[i + k * N] -= temp * a[i + j * N];
+            }
+        }
+        rdiag[j] = -ajnorm;
+    }
+}
+
+__device__ void qform(double* q, double* wa) {
+    for (int j = 1; j < N; ++j)
+        for (int i = 0; i < j; ++i) q[i + j * N] = 0;
+    for (int l = 0; l < N; ++l) {
+        const int k = N - 1 - l;
+        for (int i = k; i < N; ++i) {
+            wa[i] = q[i + k * N];
+            q[i + k * N] = 0;
+        }
+        q[k + k * N] = 1;
+        if (wa[k] == 0) continue;
+        for (int j = k; j < N; ++j) {
+            double sum = 0;
+            for (int i = k; i < N; ++i) sum += q[i + j * N] * wa[i];
+            const double temp = sum / wa[k];
+            for (int i = k; i < N; ++i) q[i + j * N] -= temp * wa[i];
+        }
+    }
+}
+
+__device__ void dogleg(const double* r, const double* diag, const double* qtb, double delta, double* x, double* wa1,
+                       double* wa2) {
+    int jj = (N * (N + 1)) / 2;
+    for (int k = 1; k <= N; ++k) {
+        const int j = N - k;
+        jj -= k;
+        int l = jj + 1;
+        double sum = 0;
+        for (int i = j + 1; i < N; ++i) sum += r[l++] * x[i];
+        double temp = r[jj];
+        if (temp == 0) {
+            int ll = j;
+            for (int i = 0; i <= j; ++i) {
+                temp = fmax(temp, fabs(r[ll]));
+                ll += N - i - 1;
+            }
+            temp = kEps * temp;
+            if (temp == 0) temp = kEps;
+        }
+        x[j] = (qtb[j] - sum) / temp;
+    }
+    for (int j = 0; j < N; ++j) {
+        wa1[j] = 0;
+        wa2[j] = diag[j] * x[j];
+    }
+    const double qnorm = enorm(N, wa2);
+    if (qnorm <= delta) return;
+    int l = 0;
+    for (int j = 0; j < N; ++j) {
+        const double temp = qtb[j];
+        for (int i = j; i < N; ++i) wa1[i] += r[l++] * temp;
+        wa1[j] /= diag[j];
+    }
+    const double gnorm = enorm(N, wa1);
+    double sgnorm = 0, alpha = delta / qnorm;
+    if (gnorm != 0) {
+        for (int j = 0; j < N; ++j) wa1[j] = (wa1[j] / gnorm) / diag[j];
+        l = 0;
+        for (int j = 0; j < N; ++j) {
+            double sum = 0;
+            for (int i = j; i < N; ++i) sum += r[l++] * wa1[i];
+            wa2[j] = sum;
+        }
+        const double temp = enorm(N, wa2);
+        sgnorm = (gnorm / temp) / temp;
+        alpha = 0;
+        if (sgnorm < delta) {
+            const double bnorm = enorm(N, qtb);
+            double t = (bnorm / gnorm) * (bnorm / qnorm) * (sgnorm / delta);
+            t = t - (delta / qnorm) * (sgnorm / delta) * (sgnorm / delta) +
+                sqrt((t - (delta / qnorm)) * (t - (delta / qnorm)) +
+                     (1 - (delta / qnorm) * (delta / qnorm)) * (1 - (sgnorm / delta) * (sgnorm / delta)));
+            alpha = ((delta / qnorm) * (1 - (sgnorm / delta) * (sgnorm / delta))) / t;
+        }
+    }
+    const double temp = (1 - alpha) * fmin(sgnorm, delta);
+    for (int j = 0; j < N; ++j) x[j] = temp * wa1[j] + alpha * x[j];
+}
+
+__device__ void r1updt(double* s, const double* u, double* v, double* w) {
+    const int m = N;
+    int jj = (N * (2 * m - N + 1)) / 2 - (m - N) - 1;
+    int l = jj;
+    for (int i = N - 1; i < m; ++i) w[i] = s[l++];
+    for (int nmj = 1; nmj <= N - 1; ++nmj) {
+        const int j = N - 1 - nmj;
+        jj -= m - j;
+        w[j] = 0;
+        if (v[j] != 0) {
+            double cs, sn, tau;
+            if (fabs(v[N - 1]) < fabs(v[j])) {
+                const double cotan = v[N - 1] / v[j];
+                sn = 0.5 / sqrt(0.25 + 0.25 * cotan * cotan);
+                cs = sn * cotan;
+                tau = 1;
+                if (fabs(cs) * kGiant > 1) tau = 1 / cs;
+            } else {
+                const double tn = v[j] / v[N - 1];
+                cs = 0.5 / sqrt(0.25 + 0.25 * tn * tn);
+                sn = cs * tn;
+                tau = sn;
+            }
+            v[N - 1] = sn * v[j] + cs * v[N - 1];
+            v[j] = tau;
+            l = jj;
+            for (int i = j; i < m; ++i) {
+                const double temp = cs * s[l] - sn * w[i];
+                w[i] = sn * s[l] + cs * w[i];
+                s[l] = temp;
+                ++l;
+            }
+        }
+    }
+    for (int i = 0; i < m; ++i) w[i] += v[N - 1] * u[i];
+    for (int j = 0; j < N - 1; ++j) {
+        if (w[j] != 0) {
+            double cs, sn, tau;
+            if (fabs(s[jj]) < fabs(w[j])) {
+                const double cotan = s[jj] / w[j];
+                sn = 0.5 / sqrt(0.25 + 0.25 * cotan * cotan);
+                cs = sn * cotan;
+                tau = 1;
+                if (fabs(cs) * kGiant > 1) tau = 1 / cs;
+            } else {
+                const double tn = w[j] / s[jj];
+                cs = 0.5 / sqrt(0.25 + 0.25 * tn * tn);
+                sn = cs * tn;
+                tau = sn;
+            }
+            l = jj;
+            for (int i = j; i < m; ++i) {
+                const double temp = cs * s[l] + sn * w[i];
+                w[i] = -sn * s[l] + cs * w[i];
+                s[l] = temp;
+                ++l;
+            }
+            w[j] = tau;
+        }
+        jj += m - j;
+    }
+    l = jj;
+    for (int i = N - 1; i < m; ++i) s[l++] = w[i];
+}
+
+__device__ void r1mpyq(int m, double* a, int lda, const double* v, const double* w) {
+    for (int nmj = 1; nmj <= N - 1; ++nmj) {
+        const int j = N - 1 - nmj;
+        double cs, sn;
+        if (fabs(v[j]) > 1) {
+            cs = 1 / v[j];
+            sn = sqrt(1 - cs * cs);
+        } else {
+            sn = v[j];
+            cs = sqrt(1 - sn * sn);
+        }
+        for (int i = 0; i < m; ++i) {
+            const double temp = cs * a[i + j * lda] - sn * a[i + (N - 1) * lda];
+            a[i + (N - 1) * lda] = sn * a[i + j * lda] + cs * a[i + (N - 1) * lda];
+            a[i + j * lda] = temp;
+        }
+    }
+    for (int j = 0; j < N - 1; ++j) {
+        double cs, sn;
+        if (fabs(w[j]) > 1) {
+            cs = 1 / w[j];
+            sn = sqrt(1 - cs * cs);
+        } else {
+            sn = w[j];
+            cs = sqrt(1 - sn * sn);
+        }
+        for (int i = 0; i < m; ++i) {
+            const double temp = cs * a[i + j * lda] + sn * a[i + (N - 1) * lda];
+            a[i + (N - 1) * lda] = -sn * a[i + j * lda] + cs * a[i + (N - 1) * lda];
+            a[i + j * lda] = temp;
+        }
+    }
+}
+
+// hybrd1 with the analytic Jacobian; returns info (1..5); at most maxfev evaluations of F
+__device__ int hybrj(const Body& s1, const Body& s2, double* x) {
+    const double p1 = 0.1, p5 = 0.5, p001 = 1e-3, p0001 = 1e-4, xtol = 1e-10, factor = 100.0;
+    const int maxfev = 200 * (N + 1);
+    double fvec[N], fjac[N * N], diag[N], r[(N * (N + 1)) / 2], qtf[N], wa1[N], wa2[N], wa3[N], wa4[N];
+    for (int j = 0; j < N; ++j) diag[j] = 1.0;
+    sese_F(s1, s2, x, fvec);
+    int nfev = 1;
+    double fnorm = enorm(N, fvec);
+    int iter = 1, ncsuc = 0, ncfail = 0, nslow1 = 0, nslow2 = 0;
+    double delta = 0, xnorm = 0;
+    for (;;) {
+        bool jeval = true;
+        sese_J(s1, s2, x, fjac);
+        qrfac(fjac, wa1, wa2);
+        if (iter == 1) {
+            for (int j = 0; j < N; ++j) wa3[j] = diag[j] * x[j];
+            xnorm = enorm(N, wa3);
+            delta = factor * xnorm;
+            if (delta == 0) delta = factor;
+        }
+        for (int i = 0; i < N; ++i) qtf[i] = fvec[i];
+        for (int j = 0; j < N; ++j) {
+            if (fjac[j + j * N] == 0) continue;
+            double sum = 0;
+            for (int i = j; i < N; ++i) sum += fjac[i + j * N] * qtf[i];
+            const double temp = -sum / fjac[j + j * N];
+            for (int i = j; i < N; ++i) qtf[i] += fjac[i + j * N] * temp;
+        }
+        for (int j = 0; j < N; ++j) {
+            int l = j;
+            for (int i = 0; i < j; ++i) {
+                r[l] = fjac[i + j * N];
+                l += N - i - 1;
+            }
+            r[l] = wa1[j];
+        }
+        qform(fjac, wa1);
+        for (;;) {
+            dogleg(r, diag, qtf, delta, wa1, wa2, wa3);
+            for (int j = 0; j < N; ++j) {
+                wa1[j] = -wa1[j];
+                wa2[j] = x[j] + wa1[j];
+                wa3[j] = diag[j] * wa1[j];
+            }
+            const double pnorm = enorm(N, wa3);
+            if (iter == 1) delta = fmin(delta, pnorm);
+            sese_F(s1, s2, wa2, wa4);
+            ++nfev;
+            const double fnorm1 = enorm(N, wa4);
+            double actred = -1;
+            if (fnorm1 < fnorm) actred = 1 - (fnorm1 / fnorm) * (fnorm1 / fnorm);
+            int l = 0;
+            for (int i = 0; i < N; ++i) {
+                double sum = 0;
+                for (int j = i; j < N; ++j) sum += r[l++] * wa1[j];
+                wa3[i] = qtf[i] + sum;
+            }
+            const double temp = enorm(N, wa3);
+            double prered = 0;
+            if (temp < fnorm) prered = 1 - (temp / fnorm) * (temp / fnorm);
+            double ratio = 0;
+            if (prered > 0) ratio = actred / prered;
+            if (ratio < p1) {
+                ncsuc = 0;
+                ++ncfail;
+                delta = p5 * delta;
+            } else {
+                ncfail = 0;
+                ++ncsuc;
+                if (ratio >= p5 || ncsuc > 1) delta = fmax(delta, pnorm / p5);
+                if (fabs(ratio - 1) <= p1) delta = pnorm / p5;
+            }
+            if (ratio >= p0001) {
+                for (int j = 0; j < N; ++j) {
+                    x[j] = wa2[j];
+                    wa2[j] = diag[j] * x[j];
+                    fvec[j] = wa4[j];
+                }
+                xnorm = enorm(N, wa2);
+                fnorm = fnorm1;
+                ++iter;
+            }
+            ++nslow1;
+            if (actred >= p001) nslow1 = 0;
+            if (jeval) ++nslow2;
+            if (actred >= p1) nslow2 = 0;
+            if (delta <= xtol * xnorm || fnorm == 0) return 1;
+            int info = 0;
+            if (nfev >= maxfev) info = 2;
+            if (p1 * fmax(p1 * delta, pnorm) <= kEps * xnorm) info = 3;
+            if (nslow2 == 5) info = 4;
+            if (nslow1 == 10) info = 5;
+            if (info != 0) return info;
+            if (ncfail == 2) break;
+            for (int j = 0; j < N; ++j) {
+                double sum = 0;
+                for (int i = 0; i < N; ++i) sum += fjac[i + j * N] * wa4[i];
+                wa2[j] = (sum - wa3[j]) / pnorm;
+                wa1[j] = diag[j] * ((diag[j] * wa1[j]) / pnorm);
+                if (ratio >= p0001) qtf[j] = sum;
+            }
+            r1updt(r, wa1, wa2, wa3);
+            r1mpyq(N, fjac, N, wa2, wa3);
+            r1mpyq(1, qtf, 1, wa2, wa3);
+            jeval = false;
+        }
+    }
+}
+
+// ------------------------------------------------------------- start grids
+// binit_xy(6) / ainit_yz(6) (superellipsoid.hpp:360-466): 4 angles per sample of [0, pi/2]
+__device__ double init_angle(const Body& s, int k, bool b_axis) {
+    const double pi = 3.14159265358979323846;
+    const int i = k >> 2, w = k & 3;
+    const double t = (0.5 * pi) * i / 5;
+    double v;
+    if (b_axis) {
+        const double x = s.r[0] * cos(t), y = s.r[1] * sin(t);
+        const double d = pow(pow(s.r[1] * x, 2.0 / s.e) + pow(s.r[0] * y, 2.0 / s.e), s.e / 2.0);
+        const double ys = y * s.r[0] * s.r[1] / d;
+        const double sb = fmax(-1.0, fmin(1.0, sqrt(pow(pow(ys / s.r[1], 2.0), 1.0 / s.e))));
+        v = asin(sb);
+    } else {
+        const double y = s.r[1] * cos(t), z = s.r[2] * sin(t);
+        const double d = pow(pow(s.r[2] * y, 2.0 / s.n) + pow(s.r[1] * z, 2.0 / s.n), s.n / 2.0);
+        const double zs = z * s.r[1] * s.r[2] / d;
+        const double sa = fmax(-1.0, fmin(1.0, sqrt(pow(pow(zs / s.r[2], 2.0), 1.0 / s.n))));
+        v = asin(sa);
+    }
+    const double a = w == 0 ? v : (w == 1 ? v + pi / 2 : (w == 2 ? v - pi : v - pi / 2));
+    return fabs(a) < 1.0e-6 ? 0.01 : a;
+}
+
+// sorted unique of the 24 values in place (one thread); returns the count
+__device__ int sort_unique(double* v, int n) {
+    for (int i = 1; i < n; ++i) {
+        const double x = v[i];
+        int j = i - 1;
+        while (j >= 0 && v[j] > x) {
+            v[j + 1] = v[j];
+            --j;
+        }
+        v[j + 1] = x;
+    }
+    int m = n > 0 ? 1 : 0;
+    for (int i = 1; i < n; ++i)
+        if (v[i] != v[m - 1]) v[m++] = v[i];
+    return m;
+}
+
+struct SeShared {
+    double ang[4][kSeGrid];   // a1, b1, a2, b2
+    int cnt[4];
+    double P[2][kSeSamples][3];
+    double Nn[2][kSeSamples][3];
+    double best_v[kSeThreads / 32];
+    long long best_i[kSeThreads / 32];
+    double u[4];
+};
+
+// 3 blocks per SM (56 KB of shared memory each); the solver on thread 0 spills to local
+// memory rather than holding registers that the sample scan of all threads needs
+__global__ void __launch_bounds__(kSeThreads, 3) k_se_pairs(Bodies B, Contacts c, const Sizes* sizes) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    SeShared& S = *reinterpret_cast<SeShared*>(smem);
+    const int C = sizes->C, C_obs = sizes->C_obs;
+    for (int k = C_obs + blockIdx.x; k < C; k += gridDim.x) {
+        const int i = c.ci[k], j = c.cj[k];
+        const Body s1 = load(B, i), s2 = load(B, j);
+        // angle lists: threads 0..95 compute one value each, 4 threads sort
+        if (threadIdx.x < 4 * kSeGrid) {
+            const int list = threadIdx.x / kSeGrid, m = threadIdx.x % kSeGrid;
+            S.ang[list][m] = init_angle(list < 2 ? s1 : s2, m, (list & 1) != 0);
+        }
+        __syncthreads();
+        if (threadIdx.x < 4) S.cnt[threadIdx.x] = sort_unique(S.ang[threadIdx.x], kSeGrid);
+        __syncthreads();
+        // surface samples: meshgrid(a, b) flattened row-major, index ia * nb + ib
+        const int na1 = S.cnt[0], nb1 = S.cnt[1], na2 = S.cnt[2], nb2 = S.cnt[3];
+        const int n1 = na1 * nb1, n2 = na2 * nb2;
+        for (int t = threadIdx.x; t < n1 + n2; t += blockDim.x) {
+            const int w = t < n1 ? 0 : 1;
+            const int q = t < n1 ? t : t - n1;
+            const int nb = w == 0 ? nb1 : nb2;
+            const double a = S.ang[2 * w][q / nb], b = S.ang[2 * w + 1][q % nb];
+            const Body& s = w == 0 ? s1 : s2;
+            point(s, a, b, S.P[w][q]);
+            normal(s, a, b, S.Nn[w][q]);
+        }
+        __syncthreads();
+        // first minimum of |p1 - p2| + 2 (1 + n1.n2) in row-major (p1 index, p2 index) order
+        double bv = INFINITY;
+        long long bi = 0x7fffffffffffffffLL;
+        for (int a = 0; a < n1; ++a) {
+            const double* pa = S.P[0][a];
+            const double* na = S.Nn[0][a];
+            for (int b = threadIdx.x; b < n2; b += blockDim.x) {
+                const double* pb = S.P[1][b];
+                const double* nb = S.Nn[1][b];
+                const double dx = pa[0] - pb[0], dy = pa[1] - pb[1], dz = pa[2] - pb[2];
+                const double v = sqrt(dx * dx + dy * dy + dz * dz) + 2 * (1 + (na[0] * nb[0] + na[1] * nb[1] + na[2] * nb[2]));
+                if (v < bv) {  // per thread, indices increase: the first minimum is kept
+                    bv = v;
+                    bi = (long long)a * n2 + b;
+                }
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ov = __shfl_down_sync(0xffffffffu, bv, o);
+            const long long oi = __shfl_down_sync(0xffffffffu, bi, o);
+            if (ov < bv || (ov == bv && oi < bi)) {
+                bv = ov;
+                bi = oi;
+            }
+        }
+        if ((threadIdx.x & 31) == 0) {
+            S.best_v[threadIdx.x >> 5] = bv;
+            S.best_i[threadIdx.x >> 5] = bi;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+                if (S.best_v[w] < bv || (S.best_v[w] == bv && S.best_i[w] < bi)) {
+                    bv = S.best_v[w];
+                    bi = S.best_i[w];
+                }
+            if (bi == 0x7fffffffffffffffLL) bi = 0;  // NaN everywhere: start at the first sample
+            const int ia = (int)(bi / n2), ib = (int)(bi % n2);
+            double u[4] = {S.ang[0][ia / nb1], S.ang[1][ia % nb1], S.ang[2][ib / nb2], S.ang[3][ib % nb2]};
+            hybrj(s1, s2, u);
+            double pi_[3], pj_[3], nij[3];
+            point(s1, u[0], u[1], pi_);
+            point(s2, u[2], u[3], pj_);
+            normal(s2, u[2], u[3], nij);
+            const double df[3] = {pi_[0] - pj_[0], pi_[1] - pj_[1], pi_[2] - pj_[2]};
+            c.dij[k] = sgn(dot3(df, nij)) * norm3(df);
+            for (int q = 0; q < 3; ++q) {
+                c.pi[3 * (long long)k + q] = pi_[q];
+                c.pj[3 * (long long)k + q] = pj_[q];
+                c.nij[3 * (long long)k + q] = nij[q];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// keep a row: obstacle rows (already exact) or dij < dmax
+__global__ void k_se_keep(Contacts c, const Sizes* sizes, double dmax, int* keep) {
+    const int C = sizes->C, C_obs = sizes->C_obs;
+    GRID_STRIDE(k, C) keep[k] = (k < C_obs || c.dij[k] < dmax) ? 1 : 0;
+}
+
+__global__ void k_se_compact(Contacts src, Contacts dst, const Sizes* sizes, const int* keep, const int* pos) {
+    const int C = sizes->C;
+    GRID_STRIDE(k, C) {
+        if (!keep[k]) continue;
+        const int d = pos[k];
+        dst.ci[d] = src.ci[k];
+        dst.cj[d] = src.cj[k];
+        dst.dij[d] = src.dij[k];
+        dst.gamma[d] = src.gamma[k];
+        for (int q = 0; q < 3; ++q) {
+            dst.nij[3 * (long long)d + q] = src.nij[3 * (long long)k + q];
+            dst.pi[3 * (long long)d + q] = src.pi[3 * (long long)k + q];
+            dst.pj[3 * (long long)d + q] = src.pj[3 * (long long)k + q];
+        }
+    }
+}
+
+__global__ void k_se_sizes(Sizes* sizes, const int* total) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) sizes->C = *total;
+}
+
+}  // namespace
+
+size_t se_pairs_smem() { return sizeof(SeShared); }
+
+void launch_se_pairs(const Bodies& b, Contacts& c, const Sizes* sizes, int grid, cudaStream_t s) {
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(k_se_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SeShared));
+        configured = true;
+    }
+    k_se_pairs<<<grid, kSeThreads, sizeof(SeShared), s>>>(b, c, sizes);
+    g_se_launches += 1;
+}
+
+void launch_se_filter(const Contacts& src, Contacts& dst, Sizes* sizes, double dmax, long long c_cap, int* keep,
+                      int* pos, int* scan_work, int* total, cudaStream_t s) {
+    const int threads = 256;
+    const int blocks = (int)std::min<long long>((c_cap + threads - 1) / threads, 4096);
+    k_se_keep<<<blocks, threads, 0, s>>>(src, sizes, dmax, keep);
+    scan_exclusive(keep, pos, &sizes->C, 0, c_cap, total, scan_work, s, &g_se_launches);
+    k_se_compact<<<blocks, threads, 0, s>>>(src, dst, sizes, keep, pos);
+    k_se_sizes<<<1, 1, 0, s>>>(sizes, total);
+    g_se_launches += 3;
+}
+
+}  // namespace scopi_gpu

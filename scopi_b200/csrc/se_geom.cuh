@@ -1,0 +1,160 @@
+// se_geom.cuh -- 3D superellipsoid geometry on the device (FP64).
+//
+// Parametrisation (include/scopi/objects/types/superellipsoid.hpp:291-325), body frame:
+//   p(a, b) = (rx C(a,n) C(b,e), ry C(a,n) S(b,e), rz S(a,n)),
+//   N(a, b) = (ry rz C(a,2-n) C(b,2-e), rx rz C(a,2-n) S(b,2-e), rx ry S(a,2-n))  (outward, unnormalised)
+// with C(t,k) = sign(cos t)|cos t|^k, S(t,k) = sign(sin t)|sin t|^k; world = R(q) p + c.
+#pragma once
+#include "common.cuh"
+
+namespace scopi_gpu {
+namespace se {
+
+struct Body {
+    double c[3];
+    double R[9];  // row-major rotation (body -> world)
+    double r[3];
+    double e, n;
+};
+
+__device__ __forceinline__ double sgn(double x) { return x > 0 ? 1.0 : (x < 0 ? -1.0 : 0.0); }
+__device__ __forceinline__ double cpow(double x, double k) {
+    const double c = cos(x);
+    return sgn(c) * pow(fabs(c), k);
+}
+__device__ __forceinline__ double spow(double x, double k) {
+    const double s = sin(x);
+    return sgn(s) * pow(fabs(s), k);
+}
+__device__ __forceinline__ double dcpow(double x, double k) { return -k * sin(x) * pow(fabs(cos(x)), k - 1); }
+__device__ __forceinline__ double dspow(double x, double k) { return k * cos(x) * pow(fabs(sin(x)), k - 1); }
+
+// rotation_matrix<3>(q), q = (w, x, y, z) (quaternion.hpp:87-124)
+__device__ __forceinline__ void rot(const double* q, double* R) {
+    const double x = q[0], y = q[1], z = q[2], w = q[3];
+    R[0] = 1 - 2 * z * z - 2 * w * w;
+    R[1] = 2 * y * z - 2 * x * w;
+    R[2] = 2 * y * w + 2 * x * z;
+    R[3] = 2 * y * z + 2 * x * w;
+    R[4] = 1 - 2 * y * y - 2 * w * w;
+    R[5] = 2 * z * w - 2 * x * y;
+    R[6] = 2 * y * w - 2 * x * z;
+    R[7] = 2 * z * w + 2 * x * y;
+    R[8] = 1 - 2 * y * y - 2 * z * z;
+}
+
+__device__ __forceinline__ Body load(const Bodies& B, int b) {
+    Body s;
+    for (int k = 0; k < 3; ++k) {
+        s.c[k] = B.pos[3 * (long long)b + k];
+        s.r[k] = B.axes[3 * (long long)b + k];
+    }
+    s.e = B.sq[2 * (long long)b];
+    s.n = B.sq[2 * (long long)b + 1];
+    rot(B.q + 4 * (long long)b, s.R);
+    return s;
+}
+
+__device__ __forceinline__ void mv(const double* R, const double* x, double* y) {
+    y[0] = R[0] * x[0] + R[1] * x[1] + R[2] * x[2];
+    y[1] = R[3] * x[0] + R[4] * x[1] + R[5] * x[2];
+    y[2] = R[6] * x[0] + R[7] * x[1] + R[8] * x[2];
+}
+__device__ __forceinline__ void cross(const double* a, const double* b, double* c) {
+    c[0] = a[1] * b[2] - a[2] * b[1];
+    c[1] = a[2] * b[0] - a[0] * b[2];
+    c[2] = a[0] * b[1] - a[1] * b[0];
+}
+__device__ __forceinline__ double dot3(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+__device__ __forceinline__ double norm3(const double* a) { return sqrt(dot3(a, a)); }
+
+// world point and unit world normal at (a, b)
+__device__ __forceinline__ void point(const Body& s, double a, double b, double* w) {
+    const double ca = cpow(a, s.n);
+    const double p[3] = {s.r[0] * ca * cpow(b, s.e), s.r[1] * ca * spow(b, s.e), s.r[2] * spow(a, s.n)};
+    mv(s.R, p, w);
+    for (int k = 0; k < 3; ++k) w[k] += s.c[k];
+}
+__device__ __forceinline__ void normal(const Body& s, double a, double b, double* w) {
+    const double ca = cpow(a, 2 - s.n);
+    const double N[3] = {s.r[1] * s.r[2] * ca * cpow(b, 2 - s.e), s.r[0] * s.r[2] * ca * spow(b, 2 - s.e),
+                         s.r[0] * s.r[1] * spow(a, 2 - s.n)};
+    mv(s.R, N, w);
+    const double l = norm3(w);
+    for (int k = 0; k < 3; ++k) w[k] /= l;
+}
+
+// body-frame point, unnormalised normal and their angle derivatives
+struct Local {
+    double p[3], pa[3], pb[3], N[3], Na[3], Nb[3];
+};
+__device__ __forceinline__ void local(const Body& s, double a, double b, Local& L) {
+    const double rx = s.r[0], ry = s.r[1], rz = s.r[2];
+    const double Ca = cpow(a, s.n), Sa = spow(a, s.n), Cb = cpow(b, s.e), Sb = spow(b, s.e);
+    const double dCa = dcpow(a, s.n), dSa = dspow(a, s.n), dCb = dcpow(b, s.e), dSb = dspow(b, s.e);
+    const double n2 = 2 - s.n, e2 = 2 - s.e;
+    const double Ca2 = cpow(a, n2), Sa2 = spow(a, n2), Cb2 = cpow(b, e2), Sb2 = spow(b, e2);
+    const double dCa2 = dcpow(a, n2), dSa2 = dspow(a, n2), dCb2 = dcpow(b, e2), dSb2 = dspow(b, e2);
+    L.p[0] = rx * Ca * Cb;
+    L.p[1] = ry * Ca * Sb;
+    L.p[2] = rz * Sa;
+    L.pa[0] = rx * dCa * Cb;
+    L.pa[1] = ry * dCa * Sb;
+    L.pa[2] = rz * dSa;
+    L.pb[0] = rx * Ca * dCb;
+    L.pb[1] = ry * Ca * dSb;
+    L.pb[2] = 0.0;
+    L.N[0] = ry * rz * Ca2 * Cb2;
+    L.N[1] = rx * rz * Ca2 * Sb2;
+    L.N[2] = rx * ry * Sa2;
+    L.Na[0] = ry * rz * dCa2 * Cb2;
+    L.Na[1] = rx * rz * dCa2 * Sb2;
+    L.Na[2] = rx * ry * dSa2;
+    L.Nb[0] = ry * rz * Ca2 * dCb2;
+    L.Nb[1] = rx * rz * Ca2 * dSb2;
+    L.Nb[2] = 0.0;
+}
+
+// Closest points of a superellipsoid and a plane (the solution of the system of
+// closest_points.hpp:1479-1759 in closed form): the body point whose outward normal is
+// opposite to the plane normal oriented toward the body, and its projection on the plane.
+// pi on the body, pj on the plane, nij = the oriented plane normal, dij = (pi - pj).nij.
+__device__ __forceinline__ void body_plane(const Body& s, const double* pc, const double* pq, double* pi, double* pj,
+                                           double* nij, double& dij) {
+    const double pi_ = 3.14159265358979323846;
+    double P[9];
+    rot(pq, P);
+    const double np[3] = {P[0], P[3], P[6]};
+    const double rel[3] = {s.c[0] - pc[0], s.c[1] - pc[1], s.c[2] - pc[2]};
+    const double sg = dot3(rel, np) < 0 ? -1.0 : 1.0;
+    // body-frame direction of the wanted outward normal: -sg np (R^T np)
+    const double m[3] = {-sg * (s.R[0] * np[0] + s.R[3] * np[1] + s.R[6] * np[2]),
+                         -sg * (s.R[1] * np[0] + s.R[4] * np[1] + s.R[7] * np[2]),
+                         -sg * (s.R[2] * np[0] + s.R[5] * np[1] + s.R[8] * np[2])};
+    const double rx = s.r[0], ry = s.r[1], rz = s.r[2];
+    const double mxy = sqrt(m[0] * m[0] + m[1] * m[1]);
+    double a, b;
+    if (mxy == 0) {
+        b = 0;
+        a = m[2] >= 0 ? pi_ / 2 : -pi_ / 2;
+    } else {
+        const double ke = 1.0 / (2 - s.e), kn = 1.0 / (2 - s.n);
+        b = atan2(sgn(m[1]) * pow(fabs(ry * m[1]), ke), sgn(m[0]) * pow(fabs(rx * m[0]), ke));
+        const double cb = cpow(b, 2 - s.e), sb = spow(b, 2 - s.e);
+        const double h = sqrt((ry * rz * cb) * (ry * rz * cb) + (rx * rz * sb) * (rx * rz * sb));
+        const double t = fabs(m[2]) * h / (rx * ry * mxy);
+        a = sgn(m[2]) * atan(pow(t, kn));
+    }
+    point(s, a, b, pi);
+    const double d[3] = {pi[0] - pc[0], pi[1] - pc[1], pi[2] - pc[2]};
+    const double h = dot3(d, np);
+    for (int k = 0; k < 3; ++k) {
+        pj[k] = pi[k] - h * np[k];
+        nij[k] = sg * np[k];
+    }
+    const double df[3] = {pi[0] - pj[0], pi[1] - pj[1], pi[2] - pj[2]};
+    dij = dot3(df, nij);
+}
+
+}  // namespace se
+}  // namespace scopi_gpu

@@ -190,7 +190,7 @@ def test_rotated_superellipsoid_above_a_plane_matches_sampling(seed):
 def test_superellipsoid_scene_runs_in_the_oracle():
     pa = configs.se_pile(count=27, side=3, seed=3)
     o = orc.OracleSolver(pa, problem=orc.FRICTION, vap=orc.VAP_FPD, dmax=0.004, mu=0.3, tolerance=1e-6,
-                         max_ite=40000)
+                         max_ite=40000, kd_tree_radius=configs.se_kd_radius(pa, 0.004))
     o.run(5e-4, 3)
     c = o.contacts()
     assert len(c["i"]) > 0
