@@ -194,12 +194,12 @@ def se_record(c, q, r, sq):
 
 def _unpack(out):
     return {"pi": out[0:3].copy(), "pj": out[3:6].copy(), "nij": out[6:9].copy(), "dij": float(out[9]),
-            "u": out[10:14].copy()}
+            "u": out[10:14].copy(), "nfev": int(out[14])}
 
 
 def se_se(s1, s2):
     """closest_points(superellipsoid<3>, superellipsoid<3>) on two body records."""
-    out = np.zeros(14)
+    out = np.zeros(15)
     a, b = np.ascontiguousarray(s1, float), np.ascontiguousarray(s2, float)
     info = lib().orc_se_se(_dp(a), _dp(b), _dp(out))
     r = _unpack(out)
@@ -209,7 +209,7 @@ def se_se(s1, s2):
 
 def se_plane(s, plane_c, plane_q):
     """closest_points(superellipsoid<3>, plane<3>); the plane record is {c[3], q[4]}."""
-    out = np.zeros(14)
+    out = np.zeros(15)
     a = np.ascontiguousarray(s, float)
     p = np.ascontiguousarray(np.concatenate([np.asarray(plane_c, float)[:3], np.asarray(plane_q, float)[:4]]))
     lib().orc_se_plane(_dp(a), _dp(p), _dp(out))

@@ -229,6 +229,14 @@ struct orc_solver {
         } else if (sa == ORC_SPHERE && sb == ORC_SEGMENT) {
             c = sphere_segment(a, b);
         } else if (dim == 3 && sa == ORC_SUPERELLIPSOID && sb == ORC_SUPERELLIPSOID) {
+            // bounding spheres (radius = |semi-axes|) farther apart than dmax: no contact, no
+            // solve.  The reference solves every kd-tree candidate; on well-separated pairs
+            // its solve can stop at a spurious root with dij < dmax (about 0.1 % of the
+            // candidates of the superellipsoid pile), which is not reproduced.
+            double s2 = 0.0;
+            for (int k = 0; k < 3; ++k) s2 += (pos[a][k] - pos[b][k]) * (pos[a][k] - pos[b][k]);
+            const double lim = radius[a] + radius[b] + p.dmax;
+            if (!(lim > 0.0) || s2 > lim * lim * (1.0 + 1e-9)) return false;
             c = from_pair(orc_se::se_se(se_of(a), se_of(b)));
         } else if (dim == 3 && sa == ORC_SUPERELLIPSOID && sb == ORC_PLANE) {
             c = from_pair(orc_se::se_plane(se_of(a), plane_of(b)));
@@ -927,6 +935,7 @@ void write_pair(const orc_se::PairOut& o, double* out) {
     }
     out[9] = o.dij;
     for (int k = 0; k < 4; ++k) out[10 + k] = o.u[k];
+    out[14] = o.nfev;
 }
 }  // namespace
 

@@ -112,7 +112,8 @@ int64_t orc_detect(orc_solver* s);
 /* Closest points of two 3D superellipsoids / a superellipsoid and a plane, as the contact
    list would record them (closest_points.hpp:263-733, 1479-1768).  A body is
    {c[3], q[4] (w, x, y, z), r[3], e, n}; a plane {c[3], q[4]}.  out = pi[3], pj[3], nij[3],
-   dij, u[4] (the solver's unknowns); returns the solver's info (hybrd) / iterations (Newton). */
+   dij, u[4] (the solver's unknowns), function evaluations; returns the solver's info (0 for
+   the closed-form superellipsoid-plane case). */
 int orc_se_se(const double* s1, const double* s2, double* out);
 int orc_se_plane(const double* s, const double* plane, double* out);
 /* The hybrid method alone from the start u (in/out); returns info, *nfev its function count. */

@@ -511,6 +511,7 @@ struct PairOut {
     V3 pi, pj, nij;
     double dij;
     int info;
+    int nfev = 0;
     double u[4];
 };
 
@@ -602,6 +603,7 @@ inline PairOut se_se(const SE& s1, const SE& s2) {
                                   [&](const double* x, double* J) { sese_J(s1, s2, x, J); }, u);
     PairOut o;
     o.info = h.info;
+    o.nfev = h.nfev;
     for (int k = 0; k < 4; ++k) o.u[k] = u[k];
     o.pi = point(s1, u[0], u[1]);
     o.pj = point(s2, u[2], u[3]);

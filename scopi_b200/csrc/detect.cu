@@ -384,12 +384,10 @@ __device__ __forceinline__ bool pair_in_contact(const StepParams& p, const doubl
         s2 += dd * dd;
     }
     if (p.kd_filter && !(s2 < p.kd_radius)) return false;
-    // superellipsoids: the candidates of the reference's kd-tree radius search (the exact
-    // solve of se.cu decides; contact_kdtree.hpp:240-262), or without that search the pairs
-    // whose bounding spheres (w = bounding radius) come within dmax
-    if (p.se_mode && p.kd_filter) return true;
     const double lim = L.w + H.w + p.dmax;
     if (!(lim > 0.0) || s2 > lim * lim * (1.0 + 1e-9)) return false;
+    // superellipsoids (w = bounding radius): the pairs whose bounding spheres come within
+    // dmax go to the exact solve of se.cu, which decides
     if (p.se_mode) return true;
     PairGeom pg;
     sphere_sphere(DIM, xl, L.w, xh, H.w, pg);

@@ -58,6 +58,7 @@ struct scopi_gpu_handle {
            *d_f = nullptr, *d_m = nullptr, *d_j = nullptr, *d_radius = nullptr, *d_length = nullptr;
     double *d_axes = nullptr, *d_sq = nullptr;  // superellipsoids
     int *d_se_keep = nullptr, *d_se_pos = nullptr;  // contact filter of superellipsoid candidates
+    double* d_se_u = nullptr;                       // start of each superellipsoid solve
     bool has_se = false;                        // some active body is a superellipsoid
     double* d_invm64 = nullptr;
     float* d_invm32 = nullptr;
@@ -511,7 +512,7 @@ struct scopi_gpu_handle {
             for (int k = 0; k < 3; ++k) A(d_lam32[k], M)
             A(d_g32, M)
         }
-        A(d_cij, cap) A(d_nc64, cap) A(d_incv64, 2 * cap) A(d_se_keep, cap + 1) A(d_se_pos, cap + 1)
+        A(d_cij, cap) A(d_nc64, cap) A(d_incv64, 2 * cap) A(d_se_keep, cap + 1) A(d_se_pos, cap + 1) A(d_se_u, 4 * cap + 4)
         if (mixed()) {
             A(d_nc32, cap) A(d_incv32, 2 * cap)
         }
@@ -563,7 +564,7 @@ struct scopi_gpu_handle {
             // the search kept bounding-sphere candidates: closest points of the superellipsoid
             // pairs, then the rows with dij < dmax into the other list (no viscous gamma to
             // carry here), which becomes the current one
-            launch_se_pairs(b, cur, d_sizes_cur, 3 * kSMs, stream);
+            launch_se_pairs(b, cur, d_sizes_cur, d_se_u, dw.tmp_total + 3, 3 * kSMs, stream);
             launch_se_filter(cur, old, d_sizes_cur, P.dmax, c_cap, d_se_keep, d_se_pos, dw.scan_work,
                              dw.tmp_total + 2, stream);
             std::swap(cur, old);

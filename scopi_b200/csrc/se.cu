@@ -9,10 +9,10 @@
 //          analytic Jacobian (n1, n2 unnormalised normals);
 //   result: pi = p1(u), pj = p2(u), nij = unit normal of body 2 at pj,
 //          dij = sign((pi - pj).nij) |pi - pj|.
-// The block computes the surface samples of both bodies into shared memory, every thread
-// scans a slice of the sample pairs, a block reduction finds the first minimum, and thread
-// 0 runs the hybrid method (4 unknowns, a few dozen function evaluations, bounded by
-// maxfev).  Built with -fmad=false like detect.cu.
+// k_se_start (one block per pair) computes the surface samples of both bodies into shared
+// memory and finds the first minimum of the start criterion (FP32 screen, FP64 decision);
+// k_se_solve (one warp per pair) runs the hybrid method from it (4 unknowns, bounded by
+// maxfev) and writes the closest points.  Built with -fmad=false like detect.cu.
 #include <math.h>
 
 #include <algorithm>
@@ -31,55 +31,6 @@ using namespace se;
 constexpr int kSeThreads = 256;
 constexpr int kSeGrid = 24;       // unique angles per grid axis at most (4 * 6)
 constexpr int kSeSamples = kSeGrid * kSeGrid;
-
-// --------------------------------------------------------------- F and Jacobian
-__device__ void sese_F(const Body& s1, const Body& s2, const double* u, double* F) {
-    Local L1, L2;
-    local(s1, u[0], u[1], L1);
-    local(s2, u[2], u[3], L2);
-    double p1[3], p2[3], n1[3], n2[3];
-    mv(s1.R, L1.p, p1);
-    mv(s2.R, L2.p, p2);
-    mv(s1.R, L1.N, n1);
-    mv(s2.R, L2.N, n2);
-    const double d[3] = {p2[0] + s2.c[0] - p1[0] - s1.c[0], p2[1] + s2.c[1] - p1[1] - s1.c[1],
-                         p2[2] + s2.c[2] - p1[2] - s1.c[2]};
-    cross(d, n1, F);
-    F[3] = dot3(n1, n2) + norm3(n1) * norm3(n2);
-}
-
-__device__ void sese_J(const Body& s1, const Body& s2, const double* u, double* J) {  // column-major
-    Local L1, L2;
-    local(s1, u[0], u[1], L1);
-    local(s2, u[2], u[3], L2);
-    double p1[3], p2[3], n1[3], n2[3];
-    mv(s1.R, L1.p, p1);
-    mv(s2.R, L2.p, p2);
-    mv(s1.R, L1.N, n1);
-    mv(s2.R, L2.N, n2);
-    const double d[3] = {p2[0] + s2.c[0] - p1[0] - s1.c[0], p2[1] + s2.c[1] - p1[1] - s1.c[1],
-                         p2[2] + s2.c[2] - p1[2] - s1.c[2]};
-    const double l1 = norm3(n1), l2 = norm3(n2);
-    for (int k = 0; k < 4; ++k) {
-        double dd[3], dn1[3] = {0, 0, 0}, dn2[3] = {0, 0, 0};
-        if (k < 2) {
-            double t[3];
-            mv(s1.R, k == 0 ? L1.pa : L1.pb, t);
-            for (int c = 0; c < 3; ++c) dd[c] = -t[c];
-            mv(s1.R, k == 0 ? L1.Na : L1.Nb, dn1);
-        } else {
-            mv(s2.R, k == 2 ? L2.pa : L2.pb, dd);
-            mv(s2.R, k == 2 ? L2.Na : L2.Nb, dn2);
-        }
-        double a[3], b[3];
-        cross(dd, n1, a);
-        cross(d, dn1, b);
-        J[0 + 4 * k] = a[0] + b[0];
-        J[1 + 4 * k] = a[1] + b[1];
-        J[2 + 4 * k] = a[2] + b[2];
-        J[3 + 4 * k] = dot3(dn1, n2) + dot3(n1, dn2) + dot3(n1, dn1) / l1 * l2 + l1 * dot3(n2, dn2) / l2;
-    }
-}
 
 // ------------------------------------------------------- MINPACK pieces (n = 4)
 constexpr int N = 4;
@@ -318,20 +269,22 @@ __device__ void r1mpyq(int m, double* a, int lda, const double* v, const double*
     }
 }
 
-// hybrd1 with the analytic Jacobian; returns info (1..5); at most maxfev evaluations of F
-__device__ int hybrj(const Body& s1, const Body& s2, double* x) {
+// hybrd1 with the analytic Jacobian; returns info (1..5); at most maxfev evaluations of F.
+// fun(x, F) and jac(x, J) (column-major) evaluate the system.
+template <typename Fun, typename Jac>
+__device__ int hybrj(Fun&& fun, Jac&& jac, double* x) {
     const double p1 = 0.1, p5 = 0.5, p001 = 1e-3, p0001 = 1e-4, xtol = 1e-10, factor = 100.0;
     const int maxfev = 200 * (N + 1);
     double fvec[N], fjac[N * N], diag[N], r[(N * (N + 1)) / 2], qtf[N], wa1[N], wa2[N], wa3[N], wa4[N];
     for (int j = 0; j < N; ++j) diag[j] = 1.0;
-    sese_F(s1, s2, x, fvec);
+    fun(x, fvec);
     int nfev = 1;
     double fnorm = enorm(N, fvec);
     int iter = 1, ncsuc = 0, ncfail = 0, nslow1 = 0, nslow2 = 0;
     double delta = 0, xnorm = 0;
     for (;;) {
         bool jeval = true;
-        sese_J(s1, s2, x, fjac);
+        jac(x, fjac);
         qrfac(fjac, wa1, wa2);
         if (iter == 1) {
             for (int j = 0; j < N; ++j) wa3[j] = diag[j] * x[j];
@@ -365,7 +318,7 @@ __device__ int hybrj(const Body& s1, const Body& s2, double* x) {
             }
             const double pnorm = enorm(N, wa3);
             if (iter == 1) delta = fmin(delta, pnorm);
-            sese_F(s1, s2, wa2, wa4);
+            fun(wa2, wa4);
             ++nfev;
             const double fnorm1 = enorm(N, wa4);
             double actred = -1;
@@ -476,19 +429,29 @@ struct SeShared {
     double Nn[2][kSeSamples][3];
     double best_v[kSeThreads / 32];
     long long best_i[kSeThreads / 32];
-    double u[4];
 };
 
-// 3 blocks per SM (56 KB of shared memory each); the solver on thread 0 spills to local
-// memory rather than holding registers that the sample scan of all threads needs
-__global__ void __launch_bounds__(kSeThreads, 3) k_se_pairs(Bodies B, Contacts c, const Sizes* sizes) {
+// |p1 - p2| + 2 (1 + n1.n2) in FP64, the start criterion of closest_points.hpp:654-660
+__device__ __forceinline__ double start_value(const double* p1, const double* n1, const double* p2, const double* n2) {
+    const double dx = p1[0] - p2[0], dy = p1[1] - p2[1], dz = p1[2] - p2[2];
+    return sqrt(dx * dx + dy * dy + dz * dz) + 2 * (1 + (n1[0] * n2[0] + n1[1] * n2[1] + n1[2] * n2[2]));
+}
+
+// Start of the solve of each superellipsoid row: the first minimum (row-major over
+// (sample of body 1, sample of body 2)) of the FP64 start criterion.  Every value is first
+// screened in FP32 (samples relative to body 1's centre, error < 1e-6); a value enters the
+// exact FP64 comparison when it is within kScreen of the thread's running FP32 minimum, so
+// the FP64 minimiser (whose FP32 value is within twice the FP32 error of every running
+// minimum) is always compared exactly.
+constexpr float kScreen = 1e-5f;
+constexpr int kJ = (kSeSamples + kSeThreads - 1) / kSeThreads;  // body-2 samples per thread
+
+__global__ void __launch_bounds__(kSeThreads, 3) k_se_start(Bodies B, Contacts c, const Sizes* sizes, double* u0) {
     extern __shared__ __align__(16) unsigned char smem[];
     SeShared& S = *reinterpret_cast<SeShared*>(smem);
     const int C = sizes->C, C_obs = sizes->C_obs;
     for (int k = C_obs + blockIdx.x; k < C; k += gridDim.x) {
-        const int i = c.ci[k], j = c.cj[k];
-        const Body s1 = load(B, i), s2 = load(B, j);
-        // angle lists: threads 0..95 compute one value each, 4 threads sort
+        const Body s1 = load(B, c.ci[k]), s2 = load(B, c.cj[k]);
         if (threadIdx.x < 4 * kSeGrid) {
             const int list = threadIdx.x / kSeGrid, m = threadIdx.x % kSeGrid;
             S.ang[list][m] = init_angle(list < 2 ? s1 : s2, m, (list & 1) != 0);
@@ -509,21 +472,40 @@ __global__ void __launch_bounds__(kSeThreads, 3) k_se_pairs(Bodies B, Contacts c
             normal(s, a, b, S.Nn[w][q]);
         }
         __syncthreads();
-        // first minimum of |p1 - p2| + 2 (1 + n1.n2) in row-major (p1 index, p2 index) order
+        // this thread's body-2 samples in registers, FP32, relative to body 1's centre
+        float q2[kJ][3], m2[kJ][3];
+        int jn = 0;
+        for (int jj = 0; jj < kJ; ++jj) {
+            const int j = threadIdx.x + jj * kSeThreads;
+            if (j < n2) {
+                for (int d = 0; d < 3; ++d) {
+                    q2[jj][d] = (float)(S.P[1][j][d] - s1.c[d]);
+                    m2[jj][d] = (float)S.Nn[1][j][d];
+                }
+                jn = jj + 1;
+            }
+        }
+        float run32 = INFINITY;
         double bv = INFINITY;
         long long bi = 0x7fffffffffffffffLL;
         for (int a = 0; a < n1; ++a) {
-            const double* pa = S.P[0][a];
-            const double* na = S.Nn[0][a];
-            for (int b = threadIdx.x; b < n2; b += blockDim.x) {
-                const double* pb = S.P[1][b];
-                const double* nb = S.Nn[1][b];
-                const double dx = pa[0] - pb[0], dy = pa[1] - pb[1], dz = pa[2] - pb[2];
-                const double v = sqrt(dx * dx + dy * dy + dz * dz) + 2 * (1 + (na[0] * nb[0] + na[1] * nb[1] + na[2] * nb[2]));
-                if (v < bv) {  // per thread, indices increase: the first minimum is kept
-                    bv = v;
-                    bi = (long long)a * n2 + b;
+            const float x = (float)(S.P[0][a][0] - s1.c[0]), y = (float)(S.P[0][a][1] - s1.c[1]),
+                        z = (float)(S.P[0][a][2] - s1.c[2]);
+            const float nx = (float)S.Nn[0][a][0], ny = (float)S.Nn[0][a][1], nz = (float)S.Nn[0][a][2];
+            for (int jj = 0; jj < jn; ++jj) {
+                const float dx = x - q2[jj][0], dy = y - q2[jj][1], dz = z - q2[jj][2];
+                const float v = sqrtf(dx * dx + dy * dy + dz * dz) +
+                                2.f * (1.f + (nx * m2[jj][0] + ny * m2[jj][1] + nz * m2[jj][2]));
+                if (v <= run32 + kScreen) {
+                    const int j = threadIdx.x + jj * kSeThreads;
+                    const double v64 = start_value(S.P[0][a], S.Nn[0][a], S.P[1][j], S.Nn[1][j]);
+                    const long long idx = (long long)a * n2 + j;
+                    if (v64 < bv || (v64 == bv && idx < bi)) {
+                        bv = v64;
+                        bi = idx;
+                    }
                 }
+                run32 = fminf(run32, v);
             }
         }
 #pragma unroll
@@ -548,21 +530,92 @@ __global__ void __launch_bounds__(kSeThreads, 3) k_se_pairs(Bodies B, Contacts c
                 }
             if (bi == 0x7fffffffffffffffLL) bi = 0;  // NaN everywhere: start at the first sample
             const int ia = (int)(bi / n2), ib = (int)(bi % n2);
-            double u[4] = {S.ang[0][ia / nb1], S.ang[1][ia % nb1], S.ang[2][ib / nb2], S.ang[3][ib % nb2]};
-            hybrj(s1, s2, u);
-            double pi_[3], pj_[3], nij[3];
-            point(s1, u[0], u[1], pi_);
-            point(s2, u[2], u[3], pj_);
-            normal(s2, u[2], u[3], nij);
-            const double df[3] = {pi_[0] - pj_[0], pi_[1] - pj_[1], pi_[2] - pj_[2]};
-            c.dij[k] = sgn(dot3(df, nij)) * norm3(df);
-            for (int q = 0; q < 3; ++q) {
-                c.pi[3 * (long long)k + q] = pi_[q];
-                c.pj[3 * (long long)k + q] = pj_[q];
-                c.nij[3 * (long long)k + q] = nij[q];
-            }
+            double* u = u0 + 4 * (long long)k;
+            u[0] = S.ang[0][ia / nb1];
+            u[1] = S.ang[1][ia % nb1];
+            u[2] = S.ang[2][ib / nb2];
+            u[3] = S.ang[3][ib % nb2];
         }
         __syncthreads();
+    }
+}
+
+// --------------------------------------------------------------- F and Jacobian
+__device__ void sese_F(const Body& s1, const Body& s2, const double* u, double* F) {
+    Local L1, L2;
+    local(s1, u[0], u[1], L1, false);
+    local(s2, u[2], u[3], L2, false);
+    double p1[3], p2[3], n1[3], n2[3];
+    mv(s1.R, L1.p, p1);
+    mv(s2.R, L2.p, p2);
+    mv(s1.R, L1.N, n1);
+    mv(s2.R, L2.N, n2);
+    const double d[3] = {p2[0] + s2.c[0] - p1[0] - s1.c[0], p2[1] + s2.c[1] - p1[1] - s1.c[1],
+                         p2[2] + s2.c[2] - p1[2] - s1.c[2]};
+    cross(d, n1, F);
+    F[3] = dot3(n1, n2) + norm3(n1) * norm3(n2);
+}
+
+__device__ void sese_J(const Body& s1, const Body& s2, const double* u, double* J) {  // column-major
+    Local L1, L2;
+    local(s1, u[0], u[1], L1);
+    local(s2, u[2], u[3], L2);
+    double p1[3], p2[3], n1[3], n2[3];
+    mv(s1.R, L1.p, p1);
+    mv(s2.R, L2.p, p2);
+    mv(s1.R, L1.N, n1);
+    mv(s2.R, L2.N, n2);
+    const double d[3] = {p2[0] + s2.c[0] - p1[0] - s1.c[0], p2[1] + s2.c[1] - p1[1] - s1.c[1],
+                         p2[2] + s2.c[2] - p1[2] - s1.c[2]};
+    const double l1 = norm3(n1), l2 = norm3(n2);
+    for (int k = 0; k < 4; ++k) {
+        double dd[3], dn1[3] = {0, 0, 0}, dn2[3] = {0, 0, 0};
+        if (k < 2) {
+            double t[3];
+            mv(s1.R, k == 0 ? L1.pa : L1.pb, t);
+            for (int c = 0; c < 3; ++c) dd[c] = -t[c];
+            mv(s1.R, k == 0 ? L1.Na : L1.Nb, dn1);
+        } else {
+            mv(s2.R, k == 2 ? L2.pa : L2.pb, dd);
+            mv(s2.R, k == 2 ? L2.Na : L2.Nb, dn2);
+        }
+        double a[3], b[3];
+        cross(dd, n1, a);
+        cross(d, dn1, b);
+        J[0 + 4 * k] = a[0] + b[0];
+        J[1 + 4 * k] = a[1] + b[1];
+        J[2 + 4 * k] = a[2] + b[2];
+        J[3 + 4 * k] = dot3(dn1, n2) + dot3(n1, dn2) + dot3(n1, dn1) / l1 * l2 + l1 * dot3(n2, dn2) / l2;
+    }
+}
+
+// the hybrid method from the start, one row per thread, and the row's closest points; the
+// rows are handed out by a counter so that a lane takes the next row when its solve ends
+// (the evaluations per solve vary from a few to maxfev).  (One warp per row, with the 32
+// powers of an evaluation spread over the lanes, measured 5x slower: the hybrid method's
+// own scalar work, then done 32 times, outweighs the powers.)
+__global__ void __launch_bounds__(128, 3) k_se_solve(Bodies B, Contacts c, const Sizes* sizes, const double* u0,
+                                                    int* next) {
+    const int C = sizes->C, C_obs = sizes->C_obs;
+    for (;;) {
+        const int k = C_obs + atomicAdd(next, 1);
+        if (k >= C) break;
+        const Body s1 = load(B, c.ci[k]), s2 = load(B, c.cj[k]);
+        double u[4];
+        for (int q = 0; q < 4; ++q) u[q] = u0[4 * (long long)k + q];
+        hybrj([&](const double* x, double* F) { sese_F(s1, s2, x, F); },
+              [&](const double* x, double* J) { sese_J(s1, s2, x, J); }, u);
+        double pi_[3], pj_[3], nij[3];
+        point(s1, u[0], u[1], pi_);
+        point(s2, u[2], u[3], pj_);
+        normal(s2, u[2], u[3], nij);
+        const double df[3] = {pi_[0] - pj_[0], pi_[1] - pj_[1], pi_[2] - pj_[2]};
+        c.dij[k] = sgn(dot3(df, nij)) * norm3(df);
+        for (int q = 0; q < 3; ++q) {
+            c.pi[3 * (long long)k + q] = pi_[q];
+            c.pj[3 * (long long)k + q] = pj_[q];
+            c.nij[3 * (long long)k + q] = nij[q];
+        }
     }
 }
 
@@ -595,16 +648,17 @@ __global__ void k_se_sizes(Sizes* sizes, const int* total) {
 
 }  // namespace
 
-size_t se_pairs_smem() { return sizeof(SeShared); }
-
-void launch_se_pairs(const Bodies& b, Contacts& c, const Sizes* sizes, int grid, cudaStream_t s) {
+void launch_se_pairs(const Bodies& b, Contacts& c, const Sizes* sizes, double* u0, int* counter, int grid,
+                     cudaStream_t s) {
     static bool configured = false;
     if (!configured) {
-        cudaFuncSetAttribute(k_se_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SeShared));
+        cudaFuncSetAttribute(k_se_start, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SeShared));
         configured = true;
     }
-    k_se_pairs<<<grid, kSeThreads, sizeof(SeShared), s>>>(b, c, sizes);
-    g_se_launches += 1;
+    k_se_start<<<grid, kSeThreads, sizeof(SeShared), s>>>(b, c, sizes, u0);
+    cudaMemsetAsync(counter, 0, sizeof(int), s);
+    k_se_solve<<<4 * kSMs, 128, 0, s>>>(b, c, sizes, u0, counter);
+    g_se_launches += 2;
 }
 
 void launch_se_filter(const Contacts& src, Contacts& dst, Sizes* sizes, double dmax, long long c_cap, int* keep,

@@ -88,30 +88,47 @@ __device__ __forceinline__ void normal(const Body& s, double a, double b, double
 struct Local {
     double p[3], pa[3], pb[3], N[3], Na[3], Nb[3];
 };
-__device__ __forceinline__ void local(const Body& s, double a, double b, Local& L) {
+// sign(t)|t|^k for t = cos or sin (given) and the derivative factors k |t|^(k-1)
+struct Pw {
+    double v, d;  // sign(t)|t|^k, k |t|^(k-1)
+};
+__device__ __forceinline__ Pw pw(double t, double k, bool deriv) {
+    const double at = fabs(t);
+    Pw r;
+    r.v = sgn(t) * pow(at, k);
+    r.d = deriv ? k * pow(at, k - 1) : 0.0;
+    return r;
+}
+// deriv = false: point and normal only (the residual); true: also their angle derivatives
+__device__ __forceinline__ void local(const Body& s, double a, double b, Local& L, bool deriv = true) {
     const double rx = s.r[0], ry = s.r[1], rz = s.r[2];
-    const double Ca = cpow(a, s.n), Sa = spow(a, s.n), Cb = cpow(b, s.e), Sb = spow(b, s.e);
-    const double dCa = dcpow(a, s.n), dSa = dspow(a, s.n), dCb = dcpow(b, s.e), dSb = dspow(b, s.e);
+    double sa, ca, sb, cb;
+    sincos(a, &sa, &ca);
+    sincos(b, &sb, &cb);
     const double n2 = 2 - s.n, e2 = 2 - s.e;
-    const double Ca2 = cpow(a, n2), Sa2 = spow(a, n2), Cb2 = cpow(b, e2), Sb2 = spow(b, e2);
-    const double dCa2 = dcpow(a, n2), dSa2 = dspow(a, n2), dCb2 = dcpow(b, e2), dSb2 = dspow(b, e2);
-    L.p[0] = rx * Ca * Cb;
-    L.p[1] = ry * Ca * Sb;
-    L.p[2] = rz * Sa;
-    L.pa[0] = rx * dCa * Cb;
-    L.pa[1] = ry * dCa * Sb;
+    const Pw Ca = pw(ca, s.n, deriv), Sa = pw(sa, s.n, deriv), Cb = pw(cb, s.e, deriv), Sb = pw(sb, s.e, deriv);
+    const Pw Ca2 = pw(ca, n2, deriv), Sa2 = pw(sa, n2, deriv), Cb2 = pw(cb, e2, deriv), Sb2 = pw(sb, e2, deriv);
+    L.p[0] = rx * Ca.v * Cb.v;
+    L.p[1] = ry * Ca.v * Sb.v;
+    L.p[2] = rz * Sa.v;
+    L.N[0] = ry * rz * Ca2.v * Cb2.v;
+    L.N[1] = rx * rz * Ca2.v * Sb2.v;
+    L.N[2] = rx * ry * Sa2.v;
+    if (!deriv) return;
+    // d/dx sign(cos x)|cos x|^k = -k sin x |cos x|^(k-1);  d/dx sign(sin x)|sin x|^k = k cos x |sin x|^(k-1)
+    const double dCa = -sa * Ca.d, dSa = ca * Sa.d, dCb = -sb * Cb.d, dSb = cb * Sb.d;
+    const double dCa2 = -sa * Ca2.d, dSa2 = ca * Sa2.d, dCb2 = -sb * Cb2.d, dSb2 = cb * Sb2.d;
+    L.pa[0] = rx * dCa * Cb.v;
+    L.pa[1] = ry * dCa * Sb.v;
     L.pa[2] = rz * dSa;
-    L.pb[0] = rx * Ca * dCb;
-    L.pb[1] = ry * Ca * dSb;
+    L.pb[0] = rx * Ca.v * dCb;
+    L.pb[1] = ry * Ca.v * dSb;
     L.pb[2] = 0.0;
-    L.N[0] = ry * rz * Ca2 * Cb2;
-    L.N[1] = rx * rz * Ca2 * Sb2;
-    L.N[2] = rx * ry * Sa2;
-    L.Na[0] = ry * rz * dCa2 * Cb2;
-    L.Na[1] = rx * rz * dCa2 * Sb2;
+    L.Na[0] = ry * rz * dCa2 * Cb2.v;
+    L.Na[1] = rx * rz * dCa2 * Sb2.v;
     L.Na[2] = rx * ry * dSa2;
-    L.Nb[0] = ry * rz * Ca2 * dCb2;
-    L.Nb[1] = rx * rz * Ca2 * dSb2;
+    L.Nb[0] = ry * rz * Ca2.v * dCb2;
+    L.Nb[1] = rx * rz * Ca2.v * dSb2;
     L.Nb[2] = 0.0;
 }
 

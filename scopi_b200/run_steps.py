@@ -13,12 +13,12 @@ from __future__ import annotations
 import argparse
 import json
 
-from . import FP64, MIXED, VISCOUS, NOFRICTION, ScopiBatch, ScopiSolver, configs
+from . import FP64, FRICTION, MIXED, NOFRICTION, VISCOUS, ScopiBatch, ScopiSolver, configs
 
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", default="spheres", choices=["spheres", "box", "disks", "piles"])
+    ap.add_argument("--workload", default="spheres", choices=["spheres", "box", "disks", "piles", "se"])
     ap.add_argument("--scenes", type=int, default=256)
     ap.add_argument("--vmax", type=float, default=0.0)
     ap.add_argument("--block-threads", type=int, default=0)
@@ -39,14 +39,21 @@ def main(argv=None):
             print(json.dumps({"step": k, "block_threads": b.block_threads(), **b.stats()}), flush=True)
         b.close()
         return
-    if a.workload == "spheres":
+    extra = {}
+    if a.workload == "se":
+        # superellipsoid pile with friction (configs.se_pile with `count` bodies)
+        pa, st = configs.se_pile(count=a.count), configs.SETTINGS["se_pile"]
+        extra = dict(mu=st["mu"], kd_tree_radius=configs.se_kd_radius(pa, st["dmax"]))
+    elif a.workload == "spheres":
         pa, st = configs.spheres_1m(side=a.side), configs.SETTINGS["spheres_1m"]
     elif a.workload == "box":
         pa, st = configs.box_3d(count=a.count), configs.SETTINGS["box_3d"]
     else:
         pa, st = configs.disks_2d(side=a.side if a.side != 100 else 32), configs.SETTINGS["disks_2d"]
-    s = ScopiSolver(pa, precision=FP64 if a.precision == "fp64" else MIXED,
-                    problem=VISCOUS if a.problem == "viscous" else NOFRICTION,
+    problem = VISCOUS if a.problem == "viscous" else NOFRICTION
+    if a.workload == "se":
+        problem = FRICTION
+    s = ScopiSolver(pa, precision=FP64 if a.precision == "fp64" else MIXED, problem=problem, **extra,
                     initial_step=a.initial_step, dmax=st["dmax"], tolerance=st["tolerance"], max_ite=st["max_ite"],
                     vap=st["vap"])
     for k in range(a.steps):
