@@ -159,11 +159,11 @@ def solver_kwargs():
     return dict(dmax=st["dmax"], tolerance=st["tolerance"], max_ite=st["max_ite"], vap=st["vap"]), st["dt"]
 
 
-def time_path(pa, precision, steps, warmup, ranks, sampler=None, **extra):
+def time_path(pa, precision, steps, warmup, ranks, sampler=None, solver=None, **extra):
     import torch
 
     from scopi_b200 import ScopiSolver
-    kw, dt = solver_kwargs()
+    kw, dt = solver if solver else solver_kwargs()
     s = ScopiSolver(pa, precision=precision, mixed_violation_tol=1e-6, device=ranks.local, **kw, **extra)
     s.step(dt, warmup)
     stream = torch.cuda.ExternalStream(s.stream_handle(), device=ranks.local)
@@ -251,7 +251,7 @@ TRAFFIC_FP32_PER_CONTACT_ITERATION = 123.06
 
 
 # ----------------------------------------------------------------------------- CPU legs
-def cpu_sample(pa, iterations_per_step, threads):
+def cpu_sample(pa, iterations_per_step, threads, solver=None, caps=(1, 3)):
     """Oracle (CPU restatement of the reference path) on the full workload.
 
     Two time steps from the same state with the APGD loop capped at 1 and at 3
@@ -260,15 +260,24 @@ def cpu_sample(pa, iterations_per_step, threads):
     1 / (t_fixed + t_per_iteration * iterations_per_step)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import py_oracle as orc
-    kw, dt = solver_kwargs()
+    kw, dt = solver if solver else solver_kwargs()
     out = {}
     t0 = time.perf_counter()
-    for cap in (1, 3):
+    for cap in caps:
         o = orc.OracleSolver(pa, **dict(kw, max_ite=cap, num_threads=threads))
         o.run(dt, 1)
         out[cap] = o.stats()
         del o
     wall = time.perf_counter() - t0
+    if len(caps) == 1:
+        # one capped step: the solve's time per iteration includes its set-up (an upper bound)
+        c = caps[0]
+        out[1] = out[3] = out[c]
+        t_iter = max(1e-9, out[c]["seconds_solve"] / max(1, out[c]["iterations"]))
+        t_fixed = out[c]["seconds_contacts"] + out[c]["seconds_other"]
+        est = 1.0 / (t_fixed + t_iter * iterations_per_step)
+        return {"value": est, "t_per_iteration_s": t_iter, "t_outside_apgd_s": t_fixed, "wall_s": wall,
+                "contacts": out[c]["contacts"], "iterations_timed": out[c]["iterations"]}
     d_it = max(1, out[3]["iterations"] - out[1]["iterations"])
     t_iter = max(1e-9, (out[3]["seconds_solve"] - out[1]["seconds_solve"]) / d_it)
     t_fixed = out[1]["seconds_contacts"] + out[1]["seconds_other"] + max(0.0, out[1]["seconds_solve"] - t_iter)
@@ -322,19 +331,23 @@ def main():
     ap.add_argument("--side", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
-    ap.add_argument("--workload", default="spheres_1m", choices=["spheres_1m", "piles"],
-                    help="spheres_1m: the headline line; piles: 256 pile scenes stepped as one batch")
+    ap.add_argument("--workload", default="spheres_1m", choices=["spheres_1m", "piles", "se_pile"],
+                    help="spheres_1m: the headline line; piles: 256 pile scenes stepped as one batch; "
+                         "se_pile: 50k superellipsoids with friction")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 0)
     if args.steps is None:
-        # the workloads' own run lengths: 100 steps (1M spheres), 1000 steps (piles)
-        args.steps = (100 if args.workload == "spheres_1m" else 1000) - args.warmup
+        # the workloads' own run lengths: 100 steps (1M spheres), 1000 steps (piles); the
+        # superellipsoid pile (300 steps, ~1 s each) is timed on 20
+        args.steps = {"spheres_1m": 100, "piles": 1000, "se_pile": 20 + args.warmup}[args.workload] - args.warmup
     ranks = Ranks(args.gpus)
     try:
         if args.impl == "reference":
             return reference_arm(args, ranks)
         if args.workload == "piles":
             return piles(args, ranks)
+        if args.workload == "se_pile":
+            return se_pile(args, ranks)
         return ours(args, ranks)
     finally:
         ranks.close()
@@ -417,6 +430,59 @@ def piles(args, ranks):
         "solver": {k: mixed[k] for k in ("violation_max", "longest_scene_iterations_mean", "contacts_mean",
                                         "converged_all", "block_threads")},
         "clocks": mixed["clocks"], "gpu_launches": mixed["launches"],
+    }
+    if ranks.rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def se_pile(args, ranks):
+    """50,000 3D superellipsoids (semi-axes U[0.004, 0.008], squareness U[0.6, 1.4], random
+    orientations) on a lattice above a floor, with friction (mu 0.3): the contact search
+    keeps the pairs whose bounding spheres come within dmax, each pair's closest points are
+    solved on the GPU (start grid + hybrid method), then the 6-dof friction problem."""
+    import torch
+    from scopi_b200 import FP64, FRICTION, MIXED, configs
+    from scopi_b200.build import build
+    build()
+    st = configs.SETTINGS["se_pile"]
+    pa = configs.se_pile(count=50_000)
+    kd = configs.se_kd_radius(pa, st["dmax"])
+    solver = (dict(dmax=st["dmax"], tolerance=st["tolerance"], max_ite=st["max_ite"], vap=st["vap"], mu=st["mu"],
+                   problem=FRICTION, kd_tree_radius=kd), st["dt"])
+    sampler = ClockSampler(ranks.local)
+    mixed = time_path(pa, MIXED, args.steps, args.warmup, ranks, sampler, solver=solver)
+    f64 = None if args.no_fp64 else time_path(pa, FP64, args.steps, args.warmup, ranks, solver=solver)
+    value = ranks.world * args.steps * 1000.0 / ranks.max(mixed["ms"])
+    per = mixed["per_step"]
+    cpu = None
+    if not args.no_cpu_baseline and ranks.rank == 0:
+        threads = os.cpu_count() or 1
+        its = statistics.mean(p["iterations"] for p in (f64["per_step"] if f64 else per))
+        r = cpu_sample(pa, its, threads, solver=solver, caps=(3,))
+        cpu = {"value": r["value"], "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": (f"oracle on one step of the 50k pile with APGD capped at 3 iterations ({r['wall_s']:.1f} s "
+                          f"wall; contacts and closest points {r['t_outside_apgd_s']:.1f} s); steps/s = "
+                          f"1/(t_outside_apgd + t_per_iteration * {its:.0f} FP64 iterations per step on the GPU)")}
+    line = {
+        "metric": "time steps/s, 50k superellipsoids with friction (mixed FP32-APGD + FP64 correction)",
+        "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ranks.max(mixed["ms"]) / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 APGD iterations, f64 closest points/correction/integration",
+        "data": "synthetic",
+        "config": {"workload": ("se_pile: 50,000 superellipsoids, semi-axes U[0.004,0.008], e, n U[0.6,1.4], random "
+                                "orientation, 37^3 lattice spacing 0.018 above a floor, gravity, Friction mu 0.3, "
+                                f"dmax 0.004, dt 5e-4, steps {args.warmup + 1}..{args.warmup + args.steps} timed"),
+                   "precision": "mixed", "parallelism": "single GPU"},
+        "fp64": ({"value": ranks.world * args.steps * 1000.0 / ranks.max(f64["ms"]), "unit": UNIT,
+                  "violation_max": max(p["violation"] for p in f64["per_step"]),
+                  "iterations_per_step": statistics.mean(p["iterations"] for p in f64["per_step"])} if f64 else None),
+        "solver": {"contacts": statistics.mean(p["contacts"] for p in per),
+                   "violation_max": max(p["violation"] for p in per),
+                   "fp32_iterations_per_step": statistics.mean(p["fp32_iterations"] for p in per),
+                   "corrections_per_step": statistics.mean(p["corrections"] for p in per),
+                   "converged_all": all(p["converged"] for p in per)},
+        "cpu_baseline": cpu, "clocks": mixed["clocks"], "gpu_launches": mixed["launches"],
     }
     if ranks.rank == 0:
         print(json.dumps(line), flush=True)
