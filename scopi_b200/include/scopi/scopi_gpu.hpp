@@ -110,6 +110,8 @@ struct object_base {
     int32_t shape = SCOPI_GPU_SPHERE;
     double radius_ = 0.0;
     double length_ = 0.0;
+    std::array<double, 3> axes_{0.0, 0.0, 0.0};  // superellipsoid semi-axes
+    std::array<double, 2> sq_{1.0, 1.0};         // superellipsoid squareness (e, n)
 };
 
 template <std::size_t dim, bool owner = true>
@@ -154,6 +156,29 @@ class segment : public object_base<dim> {
         this->length_ = std::sqrt(dx * dx + dy * dy);
         this->shape = SCOPI_GPU_SEGMENT;
     }
+};
+
+// superellipsoid<3>(pos, q, radius, squareness), superellipsoid.hpp:59-70 (3D)
+template <std::size_t dim, bool owner = true>
+class superellipsoid : public object_base<dim> {
+    static_assert(dim == 3, "superellipsoids are 3D objects here");
+
+  public:
+    superellipsoid(std::initializer_list<type::position_t<dim>> pos, std::initializer_list<type::quaternion_t> q,
+                   std::initializer_list<std::array<double, 3>> radius, std::initializer_list<std::array<double, 2>> sq) {
+        this->position = *pos.begin();
+        this->q = *q.begin();
+        this->axes_ = *radius.begin();
+        this->sq_ = *sq.begin();
+        this->radius_ = std::sqrt(this->axes_[0] * this->axes_[0] + this->axes_[1] * this->axes_[1] +
+                                  this->axes_[2] * this->axes_[2]);  // bounding radius
+        this->shape = SCOPI_GPU_SUPERELLIPSOID;
+    }
+    superellipsoid(std::initializer_list<type::position_t<dim>> pos, std::initializer_list<std::array<double, 3>> radius,
+                   std::initializer_list<std::array<double, 2>> sq)
+        : superellipsoid(pos, {quaternion(0.0)}, radius, sq) {}
+    const std::array<double, 3>& radius() const { return this->axes_; }
+    const std::array<double, 2>& squareness() const { return this->sq_; }
 };
 
 // ------------------------------------------------------------------ property
@@ -241,6 +266,8 @@ class scopi_container {
         m_m.push_back(p.mass());
         m_radius.push_back(s.radius_);
         m_length.push_back(s.length_);
+        for (double c : s.axes_) m_axes.push_back(c);
+        for (double c : s.sq_) m_sq.push_back(c);
     }
 
     std::size_t size() const { return m_shape.size(); }
@@ -279,7 +306,7 @@ class scopi_container {
 
     // C ABI view (host arrays owned by the container)
     scopi_gpu_particles abi() {
-        scopi_gpu_particles p;
+        scopi_gpu_particles p{};
         p.n = (int64_t)size();
         p.nb_inactive = (int64_t)m_nb_inactive;
         p.shape = m_shape.data();
@@ -294,6 +321,8 @@ class scopi_container {
         p.j = m_j.data();
         p.radius = m_radius.data();
         p.length = m_length.data();
+        p.axes = m_axes.data();
+        p.squareness = m_sq.data();
         return p;
     }
 
@@ -313,7 +342,7 @@ class scopi_container {
         }
     }
     std::vector<int32_t> m_shape;
-    std::vector<double> m_pos, m_q, m_v, m_w, m_vd, m_dw, m_f, m_m, m_j, m_radius, m_length;
+    std::vector<double> m_pos, m_q, m_v, m_w, m_vd, m_dw, m_f, m_m, m_j, m_radius, m_length, m_axes, m_sq;
     std::size_t m_nb_inactive = 0;
 };
 

@@ -44,3 +44,56 @@ def test_cpp_api_matches_reference_golden(exe, golden, mode, name):
             for a, b in zip(got[key], ref[key]):
                 worst = max(worst, abs(a - b))
     assert worst <= 1e-5, worst
+
+
+SE_SRC = os.path.join(ROOT, "tests", "cpp", "superellipsoids_dropin.cpp")
+
+
+def test_superellipsoid_header_compiles():
+    subprocess.run([GXX, "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", *INC, SE_SRC], check=True)
+
+
+@pytest.fixture(scope="module")
+def se_exe(tmp_path_factory):
+    from scopi_b200 import build
+    build.build()
+    out = str(tmp_path_factory.mktemp("cpp") / "superellipsoids")
+    lib = os.path.join(ROOT, "scopi_b200")
+    subprocess.run([GXX, "-O2", "-std=c++17", *INC, SE_SRC, "-L", lib, "-lscopi_gpu", f"-Wl,-rpath,{lib}", "-o", out],
+                   check=True)
+    return out
+
+
+def write_scene(path, pa, steps, dt, mu, dmax, kd, tol, max_ite):
+    with open(path, "w") as fh:
+        fh.write(f"{len(pa.shape)} {steps} {dt!r} {mu!r} {dmax!r} {kd!r} {tol!r} {max_ite}\n")
+        for b in range(len(pa.shape)):
+            vals = [int(pa.shape[b]), int(b >= pa.nb_inactive), *pa.pos[b], *pa.q[b], *pa.axes[b],
+                    *pa.squareness[b], pa.m[b], *pa.j[b], *pa.f[b], *pa.v[b]]
+            fh.write(" ".join(repr(float(x)) if not isinstance(x, int) else str(x) for x in vals) + "\n")
+
+
+@pytest.mark.gpu
+def test_cpp_superellipsoid_pile_matches_python_api_and_oracle(se_exe, tmp_path):
+    """The same pile through the C++ API, the Python API (same engine: bitwise equal) and
+    the oracle (same contacts; positions to the bound of the superellipsoid parity tests)."""
+    import numpy as np
+
+    from gpu_helpers import gpu_solver, oracle_solver, rel_err
+    from scopi_b200 import FRICTION, configs
+    pa = configs.se_pile(count=27, side=3, seed=4)
+    st = configs.SETTINGS["se_pile"]
+    kd = configs.se_kd_radius(pa, st["dmax"])
+    steps = 4
+    scene = str(tmp_path / "scene.txt")
+    write_scene(scene, pa, steps, st["dt"], st["mu"], st["dmax"], kd, st["tolerance"], st["max_ite"])
+    res = json.loads(subprocess.run([se_exe, scene], check=True, capture_output=True, text=True).stdout)
+    pos = np.array(res["positions"])
+    kw = dict(dmax=st["dmax"], tolerance=st["tolerance"], max_ite=st["max_ite"], vap=st["vap"], mu=st["mu"],
+              problem=FRICTION, kd_tree_radius=kd)
+    g = gpu_solver(configs.se_pile(count=27, side=3, seed=4), **kw).run(st["dt"], steps)
+    assert np.array_equal(pos, g.particles.pos)
+    o = oracle_solver(configs.se_pile(count=27, side=3, seed=4), **kw).run(st["dt"], steps)
+    oc = o.contacts()
+    assert [tuple(c) for c in res["contacts"]] == list(zip(oc["i"].tolist(), oc["j"].tolist()))
+    assert rel_err(pos, o.pa.pos) <= 2e-5
