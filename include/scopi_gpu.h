@@ -206,7 +206,7 @@ int32_t scopi_gpu_batch_set_block_threads(scopi_gpu_handle* h, int32_t threads);
    For callers that cannot allocate while they solve: a process whose device memory is
    owned by another allocator, or a latency-critical loop where cudaMalloc/cudaFree would
    synchronise the device.  Intermediate arrays live in a fixed device array inside this
-   library (about 3.5 MB, held by every GPU that loads the library until exit), so:
+   library (about 3.4 MB, held by every GPU that loads the library until exit), so:
      - limits: at most 16384 contacts and 8192 active bodies; larger sizes return
        SCOPI_GPU_EINVAL with a message in scopi_gpu_last_error(NULL);
      - the first call on a device looks up that array's device address (make that first

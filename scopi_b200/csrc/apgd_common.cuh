@@ -53,6 +53,60 @@ __device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int nbl
     return s_ok != 0;
 }
 
+// Grid barrier taken by ONE thread per block (the caller synchronises its block around
+// it).  bar[0] counts arrivals and only grows: it is a multiple of nblocks between
+// barriers (the host zeroes it before the launch), so an arrival's target is the next
+// multiple.  One atomic per block, then acquire loads.  A thread that waits longer than
+// kBarrierTimeoutNs sets the error flag bar[2]; every waiter sees the flag and returns
+// false, so the kernel ends with an error status instead of hanging.  Blocks must not mix
+// it with grid_barrier after their first call (grid_barrier resets bar[0]).
+__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ bool grid_arrive_wait(unsigned int* bar, unsigned int nblocks) {
+    volatile unsigned int* verr = bar + 2;
+    __threadfence();
+    const unsigned int old = atomicAdd(bar, 1u);
+    const unsigned int target = (old / nblocks + 1u) * nblocks;
+    unsigned int it = 0;
+    unsigned long long t0 = 0;
+    for (;;) {
+        if ((int)(ld_acquire_u32(bar) - target) >= 0) break;
+        if (*verr) return false;
+        if (((++it) & 1023u) == 0) {
+            const unsigned long long t = global_ns();
+            if (t0 == 0) {
+                t0 = t;
+            } else if (t - t0 > kBarrierTimeoutNs) {
+                atomicExch(bar + 2, 1u);
+                return false;
+            }
+        }
+        if (it > 32) __nanosleep(32);
+    }
+    __threadfence();
+    return *verr == 0u;
+}
+
+// Sum over the grid of per-block partials part[b*stride + k] (b < nb), computed by one
+// warp: lane l adds blocks l, l+32, ... in order, then a fixed shuffle tree.  Every block
+// gets the same bits.  The result is in lane 0.
+template <int NP>
+__device__ __forceinline__ void warp_grid_sum(const double* part, unsigned int nb, int stride, double* t) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 0; k < NP; ++k) t[k] = 0.0;
+    for (unsigned int b = lane; b < nb; b += 32)
+#pragma unroll
+        for (int k = 0; k < NP; ++k) t[k] += __ldcg(part + (size_t)b * stride + k);
+#pragma unroll
+    for (int k = 0; k < NP; ++k)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t[k] += __shfl_down_sync(0xffffffffu, t[k], o);
+}
+
 // Fixed-order sum of NP doubles over the block (up to 1024 threads); the result is
 // returned in every thread.
 template <int NP>

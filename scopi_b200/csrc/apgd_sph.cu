@@ -47,6 +47,36 @@ __device__ __forceinline__ void st4(dvec4* p, double x, double y, double z) {
 __device__ __forceinline__ int idx_of(float w) { return __float_as_int(w); }
 __device__ __forceinline__ int idx_of(double w) { return (int)__double_as_longlong(w); }
 
+// ---- asynchronous global -> shared copies (cp.async).  Each thread stages only the
+// records it consumes itself, so a stage needs no block barrier: cp.async.wait_group
+// makes the thread's own copies visible to it.  src-size 0 zero-fills the slot without
+// reading (tails past the end; the source pointer is then the array base).
+__device__ __forceinline__ unsigned sm_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void cp16(void* dst, const void* src, bool on) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sm_addr(dst)), "l"(src), "r"(on ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp8(void* dst, const void* src, bool on) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sm_addr(dst)), "l"(src), "r"(on ? 8 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp4(void* dst, const void* src, bool on) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sm_addr(dst)), "l"(src), "r"(on ? 4 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void cp_val(float* d, const float* s, bool on) { cp4(d, s, on); }
+__device__ __forceinline__ void cp_val(double* d, const double* s, bool on) { cp8(d, s, on); }
+__device__ __forceinline__ void cp_vec(float4* d, const float4* s, bool on) { cp16(d, s, on); }
+__device__ __forceinline__ void cp_vec(dvec4* d, const dvec4* s, bool on) {
+    cp16(d, s, on);
+    cp16(reinterpret_cast<double2*>(d) + 1, reinterpret_cast<const double2*>(s) + 1, on);
+}
+
 template <typename T>
 struct SphArgs {
     int nin, na;
@@ -56,7 +86,7 @@ struct SphArgs {
     const double* shift;
     const int* inc_ptr;
     const V4<T>* inc;
-    const double* invm;  // stride 4, component 0 = 1/m
+    const T* invm;  // 1/m per active body, contiguous
     T* lam0;
     T* lam1;
     T* lam2;
@@ -83,12 +113,11 @@ __device__ __forceinline__ T pick4(int k, T a, T b, T c, T d) {
     return k == 0 ? a : (k == 1 ? b : (k == 2 ? c : d));
 }
 
-// one multiplier of the contact pass
+// one multiplier of the contact pass (lm, lpm: its current and previous values)
 template <typename T>
-__device__ __forceinline__ void mult_update(const SphArgs<T>& A, long long m, T qy, T cc, const T* lam, const T* lprev,
-                                            T* lnew, T beta, bool use_prev, bool bt, double alpha, double* s) {
-    const T lm = lam[m];
-    const T y = use_prev ? lm + beta * (lm - lprev[m]) : lm;
+__device__ __forceinline__ void mult_update_v(const SphArgs<T>& A, long long m, T qy, T cc, T lm, T lpm, T* lnew,
+                                              T beta, bool use_prev, bool bt, double alpha, double* s) {
+    const T y = use_prev ? lm + beta * (lm - lpm) : lm;
     const T gm = qy + cc;
     T lp;
     if (A.shift) {
@@ -110,26 +139,60 @@ __device__ __forceinline__ void mult_update(const SphArgs<T>& A, long long m, T 
     s[5] += (double)gm * dll;
     s[6] += (double)lp * (double)lp;
 }
+template <typename T>
+__device__ __forceinline__ void mult_update(const SphArgs<T>& A, long long m, T qy, T cc, const T* lam, const T* lprev,
+                                            T* lnew, T beta, bool use_prev, bool bt, double alpha, double* s) {
+    mult_update_v<T>(A, m, qy, cc, lam[m], use_prev ? lprev[m] : (T)0, lnew, beta, use_prev, bt, alpha, s);
+}
 
 // Loop-carried scalars of the iteration (block-uniform) live in shared memory and are
 // updated by thread 0, so the registers go to the two passes.
 struct SphState {
     double alpha, lipsch, theta, beta, beta_n, theta1, Fy, last_step, lgood;
+    double tk[4];  // g.d, |d|^2, c.l+ and |l+|^2 of the candidate (contact pass sums)
     long long ite, nbt, nrs;
     int il, ip, in_, jL, jN, jY, jYN, parity, bt, use_prev, restart, done, conv, err;
 };
 
-// One block per SM: 1024 threads at 64 registers (FP32), 768 at 80 (FP64).  Fewer,
-// larger blocks cut the grid-barrier arrivals and the per-block partials that every
-// block re-reads after each barrier (148 instead of 592).
+// One block per SM: 1024 threads at 64 registers (FP32), 512 at 128 (FP64; measured at
+// 1M spheres: 115 us per iteration against 142 us with 768 threads, whose larger shared
+// memory stages leave too little L1 for the incidence records).  Fewer, larger blocks cut
+// the grid-barrier arrivals and the per-block partials read after each barrier.
+//
+// Both passes stream their per-item records through a GS-deep cp.async pipeline in
+// dynamic shared memory (the passes are separated by grid barriers, so they share it):
+//   contact pass, per contact : (ci, cj), (n, c), l, l_prev           -- 32 B (FP32), 56 B (FP64)
+//   particle pass, per body   : inc_ptr[p], inc_ptr[p+1], 1/m, u(l) and (FP32) u(y)
+// and the gathers that depend on a staged record (u(y) of the contact's bodies) are issued
+// one trip ahead.  The incidence records stay on plain loads: a body's records share L1
+// lines, which an L1-bypassing copy would fetch again from L2 for every record.
 template <typename T>
 struct SphOcc {
-    static constexpr int threads = sizeof(T) == 4 ? 1024 : 768;
+    static constexpr int threads = sizeof(T) == 4 ? 1024 : 512;
+    static constexpr int GS = 4;  // pipeline stages
+    static constexpr size_t contact_bytes = (size_t)GS * threads * (sizeof(int2) + sizeof(V4<T>) + 2 * sizeof(T));
+    static constexpr size_t particle_bytes =
+        (size_t)GS * threads * ((sizeof(T) == 4 ? 2 : 1) * sizeof(V4<T>) + sizeof(T) + 2 * sizeof(int));
+    static constexpr size_t smem = contact_bytes > particle_bytes ? contact_bytes : particle_bytes;
 };
 
 template <typename T, int DIM, int PROB>
 __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A) {
     __shared__ SphState S;
+    extern __shared__ __align__(32) unsigned char sph_dyn[];
+    constexpr int GS = SphOcc<T>::GS;
+    const int NT = blockDim.x, tid = threadIdx.x;
+    // contact-pass stages [GS][NT] of each field
+    V4<T>* s_nc = reinterpret_cast<V4<T>*>(sph_dyn);
+    int2* s_ij = reinterpret_cast<int2*>(s_nc + GS * NT);
+    T* s_l = reinterpret_cast<T*>(s_ij + GS * NT);
+    T* s_lp = s_l + GS * NT;
+    // particle-pass stages (same memory)
+    V4<T>* s_ul = reinterpret_cast<V4<T>*>(sph_dyn);
+    V4<T>* s_uy = s_ul + GS * NT;  // FP32 only
+    T* s_im = reinterpret_cast<T*>(s_ul + (sizeof(T) == 4 ? 2 : 1) * GS * NT);
+    int* s_p0 = reinterpret_cast<int*>(s_im + GS * NT);
+    int* s_p1 = s_p0 + GS * NT;
     if (threadIdx.x == 0) {
         S.alpha = A.alpha;
         S.lipsch = 1.0 / A.alpha;
@@ -192,7 +255,7 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
                 w1 += mu * e.y;
                 if (DIM == 3) w2 += mu * e.z;
             }
-            const double im = A.invm[4 * (long long)p];
+            const double im = (double)A.invm[p];
             wm[0] += im * ((double)w0 * w0 + (double)w1 * w1 + (double)w2 * w2);
         }
         block_sum<2>(wm);
@@ -231,53 +294,96 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
         {
             double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
             // ---- contact pass: g = dt^2 n.(u_i(y) - u_j(y)) + c, l+ = P(y - alpha g)
-            GRID_STRIDE(c, C) {
-                const int2 ij = A.cij[c];
-                const V4<T> nc = ld4(A.nc + c);
-                const bool ai = ij.x >= A.nin, aj = ij.y >= A.nin;
+            // Trip k of this thread handles contact c_k = base + k*S (the grid-stride order).
+            const long long S_ = (long long)gridDim.x * NT, base = (long long)blockIdx.x * NT + tid;
+            const long long ntrip = ((long long)C - (long long)blockIdx.x * NT + S_ - 1) / S_;
+            auto issue = [&](long long k) {
+                const int sl = (int)(k % GS) * NT + tid;
+                const long long c = base + k * S_;
+                const bool on = k < ntrip && c < C;
+                const long long cc = on ? c : 0;
+                cp_vec(s_nc + sl, A.nc + cc, on);
+                cp8(s_ij + sl, A.cij + cc, on);
+                cp_val(s_l + sl, lam + cc, on);
+                cp_val(s_lp + sl, lprev + cc, on && use_prev);
+                cp_commit();
+            };
+            // u(y) of the contact's two bodies (written by other blocks: L2 loads)
+            auto gather = [&](long long k, T* g) {
+                const int sl = (int)(k % GS) * NT + tid;
+                const int2 ij = s_ij[sl];
+                const bool on = k < ntrip && base + k * S_ < C;
                 V4<T> ui, uj;
-                if (ai) ui = ld4cg(uY + (ij.x - A.nin));
-                if (aj) uj = ld4cg(uY + (ij.y - A.nin));
-                T qy = 0;
-                if (ai) qy += nc.x * ui.x + nc.y * ui.y + (DIM == 3 ? nc.z * ui.z : (T)0);
-                if (aj) qy -= nc.x * uj.x + nc.y * uj.y + (DIM == 3 ? nc.z * uj.z : (T)0);
-                qy *= (T)A.dt2;
-                mult_update<T>(A, c, qy, nc.w, lam, lprev, lnew, beta, use_prev, bt, alpha, s);
-                if (PROB == kViscous) {
-                    const int sl = A.slot[c];
-                    if (sl >= 0) mult_update<T>(A, sl, -qy, -nc.w, lam, lprev, lnew, beta, use_prev, bt, alpha, s);
+                ui.x = ui.y = ui.z = uj.x = uj.y = uj.z = (T)0;
+                if (on && ij.x >= A.nin) ui = ld4cg(uY + (ij.x - A.nin));
+                if (on && ij.y >= A.nin) uj = ld4cg(uY + (ij.y - A.nin));
+                g[0] = ui.x; g[1] = ui.y; g[2] = ui.z;
+                g[3] = uj.x; g[4] = uj.y; g[5] = uj.z;
+            };
+#pragma unroll 1
+            for (int k = 0; k < GS - 1; ++k) issue(k);
+            cp_wait<GS - 2>();
+            // trip k computes with the gathers issued during trip k-1
+            T gc[6], gn[6];
+            gather(0, gc);
+#pragma unroll 1
+            for (long long k = 0; k < ntrip; ++k) {
+                issue(k + GS - 1);
+                cp_wait<GS - 2>();  // stage k+1 has landed
+                gather(k + 1, gn);
+                const long long c = base + k * S_;
+                if (c < C) {
+                    const int sl = (int)(k % GS) * NT + tid;
+                    const V4<T> nc = s_nc[sl];
+                    // bodies below nin (obstacles) gathered as zeros: same sum as skipping them
+                    T qy = 0;
+                    qy += nc.x * gc[0] + nc.y * gc[1] + (DIM == 3 ? nc.z * gc[2] : (T)0);
+                    qy -= nc.x * gc[3] + nc.y * gc[4] + (DIM == 3 ? nc.z * gc[5] : (T)0);
+                    qy *= (T)A.dt2;
+                    mult_update_v<T>(A, c, qy, nc.w, s_l[sl], s_lp[sl], lnew, beta, use_prev, bt, alpha, s);
+                    if (PROB == kViscous) {
+                        const int sv = A.slot[c];
+                        if (sv >= 0) mult_update<T>(A, sv, -qy, -nc.w, lam, lprev, lnew, beta, use_prev, bt, alpha, s);
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < 6; ++q) gc[q] = gn[q];
+            }
+            cp_wait<0>();
+            // block partials to thread 0, grid barrier and grid sum in warp 0 only
+            block_reduce_t0<8>(s);
+            if (tid < 32) {
+                bool ok = true;
+                if (tid == 0) {
+                    for (int k = 0; k < 8; ++k) part[blockIdx.x * 8 + k] = s[k];
+                    ok = grid_arrive_wait(A.bar, nb);
+                }
+                ok = __shfl_sync(0xffffffffu, ok, 0) != 0;
+                double t[8];
+                warp_grid_sum<8>(part, nb, 8, t);
+                if (tid == 0) {
+                    if (!ok) {
+                        S.err = 1;
+                        S.done = 1;
+                    }
+                    // momentum for the next y if this candidate is accepted (apgd.hpp:196-206)
+                    const double th = S.theta;
+                    S.theta1 = 0.5 * (th * sqrt(4 + th * th) - th * th);
+                    S.restart = (A.dynamic && t[5] > 0) ? 1 : 0;
+                    S.beta_n = S.restart ? 0.0 : th * (1 - th) / (th * th + S.theta1);
+                    if (!bt) S.Fy = t[3];
+                    // the scalars the decision needs after the second pass
+                    S.last_step = t[4];
+                    S.tk[0] = t[0];
+                    S.tk[1] = t[1];
+                    S.tk[2] = t[2];
+                    S.tk[3] = t[6];
                 }
             }
-            block_sum<8>(s);
-            if (threadIdx.x == 0)
-                for (int k = 0; k < 8; ++k) part[blockIdx.x * 8 + k] = s[k];
         }
-        if (!grid_barrier(A.bar, nb)) {
-            if (threadIdx.x == 0) S.err = 1;
-            break;
-        }
+        __syncthreads();
+        if (S.err) break;
         {
-            double t[8];
-            grid_sum<8>(part, nb, 8, t);
-            if (threadIdx.x == 0) {
-                // momentum for the next y if this candidate is accepted (apgd.hpp:196-206)
-                const double th = S.theta;
-                S.theta1 = 0.5 * (th * sqrt(4 + th * th) - th * th);
-                S.restart = (A.dynamic && t[5] > 0) ? 1 : 0;
-                S.beta_n = S.restart ? 0.0 : th * (1 - th) / (th * th + S.theta1);
-                if (!bt) S.Fy = t[3];
-                // keep the scalars the decision needs after the second pass
-                S.last_step = t[4];
-            }
-            // t[0..2] and |l+|^2 for thread 0, which takes the decision after the second pass
-            __shared__ double tk[4];
-            if (threadIdx.x == 0) {
-                tk[0] = t[0];
-                tk[1] = t[1];
-                tk[2] = t[2];
-                tk[3] = t[6];
-            }
-            __syncthreads();
             // ---- particle pass: w = B^T l+, u = M^-1 w, u(next y)
             V4<T>* uL = pick4(S.jL, A.u0, A.u1, A.u2, A.u3);
             V4<T>* uN = pick4(S.jN, A.u0, A.u1, A.u2, A.u3);
@@ -287,9 +393,31 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
             // one body per thread; its incidence records, then the l+ gathers they index,
             // are issued in batches so several loads are in flight per thread
             constexpr int KB = 4;
-            GRID_STRIDE(p, A.na) {
+            const long long S_ = (long long)gridDim.x * NT, base = (long long)blockIdx.x * NT + tid;
+            const long long ntrip = ((long long)A.na - (long long)blockIdx.x * NT + S_ - 1) / S_;
+            auto issue = [&](long long k) {
+                const int sl = (int)(k % GS) * NT + tid;
+                const long long p = base + k * S_;
+                const bool on = k < ntrip && p < A.na;
+                const long long pp = on ? p : 0;
+                cp4(s_p0 + sl, A.inc_ptr + pp, on);
+                cp4(s_p1 + sl, A.inc_ptr + pp + 1, on);
+                cp_val(s_im + sl, A.invm + pp, on);
+                cp_vec(s_ul + sl, uL + pp, on && bn_ != (T)0);
+                if (sizeof(T) == 4) cp_vec(s_uy + sl, uY + pp, on);
+                cp_commit();
+            };
+#pragma unroll 1
+            for (int k = 0; k < GS - 1; ++k) issue(k);
+#pragma unroll 1
+            for (long long kt = 0; kt < ntrip; ++kt) {
+                issue(kt + GS - 1);
+                cp_wait<GS - 1>();  // stage kt has landed
+                const long long p = base + kt * S_;
+                if (p >= A.na) continue;
+                const int sl = (int)(kt % GS) * NT + tid;
                 T w0 = 0, w1 = 0, w2 = 0;
-                const int k0 = A.inc_ptr[p], k1 = A.inc_ptr[p + 1];
+                const int k0 = s_p0[sl], k1 = s_p1[sl];
                 for (int kb = k0; kb < k1; kb += KB) {
                     T ex[KB], ey[KB], ez[KB], mu[KB];
                     int ci[KB];
@@ -310,8 +438,8 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
                         if (ci[q] >= 0) {
                             mu[q] = __ldcg(lnew + ci[q]);
                             if (PROB == kViscous) {
-                                const int sl = A.slot[ci[q]];
-                                if (sl >= 0) mu[q] -= __ldcg(lnew + sl);
+                                const int sv = A.slot[ci[q]];
+                                if (sv >= 0) mu[q] -= __ldcg(lnew + sv);
                             }
                         }
 #pragma unroll
@@ -321,37 +449,43 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
                         if (DIM == 3) w2 += mu[q] * ez[q];
                     }
                 }
-                const T im = (T)A.invm[4 * (long long)p];
+                const T im = s_im[sl];
                 const T n0 = im * w0, n1 = im * w1, n2 = im * w2;
                 st4(uN + p, n0, n1, n2);
                 sw += (double)w0 * (double)n0 + (double)w1 * (double)n1 + (double)w2 * (double)n2;
                 if (sizeof(T) == 4) {
                     // m |u(l+) - u(y)|^2: the curvature d^T Q d / dt^2 along d = l+ - y
-                    const V4<T> uy = ld4cg(uY + p);
+                    const V4<T> uy = s_uy[sl];
                     const double d0 = (double)n0 - (double)uy.x, d1 = (double)n1 - (double)uy.y,
                                  d2 = (double)n2 - (double)uy.z;
                     sq += (d0 * d0 + d1 * d1 + d2 * d2) / (double)im;
                 }
                 if (bn_ != (T)0) {
-                    const V4<T> ul = ld4(uL + p);
+                    const V4<T> ul = s_ul[sl];
                     st4(uYN + p, n0 + bn_ * (n0 - ul.x), n1 + bn_ * (n1 - ul.y), n2 + bn_ * (n2 - ul.z));
                 } else {
                     st4(uYN + p, n0, n1, n2);
                 }
             }
+            cp_wait<0>();
             double sw8[2] = {sw, sq};
-            block_sum<2>(sw8);
-            if (threadIdx.x == 0) {
-                part2[blockIdx.x * 8] = sw8[0];
-                part2[blockIdx.x * 8 + 1] = sw8[1];
-            }
-            if (!grid_barrier(A.bar, nb)) {
-                if (threadIdx.x == 0) S.err = 1;
-                break;
-            }
+            block_reduce_t0<2>(sw8);
+            bool ok = true;
             double t6[2];
-            grid_sum<2>(part2, nb, 8, t6);
-            if (threadIdx.x == 0) {
+            if (tid < 32) {
+                if (tid == 0) {
+                    part2[blockIdx.x * 8] = sw8[0];
+                    part2[blockIdx.x * 8 + 1] = sw8[1];
+                    ok = grid_arrive_wait(A.bar, nb);
+                }
+                ok = __shfl_sync(0xffffffffu, ok, 0) != 0;
+                warp_grid_sum<2>(part2, nb, 8, t6);
+            }
+            if (tid == 0 && !ok) {
+                S.err = 1;
+                S.done = 1;
+            } else if (tid == 0) {
+                const double* tk = S.tk;
                 S.parity ^= 1;
                 const double F_lp = 0.5 * A.dt2 * t6[0] + tk[2];
                 bool accept = true;
@@ -506,9 +640,21 @@ int blocks(long long n) {
 }
 
 template <typename T, int DIM, int PROB>
+void set_sph_smem() {
+    static bool done = false;  // per instantiation; the attribute is per function and process
+    if (!done) {
+        cudaFuncSetAttribute(k_apgd_sph<T, DIM, PROB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)SphOcc<T>::smem);
+        done = true;
+    }
+}
+
+template <typename T, int DIM, int PROB>
 int max_blocks_sph() {
+    set_sph_smem<T, DIM, PROB>();
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_apgd_sph<T, DIM, PROB>, SphOcc<T>::threads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_apgd_sph<T, DIM, PROB>, SphOcc<T>::threads,
+                                                  SphOcc<T>::smem);
     int dev = 0, sms = kSMs;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -517,9 +663,11 @@ int max_blocks_sph() {
 
 template <typename T, int DIM, int PROB>
 cudaError_t launch_t(SphArgs<T>& A, int nblocks, cudaStream_t s) {
+    set_sph_smem<T, DIM, PROB>();
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(nblocks);
     cfg.blockDim = dim3(SphOcc<T>::threads);
+    cfg.dynamicSmemBytes = SphOcc<T>::smem;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;
@@ -642,7 +790,7 @@ void launch_sph_residual64(int nin, int dim, int problem, const int2* cij, const
 // synchronise the device and stall the other streams.  They pass inputs and outputs only.
 //
 // The array is a file-scope __device__ variable, so every GPU that loads this library
-// holds it (kNoAllocBytes, about 3.5 MB) until the process exits.  Its host-side name is
+// holds it (kNoAllocBytes, about 3.4 MB) until the process exits.  Its host-side name is
 // only a stand-in for the device address, so at set-up the device address is fetched once
 // per device with cudaGetSymbolAddress (with that device current) and passed to the
 // kernels.  All calls share the array and it keeps the last call's contents: each call
@@ -660,7 +808,7 @@ constexpr size_t kOffCij = 0;
 constexpr size_t kOffNc = align_up(kOffCij + sizeof(int2) * kNoAllocMaxContacts);
 constexpr size_t kOffInc = align_up(kOffNc + sizeof(dvec4) * kNoAllocMaxContacts);
 constexpr size_t kOffInvm = align_up(kOffInc + sizeof(dvec4) * 2 * kNoAllocMaxContacts);
-constexpr size_t kOffLam = align_up(kOffInvm + sizeof(double) * 4 * kNoAllocMaxBodies);
+constexpr size_t kOffLam = align_up(kOffInvm + sizeof(double) * kNoAllocMaxBodies);
 constexpr size_t kOffU = align_up(kOffLam + sizeof(double) * 3 * kNoAllocMaxContacts);
 constexpr size_t kOffPart = align_up(kOffU + sizeof(dvec4) * 4 * kNoAllocMaxBodies);
 constexpr size_t kOffBar = align_up(kOffPart + sizeof(double) * 4 * kNoAllocMaxBlocks * 8);
@@ -691,17 +839,14 @@ cudaError_t noalloc_scratch(unsigned char** out) {
     return cudaSuccess;
 }
 
-__global__ void k_noalloc_prepare(Sizes* sizes, int C, int na, const double* inv_mass, double* invm4) {
+__global__ void k_noalloc_prepare(Sizes* sizes, int C, int na, const double* inv_mass, double* invm) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         sizes->C = C;
         sizes->C_obs = 0;
         sizes->n_extra = 0;
         sizes->overflow = 0;
     }
-    GRID_STRIDE(p, na) {
-        invm4[4 * p] = inv_mass[p];
-        invm4[4 * p + 1] = invm4[4 * p + 2] = invm4[4 * p + 3] = 0.0;
-    }
+    GRID_STRIDE(p, na) { invm[p] = inv_mass[p]; }
 }
 
 __global__ void k_noalloc_pack_nc(const double* normal, const double* cvec, dvec4* nc, int C) {
@@ -777,7 +922,7 @@ extern "C" int32_t scopi_gpu_apgd_noalloc(int32_t dim, int64_t n_active, int64_t
     int2* cij = reinterpret_cast<int2*>(base + kOffCij);
     dvec4* nc = reinterpret_cast<dvec4*>(base + kOffNc);
     dvec4* inc = reinterpret_cast<dvec4*>(base + kOffInc);
-    double* invm4 = reinterpret_cast<double*>(base + kOffInvm);
+    double* invm = reinterpret_cast<double*>(base + kOffInvm);
     double* lam = reinterpret_cast<double*>(base + kOffLam);
     dvec4* ub = reinterpret_cast<dvec4*>(base + kOffU);
     double* part = reinterpret_cast<double*>(base + kOffPart);
@@ -790,7 +935,7 @@ extern "C" int32_t scopi_gpu_apgd_noalloc(int32_t dim, int64_t n_active, int64_t
     cudaMemsetAsync(ub + 2 * kNoAllocMaxBodies, 0, sizeof(dvec4) * kNoAllocMaxBodies, s);  // u(y)
     cudaMemsetAsync(bar, 0, 4 * sizeof(unsigned int), s);
     cudaMemsetAsync(res, 0, sizeof(ApgdResult), s);
-    k_noalloc_prepare<<<blocks(na), 256, 0, s>>>(sizes, C, na, inv_mass, invm4);
+    k_noalloc_prepare<<<blocks(na), 256, 0, s>>>(sizes, C, na, inv_mass, invm);
     launch_pack_cij(ci, cj, cij, sizes, C, s);
     k_noalloc_pack_nc<<<blocks(C), 256, 0, s>>>(normal, c, nc, C);
     launch_pack_inc<double>(na, inc_ptr, inc_idx, normal, inc, 2 * (long long)C, s);
@@ -803,7 +948,7 @@ extern "C" int32_t scopi_gpu_apgd_noalloc(int32_t dim, int64_t n_active, int64_t
     A.shift = nullptr;
     A.inc_ptr = inc_ptr;
     A.inc = inc;
-    A.invm = invm4;
+    A.invm = invm;
     A.lam0 = lam;
     A.lam1 = lam + kNoAllocMaxContacts;
     A.lam2 = lam + 2 * kNoAllocMaxContacts;

@@ -193,7 +193,7 @@ struct SphSolve {
     const double* shift;
     const int* inc_ptr;
     const V4<T>* inc;
-    const double* invm;       // stride 4, component 0 = 1/m
+    const T* invm;            // 1/m per active body, contiguous
     T* lam[3];
     V4<T>* u[4];
     double* partials;         // 4 * max_blocks * 8

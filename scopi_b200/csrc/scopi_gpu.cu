@@ -62,6 +62,8 @@ struct scopi_gpu_handle {
     bool has_se = false;                        // some active body is a superellipsoid
     double* d_invm64 = nullptr;
     float* d_invm32 = nullptr;
+    double* d_imt64 = nullptr;  // 1/m per active body, contiguous (torque-free kernel)
+    float* d_imt32 = nullptr;
     // per-particle solve buffers
     double* d_u64[3] = {nullptr, nullptr, nullptr};
     double* d_ufin = nullptr;
@@ -463,6 +465,7 @@ struct scopi_gpu_handle {
         A(d_shape, n) A(d_pos, 3 * (size_t)n) A(d_q, 4 * (size_t)n) A(d_v, 3 * (size_t)n) A(d_omega, 3 * (size_t)n)
         A(d_vd, 3 * (size_t)n) A(d_omega_d, 3 * (size_t)n) A(d_f, 3 * (size_t)n) A(d_m, n) A(d_j, 3 * (size_t)n)
         A(d_radius, n) A(d_length, n) A(d_axes, 3 * (size_t)n) A(d_sq, 2 * (size_t)n) A(d_invm64, 4 * (size_t)na + 4) A(d_invm32, 4 * (size_t)na + 4)
+        A(d_imt64, (size_t)na + 1) A(d_imt32, (size_t)na + 1)
         A(d_ufin, 6 * (size_t)na + 6)
         A(d_usfin, (size_t)na + 1)
         for (int k = 0; k < 4; ++k) {
@@ -674,7 +677,7 @@ struct scopi_gpu_handle {
     }
 
     template <typename T>
-    SphSolve<T> sph_buffers(const V4<T>* nc, const V4<T>* incv, T* const* lam, V4<T>* const* u) const {
+    SphSolve<T> sph_buffers(const V4<T>* nc, const V4<T>* incv, const T* imt, T* const* lam, V4<T>* const* u) const {
         SphSolve<T> sb{};
         sb.cij = d_cij;
         sb.nc = nc;
@@ -682,7 +685,7 @@ struct scopi_gpu_handle {
         sb.shift = nullptr;
         sb.inc_ptr = inc.ptr;
         sb.inc = incv;
-        sb.invm = d_invm64;
+        sb.invm = imt;
         for (int k = 0; k < 3; ++k) sb.lam[k] = lam[k];
         for (int k = 0; k < 4; ++k) sb.u[k] = u[k];
         sb.partials = d_partials;
@@ -721,7 +724,7 @@ struct scopi_gpu_handle {
             if (!mixed()) {
                 cudaEventRecord(ev_a[0], stream);
                 if (sphere_mode()) {
-                    SphSolve<double> sb = sph_buffers<double>(d_nc64, d_incv64, d_lam64, d_us64);
+                    SphSolve<double> sb = sph_buffers<double>(d_nc64, d_incv64, d_imt64, d_lam64, d_us64);
                     rc = run_apgd_sph<double>(sb, max_sph64, dt, P.tolerance, P.max_ite, M);
                     if (rc) return rc;
                     ufin = reinterpret_cast<const double*>(d_us64[h_result->u_buf]);
@@ -818,7 +821,7 @@ struct scopi_gpu_handle {
         if (sphere_mode()) {
             launch_pack_nc<float>(as.bn, as.cvec, d_nc32, d_sizes_cur, c_cap, stream);
             launch_pack_inc<float>(na, inc.ptr, inc.idx, as.bn, d_incv32, 2 * c_cap, stream);
-            sbs = sph_buffers<float>(d_nc32, d_incv32, d_lam32, d_us32);
+            sbs = sph_buffers<float>(d_nc32, d_incv32, d_imt32, d_lam32, d_us32);
         } else {
             launch_convert<double, float>(as.bn, d_bn32, 3 * c_cap, &d_sizes_cur->C, 3, stream);
             launch_convert<double, float>(as.bai, d_bai32, 3 * c_cap, &d_sizes_cur->C, 3, stream);
@@ -1075,8 +1078,16 @@ static int32_t upload_particles(scopi_gpu_handle* h, const scopi_gpu_particles* 
         }
         for (int d = 0; d < 4; ++d) im32[k + d] = (float)im64[k + d];
     }
+    std::vector<double> imt64((size_t)(n - nin) + 1, 0.0);
+    std::vector<float> imt32((size_t)(n - nin) + 1, 0.0f);
+    for (int i = nin; i < n; ++i) {
+        imt64[i - nin] = im64[4 * (size_t)(i - nin)];
+        imt32[i - nin] = (float)imt64[i - nin];
+    }
     cudaMemcpyAsync(h->d_invm64, im64.data(), im64.size() * sizeof(double), cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(h->d_invm32, im32.data(), im32.size() * sizeof(float), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(h->d_imt64, imt64.data(), imt64.size() * sizeof(double), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(h->d_imt32, imt32.data(), imt32.size() * sizeof(float), cudaMemcpyHostToDevice, s);
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return h->cuda_fail(e, "set_particles");
     return 0;
