@@ -65,11 +65,15 @@ __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
-__device__ __forceinline__ bool grid_arrive_wait(unsigned int* bar, unsigned int nblocks) {
-    volatile unsigned int* verr = bar + 2;
+// Split form: grid_arrive publishes this block's writes and returns the arrival target;
+// the block may do independent work before grid_wait.
+__device__ __forceinline__ unsigned int grid_arrive(unsigned int* bar, unsigned int nblocks) {
     __threadfence();
     const unsigned int old = atomicAdd(bar, 1u);
-    const unsigned int target = (old / nblocks + 1u) * nblocks;
+    return (old / nblocks + 1u) * nblocks;
+}
+__device__ __forceinline__ bool grid_wait(unsigned int* bar, unsigned int target) {
+    volatile unsigned int* verr = bar + 2;
     unsigned int it = 0;
     unsigned long long t0 = 0;
     for (;;) {
@@ -88,6 +92,9 @@ __device__ __forceinline__ bool grid_arrive_wait(unsigned int* bar, unsigned int
     }
     __threadfence();
     return *verr == 0u;
+}
+__device__ __forceinline__ bool grid_arrive_wait(unsigned int* bar, unsigned int nblocks) {
+    return grid_wait(bar, grid_arrive(bar, nblocks));
 }
 
 // Sum over the grid of per-block partials part[b*stride + k] (b < nb), computed by one

@@ -217,6 +217,34 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
     __syncthreads();
     const int C = A.sizes->C;
     const unsigned int nb = gridDim.x;
+    // Trip k of a thread handles item base + k*S (the grid-stride order) in both passes.
+    const long long S_ = (long long)gridDim.x * NT, base = (long long)blockIdx.x * NT + tid;
+    const long long ntrip_c = ((long long)C - (long long)blockIdx.x * NT + S_ - 1) / S_;
+    const long long ntrip_p = ((long long)A.na - (long long)blockIdx.x * NT + S_ - 1) / S_;
+    // First stages of each pass are issued before the grid barrier that precedes the pass
+    // when they do not depend on it: a contact's geometry (n, c), (ci, cj), and a body's
+    // inc_ptr, 1/m, u(l), u(y).  Uncommitted copies join the next commit group.
+    auto issue_geom = [&](long long k) {
+        const int sl = (int)(k % GS) * NT + tid;
+        const long long c = base + k * S_;
+        const bool on = k < ntrip_c && c < C;
+        const long long cc = on ? c : 0;
+        cp_vec(s_nc + sl, A.nc + cc, on);
+        cp8(s_ij + sl, A.cij + cc, on);
+    };
+    auto issue_body = [&](long long k, const V4<T>* uL, const V4<T>* uY, bool with_ul) {
+        const int sl = (int)(k % GS) * NT + tid;
+        const long long p = base + k * S_;
+        const bool on = k < ntrip_p && p < A.na;
+        const long long pp = on ? p : 0;
+        cp4(s_p0 + sl, A.inc_ptr + pp, on);
+        cp4(s_p1 + sl, A.inc_ptr + pp + 1, on);
+        cp_val(s_im + sl, A.invm + pp, on);
+        cp_vec(s_ul + sl, uL + pp, on && with_ul);
+        if (sizeof(T) == 4) cp_vec(s_uy + sl, uY + pp, on);
+        cp_commit();
+    };
+    bool geom_issued = false;
     if (A.curvature_start) {
         // initial step from the curvature along the first descent direction d (stored in
         // the candidate buffer, which the first contact pass overwrites); partial-sum
@@ -294,18 +322,18 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
         {
             double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
             // ---- contact pass: g = dt^2 n.(u_i(y) - u_j(y)) + c, l+ = P(y - alpha g)
-            // Trip k of this thread handles contact c_k = base + k*S (the grid-stride order).
-            const long long S_ = (long long)gridDim.x * NT, base = (long long)blockIdx.x * NT + tid;
-            const long long ntrip = ((long long)C - (long long)blockIdx.x * NT + S_ - 1) / S_;
-            auto issue = [&](long long k) {
+            const long long ntrip = ntrip_c;
+            auto issue_lam = [&](long long k) {
                 const int sl = (int)(k % GS) * NT + tid;
                 const long long c = base + k * S_;
                 const bool on = k < ntrip && c < C;
                 const long long cc = on ? c : 0;
-                cp_vec(s_nc + sl, A.nc + cc, on);
-                cp8(s_ij + sl, A.cij + cc, on);
                 cp_val(s_l + sl, lam + cc, on);
                 cp_val(s_lp + sl, lprev + cc, on && use_prev);
+            };
+            auto issue = [&](long long k) {
+                issue_geom(k);
+                issue_lam(k);
                 cp_commit();
             };
             // u(y) of the contact's two bodies (written by other blocks: L2 loads)
@@ -320,8 +348,18 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
                 g[0] = ui.x; g[1] = ui.y; g[2] = ui.z;
                 g[3] = uj.x; g[4] = uj.y; g[5] = uj.z;
             };
+            // prologue: the geometry of stages 0..GS-2 in one group (issued before the
+            // last barrier when geom_issued), then their multipliers one group per stage
+            if (!geom_issued)
 #pragma unroll 1
-            for (int k = 0; k < GS - 1; ++k) issue(k);
+                for (int k = 0; k < GS - 1; ++k) issue_geom(k);
+            cp_commit();
+            geom_issued = false;
+#pragma unroll 1
+            for (int k = 0; k < GS - 1; ++k) {
+                issue_lam(k);
+                cp_commit();
+            }
             cp_wait<GS - 2>();
             // trip k computes with the gathers issued during trip k-1
             T gc[6], gn[6];
@@ -352,12 +390,21 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
             cp_wait<0>();
             // block partials to thread 0, grid barrier and grid sum in warp 0 only
             block_reduce_t0<8>(s);
+            unsigned int target = 0;
+            if (tid == 0) {
+                for (int k = 0; k < 8; ++k) part[blockIdx.x * 8 + k] = s[k];
+                target = grid_arrive(A.bar, nb);
+            }
+            // every thread is past its contact loop: the particle pass's first stages fill
+            // the shared memory while the barrier waits (u(l) copied whatever beta is)
+            {
+                const V4<T>* uL0 = pick4(S.jL, A.u0, A.u1, A.u2, A.u3);
+#pragma unroll 1
+                for (int k = 0; k < GS - 1; ++k) issue_body(k, uL0, uY, true);
+            }
             if (tid < 32) {
                 bool ok = true;
-                if (tid == 0) {
-                    for (int k = 0; k < 8; ++k) part[blockIdx.x * 8 + k] = s[k];
-                    ok = grid_arrive_wait(A.bar, nb);
-                }
+                if (tid == 0) ok = grid_wait(A.bar, target);
                 ok = __shfl_sync(0xffffffffu, ok, 0) != 0;
                 double t[8];
                 warp_grid_sum<8>(part, nb, 8, t);
@@ -393,25 +440,11 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
             // one body per thread; its incidence records, then the l+ gathers they index,
             // are issued in batches so several loads are in flight per thread
             constexpr int KB = 4;
-            const long long S_ = (long long)gridDim.x * NT, base = (long long)blockIdx.x * NT + tid;
-            const long long ntrip = ((long long)A.na - (long long)blockIdx.x * NT + S_ - 1) / S_;
-            auto issue = [&](long long k) {
-                const int sl = (int)(k % GS) * NT + tid;
-                const long long p = base + k * S_;
-                const bool on = k < ntrip && p < A.na;
-                const long long pp = on ? p : 0;
-                cp4(s_p0 + sl, A.inc_ptr + pp, on);
-                cp4(s_p1 + sl, A.inc_ptr + pp + 1, on);
-                cp_val(s_im + sl, A.invm + pp, on);
-                cp_vec(s_ul + sl, uL + pp, on && bn_ != (T)0);
-                if (sizeof(T) == 4) cp_vec(s_uy + sl, uY + pp, on);
-                cp_commit();
-            };
-#pragma unroll 1
-            for (int k = 0; k < GS - 1; ++k) issue(k);
+            const long long ntrip = ntrip_p;
+            // stages 0..GS-2 were issued before the barrier
 #pragma unroll 1
             for (long long kt = 0; kt < ntrip; ++kt) {
-                issue(kt + GS - 1);
+                issue_body(kt + GS - 1, uL, uY, bn_ != (T)0);
                 cp_wait<GS - 1>();  // stage kt has landed
                 const long long p = base + kt * S_;
                 if (p >= A.na) continue;
@@ -470,14 +503,20 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
             cp_wait<0>();
             double sw8[2] = {sw, sq};
             block_reduce_t0<2>(sw8);
+            unsigned int target2 = 0;
+            if (tid == 0) {
+                part2[blockIdx.x * 8] = sw8[0];
+                part2[blockIdx.x * 8 + 1] = sw8[1];
+                target2 = grid_arrive(A.bar, nb);
+            }
+            // the next iteration's first contact geometry, while the barrier waits
+#pragma unroll 1
+            for (int k = 0; k < GS - 1; ++k) issue_geom(k);
+            geom_issued = true;
             bool ok = true;
             double t6[2];
             if (tid < 32) {
-                if (tid == 0) {
-                    part2[blockIdx.x * 8] = sw8[0];
-                    part2[blockIdx.x * 8 + 1] = sw8[1];
-                    ok = grid_arrive_wait(A.bar, nb);
-                }
+                if (tid == 0) ok = grid_wait(A.bar, target2);
                 ok = __shfl_sync(0xffffffffu, ok, 0) != 0;
                 warp_grid_sum<2>(part2, nb, 8, t6);
             }
@@ -538,6 +577,10 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
             if (S.done) break;
         }
     }
+    // copies issued for an iteration that did not run (wait_group does not cover
+    // uncommitted copies: commit them first)
+    cp_commit();
+    cp_wait<0>();
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         A.result->iterations = S.ite;
         A.result->backtracks = S.nbt;

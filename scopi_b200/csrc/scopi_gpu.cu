@@ -1001,6 +1001,40 @@ int32_t scopi_gpu_set_particles(scopi_gpu_handle* h, const scopi_gpu_particles* 
     return upload_particles(h, p, -1);
 }
 
+// M^-1 of the active bodies (minimization_problem.hpp:11-31): per body 4 slots, 1/m then
+// 1/J (3D: x, y, z; 2D: z in the last slot), in FP64 and rounded to FP32, and 1/m alone
+// contiguous for the torque-free kernel.
+__global__ void k_inverse_mass(int n, int nin, int dim, const double* m, const double* j, double* im64, float* im32,
+                               double* imt64, float* imt32) {
+    GRID_STRIDE(i, n - nin) {
+        const long long b = i + nin;
+        double v[4] = {1. / m[b], 0.0, 0.0, 0.0};
+        if (dim == 3) {
+            for (int d = 0; d < 3; ++d) v[1 + d] = 1. / j[3 * b + d];
+        } else {
+            v[3] = 1. / j[3 * b + 2];
+        }
+        for (int d = 0; d < 4; ++d) {
+            im64[4 * i + d] = v[d];
+            im32[4 * i + d] = (float)v[d];
+        }
+        imt64[i] = v[0];
+        imt32[i] = (float)v[0];
+    }
+}
+static void launch_inverse_mass(int n, int nin, int dim, const double* m, const double* j, double* im64, float* im32,
+                                double* imt64, float* imt32, cudaStream_t s) {
+    const long long na = (long long)n - nin;
+    // the padding slots past the last body stay zero
+    cudaMemsetAsync(im64 + 4 * na, 0, 4 * sizeof(double), s);
+    cudaMemsetAsync(im32 + 4 * na, 0, 4 * sizeof(float), s);
+    cudaMemsetAsync(imt64 + na, 0, sizeof(double), s);
+    cudaMemsetAsync(imt32 + na, 0, sizeof(float), s);
+    if (na <= 0) return;
+    const int blocks = (int)std::min<long long>((na + 255) / 256, 16LL * kSMs);
+    k_inverse_mass<<<blocks, 256, 0, s>>>(n, nin, dim, m, j, im64, im32, imt64, imt32);
+}
+
 static int32_t upload_particles(scopi_gpu_handle* h, const scopi_gpu_particles* p, long long obs_cap) {
     if (!h || !p || p->n < 0 || p->nb_inactive < 0 || p->nb_inactive > p->n || p->n >= (1LL << 30))
         return h ? h->fail(SCOPI_GPU_EINVAL, "invalid particle container") : SCOPI_GPU_EINVAL;
@@ -1062,32 +1096,12 @@ static int32_t upload_particles(scopi_gpu_handle* h, const scopi_gpu_particles* 
     up(h->d_j, p->j, 3 * (size_t)n * sizeof(double));
     up(h->d_radius, p->radius, (size_t)n * sizeof(double));
     up(h->d_length, p->length, (size_t)n * sizeof(double));
-    if (p->axes) up(h->d_axes, p->axes, 3 * (size_t)n * sizeof(double));
-    if (p->squareness) up(h->d_sq, p->squareness, 2 * (size_t)n * sizeof(double));
-    // M^-1 (minimization_problem.hpp:11-31): 1/m on the translational slots, 1/J on the
-    // rotational ones (2D: z only)
-    std::vector<double> im64(4 * (size_t)(n - nin) + 4, 0.0);
-    std::vector<float> im32(4 * (size_t)(n - nin) + 4, 0.0f);
-    for (int i = nin; i < n; ++i) {
-        const size_t k = 4 * (size_t)(i - nin);
-        im64[k] = 1. / p->m[i];
-        if (h->P.dim == 3) {
-            for (int d = 0; d < 3; ++d) im64[k + 1 + d] = 1. / p->j[3 * (size_t)i + d];
-        } else {
-            im64[k + 3] = 1. / p->j[3 * (size_t)i + 2];
-        }
-        for (int d = 0; d < 4; ++d) im32[k + d] = (float)im64[k + d];
+    // semi-axes and squareness are read for superellipsoid scenes only
+    if (n_se > 0) {
+        up(h->d_axes, p->axes, 3 * (size_t)n * sizeof(double));
+        up(h->d_sq, p->squareness, 2 * (size_t)n * sizeof(double));
     }
-    std::vector<double> imt64((size_t)(n - nin) + 1, 0.0);
-    std::vector<float> imt32((size_t)(n - nin) + 1, 0.0f);
-    for (int i = nin; i < n; ++i) {
-        imt64[i - nin] = im64[4 * (size_t)(i - nin)];
-        imt32[i - nin] = (float)imt64[i - nin];
-    }
-    cudaMemcpyAsync(h->d_invm64, im64.data(), im64.size() * sizeof(double), cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(h->d_invm32, im32.data(), im32.size() * sizeof(float), cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(h->d_imt64, imt64.data(), imt64.size() * sizeof(double), cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(h->d_imt32, imt32.data(), imt32.size() * sizeof(float), cudaMemcpyHostToDevice, s);
+    launch_inverse_mass(n, nin, h->P.dim, h->d_m, h->d_j, h->d_invm64, h->d_invm32, h->d_imt64, h->d_imt32, s);
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return h->cuda_fail(e, "set_particles");
     return 0;
