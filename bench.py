@@ -246,8 +246,9 @@ def measured_peaks():
 
 # DRAM bytes (read + write) per FP32 APGD iteration per contact of k_apgd_sph on the
 # 1M-sphere workload, from one ncu capture of a whole launch (19 iterations, the curvature
-# pre-pass included): 7.015 GB / (19 x 3,000,279) (profiles/apgd_sph_spheres_1m_traffic.md)
-TRAFFIC_FP32_PER_CONTACT_ITERATION = 123.06
+# pre-pass and one backtrack included): 6.274 GB / (19 x 3,001,248)
+# (profiles/apgd_sph_spheres_1m_ncu.md)
+TRAFFIC_FP32_PER_CONTACT_ITERATION = 110.0
 
 
 # ----------------------------------------------------------------------------- CPU legs
