@@ -56,7 +56,8 @@ extern "C" {
 #define SCOPI_GPU_SPHERE 0
 #define SCOPI_GPU_PLANE 1
 #define SCOPI_GPU_SEGMENT 2
-#define SCOPI_GPU_SUPERELLIPSOID 3  /* 3D, superellipsoid<3> (superellipsoid.hpp:59-70) */
+#define SCOPI_GPU_SUPERELLIPSOID 3  /* superellipsoid<dim> (superellipsoid.hpp:59-70); 2D scenes
+                                       of superellipsoids take no obstacles */
 
 typedef struct scopi_gpu_params {
     int32_t dim;              /* 2 or 3 */
@@ -103,10 +104,12 @@ typedef struct scopi_gpu_particles {
     double* f;           /* n*3 */
     double* m;           /* n */
     double* j;           /* n*3 */
-    double* radius;      /* n (sphere radius; superellipsoid: bounding radius |(rx, ry, rz)|) */
+    double* radius;      /* n (sphere radius; superellipsoid: bounding radius |semi-axes|) */
     double* length;      /* n (segment length) */
-    double* axes;        /* n*3 superellipsoid semi-axes (rx, ry, rz); NULL when there are none */
-    double* squareness;  /* n*2 superellipsoid squareness (e, n); NULL when there are none */
+    double* axes;        /* n*3 superellipsoid semi-axes (rx, ry, rz); 2D: (rx, ry, unused);
+                            NULL when there are none */
+    double* squareness;  /* n*2 superellipsoid squareness (e, n); 2D: (e, unused); NULL when
+                            there are none */
 } scopi_gpu_particles;
 
 typedef struct scopi_gpu_stats {

@@ -7,6 +7,7 @@ the C++17 restatement of the reference time step in scopi_oracle.cpp.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 
@@ -88,6 +89,11 @@ def lib():
         L.orc_se_plane_residual.argtypes = [P, P, P, P]
         L.orc_se_se_hybrid.restype = C.c_int
         L.orc_se_se_hybrid.argtypes = [P, P, P, C.POINTER(C.c_int)]
+        L.orc_se2_se2.restype = C.c_int
+        L.orc_se2_se2.argtypes = [P, P, P]
+        L.orc_se2_hybrid.restype = C.c_int
+        L.orc_se2_hybrid.argtypes = [P, P, P, C.POINTER(C.c_int)]
+        L.orc_se2_system.argtypes = [P, P, P, P, P]
         _lib = L
     return _lib
 
@@ -229,6 +235,42 @@ def se_se_system(s1, s2, u):
     uu = np.ascontiguousarray(u, float)
     lib().orc_se_se_system(_dp(a), _dp(b), _dp(uu), _dp(F), _dp(J))
     return F, J.reshape(4, 4).T.copy()
+
+
+def se2_record(c, angle, r, e):
+    """2D body record: centre (x, y), rotation angle about z, semi-axes (rx, ry), squareness e."""
+    q = [math.cos(angle / 2), 0.0, 0.0, math.sin(angle / 2)]
+    return se_record([c[0], c[1], 0.0], q, [r[0], r[1], 0.0], [e, 1.0])
+
+
+def se2_se2(s1, s2):
+    """closest_points(superellipsoid<2>, superellipsoid<2>) on two 2D body records."""
+    out = np.zeros(15)
+    a, b = np.ascontiguousarray(s1, float), np.ascontiguousarray(s2, float)
+    info = lib().orc_se2_se2(_dp(a), _dp(b), _dp(out))
+    r = _unpack(out)
+    r["info"] = info
+    r["u"] = r["u"][:2]
+    return r
+
+
+def se2_system(s1, s2, u):
+    """F (2) and the analytic Jacobian (2 x 2) of the 2D SE-SE system at u = (b1, b2)."""
+    F = np.zeros(2)
+    J = np.zeros(4)
+    a, b = np.ascontiguousarray(s1, float), np.ascontiguousarray(s2, float)
+    uu = np.ascontiguousarray(u, float)
+    lib().orc_se2_system(_dp(a), _dp(b), _dp(uu), _dp(F), _dp(J))
+    return F, J.reshape(2, 2).T.copy()
+
+
+def hybrid_solve2(s1, s2, u0):
+    """The restated MINPACK hybrid method on the 2D SE-SE system from the start u0."""
+    u = np.ascontiguousarray(u0, float).copy()
+    nfev = C.c_int(0)
+    a, b = np.ascontiguousarray(s1, float), np.ascontiguousarray(s2, float)
+    info = lib().orc_se2_hybrid(_dp(a), _dp(b), _dp(u), C.byref(nfev))
+    return {"u": u, "info": info, "nfev": nfev.value}
 
 
 def hybrid_solve(s1, s2, u0):

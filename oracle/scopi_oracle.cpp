@@ -238,6 +238,13 @@ struct orc_solver {
             const double lim = radius[a] + radius[b] + p.dmax;
             if (!(lim > 0.0) || s2 > lim * lim * (1.0 + 1e-9)) return false;
             c = from_pair(orc_se::se_se(se_of(a), se_of(b)));
+        } else if (dim == 2 && sa == ORC_SUPERELLIPSOID && sb == ORC_SUPERELLIPSOID) {
+            // same bounding-sphere test as in 3D (radius = |semi-axes|)
+            double s2 = 0.0;
+            for (int k = 0; k < 2; ++k) s2 += (pos[a][k] - pos[b][k]) * (pos[a][k] - pos[b][k]);
+            const double lim = radius[a] + radius[b] + p.dmax;
+            if (!(lim > 0.0) || s2 > lim * lim * (1.0 + 1e-9)) return false;
+            c = from_pair(orc_se::se2_se2(se_of(a), se_of(b)));
         } else if (dim == 3 && sa == ORC_SUPERELLIPSOID && sb == ORC_PLANE) {
             c = from_pair(orc_se::se_plane(se_of(a), plane_of(b)));
         } else if (dim == 3 && sa == ORC_PLANE && sb == ORC_SUPERELLIPSOID) {  // closest_points.hpp:1761-1768
@@ -976,6 +983,26 @@ void orc_se_se_system(const double* s1, const double* s2, const double* u, doubl
     const orc_se::SE a = se_from(s1), b = se_from(s2);
     orc_se::sese_F(a, b, u, F);
     orc_se::sese_J(a, b, u, J);
+}
+
+int orc_se2_se2(const double* s1, const double* s2, double* out) {
+    const orc_se::PairOut o = orc_se::se2_se2(se_from(s1), se_from(s2));
+    write_pair(o, out);
+    return o.info;
+}
+
+int orc_se2_hybrid(const double* s1, const double* s2, double* u, int* nfev) {
+    const orc_se::SE a = se_from(s1), b = se_from(s2);
+    const orc_se::HybrResult h = orc_se::hybrj<2>([&](const double* x, double* F) { orc_se::se2_F(a, b, x, F); },
+                                                  [&](const double* x, double* J) { orc_se::se2_J(a, b, x, J); }, u);
+    if (nfev) *nfev = h.nfev;
+    return h.info;
+}
+
+void orc_se2_system(const double* s1, const double* s2, const double* u, double* F, double* J) {
+    const orc_se::SE a = se_from(s1), b = se_from(s2);
+    orc_se::se2_F(a, b, u, F);
+    orc_se::se2_J(a, b, u, J);
 }
 
 }  // extern "C"

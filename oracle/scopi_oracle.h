@@ -122,6 +122,11 @@ int orc_se_se_hybrid(const double* s1, const double* s2, double* u, int* nfev);
    the SE-plane residual (with the body's side as its sign) at u = (a, b, plane coords). */
 void orc_se_plane_residual(const double* s, const double* plane, const double* u, double* F);
 void orc_se_se_system(const double* s1, const double* s2, const double* u, double* F, double* J);
+/* 2D: closest_points(superellipsoid<2>, superellipsoid<2>) on the same body records (c[0..1],
+   rotation about z, r[0..1], e); u = (b1, b2); F (2), J (2x2 column-major). */
+int orc_se2_se2(const double* s1, const double* s2, double* out);
+int orc_se2_hybrid(const double* s1, const double* s2, double* u, int* nfev);
+void orc_se2_system(const double* s1, const double* s2, const double* u, double* F, double* J);
 /* A.u and A^T.f on the current contact list (3C and 6*na long vectors). */
 int orc_amat(const orc_solver* s, const double* u, double* out);
 int orc_atmat(const orc_solver* s, const double* f, double* out);

@@ -1,7 +1,12 @@
 // se_geometry.hpp -- superellipsoid closest points for the CPU oracle (test infrastructure:
 // only tests/, smoke() and bench.py's CPU legs use the oracle; never the product path).
 //
-// Restates, for 3D superellipsoids:
+// Restates, for 2D superellipsoids:
+//   superellipsoid::point(b) / normal(b)                  superellipsoid.hpp:282-289, 303-312
+//   closest_points(superellipsoid<2>, superellipsoid<2>)   closest_points.hpp:65-262
+//       (start = argmin over the two binit_xy(4) grids of |p1 - p2| + 2 (1 + n1.n2), then
+//        hybrd1 on F = [ (p2 - p1) x n1 ; n1.n2 + |n1||n2| ] (2 unknowns b1, b2))
+// and for 3D superellipsoids:
 //   superellipsoid::point / normal / binit_xy / ainit_yz
 //       include/scopi/objects/types/superellipsoid.hpp:282-325, 360-466
 //   closest_points(superellipsoid<3>, superellipsoid<3>)   closest_points.hpp:263-733
@@ -722,6 +727,110 @@ inline PairOut se_plane(const SE& s, const Plane& P) {
     o.u[1] = b;
     o.u[2] = P.R[0][1] * e[0] + P.R[1][1] * e[1] + P.R[2][1] * e[2];
     o.u[3] = P.R[0][2] * e[0] + P.R[1][2] * e[1] + P.R[2][2] * e[2];
+    return o;
+}
+
+// ------------------------------------------------------------- SE - SE (2D)
+// A 2D body uses c[0..1], the upper-left 2x2 block of R (a rotation about z), r[0..1], e.
+struct Local2 {
+    double p[2], N[2], pb[2], Nb[2];  // body-frame point, unnormalised normal, d/db
+};
+inline Local2 local2(const SE& s, double b) {
+    const double cb = std::cos(b), sb = std::sin(b), e = s.e, k = 2 - s.e;
+    Local2 L;
+    L.p[0] = s.r[0] * sgn(cb) * std::pow(std::abs(cb), e);
+    L.p[1] = s.r[1] * sgn(sb) * std::pow(std::abs(sb), e);
+    L.N[0] = s.r[1] * sgn(cb) * std::pow(std::abs(cb), k);
+    L.N[1] = s.r[0] * sgn(sb) * std::pow(std::abs(sb), k);
+    // d/db sign(cos b)|cos b|^m = -m sin b |cos b|^(m-1);  d/db sign(sin b)|sin b|^m = m cos b |sin b|^(m-1)
+    L.pb[0] = -s.r[0] * e * sb * std::pow(std::abs(cb), e - 1);
+    L.pb[1] = s.r[1] * e * cb * std::pow(std::abs(sb), e - 1);
+    L.Nb[0] = -s.r[1] * k * sb * std::pow(std::abs(cb), k - 1);
+    L.Nb[1] = s.r[0] * k * cb * std::pow(std::abs(sb), k - 1);
+    return L;
+}
+inline void mv2(const SE& s, const double* x, double* y) {
+    y[0] = s.R[0][0] * x[0] + s.R[0][1] * x[1];
+    y[1] = s.R[1][0] * x[0] + s.R[1][1] * x[1];
+}
+inline V3 point2(const SE& s, double b) {
+    const Local2 L = local2(s, b);
+    double w[2];
+    mv2(s, L.p, w);
+    return {w[0] + s.c[0], w[1] + s.c[1], 0.0};
+}
+inline V3 normal2(const SE& s, double b) {
+    const Local2 L = local2(s, b);
+    double w[2];
+    mv2(s, L.N, w);
+    const double l = std::sqrt(w[0] * w[0] + w[1] * w[1]);
+    return {w[0] / l, w[1] / l, 0.0};
+}
+// F and its Jacobian (column-major 2x2) for u = (b1, b2)
+inline void se2_F(const SE& s1, const SE& s2, const double* u, double* F) {
+    const Local2 L1 = local2(s1, u[0]), L2 = local2(s2, u[1]);
+    double p1[2], p2[2], n1[2], n2[2];
+    mv2(s1, L1.p, p1);
+    mv2(s2, L2.p, p2);
+    mv2(s1, L1.N, n1);
+    mv2(s2, L2.N, n2);
+    const double d[2] = {p2[0] + s2.c[0] - p1[0] - s1.c[0], p2[1] + s2.c[1] - p1[1] - s1.c[1]};
+    F[0] = d[0] * n1[1] - d[1] * n1[0];
+    F[1] = n1[0] * n2[0] + n1[1] * n2[1] + std::sqrt(n1[0] * n1[0] + n1[1] * n1[1]) *
+                                               std::sqrt(n2[0] * n2[0] + n2[1] * n2[1]);
+}
+inline void se2_J(const SE& s1, const SE& s2, const double* u, double* J) {
+    const Local2 L1 = local2(s1, u[0]), L2 = local2(s2, u[1]);
+    double p1[2], p2[2], n1[2], n2[2], pb1[2], pb2[2], nb1[2], nb2[2];
+    mv2(s1, L1.p, p1);
+    mv2(s2, L2.p, p2);
+    mv2(s1, L1.N, n1);
+    mv2(s2, L2.N, n2);
+    mv2(s1, L1.pb, pb1);
+    mv2(s2, L2.pb, pb2);
+    mv2(s1, L1.Nb, nb1);
+    mv2(s2, L2.Nb, nb2);
+    const double d[2] = {p2[0] + s2.c[0] - p1[0] - s1.c[0], p2[1] + s2.c[1] - p1[1] - s1.c[1]};
+    const double l1 = std::sqrt(n1[0] * n1[0] + n1[1] * n1[1]), l2 = std::sqrt(n2[0] * n2[0] + n2[1] * n2[1]);
+    // column b1: d' = -p1', n1' = R1 Nb1, n2' = 0
+    J[0] = -pb1[0] * n1[1] + pb1[1] * n1[0] + d[0] * nb1[1] - d[1] * nb1[0];
+    J[1] = nb1[0] * n2[0] + nb1[1] * n2[1] + (n1[0] * nb1[0] + n1[1] * nb1[1]) / l1 * l2;
+    // column b2: d' = p2', n1' = 0, n2' = R2 Nb2
+    J[2] = pb2[0] * n1[1] - pb2[1] * n1[0];
+    J[3] = n1[0] * nb2[0] + n1[1] * nb2[1] + l1 * (n2[0] * nb2[0] + n2[1] * nb2[1]) / l2;
+}
+// closest_points(superellipsoid<2>, superellipsoid<2>), closest_points.hpp:65-262
+inline PairOut se2_se2(const SE& s1, const SE& s2) {
+    const int num = 4;
+    const auto g1 = sorted_unique(binit_xy(s1, num)), g2 = sorted_unique(binit_xy(s2, num));
+    double best = INFINITY;
+    double u[2] = {g1[0], g2[0]};
+    for (double b1 : g1) {
+        const V3 P1 = point2(s1, b1), N1 = normal2(s1, b1);
+        for (double b2 : g2) {
+            const V3 P2 = point2(s2, b2), N2 = normal2(s2, b2);
+            const double dx = P1[0] - P2[0], dy = P1[1] - P2[1];
+            const double v = std::sqrt(dx * dx + dy * dy) + 2 * (1 + (N1[0] * N2[0] + N1[1] * N2[1]));
+            if (v < best) {  // first minimum in row-major order
+                best = v;
+                u[0] = b1;
+                u[1] = b2;
+            }
+        }
+    }
+    const HybrResult h = hybrj<2>([&](const double* x, double* F) { se2_F(s1, s2, x, F); },
+                                  [&](const double* x, double* J) { se2_J(s1, s2, x, J); }, u);
+    PairOut o;
+    o.info = h.info;
+    o.nfev = h.nfev;
+    o.u[0] = u[0];
+    o.u[1] = u[1];
+    o.u[2] = o.u[3] = 0.0;
+    o.pi = point2(s1, u[0]);
+    o.pj = point2(s2, u[1]);
+    o.nij = normal2(s2, u[1]);
+    const double dx = o.pi[0] - o.pj[0], dy = o.pi[1] - o.pj[1];
+    o.dij = sgn(dx * o.nij[0] + dy * o.nij[1]) * std::sqrt(dx * dx + dy * dy);
     return o;
 }
 

@@ -136,14 +136,17 @@ class Particles:
         return self._push(SEGMENT, 0.5 * (p1 + p2), quaternion(ang), prop or Property().deactivate(), length=length)
 
     def add_superellipsoid(self, pos, radius, squareness, prop: Property | None = None, q=None):
-        """``superellipsoid<3>(pos, q, radius, squareness)`` (3D): semi-axes (rx, ry, rz) and
-        squareness (e, n).  ``radius`` of the body record holds the bounding radius
-        sqrt(rx^2 + ry^2 + rz^2) (the body lies in its axis box for e, n <= 2), which the
-        contact search uses; the closest points use the exact surface."""
-        if self.dim != 3:
-            raise ValueError("superellipsoids are 3D here")
-        r = np.asarray(radius, dtype=np.float64).reshape(3)
-        sq = np.asarray(squareness, dtype=np.float64).reshape(2)
+        """``superellipsoid<dim>(pos, q, radius, squareness)``: semi-axes (rx, ry, rz) and
+        squareness (e, n) in 3D, (rx, ry) and e in 2D (superellipsoid.hpp:59-70; stored as
+        (rx, ry, 0) and (e, 1)).  ``radius`` of the body record holds the bounding radius
+        |semi-axes| (the body lies in its axis box for squareness <= 2), which the contact
+        search uses; the closest points use the exact surface."""
+        if self.dim == 3:
+            r = np.asarray(radius, dtype=np.float64).reshape(3)
+            sq = np.asarray(squareness, dtype=np.float64).reshape(2)
+        else:
+            r = np.concatenate([np.asarray(radius, dtype=np.float64).reshape(2), [0.0]])
+            sq = np.array([float(np.asarray(squareness, dtype=np.float64).reshape(-1)[0]), 1.0])
         q = quaternion(0.0) if q is None else q
         return self._push(SUPERELLIPSOID, pos, q, prop or Property(), radius=float(np.sqrt(np.dot(r, r))), axes=r,
                           squareness=sq)

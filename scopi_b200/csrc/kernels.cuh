@@ -99,7 +99,7 @@ void launch_atmat(const Bodies& b, const StepParams& p, const Contacts& c, const
 // ----------------------------------------------------------------- se.cu
 long long se_launches();
 // closest points of the superellipsoid rows [C_obs, C) of c; u0: 4 doubles per row (scratch)
-void launch_se_pairs(const Bodies& b, Contacts& c, const Sizes* sizes, double* u0, int* counter, int grid,
+void launch_se_pairs(int dim, const Bodies& b, Contacts& c, const Sizes* sizes, double* u0, int* counter, int grid,
                      cudaStream_t s);
 // rows of src with dij < dmax (obstacle rows all kept) into dst, (i, j) order kept; sizes->C updated
 void launch_se_filter(const Contacts& src, Contacts& dst, Sizes* sizes, double dmax, long long c_cap, int* keep,

@@ -567,7 +567,7 @@ struct scopi_gpu_handle {
             // the search kept bounding-sphere candidates: closest points of the superellipsoid
             // pairs, then the rows with dij < dmax into the other list (no viscous gamma to
             // carry here), which becomes the current one
-            launch_se_pairs(b, cur, d_sizes_cur, d_se_u, dw.tmp_total + 3, 3 * kSMs, stream);
+            launch_se_pairs(P.dim, b, cur, d_sizes_cur, d_se_u, dw.tmp_total + 3, 3 * kSMs, stream);
             launch_se_filter(cur, old, d_sizes_cur, P.dmax, c_cap, d_se_keep, d_se_pos, dw.scan_work,
                              dw.tmp_total + 2, stream);
             std::swap(cur, old);
@@ -1056,16 +1056,18 @@ static int32_t upload_particles(scopi_gpu_handle* h, const scopi_gpu_particles* 
         if (i >= nin) (s == SCOPI_GPU_SUPERELLIPSOID ? n_se : n_sph)++;
     }
     if (n_se > 0) {
-        if (h->P.dim != 3) return h->fail(SCOPI_GPU_EUNSUPPORTED, "superellipsoids are 3D only");
+        if (h->P.dim == 2 && nin > 0)
+            return h->fail(SCOPI_GPU_EUNSUPPORTED, "2D superellipsoids: scenes without obstacles");
         if (n_sph > 0) return h->fail(SCOPI_GPU_EUNSUPPORTED, "spheres and superellipsoids cannot be mixed");
         if (!p->axes || !p->squareness) return h->fail(SCOPI_GPU_EINVAL, "superellipsoid axes / squareness missing");
         if (h->P.problem == SCOPI_GPU_VISCOUS)
             return h->fail(SCOPI_GPU_EUNSUPPORTED, "superellipsoids: NoFriction and Friction problems");
         if (h->batch) return h->fail(SCOPI_GPU_EUNSUPPORTED, "batches hold sphere scenes");
+        const bool d3 = h->P.dim == 3;  // 2D: (rx, ry) and e
         for (int i = nin; i < n; ++i) {
             const double* r = p->axes + 3 * (size_t)i;
             const double* q = p->squareness + 2 * (size_t)i;
-            if (!(r[0] > 0 && r[1] > 0 && r[2] > 0) || !(q[0] > 0 && q[0] < 2 && q[1] > 0 && q[1] < 2))
+            if (!(r[0] > 0 && r[1] > 0 && (!d3 || r[2] > 0)) || !(q[0] > 0 && q[0] < 2 && (!d3 || (q[1] > 0 && q[1] < 2))))
                 return h->fail(SCOPI_GPU_EINVAL, "superellipsoid: semi-axes > 0 and squareness in (0, 2)");
         }
     }

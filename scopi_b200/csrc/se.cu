@@ -1,4 +1,5 @@
-// se.cu -- closest points of pairs of 3D superellipsoids, one block per pair.
+// se.cu -- closest points of pairs of superellipsoids: 3D with one block per pair for the
+// start and one thread per pair for the solve, 2D with one thread per pair.
 //
 // closest_points(superellipsoid<3>, superellipsoid<3>), closest_points.hpp:263-733:
 //   start: the angle grids of both bodies (sorted unique binit_xy(6), ainit_yz(6) of
@@ -32,8 +33,7 @@ constexpr int kSeThreads = 256;
 constexpr int kSeGrid = 24;       // unique angles per grid axis at most (4 * 6)
 constexpr int kSeSamples = kSeGrid * kSeGrid;
 
-// ------------------------------------------------------- MINPACK pieces (n = 4)
-constexpr int N = 4;
+// ------------------------------------------------------- MINPACK pieces (n = N: 4 in 3D, 2 in 2D)
 constexpr double kEps = 2.220446049250313e-16;
 constexpr double kGiant = 1.7976931348623157e308;
 
@@ -69,6 +69,7 @@ __device__ double enorm(int n, const double* x) {
     return x3max * sqrt(s3);
 }
 
+template <int N>
 __device__ void qrfac(double* a, double* rdiag, double* acnorm) {
     for (int j = 0; j < N; ++j) {
         acnorm[j] = enorm(N, a + j * N);
@@ -91,6 +92,7 @@ __device__ void qrfac(double* a, double* rdiag, double* acnorm) {
     }
 }
 
+template <int N>
 __device__ void qform(double* q, double* wa) {
     for (int j = 1; j < N; ++j)
         for (int i = 0; i < j; ++i) q[i + j * N] = 0;
@@ -111,6 +113,7 @@ __device__ void qform(double* q, double* wa) {
     }
 }
 
+template <int N>
 __device__ void dogleg(const double* r, const double* diag, const double* qtb, double delta, double* x, double* wa1,
                        double* wa2) {
     int jj = (N * (N + 1)) / 2;
@@ -170,6 +173,7 @@ __device__ void dogleg(const double* r, const double* diag, const double* qtb, d
     for (int j = 0; j < N; ++j) x[j] = temp * wa1[j] + alpha * x[j];
 }
 
+template <int N>
 __device__ void r1updt(double* s, const double* u, double* v, double* w) {
     const int m = N;
     int jj = (N * (2 * m - N + 1)) / 2 - (m - N) - 1;
@@ -235,6 +239,7 @@ __device__ void r1updt(double* s, const double* u, double* v, double* w) {
     for (int i = N - 1; i < m; ++i) s[l++] = w[i];
 }
 
+template <int N>
 __device__ void r1mpyq(int m, double* a, int lda, const double* v, const double* w) {
     for (int nmj = 1; nmj <= N - 1; ++nmj) {
         const int j = N - 1 - nmj;
@@ -271,7 +276,7 @@ __device__ void r1mpyq(int m, double* a, int lda, const double* v, const double*
 
 // hybrd1 with the analytic Jacobian; returns info (1..5); at most maxfev evaluations of F.
 // fun(x, F) and jac(x, J) (column-major) evaluate the system.
-template <typename Fun, typename Jac>
+template <int N, typename Fun, typename Jac>
 __device__ int hybrj(Fun&& fun, Jac&& jac, double* x) {
     const double p1 = 0.1, p5 = 0.5, p001 = 1e-3, p0001 = 1e-4, xtol = 1e-10, factor = 100.0;
     const int maxfev = 200 * (N + 1);
@@ -285,7 +290,7 @@ __device__ int hybrj(Fun&& fun, Jac&& jac, double* x) {
     for (;;) {
         bool jeval = true;
         jac(x, fjac);
-        qrfac(fjac, wa1, wa2);
+        qrfac<N>(fjac, wa1, wa2);
         if (iter == 1) {
             for (int j = 0; j < N; ++j) wa3[j] = diag[j] * x[j];
             xnorm = enorm(N, wa3);
@@ -308,9 +313,9 @@ __device__ int hybrj(Fun&& fun, Jac&& jac, double* x) {
             }
             r[l] = wa1[j];
         }
-        qform(fjac, wa1);
+        qform<N>(fjac, wa1);
         for (;;) {
-            dogleg(r, diag, qtf, delta, wa1, wa2, wa3);
+            dogleg<N>(r, diag, qtf, delta, wa1, wa2, wa3);
             for (int j = 0; j < N; ++j) {
                 wa1[j] = -wa1[j];
                 wa2[j] = x[j] + wa1[j];
@@ -373,27 +378,36 @@ __device__ int hybrj(Fun&& fun, Jac&& jac, double* x) {
                 wa1[j] = diag[j] * ((diag[j] * wa1[j]) / pnorm);
                 if (ratio >= p0001) qtf[j] = sum;
             }
-            r1updt(r, wa1, wa2, wa3);
-            r1mpyq(N, fjac, N, wa2, wa3);
-            r1mpyq(1, qtf, 1, wa2, wa3);
+            r1updt<N>(r, wa1, wa2, wa3);
+            r1mpyq<N>(N, fjac, N, wa2, wa3);
+            r1mpyq<N>(1, qtf, 1, wa2, wa3);
             jeval = false;
         }
     }
 }
 
 // ------------------------------------------------------------- start grids
-// binit_xy(6) / ainit_yz(6) (superellipsoid.hpp:360-466): 4 angles per sample of [0, pi/2]
+// binit_xy(num) / ainit_yz(num) (superellipsoid.hpp:360-466): 4 angles per sample of
+// [0, pi/2] (num samples: 6 in 3D, 4 in 2D); value k of the list
+__device__ double binit_angle(const double* r, double e, int k, int num) {
+    const double pi = 3.14159265358979323846;
+    const int i = k >> 2, w = k & 3;
+    const double t = (0.5 * pi) * i / (num - 1);
+    const double x = r[0] * cos(t), y = r[1] * sin(t);
+    const double d = pow(pow(r[1] * x, 2.0 / e) + pow(r[0] * y, 2.0 / e), e / 2.0);
+    const double ys = y * r[0] * r[1] / d;
+    const double sb = fmax(-1.0, fmin(1.0, sqrt(pow(pow(ys / r[1], 2.0), 1.0 / e))));
+    const double v = asin(sb);
+    const double a = w == 0 ? v : (w == 1 ? v + pi / 2 : (w == 2 ? v - pi : v - pi / 2));
+    return fabs(a) < 1.0e-6 ? 0.01 : a;
+}
 __device__ double init_angle(const Body& s, int k, bool b_axis) {
     const double pi = 3.14159265358979323846;
     const int i = k >> 2, w = k & 3;
     const double t = (0.5 * pi) * i / 5;
     double v;
     if (b_axis) {
-        const double x = s.r[0] * cos(t), y = s.r[1] * sin(t);
-        const double d = pow(pow(s.r[1] * x, 2.0 / s.e) + pow(s.r[0] * y, 2.0 / s.e), s.e / 2.0);
-        const double ys = y * s.r[0] * s.r[1] / d;
-        const double sb = fmax(-1.0, fmin(1.0, sqrt(pow(pow(ys / s.r[1], 2.0), 1.0 / s.e))));
-        v = asin(sb);
+        return binit_angle(s.r, s.e, k, 6);
     } else {
         const double y = s.r[1] * cos(t), z = s.r[2] * sin(t);
         const double d = pow(pow(s.r[2] * y, 2.0 / s.n) + pow(s.r[1] * z, 2.0 / s.n), s.n / 2.0);
@@ -603,7 +617,7 @@ __global__ void __launch_bounds__(128, 3) k_se_solve(Bodies B, Contacts c, const
         const Body s1 = load(B, c.ci[k]), s2 = load(B, c.cj[k]);
         double u[4];
         for (int q = 0; q < 4; ++q) u[q] = u0[4 * (long long)k + q];
-        hybrj([&](const double* x, double* F) { sese_F(s1, s2, x, F); },
+        hybrj<4>([&](const double* x, double* F) { sese_F(s1, s2, x, F); },
               [&](const double* x, double* J) { sese_J(s1, s2, x, J); }, u);
         double pi_[3], pj_[3], nij[3];
         point(s1, u[0], u[1], pi_);
@@ -616,6 +630,93 @@ __global__ void __launch_bounds__(128, 3) k_se_solve(Bodies B, Contacts c, const
             c.pj[3 * (long long)k + q] = pj_[q];
             c.nij[3 * (long long)k + q] = nij[q];
         }
+    }
+}
+
+// ------------------------------------------------------- 2D pairs
+// closest_points(superellipsoid<2>, superellipsoid<2>), closest_points.hpp:65-262:
+// F = [ (p2 - p1) x n1 ; n1.n2 + |n1||n2| ] in the angles u = (b1, b2), n1, n2 unnormalised.
+__device__ void se2_F(const Body2& s1, const Body2& s2, const double* u, double* F) {
+    Local2 L1, L2;
+    local2(s1, u[0], L1, false);
+    local2(s2, u[1], L2, false);
+    double p1[2], p2[2], n1[2], n2[2];
+    mv2(s1.R, L1.p, p1);
+    mv2(s2.R, L2.p, p2);
+    mv2(s1.R, L1.N, n1);
+    mv2(s2.R, L2.N, n2);
+    const double d[2] = {p2[0] + s2.c[0] - p1[0] - s1.c[0], p2[1] + s2.c[1] - p1[1] - s1.c[1]};
+    F[0] = d[0] * n1[1] - d[1] * n1[0];
+    F[1] = n1[0] * n2[0] + n1[1] * n2[1] + sqrt(n1[0] * n1[0] + n1[1] * n1[1]) * sqrt(n2[0] * n2[0] + n2[1] * n2[1]);
+}
+__device__ void se2_J(const Body2& s1, const Body2& s2, const double* u, double* J) {
+    Local2 L1, L2;
+    local2(s1, u[0], L1);
+    local2(s2, u[1], L2);
+    double p1[2], p2[2], n1[2], n2[2], pb1[2], pb2[2], nb1[2], nb2[2];
+    mv2(s1.R, L1.p, p1);
+    mv2(s2.R, L2.p, p2);
+    mv2(s1.R, L1.N, n1);
+    mv2(s2.R, L2.N, n2);
+    mv2(s1.R, L1.pb, pb1);
+    mv2(s2.R, L2.pb, pb2);
+    mv2(s1.R, L1.Nb, nb1);
+    mv2(s2.R, L2.Nb, nb2);
+    const double d[2] = {p2[0] + s2.c[0] - p1[0] - s1.c[0], p2[1] + s2.c[1] - p1[1] - s1.c[1]};
+    const double l1 = sqrt(n1[0] * n1[0] + n1[1] * n1[1]), l2 = sqrt(n2[0] * n2[0] + n2[1] * n2[1]);
+    J[0] = -pb1[0] * n1[1] + pb1[1] * n1[0] + d[0] * nb1[1] - d[1] * nb1[0];
+    J[1] = nb1[0] * n2[0] + nb1[1] * n2[1] + (n1[0] * nb1[0] + n1[1] * nb1[1]) / l1 * l2;
+    J[2] = pb2[0] * n1[1] - pb2[1] * n1[0];
+    J[3] = n1[0] * nb2[0] + n1[1] * nb2[1] + l1 * (n2[0] * nb2[0] + n2[1] * nb2[1]) / l2;
+}
+
+// One thread per row: the start grids (sorted unique binit_xy(4) of both bodies, at most
+// 16 angles each), the first minimum of |p1 - p2| + 2 (1 + n1.n2) in row-major order, the
+// hybrid method in 2 unknowns and the row's closest points (z = 0).
+__global__ void __launch_bounds__(128) k_se2_pairs(Bodies B, Contacts c, const Sizes* sizes) {
+    constexpr int kNum = 4, kG = 4 * kNum;
+    const int C = sizes->C, C_obs = sizes->C_obs;
+    for (long long k = C_obs + (long long)blockIdx.x * blockDim.x + threadIdx.x; k < C;
+         k += (long long)gridDim.x * blockDim.x) {
+        const Body2 s1 = load2(B, c.ci[k]), s2 = load2(B, c.cj[k]);
+        double g1[kG], g2[kG];
+        for (int m = 0; m < kG; ++m) {
+            g1[m] = binit_angle(s1.r, s1.e, m, kNum);
+            g2[m] = binit_angle(s2.r, s2.e, m, kNum);
+        }
+        const int n1 = sort_unique(g1, kG), n2 = sort_unique(g2, kG);
+        double best = INFINITY, u[2] = {g1[0], g2[0]};
+        for (int i = 0; i < n1; ++i) {
+            double P1[2], N1[2];
+            point2(s1, g1[i], P1);
+            normal2(s1, g1[i], N1);
+            for (int j = 0; j < n2; ++j) {
+                double P2[2], N2[2];
+                point2(s2, g2[j], P2);
+                normal2(s2, g2[j], N2);
+                const double dx = P1[0] - P2[0], dy = P1[1] - P2[1];
+                const double v = sqrt(dx * dx + dy * dy) + 2 * (1 + (N1[0] * N2[0] + N1[1] * N2[1]));
+                if (v < best) {
+                    best = v;
+                    u[0] = g1[i];
+                    u[1] = g2[j];
+                }
+            }
+        }
+        hybrj<2>([&](const double* x, double* F) { se2_F(s1, s2, x, F); },
+                 [&](const double* x, double* J) { se2_J(s1, s2, x, J); }, u);
+        double pi_[2], pj_[2], nij[2];
+        point2(s1, u[0], pi_);
+        point2(s2, u[1], pj_);
+        normal2(s2, u[1], nij);
+        const double dx = pi_[0] - pj_[0], dy = pi_[1] - pj_[1];
+        c.dij[k] = sgn(dx * nij[0] + dy * nij[1]) * sqrt(dx * dx + dy * dy);
+        for (int q = 0; q < 2; ++q) {
+            c.pi[3 * k + q] = pi_[q];
+            c.pj[3 * k + q] = pj_[q];
+            c.nij[3 * k + q] = nij[q];
+        }
+        c.pi[3 * k + 2] = c.pj[3 * k + 2] = c.nij[3 * k + 2] = 0.0;
     }
 }
 
@@ -648,8 +749,13 @@ __global__ void k_se_sizes(Sizes* sizes, const int* total) {
 
 }  // namespace
 
-void launch_se_pairs(const Bodies& b, Contacts& c, const Sizes* sizes, double* u0, int* counter, int grid,
+void launch_se_pairs(int dim, const Bodies& b, Contacts& c, const Sizes* sizes, double* u0, int* counter, int grid,
                      cudaStream_t s) {
+    if (dim == 2) {
+        k_se2_pairs<<<4 * kSMs, 128, 0, s>>>(b, c, sizes);
+        g_se_launches += 1;
+        return;
+    }
     static bool configured = false;
     if (!configured) {
         cudaFuncSetAttribute(k_se_start, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SeShared));

@@ -132,6 +132,67 @@ __device__ __forceinline__ void local(const Body& s, double a, double b, Local& 
     L.Nb[2] = 0.0;
 }
 
+// ---- 2D superellipsoids (superellipsoid.hpp:282-289, 303-312): p(b) = (rx C(b,e), ry S(b,e)),
+// N(b) = (ry C(b,2-e), rx S(b,2-e)); R is the upper-left 2x2 block of R(q) (row-major).
+struct Body2 {
+    double c[2];
+    double R[4];
+    double r[2];
+    double e;
+};
+__device__ __forceinline__ Body2 load2(const Bodies& B, int b) {
+    double R3[9];
+    rot(B.q + 4 * (long long)b, R3);
+    Body2 s;
+    s.c[0] = B.pos[3 * (long long)b];
+    s.c[1] = B.pos[3 * (long long)b + 1];
+    s.R[0] = R3[0];
+    s.R[1] = R3[1];
+    s.R[2] = R3[3];
+    s.R[3] = R3[4];
+    s.r[0] = B.axes[3 * (long long)b];
+    s.r[1] = B.axes[3 * (long long)b + 1];
+    s.e = B.sq[2 * (long long)b];
+    return s;
+}
+__device__ __forceinline__ void mv2(const double* R, const double* x, double* y) {
+    y[0] = R[0] * x[0] + R[1] * x[1];
+    y[1] = R[2] * x[0] + R[3] * x[1];
+}
+struct Local2 {
+    double p[2], N[2], pb[2], Nb[2];
+};
+__device__ __forceinline__ void local2(const Body2& s, double b, Local2& L, bool deriv = true) {
+    double sb, cb;
+    sincos(b, &sb, &cb);
+    const double k = 2 - s.e;
+    const Pw C = pw(cb, s.e, deriv), S = pw(sb, s.e, deriv), C2 = pw(cb, k, deriv), S2 = pw(sb, k, deriv);
+    L.p[0] = s.r[0] * C.v;
+    L.p[1] = s.r[1] * S.v;
+    L.N[0] = s.r[1] * C2.v;
+    L.N[1] = s.r[0] * S2.v;
+    if (!deriv) return;
+    L.pb[0] = s.r[0] * (-sb * C.d);
+    L.pb[1] = s.r[1] * (cb * S.d);
+    L.Nb[0] = s.r[1] * (-sb * C2.d);
+    L.Nb[1] = s.r[0] * (cb * S2.d);
+}
+__device__ __forceinline__ void point2(const Body2& s, double b, double* w) {
+    Local2 L;
+    local2(s, b, L, false);
+    mv2(s.R, L.p, w);
+    w[0] += s.c[0];
+    w[1] += s.c[1];
+}
+__device__ __forceinline__ void normal2(const Body2& s, double b, double* w) {
+    Local2 L;
+    local2(s, b, L, false);
+    mv2(s.R, L.N, w);
+    const double l = sqrt(w[0] * w[0] + w[1] * w[1]);
+    w[0] /= l;
+    w[1] /= l;
+}
+
 // Closest points of a superellipsoid and a plane (the solution of the system of
 // closest_points.hpp:1479-1759 in closed form): the body point whose outward normal is
 // opposite to the plane normal oriented toward the body, and its projection on the plane.

@@ -21,6 +21,13 @@ FILES = [
     "two_spheres_symmetrical",      # test/test_sphere.cpp:382-421
     "2d_case_spheres",              # test/test_sphere.cpp:423-484
     "obstacles_sphere_sphere_moving",  # test/test_obstacles.cpp:214-250
+    # superellipsoids (2D); these snapshots use an older output format (no velocities,
+    # contacts without i, j and distance), written before the motion of their step
+    "two_ellipsoids_symmetrical",           # test/test_superellipsoid.cpp:451-491
+    "two_ellipsoids_spheres_symmetrical",   # test/test_superellipsoid.cpp:493-536
+    "two_ellipsoids_asymmetrical",          # test/test_superellipsoid.cpp:538-581
+    "two_ellipsoids_spheres_asymmetrical",  # test/test_superellipsoid.cpp:583-628
+    "2d_case_superellipsoid",               # test/test_superellipsoid.cpp:630-702
 ]
 
 
@@ -32,6 +39,10 @@ def main():
             d = json.load(fh)
         objs = []
         for o in d["objects"]:
+            if "properties" not in o:  # older format: geometry only
+                objs.append({"type": o["type"], "position": o["position"], "quaternion": o["quaternion"],
+                             "radius": o["radius"], "squareness": o["squareness"]})
+                continue
             p = o["properties"]
             om = p["omega"]
             objs.append({
@@ -44,7 +55,10 @@ def main():
             })
         contacts = []
         for c in d.get("contacts") or []:
-            contacts.append({k: c[k] for k in ("i", "j", "distance", "normal", "pi", "pj")})
+            if "nij" in c:  # older format
+                contacts.append({"normal": c["nij"], "pi": c["pi"], "pj": c["pj"]})
+            else:
+                contacts.append({k: c[k] for k in ("i", "j", "distance", "normal", "pi", "pj")})
         out[name] = {"objects": objs, "contacts": contacts}
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_states.json")
     with open(dst, "w") as fh:

@@ -235,3 +235,38 @@ def analytic_inclined(alpha, mu, t, r, g, y0):
 
 
 __all__ = ["quaternion"]
+
+
+def two_ellipsoids(semi_y: float, dy: float, total_it: int):
+    """test/test_superellipsoid.cpp:451-628: two 2D superellipsoids (e = 1) at (-0.2, -dy) and
+    (0.2, dy), rotated by +-pi/4, semi-axes (0.1, semi_y), desired velocities +-0.25, vap_fixed,
+    dt 0.005, default solver.  symmetrical: dy 0, 200 steps (semi_y 0.05) or 50 (semi_y 0.1);
+    asymmetrical: dy 0.05, 1000 steps."""
+    p = Particles(2)
+    p.add_superellipsoid((-0.2, -dy), (0.1, semi_y), 1.0,
+                         Property(mass=1.0, moment_inertia=0.1, desired_velocity=(0.25, 0)), q=quaternion(PI / 4))
+    p.add_superellipsoid((0.2, dy), (0.1, semi_y), 1.0,
+                         Property(mass=1.0, moment_inertia=0.1, desired_velocity=(-0.25, 0)), q=quaternion(-PI / 4))
+    return p.finalize(), dict(vap=VAP_FIXED, contact_method=KDTREE), 0.005, total_it
+
+
+def critical_2d_superellipsoids():
+    """test/test_superellipsoid.cpp:630-702: 18 2D superellipsoids (e = 1) from
+    std::minstd_rand0(123), dt 0.01, 20 steps, default solver."""
+    n = 3
+    g = MinstdRand0(123)
+    p = Particles(2)
+    for i in range(n):
+        for j in range(n):
+            for side in (0, 1):
+                rot = g.uniform(0.0, PI)
+                r = g.uniform(0.2, 0.4)
+                r2 = g.uniform(0.2, 0.4)
+                x = (side * n + i + 0.5) + g.uniform(-0.1, 0.1)
+                y = (j + 0.5) + g.uniform(-0.1, 0.1)
+                vel = g.uniform(2.0, 5.0)
+                p.add_superellipsoid((x, y), (r, r2), 1.0,
+                                     Property(mass=1.0, moment_inertia=0.1,
+                                              desired_velocity=(vel if side == 0 else -vel, 0.0)),
+                                     q=quaternion(rot))
+    return p.finalize(), dict(vap=VAP_FIXED, contact_method=KDTREE), 0.01, 20

@@ -128,3 +128,62 @@ def test_superellipsoid_pile_mixed_precision():
     mix = gpu_solver(pa, precision=MIXED, mixed_violation_tol=1e-6, **kw).run(st["dt"], 3)
     assert mix.stats()["violation"] <= 1e-6 or mix.stats()["contacts"] == 0
     assert rel_err(mix.particles.pos, f64.particles.pos) <= 1e-6
+
+
+# ------------------------------------------------------------------ 2D superellipsoids
+import scenes as S  # noqa: E402
+
+SE2_GOLDEN = [
+    ("two_ellipsoids_symmetrical", lambda: S.two_ellipsoids(0.05, 0.0, 200), 1e-6),
+    ("two_ellipsoids_spheres_symmetrical", lambda: S.two_ellipsoids(0.1, 0.0, 50), 1e-6),
+    ("two_ellipsoids_asymmetrical", lambda: S.two_ellipsoids(0.05, 0.05, 1000), 5e-6),
+    ("two_ellipsoids_spheres_asymmetrical", lambda: S.two_ellipsoids(0.1, 0.05, 1000), 1e-6),
+    ("2d_case_superellipsoid", S.critical_2d_superellipsoids, 1e-6),
+]
+
+
+@pytest.mark.parametrize("name,scene,tol", SE2_GOLDEN, ids=[c[0] for c in SE2_GOLDEN])
+def test_gpu_2d_superellipsoid_golden(golden, name, scene, tol):
+    """The reference's 2D superellipsoid snapshots (test/test_superellipsoid.cpp:451-702)
+    through the GPU path: state after total - 1 steps, then the contact points."""
+    pa, kw, dt, total = scene()
+    g = gpu_solver(pa, **kw)
+    g.run(dt, total - 1)
+    gold = golden[name]
+    for k, o in enumerate(gold["objects"]):
+        assert np.abs(g.particles.pos[k, :2] - o["position"]).max() <= tol, k
+        assert np.abs(g.particles.q[k] - o["quaternion"]).max() <= tol, k
+    c = g.detect()
+    assert len(c["i"]) == len(gold["contacts"])
+    for k, gc in enumerate(gold["contacts"]):
+        assert np.abs(c["nij"][k, :2] - gc["normal"]).max() <= tol
+        assert np.abs(c["pi"][k, :2] - gc["pi"]).max() <= tol
+        assert np.abs(c["pj"][k, :2] - gc["pj"]).max() <= tol
+
+
+def test_gpu_2d_superellipsoid_pairs_match_the_oracle():
+    rng = np.random.default_rng(21)
+    converged = agree = 0
+    for _ in range(60):
+        r1, r2 = rng.uniform(0.004, 0.008, 2), rng.uniform(0.004, 0.008, 2)
+        e1, e2 = rng.uniform(0.6, 1.4, 2)
+        a1, a2 = rng.uniform(0, 2 * math.pi, 2)
+        d = rng.normal(size=2)
+        d /= np.linalg.norm(d)
+        c2 = d * (np.linalg.norm(r1) + np.linalg.norm(r2)) * rng.uniform(0.55, 0.8)
+        p = Particles(2)
+        p.add_superellipsoid((0.0, 0.0), r1, e1, Property(mass=1.0, moment_inertia=1e-5), q=quaternion(a1))
+        p.add_superellipsoid(c2, r2, e2, Property(mass=1.0, moment_inertia=1e-5), q=quaternion(a2))
+        pa = p.finalize()
+        ref = orc.se2_se2(orc.se_record(pa.pos[0], pa.q[0], pa.axes[0], pa.squareness[0]),
+                          orc.se_record(pa.pos[1], pa.q[1], pa.axes[1], pa.squareness[1]))
+        c = gpu_solver(pa, dmax=0.05).detect()
+        assert list(c["i"]) == [0] and list(c["j"]) == [1]
+        if ref["info"] != 1:
+            continue
+        converged += 1
+        if (abs(c["dij"][0] - ref["dij"]) <= 1e-9 and np.allclose(c["pi"][0], ref["pi"], atol=1e-9)
+                and np.allclose(c["pj"][0], ref["pj"], atol=1e-9) and np.allclose(c["nij"][0], ref["nij"], atol=1e-9)):
+            agree += 1
+    assert converged >= 30
+    assert agree >= converged - 1, (agree, converged)

