@@ -158,27 +158,51 @@ class segment : public object_base<dim> {
     }
 };
 
-// superellipsoid<3>(pos, q, radius, squareness), superellipsoid.hpp:59-70 (3D)
+// superellipsoid<dim>(pos, q, radius, squareness), superellipsoid.hpp:59-70
 template <std::size_t dim, bool owner = true>
 class superellipsoid : public object_base<dim> {
-    static_assert(dim == 3, "superellipsoids are 3D objects here");
-
   public:
+    using radius_type = std::array<double, dim>;          // (rx, ry) / (rx, ry, rz)
+    using squareness_type = std::array<double, dim - 1>;  // e / (e, n)
     superellipsoid(std::initializer_list<type::position_t<dim>> pos, std::initializer_list<type::quaternion_t> q,
-                   std::initializer_list<std::array<double, 3>> radius, std::initializer_list<std::array<double, 2>> sq) {
-        this->position = *pos.begin();
-        this->q = *q.begin();
-        this->axes_ = *radius.begin();
-        this->sq_ = *sq.begin();
-        this->radius_ = std::sqrt(this->axes_[0] * this->axes_[0] + this->axes_[1] * this->axes_[1] +
-                                  this->axes_[2] * this->axes_[2]);  // bounding radius
+                   std::initializer_list<radius_type> radius, std::initializer_list<squareness_type> sq) {
+        set(*pos.begin(), *q.begin(), *radius.begin(), *sq.begin());
+    }
+    // the reference's 2D demos and tests pass the squareness e as a number
+    superellipsoid(std::initializer_list<type::position_t<dim>> pos, std::initializer_list<type::quaternion_t> q,
+                   std::initializer_list<radius_type> radius, double e) {
+        squareness_type sq{};
+        sq.fill(e);
+        set(*pos.begin(), *q.begin(), *radius.begin(), sq);
+    }
+    superellipsoid(std::initializer_list<type::position_t<dim>> pos, std::initializer_list<radius_type> radius,
+                   std::initializer_list<squareness_type> sq)
+        : superellipsoid(pos, {quaternion(0.0)}, radius, sq) {}
+    std::array<double, dim> radius() const {
+        std::array<double, dim> r;
+        for (std::size_t d = 0; d < dim; ++d) r[d] = this->axes_[d];
+        return r;
+    }
+    std::array<double, dim - 1> squareness() const {
+        std::array<double, dim - 1> e;
+        for (std::size_t d = 0; d + 1 < dim; ++d) e[d] = this->sq_[d];
+        return e;
+    }
+
+  private:
+    void set(const type::position_t<dim>& pos, const type::quaternion_t& q, const radius_type& r,
+             const squareness_type& sq) {
+        this->position = pos;
+        this->q = q;
+        double b = 0.0;
+        for (std::size_t d = 0; d < dim; ++d) {
+            this->axes_[d] = r[d];
+            b += r[d] * r[d];
+        }
+        for (std::size_t d = 0; d + 1 < dim; ++d) this->sq_[d] = sq[d];
+        this->radius_ = std::sqrt(b);  // bounding radius
         this->shape = SCOPI_GPU_SUPERELLIPSOID;
     }
-    superellipsoid(std::initializer_list<type::position_t<dim>> pos, std::initializer_list<std::array<double, 3>> radius,
-                   std::initializer_list<std::array<double, 2>> sq)
-        : superellipsoid(pos, {quaternion(0.0)}, radius, sq) {}
-    const std::array<double, 3>& radius() const { return this->axes_; }
-    const std::array<double, 2>& squareness() const { return this->sq_; }
 };
 
 // ------------------------------------------------------------------ property

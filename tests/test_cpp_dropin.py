@@ -47,10 +47,41 @@ def test_cpp_api_matches_reference_golden(exe, golden, mode, name):
 
 
 SE_SRC = os.path.join(ROOT, "tests", "cpp", "superellipsoids_dropin.cpp")
+SE2_SRC = os.path.join(ROOT, "tests", "cpp", "two_ellipsoids_dropin.cpp")
 
 
-def test_superellipsoid_header_compiles():
-    subprocess.run([GXX, "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", *INC, SE_SRC], check=True)
+@pytest.mark.parametrize("src", [SE_SRC, SE2_SRC])
+def test_superellipsoid_header_compiles(src):
+    subprocess.run([GXX, "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", *INC, src], check=True)
+
+
+@pytest.fixture(scope="module")
+def se2_exe(tmp_path_factory):
+    from scopi_b200 import build
+    build.build()
+    out = str(tmp_path_factory.mktemp("cpp") / "two_ellipsoids")
+    lib = os.path.join(ROOT, "scopi_b200")
+    subprocess.run([GXX, "-O2", "-std=c++17", *INC, SE2_SRC, "-L", lib, "-lscopi_gpu", f"-Wl,-rpath,{lib}", "-o", out],
+                   check=True)
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode,tol", [("symmetrical", 1e-6), ("asymmetrical", 5e-6)])
+def test_cpp_two_ellipsoids_match_reference_golden(se2_exe, golden, mode, tol):
+    """test/test_superellipsoid.cpp:451-581 through the C++ API against two_ellipsoids_*.json."""
+    res = json.loads(subprocess.run([se2_exe, mode], check=True, capture_output=True, text=True).stdout)
+    gold = golden["two_ellipsoids_" + mode]
+    worst = 0.0
+    for got, ref in zip(res["objects"], gold["objects"]):
+        for key in ("position", "quaternion"):
+            worst = max(worst, max(abs(a - b) for a, b in zip(got[key], ref[key])))
+    assert len(res["contacts"]) == len(gold["contacts"])
+    for got, ref in zip(res["contacts"], gold["contacts"]):
+        worst = max(worst, max(abs(a - b) for a, b in zip(got["nij"], ref["normal"])))
+        for key in ("pi", "pj"):
+            worst = max(worst, max(abs(a - b) for a, b in zip(got[key], ref[key])))
+    assert worst <= tol, worst
 
 
 @pytest.fixture(scope="module")
