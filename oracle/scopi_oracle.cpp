@@ -237,6 +237,8 @@ struct orc_solver {
             for (int k = 0; k < 3; ++k) s2 += (pos[a][k] - pos[b][k]) * (pos[a][k] - pos[b][k]);
             const double lim = radius[a] + radius[b] + p.dmax;
             if (!(lim > 0.0) || s2 > lim * lim * (1.0 + 1e-9)) return false;
+            // nor when their gap along the line of centres exceeds dmax (convex bodies)
+            if (orc_se::support_gap(se_of(a), se_of(b), 3) > p.dmax + 1e-9 * lim) return false;
             c = from_pair(orc_se::se_se(se_of(a), se_of(b)));
         } else if (dim == 2 && sa == ORC_SUPERELLIPSOID && sb == ORC_SUPERELLIPSOID) {
             // same bounding-sphere test as in 3D (radius = |semi-axes|)
@@ -244,6 +246,7 @@ struct orc_solver {
             for (int k = 0; k < 2; ++k) s2 += (pos[a][k] - pos[b][k]) * (pos[a][k] - pos[b][k]);
             const double lim = radius[a] + radius[b] + p.dmax;
             if (!(lim > 0.0) || s2 > lim * lim * (1.0 + 1e-9)) return false;
+            if (orc_se::support_gap(se_of(a), se_of(b), 2) > p.dmax + 1e-9 * lim) return false;
             c = from_pair(orc_se::se2_se2(se_of(a), se_of(b)));
         } else if (dim == 3 && sa == ORC_SUPERELLIPSOID && sb == ORC_PLANE) {
             c = from_pair(orc_se::se_plane(se_of(a), plane_of(b)));

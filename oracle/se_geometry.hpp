@@ -730,6 +730,41 @@ inline PairOut se_plane(const SE& s, const Plane& P) {
     return o;
 }
 
+// ------------------------------------------------------------- separation bound
+// For convex bodies (squareness in (0, 2)) the distance is at least the gap along any unit
+// direction u: (support point of body 2 in -u - support point of body 1 in u).u.  With u
+// along the line of centres this bounds the pairs that cannot be in contact.
+inline double support_angle2(const SE& s, double m0, double m1) {
+    const double ke = 1.0 / (2 - s.e);
+    return std::atan2(sgn(m1) * std::pow(std::abs(s.r[1] * m1), ke), sgn(m0) * std::pow(std::abs(s.r[0] * m0), ke));
+}
+inline V3 point2(const SE& s, double b);
+inline double support_gap(const SE& s1, const SE& s2, int dim) {
+    V3 d = {s2.c[0] - s1.c[0], s2.c[1] - s1.c[1], dim == 3 ? s2.c[2] - s1.c[2] : 0.0};
+    const double l = norm(d);
+    if (!(l > 0)) return -INFINITY;
+    const V3 u = {d[0] / l, d[1] / l, d[2] / l};
+    // body-frame directions R^T u (body 1) and -R^T u (body 2)
+    V3 m1 = {0, 0, 0}, m2 = {0, 0, 0};
+    for (int k = 0; k < 3; ++k)
+        for (int r = 0; r < dim; ++r) {
+            m1[k] += s1.R[r][k] * u[r];
+            m2[k] -= s2.R[r][k] * u[r];
+        }
+    V3 p1, p2;
+    if (dim == 3) {
+        double a, b;
+        support_angles(s1, m1, a, b);
+        p1 = point(s1, a, b);
+        support_angles(s2, m2, a, b);
+        p2 = point(s2, a, b);
+    } else {
+        p1 = point2(s1, support_angle2(s1, m1[0], m1[1]));
+        p2 = point2(s2, support_angle2(s2, m2[0], m2[1]));
+    }
+    return (p2[0] - p1[0]) * u[0] + (p2[1] - p1[1]) * u[1] + (p2[2] - p1[2]) * u[2];
+}
+
 // ------------------------------------------------------------- SE - SE (2D)
 // A 2D body uses c[0..1], the upper-left 2x2 block of R (a rotation about z), r[0..1], e.
 struct Local2 {

@@ -562,8 +562,8 @@ __global__ void k_residual64(int nin, const int* ci, const int* cj, const int* s
     if (vmax > 0.0) atomicMax(viol_bits, (unsigned long long)__double_as_longlong(vmax));
 }
 
-template <int DIM, int PROB>
-__global__ void k_accumulate(const Sizes* sizes, const double* bn, const int* slot, double* lam, const float* delta,
+template <int DIM, int PROB, typename TD>
+__global__ void k_accumulate(const Sizes* sizes, const double* bn, const int* slot, double* lam, const TD* delta,
                              int first, double mu) {
     const int C = sizes->C;
     GRID_STRIDE(c, C) {
@@ -715,15 +715,20 @@ void launch_residual64(const Bodies& b, const StepParams& p, const Contacts& c, 
     g_apgd_launches += 1;
 }
 
-void launch_accumulate(const StepParams& p, const Contacts&, const Assembly& a, double* lam64, const float* delta,
+template <typename TD>
+void launch_accumulate(const StepParams& p, const Contacts&, const Assembly& a, double* lam64, const TD* delta,
                        const Sizes* sizes, long long c_cap, int first, cudaStream_t s) {
 #define AC(D, P) \
     if (p.dim == D && p.problem == P) \
-        k_accumulate<D, P><<<grid_blocks(c_cap), 256, 0, s>>>(sizes, a.bn, a.slot, lam64, delta, first, p.mu);
+        k_accumulate<D, P, TD><<<grid_blocks(c_cap), 256, 0, s>>>(sizes, a.bn, a.slot, lam64, delta, first, p.mu);
     AC(2, 0) AC(2, 1) AC(2, 2) AC(3, 0) AC(3, 1) AC(3, 2)
 #undef AC
     g_apgd_launches += 1;
 }
+template void launch_accumulate<float>(const StepParams&, const Contacts&, const Assembly&, double*, const float*,
+                                       const Sizes*, long long, int, cudaStream_t);
+template void launch_accumulate<double>(const StepParams&, const Contacts&, const Assembly&, double*, const double*,
+                                        const Sizes*, long long, int, cudaStream_t);
 
 template <typename Src, typename Dst>
 void launch_convert(const Src* in, Dst* out, long long n_max, const int* n_dev, int mult, cudaStream_t s) {

@@ -101,6 +101,10 @@ long long se_launches();
 // closest points of the superellipsoid rows [C_obs, C) of c; u0: 4 doubles per row (scratch)
 void launch_se_pairs(int dim, const Bodies& b, Contacts& c, const Sizes* sizes, double* u0, int* counter, int grid,
                      cudaStream_t s);
+// candidate rows of src whose bodies are not provably farther apart than dmax (obstacle
+// rows all kept), compacted into dst
+void launch_se_prefilter(int dim, const Bodies& b, const Contacts& src, Contacts& dst, Sizes* sizes, double dmax,
+                         long long c_cap, int* keep, int* pos, int* scan_work, int* total, cudaStream_t s);
 // rows of src with dij < dmax (obstacle rows all kept) into dst, (i, j) order kept; sizes->C updated
 void launch_se_filter(const Contacts& src, Contacts& dst, Sizes* sizes, double dmax, long long c_cap, int* keep,
                       int* pos, int* scan_work, int* total, cudaStream_t s);
@@ -162,8 +166,9 @@ void launch_particle_pass64(const Bodies& b, const StepParams& p, const Contacts
 // g = dt^2 B u + c and the violation max(0, -min gap) (bits of a non-negative double in *viol_bits).
 void launch_residual64(const Bodies& b, const StepParams& p, const Contacts& c, const Assembly& a, const double* u,
                        double* g, unsigned long long* viol_bits, const Sizes* sizes, long long c_cap, cudaStream_t s);
-// lambda64 += delta32 then projection onto the cone / orthant in FP64.
-void launch_accumulate(const StepParams& p, const Contacts& c, const Assembly& a, double* lam64, const float* delta,
+// lambda64 += delta (FP32 or FP64) then projection onto the cone / orthant in FP64.
+template <typename TD>
+void launch_accumulate(const StepParams& p, const Contacts& c, const Assembly& a, double* lam64, const TD* delta,
                        const Sizes* sizes, long long c_cap, int first, cudaStream_t s);
 
 // ----------------------------------------------------------- apgd_sph.cu

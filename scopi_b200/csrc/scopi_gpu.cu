@@ -564,9 +564,13 @@ struct scopi_gpu_handle {
         launch_geometry(b, sp, cur, d_sizes_cur, c_cap, has_old ? &old : nullptr, has_old ? &d_sizes_old->C : nullptr,
                         c_cap, stream);
         if (has_se) {
-            // the search kept bounding-sphere candidates: closest points of the superellipsoid
-            // pairs, then the rows with dij < dmax into the other list (no viscous gamma to
-            // carry here), which becomes the current one
+            // the search kept bounding-sphere candidates: the pairs that can touch (gap along
+            // the line of centres <= dmax), their closest points, then the rows with
+            // dij < dmax (no viscous gamma to carry here); each filter compacts into the other
+            // list, which becomes the current one
+            launch_se_prefilter(P.dim, b, cur, old, d_sizes_cur, P.dmax, c_cap, d_se_keep, d_se_pos, dw.scan_work,
+                                dw.tmp_total + 2, stream);
+            std::swap(cur, old);
             launch_se_pairs(P.dim, b, cur, d_sizes_cur, d_se_u, dw.tmp_total + 3, 3 * kSMs, stream);
             launch_se_filter(cur, old, d_sizes_cur, P.dmax, c_cap, d_se_keep, d_se_pos, dw.scan_work,
                              dw.tmp_total + 2, stream);
@@ -811,7 +815,9 @@ struct scopi_gpu_handle {
 
     // FP32 APGD iterations with an FP64 outer correction: after each FP32 solve the
     // residual g = Q lambda + c and the violation are recomputed in FP64, and APGD is
-    // rerun in FP32 on the correction delta (linear term g, constraint lambda + delta in K).
+    // rerun in FP32 on the correction delta (linear term g, constraint lambda + delta in K),
+    // up to mixed_max_corrections times; if the violation is still above the target, one
+    // last correction runs in FP64.
     int mixed_solve(double dt, long long M, float& ms_apgd) {
         Bodies b = bodies();
         StepParams sp = step_params(dt);
@@ -868,9 +874,54 @@ struct scopi_gpu_handle {
             accumulate_stats(true);
             return 0;
         };
+        // FP64 correction, when the FP32 corrections end above the target: FP32 steps cannot
+        // resolve a correction below their rounding floor (4 eps |lambda|)
+        auto solve64 = [&]() -> int {
+            cudaEventRecord(ev_a[0], stream);
+            int r;
+            if (sphere_mode()) {
+                launch_pack_nc<double>(as.bn, d_res64, d_nc64, d_sizes_cur, c_cap, stream);
+                SphSolve<double> s64 = sph_buffers<double>(d_nc64, d_incv64, d_imt64, d_lam64, d_us64);
+                s64.shift = d_lamacc;
+                r = run_apgd_sph<double>(s64, max_sph64, dt, P.tolerance, P.max_ite, M, alpha0);
+                // the FP64 residual reads (n, c) from the same records
+                launch_pack_nc<double>(as.bn, as.cvec, d_nc64, d_sizes_cur, c_cap, stream);
+            } else {
+                SolveBuffers<double> s64{};
+                s64.bn = as.bn;
+                s64.bai = as.bai;
+                s64.baj = as.baj;
+                s64.bP = as.bP;
+                s64.cvec = d_res64;
+                s64.shift = d_lamacc;
+                s64.inc_ptr = inc.ptr;
+                s64.inc_idx = inc.idx;
+                s64.inc_coef = inc.coef;
+                for (int k = 0; k < 3; ++k) {
+                    s64.lam[k] = d_lam64[k];
+                    s64.u[k] = d_u64[k];
+                }
+                s64.g = d_g64;
+                s64.partials = d_partials;
+                s64.barrier = d_barrier;
+                s64.result = d_result;
+                r = run_apgd<double>(s64, d_invm64, max_blocks64, dt, P.tolerance, P.max_ite, M, alpha0);
+            }
+            cudaEventRecord(ev_a[1], stream);
+            if (r) return r;
+            cudaEventSynchronize(ev_a[1]);
+            float ms = 0;
+            cudaEventElapsedTime(&ms, ev_a[0], ev_a[1]);
+            total += ms;
+            accumulate_stats(false);
+            stats.corrections += 1;
+            launch_accumulate(sp, cur, as, d_lamacc, d_lam64[h_result->lam_buf], d_sizes_cur, c_cap, 0, stream);
+            return 0;
+        };
         int rc = solve32();
         if (rc) return rc;
         launch_accumulate(sp, cur, as, d_lamacc, d_lam32[h_result->lam_buf], d_sizes_cur, c_cap, 1, stream);
+        bool fp64_done = false;
         for (int k = 0;; ++k) {
             cudaMemsetAsync(d_viol, 0, sizeof(unsigned long long), stream);
             if (sphere_mode()) {
@@ -887,7 +938,13 @@ struct scopi_gpu_handle {
             if (e != cudaSuccess) return cuda_fail(e, "mixed residual");
             double viol;
             std::memcpy(&viol, h_viol, sizeof(double));
-            if (viol <= P.mixed_violation_tol || k >= P.mixed_max_corrections) break;
+            if (viol <= P.mixed_violation_tol || fp64_done) break;
+            if (k >= P.mixed_max_corrections) {
+                rc = solve64();
+                if (rc) return rc;
+                fp64_done = true;
+                continue;
+            }
             // correction solve: linear term = FP64 residual, solution offset = lambda so far
             if (sphere_mode()) {
                 launch_pack_nc<float>(as.bn, d_res64, d_nc32, d_sizes_cur, c_cap, stream);

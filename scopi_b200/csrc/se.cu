@@ -720,6 +720,22 @@ __global__ void __launch_bounds__(128) k_se2_pairs(Bodies B, Contacts c, const S
     }
 }
 
+// before the solves: drop the candidate rows whose bodies are provably farther apart than
+// dmax (gap along the line of centres; obstacle rows kept)
+__global__ void k_se_gap_keep(int dim, Bodies B, Contacts c, const Sizes* sizes, double dmax, int* keep) {
+    const int C = sizes->C, C_obs = sizes->C_obs;
+    GRID_STRIDE(k, C) {
+        if (k < C_obs) {
+            keep[k] = 1;
+            continue;
+        }
+        const int i = c.ci[k], j = c.cj[k];
+        const double gap = dim == 3 ? support_gap3(load(B, i), load(B, j)) : support_gap2(load2(B, i), load2(B, j));
+        const double lim = B.radius[i] + B.radius[j] + dmax;
+        keep[k] = gap > dmax + 1e-9 * lim ? 0 : 1;
+    }
+}
+
 // keep a row: obstacle rows (already exact) or dij < dmax
 __global__ void k_se_keep(Contacts c, const Sizes* sizes, double dmax, int* keep) {
     const int C = sizes->C, C_obs = sizes->C_obs;
@@ -765,6 +781,17 @@ void launch_se_pairs(int dim, const Bodies& b, Contacts& c, const Sizes* sizes, 
     cudaMemsetAsync(counter, 0, sizeof(int), s);
     k_se_solve<<<4 * kSMs, 128, 0, s>>>(b, c, sizes, u0, counter);
     g_se_launches += 2;
+}
+
+void launch_se_prefilter(int dim, const Bodies& b, const Contacts& src, Contacts& dst, Sizes* sizes, double dmax,
+                         long long c_cap, int* keep, int* pos, int* scan_work, int* total, cudaStream_t s) {
+    const int threads = 256;
+    const int blocks = (int)std::min<long long>((c_cap + threads - 1) / threads, 4096);
+    k_se_gap_keep<<<blocks, threads, 0, s>>>(dim, b, src, sizes, dmax, keep);
+    scan_exclusive(keep, pos, &sizes->C, 0, c_cap, total, scan_work, s, &g_se_launches);
+    k_se_compact<<<blocks, threads, 0, s>>>(src, dst, sizes, keep, pos);
+    k_se_sizes<<<1, 1, 0, s>>>(sizes, total);
+    g_se_launches += 3;
 }
 
 void launch_se_filter(const Contacts& src, Contacts& dst, Sizes* sizes, double dmax, long long c_cap, int* keep,

@@ -197,21 +197,13 @@ __device__ __forceinline__ void normal2(const Body2& s, double b, double* w) {
 // closest_points.hpp:1479-1759 in closed form): the body point whose outward normal is
 // opposite to the plane normal oriented toward the body, and its projection on the plane.
 // pi on the body, pj on the plane, nij = the oriented plane normal, dij = (pi - pj).nij.
-__device__ __forceinline__ void body_plane(const Body& s, const double* pc, const double* pq, double* pi, double* pj,
-                                           double* nij, double& dij) {
+// Angles (a, b) of the body point whose outward normal points along the body-frame
+// direction m: b = atan2(sign(my)|ry my|^(1/(2-e)), sign(mx)|rx mx|^(1/(2-e))),
+// |tan a|^(2-n) = |mz| |(ry rz C(b,2-e), rx rz S(b,2-e))| / (rx ry |(mx, my)|), sign(a) = sign(mz).
+__device__ __forceinline__ void support_angles(const Body& s, const double* m, double& a, double& b) {
     const double pi_ = 3.14159265358979323846;
-    double P[9];
-    rot(pq, P);
-    const double np[3] = {P[0], P[3], P[6]};
-    const double rel[3] = {s.c[0] - pc[0], s.c[1] - pc[1], s.c[2] - pc[2]};
-    const double sg = dot3(rel, np) < 0 ? -1.0 : 1.0;
-    // body-frame direction of the wanted outward normal: -sg np (R^T np)
-    const double m[3] = {-sg * (s.R[0] * np[0] + s.R[3] * np[1] + s.R[6] * np[2]),
-                         -sg * (s.R[1] * np[0] + s.R[4] * np[1] + s.R[7] * np[2]),
-                         -sg * (s.R[2] * np[0] + s.R[5] * np[1] + s.R[8] * np[2])};
     const double rx = s.r[0], ry = s.r[1], rz = s.r[2];
     const double mxy = sqrt(m[0] * m[0] + m[1] * m[1]);
-    double a, b;
     if (mxy == 0) {
         b = 0;
         a = m[2] >= 0 ? pi_ / 2 : -pi_ / 2;
@@ -223,6 +215,21 @@ __device__ __forceinline__ void body_plane(const Body& s, const double* pc, cons
         const double t = fabs(m[2]) * h / (rx * ry * mxy);
         a = sgn(m[2]) * atan(pow(t, kn));
     }
+}
+
+__device__ __forceinline__ void body_plane(const Body& s, const double* pc, const double* pq, double* pi, double* pj,
+                                           double* nij, double& dij) {
+    double P[9];
+    rot(pq, P);
+    const double np[3] = {P[0], P[3], P[6]};
+    const double rel[3] = {s.c[0] - pc[0], s.c[1] - pc[1], s.c[2] - pc[2]};
+    const double sg = dot3(rel, np) < 0 ? -1.0 : 1.0;
+    // body-frame direction of the wanted outward normal: -sg np (R^T np)
+    const double m[3] = {-sg * (s.R[0] * np[0] + s.R[3] * np[1] + s.R[6] * np[2]),
+                         -sg * (s.R[1] * np[0] + s.R[4] * np[1] + s.R[7] * np[2]),
+                         -sg * (s.R[2] * np[0] + s.R[5] * np[1] + s.R[8] * np[2])};
+    double a, b;
+    support_angles(s, m, a, b);
     point(s, a, b, pi);
     const double d[3] = {pi[0] - pc[0], pi[1] - pc[1], pi[2] - pc[2]};
     const double h = dot3(d, np);
@@ -232,6 +239,43 @@ __device__ __forceinline__ void body_plane(const Body& s, const double* pc, cons
     }
     const double df[3] = {pi[0] - pj[0], pi[1] - pj[1], pi[2] - pj[2]};
     dij = dot3(df, nij);
+}
+
+// ---- separation bound.  For convex bodies (squareness in (0, 2)) the distance is at least
+// the gap along any unit direction u: (support point of body 2 in -u - support point of
+// body 1 in u).u; u is the line of centres.  -inf for coincident centres.
+__device__ __forceinline__ double support_gap3(const Body& s1, const Body& s2) {
+    const double d[3] = {s2.c[0] - s1.c[0], s2.c[1] - s1.c[1], s2.c[2] - s1.c[2]};
+    const double l = norm3(d);
+    if (!(l > 0)) return -INFINITY;
+    const double u[3] = {d[0] / l, d[1] / l, d[2] / l};
+    double m1[3], m2[3];
+    for (int k = 0; k < 3; ++k) {
+        m1[k] = s1.R[k] * u[0] + s1.R[3 + k] * u[1] + s1.R[6 + k] * u[2];
+        m2[k] = -(s2.R[k] * u[0] + s2.R[3 + k] * u[1] + s2.R[6 + k] * u[2]);
+    }
+    double a, b, p1[3], p2[3];
+    support_angles(s1, m1, a, b);
+    point(s1, a, b, p1);
+    support_angles(s2, m2, a, b);
+    point(s2, a, b, p2);
+    return (p2[0] - p1[0]) * u[0] + (p2[1] - p1[1]) * u[1] + (p2[2] - p1[2]) * u[2];
+}
+__device__ __forceinline__ double support_angle2(const Body2& s, double m0, double m1) {
+    const double ke = 1.0 / (2 - s.e);
+    return atan2(sgn(m1) * pow(fabs(s.r[1] * m1), ke), sgn(m0) * pow(fabs(s.r[0] * m0), ke));
+}
+__device__ __forceinline__ double support_gap2(const Body2& s1, const Body2& s2) {
+    const double d[2] = {s2.c[0] - s1.c[0], s2.c[1] - s1.c[1]};
+    const double l = sqrt(d[0] * d[0] + d[1] * d[1]);
+    if (!(l > 0)) return -INFINITY;
+    const double u[2] = {d[0] / l, d[1] / l};
+    const double m10 = s1.R[0] * u[0] + s1.R[2] * u[1], m11 = s1.R[1] * u[0] + s1.R[3] * u[1];
+    const double m20 = -(s2.R[0] * u[0] + s2.R[2] * u[1]), m21 = -(s2.R[1] * u[0] + s2.R[3] * u[1]);
+    double p1[2], p2[2];
+    point2(s1, support_angle2(s1, m10, m11), p1);
+    point2(s2, support_angle2(s2, m20, m21), p2);
+    return (p2[0] - p1[0]) * u[0] + (p2[1] - p1[1]) * u[1];
 }
 
 }  // namespace se

@@ -205,6 +205,19 @@ def test_mixed_precision_reaches_violation_target():
     assert rel_err(mix.particles.pos, f64.particles.pos) <= 1e-7
 
 
+def test_mixed_fp64_correction_when_fp32_corrections_run_out():
+    """No FP32 correction allowed and a target of 0 (never met): one correction runs in FP64
+    (torque-free kernel with the offset) and ends at the FP64 solve's accuracy."""
+    pa = configs.spheres_1m(side=16)
+    st = configs.SETTINGS["spheres_1m"]
+    kw = dict(dmax=st["dmax"], tolerance=st["tolerance"], max_ite=st["max_ite"], vap=st["vap"])
+    f64 = gpu_solver(pa, **kw).run(st["dt"], 3)
+    mix = gpu_solver(pa, precision=1, mixed_violation_tol=0.0, mixed_max_corrections=0, **kw).run(st["dt"], 3)
+    sm = mix.stats()
+    assert sm["corrections"] == 1 and sm["violation"] <= max(1e-10, 10 * f64.stats()["violation"]), sm
+    assert rel_err(mix.particles.pos, f64.particles.pos) <= 1e-7
+
+
 def test_deterministic_bitwise():
     pa = configs.spheres_1m(side=12)
     st = configs.SETTINGS["spheres_1m"]

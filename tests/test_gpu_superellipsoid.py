@@ -105,9 +105,7 @@ def test_superellipsoid_pile_contact_set_matches_the_oracle():
 def test_superellipsoid_pile_steps_like_the_oracle():
     """FP64 with friction, a few steps of the pile: the same contacts as the oracle every
     step; positions within 2e-5 relative.  Not 1e-9: the pairs where MINPACK stops on slow
-    progress have normals that differ by up to ~1e-2 between the two arithmetics (observed
-    5.7e-6 after 4 steps), and the lattice's rotated bodies start interpenetrating (one pair
-    of this scene lands on a spurious root with dij = -2 cm in both)."""
+    progress have normals that differ by up to ~1e-2 between the two arithmetics."""
     pa = configs.se_pile(count=27, side=3, seed=4)
     kw, st = pile_kw(pa)
     g = gpu_solver(pa, **kw)
@@ -119,6 +117,19 @@ def test_superellipsoid_pile_steps_like_the_oracle():
         assert np.array_equal(gc["i"], oc["i"]) and np.array_equal(gc["j"], oc["j"]), k
     assert rel_err(g.particles.pos, o.pa.pos) <= 2e-5
     assert g.stats()["converged"] == 1
+
+
+def test_superellipsoid_pile_fp64_correction():
+    """Friction (6-dof kernel): with no FP32 correction allowed, the FP64 correction after the
+    FP32 solve brings the violation to the target."""
+    pa = configs.se_pile(count=64, side=4, seed=5)
+    kw, st = pile_kw(pa)
+    f64 = gpu_solver(pa, **kw).run(st["dt"], 3)
+    mix = gpu_solver(pa, precision=MIXED, mixed_violation_tol=1e-8, mixed_max_corrections=0, **kw).run(st["dt"], 3)
+    sm = mix.stats()
+    assert sm["contacts"] > 0
+    assert sm["violation"] <= max(1e-8, 10 * f64.stats()["violation"]), sm
+    assert rel_err(mix.particles.pos, f64.particles.pos) <= 1e-6
 
 
 def test_superellipsoid_pile_mixed_precision():
