@@ -17,7 +17,7 @@
 // set an error flag instead of hanging.
 #include <math.h>
 
-#include "kernels.cuh"
+#include "apgd_common.cuh"
 
 namespace scopi_gpu {
 
@@ -27,7 +27,7 @@ long long apgd_launches() { return g_apgd_launches; }
 namespace {
 
 constexpr int kApgdThreads = 256;
-constexpr int kPartials = 8;  // s1..s8
+constexpr int kPartials = 9;  // s1..s8 and the FP32 curvature term
 constexpr unsigned long long kBarrierTimeoutNs = 20ull * 1000ull * 1000ull * 1000ull;
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -183,6 +183,7 @@ struct ApgdArgs {
     double alpha, tol, dt2, mu;
     long long max_ite;
     int dynamic;
+    int curvature_start;
 };
 
 template <typename T, int DIM, int PROB>
@@ -336,8 +337,11 @@ __device__ void contact_pass(const ApgdArgs<T>& A, int C, const T* lam, const T*
     }
 }
 
+// curv (FP32 iterations): s[8] += (u(l+) - u(y))^T M (u(l+) - u(y)), the curvature d^T Q d / dt^2
+// along d = l+ - y of the curvature-form backtracking test
 template <typename T, int DIM, int PROB>
-__device__ void particle_pass(const ApgdArgs<T>& A, const T* lnew, T* unew, double* s) {
+__device__ void particle_pass(const ApgdArgs<T>& A, const T* lnew, T* unew, const T* ul, const T* up, T beta,
+                              bool use_prev, bool curv, double* s) {
     GRID_STRIDE(p, A.na) {
         T w[6] = {0, 0, 0, 0, 0, 0};
         const int k0 = A.inc_ptr[p], k1 = A.inc_ptr[p + 1];
@@ -378,6 +382,20 @@ __device__ void particle_pass(const ApgdArgs<T>& A, const T* lnew, T* unew, doub
 #pragma unroll
         for (int d = 0; d < 6; ++d) acc += (double)w[d] * (double)u[d];
         s[6] += acc;
+        if (curv) {
+            T a[6], b[6];
+            load6cg(ul + 6 * (long long)p, a);
+            if (use_prev) load6cg(up + 6 * (long long)p, b);
+            const T m[6] = {im[0], im[0], im[0], im[1], im[2], im[3]};
+            double q = 0.0;
+#pragma unroll
+            for (int d = 0; d < 6; ++d) {
+                const T uy = use_prev ? a[d] + beta * (a[d] - b[d]) : a[d];
+                const double dd = (double)u[d] - (double)uy;
+                if (m[d] > (T)0) q += dd * dd / (double)m[d];
+            }
+            s[8] += q;
+        }
     }
 }
 
@@ -401,17 +419,74 @@ __global__ void __launch_bounds__(kApgdThreads) k_apgd(ApgdArgs<T> A) {
     int conv = 0, err = 0;
     int parity = 0;
     double last_step = 0.0;
+    if (A.curvature_start) {
+        // initial step from the curvature along the first projected-gradient direction d of
+        // the cold start (stored in the candidate buffers, which the first iteration
+        // overwrites): L = 1.5 dt^2 |B^T d|^2_{M^-1} / |d|^2
+        T* dbuf = lamb[in_];
+        double s[kPartials] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        GRID_STRIDE(c, C) {
+            if (PROB == kFriction) {
+                double z[3], n[3];
+                for (int d = 0; d < 3; ++d) {
+                    n[d] = (double)A.bn[3 * c + d];
+                    z[d] = -(double)A.cvec[3 * c + d] + (A.shift ? A.shift[3 * c + d] : 0.0);
+                }
+                if (DIM == 2) z[2] = A.shift ? A.shift[3 * c + 2] : 0.0;
+                cone_project<DIM>(z, n, A.mu);
+                for (int d = 0; d < 3; ++d) {
+                    const T v = (T)(z[d] - (A.shift ? A.shift[3 * c + d] : 0.0));
+                    dbuf[3 * c + d] = v;
+                    s[1] += (double)v * (double)v;
+                }
+            } else {
+                const T v = apgdc::first_descent<T>(A.cvec[c], A.shift, c);
+                dbuf[c] = v;
+                s[1] += (double)v * (double)v;
+                if (PROB == kViscous) {
+                    const int sl = A.slot[c];
+                    if (sl >= 0) {
+                        const T v2 = apgdc::first_descent<T>(-A.cvec[c], A.shift, sl);
+                        dbuf[sl] = v2;
+                        s[1] += (double)v2 * (double)v2;
+                    }
+                }
+            }
+        }
+        bool ok = grid_barrier(A.bar, nb);
+        if (ok) particle_pass<T, DIM, PROB>(A, dbuf, ub[jn], ub[jl], ub[jp], (T)0, false, false, s);
+        block_sum(s);
+        double* part = A.partials;
+        if (threadIdx.x == 0)
+            for (int k = 0; k < kPartials; ++k) part[blockIdx.x * kPartials + k] = s[k];
+        if (ok) ok = grid_barrier(A.bar, nb);
+        double t[kPartials] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (unsigned int b = threadIdx.x; b < nb; b += blockDim.x)
+            for (int k = 0; k < kPartials; ++k) t[k] += __ldcg(part + b * kPartials + k);
+        block_sum(t);
+        // the first iteration writes partials region 1, then region 0 after a barrier
+        parity = 1;
+        double l;
+        if (!ok) {
+            err = 1;
+        } else if (apgdc::initial_lipschitz(t[1], t[6], A.dt2, l)) {
+            lipsch = l;
+            alpha = 1.0 / l;
+            lgood = l;
+        }
+    }
     for (;;) {
-        double s[kPartials] = {0, 0, 0, 0, 0, 0, 0, 0};
+        if (err) break;
+        double s[kPartials] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
         contact_pass<T, DIM, PROB>(A, C, lamb[il], lamb[ip], lamb[in_], ub[jl], ub[jp], (T)beta, use_prev, bt, alpha, s);
         if (!grid_barrier(A.bar, nb)) { err = 1; break; }
-        particle_pass<T, DIM, PROB>(A, lamb[in_], ub[jn], s);
+        particle_pass<T, DIM, PROB>(A, lamb[in_], ub[jn], ub[jl], ub[jp], (T)beta, use_prev, sizeof(T) == 4, s);
         block_sum(s);
         double* part = A.partials + (size_t)parity * nb * kPartials;
         if (threadIdx.x == 0)
             for (int k = 0; k < kPartials; ++k) part[blockIdx.x * kPartials + k] = s[k];
         if (!grid_barrier(A.bar, nb)) { err = 1; break; }
-        double t[kPartials] = {0, 0, 0, 0, 0, 0, 0, 0};
+        double t[kPartials] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
         for (unsigned int b = threadIdx.x; b < nb; b += blockDim.x)
             for (int k = 0; k < kPartials; ++k) t[k] += __ldcg(part + b * kPartials + k);
         block_sum(t);
@@ -427,8 +502,8 @@ __global__ void __launch_bounds__(kApgdThreads) k_apgd(ApgdArgs<T> A) {
                 ++nbt;
             }
             alpha = 1. / lipsch;
-        } else if (A.dynamic && F_lp >= Fy + t[0] + 0.5 * lipsch * t[1]) {
-            // backtracking, apgd.hpp:172-182
+        } else if (A.dynamic && apgdc::sufficient_decrease_fails<T>(F_lp, Fy, t[0], t[1], A.dt2 * t[8], lipsch)) {
+            // backtracking, apgd.hpp:172-182 (FP32: its curvature form)
             lipsch *= 2;
             alpha = 1. / lipsch;
             bt = true;
@@ -676,6 +751,7 @@ cudaError_t launch_apgd_invm(const Bodies& b, const StepParams& p, const ApgdSet
     A.tol = st.tol;
     A.dt2 = st.dt * st.dt;
     A.mu = st.mu;
+    A.curvature_start = st.curvature_start;
     A.max_ite = st.max_ite;
     A.dynamic = st.dynamic;
 #define LA(D, P) \

@@ -637,7 +637,8 @@ struct scopi_gpu_handle {
         st.dynamic = P.dynamic_descent;
         st.dt = dt;
         st.mu = P.mu;
-        st.curvature_start = 0;  // the 6-dof kernel starts from alpha
+        // a correction solve starts from the step size of the solve before it
+        st.curvature_start = alpha0 > 0.0 ? 0 : curvature_start();
         cudaMemsetAsync(sb.lam[0], 0, M * sizeof(T), stream);
         cudaMemsetAsync(sb.lam[1], 0, M * sizeof(T), stream);
         cudaMemsetAsync(sb.u[0], 0, 6 * (size_t)na * sizeof(T), stream);
