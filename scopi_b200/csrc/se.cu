@@ -607,8 +607,10 @@ __device__ void sese_J(const Body& s1, const Body& s2, const double* u, double* 
 // rows are handed out by a counter so that a lane takes the next row when its solve ends
 // (the evaluations per solve vary from a few to maxfev).  (One warp per row, with the 32
 // powers of an evaluation spread over the lanes, measured 5x slower: the hybrid method's
-// own scalar work, then done 32 times, outweighs the powers.)
-__global__ void __launch_bounds__(128, 3) k_se_solve(Bodies B, Contacts c, const Sizes* sizes, const double* u0,
+// own scalar work, then done 32 times, outweighs the powers.)  Two 128-thread blocks per SM
+// (255 registers): the hybrid method's arrays then stay in L1 (three blocks at 168 registers
+// spilled 2.4 KB per thread and measured 20 % slower per step of the 50k pile).
+__global__ void __launch_bounds__(128, 2) k_se_solve(Bodies B, Contacts c, const Sizes* sizes, const double* u0,
                                                     int* next) {
     const int C = sizes->C, C_obs = sizes->C_obs;
     for (;;) {
