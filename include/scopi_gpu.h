@@ -43,6 +43,10 @@ extern "C" {
 #define SCOPI_GPU_NOFRICTION 0
 #define SCOPI_GPU_FRICTION 1
 #define SCOPI_GPU_VISCOUS 2
+/* FrictionFixedPoint (property.hpp:26, OptimGradient.hpp:85-176): the Friction problem with
+   the linear term c + s_c n_c, s_c = mu dt |tangential relative velocity| updated after
+   each solve until the fixed point (fixed_point_tol, fixed_point_max_iter) */
+#define SCOPI_GPU_FRICTION_FIXED_POINT 3
 /* vap policies (include/scopi/vap/vap_fixed.hpp, vap_fpd.hpp) */
 #define SCOPI_GPU_VAP_FIXED 0
 #define SCOPI_GPU_VAP_FPD 1
@@ -61,7 +65,7 @@ extern "C" {
 
 typedef struct scopi_gpu_params {
     int32_t dim;              /* 2 or 3 */
-    int32_t problem;          /* SCOPI_GPU_NOFRICTION / FRICTION / VISCOUS */
+    int32_t problem;          /* SCOPI_GPU_NOFRICTION / FRICTION / VISCOUS / FRICTION_FIXED_POINT */
     int32_t vap;              /* SCOPI_GPU_VAP_FIXED / VAP_FPD */
     int32_t contact_method;   /* SCOPI_GPU_BRUTE_FORCE / KDTREE */
     int32_t precision;        /* SCOPI_GPU_FP64 / SCOPI_GPU_MIXED */
@@ -79,14 +83,15 @@ typedef struct scopi_gpu_params {
     int32_t mixed_max_corrections;/* MIXED: FP32 correction solves after the first one */
     int32_t device;               /* CUDA device ordinal */
     int32_t initial_step;         /* SCOPI_GPU_STEP_AUTO / _REFERENCE / _CURVATURE (below) */
+    double fixed_point_tol;       /* contact_property<FixedPoint> (property.hpp:93-94): 1e-6 */
+    int64_t fixed_point_max_iter; /* and 1000 solves at most per step */
 } scopi_gpu_params;
 
 /* First APGD step of every solve.  REFERENCE: alpha as given (apgd.hpp:120, the
    reference's fixed 0.05), grown by 1/0.97 per accepted iteration.  CURVATURE: 1/L with
    L = 1.5 x the Rayleigh quotient d^T Q d / |d|^2 along the first projected-gradient
-   direction d (one extra particle pass per solve); torque-free and batched kernels only,
-   the 6-dof kernel (Friction) keeps alpha.  AUTO: REFERENCE for FP64 (the drop-in, same
-   iterates as the reference), CURVATURE for MIXED. */
+   direction d (one extra particle pass per solve).  AUTO: REFERENCE for FP64 (the drop-in,
+   same iterates as the reference), CURVATURE for MIXED. */
 #define SCOPI_GPU_STEP_AUTO (-1)
 #define SCOPI_GPU_STEP_REFERENCE 0
 #define SCOPI_GPU_STEP_CURVATURE 1
@@ -126,6 +131,7 @@ typedef struct scopi_gpu_stats {
     double ms_solve;         /* device time of the APGD part of the last step */
     double ms_apgd_kernel;   /* device time of the persistent APGD launches of the last step */
     int64_t steps;           /* steps run by this handle */
+    int64_t fixed_point_iterations; /* FRICTION_FIXED_POINT: solves of the last step */
 } scopi_gpu_stats;
 
 typedef struct scopi_gpu_handle scopi_gpu_handle;

@@ -16,7 +16,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle_scopi.so")
 
-NOFRICTION, FRICTION, VISCOUS = 0, 1, 2
+NOFRICTION, FRICTION, VISCOUS, FRICTION_FIXED_POINT = 0, 1, 2, 3
 VAP_FIXED, VAP_FPD = 0, 1
 BRUTE_FORCE, KDTREE = 0, 1
 
@@ -27,6 +27,7 @@ class OrcParams(C.Structure):
         ("dmax", C.c_double), ("kd_tree_radius", C.c_double), ("alpha", C.c_double), ("max_ite", C.c_int64),
         ("tolerance", C.c_double), ("dynamic_descent", C.c_int32), ("mu", C.c_double), ("gamma", C.c_double),
         ("gamma_min", C.c_double), ("gamma_tol", C.c_double), ("num_threads", C.c_int32),
+        ("fixed_point_tol", C.c_double), ("fixed_point_max_iter", C.c_int64),
     ]
 
 
@@ -45,7 +46,7 @@ class OrcStats(C.Structure):
     _fields_ = [
         ("contacts", C.c_int64), ("iterations", C.c_int64), ("backtracks", C.c_int64), ("restarts", C.c_int64),
         ("converged", C.c_int32), ("violation", C.c_double), ("seconds_contacts", C.c_double),
-        ("seconds_solve", C.c_double), ("seconds_other", C.c_double),
+        ("seconds_solve", C.c_double), ("seconds_other", C.c_double), ("fixed_point_iterations", C.c_int64),
     ]
 
 
@@ -116,10 +117,12 @@ class OracleSolver:
 
     def __init__(self, particles, problem=NOFRICTION, vap=VAP_FIXED, contact_method=KDTREE, dmax=2.0,
                  kd_tree_radius=17.0, alpha=0.05, max_ite=10000, tolerance=1e-7, dynamic_descent=True, mu=0.1,
-                 gamma=0.0, gamma_min=-2.0, gamma_tol=1e-6, num_threads=0):
+                 gamma=0.0, gamma_min=-2.0, gamma_tol=1e-6, num_threads=0, fixed_point_tol=1e-6,
+                 fixed_point_max_iter=1000):
         self.pa = particles.copy()
         self.params = OrcParams(particles.dim, problem, vap, contact_method, dmax, kd_tree_radius, alpha, max_ite,
-                                tolerance, 1 if dynamic_descent else 0, mu, gamma, gamma_min, gamma_tol, num_threads)
+                                tolerance, 1 if dynamic_descent else 0, mu, gamma, gamma_min, gamma_tol, num_threads,
+                                fixed_point_tol, fixed_point_max_iter)
         keep = []
         ps = _particles_struct(self.pa, keep)
         self.h = lib().orc_create(C.byref(self.params), C.byref(ps))

@@ -124,6 +124,9 @@ struct orc_solver {
     std::vector<double> lambda;
     orc_stats stats{};
     double dt = 0;
+    // FrictionFixedPoint: p.problem holds ORC_FRICTION, this flag the outer loop; sij per contact
+    bool fixed_point = false;
+    std::vector<double> sij;
 
     int64_t na() const { return n - nin; }
 
@@ -454,6 +457,7 @@ struct orc_solver {
     struct Problem {
         const orc_solver* s;
         std::vector<double> invM, C;
+        std::vector<double> S;          // FrictionFixedPoint: s_c n_c (empty otherwise)
         std::vector<int64_t> neg_slot;  // Viscous: second multiplier slot or -1
         int64_t size = 0;
         mutable std::vector<double> w1, w2, w3;
@@ -487,6 +491,13 @@ struct orc_solver {
                     const double dn = d < dim ? s->contacts[c].dij * s->contacts[c].nij[d] : 0.0;  // DMatrix
                     C[3 * c + d] = dn + s->dt * AU[3 * c + d];
                 }
+            // S vector of LagrangeMultiplier<FrictionFixedPoint> (lagrange_multiplier.hpp:286-292):
+            // s_c n_c on the first dim components of the contact's rows
+            if (s->fixed_point) {
+                S.assign(3 * nc, 0.0);
+                for (size_t c = 0; c < nc; ++c)
+                    for (int d = 0; d < dim; ++d) S[3 * c + d] = s->sij[c] * s->contacts[c].nij[d];
+            }
             // LagrangeMultiplier sizes, lagrange_multiplier.hpp:54-60,125-141,217-236
             if (s->p.problem == ORC_FRICTION) {
                 size = 3 * (int64_t)nc;
@@ -539,13 +550,17 @@ struct orc_solver {
             const double dt2 = s->dt * s->dt;
             for (auto& x : out) x = dt2 * x;
         }
-        // minimization_problem::gradient, :122-128 (S = 0 for these problems)
+        // minimization_problem::gradient, :122-128 (S = 0 except for FrictionFixedPoint)
         void gradient(const std::vector<double>& lam, std::vector<double>& out) const {
             l2g(lam, w2);
             Q(w2, w3);
             for (size_t k = 0; k < w3.size(); ++k) w3[k] = w3[k] + C[k];
             g2l(w3, out);
-            for (auto& x : out) x = x + 0.0;
+            if (S.empty()) {
+                for (auto& x : out) x = x + 0.0;
+            } else {
+                for (size_t k = 0; k < out.size(); ++k) out[k] = out[k] + S[k];
+            }
         }
         // minimization_problem::operator(), :130-134
         double objective(const std::vector<double>& lam) const {
@@ -554,7 +569,7 @@ struct orc_solver {
             double acc = 0.0;
             for (size_t k = 0; k < w3.size(); ++k) acc += w2[k] * (0.5 * w3[k] + C[k]);
             double accs = 0.0;
-            for (size_t k = 0; k < lam.size(); ++k) accs += lam[k] * 0.0;
+            for (size_t k = 0; k < lam.size(); ++k) accs += lam[k] * (S.empty() ? 0.0 : S[k]);
             return acc + accs;
         }
         // projections, lagrange_multiplier.hpp:104-107, 196-200, 243-268
@@ -699,17 +714,62 @@ struct orc_solver {
         stats.iterations = 0;
         stats.converged = 1;
         stats.violation = 0;
+        stats.fixed_point_iterations = 0;
         if (!contacts.empty()) {
+            // extra_steps_before_solve<FrictionFixedPoint> (OptimGradient.hpp:85-94): s_c = mu dt
+            if (fixed_point) sij.assign(contacts.size(), p.mu * dt);
             Problem pb(this);
             lambda = apgd(pb);
             std::vector<double> vel;
-            pb.velocities(lambda, vel);
-            for (int64_t i = 0; i < nA; ++i) {
-                for (int d = 0; d < dim; ++d) {
-                    uad[i][d] = v[i + nin][d] + dt * vel[i * 3 + d];
-                    if (dim == 3) wad[i][d] = omega[i + nin][d] + dt * vel[(i + nA) * 3 + d];
+            auto velocities = [&](const Problem& P) {
+                P.velocities(lambda, vel);
+                for (int64_t i = 0; i < nA; ++i) {
+                    for (int d = 0; d < dim; ++d) {
+                        uad[i][d] = v[i + nin][d] + dt * vel[i * 3 + d];
+                        if (dim == 3) wad[i][d] = omega[i + nin][d] + dt * vel[(i + nA) * 3 + d];
+                    }
+                    if (dim == 2) wad[i][2] = omega[i + nin][2] + dt * vel[(i + nA) * 3 + 2];
                 }
-                if (dim == 2) wad[i][2] = omega[i + nin][2] + dt * vel[(i + nA) * 3 + 2];
+            };
+            velocities(pb);
+            if (fixed_point) {
+                // extra_steps_after_solve<FrictionFixedPoint> (OptimGradient.hpp:117-176) and the
+                // solve loop of ScopiSolver::run (solver.hpp:286-291)
+                int64_t iters = stats.iterations, bts = stats.backtracks, rss = stats.restarts, fp = 0;
+                const double mudt = p.mu * dt;
+                for (;;) {
+                    std::vector<double> Uf(6 * nA, 0.0), AUf;
+                    for (int64_t i = 0; i < nA; ++i)
+                        for (int d = 0; d < 3; ++d) {
+                            Uf[3 * i + d] = d < dim ? uad[i][d] : 0.0;
+                            Uf[3 * nA + 3 * i + d] = wad[i][d];
+                        }
+                    amat(Uf, AUf);
+                    double dd = 0.0, ss = 0.0;
+                    for (size_t c = 0; c < contacts.size(); ++c) {
+                        const double dn = dot_n(&AUf[3 * c], contacts[c].nij.data(), dim);
+                        double t[3] = {0, 0, 0};
+                        for (int d = 0; d < dim; ++d) t[d] = AUf[3 * c + d] - contacts[c].nij[d] * dn;
+                        const double snew = mudt * norm_n(t, dim);
+                        dd += (snew - sij[c]) * (snew - sij[c]);
+                        ss += snew * snew;
+                        sij[c] = snew;
+                    }
+                    ++fp;
+                    if (!(mudt > 0.0)) break;  // s stays 0: one solve (the reference's 1/(mu dt) is NaN)
+                    const double err = (1 / mudt) * std::sqrt(dd) / (1 + (1 / mudt) * std::sqrt(ss));
+                    if (err < p.fixed_point_tol || fp >= p.fixed_point_max_iter) break;
+                    Problem pf(this);
+                    lambda = apgd(pf);
+                    velocities(pf);
+                    iters += stats.iterations;
+                    bts += stats.backtracks;
+                    rss += stats.restarts;
+                }
+                stats.iterations = iters;
+                stats.backtracks = bts;
+                stats.restarts = rss;
+                stats.fixed_point_iterations = fp;
             }
             // predicted gap after the step: d + dt n.(A u)
             std::vector<double> Un(6 * nA, 0.0), AU;
@@ -834,6 +894,10 @@ orc_solver* orc_create(const orc_params* p, const orc_particles* parts) {
     if (!p || !parts || (p->dim != 2 && p->dim != 3)) return nullptr;
     auto* s = new orc_solver();
     s->p = *p;
+    if (p->problem == ORC_FRICTION_FIXED_POINT) {
+        s->fixed_point = true;
+        s->p.problem = ORC_FRICTION;
+    }
     s->dim = p->dim;
     s->load(parts);
 #ifdef _OPENMP

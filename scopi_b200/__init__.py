@@ -5,5 +5,5 @@ package holds the host-side mirror of the reference's interface (ScopiSolver,
 particle container) and seeded synthetic workloads.
 """
 from .container import PLANE, SEGMENT, SPHERE, ParticleArrays, Particles, Property, quaternion  # noqa: F401
-from .solver import (BRUTE_FORCE, FP64, FRICTION, KDTREE, MIXED, NOFRICTION, VAP_FIXED, VAP_FPD,  # noqa: F401
-                     VISCOUS, ScopiBatch, ScopiGPUError, ScopiSolver)
+from .solver import (BRUTE_FORCE, FP64, FRICTION, FRICTION_FIXED_POINT, KDTREE, MIXED, NOFRICTION,  # noqa: F401
+                     VAP_FIXED, VAP_FPD, VISCOUS, ScopiBatch, ScopiGPUError, ScopiSolver)

@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libscopi_gpu.so")
 
 OK, EINVAL, ECUDA, ENOMEM, EUNSUPPORTED, ETIMEOUT, ENOCONV = 0, -1, -2, -3, -4, -5, 1
-NOFRICTION, FRICTION, VISCOUS = 0, 1, 2
+NOFRICTION, FRICTION, VISCOUS, FRICTION_FIXED_POINT = 0, 1, 2, 3
 VAP_FIXED, VAP_FPD = 0, 1
 BRUTE_FORCE, KDTREE = 0, 1
 FP64, MIXED = 0, 1
@@ -34,7 +34,7 @@ class Params(C.Structure):
         ("kd_tree_radius", C.c_double), ("alpha", C.c_double), ("tolerance", C.c_double), ("mu", C.c_double),
         ("gamma", C.c_double), ("gamma_min", C.c_double), ("gamma_tol", C.c_double),
         ("mixed_violation_tol", C.c_double), ("mixed_max_corrections", C.c_int32), ("device", C.c_int32),
-        ("initial_step", C.c_int32),
+        ("initial_step", C.c_int32), ("fixed_point_tol", C.c_double), ("fixed_point_max_iter", C.c_int64),
     ]
 
 
@@ -54,7 +54,7 @@ class Stats(C.Structure):
         ("contacts", C.c_int64), ("iterations", C.c_int64), ("backtracks", C.c_int64), ("restarts", C.c_int64),
         ("fp32_iterations", C.c_int64), ("corrections", C.c_int64), ("converged", C.c_int32),
         ("status", C.c_int32), ("violation", C.c_double), ("ms_step", C.c_double), ("ms_solve", C.c_double),
-        ("ms_apgd_kernel", C.c_double), ("steps", C.c_int64),
+        ("ms_apgd_kernel", C.c_double), ("steps", C.c_int64), ("fixed_point_iterations", C.c_int64),
     ]
 
 

@@ -17,6 +17,8 @@
 // set an error flag instead of hanging.
 #include <math.h>
 
+#include <algorithm>
+
 #include "apgd_common.cuh"
 
 namespace scopi_gpu {
@@ -662,6 +664,71 @@ __global__ void k_accumulate(const Sizes* sizes, const double* bn, const int* sl
     }
 }
 
+// ---------------------------------------------------------------- FrictionFixedPoint
+// Linear term of one fixed-point solve: c + s_c n_c (the S vector of
+// LagrangeMultiplier<FrictionFixedPoint>, lagrange_multiplier.hpp:286-292; dim components).
+template <int DIM>
+__global__ void k_fixed_point_c(const Sizes* sizes, const double* base, const double* bn, const double* sv,
+                                double* cvec) {
+    GRID_STRIDE(c, sizes->C) {
+        for (int d = 0; d < 3; ++d)
+            cvec[3 * c + d] = d < DIM ? base[3 * c + d] + sv[c] * bn[3 * c + d] : base[3 * c + d];
+    }
+}
+
+// s_c = mu dt before the first solve of a step (OptimGradient.hpp:85-94)
+__global__ void k_fixed_point_init(const Sizes* sizes, double* sv, double v) {
+    GRID_STRIDE(c, sizes->C) sv[c] = v;
+}
+
+// After a solve (OptimGradient.hpp:117-176): U = v + dt M^-1 B^T l of the active bodies,
+// (A U)_c the contact's relative velocity (active bodies only, AMatrix::mat_mult), s_c =
+// mu dt |(A U)_c - n_c ((A U)_c.n_c)| over dim components; per block the sums of
+// (s_new - s_old)^2 and s_new^2 in a fixed order for the stopping test.
+template <int DIM>
+__global__ void __launch_bounds__(kApgdThreads) k_fixed_point_s(const Sizes* sizes, int nin, const int* ci,
+                                                                const int* cj, const double* bn, const double* bP,
+                                                                const double* v, const double* omega,
+                                                                const double* u, double dt, double mu, double* sv,
+                                                                double* part) {
+    const int C = sizes->C;
+    double s[kPartials] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    GRID_STRIDE(c, C) {
+        const int bi[2] = {ci[c], cj[c]};
+        double au[3] = {0, 0, 0};
+        for (int side = 0; side < 2; ++side) {
+            const int b = bi[side];
+            if (b < nin) continue;
+            const double* uu = u + 6 * (long long)(b - nin);
+            double U[6];
+            for (int d = 0; d < 3; ++d) {
+                U[d] = (DIM == 2 && d == 2) ? 0.0 : v[3 * (long long)b + d] + dt * uu[d];
+                U[3 + d] = (DIM == 2 && d < 2) ? 0.0 : omega[3 * (long long)b + d] + dt * uu[3 + d];
+            }
+            const double* P = bP + 18 * c + 9 * side;
+            const double sg = side == 0 ? 1.0 : -1.0;
+            for (int d = 0; d < 3; ++d) au[d] += sg * (U[d] + P[d] * U[3] + P[3 + d] * U[4] + P[6 + d] * U[5]);
+        }
+        double dn = 0.0;
+        for (int d = 0; d < DIM; ++d) dn += au[d] * bn[3 * c + d];
+        double t2 = 0.0;
+        for (int d = 0; d < DIM; ++d) {
+            const double t = au[d] - bn[3 * c + d] * dn;
+            t2 += t * t;
+        }
+        const double snew = mu * dt * sqrt(t2);
+        const double ds = snew - sv[c];
+        s[0] += ds * ds;
+        s[1] += snew * snew;
+        sv[c] = snew;
+    }
+    block_sum(s);
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = s[0];
+        part[2 * blockIdx.x + 1] = s[1];
+    }
+}
+
 template <typename Src, typename Dst>
 __global__ void k_convert(const Src* in, Dst* out, long long n_max, const int* n_dev, int mult) {
     const long long n = n_dev ? (long long)(*n_dev) * mult : n_max;
@@ -788,6 +855,34 @@ void launch_residual64(const Bodies& b, const StepParams& p, const Contacts& c, 
         k_residual64<D, P><<<grid_blocks(c_cap), 256, 0, s>>>(b.nin, c.ci, c.cj, a.slot, a.bn, a.bai, a.baj, a.bP, a.cvec, dt2, u, g, viol_bits, sizes);
     RR(2, 0) RR(2, 1) RR(2, 2) RR(3, 0) RR(3, 1) RR(3, 2)
 #undef RR
+    g_apgd_launches += 1;
+}
+
+void launch_fixed_point_c(const StepParams& p, const Assembly& a, const double* base, const double* sv,
+                          const Sizes* sizes, long long c_cap, cudaStream_t s) {
+    if (p.dim == 3)
+        k_fixed_point_c<3><<<grid_blocks(c_cap), 256, 0, s>>>(sizes, base, a.bn, sv, a.cvec);
+    else
+        k_fixed_point_c<2><<<grid_blocks(c_cap), 256, 0, s>>>(sizes, base, a.bn, sv, a.cvec);
+    g_apgd_launches += 1;
+}
+void launch_fixed_point_init(double* sv, double v, const Sizes* sizes, long long c_cap, cudaStream_t s) {
+    k_fixed_point_init<<<grid_blocks(c_cap), 256, 0, s>>>(sizes, sv, v);
+    g_apgd_launches += 1;
+}
+int fixed_point_blocks(long long c_cap) {
+    const long long b = (c_cap + kApgdThreads - 1) / kApgdThreads;
+    return (int)std::max<long long>(1, std::min<long long>(b, kFixedPointMaxBlocks));
+}
+void launch_fixed_point_s(const Bodies& b, const StepParams& p, const Contacts& c, const Assembly& a, const double* u,
+                          double* sv, double* part, const Sizes* sizes, long long c_cap, cudaStream_t s) {
+    const int nb = fixed_point_blocks(c_cap);
+    if (p.dim == 3)
+        k_fixed_point_s<3><<<nb, kApgdThreads, 0, s>>>(sizes, b.nin, c.ci, c.cj, a.bn, a.bP, b.v, b.omega, u, p.dt,
+                                                       p.mu, sv, part);
+    else
+        k_fixed_point_s<2><<<nb, kApgdThreads, 0, s>>>(sizes, b.nin, c.ci, c.cj, a.bn, a.bP, b.v, b.omega, u, p.dt,
+                                                       p.mu, sv, part);
     g_apgd_launches += 1;
 }
 

@@ -166,6 +166,16 @@ void launch_particle_pass64(const Bodies& b, const StepParams& p, const Contacts
 // g = dt^2 B u + c and the violation max(0, -min gap) (bits of a non-negative double in *viol_bits).
 void launch_residual64(const Bodies& b, const StepParams& p, const Contacts& c, const Assembly& a, const double* u,
                        double* g, unsigned long long* viol_bits, const Sizes* sizes, long long c_cap, cudaStream_t s);
+// FrictionFixedPoint: cvec = base + s n (dim components), and the s update after a solve
+// (u = M^-1 B^T l of the active bodies) with per-block partial sums (2 per block,
+// fixed_point_blocks(c_cap) blocks, at most kFixedPointMaxBlocks) of (s_new - s_old)^2, s_new^2.
+constexpr int kFixedPointMaxBlocks = 1024;
+int fixed_point_blocks(long long c_cap);
+void launch_fixed_point_init(double* sv, double v, const Sizes* sizes, long long c_cap, cudaStream_t s);
+void launch_fixed_point_c(const StepParams& p, const Assembly& a, const double* base, const double* sv,
+                          const Sizes* sizes, long long c_cap, cudaStream_t s);
+void launch_fixed_point_s(const Bodies& b, const StepParams& p, const Contacts& c, const Assembly& a, const double* u,
+                          double* sv, double* part, const Sizes* sizes, long long c_cap, cudaStream_t s);
 // lambda64 += delta (FP32 or FP64) then projection onto the cone / orthant in FP64.
 template <typename TD>
 void launch_accumulate(const StepParams& p, const Contacts& c, const Assembly& a, double* lam64, const TD* delta,

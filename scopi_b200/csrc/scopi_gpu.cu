@@ -107,6 +107,12 @@ struct scopi_gpu_handle {
     ApgdResult* h_result = nullptr;    // pinned
     unsigned long long* h_viol = nullptr;
     int max_blocks64 = 0, max_blocks32 = 0, max_sph64 = 0, max_sph32 = 0;
+    // FrictionFixedPoint: P.problem holds FRICTION (the kernels' problem), this flag the loop
+    bool fixed_point = false;
+    double* d_cvec_base = nullptr;  // 3C: the Friction linear term of the step
+    double* d_fp_s = nullptr;       // C: s_c
+    double* d_fp_part = nullptr;    // 2 per block of the s update
+    double* h_fp_part = nullptr;    // pinned copy
 
     // results of the last step
     const double* last_lambda = nullptr;
@@ -446,6 +452,12 @@ struct scopi_gpu_handle {
         if ((e = cudaMallocHost(&h_result, sizeof(ApgdResult))) != cudaSuccess) return cuda_fail(e, "cudaMallocHost");
         if ((e = cudaMallocHost(&h_viol, sizeof(unsigned long long))) != cudaSuccess)
             return cuda_fail(e, "cudaMallocHost");
+        if (fixed_point) {
+            if ((e = alloc(fixed_mem, d_fp_part, 2 * (size_t)kFixedPointMaxBlocks)) != cudaSuccess)
+                return cuda_fail(e, "alloc");
+            if ((e = cudaMallocHost(&h_fp_part, 2 * sizeof(double) * kFixedPointMaxBlocks)) != cudaSuccess)
+                return cuda_fail(e, "cudaMallocHost");
+        }
         for (auto& x : ev)
             if ((e = cudaEventCreate(&x)) != cudaSuccess) return cuda_fail(e, "cudaEventCreate");
         for (auto& x : ev_a)
@@ -505,6 +517,9 @@ struct scopi_gpu_handle {
         A(as.bn, 3 * cap) A(as.bai, 3 * cap) A(as.baj, 3 * cap)
         if (P.problem == SCOPI_GPU_FRICTION) A(as.bP, 18 * cap)
         A(as.cvec, (P.problem == SCOPI_GPU_FRICTION ? 3 : 1) * cap) A(as.vflag, cap) A(as.slot, cap)
+        if (fixed_point) {
+            A(d_cvec_base, 3 * cap) A(d_fp_s, cap)
+        }
         A(inc.idx, 2 * cap) A(inc.coef, 12 * cap)
         for (int k = 0; k < 3; ++k) A(d_lam64[k], M)
         A(d_g64, M) A(d_res64, M) A(d_lamacc, M)
@@ -714,6 +729,7 @@ struct scopi_gpu_handle {
         const double* ufin = nullptr;
         int ustride = 6, urot = 1;
         stats.iterations = stats.backtracks = stats.restarts = stats.fp32_iterations = stats.corrections = 0;
+        stats.fixed_point_iterations = 0;
         stats.converged = 1;
         stats.status = 0;
         stats.violation = 0.0;
@@ -726,7 +742,9 @@ struct scopi_gpu_handle {
                 ustride = 4;
                 urot = 0;
             }
+            auto solve = [&]() -> int {
             if (!mixed()) {
+                float ms = 0.0f;
                 cudaEventRecord(ev_a[0], stream);
                 if (sphere_mode()) {
                     SphSolve<double> sb = sph_buffers<double>(d_nc64, d_incv64, d_imt64, d_lam64, d_us64);
@@ -758,14 +776,54 @@ struct scopi_gpu_handle {
                 }
                 cudaEventRecord(ev_a[1], stream);
                 cudaEventSynchronize(ev_a[1]);
-                cudaEventElapsedTime(&ms_apgd, ev_a[0], ev_a[1]);
+                cudaEventElapsedTime(&ms, ev_a[0], ev_a[1]);
+                ms_apgd += ms;
                 accumulate_stats(false);
                 last_lambda = d_lam64[h_result->lam_buf];
             } else {
-                rc = mixed_solve(dt, M, ms_apgd);
+                float ms = 0.0f;
+                rc = mixed_solve(dt, M, ms);
                 if (rc) return rc;
+                ms_apgd += ms;
                 last_lambda = d_lamacc;
                 ufin = sphere_mode() ? reinterpret_cast<const double*>(d_usfin) : d_ufin;
+            }
+            return 0;
+            };
+            if (fixed_point) {
+                // FrictionFixedPoint (OptimGradient.hpp:85-176, solver.hpp:286-291): s_c = mu dt,
+                // then solve with the linear term c + s n, update s from the tangential relative
+                // velocity, until the relative change of s is below fixed_point_tol
+                cudaMemcpyAsync(d_cvec_base, as.cvec, 3 * (size_t)C * sizeof(double), cudaMemcpyDeviceToDevice,
+                                stream);
+                const double mudt = P.mu * dt;
+                launch_fixed_point_init(d_fp_s, mudt, d_sizes_cur, c_cap, stream);
+                const int nbk = fixed_point_blocks(c_cap);
+                long long it = 0;
+                for (;;) {
+                    launch_fixed_point_c(sp, as, d_cvec_base, d_fp_s, d_sizes_cur, c_cap, stream);
+                    rc = solve();
+                    if (rc) return rc;
+                    launch_fixed_point_s(b, sp, cur, as, ufin, d_fp_s, d_fp_part, d_sizes_cur, c_cap, stream);
+                    cudaMemcpyAsync(h_fp_part, d_fp_part, 2 * sizeof(double) * nbk, cudaMemcpyDeviceToHost, stream);
+                    cudaError_t e = cudaStreamSynchronize(stream);
+                    if (e != cudaSuccess) return cuda_fail(e, "fixed point");
+                    double dd = 0.0, ss = 0.0;
+                    for (int k = 0; k < nbk; ++k) {
+                        dd += h_fp_part[2 * k];
+                        ss += h_fp_part[2 * k + 1];
+                    }
+                    ++it;
+                    // mu dt = 0: s stays 0 and one solve is the answer (the reference's
+                    // normalisation by 1/(mu dt) would give NaN and run fixed_point_max_iter solves)
+                    if (!(mudt > 0.0)) break;
+                    const double err = (std::sqrt(dd) / mudt) / (1.0 + std::sqrt(ss) / mudt);
+                    if (err < P.fixed_point_tol || it >= P.fixed_point_max_iter) break;
+                }
+                stats.fixed_point_iterations = it;
+            } else {
+                rc = solve();
+                if (rc) return rc;
             }
             // violation of the returned multipliers (FP64 residual)
             cudaMemsetAsync(d_viol, 0, sizeof(unsigned long long), stream);
@@ -988,6 +1046,8 @@ void scopi_gpu_default_params(scopi_gpu_params* p, int32_t dim) {
     p->mixed_max_corrections = 3;
     p->device = 0;
     p->initial_step = SCOPI_GPU_STEP_AUTO;
+    p->fixed_point_tol = 1e-6;
+    p->fixed_point_max_iter = 1000;
 }
 
 int32_t scopi_gpu_create(const scopi_gpu_params* p, scopi_gpu_handle** out) {
@@ -1000,8 +1060,9 @@ int32_t scopi_gpu_create(const scopi_gpu_params* p, scopi_gpu_handle** out) {
         scopi_gpu::set_global_error("dim must be 2 or 3");
         return SCOPI_GPU_EINVAL;
     }
-    if (p->problem < 0 || p->problem > 2 || p->vap < 0 || p->vap > 1 || p->contact_method < 0 ||
-        p->contact_method > 1 || p->precision < 0 || p->precision > 1 || p->alpha <= 0 || p->max_ite < 1) {
+    if (p->problem < 0 || p->problem > 3 || p->vap < 0 || p->vap > 1 || p->contact_method < 0 ||
+        p->contact_method > 1 || p->precision < 0 || p->precision > 1 || p->alpha <= 0 || p->max_ite < 1 ||
+        (p->problem == SCOPI_GPU_FRICTION_FIXED_POINT && (!(p->fixed_point_tol >= 0) || p->fixed_point_max_iter < 1))) {
         scopi_gpu::set_global_error("invalid parameter");
         return SCOPI_GPU_EINVAL;
     }
@@ -1013,6 +1074,10 @@ int32_t scopi_gpu_create(const scopi_gpu_params* p, scopi_gpu_handle** out) {
     }
     auto* h = new scopi_gpu_handle();
     h->P = *p;
+    if (p->problem == SCOPI_GPU_FRICTION_FIXED_POINT) {
+        h->fixed_point = true;
+        h->P.problem = SCOPI_GPU_FRICTION;  // the Friction problem plus the s term and the loop
+    }
     h->dev = p->device;
     cudaSetDevice(h->dev);
     if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess) {
@@ -1043,6 +1108,7 @@ int32_t scopi_gpu_destroy(scopi_gpu_handle* h) {
     if (h->h_sizes) cudaFreeHost(h->h_sizes);
     if (h->h_result) cudaFreeHost(h->h_result);
     if (h->h_viol) cudaFreeHost(h->h_viol);
+    if (h->h_fp_part) cudaFreeHost(h->h_fp_part);
     for (auto& x : h->ev)
         if (x) cudaEventDestroy(x);
     for (auto& x : h->ev_a)

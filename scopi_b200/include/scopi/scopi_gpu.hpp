@@ -79,6 +79,7 @@ inline type::quaternion_t mult_quaternion(const type::quaternion_t& a, const typ
 class NoFriction {};
 class Friction {};
 class Viscous {};
+class FrictionFixedPoint {};  // property.hpp:26
 
 template <class problem_t>
 struct contact_property;
@@ -94,11 +95,17 @@ struct contact_property<Viscous> {
     double gamma_min = -2.;
     double gamma_tol = 1e-6;
 };
+template <>
+struct contact_property<FrictionFixedPoint> : contact_property<Friction> {  // property.hpp:84-96,131-147
+    double fixed_point_tol = 1e-6;
+    double fixed_point_max_iter = 1000;
+};
 
 template <class problem_t>
 constexpr int32_t problem_code() {
     if constexpr (std::is_same_v<problem_t, Friction>) return SCOPI_GPU_FRICTION;
     if constexpr (std::is_same_v<problem_t, Viscous>) return SCOPI_GPU_VISCOUS;
+    if constexpr (std::is_same_v<problem_t, FrictionFixedPoint>) return SCOPI_GPU_FRICTION_FIXED_POINT;
     return SCOPI_GPU_NOFRICTION;
 }
 
@@ -582,6 +589,11 @@ class ScopiSolver {
         if constexpr (std::is_same_v<contact_method_t, gpu::contact_kdtree<problem_t>>)
             p.kd_tree_radius = m_contact_params.kd_tree_radius;
         if constexpr (std::is_same_v<problem_t, Friction>) p.mu = m_default_property.mu;
+        if constexpr (std::is_same_v<problem_t, FrictionFixedPoint>) {
+            p.mu = m_default_property.mu;
+            p.fixed_point_tol = m_default_property.fixed_point_tol;
+            p.fixed_point_max_iter = (int64_t)m_default_property.fixed_point_max_iter;
+        }
         if constexpr (std::is_same_v<problem_t, Viscous>) {
             p.gamma = m_default_property.gamma;
             p.gamma_min = m_default_property.gamma_min;

@@ -18,8 +18,8 @@ from types import SimpleNamespace
 import numpy as np
 
 from . import _abi
-from ._abi import (BRUTE_FORCE, FP64, FRICTION, KDTREE, MIXED, NOFRICTION, VAP_FIXED, VAP_FPD,  # noqa: F401
-                   VISCOUS)
+from ._abi import (BRUTE_FORCE, FP64, FRICTION, FRICTION_FIXED_POINT, KDTREE, MIXED, NOFRICTION,  # noqa: F401
+                   VAP_FIXED, VAP_FPD, VISCOUS)
 from .container import ParticleArrays
 
 
@@ -64,7 +64,9 @@ class ScopiSolver:
             optim_params=_ParamGroup(alpha=p.alpha, max_ite=p.max_ite, tolerance=p.tolerance,
                                      dynamic_descent=bool(p.dynamic_descent)),
             contact_method_params=_ParamGroup(dmax=p.dmax, kd_tree_radius=p.kd_tree_radius),
-            default_contact_property=_ParamGroup(mu=p.mu, gamma=p.gamma, gamma_min=p.gamma_min, gamma_tol=p.gamma_tol),
+            default_contact_property=_ParamGroup(mu=p.mu, gamma=p.gamma, gamma_min=p.gamma_min, gamma_tol=p.gamma_tol,
+                                                 fixed_point_tol=p.fixed_point_tol,
+                                                 fixed_point_max_iter=p.fixed_point_max_iter),
         )
 
     def set_params(self, **kw):

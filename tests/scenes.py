@@ -270,3 +270,39 @@ def critical_2d_superellipsoids():
                                               desired_velocity=(vel if side == 0 else -vel, 0.0)),
                                      q=quaternion(rot))
     return p.finalize(), dict(vap=VAP_FIXED, contact_method=KDTREE), 0.01, 20
+
+
+def sphere_plane_fixed_point():
+    """test/test_gradient.cpp:215-283: FrictionFixedPoint, sphere on plane(pi/2) under tilted gravity
+    g(sin a, -cos a), a = pi/4, mu 0.5, fixed point tol 1e-6 / 1000, dt 0.01, 500 steps, vap_fpd."""
+    radius, g, h, alpha = 1.0, 1.0, 2.0, PI / 4
+    p = Particles(2)
+    p.add_plane((0.0, 0.0), PI / 2)
+    p.add_sphere((0.0, h), radius, Property(mass=1, moment_inertia=radius * radius / 2.0,
+                                            force=(g * math.sin(alpha), -g * math.cos(alpha))))
+    kw = dict(problem=3, vap=VAP_FPD, tolerance=1e-7, max_ite=10000, alpha=0.01, mu=0.5, fixed_point_tol=1e-6,
+              fixed_point_max_iter=1000)
+    return p.finalize(), kw, 0.01, 500
+
+
+def analytic_friction(alpha, mu, t, r, g, y0):
+    """test/analytical_solution.cpp:130-187: position, angle, velocity and angular velocity of the
+    sphere on the plane under tilted gravity, with friction mu."""
+    t_imp = math.sqrt(2 * (y0 - r) / (g * math.cos(alpha)))
+    sa, ca = math.sin(alpha), math.cos(alpha)
+    if t <= t_imp:
+        return (g * t * t * sa / 2, -g * t * t * ca / 2 + y0), 0.0, (g * t * sa, -g * t * ca), 0.0
+    vtm, vnm = g * t_imp * sa, -g * t_imp * ca
+    t2 = t - t_imp
+    x_imp = g * t_imp * t_imp * sa / 2
+    if math.tan(alpha) <= 3 * mu:
+        x = g * sa * t2 * t2 / 3.0 + 2.0 * vtm * t2 / 3.0 + x_imp
+        theta = -g * sa * t2 * t2 / (3.0 * r) - 2 * vtm * t2 / (3.0 * r)
+        v = 2.0 * g * sa * t2 / 3.0 + 2.0 * vtm / 3.0
+        om = -2.0 * g * sa * t2 / (3.0 * r) - 2 * vtm / (3.0 * r)
+    else:
+        x = g * (sa - mu * ca) * t2 * t2 / 2.0 + (vtm + mu * vnm) * t2 + x_imp
+        theta = -mu * g * ca * t2 * t2 / r + 2 * mu * vnm * t2 / r
+        v = g * (sa - mu * ca) * t2 + (vtm + mu * vnm)
+        om = -2.0 * mu * g * ca * t2 / r + 2 * mu * vnm / r
+    return (x, r), theta, (v, 0.0), om

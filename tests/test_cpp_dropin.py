@@ -48,9 +48,10 @@ def test_cpp_api_matches_reference_golden(exe, golden, mode, name):
 
 SE_SRC = os.path.join(ROOT, "tests", "cpp", "superellipsoids_dropin.cpp")
 SE2_SRC = os.path.join(ROOT, "tests", "cpp", "two_ellipsoids_dropin.cpp")
+FP_SRC = os.path.join(ROOT, "tests", "cpp", "fixed_point_dropin.cpp")
 
 
-@pytest.mark.parametrize("src", [SE_SRC, SE2_SRC])
+@pytest.mark.parametrize("src", [SE_SRC, SE2_SRC, FP_SRC])
 def test_superellipsoid_header_compiles(src):
     subprocess.run([GXX, "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", *INC, src], check=True)
 
@@ -128,3 +129,32 @@ def test_cpp_superellipsoid_pile_matches_python_api_and_oracle(se_exe, tmp_path)
     oc = o.contacts()
     assert [tuple(c) for c in res["contacts"]] == list(zip(oc["i"].tolist(), oc["j"].tolist()))
     assert rel_err(pos, o.pa.pos) <= 2e-5
+
+
+@pytest.fixture(scope="module")
+def fp_exe(tmp_path_factory):
+    from scopi_b200 import build
+    build.build()
+    out = str(tmp_path_factory.mktemp("cpp") / "fixed_point")
+    lib = os.path.join(ROOT, "scopi_b200")
+    subprocess.run([GXX, "-O2", "-std=c++17", *INC, FP_SRC, "-L", lib, "-lscopi_gpu", f"-Wl,-rpath,{lib}", "-o", out],
+                   check=True)
+    return out
+
+
+@pytest.mark.gpu
+def test_cpp_friction_fixed_point_matches_analytic(fp_exe):
+    """test/test_gradient.cpp:215-283 through the C++ API: errors against the analytic rolling
+    solution within the reference's bounds (pos, q 1e-2; v, omega 1e-12 under doctest::Approx)."""
+    import math
+
+    import scenes as S
+    res = json.loads(subprocess.run([fp_exe], check=True, capture_output=True, text=True).stdout)
+    x, theta, v, om = S.analytic_friction(math.pi / 4, 0.5, 0.01 * 500, 1.0, 1.0, 2.0)
+    qa = S.quaternion(theta)
+    e_pos = math.hypot(res["position"][0] - x[0], res["position"][1] - x[1]) / math.hypot(*x)
+    e_q = math.sqrt(sum((a - b) ** 2 for a, b in zip(res["quaternion"], qa))) / math.sqrt(sum(b * b for b in qa))
+    e_v = math.hypot(res["velocity"][0] - v[0], res["velocity"][1] - v[1]) / math.hypot(*v)
+    e_om = (res["omega"] - om) ** 2 / om ** 2
+    assert e_pos <= 1e-2 and e_q <= 1e-2, (e_pos, e_q)
+    assert e_v <= 1.2e-5 and e_om <= 1.2e-5, (e_v, e_om)

@@ -256,3 +256,24 @@ def test_initial_step_choices(precision, init):
     if init == 1:
         assert sa["iterations"] < sr["iterations"] / 4, (sa, sr)
     assert rel_err(alt.particles.pos, ref.particles.pos) <= 1e-7
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_friction_fixed_point_sphere_plane(precision):
+    """FrictionFixedPoint on the reference's analytic case (test/test_gradient.cpp:215-283):
+    the reference's error bounds against the rolling solution, and (FP64) the oracle's
+    trajectory, which runs the same fixed-point loop."""
+    import math
+
+    from test_oracle_golden import fixed_point_errors
+    pa, kw, dt, total = S.sphere_plane_fixed_point()
+    g = gpu_solver(pa, precision=precision, **kw).run(dt, total)
+    e_pos, e_q, e_v, e_om = fixed_point_errors(g.particles, dt, total)
+    assert e_pos <= 1e-2 and e_q <= 1e-2, (e_pos, e_q)
+    assert e_v <= 1.2e-5 and e_om <= 1.2e-5, (e_v, e_om)
+    assert g.stats()["fixed_point_iterations"] >= 2
+    if precision == 0:
+        o = oracle_solver(pa, **kw).run(dt, total)
+        assert rel_err(g.particles.pos, o.pa.pos) <= 1e-7
+        assert rel_err(g.particles.v, o.pa.v) <= 1e-5
+        assert math.isclose(g.particles.omega[1, 2], o.pa.omega[1, 2], rel_tol=1e-5)

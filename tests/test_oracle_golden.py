@@ -194,3 +194,27 @@ def test_sphere_plane_viscous_analytic():
     assert np.linalg.norm(s.pa.pos[1, :2] - x) / np.linalg.norm(x) <= 1e-3
     assert np.linalg.norm(s.pa.v[1, :2] - v) / np.linalg.norm(v) <= 1e-3
     assert approx(s.pa.omega[1, 2], 0.0)
+
+
+def fixed_point_errors(pa, dt, total):
+    """Errors of test/test_gradient.cpp:264-283 (relative norms; omega with std::norm, i.e. squared)."""
+    x, theta, v, om = S.analytic_friction(math.pi / 4, 0.5, dt * total, 1.0, 1.0, 2.0)
+    qa = S.quaternion(theta)
+    e_pos = math.hypot(pa.pos[1, 0] - x[0], pa.pos[1, 1] - x[1]) / math.hypot(*x)
+    e_q = float(np.linalg.norm(pa.q[1] - qa) / np.linalg.norm(qa))
+    e_v = math.hypot(pa.v[1, 0] - v[0], pa.v[1, 1] - v[1]) / math.hypot(*v)
+    e_om = (pa.omega[1, 2] - om) ** 2 / om ** 2
+    return e_pos, e_q, e_v, e_om
+
+
+def test_sphere_plane_friction_fixed_point_analytic():
+    """test/test_gradient.cpp:215-283 (FrictionFixedPoint): pos and q within 1e-2 of the
+    analytic rolling solution, v and omega within doctest::Approx of 1e-12."""
+    pa, kw, dt, total = S.sphere_plane_fixed_point()
+    s = orc.OracleSolver(pa, **kw)
+    s.run(dt, total)
+    e_pos, e_q, e_v, e_om = fixed_point_errors(s.pa, dt, total)
+    assert e_pos <= 1e-2 and e_q <= 1e-2, (e_pos, e_q)
+    assert approx(e_v, 1e-12) or e_v <= 1e-12, e_v
+    assert approx(e_om, 1e-12) or e_om <= 1e-12, e_om
+    assert s.stats()["fixed_point_iterations"] >= 2
