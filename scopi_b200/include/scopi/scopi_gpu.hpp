@@ -25,11 +25,16 @@
 // arithmetic) or gpu::apgd<gpu::mixed> (FP32 iterations + FP64 outer correction).
 #pragma once
 
+#include <algorithm>
 #include <array>
 #include <cmath>
 #include <cstddef>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <filesystem>
+#include <fstream>
+#include <utility>
 #include <initializer_list>
 #include <iostream>
 #include <stdexcept>
@@ -246,6 +251,163 @@ class property {
     bool m_active = true;
 };
 
+// ------------------------------------------------------------------ snapshot documents
+// A small document tree for the snapshot files of ScopiSolver::write_output_files
+// (solver.hpp:368-438): objects keep their keys sorted (the order the reference's JSON
+// library writes), written as indented JSON or as BSON.
+namespace io {
+struct Value {
+    enum Kind { Null, Bool, Int, Double, String, Array, Object } kind = Null;
+    bool b = false;
+    int64_t i = 0;
+    double d = 0.0;
+    std::string s;
+    std::vector<Value> items;                             // Array
+    std::vector<std::pair<std::string, Value>> fields;    // Object, sorted by key
+
+    static Value boolean(bool v) { Value x; x.kind = Bool; x.b = v; return x; }
+    static Value integer(int64_t v) { Value x; x.kind = Int; x.i = v; return x; }
+    static Value number(double v) { Value x; x.kind = Double; x.d = v; return x; }
+    static Value string(std::string v) { Value x; x.kind = String; x.s = std::move(v); return x; }
+    static Value array() { Value x; x.kind = Array; return x; }
+    static Value object() { Value x; x.kind = Object; return x; }
+    static Value numbers(const double* v, std::size_t n) {
+        Value x = array();
+        for (std::size_t k = 0; k < n; ++k) x.items.push_back(number(v[k]));
+        return x;
+    }
+    Value& set(const std::string& key, Value v) {
+        auto it = std::lower_bound(fields.begin(), fields.end(), key,
+                                   [](const std::pair<std::string, Value>& f, const std::string& k) { return f.first < k; });
+        if (it != fields.end() && it->first == key)
+            it->second = std::move(v);
+        else
+            fields.insert(it, {key, std::move(v)});
+        return *this;
+    }
+};
+
+// shortest decimal that reads back to the same double; integral values keep a ".0"
+inline std::string format_double(double v) {
+    if (!std::isfinite(v)) return "null";
+    char buf[40];
+    for (int prec = 15; prec <= 17; ++prec) {
+        std::snprintf(buf, sizeof(buf), "%.*g", prec, v);
+        if (std::strtod(buf, nullptr) == v) break;
+    }
+    std::string out(buf);
+    if (out.find_first_of(".eE") == std::string::npos) out += ".0";
+    return out;
+}
+inline void write_json(std::ostream& o, const Value& v, int indent = 0) {
+    const std::string pad(indent + 4, ' '), end(indent, ' ');
+    switch (v.kind) {
+        case Value::Null: o << "null"; break;
+        case Value::Bool: o << (v.b ? "true" : "false"); break;
+        case Value::Int: o << v.i; break;
+        case Value::Double: o << format_double(v.d); break;
+        case Value::String: o << '"' << v.s << '"'; break;
+        case Value::Array:
+            if (v.items.empty()) {
+                o << "[]";
+                break;
+            }
+            o << "[\n";
+            for (std::size_t k = 0; k < v.items.size(); ++k) {
+                o << pad;
+                write_json(o, v.items[k], indent + 4);
+                o << (k + 1 < v.items.size() ? ",\n" : "\n");
+            }
+            o << end << ']';
+            break;
+        case Value::Object:
+            if (v.fields.empty()) {
+                o << "{}";
+                break;
+            }
+            o << "{\n";
+            for (std::size_t k = 0; k < v.fields.size(); ++k) {
+                o << pad << '"' << v.fields[k].first << "\": ";
+                write_json(o, v.fields[k].second, indent + 4);
+                o << (k + 1 < v.fields.size() ? ",\n" : "\n");
+            }
+            o << end << '}';
+            break;
+    }
+}
+// BSON (bsonspec.org): int32/int64 by range, double, UTF-8 string, embedded documents;
+// arrays are documents keyed "0", "1", ...
+inline void bson_put(std::vector<uint8_t>& b, const void* p, std::size_t n) {
+    const uint8_t* c = static_cast<const uint8_t*>(p);
+    b.insert(b.end(), c, c + n);  // little-endian hosts (x86-64, aarch64)
+}
+inline void bson_document(std::vector<uint8_t>& b, const Value& v);
+inline void bson_element(std::vector<uint8_t>& b, const std::string& key, const Value& v) {
+    uint8_t type = 0x0A;
+    switch (v.kind) {
+        case Value::Null: type = 0x0A; break;
+        case Value::Bool: type = 0x08; break;
+        case Value::Int: type = (v.i >= INT32_MIN && v.i <= INT32_MAX) ? 0x10 : 0x12; break;
+        case Value::Double: type = 0x01; break;
+        case Value::String: type = 0x02; break;
+        case Value::Array: type = 0x04; break;
+        case Value::Object: type = 0x03; break;
+    }
+    b.push_back(type);
+    bson_put(b, key.c_str(), key.size() + 1);
+    switch (v.kind) {
+        case Value::Null: break;
+        case Value::Bool: b.push_back(v.b ? 1 : 0); break;
+        case Value::Int:
+            if (type == 0x10) {
+                const int32_t x = (int32_t)v.i;
+                bson_put(b, &x, 4);
+            } else {
+                bson_put(b, &v.i, 8);
+            }
+            break;
+        case Value::Double: bson_put(b, &v.d, 8); break;
+        case Value::String: {
+            const int32_t n = (int32_t)v.s.size() + 1;
+            bson_put(b, &n, 4);
+            bson_put(b, v.s.c_str(), v.s.size() + 1);
+            break;
+        }
+        case Value::Array:
+        case Value::Object: bson_document(b, v); break;
+    }
+}
+inline void bson_document(std::vector<uint8_t>& b, const Value& v) {
+    const std::size_t start = b.size();
+    b.resize(start + 4);
+    if (v.kind == Value::Array)
+        for (std::size_t k = 0; k < v.items.size(); ++k) bson_element(b, std::to_string(k), v.items[k]);
+    else
+        for (const auto& f : v.fields) bson_element(b, f.first, f.second);
+    b.push_back(0);
+    const int32_t n = (int32_t)(b.size() - start);
+    std::copy(reinterpret_cast<const uint8_t*>(&n), reinterpret_cast<const uint8_t*>(&n) + 4, b.begin() + start);
+}
+inline std::vector<uint8_t> to_bson(const Value& v) {
+    std::vector<uint8_t> b;
+    bson_document(b, v);
+    return b;
+}
+
+// rotation_matrix<dim>(q), quaternion.hpp:66-124 (q = (w, x, y, z)), row-major
+template <std::size_t dim>
+inline std::array<double, dim * dim> rotation(const type::quaternion_t& q) {
+    const double x = q[0], y = q[1], z = q[2], w = q[3];
+    if constexpr (dim == 2) {
+        return {1 - 2 * w * w, -2 * x * w, 2 * x * w, 1 - 2 * w * w};
+    } else {
+        return {1 - 2 * z * z - 2 * w * w, 2 * y * z - 2 * x * w,     2 * y * w + 2 * x * z,
+                2 * y * z + 2 * x * w,     1 - 2 * y * y - 2 * w * w, 2 * z * w - 2 * x * y,
+                2 * y * w - 2 * x * z,     2 * z * w + 2 * x * y,     1 - 2 * y * y - 2 * z * z};
+    }
+}
+}  // namespace io
+
 // ------------------------------------------------------------------ container
 template <std::size_t dim>
 class vec_ref {
@@ -357,6 +519,72 @@ class scopi_container {
         return p;
     }
 
+    // The "objects" array of a snapshot: write_objects.hpp (per shape) and the properties
+    // written by write_output_files (solver.hpp:383-400).
+    io::Value snapshot_objects() const {
+        using io::Value;
+        Value out = Value::array();
+        for (std::size_t i = 0; i < size(); ++i) {
+            const double* x = &m_pos[3 * i];
+            type::quaternion_t q = {m_q[4 * i], m_q[4 * i + 1], m_q[4 * i + 2], m_q[4 * i + 3]};
+            const auto R = io::rotation<dim>(q);
+            Value o = Value::object();
+            o.set("id", Value::integer((int64_t)i));
+            o.set("quaternion", Value::numbers(q.data(), 4));
+            double col0[dim];
+            for (std::size_t d = 0; d < dim; ++d) col0[d] = R[d * dim];
+            switch (m_shape[i]) {
+                case SCOPI_GPU_PLANE:
+                    o.set("type", Value::string("plane"));
+                    o.set("position", Value::numbers(x, dim));
+                    o.set("normal", Value::numbers(col0, dim));
+                    o.set("rotation", Value::numbers(R.data(), dim * dim));
+                    break;
+                case SCOPI_GPU_SEGMENT: {
+                    o.set("type", Value::string("segment"));
+                    const double t[2] = {-col0[1], col0[0]};
+                    const double h = 0.5 * m_length[i];
+                    // extrema: R (0, -+L/2) + centre (segment.hpp:168-177)
+                    const double p1[2] = {R[1] * -h + x[0], R[3] * -h + x[1]};
+                    const double p2[2] = {R[1] * h + x[0], R[3] * h + x[1]};
+                    o.set("p1", Value::numbers(p1, 2));
+                    o.set("p2", Value::numbers(p2, 2));
+                    o.set("normal", Value::numbers(col0, 2));
+                    o.set("tangent", Value::numbers(t, 2));
+                    break;
+                }
+                case SCOPI_GPU_SUPERELLIPSOID:
+                    o.set("type", Value::string("superellipsoid"));
+                    o.set("position", Value::numbers(x, dim));
+                    o.set("radius", Value::numbers(&m_axes[3 * i], dim));
+                    o.set("squareness", Value::numbers(&m_sq[2 * i], dim - 1));
+                    o.set("rotation", Value::numbers(R.data(), dim * dim));
+                    break;
+                default:
+                    o.set("type", Value::string("sphere"));
+                    o.set("position", Value::numbers(x, dim));
+                    o.set("radius", Value::number(m_radius[i]));
+                    o.set("rotation", Value::numbers(R.data(), dim * dim));
+                    break;
+            }
+            auto rot = [&](const std::vector<double>& a) {
+                return dim == 2 ? Value::number(a[3 * i + 2]) : Value::numbers(&a[3 * i], 3);
+            };
+            Value pr = Value::object();
+            pr.set("velocity", Value::numbers(&m_v[3 * i], dim));
+            pr.set("desired_velocity", Value::numbers(&m_vd[3 * i], dim));
+            pr.set("omega", rot(m_w));
+            pr.set("desired_omega", rot(m_dw));
+            pr.set("force", Value::numbers(&m_f[3 * i], dim));
+            pr.set("mass", Value::number(m_m[i]));
+            pr.set("moment_inertia", rot(m_j));
+            pr.set("active", Value::boolean(i >= m_nb_inactive));
+            o.set("properties", std::move(pr));
+            out.items.push_back(std::move(o));
+        }
+        return out;
+    }
+
   private:
     template <class V>
     static void append3(std::vector<double>& dst, const V& v) {
@@ -465,7 +693,7 @@ using ContactsParams = gpu::ContactsParams<D>;
 using vap_fixed = gpu::vap_fixed;
 using vap_fpd = gpu::vap_fpd;
 
-struct ScopiParams {  // params.hpp:89-134 (output is not produced by the GPU engine)
+struct ScopiParams {  // params.hpp:89-134 (snapshot files: ScopiSolver::write_output_files)
     std::size_t output_frequency = std::size_t(-1);
     std::filesystem::path path = "Results";
     std::string filename = "scopi_objects";
@@ -512,15 +740,76 @@ class ScopiSolver {
     }
 
     // ScopiSolver::run (solver.hpp:267-303): the container is uploaded, the steps run on
-    // the GPU, and positions, quaternions and velocities are copied back.
+    // the GPU, and positions, quaternions and velocities are copied back.  Snapshot files as
+    // the reference writes them: one at the start (index initial_iter, with the contacts of
+    // the previous step), then after every step nite with (nite + 1) % output_frequency == 0
+    // (index nite + 1); the steps between two snapshots run on the GPU in one call.
     void run(double dt, std::size_t total_it, std::size_t initial_iter = 0) {
         ensure();
         scopi_gpu_particles p = m_particles.abi();
         check(scopi_gpu_set_particles(m_h, &p), "set_particles");
-        const int32_t rc = scopi_gpu_run(m_h, dt, (int64_t)total_it, (int64_t)initial_iter);
-        if (rc < 0) check(rc, "run");
-        if (rc == SCOPI_GPU_ENOCONV) std::cerr << "APGD didn't converge." << std::endl;
+        write_output_files(initial_iter);
+        const std::size_t freq = m_params.output_frequency;
+        std::size_t nite = initial_iter;
+        bool noconv = false;
+        while (nite < total_it) {
+            std::size_t end = total_it;
+            if (freq != std::size_t(-1) && freq > 0) end = std::min(total_it, (nite / freq + 1) * freq);
+            const int32_t rc = scopi_gpu_run(m_h, dt, (int64_t)end, (int64_t)nite);
+            if (rc < 0) check(rc, "run");
+            noconv = noconv || rc == SCOPI_GPU_ENOCONV;
+            nite = end;
+            if (freq != std::size_t(-1) && freq > 0 && nite % freq == 0) {
+                check(scopi_gpu_get_particles(m_h, &p), "get_particles");
+                write_output_files(nite);
+            }
+        }
+        if (noconv) std::cerr << "APGD didn't converge." << std::endl;
         check(scopi_gpu_get_particles(m_h, &p), "get_particles");
+    }
+
+    // write_output_files (solver.hpp:368-438): {path}/{filename}_{nite:04d}.json (or .bson
+    // with binary_output) holding the objects of the container and the contacts of the last
+    // step (null when there are none), each with the multiplier of the same index when
+    // write_lagrange_multiplier is set (as the reference indexes it).
+    void write_output_files(std::size_t nite) {
+        using io::Value;
+        std::filesystem::create_directories(m_params.path);
+        Value doc = Value::object();
+        doc.set("objects", m_particles.snapshot_objects());
+        const auto& cc = current_contacts();
+        std::vector<double> lam;
+        if (m_params.write_lagrange_multiplier && !cc.empty()) lam = lagrange_multiplier();
+        Value contacts;  // null without contacts
+        if (!cc.empty()) {
+            contacts = Value::array();
+            for (std::size_t k = 0; k < cc.size(); ++k) {
+                const auto& c = cc[k];
+                Value o = Value::object();
+                o.set("i", Value::integer((int64_t)c.i));
+                o.set("j", Value::integer((int64_t)c.j));
+                o.set("pi", Value::numbers(c.pi.data(), dim));
+                o.set("pj", Value::numbers(c.pj.data(), dim));
+                o.set("normal", Value::numbers(c.nij.data(), dim));
+                o.set("distance", Value::number(c.dij));
+                o.set("property", property_json(c));
+                if (m_params.write_lagrange_multiplier && k < lam.size())
+                    o.set("lagrange multiplier", Value::number(lam[k]));
+                contacts.items.push_back(std::move(o));
+            }
+        }
+        doc.set("contacts", std::move(contacts));
+        char idx[32];
+        std::snprintf(idx, sizeof(idx), "_%04zu", nite);
+        const std::string base = (m_params.path / m_params.filename).string() + idx;
+        if (m_params.binary_output) {
+            const std::vector<uint8_t> b = io::to_bson(doc);
+            std::ofstream f(base + ".bson", std::ios::out | std::ios::binary);
+            f.write(reinterpret_cast<const char*>(b.data()), (std::streamsize)b.size());
+        } else {
+            std::ofstream f(base + ".json");
+            io::write_json(f, doc);
+        }
     }
 
     // current_contacts (solver.hpp:314-317)
@@ -566,6 +855,30 @@ class ScopiSolver {
     }
 
   private:
+    // contact_property<problem_t>::to_json (property.hpp): the contact's own gamma for Viscous
+    io::Value property_json(const neighbor<dim, problem_t>& c) const {
+        using io::Value;
+        Value o = Value::object();
+        if constexpr (std::is_same_v<problem_t, Friction>) {
+            o.set("type", Value::string("friction"));
+            o.set("mu", Value::number(m_default_property.mu));
+        } else if constexpr (std::is_same_v<problem_t, FrictionFixedPoint>) {
+            o.set("type", Value::string("friction fixed point"));
+            o.set("mu", Value::number(m_default_property.mu));
+            o.set("fixed_point_tol", Value::number(m_default_property.fixed_point_tol));
+            o.set("fixed_point_max_iter", Value::number(m_default_property.fixed_point_max_iter));
+        } else if constexpr (std::is_same_v<problem_t, Viscous>) {
+            o.set("type", Value::string("viscous"));
+            o.set("gamma", Value::number(c.property.gamma));
+            o.set("gamma_min", Value::number(m_default_property.gamma_min));
+            o.set("gamma_tol", Value::number(m_default_property.gamma_tol));
+        } else {
+            (void)c;
+            o.set("type", Value::string("no friction"));
+        }
+        return o;
+    }
+
     void check(int32_t rc, const char* what) {
         if (rc < 0) throw gpu_error(std::string("scopi_gpu_") + what + ": " + scopi_gpu_last_error(m_h));
     }

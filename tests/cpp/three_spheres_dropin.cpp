@@ -1,7 +1,9 @@
 // Drop-in check: the "3 Spheres NoFriction / Viscous" scenes of the reference's solver
 // tests (test/test_gradient.cpp:377-503) written against the scopi:: API exactly as a
 // reference user writes them; only the headers differ (B200 engine through the C ABI).
-// Prints the final state as JSON for the Python side to compare with the golden files.
+// Prints the final state as JSON for the Python side to compare with the golden files; with
+// an output directory as second argument the solver also writes its snapshot files there,
+// the last one after the final step (output_frequency = total_it).
 #include <cstdio>
 #include <cstring>
 
@@ -14,7 +16,7 @@
 #include <scopi/vap/vap_fpd.hpp>
 
 template <class problem_t>
-int run(double Tf) {
+int run(double Tf, const char* outdir, const char* name) {
     constexpr std::size_t dim = 2;
     scopi::scopi_container<dim> particles;
     scopi::sphere<dim> s1({{-1.7, 1.3}}, 0.5);
@@ -32,6 +34,11 @@ int run(double Tf) {
     params.optim_params.alpha = 0.1;
     params.optim_params.dynamic_descent = true;
     std::size_t total_it = Tf / dt;
+    if (outdir) {
+        params.solver_params.output_frequency = total_it;
+        params.solver_params.path = outdir;
+        params.solver_params.filename = name;
+    }
     solver.run(dt, total_it);
     std::printf("{\"objects\": [");
     for (std::size_t i = 0; i < particles.size(); ++i) {
@@ -47,6 +54,7 @@ int run(double Tf) {
 }
 
 int main(int argc, char** argv) {
-    if (argc > 1 && std::strcmp(argv[1], "viscous") == 0) return run<scopi::Viscous>(7.0);
-    return run<scopi::NoFriction>(6.0);
+    const char* outdir = argc > 2 ? argv[2] : nullptr;
+    if (argc > 1 && std::strcmp(argv[1], "viscous") == 0) return run<scopi::Viscous>(7.0, outdir, "3spheres_viscous");
+    return run<scopi::NoFriction>(6.0, outdir, "3spheres_nofriction");
 }

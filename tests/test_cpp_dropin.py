@@ -36,8 +36,8 @@ def exe(tmp_path_factory):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("mode,name", [("nofriction", "3spheres_nofriction"), ("viscous", "3spheres_viscous")])
-def test_cpp_api_matches_reference_golden(exe, golden, mode, name):
-    res = json.loads(subprocess.run([exe, mode], check=True, capture_output=True, text=True).stdout)
+def test_cpp_api_matches_reference_golden(exe, golden, mode, name, tmp_path):
+    res = json.loads(subprocess.run([exe, mode], check=True, capture_output=True, text=True, cwd=tmp_path).stdout)
     worst = 0.0
     for got, ref in zip(res["objects"], golden[name]["objects"]):
         for key in ("position", "velocity", "omega", "quaternion"):
@@ -69,9 +69,9 @@ def se2_exe(tmp_path_factory):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("mode,tol", [("symmetrical", 1e-6), ("asymmetrical", 5e-6)])
-def test_cpp_two_ellipsoids_match_reference_golden(se2_exe, golden, mode, tol):
+def test_cpp_two_ellipsoids_match_reference_golden(se2_exe, golden, mode, tol, tmp_path):
     """test/test_superellipsoid.cpp:451-581 through the C++ API against two_ellipsoids_*.json."""
-    res = json.loads(subprocess.run([se2_exe, mode], check=True, capture_output=True, text=True).stdout)
+    res = json.loads(subprocess.run([se2_exe, mode], check=True, capture_output=True, text=True, cwd=tmp_path).stdout)
     gold = golden["two_ellipsoids_" + mode]
     worst = 0.0
     for got, ref in zip(res["objects"], gold["objects"]):
@@ -119,7 +119,7 @@ def test_cpp_superellipsoid_pile_matches_python_api_and_oracle(se_exe, tmp_path)
     steps = 4
     scene = str(tmp_path / "scene.txt")
     write_scene(scene, pa, steps, st["dt"], st["mu"], st["dmax"], kd, st["tolerance"], st["max_ite"])
-    res = json.loads(subprocess.run([se_exe, scene], check=True, capture_output=True, text=True).stdout)
+    res = json.loads(subprocess.run([se_exe, scene], check=True, capture_output=True, text=True, cwd=tmp_path).stdout)
     pos = np.array(res["positions"])
     kw = dict(dmax=st["dmax"], tolerance=st["tolerance"], max_ite=st["max_ite"], vap=st["vap"], mu=st["mu"],
               problem=FRICTION, kd_tree_radius=kd)
@@ -143,13 +143,13 @@ def fp_exe(tmp_path_factory):
 
 
 @pytest.mark.gpu
-def test_cpp_friction_fixed_point_matches_analytic(fp_exe):
+def test_cpp_friction_fixed_point_matches_analytic(fp_exe, tmp_path):
     """test/test_gradient.cpp:215-283 through the C++ API: errors against the analytic rolling
     solution within the reference's bounds (pos, q 1e-2; v, omega 1e-12 under doctest::Approx)."""
     import math
 
     import scenes as S
-    res = json.loads(subprocess.run([fp_exe], check=True, capture_output=True, text=True).stdout)
+    res = json.loads(subprocess.run([fp_exe], check=True, capture_output=True, text=True, cwd=tmp_path).stdout)
     x, theta, v, om = S.analytic_friction(math.pi / 4, 0.5, 0.01 * 500, 1.0, 1.0, 2.0)
     qa = S.quaternion(theta)
     e_pos = math.hypot(res["position"][0] - x[0], res["position"][1] - x[1]) / math.hypot(*x)
@@ -158,3 +158,105 @@ def test_cpp_friction_fixed_point_matches_analytic(fp_exe):
     e_om = (res["omega"] - om) ** 2 / om ** 2
     assert e_pos <= 1e-2 and e_q <= 1e-2, (e_pos, e_q)
     assert e_v <= 1.2e-5 and e_om <= 1.2e-5, (e_v, e_om)
+
+
+# ------------------------------------------------------------------ snapshot files
+SNAP_SRC = os.path.join(ROOT, "tests", "cpp", "snapshot_writer.cpp")
+# keys of write_objects.hpp per shape and of the properties written by solver.hpp:383-400
+OBJECT_KEYS = {
+    "sphere": {"id", "position", "properties", "quaternion", "radius", "rotation", "type"},
+    "plane": {"id", "normal", "position", "properties", "quaternion", "rotation", "type"},
+    "segment": {"id", "normal", "p1", "p2", "properties", "quaternion", "tangent", "type"},
+    "superellipsoid": {"id", "position", "properties", "quaternion", "radius", "rotation", "squareness", "type"},
+}
+PROPERTY_KEYS = {"active", "desired_omega", "desired_velocity", "force", "mass", "moment_inertia", "omega", "velocity"}
+
+
+def bson_decode(b, pos=0, array=False):
+    """Minimal BSON reader (the element types the writer emits)."""
+    import struct
+    n = struct.unpack_from("<i", b, pos)[0]
+    end, pos = pos + n - 1, pos + 4
+    out = {}
+    while pos < end:
+        t = b[pos]
+        k = b.index(b"\0", pos + 1)
+        key, pos = b[pos + 1:k].decode(), k + 1
+        if t == 0x01:
+            v, pos = struct.unpack_from("<d", b, pos)[0], pos + 8
+        elif t == 0x02:
+            ln = struct.unpack_from("<i", b, pos)[0]
+            v, pos = b[pos + 4:pos + 4 + ln - 1].decode(), pos + 4 + ln
+        elif t in (0x03, 0x04):
+            ln = struct.unpack_from("<i", b, pos)[0]
+            v, pos = bson_decode(b, pos, t == 0x04), pos + ln
+        elif t == 0x08:
+            v, pos = bool(b[pos]), pos + 1
+        elif t == 0x0A:
+            v = None
+        elif t == 0x10:
+            v, pos = struct.unpack_from("<i", b, pos)[0], pos + 4
+        elif t == 0x12:
+            v, pos = struct.unpack_from("<q", b, pos)[0], pos + 8
+        else:
+            raise ValueError(f"BSON type {t:#x}")
+        out[key] = v
+    return [out[str(i)] for i in range(len(out))] if array else out
+
+
+def test_snapshot_writer_formats(tmp_path):
+    """write_output_files' documents for every shape (2D and 3D): the reference's fields per
+    object, the values of the container, and the same document in BSON."""
+    import math
+    exe = str(tmp_path / "snapw")
+    subprocess.run([GXX, "-std=c++17", "-Wall", "-Werror", *INC, SNAP_SRC, "-o", exe], check=True)
+    subprocess.run([exe, str(tmp_path)], check=True)
+    for name in ("snap2d", "snap3d"):
+        with open(tmp_path / f"{name}.json") as fh:
+            doc = json.load(fh)
+        with open(tmp_path / f"{name}.bson", "rb") as fh:
+            assert bson_decode(fh.read()) == doc
+        assert doc["contacts"] is None
+        for o in doc["objects"]:
+            assert set(o) == OBJECT_KEYS[o["type"]], o["type"]
+            assert set(o["properties"]) == PROPERTY_KEYS
+    d2 = json.load(open(tmp_path / "snap2d.json"))["objects"]
+    assert [o["type"] for o in d2] == ["plane", "segment", "sphere", "superellipsoid"]
+    assert [o["properties"]["active"] for o in d2] == [False, False, True, True]
+    # plane(pi/3): normal = column 0 of R; segment: the given extrema, tangent = (-n1, n0)
+    assert abs(d2[0]["normal"][0] - 0.5) < 1e-15 and abs(d2[0]["normal"][1] - math.sqrt(3) / 2) < 1e-15
+    assert max(abs(a - b) for a, b in zip(d2[1]["p1"] + d2[1]["p2"], [-1.0, 0.5, 2.0, 1.5])) < 1e-14
+    assert d2[1]["tangent"] == [-d2[1]["normal"][1], d2[1]["normal"][0]]
+    s = d2[2]
+    assert s["position"] == [0.3, 1.2] and s["radius"] == 0.25
+    assert s["properties"]["velocity"] == [1.0, -2.0] and s["properties"]["mass"] == 2.0
+    assert s["properties"]["moment_inertia"] == 0.3 and s["properties"]["force"] == [0.0, -9.81]
+    assert d2[3]["radius"] == [0.2, 0.1] and d2[3]["squareness"] == [1.2] and d2[3]["properties"]["omega"] == 0.5
+    d3 = json.load(open(tmp_path / "snap3d.json"))["objects"]
+    assert d3[0]["properties"]["moment_inertia"] == [0.1, 0.2, 0.3] and d3[0]["properties"]["omega"] == [1.0, 2.0, 3.0]
+    assert d3[1]["radius"] == [0.3, 0.2, 0.1] and d3[1]["squareness"] == [0.8, 1.3]
+    assert len(d3[1]["rotation"]) == 9
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode,name", [("nofriction", "3spheres_nofriction"), ("viscous", "3spheres_viscous")])
+def test_cpp_snapshot_files_match_reference_golden(exe, golden, mode, name, tmp_path):
+    """The reference's "3 Spheres" tests with snapshot files (output_frequency = total_it):
+    the initial snapshot and the final one, whose objects agree with the reference's golden
+    file as its diffFile checks them (test/utils.cpp:14-75, numbers within 1e-5)."""
+    subprocess.run([exe, mode, str(tmp_path / "out")], check=True, capture_output=True, cwd=tmp_path)
+    total = 60 if mode == "nofriction" else 70
+    first = json.load(open(tmp_path / "out" / f"{name}_0000.json"))
+    last = json.load(open(tmp_path / "out" / f"{name}_{total:04d}.json"))
+    assert sorted(os.listdir(tmp_path / "out")) == [f"{name}_0000.json", f"{name}_{total:04d}.json"]
+    assert first["contacts"] is None and [o["position"] for o in first["objects"]] == [
+        [-1.7, 1.3], [0.5, 1.7], [4.5, 1.3]]
+    worst = 0.0
+    for got, ref in zip(last["objects"], golden[name]["objects"]):
+        assert set(got) == OBJECT_KEYS["sphere"] and set(got["properties"]) == PROPERTY_KEYS
+        assert got["type"] == ref["type"] and got["properties"]["active"] == ref["active"]
+        for key in ("position", "quaternion"):
+            worst = max(worst, max(abs(a - b) for a, b in zip(got[key], ref[key])))
+        worst = max(worst, max(abs(a - b) for a, b in zip(got["properties"]["velocity"], ref["velocity"])))
+        worst = max(worst, abs(got["properties"]["omega"] - ref["omega"][0]))
+    assert worst <= 1e-5, worst
