@@ -34,6 +34,7 @@
 #include <cstdlib>
 #include <filesystem>
 #include <fstream>
+#include <iterator>
 #include <utility>
 #include <initializer_list>
 #include <iostream>
@@ -394,6 +395,116 @@ inline std::vector<uint8_t> to_bson(const Value& v) {
     return b;
 }
 
+// Reader for snapshot files (the JSON subset they use: objects, arrays, numbers, strings
+// with plain escapes, true/false/null).  Integers without '.', 'e' or 'E' become Int.
+class JsonReader {
+  public:
+    explicit JsonReader(const std::string& text) : s_(text) {}
+    Value parse() {
+        Value v = value();
+        ws();
+        if (k_ != s_.size()) fail("trailing characters");
+        return v;
+    }
+
+  private:
+    [[noreturn]] void fail(const char* what) const {
+        throw std::runtime_error(std::string("snapshot JSON: ") + what + " at offset " + std::to_string(k_));
+    }
+    void ws() {
+        while (k_ < s_.size() && (s_[k_] == ' ' || s_[k_] == '\n' || s_[k_] == '\t' || s_[k_] == '\r')) ++k_;
+    }
+    bool eat(char c) {
+        ws();
+        if (k_ < s_.size() && s_[k_] == c) {
+            ++k_;
+            return true;
+        }
+        return false;
+    }
+    void expect(char c) {
+        if (!eat(c)) fail("unexpected character");
+    }
+    std::string str() {
+        expect('"');
+        std::string out;
+        while (k_ < s_.size() && s_[k_] != '"') {
+            char c = s_[k_++];
+            if (c == '\\') {
+                if (k_ >= s_.size()) fail("bad escape");
+                const char e = s_[k_++];
+                c = e == 'n' ? '\n' : e == 't' ? '\t' : e == 'r' ? '\r' : e == 'b' ? '\b' : e == 'f' ? '\f' : e;
+                if (e == 'u') fail("unicode escapes are not used by snapshot files");
+            }
+            out += c;
+        }
+        expect('"');
+        return out;
+    }
+    Value value() {
+        ws();
+        if (k_ >= s_.size()) fail("unexpected end");
+        const char c = s_[k_];
+        if (c == '{') {
+            ++k_;
+            Value o = Value::object();
+            if (eat('}')) return o;
+            do {
+                const std::string key = str();
+                expect(':');
+                o.set(key, value());
+            } while (eat(','));
+            expect('}');
+            return o;
+        }
+        if (c == '[') {
+            ++k_;
+            Value a = Value::array();
+            if (eat(']')) return a;
+            do {
+                a.items.push_back(value());
+            } while (eat(','));
+            expect(']');
+            return a;
+        }
+        if (c == '"') return Value::string(str());
+        if (s_.compare(k_, 4, "true") == 0) { k_ += 4; return Value::boolean(true); }
+        if (s_.compare(k_, 5, "false") == 0) { k_ += 5; return Value::boolean(false); }
+        if (s_.compare(k_, 4, "null") == 0) { k_ += 4; return Value(); }
+        const std::size_t start = k_;
+        while (k_ < s_.size() && std::string("+-0123456789.eE").find(s_[k_]) != std::string::npos) ++k_;
+        if (k_ == start) fail("unexpected character");
+        const std::string num = s_.substr(start, k_ - start);
+        if (num.find_first_of(".eE") == std::string::npos) return Value::integer(std::strtoll(num.c_str(), nullptr, 10));
+        return Value::number(std::strtod(num.c_str(), nullptr));
+    }
+    const std::string& s_;
+    std::size_t k_ = 0;
+};
+inline Value read_json_file(const std::filesystem::path& path) {
+    std::ifstream f(path);
+    if (!f) throw std::runtime_error("cannot open " + path.string());
+    const std::string text((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+    return JsonReader(text).parse();
+}
+inline const Value& field(const Value& o, const std::string& key) {
+    for (const auto& f : o.fields)
+        if (f.first == key) return f.second;
+    throw std::runtime_error("snapshot JSON: missing \"" + key + "\"");
+}
+inline double as_number(const Value& v) {
+    if (v.kind == Value::Double) return v.d;
+    if (v.kind == Value::Int) return (double)v.i;
+    throw std::runtime_error("snapshot JSON: number expected");
+}
+template <std::size_t n>
+inline std::array<double, n> as_array(const Value& v) {
+    if (v.kind != Value::Array || v.items.size() != n) throw std::runtime_error("snapshot JSON: array size");
+    std::array<double, n> out{};
+    for (std::size_t k = 0; k < n; ++k) out[k] = as_number(v.items[k]);
+    return out;
+}
+
 // rotation_matrix<dim>(q), quaternion.hpp:66-124 (q = (w, x, y, z)), row-major
 template <std::size_t dim>
 inline std::array<double, dim * dim> rotation(const type::quaternion_t& q) {
@@ -604,6 +715,64 @@ class scopi_container {
     std::vector<double> m_pos, m_q, m_v, m_w, m_vd, m_dw, m_f, m_m, m_j, m_radius, m_length, m_axes, m_sq;
     std::size_t m_nb_inactive = 0;
 };
+
+// ------------------------------------------------------------------ restart
+// from_json<dim> (restart.hpp:20-67, properties as json.hpp:26-44 reads them): a container
+// rebuilt from the "objects" of a snapshot document (spheres, superellipsoids, segments,
+// planes), obstacles first as the snapshot lists them.
+template <std::size_t dim>
+scopi_container<dim> from_json(const io::Value& j) {
+    using io::as_array;
+    using io::as_number;
+    using io::field;
+    scopi_container<dim> container;
+    for (const auto& o : field(j, "objects").items) {
+        const auto& pr = field(o, "properties");
+        property<dim> p;
+        p.velocity(as_array<dim>(field(pr, "velocity")))
+            .desired_velocity(as_array<dim>(field(pr, "desired_velocity")))
+            .force(as_array<dim>(field(pr, "force")))
+            .mass(as_number(field(pr, "mass")));
+        if constexpr (dim == 2) {
+            p.omega(as_number(field(pr, "omega")))
+                .desired_omega(as_number(field(pr, "desired_omega")))
+                .moment_inertia(as_number(field(pr, "moment_inertia")));
+        } else {
+            p.omega(as_array<3>(field(pr, "omega")))
+                .desired_omega(as_array<3>(field(pr, "desired_omega")))
+                .moment_inertia(as_array<3>(field(pr, "moment_inertia")));
+        }
+        if (field(pr, "active").b)
+            p.activate();
+        else
+            p.deactivate();
+        const std::string type = field(o, "type").s;
+        if (type == "sphere") {
+            container.push_back(sphere<dim>({as_array<dim>(field(o, "position"))}, as_array<4>(field(o, "quaternion")),
+                                            as_number(field(o, "radius"))),
+                                p);
+        } else if (type == "superellipsoid") {
+            container.push_back(superellipsoid<dim>({as_array<dim>(field(o, "position"))},
+                                                    {as_array<4>(field(o, "quaternion"))},
+                                                    {as_array<dim>(field(o, "radius"))},
+                                                    {as_array<dim - 1>(field(o, "squareness"))}),
+                                p);
+        } else if (type == "segment") {
+            if constexpr (dim == 2)
+                container.push_back(segment<dim>(as_array<2>(field(o, "p1")), as_array<2>(field(o, "p2"))), p);
+        } else if (type == "plane") {
+            container.push_back(
+                plane<dim>({as_array<dim>(field(o, "position"))}, {as_array<4>(field(o, "quaternion"))}), p);
+        } else {
+            throw std::runtime_error("from_json: object type \"" + type + "\" is not supported");
+        }
+    }
+    return container;
+}
+template <std::size_t dim>
+scopi_container<dim> from_json(const std::filesystem::path& path) {
+    return from_json<dim>(io::read_json_file(path));
+}
 
 // ------------------------------------------------------------------ contacts record
 template <std::size_t dim, class problem_t>

@@ -1,6 +1,8 @@
-// The snapshot writer of the C++ drop-in (write_output_files, solver.hpp:368-438) on
-// containers of every shape, without a GPU: writes the "objects" document of a 2D and a
-// 3D container as JSON and as BSON into the directory given as argument.
+// The snapshot writer of the C++ drop-in (write_output_files, solver.hpp:368-438) and its
+// reader (from_json, restart.hpp:20-67) on containers of every shape, without a GPU: writes
+// the "objects" document of a 2D and a 3D container as JSON and as BSON into the directory
+// given as argument, each read back and written again (*_rt.json); with a snapshot file as
+// second argument, that file read and written again as snapfile_rt.json.
 #include <cmath>
 #include <fstream>
 
@@ -10,6 +12,7 @@
 #include <scopi/objects/types/sphere.hpp>
 #include <scopi/objects/types/superellipsoid.hpp>
 #include <scopi/property.hpp>
+#include <scopi/restart.hpp>
 #include <scopi/solver.hpp>
 
 template <std::size_t dim>
@@ -22,6 +25,15 @@ void write(const scopi::scopi_container<dim>& c, const std::string& base) {
     const auto b = scopi::io::to_bson(doc);
     std::ofstream f(base + ".bson", std::ios::binary);
     f.write(reinterpret_cast<const char*>(b.data()), (std::streamsize)b.size());
+}
+template <std::size_t dim>
+void round_trip(const std::string& in, const std::string& out) {
+    const scopi::scopi_container<dim> c = scopi::from_json<dim>(std::filesystem::path(in));
+    scopi::io::Value doc = scopi::io::Value::object();
+    doc.set("objects", c.snapshot_objects());
+    doc.set("contacts", scopi::io::Value());
+    std::ofstream j(out);
+    scopi::io::write_json(j, doc);
 }
 
 int main(int argc, char** argv) {
@@ -47,5 +59,8 @@ int main(int argc, char** argv) {
                     scopi::property<3>().velocity({{0., 0., -1.}}));
         write(p, dir + "/snap3d");
     }
+    round_trip<2>(dir + "/snap2d.json", dir + "/snap2d_rt.json");
+    round_trip<3>(dir + "/snap3d.json", dir + "/snap3d_rt.json");
+    if (argc > 2) round_trip<2>(argv[2], dir + "/snapfile_rt.json");
     return 0;
 }

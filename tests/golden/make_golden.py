@@ -4,7 +4,9 @@ Reads the reference's own golden snapshots (test/references/*.json of
 hpc-maths/scopi, written by ScopiSolver::write_output_files) and keeps only what
 the parity tests compare: per object position, quaternion, velocity and omega
 (the fields test/utils.cpp:14-75 diffs), plus the contact list of the last
-step (i, j, distance, normal, pi, pj).  Writes tests/golden/reference_states.json.
+step (i, j, distance, normal, pi, pj).  Writes tests/golden/reference_states.json, and
+one snapshot file unchanged (snapshot_obstacles_sphere_sphere_moving.json) for the
+restart tests.
 
 Run once in a checkout that has the reference at REF (default /root/reference):
     python tests/golden/make_golden.py [REF]
@@ -63,6 +65,13 @@ def main():
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_states.json")
     with open(dst, "w") as fh:
         json.dump(out, fh, indent=1)
+    print("wrote", dst)
+    # one snapshot kept whole, as the reference wrote it: the input of the restart tests
+    # (from_json, restart.hpp:20-67)
+    src = os.path.join(ref, "test", "references", "obstacles_sphere_sphere_moving.json")
+    dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "snapshot_obstacles_sphere_sphere_moving.json")
+    with open(src) as fh, open(dst, "w") as out_fh:
+        out_fh.write(fh.read())
     print("wrote", dst)
 
 

@@ -49,9 +49,10 @@ def test_cpp_api_matches_reference_golden(exe, golden, mode, name, tmp_path):
 SE_SRC = os.path.join(ROOT, "tests", "cpp", "superellipsoids_dropin.cpp")
 SE2_SRC = os.path.join(ROOT, "tests", "cpp", "two_ellipsoids_dropin.cpp")
 FP_SRC = os.path.join(ROOT, "tests", "cpp", "fixed_point_dropin.cpp")
+RS_SRC = os.path.join(ROOT, "tests", "cpp", "restart_dropin.cpp")
 
 
-@pytest.mark.parametrize("src", [SE_SRC, SE2_SRC, FP_SRC])
+@pytest.mark.parametrize("src", [SE_SRC, SE2_SRC, FP_SRC, RS_SRC])
 def test_superellipsoid_header_compiles(src):
     subprocess.run([GXX, "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", *INC, src], check=True)
 
@@ -162,6 +163,7 @@ def test_cpp_friction_fixed_point_matches_analytic(fp_exe, tmp_path):
 
 # ------------------------------------------------------------------ snapshot files
 SNAP_SRC = os.path.join(ROOT, "tests", "cpp", "snapshot_writer.cpp")
+SNAPSHOT_FIXTURE = os.path.join(ROOT, "tests", "golden", "snapshot_obstacles_sphere_sphere_moving.json")
 # keys of write_objects.hpp per shape and of the properties written by solver.hpp:383-400
 OBJECT_KEYS = {
     "sphere": {"id", "position", "properties", "quaternion", "radius", "rotation", "type"},
@@ -210,7 +212,7 @@ def test_snapshot_writer_formats(tmp_path):
     import math
     exe = str(tmp_path / "snapw")
     subprocess.run([GXX, "-std=c++17", "-Wall", "-Werror", *INC, SNAP_SRC, "-o", exe], check=True)
-    subprocess.run([exe, str(tmp_path)], check=True)
+    subprocess.run([exe, str(tmp_path), SNAPSHOT_FIXTURE], check=True)
     for name in ("snap2d", "snap3d"):
         with open(tmp_path / f"{name}.json") as fh:
             doc = json.load(fh)
@@ -260,3 +262,48 @@ def test_cpp_snapshot_files_match_reference_golden(exe, golden, mode, name, tmp_
         worst = max(worst, max(abs(a - b) for a, b in zip(got["properties"]["velocity"], ref["velocity"])))
         worst = max(worst, abs(got["properties"]["omega"] - ref["omega"][0]))
     assert worst <= 1e-5, worst
+
+
+def test_restart_reads_snapshots(tmp_path):
+    """from_json (restart.hpp:20-67): the writer's own files read back and written again give
+    the same document (numbers to 1e-12: a segment is rebuilt from its extrema, which moves
+    them by an ulp, as in the reference), and a snapshot the reference wrote (test/references/
+    obstacles_sphere_sphere_moving.json) gives back every object and property it holds."""
+    exe = str(tmp_path / "snapw")
+    subprocess.run([GXX, "-std=c++17", "-Wall", "-Werror", *INC, SNAP_SRC, "-o", exe], check=True)
+    subprocess.run([exe, str(tmp_path), SNAPSHOT_FIXTURE], check=True)
+    def close(a, b):
+        if isinstance(a, dict):
+            return isinstance(b, dict) and a.keys() == b.keys() and all(close(a[k], b[k]) for k in a)
+        if isinstance(a, list):
+            return isinstance(b, list) and len(a) == len(b) and all(close(x, y) for x, y in zip(a, b))
+        if isinstance(a, float):
+            return isinstance(b, float) and abs(a - b) <= 1e-12
+        return a == b
+
+    for name in ("snap2d", "snap3d"):
+        assert close(json.load(open(tmp_path / f"{name}.json")), json.load(open(tmp_path / f"{name}_rt.json")))
+    ref = json.load(open(SNAPSHOT_FIXTURE))["objects"]
+    got = json.load(open(tmp_path / "snapfile_rt.json"))["objects"]
+    assert len(got) == len(ref)
+    for g, r in zip(got, ref):
+        for key in ("type", "id", "position", "quaternion", "radius", "rotation", "properties"):
+            assert g[key] == r[key], (key, g[key], r[key])
+
+
+@pytest.mark.gpu
+def test_cpp_restart_continues_like_one_run(tmp_path):
+    """30 steps, a snapshot, from_json and 30 more steps with a new solver end in the state
+    of 60 steps in one run, bit for bit (NoFriction carries nothing else between steps, and
+    the snapshot's numbers read back exactly)."""
+    from scopi_b200 import build
+    build.build()
+    exe = str(tmp_path / "restart")
+    lib = os.path.join(ROOT, "scopi_b200")
+    subprocess.run([GXX, "-O2", "-std=c++17", *INC, RS_SRC, "-L", lib, "-lscopi_gpu", f"-Wl,-rpath,{lib}", "-o", exe],
+                   check=True)
+    one = json.loads(subprocess.run([exe], check=True, capture_output=True, text=True, cwd=tmp_path).stdout)
+    two = json.loads(subprocess.run([exe, "restart", str(tmp_path / "snap")], check=True, capture_output=True,
+                                    text=True, cwd=tmp_path).stdout)
+    assert os.path.exists(tmp_path / "snap" / "restart_0030.json")
+    assert one == two
