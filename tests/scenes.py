@@ -72,13 +72,16 @@ def matrix_a_case2():
 
 
 def three_spheres(problem=NOFRICTION):
-    """test/test_gradient.cpp:377-503 (NoFriction Tf=6, Viscous Tf=7; dt 0.1, vap_fpd, alpha 0.1)."""
+    """test/test_gradient.cpp:377-548 (NoFriction Tf=6, Viscous and FrictionFixedPoint (mu 0.5,
+    fixed point 1e-6 / 1000) Tf=7; dt 0.1, vap_fpd, alpha 0.1)."""
     p = Particles(2)
     for (x, y) in ((-1.7, 1.3), (0.5, 1.7), (4.5, 1.3)):
         p.add_sphere((x, y), 0.5, Property(mass=1, moment_inertia=1, force=(-x, -y)))
     tf = 6.0 if problem == NOFRICTION else 7.0
     dt = 0.1
     kw = dict(problem=problem, vap=VAP_FPD, contact_method=KDTREE, tolerance=1e-7, max_ite=10000, alpha=0.1)
+    if problem == 3:
+        kw.update(mu=0.5, fixed_point_tol=1e-6, fixed_point_max_iter=1000)
     return p.finalize(), kw, dt, int(tf / dt)
 
 

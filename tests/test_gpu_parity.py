@@ -80,6 +80,7 @@ def test_matrix_known_values_and_adjoint():
 GOLDEN_CASES = [
     ("3spheres_nofriction", lambda: S.three_spheres(S.NOFRICTION), 1e-5),
     ("3spheres_viscous", lambda: S.three_spheres(S.VISCOUS), 1e-5),
+    ("3spheres_friction_fp", lambda: S.three_spheres(3), 1e-5),
     ("sphere_plane_friction_mu01", S.sphere_plane_friction_mu01, 1e-5),
     ("two_spheres_asymmetrical", lambda: S.two_spheres(False), 1e-6),
     ("two_spheres_symmetrical", lambda: S.two_spheres(True), 1e-6),

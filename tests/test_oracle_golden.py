@@ -79,9 +79,10 @@ def test_matrix_a_case2():
     assert approx(sol[0], -0.18595809) and approx(sol[1], 1.18278683)
 
 
-@pytest.mark.parametrize("name,problem", [("3spheres_nofriction", S.NOFRICTION), ("3spheres_viscous", S.VISCOUS)])
+@pytest.mark.parametrize("name,problem", [("3spheres_nofriction", S.NOFRICTION), ("3spheres_viscous", S.VISCOUS),
+                                          ("3spheres_friction_fp", 3)])
 def test_three_spheres_golden(golden, name, problem):
-    """test/test_gradient.cpp:377-503 against test/references/3spheres_*.json (tol 1e-5)."""
+    """test/test_gradient.cpp:377-548 against test/references/3spheres_*.json (tol 1e-5)."""
     s = run_oracle(S.three_spheres(problem))
     compare_objects(s.pa, golden[name]["objects"], 2, 1e-5)
 
