@@ -16,7 +16,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle_scopi.so")
 
-NOFRICTION, FRICTION, VISCOUS, FRICTION_FIXED_POINT = 0, 1, 2, 3
+NOFRICTION, FRICTION, VISCOUS, FRICTION_FIXED_POINT, VISCOUS_FRICTION = 0, 1, 2, 3, 4
 VAP_FIXED, VAP_FPD = 0, 1
 BRUTE_FORCE, KDTREE = 0, 1
 

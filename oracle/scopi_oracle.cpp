@@ -459,6 +459,8 @@ struct orc_solver {
         std::vector<double> invM, C;
         std::vector<double> S;          // FrictionFixedPoint: s_c n_c (empty otherwise)
         std::vector<int64_t> neg_slot;  // Viscous: second multiplier slot or -1
+        std::vector<int64_t> row;       // ViscousFriction: first local row of each contact
+        std::vector<int> mode;          // ViscousFriction: 1, 2 or 4 multipliers (0, 1, 2)
         int64_t size = 0;
         mutable std::vector<double> w1, w2, w3;
 
@@ -501,6 +503,29 @@ struct orc_solver {
             // LagrangeMultiplier sizes, lagrange_multiplier.hpp:54-60,125-141,217-236
             if (s->p.problem == ORC_FRICTION) {
                 size = 3 * (int64_t)nc;
+            } else if (s->p.problem == ORC_VISCOUS_FRICTION) {
+                // LagrangeMultiplier<ViscousFriction>, lagrange_multiplier.hpp:358-398: one
+                // multiplier while gamma >= -gamma_tol, two (l+, l-) while gamma_min < gamma <
+                // -gamma_tol, four (l0, f) at gamma == gamma_min; S = dt mu s_c n_c on f
+                row.assign(nc, 0);
+                mode.assign(nc, 0);
+                int64_t r = 0;
+                for (size_t c = 0; c < nc; ++c) {
+                    row[c] = r;
+                    const double gm = s->contacts[c].gamma;
+                    if (gm < -s->p.gamma_tol) {
+                        mode[c] = gm != s->p.gamma_min ? 1 : 2;
+                        r += gm != s->p.gamma_min ? 2 : 4;
+                    } else {
+                        r += 1;
+                    }
+                }
+                size = r;
+                S.assign(size, 0.0);
+                for (size_t c = 0; c < nc; ++c)
+                    if (mode[c] == 2)
+                        for (int d = 0; d < dim; ++d)
+                            S[row[c] + 1 + d] = s->dt * s->p.mu * s->sij[c] * s->contacts[c].nij[d];
             } else if (s->p.problem == ORC_VISCOUS) {
                 neg_slot.assign(nc, -1);
                 int64_t next = (int64_t)nc;
@@ -520,6 +545,21 @@ struct orc_solver {
                 return;
             }
             out.assign(3 * nc, 0.0);
+            if (s->p.problem == ORC_VISCOUS_FRICTION) {  // lagrange_multiplier.hpp:428-454
+                for (size_t c = 0; c < nc; ++c) {
+                    const double* xr = &x[row[c]];
+                    const V3& nn = s->contacts[c].nij;
+                    for (int d = 0; d < dim; ++d) {
+                        if (mode[c] == 0)
+                            out[3 * c + d] = xr[0] * nn[d];
+                        else if (mode[c] == 1)
+                            out[3 * c + d] = (xr[0] - xr[1]) * nn[d];
+                        else
+                            out[3 * c + d] = (-xr[0]) * nn[d] + xr[1 + d];
+                    }
+                }
+                return;
+            }
             for (size_t c = 0; c < nc; ++c) {
                 double lc = x[c];
                 if (s->p.problem == ORC_VISCOUS && neg_slot[c] >= 0) lc = x[c] - x[neg_slot[c]];
@@ -535,6 +575,23 @@ struct orc_solver {
                 return;
             }
             out.assign(size, 0.0);
+            if (s->p.problem == ORC_VISCOUS_FRICTION) {  // lagrange_multiplier.hpp:400-426
+                for (size_t c = 0; c < nc; ++c) {
+                    double acc = 0;
+                    for (int d = 0; d < dim; ++d) acc += x[3 * c + d] * s->contacts[c].nij[d];
+                    double* o = &out[row[c]];
+                    if (mode[c] == 0) {
+                        o[0] = acc;
+                    } else if (mode[c] == 1) {
+                        o[0] = acc;
+                        o[1] = -acc;
+                    } else {
+                        o[0] = -acc;
+                        for (int d = 0; d < dim; ++d) o[1 + d] = x[3 * c + d];
+                    }
+                }
+                return;
+            }
             for (size_t c = 0; c < nc; ++c) {
                 double acc = 0;
                 for (int d = 0; d < dim; ++d) acc += x[3 * c + d] * s->contacts[c].nij[d];
@@ -574,6 +631,10 @@ struct orc_solver {
         }
         // projections, lagrange_multiplier.hpp:104-107, 196-200, 243-268
         void projection(std::vector<double>& lam) const {
+            if (s->p.problem == ORC_VISCOUS_FRICTION) {
+                projection_viscous_friction(lam);
+                return;
+            }
             if (s->p.problem != ORC_FRICTION) {
                 for (auto& x : lam) x = std::max(x, 0.);
                 return;
@@ -597,6 +658,49 @@ struct orc_solver {
                         for (int d = 0; d < dim; ++d) li[d] = new_norm * lt[d] + new_ln * nn[d];
                     }
                 }
+            }
+        }
+        // LagrangeMultiplier<ViscousFriction>::projection, lagrange_multiplier.hpp:466-536: on the
+        // four-multiplier rows, the nearer (Euclidean, over the 1 + dim entries) of (0, P_cone(f))
+        // and (max(l0, 0), 0)
+        void projection_viscous_friction(std::vector<double>& lam) const {
+            const int dim = s->dim;
+            const double mu = s->p.mu;
+            for (size_t c = 0; c < s->contacts.size(); ++c) {
+                double* li = &lam[row[c]];
+                if (mode[c] == 0) {
+                    li[0] = std::max(li[0], 0.);
+                    continue;
+                }
+                if (mode[c] == 1) {
+                    li[0] = std::max(li[0], 0.);
+                    li[1] = std::max(li[1], 0.);
+                    continue;
+                }
+                const V3& nn = s->contacts[c].nij;
+                const double* lf = li + 1;
+                const double ln = dot_n(lf, nn.data(), dim);
+                double lt[3] = {0, 0, 0};
+                for (int d = 0; d < dim; ++d) lt[d] = lf[d] - ln * nn[d];
+                const double nrm = norm_n(lt, dim);
+                double fric[4] = {0, 0, 0, 0};
+                if (nrm > mu * ln) {
+                    if (!(ln <= -mu * nrm)) {
+                        const double new_norm = (mu * mu) * (nrm + ln / mu) / (mu * mu + 1);
+                        const double new_ln = new_norm / mu;
+                        for (int d = 0; d < dim; ++d) fric[1 + d] = new_norm * (lt[d] / nrm) + new_ln * nn[d];
+                    }
+                } else {
+                    for (int d = 0; d < dim; ++d) fric[1 + d] = lf[d];
+                }
+                double moins[4] = {std::max(li[0], 0.), 0, 0, 0};
+                double df = 0.0, dm = 0.0;
+                for (int k = 0; k < 1 + dim; ++k) {
+                    df += (fric[k] - li[k]) * (fric[k] - li[k]);
+                    dm += (moins[k] - li[k]) * (moins[k] - li[k]);
+                }
+                const double* pick = std::sqrt(df) < std::sqrt(dm) ? fric : moins;
+                for (int k = 0; k < 1 + dim; ++k) li[k] = pick[k];
             }
         }
         void velocities(const std::vector<double>& lam, std::vector<double>& out) const {
@@ -718,6 +822,14 @@ struct orc_solver {
         if (!contacts.empty()) {
             // extra_steps_before_solve<FrictionFixedPoint> (OptimGradient.hpp:85-94): s_c = mu dt
             if (fixed_point) sij.assign(contacts.size(), p.mu * dt);
+            // extra_steps_before_solve<ViscousFriction> (OptimGradient.hpp:96-107): s_c = 1 on
+            // the contacts at gamma_min
+            const bool vf = p.problem == ORC_VISCOUS_FRICTION;
+            if (vf) {
+                sij.assign(contacts.size(), 0.0);
+                for (size_t c = 0; c < contacts.size(); ++c)
+                    if (contacts[c].gamma == p.gamma_min) sij[c] = 1.;
+            }
             Problem pb(this);
             lambda = apgd(pb);
             std::vector<double> vel;
@@ -732,9 +844,11 @@ struct orc_solver {
                 }
             };
             velocities(pb);
-            if (fixed_point) {
-                // extra_steps_after_solve<FrictionFixedPoint> (OptimGradient.hpp:117-176) and the
-                // solve loop of ScopiSolver::run (solver.hpp:286-291)
+            if (fixed_point || vf) {
+                // extra_steps_after_solve<FrictionFixedPoint> (OptimGradient.hpp:117-176), its
+                // <ViscousFriction> twin (:178-250: s_c = |(A u)_t| on the contacts at gamma_min,
+                // err = |s - s_old| / (1 + |s|)) and the solve loop of ScopiSolver::run
+                // (solver.hpp:286-291)
                 int64_t iters = stats.iterations, bts = stats.backtracks, rss = stats.restarts, fp = 0;
                 const double mudt = p.mu * dt;
                 for (;;) {
@@ -747,17 +861,23 @@ struct orc_solver {
                     amat(Uf, AUf);
                     double dd = 0.0, ss = 0.0;
                     for (size_t c = 0; c < contacts.size(); ++c) {
+                        if (vf && contacts[c].gamma != p.gamma_min) continue;
                         const double dn = dot_n(&AUf[3 * c], contacts[c].nij.data(), dim);
                         double t[3] = {0, 0, 0};
                         for (int d = 0; d < dim; ++d) t[d] = AUf[3 * c + d] - contacts[c].nij[d] * dn;
-                        const double snew = mudt * norm_n(t, dim);
+                        const double snew = vf ? norm_n(t, dim) : mudt * norm_n(t, dim);
                         dd += (snew - sij[c]) * (snew - sij[c]);
                         ss += snew * snew;
                         sij[c] = snew;
                     }
                     ++fp;
-                    if (!(mudt > 0.0)) break;  // s stays 0: one solve (the reference's 1/(mu dt) is NaN)
-                    const double err = (1 / mudt) * std::sqrt(dd) / (1 + (1 / mudt) * std::sqrt(ss));
+                    double err;
+                    if (vf) {
+                        err = std::sqrt(dd) / (1 + std::sqrt(ss));
+                    } else {
+                        if (!(mudt > 0.0)) break;  // s stays 0: one solve (the reference's 1/(mu dt) is NaN)
+                        err = (1 / mudt) * std::sqrt(dd) / (1 + (1 / mudt) * std::sqrt(ss));
+                    }
                     if (err < p.fixed_point_tol || fp >= p.fixed_point_max_iter) break;
                     Problem pf(this);
                     lambda = apgd(pf);
@@ -786,8 +906,9 @@ struct orc_solver {
                 viol = std::max(viol, -g);
             }
             stats.violation = viol;
-            // update_contact_properties_impl<Viscous>, OptimGradient.hpp:19-35
-            if (p.problem == ORC_VISCOUS) {
+            // update_contact_properties_impl<Viscous>, OptimGradient.hpp:19-35 (<ViscousFriction>
+            // :36-52, the same update on its own local-to-global map)
+            if (p.problem == ORC_VISCOUS || vf) {
                 std::vector<double> lg;
                 pb.l2g(lambda, lg);
                 for (size_t c = 0; c < contacts.size(); ++c) {

@@ -41,13 +41,14 @@ extern "C" {
 #endif
 
 enum { ORC_SPHERE = 0, ORC_PLANE = 1, ORC_SEGMENT = 2, ORC_SUPERELLIPSOID = 3 };
-enum { ORC_NOFRICTION = 0, ORC_FRICTION = 1, ORC_VISCOUS = 2, ORC_FRICTION_FIXED_POINT = 3 };
+enum { ORC_NOFRICTION = 0, ORC_FRICTION = 1, ORC_VISCOUS = 2, ORC_FRICTION_FIXED_POINT = 3,
+       ORC_VISCOUS_FRICTION = 4 };
 enum { ORC_VAP_FIXED = 0, ORC_VAP_FPD = 1 };
 enum { ORC_BRUTE_FORCE = 0, ORC_KDTREE = 1 };
 
 typedef struct {
     int32_t dim;
-    int32_t problem;          /* ORC_NOFRICTION / ORC_FRICTION / ORC_VISCOUS */
+    int32_t problem;          /* ORC_NOFRICTION / FRICTION / VISCOUS / FRICTION_FIXED_POINT / VISCOUS_FRICTION */
     int32_t vap;              /* ORC_VAP_FIXED / ORC_VAP_FPD */
     int32_t contact_method;   /* ORC_BRUTE_FORCE / ORC_KDTREE */
     double dmax;              /* ContactsParams::dmax (default 2) */
@@ -61,7 +62,7 @@ typedef struct {
     double gamma_min;
     double gamma_tol;
     int32_t num_threads;      /* OpenMP threads for the loops the reference parallelises (0 = default) */
-    double fixed_point_tol;   /* contact_property<FixedPoint> (1e-6, 1000), FrictionFixedPoint only */
+    double fixed_point_tol;   /* contact_property<FixedPoint> (1e-6, 1000): FrictionFixedPoint, ViscousFriction */
     int64_t fixed_point_max_iter;
 } orc_params;
 
@@ -92,7 +93,7 @@ typedef struct {
     int32_t converged;
     double violation;         /* max_c max(0, -(d_c + dt n_c.(A u)_c)) after the solve */
     double seconds_contacts, seconds_solve, seconds_other;
-    int64_t fixed_point_iterations; /* FrictionFixedPoint: solves of the last step */
+    int64_t fixed_point_iterations; /* FrictionFixedPoint, ViscousFriction: solves of the last step */
 } orc_stats;
 
 typedef struct orc_solver orc_solver;

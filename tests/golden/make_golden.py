@@ -18,7 +18,8 @@ import sys
 FILES = [
     "3spheres_nofriction",          # test/test_gradient.cpp:377-439
     "3spheres_viscous",             # test/test_gradient.cpp:441-503
-    "3spheres_friction_fp",         # test/test_gradient.cpp:505-548 (FrictionFixedPoint)
+    "3spheres_friction_fp",         # test/test_gradient.cpp:505-572 (FrictionFixedPoint)
+    "3spheres_viscous_friction",    # test/test_gradient.cpp:574-642 (ViscousFriction)
     "sphere_plane_friction_mu01",   # test/test_gradient.cpp:156-213
     "two_spheres_asymmetrical",     # test/test_sphere.cpp:341-380
     "two_spheres_symmetrical",      # test/test_sphere.cpp:382-421

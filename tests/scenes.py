@@ -13,7 +13,7 @@ import math
 from scopi_b200.container import Particles, Property, quaternion
 
 PI = math.pi
-NOFRICTION, FRICTION, VISCOUS = 0, 1, 2
+NOFRICTION, FRICTION, VISCOUS, FRICTION_FIXED_POINT, VISCOUS_FRICTION = 0, 1, 2, 3, 4
 VAP_FIXED, VAP_FPD = 0, 1
 BRUTE_FORCE, KDTREE = 0, 1
 
@@ -72,8 +72,9 @@ def matrix_a_case2():
 
 
 def three_spheres(problem=NOFRICTION):
-    """test/test_gradient.cpp:377-548 (NoFriction Tf=6, Viscous and FrictionFixedPoint (mu 0.5,
-    fixed point 1e-6 / 1000) Tf=7; dt 0.1, vap_fpd, alpha 0.1)."""
+    """test/test_gradient.cpp:377-642 (NoFriction Tf=6; Viscous, FrictionFixedPoint (mu 0.5,
+    fixed point 1e-6 / 1000) and ViscousFriction (mu 0.5, fixed point 1e-3 / 1000, gamma_min -1.4)
+    Tf=7; dt 0.1, vap_fpd, alpha 0.1)."""
     p = Particles(2)
     for (x, y) in ((-1.7, 1.3), (0.5, 1.7), (4.5, 1.3)):
         p.add_sphere((x, y), 0.5, Property(mass=1, moment_inertia=1, force=(-x, -y)))
@@ -82,6 +83,8 @@ def three_spheres(problem=NOFRICTION):
     kw = dict(problem=problem, vap=VAP_FPD, contact_method=KDTREE, tolerance=1e-7, max_ite=10000, alpha=0.1)
     if problem == 3:
         kw.update(mu=0.5, fixed_point_tol=1e-6, fixed_point_max_iter=1000)
+    if problem == 4:
+        kw.update(mu=0.5, fixed_point_tol=1e-3, fixed_point_max_iter=1000, gamma=0.0, gamma_min=-1.4, gamma_tol=1e-6)
     return p.finalize(), kw, dt, int(tf / dt)
 
 
@@ -309,3 +312,76 @@ def analytic_friction(alpha, mu, t, r, g, y0):
         v = g * (sa - mu * ca) * t2 + (vtm + mu * vnm)
         om = -2.0 * mu * g * ca * t2 / r + 2 * mu * vnm / r
     return (x, r), theta, (v, 0.0), om
+
+
+def sphere_plane_viscous_friction():
+    """test/test_gradient.cpp:284-372: ViscousFriction, sphere on plane(pi/2) under tilted gravity
+    g(sin a, -cos a), a = pi/4, mu 0.5, fixed point 1e-3 / 1000, gamma 0, gamma_min -1.4, gamma_tol
+    1e-6, alpha 0.1, dt 0.01: 500 steps, then the force flipped for 100 more."""
+    radius, g, h, alpha = 1.0, 1.0, 2.0, PI / 4
+    p = Particles(2)
+    p.add_plane((0.0, 0.0), PI / 2)
+    p.add_sphere((0.0, h), radius, Property(mass=1, moment_inertia=radius * radius / 2.0,
+                                            force=(g * math.sin(alpha), -g * math.cos(alpha))))
+    kw = dict(problem=VISCOUS_FRICTION, vap=VAP_FPD, tolerance=1e-7, max_ite=10000, alpha=0.1, mu=0.5,
+              fixed_point_tol=1e-3, fixed_point_max_iter=1000, gamma=0.0, gamma_min=-1.4, gamma_tol=1e-6)
+    return p.finalize(), kw, 0.01, 500
+
+
+def analytic_viscous_friction(alpha, mu, t, r, g, y0, gamma_min, t_inv):
+    """test/analytical_solution.cpp:193-417: the sphere falls, sticks, slides with friction once the
+    adhesion potential has reached gamma_min (rolling without slip after t_no_slide when
+    tan a <= 3 mu), and after the force flips at t_inv moves back and unsticks.
+    Returns position, angle, velocity, angular velocity.  The reference's velocity branch writes
+    t_no_slide as -tan(a) t_gm / (g (tan a - 3 mu)) + t_gm and its position branch as
+    -v_gm / (g cos(a) (tan a - 3 mu)) + t_gm (equal when g = 1); both are kept."""
+    sa, ca, ta = math.sin(alpha), math.cos(alpha), math.tan(alpha)
+    t_imp = math.sqrt(2 * (y0 - r) / (g * ca))
+    t_gm = -gamma_min / (g * ca)
+    gamma_inv = gamma_min if t_inv > t_gm else -g * t_inv * ca
+    if t < t_imp:
+        return (g * t * t * sa / 2, -g * t * t * ca / 2 + y0), 0.0, (g * t * sa, -g * t * ca), 0.0
+    if t < t_gm:
+        return (g * t * t * sa / 2, r), 0.0, (g * t * sa, 0.0), 0.0
+    v_gm = -gamma_min * ta
+    x_gm = g * t_gm * t_gm * sa / 2
+
+    def slide(tt):
+        """(x, angle, v, omega) while sliding at gamma_min, tt >= t_gm."""
+        t2 = tt - t_gm
+        return (g * (sa - mu * ca) * t2 * t2 / 2 + v_gm * t2 + x_gm, -mu * g * ca * t2 * t2 / r,
+                g * (sa - mu * ca) * t2 + v_gm, -2.0 * mu * g * ca * t2 / r)
+
+    def state(tt):
+        """(x, angle, v, omega) at gamma_min before the flip, rolling after t_no_slide."""
+        out = list(slide(tt))
+        if ta > 3 * mu:
+            return out
+        t_ns_x = -v_gm / (g * ca * (ta - 3 * mu)) + t_gm
+        t_ns_v = -ta * t_gm / (g * (ta - 3 * mu)) + t_gm
+        if tt > t_ns_x:
+            x_ns, a_ns, v_ns, w_ns = slide(t_ns_x)
+            t3 = tt - t_ns_x
+            out[0] = g * sa * t3 * t3 / 3.0 + v_ns * t3 + x_ns
+            out[1] = -g * sa * t3 * t3 / (3.0 * r) + w_ns * t3 + a_ns
+        if tt > t_ns_v:
+            _, _, v_ns, w_ns = slide(t_ns_v)
+            t3 = tt - t_ns_v
+            out[2] = 2.0 * g * sa * t3 / 3.0 + v_ns
+            out[3] = -2.0 * g * sa * t3 / (3.0 * r) + w_ns
+        return out
+
+    if t < t_inv:
+        x, ang, vx, w = state(t)
+        return (x, r), ang, (vx, 0.0), w
+    x_i, a_i, v_i, w_i = state(t_inv)
+    t_unstick = t_inv - gamma_inv / (g * ca)
+    t4 = t - t_inv
+    x = v_i * t4 - g * sa * t4 * t4 / 2 + x_i
+    ang = w_i * t4 + a_i
+    vx = v_i - g * sa * t4
+    if t < t_unstick:
+        y, vy = r, 0.0
+    else:
+        y, vy = g * ca * (t - t_unstick) ** 2 / 2 + r, g * ca * (t - t_unstick)
+    return (x, y), ang, (vx, vy), w_i

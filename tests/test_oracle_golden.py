@@ -80,9 +80,10 @@ def test_matrix_a_case2():
 
 
 @pytest.mark.parametrize("name,problem", [("3spheres_nofriction", S.NOFRICTION), ("3spheres_viscous", S.VISCOUS),
-                                          ("3spheres_friction_fp", 3)])
+                                          ("3spheres_friction_fp", S.FRICTION_FIXED_POINT),
+                                          ("3spheres_viscous_friction", S.VISCOUS_FRICTION)])
 def test_three_spheres_golden(golden, name, problem):
-    """test/test_gradient.cpp:377-548 against test/references/3spheres_*.json (tol 1e-5)."""
+    """test/test_gradient.cpp:377-642 against test/references/3spheres_*.json (tol 1e-5)."""
     s = run_oracle(S.three_spheres(problem))
     compare_objects(s.pa, golden[name]["objects"], 2, 1e-5)
 
@@ -219,3 +220,30 @@ def test_sphere_plane_friction_fixed_point_analytic():
     assert approx(e_v, 1e-12) or e_v <= 1e-12, e_v
     assert approx(e_om, 1e-12) or e_om <= 1e-12, e_om
     assert s.stats()["fixed_point_iterations"] >= 2
+
+
+def viscous_friction_errors(pa, dt, total, total2):
+    """Errors of test/test_gradient.cpp:341-366 (relative norms; omega with std::norm)."""
+    x, theta, v, om = S.analytic_viscous_friction(math.pi / 4, 0.5, dt * (total + total2), 1.0, 1.0, 2.0, -1.4,
+                                                  dt * total)
+    qa = S.quaternion(theta)
+    e_pos = math.hypot(pa.pos[1, 0] - x[0], pa.pos[1, 1] - x[1]) / math.hypot(*x)
+    e_q = float(np.linalg.norm(pa.q[1] - qa) / np.linalg.norm(qa))
+    e_v = math.hypot(pa.v[1, 0] - v[0], pa.v[1, 1] - v[1]) / math.hypot(*v)
+    e_om = (pa.omega[1, 2] - om) ** 2 / om ** 2
+    return e_pos, e_q, e_v, e_om
+
+
+def test_sphere_plane_viscous_friction_analytic():
+    """test/test_gradient.cpp:284-372 (ViscousFriction): 500 steps, the force flipped, 100 more;
+    pos and q within 1e-1 of the analytic solution, v and omega within 1e-3."""
+    pa, kw, dt, total = S.sphere_plane_viscous_friction()
+    s = orc.OracleSolver(pa, **kw)
+    s.run(dt, total)
+    p2 = s.pa.copy()
+    p2.f[1, :2] = (-math.sin(math.pi / 4), math.cos(math.pi / 4))
+    s.set_particles(p2)
+    s.run(dt, 100)
+    e_pos, e_q, e_v, e_om = viscous_friction_errors(s.pa, dt, total, 100)
+    assert e_pos <= 1e-1 and e_q <= 1e-1, (e_pos, e_q)
+    assert e_v <= 1e-3 * (1 + APPROX) and e_om <= 1e-3 * (1 + APPROX), (e_v, e_om)
