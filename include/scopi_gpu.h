@@ -47,6 +47,14 @@ extern "C" {
    the linear term c + s_c n_c, s_c = mu dt |tangential relative velocity| updated after
    each solve until the fixed point (fixed_point_tol, fixed_point_max_iter) */
 #define SCOPI_GPU_FRICTION_FIXED_POINT 3
+/* ViscousFriction (property.hpp:34, lagrange_multiplier.hpp:347-541, OptimGradient.hpp:36-52,
+   96-107, 178-250): per contact 1, 2 or 4 multipliers by its adhesion potential gamma
+   (gamma >= -gamma_tol: normal; gamma_min < gamma < -gamma_tol: the viscous pair; gamma ==
+   gamma_min: a normal multiplier and a friction-cone force, projected onto the nearer of the
+   two), the linear term dt mu s_c n_c on the friction force, s_c = |tangential relative
+   velocity| updated after each solve until the fixed point (fixed_point_tol,
+   fixed_point_max_iter); gamma updated after the step */
+#define SCOPI_GPU_VISCOUS_FRICTION 4
 /* vap policies (include/scopi/vap/vap_fixed.hpp, vap_fpd.hpp) */
 #define SCOPI_GPU_VAP_FIXED 0
 #define SCOPI_GPU_VAP_FPD 1
@@ -65,7 +73,8 @@ extern "C" {
 
 typedef struct scopi_gpu_params {
     int32_t dim;              /* 2 or 3 */
-    int32_t problem;          /* SCOPI_GPU_NOFRICTION / FRICTION / VISCOUS / FRICTION_FIXED_POINT */
+    int32_t problem;          /* SCOPI_GPU_NOFRICTION / FRICTION / VISCOUS / FRICTION_FIXED_POINT /
+                                 VISCOUS_FRICTION */
     int32_t vap;              /* SCOPI_GPU_VAP_FIXED / VAP_FPD */
     int32_t contact_method;   /* SCOPI_GPU_BRUTE_FORCE / KDTREE */
     int32_t precision;        /* SCOPI_GPU_FP64 / SCOPI_GPU_MIXED */
@@ -131,7 +140,7 @@ typedef struct scopi_gpu_stats {
     double ms_solve;         /* device time of the APGD part of the last step */
     double ms_apgd_kernel;   /* device time of the persistent APGD launches of the last step */
     int64_t steps;           /* steps run by this handle */
-    int64_t fixed_point_iterations; /* FRICTION_FIXED_POINT: solves of the last step */
+    int64_t fixed_point_iterations; /* FRICTION_FIXED_POINT, VISCOUS_FRICTION: solves of the last step */
 } scopi_gpu_stats;
 
 typedef struct scopi_gpu_handle scopi_gpu_handle;

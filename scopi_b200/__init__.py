@@ -6,4 +6,4 @@ particle container) and seeded synthetic workloads.
 """
 from .container import PLANE, SEGMENT, SPHERE, ParticleArrays, Particles, Property, quaternion  # noqa: F401
 from .solver import (BRUTE_FORCE, FP64, FRICTION, FRICTION_FIXED_POINT, KDTREE, MIXED, NOFRICTION,  # noqa: F401
-                     VAP_FIXED, VAP_FPD, VISCOUS, ScopiBatch, ScopiGPUError, ScopiSolver)
+                     VAP_FIXED, VAP_FPD, VISCOUS, VISCOUS_FRICTION, ScopiBatch, ScopiGPUError, ScopiSolver)

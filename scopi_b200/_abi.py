@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libscopi_gpu.so")
 
 OK, EINVAL, ECUDA, ENOMEM, EUNSUPPORTED, ETIMEOUT, ENOCONV = 0, -1, -2, -3, -4, -5, 1
-NOFRICTION, FRICTION, VISCOUS, FRICTION_FIXED_POINT = 0, 1, 2, 3
+NOFRICTION, FRICTION, VISCOUS, FRICTION_FIXED_POINT, VISCOUS_FRICTION = 0, 1, 2, 3, 4
 VAP_FIXED, VAP_FPD = 0, 1
 BRUTE_FORCE, KDTREE = 0, 1
 FP64, MIXED = 0, 1

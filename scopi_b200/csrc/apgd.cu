@@ -154,6 +154,56 @@ __device__ __forceinline__ void cone_project(double* l, const double* n, double 
     }
 }
 
+// ViscousFriction: four multiplier slots per contact; the contact's mode (set from gamma at
+// assembly, LagrangeMultiplier<ViscousFriction>, lagrange_multiplier.hpp:358-398) says which
+// are live: 0 (l) with force l n, 1 (l+, l-) with force (l+ - l-) n, 2 (l0, f) with force
+// -l0 n + f.  Unused slots stay 0.
+// local2global of one contact's slots (lagrange_multiplier.hpp:428-454)
+template <typename T, int DIM>
+__device__ __forceinline__ void vf_force(int mode, const T* l, const T* n, T* f) {
+    for (int d = 0; d < 3; ++d) {
+        if (mode == 0)
+            f[d] = l[0] * n[d];
+        else if (mode == 1)
+            f[d] = (l[0] - l[1]) * n[d];
+        else
+            f[d] = (-l[0]) * n[d] + ((DIM == 2 && d == 2) ? (T)0 : l[1 + d]);
+    }
+}
+// global2local of a 3-vector x (lagrange_multiplier.hpp:400-426)
+template <typename T, int DIM>
+__device__ __forceinline__ void vf_local(int mode, const T* x, const T* n, T* o) {
+    T xn = 0;
+    for (int d = 0; d < DIM; ++d) xn += x[d] * n[d];
+    o[0] = mode == 2 ? -xn : xn;
+    o[1] = mode == 1 ? -xn : (mode == 2 ? x[0] : (T)0);
+    o[2] = mode == 2 ? x[1] : (T)0;
+    o[3] = (mode == 2 && DIM == 3) ? x[2] : (T)0;
+}
+// projection of one contact's slots (lagrange_multiplier.hpp:466-536): R+ per live slot in
+// modes 0 and 1; in mode 2 the nearer of (0, P_cone(f)) and (max(l0, 0), 0)
+template <int DIM>
+__device__ __forceinline__ void vf_project(int mode, double* z, const double* n, double mu) {
+    if (mode != 2) {
+        z[0] = z[0] > 0.0 ? z[0] : 0.0;
+        z[1] = mode == 1 ? (z[1] > 0.0 ? z[1] : 0.0) : 0.0;
+        z[2] = 0.0;
+        z[3] = 0.0;
+        return;
+    }
+    double fr[4] = {0.0, z[1], z[2], DIM == 3 ? z[3] : 0.0};
+    cone_project<DIM>(fr + 1, n, mu);
+    const double mo[4] = {z[0] > 0.0 ? z[0] : 0.0, 0.0, 0.0, 0.0};
+    double df = 0.0, dm = 0.0;
+    for (int k = 0; k < 1 + DIM; ++k) {
+        df += (fr[k] - z[k]) * (fr[k] - z[k]);
+        dm += (mo[k] - z[k]) * (mo[k] - z[k]);
+    }
+    const double* pick = sqrt(df) < sqrt(dm) ? fr : mo;
+    for (int k = 0; k < 1 + DIM; ++k) z[k] = pick[k];
+    if (DIM == 2) z[3] = 0.0;
+}
+
 template <typename T>
 struct ApgdArgs {
     int nin;
@@ -161,6 +211,7 @@ struct ApgdArgs {
     const int* ci;
     const int* cj;
     const int* slot;       // viscous
+    const int* mode;       // viscous friction
     const T* bn;
     const T* bai;
     const T* baj;
@@ -245,7 +296,7 @@ __device__ void contact_pass(const ApgdArgs<T>& A, int C, const T* lam, const T*
                              const T* up, T beta, bool use_prev, bool bt, double alpha, double* s) {
     GRID_STRIDE(c, C) {
         const int i = A.ci[c], j = A.cj[c];
-        if (PROB != kFriction) {
+        if (PROB != kFriction && PROB != kViscousFriction) {
             T qy = 0;
             if (!bt) {
                 T n[3];
@@ -282,7 +333,7 @@ __device__ void contact_pass(const ApgdArgs<T>& A, int C, const T* lam, const T*
                 if (sl >= 0) contact_scalar<T, DIM, PROB>(A, sl, -qy, -cc, lam, lprev, lnew, beta, use_prev, bt, alpha, s);
             }
         } else {
-            // friction: three multipliers per contact, A_c u = v_i + P_i^T w_i - v_j - P_j^T w_j
+            // friction rows: A_c u = v_i + P_i^T w_i - v_j - P_j^T w_j (three per contact)
             T qy[3] = {0, 0, 0};
             if (!bt) {
                 for (int side = 0; side < 2; ++side) {
@@ -300,40 +351,79 @@ __device__ void contact_pass(const ApgdArgs<T>& A, int C, const T* lam, const T*
                 }
                 for (int d = 0; d < 3; ++d) qy[d] *= (T)A.dt2;
             }
-            double y[3], gm[3], lm[3];
-            for (int d = 0; d < 3; ++d) {
-                const long long m = 3 * c + d;
-                lm[d] = (double)lam[m];
-                y[d] = use_prev ? (double)(lam[m] + beta * (lam[m] - lprev[m])) : lm[d];
-                if (bt) {
-                    gm[d] = (double)A.g[m];
-                } else {
-                    const T gg = qy[d] + A.cvec[m];
-                    A.g[m] = gg;
-                    gm[d] = (double)gg;
+            if constexpr (PROB == kViscousFriction) {
+                // four slots: g = global2local(Q y) + c, then the mode's projection
+                const int md = A.mode[c];
+                T nt[3] = {A.bn[3 * c], A.bn[3 * c + 1], A.bn[3 * c + 2]};
+                T ql[4];
+                vf_local<T, DIM>(md, qy, nt, ql);
+                double y[4], gm[4], lm[4], z[4], nd[3];
+                for (int k = 0; k < 4; ++k) {
+                    const long long m = 4 * c + k;
+                    lm[k] = (double)lam[m];
+                    y[k] = use_prev ? (double)(lam[m] + beta * (lam[m] - lprev[m])) : lm[k];
+                    if (bt) {
+                        gm[k] = (double)A.g[m];
+                    } else {
+                        const T gg = ql[k] + A.cvec[m];
+                        A.g[m] = gg;
+                        gm[k] = (double)gg;
+                    }
+                    z[k] = y[k] - alpha * gm[k];
+                    if (A.shift) z[k] += A.shift[m];
                 }
-            }
-            double z[3], n[3];
-            for (int d = 0; d < 3; ++d) {
-                n[d] = (double)A.bn[3 * c + d];
-                z[d] = y[d] - alpha * gm[d];
-                if (A.shift) z[d] += A.shift[3 * c + d];
-            }
-            if (DIM == 2) z[2] = A.shift ? A.shift[3 * c + 2] : 0.0;
-            cone_project<DIM>(z, n, A.mu);
-            for (int d = 0; d < 3; ++d) {
-                const long long m = 3 * c + d;
-                const T lp = (T)(A.shift ? z[d] - A.shift[m] : z[d]);
-                lnew[m] = lp;
-                const double dly = (double)lp - y[d], dll = (double)lp - lm[d];
-                const double cc = (double)A.cvec[m];
-                s[0] += gm[d] * dly;
-                s[1] += dly * dly;
-                s[2] += cc * (double)lp;
-                if (!bt) s[3] += y[d] * (0.5 * (double)qy[d] + cc);
-                s[4] += dll * dll;
-                s[5] += gm[d] * dll;
-                s[7] += (double)lp * (double)lp;
+                for (int d = 0; d < 3; ++d) nd[d] = (double)nt[d];
+                vf_project<DIM>(md, z, nd, A.mu);
+                for (int k = 0; k < 4; ++k) {
+                    const long long m = 4 * c + k;
+                    const T lp = (T)(A.shift ? z[k] - A.shift[m] : z[k]);
+                    lnew[m] = lp;
+                    const double dly = (double)lp - y[k], dll = (double)lp - lm[k];
+                    const double cc = (double)A.cvec[m];
+                    s[0] += gm[k] * dly;
+                    s[1] += dly * dly;
+                    s[2] += cc * (double)lp;
+                    if (!bt) s[3] += y[k] * (0.5 * (double)ql[k] + cc);
+                    s[4] += dll * dll;
+                    s[5] += gm[k] * dll;
+                    s[7] += (double)lp * (double)lp;
+                }
+            } else {
+                double y[3], gm[3], lm[3];
+                for (int d = 0; d < 3; ++d) {
+                    const long long m = 3 * c + d;
+                    lm[d] = (double)lam[m];
+                    y[d] = use_prev ? (double)(lam[m] + beta * (lam[m] - lprev[m])) : lm[d];
+                    if (bt) {
+                        gm[d] = (double)A.g[m];
+                    } else {
+                        const T gg = qy[d] + A.cvec[m];
+                        A.g[m] = gg;
+                        gm[d] = (double)gg;
+                    }
+                }
+                double z[3], n[3];
+                for (int d = 0; d < 3; ++d) {
+                    n[d] = (double)A.bn[3 * c + d];
+                    z[d] = y[d] - alpha * gm[d];
+                    if (A.shift) z[d] += A.shift[3 * c + d];
+                }
+                if (DIM == 2) z[2] = A.shift ? A.shift[3 * c + 2] : 0.0;
+                cone_project<DIM>(z, n, A.mu);
+                for (int d = 0; d < 3; ++d) {
+                    const long long m = 3 * c + d;
+                    const T lp = (T)(A.shift ? z[d] - A.shift[m] : z[d]);
+                    lnew[m] = lp;
+                    const double dly = (double)lp - y[d], dll = (double)lp - lm[d];
+                    const double cc = (double)A.cvec[m];
+                    s[0] += gm[d] * dly;
+                    s[1] += dly * dly;
+                    s[2] += cc * (double)lp;
+                    if (!bt) s[3] += y[d] * (0.5 * (double)qy[d] + cc);
+                    s[4] += dll * dll;
+                    s[5] += gm[d] * dll;
+                    s[7] += (double)lp * (double)lp;
+                }
             }
         }
     }
@@ -350,7 +440,7 @@ __device__ void particle_pass(const ApgdArgs<T>& A, const T* lnew, T* unew, cons
         for (int k = k0; k < k1; ++k) {
             const unsigned e = (unsigned)A.inc_idx[k];
             const long long c = e & 0x7fffffffu;
-            if (PROB != kFriction) {
+            if (PROB != kFriction && PROB != kViscousFriction) {
                 T mu = __ldcg(lnew + c);
                 if (PROB == kViscous) {
                     const int sl = A.slot[c];
@@ -363,7 +453,17 @@ __device__ void particle_pass(const ApgdArgs<T>& A, const T* lnew, T* unew, cons
             } else {
                 const int side = (int)(e >> 31);
                 const T sg = side == 0 ? (T)1 : (T)-1;
-                const T f[3] = {__ldcg(lnew + 3 * c), __ldcg(lnew + 3 * c + 1), __ldcg(lnew + 3 * c + 2)};
+                T f[3];
+                if (PROB == kViscousFriction) {
+                    const T l4[4] = {__ldcg(lnew + 4 * c), __ldcg(lnew + 4 * c + 1), __ldcg(lnew + 4 * c + 2),
+                                     __ldcg(lnew + 4 * c + 3)};
+                    const T nt[3] = {A.bn[3 * c], A.bn[3 * c + 1], A.bn[3 * c + 2]};
+                    vf_force<T, DIM>(A.mode[c], l4, nt, f);
+                } else {
+                    f[0] = __ldcg(lnew + 3 * c);
+                    f[1] = __ldcg(lnew + 3 * c + 1);
+                    f[2] = __ldcg(lnew + 3 * c + 2);
+                }
                 const T* P = A.bP + 18 * c + 9 * side;
                 for (int d = 0; d < 3; ++d) {
                     w[d] += sg * f[d];
@@ -428,7 +528,17 @@ __global__ void __launch_bounds__(kApgdThreads) k_apgd(ApgdArgs<T> A) {
         T* dbuf = lamb[in_];
         double s[kPartials] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
         GRID_STRIDE(c, C) {
-            if (PROB == kFriction) {
+            if (PROB == kViscousFriction) {
+                double z[4], n[3];
+                for (int d = 0; d < 3; ++d) n[d] = (double)A.bn[3 * c + d];
+                for (int k = 0; k < 4; ++k) z[k] = -(double)A.cvec[4 * c + k] + (A.shift ? A.shift[4 * c + k] : 0.0);
+                vf_project<DIM>(A.mode[c], z, n, A.mu);
+                for (int k = 0; k < 4; ++k) {
+                    const T v = (T)(z[k] - (A.shift ? A.shift[4 * c + k] : 0.0));
+                    dbuf[4 * c + k] = v;
+                    s[1] += (double)v * (double)v;
+                }
+            } else if (PROB == kFriction) {
                 double z[3], n[3];
                 for (int d = 0; d < 3; ++d) {
                     n[d] = (double)A.bn[3 * c + d];
@@ -559,13 +669,14 @@ __global__ void __launch_bounds__(kApgdThreads) k_apgd(ApgdArgs<T> A) {
 
 template <int DIM, int PROB>
 __global__ void k_particle_pass64(int nin, int na, const int* inc_ptr, const int* inc_idx, const double* coef,
-                                  const int* slot, const double* bP, const double* invm, const double* lam, double* u) {
+                                  const int* slot, const int* mode, const double* bn, const double* bP,
+                                  const double* invm, const double* lam, double* u) {
     GRID_STRIDE(p, na) {
         double w[6] = {0, 0, 0, 0, 0, 0};
         for (int k = inc_ptr[p]; k < inc_ptr[p + 1]; ++k) {
             const unsigned e = (unsigned)inc_idx[k];
             const long long c = e & 0x7fffffffu;
-            if (PROB != kFriction) {
+            if (PROB != kFriction && PROB != kViscousFriction) {
                 double mu = lam[c];
                 if (PROB == kViscous && slot[c] >= 0) mu -= lam[slot[c]];
                 for (int d = 0; d < 6; ++d) w[d] += mu * coef[6 * (long long)k + d];
@@ -573,7 +684,12 @@ __global__ void k_particle_pass64(int nin, int na, const int* inc_ptr, const int
                 const int side = (int)(e >> 31);
                 const double sg = side == 0 ? 1.0 : -1.0;
                 const double* P = bP + 18 * c + 9 * side;
-                const double f[3] = {lam[3 * c], lam[3 * c + 1], lam[3 * c + 2]};
+                double f[3];
+                if (PROB == kViscousFriction) {
+                    vf_force<double, DIM>(mode[c], lam + 4 * c, bn + 3 * c, f);
+                } else {
+                    for (int d = 0; d < 3; ++d) f[d] = lam[3 * c + d];
+                }
                 for (int d = 0; d < 3; ++d) {
                     w[d] += sg * f[d];
                     w[3 + d] += sg * (P[3 * d] * f[0] + P[3 * d + 1] * f[1] + P[3 * d + 2] * f[2]);
@@ -591,14 +707,15 @@ __global__ void k_particle_pass64(int nin, int na, const int* inc_ptr, const int
 }
 
 template <int DIM, int PROB>
-__global__ void k_residual64(int nin, const int* ci, const int* cj, const int* slot, const double* bn, const double* bai,
+__global__ void k_residual64(int nin, const int* ci, const int* cj, const int* slot, const int* mode,
+                             const double* bn, const double* bai,
                              const double* baj, const double* bP, const double* cvec, double dt2, const double* u,
                              double* g, unsigned long long* viol_bits, const Sizes* sizes) {
     const int C = sizes->C;
     double vmax = 0.0;
     GRID_STRIDE(c, C) {
         const int bi[2] = {ci[c], cj[c]};
-        if (PROB != kFriction) {
+        if (PROB != kFriction && PROB != kViscousFriction) {
             double qy = 0.0;
             for (int s = 0; s < 2; ++s) {
                 if (bi[s] < nin) continue;
@@ -627,6 +744,19 @@ __global__ void k_residual64(int nin, const int* ci, const int* cj, const int* s
                     q3[d] += sg * (vd + P[d] * uu[3] + P[3 + d] * uu[4] + P[6 + d] * uu[5]);
                 }
             }
+            if (PROB == kViscousFriction) {
+                // local residual global2local(Q l) + c; the gap n.(Q l + C) from the normal slot
+                // of c, which the S term does not touch
+                const int md = mode[c];
+                double qd[3], ql[4];
+                for (int d = 0; d < 3; ++d) qd[d] = dt2 * q3[d];
+                vf_local<double, DIM>(md, qd, bn + 3 * c, ql);
+                for (int k = 0; k < 4; ++k) g[4 * c + k] = ql[k] + cvec[4 * c + k];
+                const double qn = md == 2 ? -ql[0] : ql[0];
+                const double gap = qn + (md == 2 ? -cvec[4 * c] : cvec[4 * c]);
+                vmax = fmax(vmax, -gap);
+                continue;
+            }
             double gap = 0.0;
             for (int d = 0; d < 3; ++d) {
                 const double gg = dt2 * q3[d] + cvec[3 * c + d];
@@ -640,11 +770,16 @@ __global__ void k_residual64(int nin, const int* ci, const int* cj, const int* s
 }
 
 template <int DIM, int PROB, typename TD>
-__global__ void k_accumulate(const Sizes* sizes, const double* bn, const int* slot, double* lam, const TD* delta,
-                             int first, double mu) {
+__global__ void k_accumulate(const Sizes* sizes, const double* bn, const int* slot, const int* mode, double* lam,
+                             const TD* delta, int first, double mu) {
     const int C = sizes->C;
     GRID_STRIDE(c, C) {
-        if (PROB != kFriction) {
+        if (PROB == kViscousFriction) {
+            double z[4];
+            for (int k = 0; k < 4; ++k) z[k] = (first ? 0.0 : lam[4 * c + k]) + (double)delta[4 * c + k];
+            vf_project<DIM>(mode[c], z, bn + 3 * c, mu);
+            for (int k = 0; k < 4; ++k) lam[4 * c + k] = z[k];
+        } else if (PROB != kFriction) {
             const double v = (first ? 0.0 : lam[c]) + (double)delta[c];
             lam[c] = v > 0.0 ? v : 0.0;
             if (PROB == kViscous && slot[c] >= 0) {
@@ -676,6 +811,26 @@ __global__ void k_fixed_point_c(const Sizes* sizes, const double* base, const do
     }
 }
 
+// ViscousFriction: the S vector of LagrangeMultiplier<ViscousFriction>
+// (lagrange_multiplier.hpp:381-384), dt mu s_c n_c on the f slots of the mode-2 contacts
+template <int DIM>
+__global__ void k_vf_fixed_point_c(const Sizes* sizes, const double* base, const double* bn, const int* mode,
+                                   const double* sv, double dtmu, double* cvec) {
+    GRID_STRIDE(c, sizes->C) {
+        cvec[4 * c] = base[4 * c];
+        for (int d = 0; d < 3; ++d) {
+            const long long m = 4 * c + 1 + d;
+            cvec[m] = (mode[c] == 2 && d < DIM) ? base[m] + dtmu * sv[c] * bn[3 * c + d] : base[m];
+        }
+    }
+}
+
+// ViscousFriction: s_c = 1 on the contacts at gamma_min before the first solve
+// (OptimGradient.hpp:96-107); 0 elsewhere (never read)
+__global__ void k_vf_fixed_point_init(const Sizes* sizes, const double* gamma, double gamma_min, double* sv) {
+    GRID_STRIDE(c, sizes->C) sv[c] = gamma[c] == gamma_min ? 1. : 0.;
+}
+
 // s_c = mu dt before the first solve of a step (OptimGradient.hpp:85-94)
 __global__ void k_fixed_point_init(const Sizes* sizes, double* sv, double v) {
     GRID_STRIDE(c, sizes->C) sv[c] = v;
@@ -683,17 +838,21 @@ __global__ void k_fixed_point_init(const Sizes* sizes, double* sv, double v) {
 
 // After a solve (OptimGradient.hpp:117-176): U = v + dt M^-1 B^T l of the active bodies,
 // (A U)_c the contact's relative velocity (active bodies only, AMatrix::mat_mult), s_c =
-// mu dt |(A U)_c - n_c ((A U)_c.n_c)| over dim components; per block the sums of
-// (s_new - s_old)^2 and s_new^2 in a fixed order for the stopping test.
+// scale |(A U)_c - n_c ((A U)_c.n_c)| over dim components; per block the sums of
+// (s_new - s_old)^2 and s_new^2 in a fixed order for the stopping test.  FrictionFixedPoint:
+// scale = mu dt, every contact; ViscousFriction (:178-250): scale = 1, only the contacts
+// whose gamma equals gamma_min (gamma != nullptr).
 template <int DIM>
 __global__ void __launch_bounds__(kApgdThreads) k_fixed_point_s(const Sizes* sizes, int nin, const int* ci,
                                                                 const int* cj, const double* bn, const double* bP,
                                                                 const double* v, const double* omega,
-                                                                const double* u, double dt, double mu, double* sv,
+                                                                const double* u, double dt, double scale,
+                                                                const double* gamma, double gamma_min, double* sv,
                                                                 double* part) {
     const int C = sizes->C;
     double s[kPartials] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     GRID_STRIDE(c, C) {
+        if (gamma && gamma[c] != gamma_min) continue;
         const int bi[2] = {ci[c], cj[c]};
         double au[3] = {0, 0, 0};
         for (int side = 0; side < 2; ++side) {
@@ -716,7 +875,7 @@ __global__ void __launch_bounds__(kApgdThreads) k_fixed_point_s(const Sizes* siz
             const double t = au[d] - bn[3 * c + d] * dn;
             t2 += t * t;
         }
-        const double snew = mu * dt * sqrt(t2);
+        const double snew = scale * sqrt(t2);
         const double ds = snew - sv[c];
         s[0] += ds * ds;
         s[1] += snew * snew;
@@ -775,9 +934,11 @@ int apgd_max_blocks(int problem, int dim, bool fp32) {
 #define MB(T, D, P) \
     if (dim == D && problem == P) return max_blocks_t<T, D, P>();
     if (fp32) {
-        MB(float, 2, 0) MB(float, 2, 1) MB(float, 2, 2) MB(float, 3, 0) MB(float, 3, 1) MB(float, 3, 2)
+        MB(float, 2, 0) MB(float, 2, 1) MB(float, 2, 2) MB(float, 2, 4)
+        MB(float, 3, 0) MB(float, 3, 1) MB(float, 3, 2) MB(float, 3, 4)
     } else {
-        MB(double, 2, 0) MB(double, 2, 1) MB(double, 2, 2) MB(double, 3, 0) MB(double, 3, 1) MB(double, 3, 2)
+        MB(double, 2, 0) MB(double, 2, 1) MB(double, 2, 2) MB(double, 2, 4)
+        MB(double, 3, 0) MB(double, 3, 1) MB(double, 3, 2) MB(double, 3, 4)
     }
 #undef MB
     return 0;
@@ -793,6 +954,7 @@ cudaError_t launch_apgd_invm(const Bodies& b, const StepParams& p, const ApgdSet
     A.ci = c.ci;
     A.cj = c.cj;
     A.slot = a.slot;
+    A.mode = a.vflag;
     A.bn = sb.bn;
     A.bai = sb.bai;
     A.baj = sb.baj;
@@ -823,7 +985,7 @@ cudaError_t launch_apgd_invm(const Bodies& b, const StepParams& p, const ApgdSet
     A.dynamic = st.dynamic;
 #define LA(D, P) \
     if (p.dim == D && p.problem == P) return launch_apgd_t<T, D, P>(A, nblocks, s);
-    LA(2, 0) LA(2, 1) LA(2, 2) LA(3, 0) LA(3, 1) LA(3, 2)
+    LA(2, 0) LA(2, 1) LA(2, 2) LA(2, 4) LA(3, 0) LA(3, 1) LA(3, 2) LA(3, 4)
 #undef LA
     return cudaErrorInvalidValue;
 }
@@ -841,8 +1003,9 @@ void launch_particle_pass64(const Bodies& b, const StepParams& p, const Contacts
     if (na <= 0) return;
 #define PP(D, P) \
     if (p.dim == D && p.problem == P) \
-        k_particle_pass64<D, P><<<grid_blocks(na), 256, 0, s>>>(b.nin, na, inc.ptr, inc.idx, inc.coef, a.slot, a.bP, invm, lam, u);
-    PP(2, 0) PP(2, 1) PP(2, 2) PP(3, 0) PP(3, 1) PP(3, 2)
+        k_particle_pass64<D, P><<<grid_blocks(na), 256, 0, s>>>(b.nin, na, inc.ptr, inc.idx, inc.coef, a.slot, \
+                                                                a.vflag, a.bn, a.bP, invm, lam, u);
+    PP(2, 0) PP(2, 1) PP(2, 2) PP(2, 4) PP(3, 0) PP(3, 1) PP(3, 2) PP(3, 4)
 #undef PP
     g_apgd_launches += 1;
 }
@@ -852,14 +1015,24 @@ void launch_residual64(const Bodies& b, const StepParams& p, const Contacts& c, 
     const double dt2 = p.dt * p.dt;
 #define RR(D, P) \
     if (p.dim == D && p.problem == P) \
-        k_residual64<D, P><<<grid_blocks(c_cap), 256, 0, s>>>(b.nin, c.ci, c.cj, a.slot, a.bn, a.bai, a.baj, a.bP, a.cvec, dt2, u, g, viol_bits, sizes);
-    RR(2, 0) RR(2, 1) RR(2, 2) RR(3, 0) RR(3, 1) RR(3, 2)
+        k_residual64<D, P><<<grid_blocks(c_cap), 256, 0, s>>>(b.nin, c.ci, c.cj, a.slot, a.vflag, a.bn, a.bai, \
+                                                              a.baj, a.bP, a.cvec, dt2, u, g, viol_bits, sizes);
+    RR(2, 0) RR(2, 1) RR(2, 2) RR(2, 4) RR(3, 0) RR(3, 1) RR(3, 2) RR(3, 4)
 #undef RR
     g_apgd_launches += 1;
 }
 
 void launch_fixed_point_c(const StepParams& p, const Assembly& a, const double* base, const double* sv,
                           const Sizes* sizes, long long c_cap, cudaStream_t s) {
+    if (p.problem == kViscousFriction) {
+        const double dtmu = p.dt * p.mu;
+        if (p.dim == 3)
+            k_vf_fixed_point_c<3><<<grid_blocks(c_cap), 256, 0, s>>>(sizes, base, a.bn, a.vflag, sv, dtmu, a.cvec);
+        else
+            k_vf_fixed_point_c<2><<<grid_blocks(c_cap), 256, 0, s>>>(sizes, base, a.bn, a.vflag, sv, dtmu, a.cvec);
+        g_apgd_launches += 1;
+        return;
+    }
     if (p.dim == 3)
         k_fixed_point_c<3><<<grid_blocks(c_cap), 256, 0, s>>>(sizes, base, a.bn, sv, a.cvec);
     else
@@ -870,6 +1043,11 @@ void launch_fixed_point_init(double* sv, double v, const Sizes* sizes, long long
     k_fixed_point_init<<<grid_blocks(c_cap), 256, 0, s>>>(sizes, sv, v);
     g_apgd_launches += 1;
 }
+void launch_vf_fixed_point_init(double* sv, const double* gamma, double gamma_min, const Sizes* sizes,
+                                long long c_cap, cudaStream_t s) {
+    k_vf_fixed_point_init<<<grid_blocks(c_cap), 256, 0, s>>>(sizes, gamma, gamma_min, sv);
+    g_apgd_launches += 1;
+}
 int fixed_point_blocks(long long c_cap) {
     const long long b = (c_cap + kApgdThreads - 1) / kApgdThreads;
     return (int)std::max<long long>(1, std::min<long long>(b, kFixedPointMaxBlocks));
@@ -877,12 +1055,15 @@ int fixed_point_blocks(long long c_cap) {
 void launch_fixed_point_s(const Bodies& b, const StepParams& p, const Contacts& c, const Assembly& a, const double* u,
                           double* sv, double* part, const Sizes* sizes, long long c_cap, cudaStream_t s) {
     const int nb = fixed_point_blocks(c_cap);
+    const bool vf = p.problem == kViscousFriction;
+    const double scale = vf ? 1.0 : p.mu * p.dt;
+    const double* gam = vf ? c.gamma : nullptr;
     if (p.dim == 3)
         k_fixed_point_s<3><<<nb, kApgdThreads, 0, s>>>(sizes, b.nin, c.ci, c.cj, a.bn, a.bP, b.v, b.omega, u, p.dt,
-                                                       p.mu, sv, part);
+                                                       scale, gam, p.gamma_min, sv, part);
     else
         k_fixed_point_s<2><<<nb, kApgdThreads, 0, s>>>(sizes, b.nin, c.ci, c.cj, a.bn, a.bP, b.v, b.omega, u, p.dt,
-                                                       p.mu, sv, part);
+                                                       scale, gam, p.gamma_min, sv, part);
     g_apgd_launches += 1;
 }
 
@@ -891,8 +1072,9 @@ void launch_accumulate(const StepParams& p, const Contacts&, const Assembly& a, 
                        const Sizes* sizes, long long c_cap, int first, cudaStream_t s) {
 #define AC(D, P) \
     if (p.dim == D && p.problem == P) \
-        k_accumulate<D, P, TD><<<grid_blocks(c_cap), 256, 0, s>>>(sizes, a.bn, a.slot, lam64, delta, first, p.mu);
-    AC(2, 0) AC(2, 1) AC(2, 2) AC(3, 0) AC(3, 1) AC(3, 2)
+        k_accumulate<D, P, TD><<<grid_blocks(c_cap), 256, 0, s>>>(sizes, a.bn, a.slot, a.vflag, lam64, delta, \
+                                                                  first, p.mu);
+    AC(2, 0) AC(2, 1) AC(2, 2) AC(2, 4) AC(3, 0) AC(3, 1) AC(3, 2) AC(3, 4)
 #undef AC
     g_apgd_launches += 1;
 }

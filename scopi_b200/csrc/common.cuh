@@ -67,10 +67,11 @@ struct Contacts {
     double* nij;     // C*3
     double* pi;      // C*3
     double* pj;      // C*3
-    double* gamma;   // Viscous property
+    double* gamma;   // Viscous / ViscousFriction property
 };
 
-enum Problem { kNoFriction = 0, kFriction = 1, kViscous = 2 };
+// kernel problem codes; FrictionFixedPoint (3) runs the kFriction kernels inside its loop
+enum Problem { kNoFriction = 0, kFriction = 1, kViscous = 2, kViscousFriction = 4 };
 
 __host__ __device__ inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 

@@ -680,12 +680,26 @@ __global__ void k_assemble(Bodies B, StepParams p, Contacts c, Assembly a, const
         }
         double Cv[3];
         for (int d = 0; d < 3; ++d) Cv[d] = (d < DIM ? c.dij[k] * n[d] : 0.0) + p.dt * AU[d];
-        if (p.problem == kFriction) {
-            for (int d = 0; d < 3; ++d) a.cvec[3 * k + d] = Cv[d];
+        if (p.problem == kFriction || p.problem == kViscousFriction) {
             for (int e = 0; e < 9; ++e) {
                 a.bP[18 * (long long)k + e] = P[0][e];
                 a.bP[18 * (long long)k + 9 + e] = P[1][e];
             }
+        }
+        if (p.problem == kFriction) {
+            for (int d = 0; d < 3; ++d) a.cvec[3 * k + d] = Cv[d];
+        } else if (p.problem == kViscousFriction) {
+            // mode from gamma and c = global2local(C) on four slots (lagrange_multiplier.hpp:358-426)
+            double cn = 0.0;
+            for (int d = 0; d < DIM; ++d) cn += Cv[d] * n[d];
+            const double gm = c.gamma[k];
+            const int md = gm < -p.gamma_tol ? (gm != p.gamma_min ? 1 : 2) : 0;
+            a.vflag[k] = md;
+            double* cv = a.cvec + 4 * (long long)k;
+            cv[0] = md == 2 ? -cn : cn;
+            cv[1] = md == 1 ? -cn : (md == 2 ? Cv[0] : 0.0);
+            cv[2] = md == 2 ? Cv[1] : 0.0;
+            cv[3] = (md == 2 && DIM == 3) ? Cv[2] : 0.0;
         } else {
             double cc = 0.0;
             for (int d = 0; d < DIM; ++d) cc += Cv[d] * n[d];
@@ -773,6 +787,23 @@ __global__ void k_gamma_update(StepParams p, Contacts c, Assembly a, const doubl
         if (a.slot[k] >= 0) mu = lam[k] - lam[a.slot[k]];
         double dl = 0.0;
         for (int d = 0; d < p.dim; ++d) dl += c.nij[3 * k + d] * (mu * c.nij[3 * k + d]);
+        c.gamma[k] = fmin(fmax(c.gamma[k] - p.dt * dl, p.gamma_min), 0.);
+    }
+}
+
+// update_contact_properties_impl<ViscousFriction>, OptimGradient.hpp:36-52: the same update
+// with the force of the contact's four slots (mode in vflag: l n, (l+ - l-) n or -l0 n + f)
+__global__ void k_gamma_update_vf(StepParams p, Contacts c, Assembly a, const double* lam, const Sizes* sizes) {
+    const int C = sizes->C;
+    GRID_STRIDE(k, C) {
+        const double* l = lam + 4 * k;
+        const int md = a.vflag[k];
+        double dl = 0.0;
+        for (int d = 0; d < p.dim; ++d) {
+            const double nd = c.nij[3 * k + d];
+            const double f = md == 0 ? l[0] * nd : (md == 1 ? (l[0] - l[1]) * nd : (-l[0]) * nd + l[1 + d]);
+            dl += nd * f;
+        }
         c.gamma[k] = fmin(fmax(c.gamma[k] - p.dt * dl, p.gamma_min), 0.);
     }
 }
@@ -995,7 +1026,7 @@ void launch_incidence(const Bodies& b, const StepParams& p, const Contacts& c, c
     k_inc_fill<<<blocks_for(c_cap), kThreads, 0, s>>>(b.nin, c, sizes, inc.ptr, inc.jcount, inc.idx);
     k_inc_sort<<<blocks_for(na), kThreads, 0, s>>>(na, inc.ptr, inc.idx);
     LAUNCHED(3);
-    if (with_coef && p.problem != kFriction) {
+    if (with_coef && p.problem != kFriction && p.problem != kViscousFriction) {
         k_inc_coef<<<blocks_for(2 * c_cap), kThreads, 0, s>>>(na, inc.ptr, inc.idx, a, inc.coef);
         LAUNCHED(1);
     }
@@ -1003,7 +1034,10 @@ void launch_incidence(const Bodies& b, const StepParams& p, const Contacts& c, c
 
 void launch_gamma_update(const StepParams& p, Contacts& c, const Assembly& a, const double* lambda, const Sizes* sizes,
                          long long c_cap, cudaStream_t s) {
-    k_gamma_update<<<blocks_for(c_cap), kThreads, 0, s>>>(p, c, a, lambda, sizes);
+    if (p.problem == kViscousFriction)
+        k_gamma_update_vf<<<blocks_for(c_cap), kThreads, 0, s>>>(p, c, a, lambda, sizes);
+    else
+        k_gamma_update<<<blocks_for(c_cap), kThreads, 0, s>>>(p, c, a, lambda, sizes);
     LAUNCHED(1);
 }
 

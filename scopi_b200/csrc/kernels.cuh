@@ -55,8 +55,8 @@ struct Assembly {             // FP64 Jacobian rows, K = 1 (normal) problems
     double* bai;              // C*3  R_i^T (r_i x n)
     double* baj;              // C*3  -R_j^T (r_j x n)
     double* bP;               // C*18 friction: P_i = R_i^T [r_i]x, P_j = R_j^T [r_j]x
-    double* cvec;             // C (K=1) or 3C (friction)
-    int* vflag;               // C viscous flag, then scanned -> slot
+    double* cvec;             // C (K=1), 3C (friction) or 4C (viscous friction, local slots)
+    int* vflag;               // C viscous flag, then scanned -> slot; viscous friction: mode 0/1/2
     int* slot;                // C viscous second multiplier (-1 = none)
 };
 
@@ -169,9 +169,13 @@ void launch_residual64(const Bodies& b, const StepParams& p, const Contacts& c, 
 // FrictionFixedPoint: cvec = base + s n (dim components), and the s update after a solve
 // (u = M^-1 B^T l of the active bodies) with per-block partial sums (2 per block,
 // fixed_point_blocks(c_cap) blocks, at most kFixedPointMaxBlocks) of (s_new - s_old)^2, s_new^2.
+// ViscousFriction (p.problem == kViscousFriction): cvec = base + dt mu s n on the f slots of
+// the mode-2 contacts, s = 1 there before the first solve, s = |(A U)_t| after each.
 constexpr int kFixedPointMaxBlocks = 1024;
 int fixed_point_blocks(long long c_cap);
 void launch_fixed_point_init(double* sv, double v, const Sizes* sizes, long long c_cap, cudaStream_t s);
+void launch_vf_fixed_point_init(double* sv, const double* gamma, double gamma_min, const Sizes* sizes,
+                                long long c_cap, cudaStream_t s);
 void launch_fixed_point_c(const StepParams& p, const Assembly& a, const double* base, const double* sv,
                           const Sizes* sizes, long long c_cap, cudaStream_t s);
 void launch_fixed_point_s(const Bodies& b, const StepParams& p, const Contacts& c, const Assembly& a, const double* u,

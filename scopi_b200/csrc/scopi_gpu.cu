@@ -108,8 +108,9 @@ struct scopi_gpu_handle {
     unsigned long long* h_viol = nullptr;
     int max_blocks64 = 0, max_blocks32 = 0, max_sph64 = 0, max_sph32 = 0;
     // FrictionFixedPoint: P.problem holds FRICTION (the kernels' problem), this flag the loop
+    // (ViscousFriction keeps its own problem code and runs the same loop)
     bool fixed_point = false;
-    double* d_cvec_base = nullptr;  // 3C: the Friction linear term of the step
+    double* d_cvec_base = nullptr;  // 3C (4C): the linear term of the step without the s term
     double* d_fp_s = nullptr;       // C: s_c
     double* d_fp_part = nullptr;    // 2 per block of the s update
     double* h_fp_part = nullptr;    // pinned copy
@@ -129,14 +130,22 @@ struct scopi_gpu_handle {
         err = std::string(where) + ": " + cudaGetErrorString(e);
         return SCOPI_GPU_ECUDA;
     }
-    int mult_per_contact() const { return P.problem == SCOPI_GPU_FRICTION ? 3 : (P.problem == SCOPI_GPU_VISCOUS ? 2 : 1); }
+    int mult_per_contact() const {
+        return P.problem == SCOPI_GPU_VISCOUS_FRICTION ? 4
+                                                       : (friction_rows() ? 3 : (P.problem == SCOPI_GPU_VISCOUS ? 2 : 1));
+    }
+    // multipliers in c (and the Jacobian kept as the three rows of A) per contact
+    int cvec_per() const { return P.problem == SCOPI_GPU_VISCOUS_FRICTION ? 4 : (friction_rows() ? 3 : 1); }
+    bool friction_rows() const { return P.problem == SCOPI_GPU_FRICTION || P.problem == SCOPI_GPU_VISCOUS_FRICTION; }
+    bool viscous_friction() const { return P.problem == SCOPI_GPU_VISCOUS_FRICTION; }
+    bool fp_loop() const { return fixed_point || viscous_friction(); }
     bool mixed() const { return P.precision == SCOPI_GPU_MIXED; }
     // Normal-only problems: every pair type of the hot path (sphere-sphere, sphere-plane,
     // sphere-segment) has its lever arm along the normal, so the rotational Jacobian terms
     // vanish and the translational kernels apply.
     // torque-free rows: every contact's lever arms are parallel to its normal (spheres,
     // planes, segments); superellipsoid contacts need the 6-dof rows
-    bool sphere_mode() const { return P.problem != SCOPI_GPU_FRICTION && !has_se; }
+    bool sphere_mode() const { return !friction_rows() && !has_se; }
 
     Bodies bodies() const {
         Bodies b;
@@ -452,7 +461,7 @@ struct scopi_gpu_handle {
         if ((e = cudaMallocHost(&h_result, sizeof(ApgdResult))) != cudaSuccess) return cuda_fail(e, "cudaMallocHost");
         if ((e = cudaMallocHost(&h_viol, sizeof(unsigned long long))) != cudaSuccess)
             return cuda_fail(e, "cudaMallocHost");
-        if (fixed_point) {
+        if (fp_loop()) {
             if ((e = alloc(fixed_mem, d_fp_part, 2 * (size_t)kFixedPointMaxBlocks)) != cudaSuccess)
                 return cuda_fail(e, "alloc");
             if ((e = cudaMallocHost(&h_fp_part, 2 * sizeof(double) * kFixedPointMaxBlocks)) != cudaSuccess)
@@ -515,18 +524,18 @@ struct scopi_gpu_handle {
             A(c->gamma, cap)
         }
         A(as.bn, 3 * cap) A(as.bai, 3 * cap) A(as.baj, 3 * cap)
-        if (P.problem == SCOPI_GPU_FRICTION) A(as.bP, 18 * cap)
-        A(as.cvec, (P.problem == SCOPI_GPU_FRICTION ? 3 : 1) * cap) A(as.vflag, cap) A(as.slot, cap)
-        if (fixed_point) {
-            A(d_cvec_base, 3 * cap) A(d_fp_s, cap)
+        if (friction_rows()) A(as.bP, 18 * cap)
+        A(as.cvec, cvec_per() * cap) A(as.vflag, cap) A(as.slot, cap)
+        if (fp_loop()) {
+            A(d_cvec_base, cvec_per() * cap) A(d_fp_s, cap)
         }
         A(inc.idx, 2 * cap) A(inc.coef, 12 * cap)
         for (int k = 0; k < 3; ++k) A(d_lam64[k], M)
         A(d_g64, M) A(d_res64, M) A(d_lamacc, M)
         if (mixed()) {
             A(d_bn32, 3 * cap) A(d_bai32, 3 * cap) A(d_baj32, 3 * cap)
-            if (P.problem == SCOPI_GPU_FRICTION) A(d_bP32, 18 * cap)
-            A(d_cvec32, (P.problem == SCOPI_GPU_FRICTION ? 3 : 1) * cap) A(d_coef32, 12 * cap)
+            if (friction_rows()) A(d_bP32, 18 * cap)
+            A(d_cvec32, cvec_per() * cap) A(d_coef32, 12 * cap)
             for (int k = 0; k < 3; ++k) A(d_lam32[k], M)
             A(d_g32, M)
         }
@@ -724,7 +733,7 @@ struct scopi_gpu_handle {
         int rc = detect_and_assemble(dt, true);
         if (rc) return rc;
         const int C = h_sizes->C;
-        const long long M = P.problem == SCOPI_GPU_FRICTION ? 3LL * C : (long long)C + h_sizes->n_extra;
+        const long long M = friction_rows() ? (long long)mult_per_contact() * C : (long long)C + h_sizes->n_extra;
         cudaEventRecord(ev[1], stream);
         const double* ufin = nullptr;
         int ustride = 6, urot = 1;
@@ -790,14 +799,21 @@ struct scopi_gpu_handle {
             }
             return 0;
             };
-            if (fixed_point) {
+            if (fp_loop()) {
                 // FrictionFixedPoint (OptimGradient.hpp:85-176, solver.hpp:286-291): s_c = mu dt,
                 // then solve with the linear term c + s n, update s from the tangential relative
-                // velocity, until the relative change of s is below fixed_point_tol
-                cudaMemcpyAsync(d_cvec_base, as.cvec, 3 * (size_t)C * sizeof(double), cudaMemcpyDeviceToDevice,
-                                stream);
+                // velocity, until the relative change of s is below fixed_point_tol.
+                // ViscousFriction (OptimGradient.hpp:96-107, 178-250): s_c = 1 on the contacts at
+                // gamma_min, linear term c + dt mu s n on their friction slots, s = |(A u)_t|, the
+                // change measured without the 1/(mu dt) scale.
+                const bool vf = viscous_friction();
+                cudaMemcpyAsync(d_cvec_base, as.cvec, (size_t)cvec_per() * C * sizeof(double),
+                                cudaMemcpyDeviceToDevice, stream);
                 const double mudt = P.mu * dt;
-                launch_fixed_point_init(d_fp_s, mudt, d_sizes_cur, c_cap, stream);
+                if (vf)
+                    launch_vf_fixed_point_init(d_fp_s, cur.gamma, P.gamma_min, d_sizes_cur, c_cap, stream);
+                else
+                    launch_fixed_point_init(d_fp_s, mudt, d_sizes_cur, c_cap, stream);
                 const int nbk = fixed_point_blocks(c_cap);
                 long long it = 0;
                 for (;;) {
@@ -814,10 +830,15 @@ struct scopi_gpu_handle {
                         ss += h_fp_part[2 * k + 1];
                     }
                     ++it;
-                    // mu dt = 0: s stays 0 and one solve is the answer (the reference's
-                    // normalisation by 1/(mu dt) would give NaN and run fixed_point_max_iter solves)
-                    if (!(mudt > 0.0)) break;
-                    const double err = (std::sqrt(dd) / mudt) / (1.0 + std::sqrt(ss) / mudt);
+                    double err;
+                    if (vf) {
+                        err = std::sqrt(dd) / (1.0 + std::sqrt(ss));
+                    } else {
+                        // mu dt = 0: s stays 0 and one solve is the answer (the reference's
+                        // normalisation by 1/(mu dt) would give NaN and run fixed_point_max_iter solves)
+                        if (!(mudt > 0.0)) break;
+                        err = (std::sqrt(dd) / mudt) / (1.0 + std::sqrt(ss) / mudt);
+                    }
                     if (err < P.fixed_point_tol || it >= P.fixed_point_max_iter) break;
                 }
                 stats.fixed_point_iterations = it;
@@ -834,7 +855,8 @@ struct scopi_gpu_handle {
             else
                 launch_residual64(b, sp, cur, as, ufin, d_res64, d_viol, d_sizes_cur, c_cap, stream);
             cudaMemcpyAsync(h_viol, d_viol, sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream);
-            if (P.problem == SCOPI_GPU_VISCOUS) launch_gamma_update(sp, cur, as, last_lambda, d_sizes_cur, c_cap, stream);
+            if (P.problem == SCOPI_GPU_VISCOUS || viscous_friction())
+                launch_gamma_update(sp, cur, as, last_lambda, d_sizes_cur, c_cap, stream);
         } else {
             last_lambda = nullptr;
             *h_viol = 0;
@@ -880,7 +902,7 @@ struct scopi_gpu_handle {
     int mixed_solve(double dt, long long M, float& ms_apgd) {
         Bodies b = bodies();
         StepParams sp = step_params(dt);
-        const int per = P.problem == SCOPI_GPU_FRICTION ? 3 : 1;
+        const int per = cvec_per();
         SphSolve<float> sbs{};
         SolveBuffers<float> sb{};
         if (sphere_mode()) {
@@ -891,7 +913,7 @@ struct scopi_gpu_handle {
             launch_convert<double, float>(as.bn, d_bn32, 3 * c_cap, &d_sizes_cur->C, 3, stream);
             launch_convert<double, float>(as.bai, d_bai32, 3 * c_cap, &d_sizes_cur->C, 3, stream);
             launch_convert<double, float>(as.baj, d_baj32, 3 * c_cap, &d_sizes_cur->C, 3, stream);
-            if (P.problem == SCOPI_GPU_FRICTION)
+            if (friction_rows())
                 launch_convert<double, float>(as.bP, d_bP32, 18 * c_cap, &d_sizes_cur->C, 18, stream);
             else
                 launch_convert<double, float>(inc.coef, d_coef32, 12 * c_cap, &d_sizes_cur->C, 12, stream);
@@ -1060,9 +1082,10 @@ int32_t scopi_gpu_create(const scopi_gpu_params* p, scopi_gpu_handle** out) {
         scopi_gpu::set_global_error("dim must be 2 or 3");
         return SCOPI_GPU_EINVAL;
     }
-    if (p->problem < 0 || p->problem > 3 || p->vap < 0 || p->vap > 1 || p->contact_method < 0 ||
+    const bool loop = p->problem == SCOPI_GPU_FRICTION_FIXED_POINT || p->problem == SCOPI_GPU_VISCOUS_FRICTION;
+    if (p->problem < 0 || p->problem > 4 || p->vap < 0 || p->vap > 1 || p->contact_method < 0 ||
         p->contact_method > 1 || p->precision < 0 || p->precision > 1 || p->alpha <= 0 || p->max_ite < 1 ||
-        (p->problem == SCOPI_GPU_FRICTION_FIXED_POINT && (!(p->fixed_point_tol >= 0) || p->fixed_point_max_iter < 1))) {
+        (loop && (!(p->fixed_point_tol >= 0) || p->fixed_point_max_iter < 1))) {
         scopi_gpu::set_global_error("invalid parameter");
         return SCOPI_GPU_EINVAL;
     }
@@ -1184,7 +1207,7 @@ static int32_t upload_particles(scopi_gpu_handle* h, const scopi_gpu_particles* 
             return h->fail(SCOPI_GPU_EUNSUPPORTED, "2D superellipsoids: scenes without obstacles");
         if (n_sph > 0) return h->fail(SCOPI_GPU_EUNSUPPORTED, "spheres and superellipsoids cannot be mixed");
         if (!p->axes || !p->squareness) return h->fail(SCOPI_GPU_EINVAL, "superellipsoid axes / squareness missing");
-        if (h->P.problem == SCOPI_GPU_VISCOUS)
+        if (h->P.problem == SCOPI_GPU_VISCOUS || h->P.problem == SCOPI_GPU_VISCOUS_FRICTION)
             return h->fail(SCOPI_GPU_EUNSUPPORTED, "superellipsoids: NoFriction and Friction problems");
         if (h->batch) return h->fail(SCOPI_GPU_EUNSUPPORTED, "batches hold sphere scenes");
         const bool d3 = h->P.dim == 3;  // 2D: (rx, ry) and e
@@ -1309,6 +1332,25 @@ int32_t scopi_gpu_get_lambda(scopi_gpu_handle* h, int64_t cap, int64_t* nout, do
     if (!h) return SCOPI_GPU_EINVAL;
     cudaSetDevice(h->dev);
     const long long M = h->last_lambda ? h->last_M : 0;
+    if (h->viscous_friction() && M > 0) {
+        // four slots per contact on the device; the reference's rows are 1, 2 or 4 per contact
+        // by mode (lagrange_multiplier.hpp:358-379), in contact order
+        const long long C = M / 4;
+        std::vector<double> l4(M);
+        std::vector<int> md(C);
+        cudaError_t e = cudaMemcpy(l4.data(), h->last_lambda, M * sizeof(double), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(md.data(), h->as.vflag, C * sizeof(int), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return h->cuda_fail(e, "get_lambda");
+        std::vector<double> rows;
+        rows.reserve(M);
+        for (long long c = 0; c < C; ++c) {
+            const int k = md[c] == 2 ? 4 : (md[c] == 1 ? 2 : 1);
+            for (int r = 0; r < k; ++r) rows.push_back(l4[4 * c + r]);
+        }
+        if (nout) *nout = (int64_t)rows.size();
+        if (lambda) std::copy(rows.begin(), rows.begin() + std::min<long long>((long long)rows.size(), cap), lambda);
+        return 0;
+    }
     if (nout) *nout = M;
     const long long k = std::min<long long>(M, cap);
     if (k > 0 && lambda) {

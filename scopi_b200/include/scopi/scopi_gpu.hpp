@@ -86,6 +86,7 @@ class NoFriction {};
 class Friction {};
 class Viscous {};
 class FrictionFixedPoint {};  // property.hpp:26
+class ViscousFriction {};     // property.hpp:34
 
 template <class problem_t>
 struct contact_property;
@@ -106,12 +107,19 @@ struct contact_property<FrictionFixedPoint> : contact_property<Friction> {  // p
     double fixed_point_tol = 1e-6;
     double fixed_point_max_iter = 1000;
 };
+template <>
+struct contact_property<ViscousFriction> : contact_property<Viscous>,  // property.hpp:149-172
+                                           contact_property<Friction> {
+    double fixed_point_tol = 1e-6;
+    double fixed_point_max_iter = 1000;
+};
 
 template <class problem_t>
 constexpr int32_t problem_code() {
     if constexpr (std::is_same_v<problem_t, Friction>) return SCOPI_GPU_FRICTION;
     if constexpr (std::is_same_v<problem_t, Viscous>) return SCOPI_GPU_VISCOUS;
     if constexpr (std::is_same_v<problem_t, FrictionFixedPoint>) return SCOPI_GPU_FRICTION_FIXED_POINT;
+    if constexpr (std::is_same_v<problem_t, ViscousFriction>) return SCOPI_GPU_VISCOUS_FRICTION;
     return SCOPI_GPU_NOFRICTION;
 }
 
@@ -1003,7 +1011,8 @@ class ScopiSolver {
                 c.pi[x] = pi[3 * k + x];
                 c.pj[x] = pj[3 * k + x];
             }
-            if constexpr (std::is_same_v<problem_t, Viscous>) c.property.gamma = g[k];
+            if constexpr (std::is_same_v<problem_t, Viscous> || std::is_same_v<problem_t, ViscousFriction>)
+                c.property.gamma = g[k];
         }
         return m_contacts;
     }
@@ -1041,6 +1050,14 @@ class ScopiSolver {
             o.set("gamma", Value::number(c.property.gamma));
             o.set("gamma_min", Value::number(m_default_property.gamma_min));
             o.set("gamma_tol", Value::number(m_default_property.gamma_tol));
+        } else if constexpr (std::is_same_v<problem_t, ViscousFriction>) {
+            o.set("type", Value::string("viscous friction"));
+            o.set("gamma", Value::number(c.property.gamma));
+            o.set("gamma_min", Value::number(m_default_property.gamma_min));
+            o.set("gamma_tol", Value::number(m_default_property.gamma_tol));
+            o.set("mu", Value::number(m_default_property.mu));
+            o.set("fixed_point_tol", Value::number(m_default_property.fixed_point_tol));
+            o.set("fixed_point_max_iter", Value::number(m_default_property.fixed_point_max_iter));
         } else {
             (void)c;
             o.set("type", Value::string("no friction"));
@@ -1076,10 +1093,15 @@ class ScopiSolver {
             p.fixed_point_tol = m_default_property.fixed_point_tol;
             p.fixed_point_max_iter = (int64_t)m_default_property.fixed_point_max_iter;
         }
-        if constexpr (std::is_same_v<problem_t, Viscous>) {
+        if constexpr (std::is_same_v<problem_t, Viscous> || std::is_same_v<problem_t, ViscousFriction>) {
             p.gamma = m_default_property.gamma;
             p.gamma_min = m_default_property.gamma_min;
             p.gamma_tol = m_default_property.gamma_tol;
+        }
+        if constexpr (std::is_same_v<problem_t, ViscousFriction>) {
+            p.mu = m_default_property.mu;
+            p.fixed_point_tol = m_default_property.fixed_point_tol;
+            p.fixed_point_max_iter = (int64_t)m_default_property.fixed_point_max_iter;
         }
         const int32_t rc = scopi_gpu_create(&p, &m_h);
         if (rc < 0) throw gpu_error(std::string("scopi_gpu_create: ") + scopi_gpu_last_error(nullptr));

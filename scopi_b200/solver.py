@@ -19,7 +19,7 @@ import numpy as np
 
 from . import _abi
 from ._abi import (BRUTE_FORCE, FP64, FRICTION, FRICTION_FIXED_POINT, KDTREE, MIXED, NOFRICTION,  # noqa: F401
-                   VAP_FIXED, VAP_FPD, VISCOUS)
+                   VAP_FIXED, VAP_FPD, VISCOUS, VISCOUS_FRICTION)
 from .container import ParticleArrays
 
 

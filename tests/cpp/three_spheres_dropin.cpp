@@ -1,11 +1,12 @@
-// Drop-in check: the "3 Spheres NoFriction / Viscous" scenes of the reference's solver
-// tests (test/test_gradient.cpp:377-503) written against the scopi:: API exactly as a
+// Drop-in check: the "3 Spheres NoFriction / Viscous / Viscous Friction" scenes of the
+// reference's solver tests (test/test_gradient.cpp:377-503, 574-642) written against the scopi:: API exactly as a
 // reference user writes them; only the headers differ (B200 engine through the C ABI).
 // Prints the final state as JSON for the Python side to compare with the golden files; with
 // an output directory as second argument the solver also writes its snapshot files there,
 // the last one after the final step (output_frequency = total_it).
 #include <cstdio>
 #include <cstring>
+#include <type_traits>
 
 #include <scopi/container.hpp>
 #include <scopi/objects/types/sphere.hpp>
@@ -33,6 +34,14 @@ int run(double Tf, const char* outdir, const char* name) {
     params.optim_params.max_ite = 10000;
     params.optim_params.alpha = 0.1;
     params.optim_params.dynamic_descent = true;
+    if constexpr (std::is_same_v<problem_t, scopi::ViscousFriction>) {
+        params.default_contact_property.mu = 0.5;
+        params.default_contact_property.fixed_point_tol = 1e-3;
+        params.default_contact_property.fixed_point_max_iter = 1000;
+        params.default_contact_property.gamma = 0;
+        params.default_contact_property.gamma_min = -1.4;
+        params.default_contact_property.gamma_tol = 1e-6;
+    }
     std::size_t total_it = Tf / dt;
     if (outdir) {
         params.solver_params.output_frequency = total_it;
@@ -56,5 +65,7 @@ int run(double Tf, const char* outdir, const char* name) {
 int main(int argc, char** argv) {
     const char* outdir = argc > 2 ? argv[2] : nullptr;
     if (argc > 1 && std::strcmp(argv[1], "viscous") == 0) return run<scopi::Viscous>(7.0, outdir, "3spheres_viscous");
+    if (argc > 1 && std::strcmp(argv[1], "viscous_friction") == 0)
+        return run<scopi::ViscousFriction>(7.0, outdir, "3spheres_viscous_friction");
     return run<scopi::NoFriction>(6.0, outdir, "3spheres_nofriction");
 }

@@ -385,3 +385,24 @@ def analytic_viscous_friction(alpha, mu, t, r, g, y0, gamma_min, t_inv):
     else:
         y, vy = g * ca * (t - t_unstick) ** 2 / 2 + r, g * ca * (t - t_unstick)
     return (x, y), ang, (vx, vy), w_i
+
+
+def viscous_friction_3d(mu=0.3, gamma_min=-0.03):
+    """ViscousFriction in 3D: a 3x3 layer of touching spheres (r 0.5) on the floor plane z = 0
+    with a 2x2 layer in its pockets, under gravity tilted by pi/6 along x, vap_fpd, dt 0.01.
+    The floor contacts pass through the viscous pair to gamma_min within a few steps, then
+    slide on the friction cone."""
+    p = Particles(3)
+    p.add_plane((0.0, 0.0, 0.0), q=quaternion(PI / 2, (0, 1, 0)))
+    r, a = 0.5, PI / 6
+    prop = dict(mass=1.0, moment_inertia=(0.1, 0.1, 0.1), force=(math.sin(a), 0.0, -math.cos(a)))
+    for i in range(3):
+        for j in range(3):
+            p.add_sphere((float(i), float(j), r), r, Property(**prop))
+    z2 = r + math.sqrt(0.5)
+    for i in range(2):
+        for j in range(2):
+            p.add_sphere((i + 0.5, j + 0.5, z2), r, Property(**prop))
+    kw = dict(problem=VISCOUS_FRICTION, vap=VAP_FPD, tolerance=1e-7, max_ite=10000, alpha=0.1, mu=mu, dmax=0.1,
+              fixed_point_tol=1e-3, fixed_point_max_iter=1000, gamma=0.0, gamma_min=gamma_min, gamma_tol=1e-6)
+    return p.finalize(), kw, 0.01, 40

@@ -35,7 +35,8 @@ def exe(tmp_path_factory):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("mode,name", [("nofriction", "3spheres_nofriction"), ("viscous", "3spheres_viscous")])
+@pytest.mark.parametrize("mode,name", [("nofriction", "3spheres_nofriction"), ("viscous", "3spheres_viscous"),
+                                       ("viscous_friction", "3spheres_viscous_friction")])
 def test_cpp_api_matches_reference_golden(exe, golden, mode, name, tmp_path):
     res = json.loads(subprocess.run([exe, mode], check=True, capture_output=True, text=True, cwd=tmp_path).stdout)
     worst = 0.0
@@ -241,7 +242,8 @@ def test_snapshot_writer_formats(tmp_path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("mode,name", [("nofriction", "3spheres_nofriction"), ("viscous", "3spheres_viscous")])
+@pytest.mark.parametrize("mode,name", [("nofriction", "3spheres_nofriction"), ("viscous", "3spheres_viscous"),
+                                       ("viscous_friction", "3spheres_viscous_friction")])
 def test_cpp_snapshot_files_match_reference_golden(exe, golden, mode, name, tmp_path):
     """The reference's "3 Spheres" tests with snapshot files (output_frequency = total_it):
     the initial snapshot and the final one, whose objects agree with the reference's golden

@@ -80,7 +80,8 @@ def test_matrix_known_values_and_adjoint():
 GOLDEN_CASES = [
     ("3spheres_nofriction", lambda: S.three_spheres(S.NOFRICTION), 1e-5),
     ("3spheres_viscous", lambda: S.three_spheres(S.VISCOUS), 1e-5),
-    ("3spheres_friction_fp", lambda: S.three_spheres(3), 1e-5),
+    ("3spheres_friction_fp", lambda: S.three_spheres(S.FRICTION_FIXED_POINT), 1e-5),
+    ("3spheres_viscous_friction", lambda: S.three_spheres(S.VISCOUS_FRICTION), 1e-5),
     ("sphere_plane_friction_mu01", S.sphere_plane_friction_mu01, 1e-5),
     ("two_spheres_asymmetrical", lambda: S.two_spheres(False), 1e-6),
     ("two_spheres_symmetrical", lambda: S.two_spheres(True), 1e-6),
@@ -278,3 +279,81 @@ def test_friction_fixed_point_sphere_plane(precision):
         assert rel_err(g.particles.pos, o.pa.pos) <= 1e-7
         assert rel_err(g.particles.v, o.pa.v) <= 1e-5
         assert math.isclose(g.particles.omega[1, 2], o.pa.omega[1, 2], rel_tol=1e-5)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_viscous_friction_sphere_plane(precision):
+    """ViscousFriction on the reference's analytic case (test/test_gradient.cpp:284-372): 500
+    steps, the force flipped, 100 more; the reference's bounds (pos, q 1e-1; v, omega 1e-3) and
+    (FP64) the oracle's trajectory, which runs the same fixed-point loop."""
+    from test_oracle_golden import viscous_friction_errors
+    pa, kw, dt, total = S.sphere_plane_viscous_friction()
+    g = gpu_solver(pa, precision=precision, **kw)
+    g.run(dt, total)
+    p2 = g.particles.copy()
+    p2.f[1, :2] = (-math.sin(math.pi / 4), math.cos(math.pi / 4))
+    g.set_particles(p2)
+    g.run(dt, 100)
+    e_pos, e_q, e_v, e_om = viscous_friction_errors(g.particles, dt, total, 100)
+    assert e_pos <= 1e-1 and e_q <= 1e-1, (e_pos, e_q)
+    assert e_v <= 1e-3 and e_om <= 1e-3, (e_v, e_om)
+    if precision == 0:
+        o = oracle_solver(pa, **kw)
+        o.run(dt, total)
+        q2 = o.pa.copy()
+        q2.f[1, :2] = (-math.sin(math.pi / 4), math.cos(math.pi / 4))
+        o.set_particles(q2)
+        o.run(dt, 100)
+        assert rel_err(g.particles.pos, o.pa.pos) <= 1e-7
+        assert rel_err(g.particles.v, o.pa.v) <= 1e-5
+        assert math.isclose(g.particles.omega[1, 2], o.pa.omega[1, 2], rel_tol=1e-5, abs_tol=1e-9)
+
+
+def viscous_friction_3d_deviations(steps=None):
+    """Step the GPU (FP64) and the oracle together on the 3D ViscousFriction scene; the contact
+    pairs and the modes (gamma at gamma_min, and the multipliers' row count in the reference's
+    layout) must agree on every step; returns the worst deviations and the modes seen."""
+    pa, kw, dt, total = S.viscous_friction_3d()
+    g = gpu_solver(pa, **kw)
+    o = oracle_solver(pa, **kw)
+    seen = set()
+    worst = {"gamma": 0.0, "lambda_rel": 0.0, "pos": 0.0, "v": 0.0}
+    gmin = kw["gamma_min"]
+    for k in range(total if steps is None else steps):
+        g.run(dt, 1)
+        o.run(dt, 1)
+        gc, oc = g.current_contacts(), o.contacts()
+        assert np.array_equal(gc["i"], oc["i"]) and np.array_equal(gc["j"], oc["j"]), k
+        for gam in oc["gamma"]:
+            seen.add(0 if gam >= -kw["gamma_tol"] else (2 if gam == gmin else 1))
+        assert np.array_equal(gc["gamma"] == gmin, oc["gamma"] == gmin), k
+        lg, lo = g.lagrange_multiplier(), o.lagrange_multiplier()
+        assert len(lg) == len(lo), k
+        assert g.stats()["fixed_point_iterations"] >= 1
+        worst["gamma"] = max(worst["gamma"], float(np.max(np.abs(gc["gamma"] - oc["gamma"]))))
+        worst["lambda_rel"] = max(worst["lambda_rel"], float(np.linalg.norm(lg - lo) / (1 + np.linalg.norm(lo))))
+        worst["pos"] = max(worst["pos"], rel_err(g.particles.pos, o.pa.pos))
+        worst["v"] = max(worst["v"], rel_err(g.particles.v, o.pa.v))
+    return worst, seen
+
+
+def test_viscous_friction_3d_matches_oracle():
+    """ViscousFriction in 3D with all three multiplier layouts live (normal, viscous pair,
+    gamma_min with the friction cone), FP64 against the oracle step by step.  The multipliers
+    agree to the solver's accuracy (APGD tolerance 1e-7, a few solves per step), gamma
+    accumulates dt n.lambda of each step (40 steps of dt 0.01), positions and velocities
+    follow."""
+    worst, seen = viscous_friction_3d_deviations()
+    assert seen == {0, 1, 2}, seen
+    assert worst["lambda_rel"] <= 1e-5 and worst["gamma"] <= 1e-7, worst
+    assert worst["pos"] <= 1e-7 and worst["v"] <= 1e-5, worst
+
+
+def test_viscous_friction_3d_mixed_precision():
+    """The mixed path (FP32 iterations, FP64 corrections) on the same 3D scene: the
+    trajectory of the FP64 solve within the FP32 solves' accuracy."""
+    pa, kw, dt, total = S.viscous_friction_3d()
+    f64 = gpu_solver(pa, **kw).run(dt, total)
+    mix = gpu_solver(pa, precision=1, mixed_violation_tol=1e-6, **kw).run(dt, total)
+    assert rel_err(mix.particles.pos, f64.particles.pos) <= 1e-6
+    assert rel_err(mix.particles.v, f64.particles.v) <= 1e-3
