@@ -38,7 +38,7 @@ class OrcParticles(C.Structure):
         ("omega", C.POINTER(C.c_double)), ("vd", C.POINTER(C.c_double)), ("omega_d", C.POINTER(C.c_double)),
         ("f", C.POINTER(C.c_double)), ("m", C.POINTER(C.c_double)), ("j", C.POINTER(C.c_double)),
         ("radius", C.POINTER(C.c_double)), ("length", C.POINTER(C.c_double)),
-        ("axes", C.POINTER(C.c_double)), ("squareness", C.POINTER(C.c_double)),
+        ("axes", C.POINTER(C.c_double)), ("squareness", C.POINTER(C.c_double)), ("worm", C.POINTER(C.c_int32)),
     ]
 
 
@@ -108,7 +108,7 @@ def _particles_struct(pa, keep):
     return OrcParticles(
         pa.n, pa.nb_inactive, pa.shape.ctypes.data_as(C.POINTER(C.c_int32)), _dp(pa.pos), _dp(pa.q), _dp(pa.v),
         _dp(pa.omega), _dp(pa.vd), _dp(pa.omega_d), _dp(pa.f), _dp(pa.m), _dp(pa.j), _dp(pa.radius), _dp(pa.length),
-        _dp(pa.axes), _dp(pa.squareness),
+        _dp(pa.axes), _dp(pa.squareness), pa.worm.ctypes.data_as(C.POINTER(C.c_int32)),
     )
 
 

@@ -120,6 +120,8 @@ struct orc_solver {
     std::vector<Q4> q;
     std::vector<double> m, radius, length;
     std::vector<std::array<double, 5>> se_par;  // superellipsoids: semi-axes, e, n
+    std::vector<int32_t> worm;                  // worm index per body, -1 if none
+    bool has_worms = false;
     std::vector<Contact> contacts, old_contacts;
     std::vector<double> lambda;
     orc_stats stats{};
@@ -382,6 +384,24 @@ struct orc_solver {
             return x.i < y.i || (x.i == y.i && x.j < y.j);
         });
         contacts.swap(out);
+    }
+
+    // compute_contacts (solver.hpp:358-367): after the contact method's sorted list, per worm
+    // (objects in order) the contacts of its consecutive spheres with normal and distance
+    // negated (add_contact_from_object<worm>, add_contact.hpp:11-28), which keep the gap of
+    // each link from opening
+    void add_worm_contacts() {
+        if (!has_worms) return;
+        for (int64_t a = nin; a + 1 < n; ++a) {
+            if (worm[a] < 0 || worm[a + 1] != worm[a]) continue;
+            Contact c = sphere_sphere(a, a + 1);
+            for (auto& x : c.nij) x *= -1.;
+            c.dij *= -1.;
+            c.i = a;
+            c.j = a + 1;
+            c.gamma = 0.0;
+            contacts.push_back(c);
+        }
     }
 
     // transfer(old, new), solver.hpp:241-258
@@ -794,6 +814,7 @@ struct orc_solver {
         }
         auto t1 = clk::now();
         detect();
+        add_worm_contacts();
         transfer();
         auto t2 = clk::now();
         // vap, vap_fixed.hpp:45-55 / vap_fpd.hpp:69-81
@@ -978,6 +999,13 @@ struct orc_solver {
         m.assign(in->m, in->m + n);
         radius.assign(in->radius, in->radius + n);
         length.assign(in->length, in->length + n);
+        worm.assign(n, -1);
+        has_worms = false;
+        if (in->worm)
+            for (int64_t i = 0; i < n; ++i) {
+                worm[i] = in->worm[i];
+                if (worm[i] >= 0) has_worms = true;
+            }
         se_par.assign(n, {0, 0, 0, 1, 1});
         if (in->axes && in->squareness)
             for (int64_t i = 0; i < n; ++i)
@@ -1021,6 +1049,10 @@ orc_solver* orc_create(const orc_params* p, const orc_particles* parts) {
     }
     s->dim = p->dim;
     s->load(parts);
+    if (s->has_worms && p->problem != ORC_NOFRICTION) {
+        delete s;
+        return nullptr;
+    }
 #ifdef _OPENMP
     if (p->num_threads > 0) omp_set_num_threads(p->num_threads);
 #endif
@@ -1039,6 +1071,7 @@ int orc_run(orc_solver* s, double dt, int64_t total_it, int64_t initial_iter) {
 int orc_set_particles(orc_solver* s, const orc_particles* in) {
     if (!s || !in) return -1;
     s->load(in);
+    if (s->has_worms && s->p.problem != ORC_NOFRICTION) return -1;
     return 0;
 }
 

@@ -83,6 +83,8 @@ typedef struct {
     double* length;           /* n   (segment length) */
     double* axes;             /* n*3 superellipsoid semi-axes (may be NULL without superellipsoids) */
     double* squareness;       /* n*2 superellipsoid squareness (e, n) */
+    int32_t* worm;            /* n: index of the worm a sphere belongs to, -1 if none (may be NULL);
+                                 worms need the NoFriction problem */
 } orc_particles;
 
 typedef struct {

@@ -45,7 +45,7 @@ class ParticlesC(C.Structure):
         ("omega", C.POINTER(C.c_double)), ("vd", C.POINTER(C.c_double)), ("omega_d", C.POINTER(C.c_double)),
         ("f", C.POINTER(C.c_double)), ("m", C.POINTER(C.c_double)), ("j", C.POINTER(C.c_double)),
         ("radius", C.POINTER(C.c_double)), ("length", C.POINTER(C.c_double)),
-        ("axes", C.POINTER(C.c_double)), ("squareness", C.POINTER(C.c_double)),
+        ("axes", C.POINTER(C.c_double)), ("squareness", C.POINTER(C.c_double)), ("worm", C.POINTER(C.c_int32)),
     ]
 
 

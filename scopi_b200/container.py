@@ -92,10 +92,13 @@ class Particles:
     length: list = field(default_factory=list)
     axes: list = field(default_factory=list)
     squareness: list = field(default_factory=list)
+    worm: list = field(default_factory=list)
     nb_inactive: int = 0
+    n_worms: int = 0
 
     # --- builders --------------------------------------------------------
-    def _push(self, shape, pos, q, prop: Property, radius=0.0, length=0.0, axes=(0.0, 0.0, 0.0), squareness=(1.0, 1.0)):
+    def _push(self, shape, pos, q, prop: Property, radius=0.0, length=0.0, axes=(0.0, 0.0, 0.0), squareness=(1.0, 1.0),
+              worm=-1):
         n = len(self.shape)
         if not prop.active:
             if self.nb_inactive != n:
@@ -115,6 +118,7 @@ class Particles:
         self.length.append(float(length))
         self.axes.append(np.asarray(axes, dtype=np.float64))
         self.squareness.append(np.asarray(squareness, dtype=np.float64))
+        self.worm.append(int(worm))
         return self
 
     def add_sphere(self, pos, radius, prop: Property | None = None, q=None):
@@ -151,6 +155,21 @@ class Particles:
         return self._push(SUPERELLIPSOID, pos, q, prop or Property(), radius=float(np.sqrt(np.dot(r, r))), axes=r,
                           squareness=sq)
 
+    def add_worm(self, positions, radius, prop: Property | None = None, q=None):
+        """``worm<dim>(pos, q, radius, size)`` (objects/types/worm.hpp:118-131) pushed with one
+        property (container.hpp:338-384): one sphere body per position, all of ``radius``,
+        each with the property's values, tagged with the worm's index.  The solver glues
+        consecutive spheres of a worm (add_contact.hpp:11-28)."""
+        prop = prop or Property()
+        if not prop.active:
+            raise ValueError("worms are active objects")
+        w = self.n_worms
+        self.n_worms += 1
+        qs = [quaternion(0.0)] * len(positions) if q is None else list(q)
+        for pos, qq in zip(positions, qs):
+            self._push(SPHERE, pos, qq, prop, radius=radius, worm=w)
+        return self
+
     # --- array views -----------------------------------------------------
     def finalize(self) -> "ParticleArrays":
         return ParticleArrays.from_lists(self)
@@ -176,6 +195,7 @@ class ParticleArrays:
     length: np.ndarray
     axes: np.ndarray = None        # n x 3 superellipsoid semi-axes (0 for other shapes)
     squareness: np.ndarray = None  # n x 2 superellipsoid squareness (e, n)
+    worm: np.ndarray = None        # n int32: index of the worm a sphere belongs to, -1 if none
 
     def __post_init__(self):
         n = int(self.shape.shape[0])
@@ -185,6 +205,9 @@ class ParticleArrays:
             self.squareness = np.ones((n, 2))
         self.axes = np.ascontiguousarray(self.axes, dtype=np.float64).reshape(n, 3)
         self.squareness = np.ascontiguousarray(self.squareness, dtype=np.float64).reshape(n, 2)
+        if self.worm is None:
+            self.worm = np.full(n, -1, np.int32)
+        self.worm = np.ascontiguousarray(self.worm, dtype=np.int32).reshape(n)
 
     @property
     def n(self) -> int:
@@ -207,6 +230,7 @@ class ParticleArrays:
             length=np.ascontiguousarray(np.asarray(p.length, dtype=np.float64)),
             axes=a2(p.axes, 3) if p.axes else None,
             squareness=a2(p.squareness, 2) if p.squareness else None,
+            worm=np.ascontiguousarray(np.asarray(p.worm, dtype=np.int32)) if p.worm else None,
         )
 
     def copy(self) -> "ParticleArrays":

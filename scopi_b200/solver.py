@@ -97,7 +97,8 @@ class ScopiSolver:
         self._keep = pa
         return _abi.ParticlesC(pa.n, pa.nb_inactive, pa.shape.ctypes.data_as(C.POINTER(C.c_int32)), _dp(pa.pos),
                                _dp(pa.q), _dp(pa.v), _dp(pa.omega), _dp(pa.vd), _dp(pa.omega_d), _dp(pa.f), _dp(pa.m),
-                               _dp(pa.j), _dp(pa.radius), _dp(pa.length), _dp(pa.axes), _dp(pa.squareness))
+                               _dp(pa.j), _dp(pa.radius), _dp(pa.length), _dp(pa.axes), _dp(pa.squareness),
+                               pa.worm.ctypes.data_as(C.POINTER(C.c_int32)))
 
     def _upload(self):
         s = self._struct(self.particles)

@@ -3,7 +3,8 @@
 Reads the reference's own golden snapshots (test/references/*.json of
 hpc-maths/scopi, written by ScopiSolver::write_output_files) and keeps only what
 the parity tests compare: per object position, quaternion, velocity and omega
-(the fields test/utils.cpp:14-75 diffs), plus the contact list of the last
+(the fields test/utils.cpp:14-75 diffs; for a worm the position and quaternion of
+each of its spheres), plus the contact list of the last
 step (i, j, distance, normal, pi, pj).  Writes tests/golden/reference_states.json, and
 one snapshot file unchanged (snapshot_obstacles_sphere_sphere_moving.json) for the
 restart tests.
@@ -25,6 +26,7 @@ FILES = [
     "two_spheres_symmetrical",      # test/test_sphere.cpp:382-421
     "2d_case_spheres",              # test/test_sphere.cpp:423-484
     "obstacles_sphere_sphere_moving",  # test/test_obstacles.cpp:214-250
+    "two_worms",                    # test/test_worm.cpp:480-530
     # superellipsoids (2D); these snapshots use an older output format (no velocities,
     # contacts without i, j and distance), written before the motion of their step
     "two_ellipsoids_symmetrical",           # test/test_superellipsoid.cpp:451-491
@@ -49,6 +51,16 @@ def main():
                 continue
             p = o["properties"]
             om = p["omega"]
+            if o["type"] == "worm":  # one object, one sphere per body; properties of its first body
+                objs.append({
+                    "type": "worm",
+                    "active": p["active"],
+                    "spheres": [{"id": w["id"], "position": w["position"], "quaternion": w["quaternion"],
+                                 "radius": w["radius"]} for w in o["worm"]],
+                    "velocity": p["velocity"],
+                    "omega": om if isinstance(om, list) else [om],
+                })
+                continue
             objs.append({
                 "type": o["type"],
                 "active": p["active"],

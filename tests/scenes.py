@@ -406,3 +406,15 @@ def viscous_friction_3d(mu=0.3, gamma_min=-0.03):
     kw = dict(problem=VISCOUS_FRICTION, vap=VAP_FPD, tolerance=1e-7, max_ite=10000, alpha=0.1, mu=mu, dmax=0.1,
               fixed_point_tol=1e-3, fixed_point_max_iter=1000, gamma=0.0, gamma_min=gamma_min, gamma_tol=1e-6)
     return p.finalize(), kw, 0.01, 40
+
+
+def two_worms(contact_method=KDTREE):
+    """test/test_worm.cpp:480-530: two 2D worms of six unit spheres (mass 1, moment of inertia
+    0.1) driven into each other by vap_fixed at desired velocities (-1, 0) and (1, 0),
+    NoFriction, dmax 1, default solver parameters, dt 0.005, 1000 steps."""
+    p = Particles(2)
+    prop = dict(mass=1.0, moment_inertia=0.1)
+    p.add_worm([(1.0 + 2 * k, 0.7) for k in range(6)], 1.0, Property(desired_velocity=(-1.0, 0.0), **prop))
+    p.add_worm([(-1.0 - 2 * k, -0.7) for k in range(6)], 1.0, Property(desired_velocity=(1.0, 0.0), **prop))
+    kw = dict(problem=NOFRICTION, vap=VAP_FIXED, contact_method=contact_method, dmax=1.0)
+    return p.finalize(), kw, 0.005, 1000

@@ -247,3 +247,49 @@ def test_sphere_plane_viscous_friction_analytic():
     e_pos, e_q, e_v, e_om = viscous_friction_errors(s.pa, dt, total, 100)
     assert e_pos <= 1e-1 and e_q <= 1e-1, (e_pos, e_q)
     assert e_v <= 1e-3 * (1 + APPROX) and e_om <= 1e-3 * (1 + APPROX), (e_v, e_om)
+
+
+def compare_worms(state, gold_objs, dim, tol):
+    """The fields of a worm that test/utils.cpp:14-75 diffs: each sphere's position and
+    quaternion, and the velocity and omega of the worm's first sphere."""
+    worst, b = 0.0, 0
+    for o in gold_objs:
+        assert o["type"] == "worm"
+        first = b
+        for sph in o["spheres"]:
+            assert sph["id"] == b
+            for d in range(dim):
+                worst = max(worst, abs(state.pos[b, d] - sph["position"][d]))
+            for d in range(4):
+                worst = max(worst, abs(state.q[b, d] - sph["quaternion"][d]))
+            b += 1
+        for d in range(dim):
+            worst = max(worst, abs(state.v[first, d] - o["velocity"][d]))
+        worst = max(worst, abs(state.omega[first, 2] - o["omega"][0]))
+    assert b == state.n, (b, state.n)
+    assert worst <= tol, f"max abs deviation {worst:.3e} > {tol}"
+    return worst
+
+
+@pytest.mark.parametrize("method", [S.KDTREE, S.BRUTE_FORCE])
+def test_two_worms_golden(golden, method):
+    """test/test_worm.cpp:480-530 against test/references/two_worms.json (tol 1e-6), and its
+    final contact list: the contact method's sorted pairs, then one glued link per pair of
+    consecutive spheres with normal and distance negated."""
+    s = run_oracle(S.two_worms(method))
+    compare_worms(s.pa, golden["two_worms"]["objects"], 2, 1e-6)
+    c = s.contacts()
+    gold = golden["two_worms"]["contacts"]
+    assert list(zip(c["i"].tolist(), c["j"].tolist())) == [(g["i"], g["j"]) for g in gold]
+    for k, g in enumerate(gold):
+        assert abs(c["dij"][k] - g["distance"]) < 1e-6
+        for d in range(2):
+            assert abs(c["nij"][k, d] - g["normal"][d]) < 1e-6
+
+
+def test_worms_need_nofriction():
+    """Worm links carry the reference's default-constructed contact property; only the
+    NoFriction problem, where the property is empty, is accepted."""
+    pa, kw, _, _ = S.two_worms()
+    with pytest.raises(RuntimeError):
+        orc.OracleSolver(pa, **dict(kw, problem=S.FRICTION))
