@@ -124,6 +124,11 @@ typedef struct scopi_gpu_particles {
                             NULL when there are none */
     double* squareness;  /* n*2 superellipsoid squareness (e, n); 2D: (e, unused); NULL when
                             there are none */
+    int32_t* worm;       /* n: index of the worm<dim> (objects/types/worm.hpp) an active sphere
+                            belongs to, -1 if none; NULL when there are none.  A worm is a run of
+                            consecutive bodies with the same index; each step appends, after the
+                            sorted contacts, the contacts of its consecutive spheres with normal
+                            and distance negated (add_contact.hpp:11-28).  NoFriction only. */
 } scopi_gpu_particles;
 
 typedef struct scopi_gpu_stats {

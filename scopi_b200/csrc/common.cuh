@@ -47,7 +47,8 @@ struct Sizes {
     int n_extra;        // Viscous: second multipliers
     int overflow;       // capacity exceeded somewhere (host grows and redoes the step)
     int ncell;          // cells of the uniform grid
-    int pad[3];
+    int n_links;        // worm links: the last n_links contacts (normal and distance negated)
+    int pad[2];
 };
 
 struct Grid {

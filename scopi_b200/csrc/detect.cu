@@ -601,10 +601,12 @@ __global__ void k_set_cobs(const int* totals, Sizes* sizes) {
 }
 
 // closest points of the listed pairs; viscous gamma carried over from the previous list
-// by (i, j) (transfer, include/scopi/solver.hpp:241-258).
+// by (i, j) (transfer, include/scopi/solver.hpp:241-258); the last n_links rows are worm
+// links, whose normal and distance are negated (add_contact.hpp:17-18).
 template <int DIM>
 __global__ void k_geometry(Bodies B, StepParams p, Contacts c, const Sizes* sizes, Contacts old_c, const int* old_C) {
     const int C = sizes->C;
+    const int first_link = C - sizes->n_links;
     const int oC = old_C ? *old_C : 0;
     GRID_STRIDE(k, C) {
         const int a = c.ci[k], b = c.cj[k];
@@ -612,6 +614,10 @@ __global__ void k_geometry(Bodies B, StepParams p, Contacts c, const Sizes* size
         if (!exact_pair(B, DIM, a, b, g)) {
             g.dij = 0.0;
             for (int d = 0; d < 3; ++d) g.nij[d] = g.pi[d] = g.pj[d] = 0.0;
+        }
+        if (k >= first_link) {
+            g.dij *= -1.;
+            for (int d = 0; d < 3; ++d) g.nij[d] *= -1.;
         }
         c.dij[k] = g.dij;
         for (int d = 0; d < 3; ++d) {
@@ -793,6 +799,17 @@ __global__ void k_gamma_update(StepParams p, Contacts c, Assembly a, const doubl
 
 // update_contact_properties_impl<ViscousFriction>, OptimGradient.hpp:36-52: the same update
 // with the force of the contact's four slots (mode in vflag: l n, (l+ - l-) n or -l0 n + f)
+__global__ void k_append_links(int C, int W, const int* links, Contacts c, Sizes* sizes) {
+    GRID_STRIDE(k, W) {
+        c.ci[C + k] = links[k];
+        c.cj[C + k] = links[k] + 1;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        sizes->C = C + W;
+        sizes->n_links = W;
+    }
+}
+
 __global__ void k_gamma_update_vf(StepParams p, Contacts c, Assembly a, const double* lam, const Sizes* sizes) {
     const int C = sizes->C;
     GRID_STRIDE(k, C) {
@@ -1030,6 +1047,11 @@ void launch_incidence(const Bodies& b, const StepParams& p, const Contacts& c, c
         k_inc_coef<<<blocks_for(2 * c_cap), kThreads, 0, s>>>(na, inc.ptr, inc.idx, a, inc.coef);
         LAUNCHED(1);
     }
+}
+
+void launch_append_links(int C, int W, const int* links, Contacts& c, Sizes* sizes, cudaStream_t s) {
+    k_append_links<<<blocks_for(W), kThreads, 0, s>>>(C, W, links, c, sizes);
+    LAUNCHED(1);
 }
 
 void launch_gamma_update(const StepParams& p, Contacts& c, const Assembly& a, const double* lambda, const Sizes* sizes,

@@ -84,6 +84,10 @@ void launch_assemble(const Bodies& b, const StepParams& p, const Contacts& c, As
 void launch_incidence(const Bodies& b, const StepParams& p, const Contacts& c, const Assembly& a, Incidence& inc,
                       const Sizes* sizes, long long c_cap, int* scan_work, int* tmp_total, cudaStream_t s,
                       bool with_coef);
+// Worm links (compute_contacts, solver.hpp:358-367): contacts (links[k], links[k] + 1) appended
+// at C..C+W-1 after the sorted list (C on the host, the list's count), sizes->C = C + W and
+// sizes->n_links = W; k_geometry negates their normal and distance.
+void launch_append_links(int C, int W, const int* links, Contacts& c, Sizes* sizes, cudaStream_t s);
 void launch_gamma_update(const StepParams& p, Contacts& c, const Assembly& a, const double* lambda, const Sizes* sizes,
                          long long c_cap, cudaStream_t s);
 // v += dt*u_v, omega += dt*u_w, then pos/q integration (u = M^-1 B^T lambda, may be null).

@@ -57,6 +57,8 @@ struct scopi_gpu_handle {
     double *d_pos = nullptr, *d_q = nullptr, *d_v = nullptr, *d_omega = nullptr, *d_vd = nullptr, *d_omega_d = nullptr,
            *d_f = nullptr, *d_m = nullptr, *d_j = nullptr, *d_radius = nullptr, *d_length = nullptr;
     double *d_axes = nullptr, *d_sq = nullptr;  // superellipsoids
+    int* d_links = nullptr;  // worm links: first body of each (n entries at most)
+    int n_links = 0;
     int *d_se_keep = nullptr, *d_se_pos = nullptr;  // contact filter of superellipsoid candidates
     double* d_se_u = nullptr;                       // start of each superellipsoid solve
     bool has_se = false;                        // some active body is a superellipsoid
@@ -486,6 +488,7 @@ struct scopi_gpu_handle {
         A(d_shape, n) A(d_pos, 3 * (size_t)n) A(d_q, 4 * (size_t)n) A(d_v, 3 * (size_t)n) A(d_omega, 3 * (size_t)n)
         A(d_vd, 3 * (size_t)n) A(d_omega_d, 3 * (size_t)n) A(d_f, 3 * (size_t)n) A(d_m, n) A(d_j, 3 * (size_t)n)
         A(d_radius, n) A(d_length, n) A(d_axes, 3 * (size_t)n) A(d_sq, 2 * (size_t)n) A(d_invm64, 4 * (size_t)na + 4) A(d_invm32, 4 * (size_t)na + 4)
+        A(d_links, n)
         A(d_imt64, (size_t)na + 1) A(d_imt32, (size_t)na + 1)
         A(d_ufin, 6 * (size_t)na + 6)
         A(d_usfin, (size_t)na + 1)
@@ -570,9 +573,10 @@ struct scopi_gpu_handle {
             cudaMemcpyAsync(h_sizes, d_sizes_cur, sizeof(Sizes), cudaMemcpyDeviceToHost, stream);
             cudaError_t e = cudaStreamSynchronize(stream);
             if (e != cudaSuccess) return cuda_fail(e, "detect");
-            if (!h_sizes->overflow) break;
+            const int links = assemble ? n_links : 0;
+            if (!h_sizes->overflow && (long long)h_sizes->C + links <= c_cap) break;
             // grow: keep the previous contacts (viscous gamma transfer) across the reallocation
-            const long long need = (long long)std::ceil(1.3 * ((double)h_sizes->C + 1.0)) + 1024;
+            const long long need = (long long)std::ceil(1.3 * ((double)h_sizes->C + links + 1.0)) + 1024;
             long long total = 0;
             {
                 // the true count is C_obs + active rows; recompute it from the scan totals
@@ -585,6 +589,9 @@ struct scopi_gpu_handle {
             if (rc) return rc;
             if (attempt == 3) return fail(SCOPI_GPU_ENOMEM, "contact capacity could not be grown");
         }
+        // the step's list is the contact method's plus the worm links (compute_contacts,
+        // solver.hpp:358-367); detection alone (assemble == false) is the contact method's
+        if (assemble && n_links > 0) launch_append_links(h_sizes->C, n_links, d_links, cur, d_sizes_cur, stream);
         launch_geometry(b, sp, cur, d_sizes_cur, c_cap, has_old ? &old : nullptr, has_old ? &d_sizes_old->C : nullptr,
                         c_cap, stream);
         if (has_se) {
@@ -1218,6 +1225,18 @@ static int32_t upload_particles(scopi_gpu_handle* h, const scopi_gpu_particles* 
                 return h->fail(SCOPI_GPU_EINVAL, "superellipsoid: semi-axes > 0 and squareness in (0, 2)");
         }
     }
+    // worms: a link per pair of consecutive active spheres with the same worm index
+    std::vector<int> links;
+    if (p->worm) {
+        for (int i = 0; i < n; ++i) {
+            if (p->worm[i] < 0) continue;
+            if (i < nin || p->shape[i] != SCOPI_GPU_SPHERE)
+                return h->fail(SCOPI_GPU_EINVAL, "worms are runs of active spheres");
+            if (i + 1 < n && p->worm[i + 1] == p->worm[i]) links.push_back(i);
+        }
+        if (!links.empty() && (h->batch || h->P.problem != SCOPI_GPU_NOFRICTION))
+            return h->fail(SCOPI_GPU_EUNSUPPORTED, "worms: single scenes with the NoFriction problem");
+    }
     h->has_se = n_se > 0;
     cudaSetDevice(h->dev);
     cudaStreamSynchronize(h->stream);
@@ -1233,6 +1252,8 @@ static int32_t upload_particles(scopi_gpu_handle* h, const scopi_gpu_particles* 
     }
     cudaStream_t s = h->stream;
     auto up = [&](void* dst, const void* src, size_t bytes) { cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s); };
+    h->n_links = (int)links.size();
+    if (!links.empty()) cudaMemcpy(h->d_links, links.data(), links.size() * sizeof(int), cudaMemcpyHostToDevice);
     up(h->d_shape, p->shape, n * sizeof(int));
     up(h->d_pos, p->pos, 3 * (size_t)n * sizeof(double));
     up(h->d_q, p->q, 4 * (size_t)n * sizeof(double));
@@ -1429,6 +1450,12 @@ int32_t scopi_gpu_batch_create(const scopi_gpu_params* p, int32_t n_scenes, cons
             scopi_gpu::set_global_error("scopi_gpu_batch_create: invalid scene container");
             return SCOPI_GPU_EINVAL;
         }
+        if (sc.worm)
+            for (long long i = 0; i < sc.n; ++i)
+                if (sc.worm[i] >= 0) {
+                    scopi_gpu::set_global_error("scopi_gpu_batch_create: worms: single scenes only");
+                    return SCOPI_GPU_EUNSUPPORTED;
+                }
         ntot += sc.n;
         nin_tot += sc.nb_inactive;
     }

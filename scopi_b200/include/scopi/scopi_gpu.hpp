@@ -226,6 +226,31 @@ class superellipsoid : public object_base<dim> {
     }
 };
 
+// worm<dim>(pos, q, radius, size), objects/types/worm.hpp:118-131: a chain of `size` spheres
+// of one radius; each sphere is a body of its own and the solver keeps consecutive spheres
+// in contact (add_contact.hpp:11-28)
+template <std::size_t dim, bool owner = true>
+class worm {
+  public:
+    worm(std::vector<type::position_t<dim>> pos, std::vector<type::quaternion_t> q, double radius, std::size_t size)
+        : m_pos(std::move(pos)), m_q(std::move(q)), m_radius(radius), m_size(size) {
+        if (m_pos.size() != m_size || m_q.size() != m_size)
+            throw std::runtime_error("worm: one position and one quaternion per sphere");
+    }
+    worm(std::vector<type::position_t<dim>> pos, double radius, std::size_t size)
+        : worm(pos, std::vector<type::quaternion_t>(pos.size(), quaternion(0.0)), radius, size) {}
+    const type::position_t<dim>& pos(std::size_t i) const { return m_pos[i]; }
+    const type::quaternion_t& q(std::size_t i) const { return m_q[i]; }
+    double radius() const { return m_radius; }
+    std::size_t size() const { return m_size; }
+
+  private:
+    std::vector<type::position_t<dim>> m_pos;
+    std::vector<type::quaternion_t> m_q;
+    double m_radius;
+    std::size_t m_size;
+};
+
 // ------------------------------------------------------------------ property
 template <std::size_t dim>
 class property {
@@ -561,11 +586,34 @@ class scopi_container {
 
     template <class Obj>
     void push_back(const Obj& s, const property<dim>& p = property<dim>()) {
+        push_body(s, p, -1);
+        m_objects.push_back({size() - 1, 1, false});
+    }
+    // a worm's spheres, one body each with the worm's property (container.hpp:338-384)
+    void push_back(const worm<dim>& w, const property<dim>& p = property<dim>()) {
+        if (!p.is_active()) throw std::runtime_error("worms are active objects");
+        const std::size_t first = size();
+        for (std::size_t i = 0; i < w.size(); ++i) {
+            sphere<dim> s({w.pos(i)}, w.q(i), w.radius());
+            push_body(s, p, (int32_t)m_n_worms);
+        }
+        ++m_n_worms;
+        m_objects.push_back({first, w.size(), true});
+    }
+
+    // bodies (the reference's size() counts objects: the two differ only with worms)
+    std::size_t size() const { return m_shape.size(); }
+    std::size_t nb_objects() const { return m_objects.size(); }
+
+  private:
+    template <class Obj>
+    void push_body(const Obj& s, const property<dim>& p, int32_t worm_index) {
         if (!p.is_active()) {
             if (m_nb_inactive != size())
                 throw std::runtime_error("All the obstacles must be pushed before the active particles.");
             ++m_nb_inactive;
         }
+        m_worm.push_back(worm_index);
         m_shape.push_back(s.shape);
         append3(m_pos, s.position);
         for (double c : s.q) m_q.push_back(c);
@@ -582,7 +630,7 @@ class scopi_container {
         for (double c : s.sq_) m_sq.push_back(c);
     }
 
-    std::size_t size() const { return m_shape.size(); }
+  public:
     std::size_t nb_inactive() const { return m_nb_inactive; }
     std::size_t nb_active() const { return size() - m_nb_inactive; }
 
@@ -635,6 +683,7 @@ class scopi_container {
         p.length = m_length.data();
         p.axes = m_axes.data();
         p.squareness = m_sq.data();
+        p.worm = m_n_worms > 0 ? m_worm.data() : nullptr;
         return p;
     }
 
@@ -643,15 +692,31 @@ class scopi_container {
     io::Value snapshot_objects() const {
         using io::Value;
         Value out = Value::array();
-        for (std::size_t i = 0; i < size(); ++i) {
+        for (const auto& ob : m_objects) {
+            const std::size_t i = ob.first;
             const double* x = &m_pos[3 * i];
             type::quaternion_t q = {m_q[4 * i], m_q[4 * i + 1], m_q[4 * i + 2], m_q[4 * i + 3]};
             const auto R = io::rotation<dim>(q);
             Value o = Value::object();
-            o.set("id", Value::integer((int64_t)i));
-            o.set("quaternion", Value::numbers(q.data(), 4));
             double col0[dim];
             for (std::size_t d = 0; d < dim; ++d) col0[d] = R[d * dim];
+            if (ob.worm) {
+                // write_objects(worm), write_objects.hpp:183-198: one entry per sphere
+                o.set("type", Value::string("worm"));
+                Value spheres = Value::array();
+                for (std::size_t k = 0; k < ob.count; ++k) {
+                    const std::size_t b = i + k;
+                    Value e = Value::object();
+                    e.set("id", Value::integer((int64_t)b));
+                    e.set("position", Value::numbers(&m_pos[3 * b], dim));
+                    e.set("quaternion", Value::numbers(&m_q[4 * b], 4));
+                    e.set("radius", Value::number(m_radius[b]));
+                    spheres.items.push_back(std::move(e));
+                }
+                o.set("worm", std::move(spheres));
+            } else {
+            o.set("id", Value::integer((int64_t)i));
+            o.set("quaternion", Value::numbers(q.data(), 4));
             switch (m_shape[i]) {
                 case SCOPI_GPU_PLANE:
                     o.set("type", Value::string("plane"));
@@ -686,6 +751,7 @@ class scopi_container {
                     o.set("rotation", Value::numbers(R.data(), dim * dim));
                     break;
             }
+            }
             auto rot = [&](const std::vector<double>& a) {
                 return dim == 2 ? Value::number(a[3 * i + 2]) : Value::numbers(&a[3 * i], 3);
             };
@@ -719,15 +785,20 @@ class scopi_container {
             for (std::size_t d = 0; d < 3; ++d) dst.push_back(r[d]);
         }
     }
-    std::vector<int32_t> m_shape;
+    struct object_range {
+        std::size_t first, count;
+        bool worm;
+    };
+    std::vector<int32_t> m_shape, m_worm;
     std::vector<double> m_pos, m_q, m_v, m_w, m_vd, m_dw, m_f, m_m, m_j, m_radius, m_length, m_axes, m_sq;
-    std::size_t m_nb_inactive = 0;
+    std::vector<object_range> m_objects;  // the objects as pushed: first body, bodies, worm or not
+    std::size_t m_nb_inactive = 0, m_n_worms = 0;
 };
 
 // ------------------------------------------------------------------ restart
 // from_json<dim> (restart.hpp:20-67, properties as json.hpp:26-44 reads them): a container
 // rebuilt from the "objects" of a snapshot document (spheres, superellipsoids, segments,
-// planes), obstacles first as the snapshot lists them.
+// planes, worms), obstacles first as the snapshot lists them.
 template <std::size_t dim>
 scopi_container<dim> from_json(const io::Value& j) {
     using io::as_array;
@@ -771,6 +842,16 @@ scopi_container<dim> from_json(const io::Value& j) {
         } else if (type == "plane") {
             container.push_back(
                 plane<dim>({as_array<dim>(field(o, "position"))}, {as_array<4>(field(o, "quaternion"))}), p);
+        } else if (type == "worm") {  // restart.hpp:53-64
+            std::vector<type::position_t<dim>> pos;
+            std::vector<type::quaternion_t> q;
+            const auto& spheres = field(o, "worm").items;
+            for (const auto& e : spheres) {
+                pos.push_back(as_array<dim>(field(e, "position")));
+                q.push_back(as_array<4>(field(e, "quaternion")));
+            }
+            if (spheres.empty()) throw std::runtime_error("from_json: empty worm");
+            container.push_back(worm<dim>(pos, q, as_number(field(spheres[0], "radius")), pos.size()), p);
         } else {
             throw std::runtime_error("from_json: object type \"" + type + "\" is not supported");
         }

@@ -62,5 +62,6 @@ int main(int argc, char** argv) {
     round_trip<2>(dir + "/snap2d.json", dir + "/snap2d_rt.json");
     round_trip<3>(dir + "/snap3d.json", dir + "/snap3d_rt.json");
     if (argc > 2) round_trip<2>(argv[2], dir + "/snapfile_rt.json");
+    if (argc > 3) round_trip<2>(argv[3], dir + "/wormfile_rt.json");
     return 0;
 }

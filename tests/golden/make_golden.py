@@ -6,8 +6,8 @@ the parity tests compare: per object position, quaternion, velocity and omega
 (the fields test/utils.cpp:14-75 diffs; for a worm the position and quaternion of
 each of its spheres), plus the contact list of the last
 step (i, j, distance, normal, pi, pj).  Writes tests/golden/reference_states.json, and
-one snapshot file unchanged (snapshot_obstacles_sphere_sphere_moving.json) for the
-restart tests.
+two snapshot files unchanged (snapshot_obstacles_sphere_sphere_moving.json,
+snapshot_two_worms.json) for the restart tests.
 
 Run once in a checkout that has the reference at REF (default /root/reference):
     python tests/golden/make_golden.py [REF]
@@ -80,13 +80,14 @@ def main():
     with open(dst, "w") as fh:
         json.dump(out, fh, indent=1)
     print("wrote", dst)
-    # one snapshot kept whole, as the reference wrote it: the input of the restart tests
+    # two snapshots kept whole, as the reference wrote them: the inputs of the restart tests
     # (from_json, restart.hpp:20-67)
-    src = os.path.join(ref, "test", "references", "obstacles_sphere_sphere_moving.json")
-    dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "snapshot_obstacles_sphere_sphere_moving.json")
-    with open(src) as fh, open(dst, "w") as out_fh:
-        out_fh.write(fh.read())
-    print("wrote", dst)
+    for name in ("obstacles_sphere_sphere_moving", "two_worms"):
+        src = os.path.join(ref, "test", "references", name + ".json")
+        dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "snapshot_" + name + ".json")
+        with open(src) as fh, open(dst, "w") as out_fh:
+            out_fh.write(fh.read())
+        print("wrote", dst)
 
 
 if __name__ == "__main__":

@@ -47,13 +47,14 @@ def test_cpp_api_matches_reference_golden(exe, golden, mode, name, tmp_path):
     assert worst <= 1e-5, worst
 
 
+WORM_SRC = os.path.join(ROOT, "tests", "cpp", "two_worms_dropin.cpp")
 SE_SRC = os.path.join(ROOT, "tests", "cpp", "superellipsoids_dropin.cpp")
 SE2_SRC = os.path.join(ROOT, "tests", "cpp", "two_ellipsoids_dropin.cpp")
 FP_SRC = os.path.join(ROOT, "tests", "cpp", "fixed_point_dropin.cpp")
 RS_SRC = os.path.join(ROOT, "tests", "cpp", "restart_dropin.cpp")
 
 
-@pytest.mark.parametrize("src", [SE_SRC, SE2_SRC, FP_SRC, RS_SRC])
+@pytest.mark.parametrize("src", [SE_SRC, SE2_SRC, FP_SRC, RS_SRC, WORM_SRC])
 def test_superellipsoid_header_compiles(src):
     subprocess.run([GXX, "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", *INC, src], check=True)
 
@@ -165,6 +166,7 @@ def test_cpp_friction_fixed_point_matches_analytic(fp_exe, tmp_path):
 # ------------------------------------------------------------------ snapshot files
 SNAP_SRC = os.path.join(ROOT, "tests", "cpp", "snapshot_writer.cpp")
 SNAPSHOT_FIXTURE = os.path.join(ROOT, "tests", "golden", "snapshot_obstacles_sphere_sphere_moving.json")
+WORM_FIXTURE = os.path.join(ROOT, "tests", "golden", "snapshot_two_worms.json")
 # keys of write_objects.hpp per shape and of the properties written by solver.hpp:383-400
 OBJECT_KEYS = {
     "sphere": {"id", "position", "properties", "quaternion", "radius", "rotation", "type"},
@@ -269,11 +271,12 @@ def test_cpp_snapshot_files_match_reference_golden(exe, golden, mode, name, tmp_
 def test_restart_reads_snapshots(tmp_path):
     """from_json (restart.hpp:20-67): the writer's own files read back and written again give
     the same document (numbers to 1e-12: a segment is rebuilt from its extrema, which moves
-    them by an ulp, as in the reference), and a snapshot the reference wrote (test/references/
-    obstacles_sphere_sphere_moving.json) gives back every object and property it holds."""
+    them by an ulp, as in the reference), and two snapshots the reference wrote (test/references/
+    obstacles_sphere_sphere_moving.json, two_worms.json) give back every object and property
+    they hold."""
     exe = str(tmp_path / "snapw")
     subprocess.run([GXX, "-std=c++17", "-Wall", "-Werror", *INC, SNAP_SRC, "-o", exe], check=True)
-    subprocess.run([exe, str(tmp_path), SNAPSHOT_FIXTURE], check=True)
+    subprocess.run([exe, str(tmp_path), SNAPSHOT_FIXTURE, WORM_FIXTURE], check=True)
     def close(a, b):
         if isinstance(a, dict):
             return isinstance(b, dict) and a.keys() == b.keys() and all(close(a[k], b[k]) for k in a)
@@ -291,6 +294,13 @@ def test_restart_reads_snapshots(tmp_path):
     for g, r in zip(got, ref):
         for key in ("type", "id", "position", "quaternion", "radius", "rotation", "properties"):
             assert g[key] == r[key], (key, g[key], r[key])
+    # worms (restart.hpp:53-64, write_objects.hpp:183-198): two objects of six spheres each
+    ref = json.load(open(WORM_FIXTURE))["objects"]
+    got = json.load(open(tmp_path / "wormfile_rt.json"))["objects"]
+    assert len(got) == len(ref) == 2
+    for g, r in zip(got, ref):
+        assert g.keys() == r.keys() and g["type"] == "worm"
+        assert g["worm"] == r["worm"] and g["properties"] == r["properties"]
 
 
 @pytest.mark.gpu
@@ -309,3 +319,43 @@ def test_cpp_restart_continues_like_one_run(tmp_path):
                                     text=True, cwd=tmp_path).stdout)
     assert os.path.exists(tmp_path / "snap" / "restart_0030.json")
     assert one == two
+
+
+def diff_file(result, ref, tol):
+    """test/utils.cpp:14-75 (diffFile): the "objects" of the two documents may differ only in
+    floating-point entries, each by at most tol."""
+    def walk(a, b, path):
+        if isinstance(b, float) and isinstance(a, float):
+            assert abs(a - b) <= tol, (path, a, b)
+        elif isinstance(b, dict):
+            assert isinstance(a, dict) and a.keys() == b.keys(), path
+            for k in b:
+                walk(a[k], b[k], path + "/" + k)
+        elif isinstance(b, list):
+            assert isinstance(a, list) and len(a) == len(b), path
+            for k, (x, y) in enumerate(zip(a, b)):
+                walk(x, y, f"{path}/{k}")
+        else:
+            assert a == b and type(a) is type(b), (path, a, b)
+    walk(result["objects"], ref["objects"], "")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("method", ["kdtree", "brute_force"])
+def test_cpp_two_worms_match_reference_golden(method, tmp_path):
+    """The reference's "two worms" test (test/test_worm.cpp:480-530, both contact methods)
+    through the C++ drop-in: its final snapshot file passes the reference's own golden-file
+    check against test/references/two_worms.json (tolerance 1e-6), and its contact list is the
+    reference's (pairs, and the glued links after the sorted list)."""
+    exe = str(tmp_path / "worms")
+    lib = os.path.join(ROOT, "scopi_b200")
+    subprocess.run([GXX, "-O2", "-std=c++17", *INC, WORM_SRC, "-L", lib, "-lscopi_gpu", f"-Wl,-rpath,{lib}", "-o", exe],
+                   check=True)
+    subprocess.run([exe, method, str(tmp_path / "out")], check=True, capture_output=True, cwd=tmp_path)
+    got = json.load(open(tmp_path / "out" / "two_worms_1000.json"))
+    ref = json.load(open(WORM_FIXTURE))
+    diff_file(got, ref, 1e-6)
+    assert [(c["i"], c["j"]) for c in got["contacts"]] == [(c["i"], c["j"]) for c in ref["contacts"]]
+    for g, r in zip(got["contacts"], ref["contacts"]):
+        assert abs(g["distance"] - r["distance"]) <= 1e-6
+        assert max(abs(a - b) for a, b in zip(g["normal"], r["normal"])) <= 1e-6

@@ -357,3 +357,30 @@ def test_viscous_friction_3d_mixed_precision():
     mix = gpu_solver(pa, precision=1, mixed_violation_tol=1e-6, **kw).run(dt, total)
     assert rel_err(mix.particles.pos, f64.particles.pos) <= 1e-6
     assert rel_err(mix.particles.v, f64.particles.v) <= 1e-3
+
+
+@pytest.mark.parametrize("method", [S.KDTREE, S.BRUTE_FORCE])
+def test_two_worms_on_gpu(golden, method):
+    """test/test_worm.cpp:480-530 on the GPU: two_worms.json within its 1e-6, the final contact
+    list (sorted pairs, then the glued links with normal and distance negated) equal to the
+    reference's, and the trajectory of the oracle, which appends the same links."""
+    from test_oracle_golden import compare_worms
+    pa, kw, dt, total = S.two_worms(method)
+    g = gpu_solver(pa, **kw).run(dt, total)
+    compare_worms(g.particles, golden["two_worms"]["objects"], 2, 1e-6)
+    c = g.current_contacts()
+    gold = golden["two_worms"]["contacts"]
+    assert list(zip(c["i"].tolist(), c["j"].tolist())) == [(x["i"], x["j"]) for x in gold]
+    for k, x in enumerate(gold):
+        assert abs(c["dij"][k] - x["distance"]) < 1e-6
+        assert max(abs(c["nij"][k, d] - x["normal"][d]) for d in range(2)) < 1e-6
+    o = oracle_solver(pa, **kw).run(dt, total)
+    assert rel_err(g.particles.pos, o.pa.pos) <= 1e-9
+    assert rel_err(g.particles.v, o.pa.v) <= 1e-6
+
+
+def test_worms_need_nofriction_on_gpu():
+    from scopi_b200 import ScopiGPUError
+    pa, kw, dt, _ = S.two_worms()
+    with pytest.raises(ScopiGPUError):
+        gpu_solver(pa, **dict(kw, problem=S.FRICTION)).run(dt, 1)
