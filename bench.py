@@ -11,8 +11,9 @@ timed on the same steps from the same state and reported beside it.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-N>1 runs under torchrun, one independent replica per GPU (the solve has no data-path
-exchange), timed on the device and reduced as the max over ranks.
+N>1 runs under torchrun, one independent replica per GPU (every APGD iteration needs
+global reductions over the scene, so the solve has no data-path exchange to shard), timed
+on the device and reduced as the max over ranks.
 """
 from __future__ import annotations
 
