@@ -94,6 +94,15 @@ typedef struct scopi_gpu_params {
     int32_t initial_step;         /* SCOPI_GPU_STEP_AUTO / _REFERENCE / _CURVATURE (below) */
     double fixed_point_tol;       /* contact_property<FixedPoint> (property.hpp:93-94): 1e-6 */
     int64_t fixed_point_max_iter; /* and 1000 solves at most per step */
+    double box_lower[3];          /* BoxDomain<dim> (box.hpp): corners and periodic axes (0/1); */
+    double box_upper[3];          /* with no periodic axis there is no box.  Each step the active */
+    int32_t periodic[3];          /* spheres within dmax of a periodic lower bound are copied shifted
+                                     by upper - lower into the contact search; a contact with a copy
+                                     takes its body's index and its closest point moved back by
+                                     upper - lower on every periodic axis; after the move a body
+                                     beyond a bound is wrapped (utils.hpp:229-257, base.hpp:118-137,
+                                     solver.hpp:482-522).  Scenes of spheres (planes and segments as
+                                     static obstacles away from the periodic lower bounds) */
 } scopi_gpu_params;
 
 /* First APGD step of every solve.  REFERENCE: alpha as given (apgd.hpp:120, the

@@ -28,6 +28,7 @@ class OrcParams(C.Structure):
         ("tolerance", C.c_double), ("dynamic_descent", C.c_int32), ("mu", C.c_double), ("gamma", C.c_double),
         ("gamma_min", C.c_double), ("gamma_tol", C.c_double), ("num_threads", C.c_int32),
         ("fixed_point_tol", C.c_double), ("fixed_point_max_iter", C.c_int64),
+        ("box_lower", C.c_double * 3), ("box_upper", C.c_double * 3), ("periodic", C.c_int32 * 3),
     ]
 
 
@@ -118,11 +119,12 @@ class OracleSolver:
     def __init__(self, particles, problem=NOFRICTION, vap=VAP_FIXED, contact_method=KDTREE, dmax=2.0,
                  kd_tree_radius=17.0, alpha=0.05, max_ite=10000, tolerance=1e-7, dynamic_descent=True, mu=0.1,
                  gamma=0.0, gamma_min=-2.0, gamma_tol=1e-6, num_threads=0, fixed_point_tol=1e-6,
-                 fixed_point_max_iter=1000):
+                 fixed_point_max_iter=1000, box_lower=(0.0, 0.0, 0.0), box_upper=(0.0, 0.0, 0.0), periodic=(0, 0, 0)):
         self.pa = particles.copy()
         self.params = OrcParams(particles.dim, problem, vap, contact_method, dmax, kd_tree_radius, alpha, max_ite,
                                 tolerance, 1 if dynamic_descent else 0, mu, gamma, gamma_min, gamma_tol, num_threads,
-                                fixed_point_tol, fixed_point_max_iter)
+                                fixed_point_tol, fixed_point_max_iter, (C.c_double * 3)(*box_lower),
+                                (C.c_double * 3)(*box_upper), (C.c_int32 * 3)(*[int(bool(x)) for x in periodic]))
         keep = []
         ps = _particles_struct(self.pa, keep)
         self.h = lib().orc_create(C.byref(self.params), C.byref(ps))

@@ -122,6 +122,12 @@ struct orc_solver {
     std::vector<std::array<double, 5>> se_par;  // superellipsoids: semi-axes, e, n
     std::vector<int32_t> worm;                  // worm index per body, -1 if none
     bool has_worms = false;
+    bool periodic_error = false;                // an obstacle would be copied across a periodic bound
+    bool periodic_any() const {
+        for (int d = 0; d < dim; ++d)
+            if (p.periodic[d]) return true;
+        return false;
+    }
     std::vector<Contact> contacts, old_contacts;
     std::vector<double> lambda;
     orc_stats stats{};
@@ -276,6 +282,37 @@ struct orc_solver {
     // are enumerated with a uniform grid instead of O(N^2) loops.
     void detect() {
         std::vector<Contact> out;
+        // add_objects_from_periodicity (utils.hpp:229-257): per periodic axis d, a copy shifted
+        // by +L_d of every original body within dmax of the lower bound, appended after the
+        // bodies for the search (contact_base::run, base.hpp:71-77)
+        const int64_t n0 = n;
+        std::vector<std::pair<int64_t, int>> ghosts;
+        if (periodic_any()) {
+            for (int d = 0; d < dim; ++d) {
+                if (!p.periodic[d]) continue;
+                for (int64_t b = 0; b < n0; ++b)
+                    if (pos[b][d] - p.dmax < p.box_lower[d]) {
+                        if (b < nin) {
+                            periodic_error = true;
+                            continue;
+                        }
+                        ghosts.push_back({b, d});
+                    }
+            }
+            for (const auto& gd : ghosts) {
+                const int64_t b = gd.first;
+                V3 x = pos[b];
+                x[gd.second] += p.box_upper[gd.second] - p.box_lower[gd.second];
+                pos.push_back(x);
+                q.push_back(q[b]);
+                shape.push_back(shape[b]);
+                radius.push_back(radius[b]);
+                length.push_back(length[b]);
+                se_par.push_back(se_par[b]);
+                worm.push_back(-1);
+            }
+            n = n0 + (int64_t)ghosts.size();
+        }
         const int64_t nA = na();
         const bool use_kd = (p.contact_method == ORC_KDTREE);
         auto kd_ok = [&](int64_t a, int64_t b) {
@@ -380,6 +417,56 @@ struct orc_solver {
                 Contact c;
                 if (exact(a, b, c)) out.push_back(c);
             }
+        std::vector<char> via_copy;  // periodic: the pair was found with a copy
+        if (!ghosts.empty()) {
+            // compute_exact_distance (base.hpp:118-137): pairs of two copies are dropped; a copy's
+            // index becomes its original's and its closest point moves back by L_d on every
+            // periodic axis d
+            std::vector<Contact> kept;
+            kept.reserve(out.size());
+            for (auto& c : out) {
+                if (c.i >= n0 && c.j >= n0) continue;
+                via_copy.push_back(c.i >= n0 || c.j >= n0);
+                for (int d = 0; d < dim; ++d) {
+                    if (!p.periodic[d]) continue;
+                    const double L = p.box_upper[d] - p.box_lower[d];
+                    if (c.i >= n0) c.pi[d] -= L;
+                    if (c.j >= n0) c.pj[d] -= L;
+                }
+                if (c.i >= n0) c.i = ghosts[c.i - n0].first;
+                if (c.j >= n0) c.j = ghosts[c.j - n0].first;
+                kept.push_back(c);
+            }
+            out.swap(kept);
+        }
+        if (n != n0) {  // reset_periodic
+            pos.resize(n0);
+            q.resize(n0);
+            shape.resize(n0);
+            radius.resize(n0);
+            length.resize(n0);
+            se_par.resize(n0);
+            worm.resize(n0);
+            n = n0;
+        }
+        if (!via_copy.empty()) {
+            // a body near the lower bound touching an obstacle is paired with it twice (once as
+            // itself, once as its copy); the reference's std::sort leaves the order of such equal
+            // (i, j) unspecified: here the pair found without a copy comes first
+            std::vector<size_t> order(out.size());
+            for (size_t k = 0; k < order.size(); ++k) order[k] = k;
+            std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) {
+                const Contact &a = out[x], &b = out[y];
+                if (a.i != b.i) return a.i < b.i;
+                if (a.j != b.j) return a.j < b.j;
+                return via_copy[x] < via_copy[y];
+            });
+            std::vector<Contact> sorted;
+            sorted.reserve(out.size());
+            for (size_t k : order) sorted.push_back(out[k]);
+            contacts.swap(sorted);
+            return;
+        }
         std::sort(out.begin(), out.end(), [](const Contact& x, const Contact& y) {
             return x.i < y.i || (x.i == y.i && x.j < y.j);
         });
@@ -971,6 +1058,16 @@ struct orc_solver {
             for (int d = 0; d < dim; ++d) pos[b][d] += dt * v[b][d];
             rotate_body(q[b], w, nw, dt);
         }
+        // periodic wrap of every object beyond a periodic bound (solver.hpp:482-522)
+        for (int d = 0; d < dim; ++d) {
+            if (!p.periodic[d]) continue;
+            const double L = p.box_upper[d] - p.box_lower[d];
+            for (int64_t b = 0; b < n; ++b) {
+                const bool plus = pos[b][d] > p.box_upper[d], minus = pos[b][d] < p.box_lower[d];
+                if (plus) pos[b][d] -= L;
+                if (minus) pos[b][d] += L;
+            }
+        }
         auto t4 = clk::now();
         auto sec = [](clk::time_point a, clk::time_point b) { return std::chrono::duration<double>(b - a).count(); };
         stats.seconds_contacts += sec(t1, t2);
@@ -1049,7 +1146,7 @@ orc_solver* orc_create(const orc_params* p, const orc_particles* parts) {
     }
     s->dim = p->dim;
     s->load(parts);
-    if (s->has_worms && p->problem != ORC_NOFRICTION) {
+    if ((s->has_worms && p->problem != ORC_NOFRICTION) || (s->has_worms && s->periodic_any())) {
         delete s;
         return nullptr;
     }
@@ -1064,7 +1161,10 @@ void orc_destroy(orc_solver* s) { delete s; }
 int orc_run(orc_solver* s, double dt, int64_t total_it, int64_t initial_iter) {
     if (!s) return -1;
     s->dt = dt;
-    for (int64_t it = initial_iter; it < total_it; ++it) s->step();
+    for (int64_t it = initial_iter; it < total_it; ++it) {
+        s->step();
+        if (s->periodic_error) return -2;
+    }
     return 0;
 }
 

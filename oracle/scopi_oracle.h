@@ -64,6 +64,9 @@ typedef struct {
     int32_t num_threads;      /* OpenMP threads for the loops the reference parallelises (0 = default) */
     double fixed_point_tol;   /* contact_property<FixedPoint> (1e-6, 1000): FrictionFixedPoint, ViscousFriction */
     int64_t fixed_point_max_iter;
+    double box_lower[3];      /* BoxDomain<dim> (box.hpp): corners, and the periodic axes (none: */
+    double box_upper[3];      /* no box); an obstacle within dmax of a periodic lower bound makes */
+    int32_t periodic[3];      /* orc_run fail (the reference pairs it with its own ghost) */
 } orc_params;
 
 typedef struct {

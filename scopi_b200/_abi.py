@@ -35,6 +35,7 @@ class Params(C.Structure):
         ("gamma", C.c_double), ("gamma_min", C.c_double), ("gamma_tol", C.c_double),
         ("mixed_violation_tol", C.c_double), ("mixed_max_corrections", C.c_int32), ("device", C.c_int32),
         ("initial_step", C.c_int32), ("fixed_point_tol", C.c_double), ("fixed_point_max_iter", C.c_int64),
+        ("box_lower", C.c_double * 3), ("box_upper", C.c_double * 3), ("periodic", C.c_int32 * 3),
     ]
 
 

@@ -810,6 +810,166 @@ __global__ void k_append_links(int C, int W, const int* links, Contacts c, Sizes
     }
 }
 
+// ---------------------------------------------------------------- periodic box
+__global__ void k_ghost_flags(Bodies B, PeriodicBox box, double dmax, int dim, int* flag) {
+    const int na = B.n - B.nin;
+    GRID_STRIDE(t, (long long)dim * na) {
+        const int d = (int)(t / na), a = B.nin + (int)(t - (long long)d * na);
+        flag[t] = (box.per[d] && B.pos[3 * (long long)a + d] - dmax < box.lo[d]) ? 1 : 0;
+    }
+}
+
+__global__ void k_ghost_fill(Bodies B, PeriodicBox box, int dim, GhostBodies g) {
+    const int n = B.n, na = B.n - B.nin;
+    GRID_STRIDE(k, n) {
+        for (int d = 0; d < 3; ++d) g.pos[3 * k + d] = B.pos[3 * k + d];
+        for (int d = 0; d < 4; ++d) g.q[4 * k + d] = B.q[4 * k + d];
+        g.shape[k] = B.shape[k];
+        g.radius[k] = B.radius[k];
+        g.length[k] = B.length[k];
+    }
+    GRID_STRIDE(t, (long long)dim * na) {
+        if (!g.flag[t]) continue;
+        const int d = (int)(t / na), a = B.nin + (int)(t - (long long)d * na);
+        const long long k = n + g.rank[t];
+        for (int e = 0; e < 3; ++e) g.pos[3 * k + e] = B.pos[3 * (long long)a + e];
+        g.pos[3 * k + d] += box.up[d] - box.lo[d];
+        for (int e = 0; e < 4; ++e) g.q[4 * k + e] = B.q[4 * (long long)a + e];
+        g.shape[k] = B.shape[a];
+        g.radius[k] = B.radius[a];
+        g.length[k] = B.length[a];
+        g.src[g.rank[t]] = a;
+    }
+}
+
+__global__ void k_per_classify(const Sizes* sizes, int n, const int* ci, const int* cj, int* fr, int* fg) {
+    GRID_STRIDE(k, sizes->C) {
+        const bool gi = ci[k] >= n, gj = cj[k] >= n;
+        fr[k] = (!gi && !gj) ? 1 : 0;
+        fg[k] = (!gi && gj) ? 1 : 0;
+    }
+}
+
+__global__ void k_per_gather(const Sizes* sizes, int n, const int* ci, const int* cj, PeriodicScratch w,
+                             const int* src) {
+    GRID_STRIDE(k, sizes->C) {
+        if (w.fr[k]) {
+            w.r_ci[w.pr[k]] = ci[k];
+            w.r_cj[w.pr[k]] = cj[k];
+        }
+        if (w.fg[k]) {
+            w.g_ci[w.pg[k]] = ci[k];
+            w.g_cj[w.pg[k]] = src[cj[k] - n];
+            w.g_k[w.pg[k]] = (int)k;
+        }
+    }
+}
+
+__device__ __forceinline__ bool key_less(int ai, int aj, int bi, int bj) { return ai < bi || (ai == bi && aj < bj); }
+
+// rank of each copy's pair among the copies' pairs: they come sorted by i, so its segment
+// of equal i is found by binary search and ordered by (j, position) by counting
+__global__ void k_per_rank(const int* totals, PeriodicScratch w) {
+    const int G = totals[1];
+    GRID_STRIDE(g, G) {
+        const int i = w.g_ci[g], j = w.g_cj[g];
+        int lo = 0, hi = (int)g;  // first index with g_ci == i
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (w.g_ci[mid] < i)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        int r = lo;
+        for (int h = lo; h < G && w.g_ci[h] == i; ++h)
+            if (w.g_cj[h] < j || (w.g_cj[h] == j && h < g)) ++r;
+        w.g_rank[g] = r;
+        w.s_ci[r] = i;
+        w.s_cj[r] = j;
+    }
+}
+
+// number of keys of the sorted list (ki, kj)[0, m) below (i, j) (or not above, when `le`)
+__device__ __forceinline__ int count_below(const int* ki, const int* kj, int m, int i, int j, bool le) {
+    int lo = 0, hi = m;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        const bool below = le ? !key_less(i, j, ki[mid], kj[mid]) : key_less(ki[mid], kj[mid], i, j);
+        if (below)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__global__ void k_per_scatter(const Sizes* sizes, const int* totals, int dim, PeriodicBox box, Contacts ext,
+                              Contacts out, PeriodicScratch w) {
+    const int R = totals[0], G = totals[1];
+    GRID_STRIDE(k, sizes->C) {
+        const bool r = w.fr[k], g = w.fg[k];
+        if (!r && !g) continue;
+        const int i = ext.ci[k];
+        int j, at;
+        if (r) {
+            j = ext.cj[k];
+            at = w.pr[k] + count_below(w.s_ci, w.s_cj, G, i, j, false);
+        } else {
+            const int pg = w.pg[k];
+            j = w.g_cj[pg];
+            at = w.g_rank[pg] + count_below(w.r_ci, w.r_cj, R, i, j, true);
+        }
+        out.ci[at] = i;
+        out.cj[at] = j;
+        out.dij[at] = ext.dij[k];
+        for (int d = 0; d < 3; ++d) {
+            out.nij[3 * (long long)at + d] = ext.nij[3 * k + d];
+            out.pi[3 * (long long)at + d] = ext.pi[3 * k + d];
+            double pj = ext.pj[3 * k + d];
+            if (g && d < dim && box.per[d]) pj -= box.up[d] - box.lo[d];
+            out.pj[3 * (long long)at + d] = pj;
+        }
+    }
+}
+
+__global__ void k_per_size(const int* totals, Sizes* sizes) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) sizes->C = totals[0] + totals[1];
+}
+
+__global__ void k_transfer(StepParams p, Contacts c, const Sizes* sizes, Contacts old_c, const int* old_C) {
+    const int C = sizes->C;
+    const int oC = old_C ? *old_C : 0;
+    GRID_STRIDE(k, C) {
+        const int a = c.ci[k], b = c.cj[k];
+        double gam = p.gamma0;
+        if (oC > 0) {
+            int lo = 0, hi = oC;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (key_less(old_c.ci[mid], old_c.cj[mid], a, b))
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            if (lo < oC && old_c.ci[lo] == a && old_c.cj[lo] == b) gam = old_c.gamma[lo];
+        }
+        c.gamma[k] = gam;
+    }
+}
+
+__global__ void k_periodic_wrap(Bodies B, PeriodicBox box, int dim) {
+    GRID_STRIDE(k, B.n) {
+        for (int d = 0; d < dim; ++d) {
+            if (!box.per[d]) continue;
+            double& x = B.pos[3 * k + d];
+            const bool plus = x > box.up[d], minus = x < box.lo[d];
+            if (plus) x -= box.up[d] - box.lo[d];
+            if (minus) x += box.up[d] - box.lo[d];
+        }
+    }
+}
+
 __global__ void k_gamma_update_vf(StepParams p, Contacts c, Assembly a, const double* lam, const Sizes* sizes) {
     const int C = sizes->C;
     GRID_STRIDE(k, C) {
@@ -1051,6 +1211,53 @@ void launch_incidence(const Bodies& b, const StepParams& p, const Contacts& c, c
 
 void launch_append_links(int C, int W, const int* links, Contacts& c, Sizes* sizes, cudaStream_t s) {
     k_append_links<<<blocks_for(W), kThreads, 0, s>>>(C, W, links, c, sizes);
+    LAUNCHED(1);
+}
+
+void launch_ghost_flags(const Bodies& b, const PeriodicBox& box, double dmax, int dim, GhostBodies& g, int* total,
+                        int* scan_work, cudaStream_t s) {
+    const long long m = (long long)dim * (b.n - b.nin);
+    k_ghost_flags<<<blocks_for(m + 1), kThreads, 0, s>>>(b, box, dmax, dim, g.flag);
+    LAUNCHED(1);
+    scan_exclusive(g.flag, g.rank, nullptr, (int)m, m, total, scan_work, s, &g_detect_launches);
+}
+
+Bodies launch_ghost_fill(const Bodies& b, const PeriodicBox& box, int dim, int n_ghosts, GhostBodies& g,
+                         cudaStream_t s) {
+    const long long m = std::max<long long>((long long)dim * (b.n - b.nin), b.n);
+    k_ghost_fill<<<blocks_for(m), kThreads, 0, s>>>(b, box, dim, g);
+    LAUNCHED(1);
+    Bodies e = b;
+    e.n = b.n + n_ghosts;
+    e.pos = g.pos;
+    e.q = g.q;
+    e.shape = g.shape;
+    e.radius = g.radius;
+    e.length = g.length;
+    return e;
+}
+
+void launch_periodic_remap(int n, int dim, const PeriodicBox& box, const GhostBodies& g, const Contacts& ext,
+                           Contacts& out, PeriodicScratch& w, Sizes* sizes, long long c_cap, int* totals,
+                           int* scan_work, cudaStream_t s) {
+    k_per_classify<<<blocks_for(c_cap), kThreads, 0, s>>>(sizes, n, ext.ci, ext.cj, w.fr, w.fg);
+    scan_exclusive(w.fr, w.pr, &sizes->C, 0, c_cap, totals + 0, scan_work, s, &g_detect_launches);
+    scan_exclusive(w.fg, w.pg, &sizes->C, 0, c_cap, totals + 1, scan_work, s, &g_detect_launches);
+    k_per_gather<<<blocks_for(c_cap), kThreads, 0, s>>>(sizes, n, ext.ci, ext.cj, w, g.src);
+    k_per_rank<<<blocks_for(c_cap), kThreads, 0, s>>>(totals, w);
+    k_per_scatter<<<blocks_for(c_cap), kThreads, 0, s>>>(sizes, totals, dim, box, ext, out, w);
+    k_per_size<<<1, 1, 0, s>>>(totals, sizes);
+    LAUNCHED(5);
+}
+
+void launch_transfer(const StepParams& p, Contacts& c, const Sizes* sizes, const Contacts& old, const int* old_C,
+                     long long c_cap, cudaStream_t s) {
+    k_transfer<<<blocks_for(c_cap), kThreads, 0, s>>>(p, c, sizes, old, old_C);
+    LAUNCHED(1);
+}
+
+void launch_periodic_wrap(const Bodies& b, const PeriodicBox& box, int dim, cudaStream_t s) {
+    k_periodic_wrap<<<blocks_for(b.n), kThreads, 0, s>>>(b, box, dim);
     LAUNCHED(1);
 }
 

@@ -88,6 +88,48 @@ void launch_incidence(const Bodies& b, const StepParams& p, const Contacts& c, c
 // at C..C+W-1 after the sorted list (C on the host, the list's count), sizes->C = C + W and
 // sizes->n_links = W; k_geometry negates their normal and distance.
 void launch_append_links(int C, int W, const int* links, Contacts& c, Sizes* sizes, cudaStream_t s);
+
+// Periodic BoxDomain (box.hpp, utils.hpp:229-257, base.hpp:71-77,118-137, solver.hpp:482-522).
+struct PeriodicBox {
+    double lo[3], up[3];
+    int per[3];
+};
+// Body arrays of the search: the n bodies, then per periodic axis d the copies shifted by
+// up[d] - lo[d] of the active bodies within dmax of lo[d] (t = d * na + a order).
+struct GhostBodies {
+    double* pos;   // (n + ghosts) * 3
+    double* q;     // * 4
+    int* shape;
+    double* radius;
+    double* length;
+    int* src;      // ghost -> its body
+    int* flag;     // dim * na + 1
+    int* rank;     // dim * na + 1
+};
+// flags and ranks of the copies; the count lands in *total (device)
+void launch_ghost_flags(const Bodies& b, const PeriodicBox& box, double dmax, int dim, GhostBodies& g, int* total,
+                        int* scan_work, cudaStream_t s);
+// fills the search arrays with the bodies and the copies; returns the search's Bodies view
+Bodies launch_ghost_fill(const Bodies& b, const PeriodicBox& box, int dim, int n_ghosts, GhostBodies& g,
+                         cudaStream_t s);
+// Scratch of the remap: per contact two flags and two ranks, the real pairs' keys and the
+// copies' entries (cap each).
+struct PeriodicScratch {
+    int *fr, *fg, *pr, *pg;
+    int *r_ci, *r_cj, *g_ci, *g_cj, *g_k, *g_rank, *s_ci, *s_cj;
+};
+// The search's list (over bodies and copies, sorted, geometry from the copies' positions) ->
+// `out`: pairs of two copies dropped, a copy's index replaced by its body's and its closest
+// point moved back by up[d] - lo[d] on every periodic axis, the list sorted again by (i, j)
+// (a real pair before a copy's pair of the same (i, j)); sizes->C updated.
+void launch_periodic_remap(int n, int dim, const PeriodicBox& box, const GhostBodies& g, const Contacts& ext,
+                           Contacts& out, PeriodicScratch& w, Sizes* sizes, long long c_cap, int* totals,
+                           int* scan_work, cudaStream_t s);
+// viscous gamma carried over from the previous list by (i, j) (transfer, solver.hpp:241-258)
+void launch_transfer(const StepParams& p, Contacts& c, const Sizes* sizes, const Contacts& old, const int* old_C,
+                     long long c_cap, cudaStream_t s);
+// wrap of the bodies beyond a periodic bound after the move (solver.hpp:482-522)
+void launch_periodic_wrap(const Bodies& b, const PeriodicBox& box, int dim, cudaStream_t s);
 void launch_gamma_update(const StepParams& p, Contacts& c, const Assembly& a, const double* lambda, const Sizes* sizes,
                          long long c_cap, cudaStream_t s);
 // v += dt*u_v, omega += dt*u_w, then pos/q integration (u = M^-1 B^T lambda, may be null).

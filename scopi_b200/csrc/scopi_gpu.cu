@@ -76,6 +76,14 @@ struct scopi_gpu_handle {
     long long c_cap = 0;
     DevMem cap_mem;
     Contacts cur{}, old{};
+    // periodic BoxDomain: the search runs over the bodies and their copies into `ext`
+    bool periodic = false;
+    PeriodicBox box{};
+    GhostBodies gb{};
+    PeriodicScratch pw{};
+    Contacts ext{};
+    int* d_gcount = nullptr;  // 1 + 2: copies, remap totals
+    int* h_gcount = nullptr;  // pinned
     Sizes* d_sizes_cur = nullptr;
     Sizes* d_sizes_old = nullptr;
     bool has_old = false;
@@ -463,6 +471,10 @@ struct scopi_gpu_handle {
         if ((e = cudaMallocHost(&h_result, sizeof(ApgdResult))) != cudaSuccess) return cuda_fail(e, "cudaMallocHost");
         if ((e = cudaMallocHost(&h_viol, sizeof(unsigned long long))) != cudaSuccess)
             return cuda_fail(e, "cudaMallocHost");
+        if (periodic) {
+            if ((e = alloc(fixed_mem, d_gcount, 3)) != cudaSuccess) return cuda_fail(e, "alloc");
+            if ((e = cudaMallocHost(&h_gcount, sizeof(int))) != cudaSuccess) return cuda_fail(e, "cudaMallocHost");
+        }
         if (fp_loop()) {
             if ((e = alloc(fixed_mem, d_fp_part, 2 * (size_t)kFixedPointMaxBlocks)) != cudaSuccess)
                 return cuda_fail(e, "alloc");
@@ -500,13 +512,21 @@ struct scopi_gpu_handle {
             A(d_u64[k], 6 * (size_t)na + 6)
             A(d_u32[k], 6 * (size_t)na + 6)
         }
-        dw.cell_cap = std::max<long long>({4LL * na, 4096LL, cell_cap_hint});
-        dw.obs_cap = obs_cap >= 0 ? obs_cap : (long long)nin * na;
+        // the search of a periodic box also holds the copies: up to dim per active body
+        const long long naw = periodic ? (long long)na * (1 + P.dim) : na;
+        dw.cell_cap = std::max<long long>({4LL * naw, 4096LL, cell_cap_hint});
+        dw.obs_cap = obs_cap >= 0 ? obs_cap : (long long)nin * naw;
         A(dw.grid, 1) A(dw.bbox_partial, 8 * 4 * kSMs) A(dw.cell_count, dw.cell_cap + 1) A(dw.cell_start, dw.cell_cap + 1)
-        A(dw.cell_fill, dw.cell_cap) A(dw.cell_of, na + 1) A(dw.cell_body, na + 1) A(dw.cell_pr, na + 1)
-        A(dw.row_count, na + 1) A(dw.row_ptr, na + 1) A(dw.row_tmp, (size_t)na * kRowCap + 1) A(dw.obs_flag, dw.obs_cap + 1) A(dw.obs_pos, dw.obs_cap + 1)
+        A(dw.cell_fill, dw.cell_cap) A(dw.cell_of, naw + 1) A(dw.cell_body, naw + 1) A(dw.cell_pr, naw + 1)
+        A(dw.row_count, naw + 1) A(dw.row_ptr, naw + 1) A(dw.row_tmp, (size_t)naw * kRowCap + 1) A(dw.obs_flag, dw.obs_cap + 1) A(dw.obs_pos, dw.obs_cap + 1)
         A(dw.tmp_total, 4)
-        const long long scan_max = std::max<long long>(std::max<long long>(dw.cell_cap + 1, dw.obs_cap + 1), na + 1);
+        if (periodic) {
+            const long long ne = n + (naw - na), m = (long long)P.dim * na + 1;
+            A(gb.pos, 3 * ne) A(gb.q, 4 * ne) A(gb.shape, ne) A(gb.radius, ne) A(gb.length, ne) A(gb.src, m)
+            A(gb.flag, m) A(gb.rank, m)
+        }
+        const long long scan_max =
+            std::max<long long>(std::max<long long>(dw.cell_cap + 1, dw.obs_cap + 1), std::max<long long>(naw, 1) * 3 + 1);
         A(dw.scan_work, scan_work_ints(std::max<long long>(scan_max, 1LL << 26)))
         A(inc.count, na + 1) A(inc.jcount, na + 1) A(inc.ptr, na + 1)
 #undef A
@@ -525,6 +545,13 @@ struct scopi_gpu_handle {
         for (Contacts* c : {&cur, &old}) {
             A(c->ci, cap) A(c->cj, cap) A(c->dij, cap) A(c->nij, 3 * cap) A(c->pi, 3 * cap) A(c->pj, 3 * cap)
             A(c->gamma, cap)
+        }
+        if (periodic) {
+            A(ext.ci, cap) A(ext.cj, cap) A(ext.dij, cap) A(ext.nij, 3 * cap) A(ext.pi, 3 * cap) A(ext.pj, 3 * cap)
+            A(ext.gamma, cap)
+            for (int** q : {&pw.fr, &pw.fg, &pw.pr, &pw.pg, &pw.r_ci, &pw.r_cj, &pw.g_ci, &pw.g_cj, &pw.g_k, &pw.g_rank,
+                            &pw.s_ci, &pw.s_cj})
+                A(*q, cap + 1)
         }
         A(as.bn, 3 * cap) A(as.bai, 3 * cap) A(as.baj, 3 * cap)
         if (friction_rows()) A(as.bP, 18 * cap)
@@ -564,7 +591,49 @@ struct scopi_gpu_handle {
     }
 
     // contact detection + closest points + assembly + incidence lists into `cur`
+    // Detection in a periodic box: copies of the active bodies near the lower bounds join the
+    // search (contact_base::run, base.hpp:71-77), the list is mapped back to the bodies and
+    // sorted again (compute_exact_distance, base.hpp:118-137), then gamma is carried over.
+    int detect_periodic(double dt, bool assemble) {
+        Bodies b = bodies();
+        StepParams sp = step_params(dt);
+        launch_ghost_flags(b, box, P.dmax, P.dim, gb, d_gcount, dw.scan_work, stream);
+        cudaMemcpyAsync(h_gcount, d_gcount, sizeof(int), cudaMemcpyDeviceToHost, stream);
+        cudaError_t e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cuda_fail(e, "periodic copies");
+        const Bodies eb = launch_ghost_fill(b, box, P.dim, *h_gcount, gb, stream);
+        dw.obs_cap = (long long)nin * (eb.n - eb.nin);
+        for (int attempt = 0; attempt < 4; ++attempt) {
+            cudaMemsetAsync(d_sizes_cur, 0, sizeof(Sizes), stream);
+            launch_detect(eb, sp, dw, ext, d_sizes_cur, c_cap, stream);
+            cudaMemcpyAsync(h_sizes, d_sizes_cur, sizeof(Sizes), cudaMemcpyDeviceToHost, stream);
+            e = cudaStreamSynchronize(stream);
+            if (e != cudaSuccess) return cuda_fail(e, "detect");
+            if (!h_sizes->overflow) break;
+            int tot[2] = {0, 0};
+            cudaMemcpy(tot, dw.tmp_total, 2 * sizeof(int), cudaMemcpyDeviceToHost);
+            const long long total = (long long)tot[0] + tot[1];
+            const long long need = (long long)std::ceil(1.3 * ((double)h_sizes->C + 1.0)) + 1024;
+            int rc = regrow(std::max(need, (long long)(1.3 * total) + 1024));
+            if (rc) return rc;
+            if (attempt == 3) return fail(SCOPI_GPU_ENOMEM, "contact capacity could not be grown");
+        }
+        launch_geometry(eb, sp, ext, d_sizes_cur, c_cap, nullptr, nullptr, c_cap, stream);
+        launch_periodic_remap(n, P.dim, box, gb, ext, cur, pw, d_sizes_cur, c_cap, d_gcount + 1, dw.scan_work, stream);
+        launch_transfer(sp, cur, d_sizes_cur, old, has_old ? &d_sizes_old->C : nullptr, c_cap, stream);
+        if (assemble) {
+            launch_assemble(b, sp, cur, as, d_sizes_cur, c_cap, dw.scan_work, dw.tmp_total + 2, stream);
+            launch_incidence(b, sp, cur, as, inc, d_sizes_cur, c_cap, dw.scan_work, dw.tmp_total + 2, stream,
+                             !sphere_mode());
+        }
+        cudaMemcpyAsync(h_sizes, d_sizes_cur, sizeof(Sizes), cudaMemcpyDeviceToHost, stream);
+        e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cuda_fail(e, "assemble");
+        return 0;
+    }
+
     int detect_and_assemble(double dt, bool assemble) {
+        if (periodic) return detect_periodic(dt, assemble);
         Bodies b = bodies();
         StepParams sp = step_params(dt);
         for (int attempt = 0; attempt < 4; ++attempt) {
@@ -871,6 +940,7 @@ struct scopi_gpu_handle {
         last_M = M;
         cudaEventRecord(ev[2], stream);
         launch_update(b, sp, ufin, ustride, urot, d_sizes_cur, stream);
+        if (periodic) launch_periodic_wrap(b, box, P.dim, stream);
         cudaEventRecord(ev[3], stream);
         cudaError_t e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) return cuda_fail(e, "step");
@@ -1108,6 +1178,20 @@ int32_t scopi_gpu_create(const scopi_gpu_params* p, scopi_gpu_handle** out) {
         h->fixed_point = true;
         h->P.problem = SCOPI_GPU_FRICTION;  // the Friction problem plus the s term and the loop
     }
+    for (int d = 0; d < p->dim; ++d)
+        if (p->periodic[d]) {
+            if (!(p->box_upper[d] > p->box_lower[d])) {
+                delete h;
+                scopi_gpu::set_global_error("periodic box: upper bound must exceed the lower bound");
+                return SCOPI_GPU_EINVAL;
+            }
+            h->periodic = true;
+        }
+    for (int d = 0; d < 3; ++d) {
+        h->box.lo[d] = p->box_lower[d];
+        h->box.up[d] = p->box_upper[d];
+        h->box.per[d] = (d < p->dim && p->periodic[d]) ? 1 : 0;
+    }
     h->dev = p->device;
     cudaSetDevice(h->dev);
     if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess) {
@@ -1139,6 +1223,7 @@ int32_t scopi_gpu_destroy(scopi_gpu_handle* h) {
     if (h->h_result) cudaFreeHost(h->h_result);
     if (h->h_viol) cudaFreeHost(h->h_viol);
     if (h->h_fp_part) cudaFreeHost(h->h_fp_part);
+    if (h->h_gcount) cudaFreeHost(h->h_gcount);
     for (auto& x : h->ev)
         if (x) cudaEventDestroy(x);
     for (auto& x : h->ev_a)
@@ -1236,6 +1321,23 @@ static int32_t upload_particles(scopi_gpu_handle* h, const scopi_gpu_particles* 
         }
         if (!links.empty() && (h->batch || h->P.problem != SCOPI_GPU_NOFRICTION))
             return h->fail(SCOPI_GPU_EUNSUPPORTED, "worms: single scenes with the NoFriction problem");
+    }
+    if (h->periodic) {
+        if (n_se > 0 || !links.empty() || h->batch)
+            return h->fail(SCOPI_GPU_EUNSUPPORTED, "periodic box: single scenes of spheres, no worms");
+        if ((long long)nin * (n - nin) * (1 + h->P.dim) >= (1LL << 31))
+            return h->fail(SCOPI_GPU_EUNSUPPORTED, "obstacles x active bodies and copies must stay below 2^31");
+        for (int i = 0; i < nin; ++i) {
+            for (int d = 0; d < 3; ++d)
+                if (p->vd[3 * (size_t)i + d] != 0.0 || p->omega_d[3 * (size_t)i + d] != 0.0)
+                    return h->fail(SCOPI_GPU_EUNSUPPORTED, "periodic box: obstacles must be static");
+            // the reference copies such an obstacle too and pairs it with its original through
+            // the plane-plane case its dispatcher leaves unimplemented (an empty contact)
+            for (int d = 0; d < h->P.dim; ++d)
+                if (h->box.per[d] && p->pos[3 * (size_t)i + d] - h->P.dmax < h->box.lo[d])
+                    return h->fail(SCOPI_GPU_EUNSUPPORTED,
+                                   "periodic box: an obstacle lies within dmax of a periodic lower bound");
+        }
     }
     h->has_se = n_se > 0;
     cudaSetDevice(h->dev);

@@ -39,6 +39,17 @@ class _ParamGroup(SimpleNamespace):
     pass
 
 
+def _set_param(p, k, v):
+    """One field of scopi_gpu_params; booleans and the box's 3-vectors converted."""
+    if k == "dynamic_descent":
+        v = 1 if v else 0
+    elif k in ("box_lower", "box_upper"):
+        v = (C.c_double * 3)(*([float(x) for x in v] + [0.0] * (3 - len(v))))
+    elif k == "periodic":
+        v = (C.c_int32 * 3)(*([int(bool(x)) for x in v] + [0] * (3 - len(v))))
+    setattr(p, k, v)
+
+
 class ScopiSolver:
     """GPU ScopiSolver.  ``particles`` is a ``ParticleArrays`` (obstacles first)."""
 
@@ -49,9 +60,7 @@ class ScopiSolver:
         self._lib.scopi_gpu_default_params(C.byref(p), particles.dim)
         p.problem, p.vap, p.contact_method, p.precision, p.device = problem, vap, contact_method, precision, device
         for k, v in overrides.items():
-            if k == "dynamic_descent":
-                v = 1 if v else 0
-            setattr(p, k, v)
+            _set_param(p, k, v)
         self._params = p
         self._h = None
         self.particles = particles.copy()
@@ -227,9 +236,7 @@ class ScopiBatch:
         self._lib.scopi_gpu_default_params(C.byref(p), scenes[0].dim)
         p.problem, p.vap, p.contact_method, p.precision, p.device = NOFRICTION, vap, contact_method, precision, device
         for k, v in overrides.items():
-            if k == "dynamic_descent":
-                v = 1 if v else 0
-            setattr(p, k, v)
+            _set_param(p, k, v)
         self._params = p
         self.scenes = [s.copy() for s in scenes]
         arr = (_abi.ParticlesC * len(self.scenes))()

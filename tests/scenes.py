@@ -418,3 +418,37 @@ def two_worms(contact_method=KDTREE):
     p.add_worm([(-1.0 - 2 * k, -0.7) for k in range(6)], 1.0, Property(desired_velocity=(1.0, 0.0), **prop))
     kw = dict(problem=NOFRICTION, vap=VAP_FIXED, contact_method=contact_method, dmax=1.0)
     return p.finalize(), kw, 0.005, 1000
+
+
+def periodic_disks(problem=NOFRICTION, contact_method=KDTREE):
+    """A periodic BoxDomain (box.hpp) along x, [0, 4]: two rows of eight disks (r 0.2) on a
+    horizontal floor plane whose position (x = 2) stays away from the periodic bound, the
+    lower row moving at +1, the upper at -0.6, gravity -1, vap_fpd, dmax 0.3, dt 0.01, 150
+    steps; the rows cross the bound several times and meet their copies."""
+    p = Particles(2)
+    p.add_plane((2.0, 0.0), PI / 2)
+    for k in range(8):
+        p.add_sphere((0.25 + 0.5 * k, 0.2), 0.2, Property(mass=1.0, moment_inertia=0.02, velocity=(1.0, 0.0),
+                                                          force=(0.0, -1.0)))
+    for k in range(8):
+        p.add_sphere((0.5 * k, 0.6), 0.2, Property(mass=1.0, moment_inertia=0.02, velocity=(-0.6, 0.0),
+                                                   force=(0.0, -1.0)))
+    kw = dict(problem=problem, vap=VAP_FPD, contact_method=contact_method, dmax=0.3, tolerance=1e-9,
+              max_ite=20000, alpha=0.1, box_lower=(0.0, 0.0, 0.0), box_upper=(4.0, 0.0, 0.0), periodic=(1, 0, 0))
+    if problem == FRICTION:
+        kw["mu"] = 0.3
+    return p.finalize(), kw, 0.01, 150
+
+
+def periodic_two_disks(unwrapped=False):
+    """Two disks (r 0.25) meeting across the periodic bound x = 0 of the box [0, 4]: A at 0.3
+    moving at -0.5, B at 3.7 moving at +0.5 (vap_fixed, dmax 0.5, so that A's copy joins the
+    search); with ``unwrapped`` the same scene without a box, B at 3.7 - 4."""
+    p = Particles(2)
+    p.add_sphere((0.3, 0.0), 0.25, Property(mass=1.0, moment_inertia=0.1, desired_velocity=(-0.5, 0.0)))
+    p.add_sphere((-0.3 if unwrapped else 3.7, 0.0), 0.25, Property(mass=1.0, moment_inertia=0.1,
+                                                                   desired_velocity=(0.5, 0.0)))
+    kw = dict(problem=NOFRICTION, vap=VAP_FIXED, dmax=0.5, tolerance=1e-10, max_ite=20000, alpha=0.1)
+    if not unwrapped:
+        kw.update(box_lower=(0.0, 0.0, 0.0), box_upper=(4.0, 0.0, 0.0), periodic=(1, 0, 0))
+    return p.finalize(), kw, 0.01, 40

@@ -384,3 +384,62 @@ def test_worms_need_nofriction_on_gpu():
     pa, kw, dt, _ = S.two_worms()
     with pytest.raises(ScopiGPUError):
         gpu_solver(pa, **dict(kw, problem=S.FRICTION)).run(dt, 1)
+
+
+def test_periodic_two_disks_on_gpu():
+    """Periodic BoxDomain: the two disks meeting across the bound follow the oracle, and the
+    same disks side by side without a box, modulo the period."""
+    pa, kw, dt, total = S.periodic_two_disks()
+    g = gpu_solver(pa, **kw)
+    o = oracle_solver(pa, **kw)
+    pu, kwu, _, _ = S.periodic_two_disks(unwrapped=True)
+    u = gpu_solver(pu, **kwu)
+    same_contacts(g.detect(), o.detect())
+    for _ in range(total):
+        g.run(dt, 1)
+        o.run(dt, 1)
+        u.run(dt, 1)
+        gc, oc = g.current_contacts(), o.contacts()
+        assert np.array_equal(gc["i"], oc["i"]) and np.array_equal(gc["j"], oc["j"])
+        assert np.max(np.abs(g.particles.pos - o.pa.pos)) <= 1e-8
+        dx = (g.particles.pos[:, 0] - u.particles.pos[:, 0]) % 4.0
+        assert np.all(np.minimum(dx, 4.0 - dx) <= 1e-8)
+
+
+@pytest.mark.parametrize("problem", [S.NOFRICTION, S.FRICTION])
+@pytest.mark.parametrize("method", [S.KDTREE, S.BRUTE_FORCE])
+def test_periodic_disks_match_oracle(problem, method):
+    """Rows of disks crossing a periodic bound, GPU (FP64) against the oracle: on the same
+    input the contact lists (copies mapped back to their bodies, closest points moved by the
+    period, sorted by (i, j) with i > j across the bound) are equal bit for bit; stepped
+    together, the pairs of every step and the trajectories agree."""
+    pa, kw, dt, total = S.periodic_disks(problem, method)
+    g = gpu_solver(pa, **kw)
+    o = oracle_solver(pa, **kw)
+    same_contacts(g.detect(), o.detect())
+    across = 0
+    for k in range(total):
+        g.run(dt, 1)
+        o.run(dt, 1)
+        gc, oc = g.current_contacts(), o.contacts()
+        assert np.array_equal(gc["i"], oc["i"]) and np.array_equal(gc["j"], oc["j"]), k
+        across += int(np.sum(gc["i"] > gc["j"]))
+    assert across > 0
+    assert rel_err(g.particles.pos, o.pa.pos) <= 1e-9
+    assert rel_err(g.particles.v, o.pa.v) <= 1e-6
+
+
+def test_periodic_mixed_precision():
+    pa, kw, dt, total = S.periodic_disks()
+    f64 = gpu_solver(pa, **kw).run(dt, total)
+    mix = gpu_solver(pa, precision=1, mixed_violation_tol=1e-6, **dict(kw, tolerance=1e-7)).run(dt, total)
+    assert mix.stats()["violation"] <= 1e-6
+    assert rel_err(mix.particles.pos, f64.particles.pos) <= 1e-5
+
+
+def test_periodic_obstacle_near_bound_rejected():
+    from scopi_b200 import ScopiGPUError
+    pa, kw, dt, _ = S.periodic_disks()
+    pa.pos[0, 0] = 0.1
+    with pytest.raises(ScopiGPUError):
+        gpu_solver(pa, **kw).run(dt, 1)

@@ -293,3 +293,66 @@ def test_worms_need_nofriction():
     pa, kw, _, _ = S.two_worms()
     with pytest.raises(RuntimeError):
         orc.OracleSolver(pa, **dict(kw, problem=S.FRICTION))
+
+
+def test_periodic_two_disks_match_unwrapped():
+    """BoxDomain periodic along x (box.hpp, utils.hpp:229-257, base.hpp:118-137,
+    solver.hpp:482-522): two disks meeting across the bound move as the same two disks
+    side by side without a box, positions equal modulo the period (to the solver's
+    accuracy: the contact across the bound is listed as (B, A), the other as (A, B))."""
+    pa, kw, dt, total = S.periodic_two_disks()
+    s = orc.OracleSolver(pa, **kw)
+    pu, kwu, _, _ = S.periodic_two_disks(unwrapped=True)
+    u = orc.OracleSolver(pu, **kwu)
+    met = False
+    for _ in range(total):
+        s.run(dt, 1)
+        u.run(dt, 1)
+        c = s.contacts()
+        met = met or len(c["i"]) > 0
+        for k in range(2):
+            dx = (s.pa.pos[k, 0] - u.pa.pos[k, 0]) % 4.0
+            assert min(dx, 4.0 - dx) <= 1e-8 and abs(s.pa.pos[k, 1] - u.pa.pos[k, 1]) <= 1e-8
+            assert 0.0 <= s.pa.pos[k, 0] <= 4.0
+    assert met
+    # the disks stopped against each other across the bound: gap closed, not crossed
+    gap = (s.pa.pos[0, 0] + 4.0 - s.pa.pos[1, 0]) - 0.5
+    assert abs(gap) <= 1e-9, gap
+
+
+def test_periodic_disks_invariants():
+    """Rows of disks crossing the periodic bound: every body stays in the box, a contact
+    across the bound has each closest point on its own body, and the x momentum (no
+    external x force, frictionless floor) is kept."""
+    pa, kw, dt, total = S.periodic_disks()
+    s = orc.OracleSolver(pa, **kw)
+    px0 = float(np.sum(s.pa.v[1:, 0] * s.pa.m[1:]))
+    across = 0
+    for _ in range(total):
+        before = s.pa.pos.copy()  # the step's contacts are those of the positions it starts from
+        s.run(dt, 1)
+        assert np.all(s.pa.pos[1:, 0] >= 0.0) and np.all(s.pa.pos[1:, 0] <= 4.0)
+        c = s.contacts()
+        for k in range(len(c["i"])):
+            i, j = int(c["i"][k]), int(c["j"][k])
+            if i == 0:
+                continue
+            if abs(before[i, 0] - before[j, 0]) > 2.0:
+                across += 1
+                # pi on body i; pj found on the copy of body j and moved back by the period,
+                # so on body j itself (the lever arm pj - x_j of the A matrix)
+                assert abs(np.linalg.norm(c["pi"][k, :2] - before[i, :2]) - 0.2) <= 1e-12
+                assert abs(np.linalg.norm(c["pj"][k, :2] - before[j, :2]) - 0.2) <= 1e-12
+        px = float(np.sum(s.pa.v[1:, 0] * s.pa.m[1:]))
+        assert abs(px - px0) <= 1e-7 * (1 + abs(px0)), (px, px0)
+    assert across > 0
+
+
+def test_periodic_obstacle_near_bound_fails():
+    """An obstacle within dmax of a periodic lower bound: the reference copies it and pairs it
+    with itself through the unimplemented plane-plane case; the oracle refuses the step."""
+    pa, kw, dt, _ = S.periodic_disks()
+    pa.pos[0, 0] = 0.1
+    s = orc.OracleSolver(pa, **kw)
+    with pytest.raises(RuntimeError):
+        s.run(dt, 1)
