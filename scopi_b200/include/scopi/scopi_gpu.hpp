@@ -251,6 +251,45 @@ class worm {
     std::size_t m_size;
 };
 
+// ------------------------------------------------------------------ box
+// BoxDomain<dim> (box.hpp): corners and periodic axes; ScopiSolver(box, particles) runs the
+// contact search with the copies across the periodic bounds and wraps the bodies after the move
+template <std::size_t dim>
+class BoxDomain {
+  public:
+    BoxDomain() {
+        m_min.fill(0.0);
+        m_max.fill(0.0);
+        m_periodic.fill(false);
+    }
+    BoxDomain(const std::array<double, dim>& min_corner, const std::array<double, dim>& max_corner)
+        : m_min(min_corner), m_max(max_corner) {
+        m_periodic.fill(false);
+    }
+    BoxDomain& with_periodicity() {
+        m_periodic.fill(true);
+        return *this;
+    }
+    BoxDomain& with_periodicity(std::size_t axis) {
+        m_periodic[axis] = true;
+        return *this;
+    }
+    BoxDomain& with_periodicity(const std::initializer_list<std::size_t>& axis) {
+        for (auto a : axis) m_periodic[a] = true;
+        return *this;
+    }
+    const std::array<bool, dim>& is_periodic() const { return m_periodic; }
+    bool is_periodic(std::size_t axis) const { return m_periodic[axis]; }
+    const std::array<double, dim>& min_corner() const { return m_min; }
+    const std::array<double, dim>& max_corner() const { return m_max; }
+    double lower_bound(std::size_t axis) const { return m_min[axis]; }
+    double upper_bound(std::size_t axis) const { return m_max[axis]; }
+
+  private:
+    std::array<double, dim> m_min, m_max;
+    std::array<bool, dim> m_periodic;
+};
+
 // ------------------------------------------------------------------ property
 template <std::size_t dim>
 class property {
@@ -987,6 +1026,7 @@ class ScopiSolver {
     using params_t = Params<ScopiSolver>;
 
     explicit ScopiSolver(scopi_container<dim>& particles) : m_particles(particles) {}
+    ScopiSolver(const BoxDomain<dim>& box, scopi_container<dim>& particles) : m_particles(particles), m_box(box) {}
     ~ScopiSolver() {
         if (m_h) scopi_gpu_destroy(m_h);
     }
@@ -1184,11 +1224,17 @@ class ScopiSolver {
             p.fixed_point_tol = m_default_property.fixed_point_tol;
             p.fixed_point_max_iter = (int64_t)m_default_property.fixed_point_max_iter;
         }
+        for (std::size_t d = 0; d < dim; ++d) {
+            p.box_lower[d] = m_box.lower_bound(d);
+            p.box_upper[d] = m_box.upper_bound(d);
+            p.periodic[d] = m_box.is_periodic(d) ? 1 : 0;
+        }
         const int32_t rc = scopi_gpu_create(&p, &m_h);
         if (rc < 0) throw gpu_error(std::string("scopi_gpu_create: ") + scopi_gpu_last_error(nullptr));
     }
 
     scopi_container<dim>& m_particles;
+    BoxDomain<dim> m_box;
     optim_solver_t m_optim;
     contact_property<problem_t> m_default_property;
     contact_params_t m_contact_params;

@@ -48,13 +48,14 @@ def test_cpp_api_matches_reference_golden(exe, golden, mode, name, tmp_path):
 
 
 WORM_SRC = os.path.join(ROOT, "tests", "cpp", "two_worms_dropin.cpp")
+PER_SRC = os.path.join(ROOT, "tests", "cpp", "periodic_dropin.cpp")
 SE_SRC = os.path.join(ROOT, "tests", "cpp", "superellipsoids_dropin.cpp")
 SE2_SRC = os.path.join(ROOT, "tests", "cpp", "two_ellipsoids_dropin.cpp")
 FP_SRC = os.path.join(ROOT, "tests", "cpp", "fixed_point_dropin.cpp")
 RS_SRC = os.path.join(ROOT, "tests", "cpp", "restart_dropin.cpp")
 
 
-@pytest.mark.parametrize("src", [SE_SRC, SE2_SRC, FP_SRC, RS_SRC, WORM_SRC])
+@pytest.mark.parametrize("src", [SE_SRC, SE2_SRC, FP_SRC, RS_SRC, WORM_SRC, PER_SRC])
 def test_superellipsoid_header_compiles(src):
     subprocess.run([GXX, "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", *INC, src], check=True)
 
@@ -359,3 +360,22 @@ def test_cpp_two_worms_match_reference_golden(method, tmp_path):
     for g, r in zip(got["contacts"], ref["contacts"]):
         assert abs(g["distance"] - r["distance"]) <= 1e-6
         assert max(abs(a - b) for a, b in zip(g["normal"], r["normal"])) <= 1e-6
+
+
+@pytest.mark.gpu
+def test_cpp_periodic_box_matches_oracle(tmp_path):
+    """ScopiSolver(BoxDomain, particles) through the C++ drop-in: the two disks meeting across
+    the periodic bound end where the oracle's do."""
+    import scenes as S
+    from gpu_helpers import oracle_solver
+    exe = str(tmp_path / "periodic")
+    lib = os.path.join(ROOT, "scopi_b200")
+    subprocess.run([GXX, "-O2", "-std=c++17", *INC, PER_SRC, "-L", lib, "-lscopi_gpu", f"-Wl,-rpath,{lib}", "-o", exe],
+                   check=True)
+    res = json.loads(subprocess.run([exe], check=True, capture_output=True, text=True, cwd=tmp_path).stdout)
+    pa, kw, dt, total = S.periodic_two_disks()
+    o = oracle_solver(pa, **kw).run(dt, total)
+    for k in range(2):
+        for d in range(2):
+            assert abs(res["positions"][k][d] - o.pa.pos[k, d]) <= 1e-8
+    assert res["contacts"] == 1
