@@ -452,3 +452,21 @@ def periodic_two_disks(unwrapped=False):
     if not unwrapped:
         kw.update(box_lower=(0.0, 0.0, 0.0), box_upper=(4.0, 0.0, 0.0), periodic=(1, 0, 0))
     return p.finalize(), kw, 0.01, 40
+
+
+def periodic_spheres_3d(problem=NOFRICTION):
+    """A 3D box periodic along x, [0, 2]: a 4 x 4 layer of spheres (r 0.2) on the floor plane
+    z = 0 (its position x = 1 away from the bound) sliding at (1, 0.3, 0) under gravity -z,
+    vap_fpd, dmax 0.3, dt 0.01, 100 steps."""
+    p = Particles(3)
+    p.add_plane((1.0, 0.5, 0.0), q=quaternion(PI / 2, (0, 1, 0)))
+    for i in range(4):
+        for j in range(4):
+            p.add_sphere((0.25 + 0.5 * i, 0.25 + 0.45 * j, 0.2), 0.2,
+                         Property(mass=1.0, moment_inertia=(0.016, 0.016, 0.016), velocity=(1.0, 0.3, 0.0),
+                                  force=(0.0, 0.0, -1.0)))
+    kw = dict(problem=problem, vap=VAP_FPD, dmax=0.3, tolerance=1e-9, max_ite=20000, alpha=0.1,
+              box_lower=(0.0, 0.0, 0.0), box_upper=(2.0, 0.0, 0.0), periodic=(1, 0, 0))
+    if problem == FRICTION:
+        kw["mu"] = 0.3
+    return p.finalize(), kw, 0.01, 100

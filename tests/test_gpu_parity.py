@@ -443,3 +443,23 @@ def test_periodic_obstacle_near_bound_rejected():
     pa.pos[0, 0] = 0.1
     with pytest.raises(ScopiGPUError):
         gpu_solver(pa, **kw).run(dt, 1)
+
+
+@pytest.mark.parametrize("problem", [S.NOFRICTION, S.FRICTION])
+def test_periodic_spheres_3d_match_oracle(problem):
+    """The 3D periodic box (one periodic axis, floor plane): the same contact list bit for bit
+    on the same input, the same pairs every step and the oracle's trajectory."""
+    pa, kw, dt, total = S.periodic_spheres_3d(problem)
+    g = gpu_solver(pa, **kw)
+    o = oracle_solver(pa, **kw)
+    same_contacts(g.detect(), o.detect())
+    across = 0
+    for k in range(total):
+        g.run(dt, 1)
+        o.run(dt, 1)
+        gc, oc = g.current_contacts(), o.contacts()
+        assert np.array_equal(gc["i"], oc["i"]) and np.array_equal(gc["j"], oc["j"]), k
+        across += int(np.sum(gc["i"] > gc["j"]))
+    assert across > 0
+    assert rel_err(g.particles.pos, o.pa.pos) <= 1e-9
+    assert np.all(g.particles.pos[1:, 0] >= 0.0) and np.all(g.particles.pos[1:, 0] <= 2.0)
