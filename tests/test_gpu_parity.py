@@ -406,7 +406,7 @@ def test_periodic_two_disks_on_gpu():
         assert np.all(np.minimum(dx, 4.0 - dx) <= 1e-8)
 
 
-@pytest.mark.parametrize("problem", [S.NOFRICTION, S.FRICTION])
+@pytest.mark.parametrize("problem", [S.NOFRICTION, S.FRICTION, S.VISCOUS])
 @pytest.mark.parametrize("method", [S.KDTREE, S.BRUTE_FORCE])
 def test_periodic_disks_match_oracle(problem, method):
     """Rows of disks crossing a periodic bound, GPU (FP64) against the oracle: on the same
@@ -423,6 +423,8 @@ def test_periodic_disks_match_oracle(problem, method):
         o.run(dt, 1)
         gc, oc = g.current_contacts(), o.contacts()
         assert np.array_equal(gc["i"], oc["i"]) and np.array_equal(gc["j"], oc["j"]), k
+        # viscous gamma carried over by the mapped (i, j), pairs across the bound included
+        assert np.max(np.abs(gc["gamma"] - oc["gamma"]), initial=0.0) <= 1e-7, k
         across += int(np.sum(gc["i"] > gc["j"]))
     assert across > 0
     assert rel_err(g.particles.pos, o.pa.pos) <= 1e-9
