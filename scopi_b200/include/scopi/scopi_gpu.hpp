@@ -35,6 +35,7 @@
 #include <filesystem>
 #include <fstream>
 #include <iterator>
+#include <memory>
 #include <utility>
 #include <initializer_list>
 #include <iostream>
@@ -229,6 +230,23 @@ class superellipsoid : public object_base<dim> {
 // worm<dim>(pos, q, radius, size), objects/types/worm.hpp:118-131: a chain of `size` spheres
 // of one radius; each sphere is a body of its own and the solver keeps consecutive spheres
 // in contact (add_contact.hpp:11-28)
+// read-only view of n contiguous doubles with the reference's element access ((d) and [d])
+template <std::size_t n>
+class const_view {
+  public:
+    explicit const_view(const double* p) : m_p(p) {}
+    double operator()(std::size_t d) const { return m_p[d]; }
+    double operator[](std::size_t d) const { return m_p[d]; }
+    operator std::array<double, n>() const {
+        std::array<double, n> o;
+        for (std::size_t d = 0; d < n; ++d) o[d] = m_p[d];
+        return o;
+    }
+
+  private:
+    const double* m_p;
+};
+
 template <std::size_t dim, bool owner = true>
 class worm {
   public:
@@ -239,8 +257,8 @@ class worm {
     }
     worm(std::vector<type::position_t<dim>> pos, double radius, std::size_t size)
         : worm(pos, std::vector<type::quaternion_t>(pos.size(), quaternion(0.0)), radius, size) {}
-    const type::position_t<dim>& pos(std::size_t i) const { return m_pos[i]; }
-    const type::quaternion_t& q(std::size_t i) const { return m_q[i]; }
+    const_view<dim> pos(std::size_t i) const { return const_view<dim>(m_pos[i].data()); }
+    const_view<4> q(std::size_t i) const { return const_view<4>(m_q[i].data()); }
     double radius() const { return m_radius; }
     std::size_t size() const { return m_size; }
 
@@ -643,6 +661,24 @@ class scopi_container {
     // bodies (the reference's size() counts objects: the two differ only with worms)
     std::size_t size() const { return m_shape.size(); }
     std::size_t nb_objects() const { return m_objects.size(); }
+
+    // object io as the reference's operator[] gives it (container.hpp:325-336): pos(i) and
+    // q(i) of its i-th body
+    class object_view {
+      public:
+        object_view(double* pos, double* q, std::size_t count) : m_pos(pos), m_q(q), m_count(count) {}
+        vec_ref<dim> pos(std::size_t i) const { return vec_ref<dim>(m_pos + 3 * i); }
+        vec_ref<4> q(std::size_t i) const { return vec_ref<4>(m_q + 4 * i); }
+        std::size_t size() const { return m_count; }
+
+      private:
+        double *m_pos, *m_q;
+        std::size_t m_count;
+    };
+    std::unique_ptr<object_view> operator[](std::size_t io) {
+        const auto& ob = m_objects.at(io);
+        return std::make_unique<object_view>(&m_pos[3 * ob.first], &m_q[4 * ob.first], ob.count);
+    }
 
   private:
     template <class Obj>

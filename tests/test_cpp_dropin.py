@@ -379,3 +379,13 @@ def test_cpp_periodic_box_matches_oracle(tmp_path):
         for d in range(2):
             assert abs(res["positions"][k][d] - o.pa.pos[k, d]) <= 1e-8
     assert res["contacts"] == 1
+
+
+def test_worm_container_like_reference(tmp_path):
+    """test/test_worm.cpp:26-478 (construction and indexing of 2D and 3D worms, alone and in a
+    container) on the drop-in's worm<dim> and scopi_container, without a GPU."""
+    exe = str(tmp_path / "wormc")
+    src = os.path.join(ROOT, "tests", "cpp", "worm_container.cpp")
+    subprocess.run([GXX, "-std=c++17", "-Wall", "-Werror", *INC, src, "-o", exe], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
