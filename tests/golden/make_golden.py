@@ -27,6 +27,10 @@ FILES = [
     "2d_case_spheres",              # test/test_sphere.cpp:423-484
     "obstacles_sphere_sphere_moving",  # test/test_obstacles.cpp:214-250
     "two_worms",                    # test/test_worm.cpp:480-530
+    # Friction with vap_fixed (test/test_friction.cpp, which the reference's test build leaves
+    # out); older output format, written before the motion of their step
+    "two_spheres_asymmetrical_friction",  # test/test_friction.cpp:17-53
+    "2d_case_spheres_friction",           # test/test_friction.cpp:55-112
     # superellipsoids (2D); these snapshots use an older output format (no velocities,
     # contacts without i, j and distance), written before the motion of their step
     "two_ellipsoids_symmetrical",           # test/test_superellipsoid.cpp:451-491
@@ -47,7 +51,7 @@ def main():
         for o in d["objects"]:
             if "properties" not in o:  # older format: geometry only
                 objs.append({"type": o["type"], "position": o["position"], "quaternion": o["quaternion"],
-                             "radius": o["radius"], "squareness": o["squareness"]})
+                             "radius": o["radius"], "squareness": o.get("squareness")})
                 continue
             p = o["properties"]
             om = p["omega"]

@@ -108,10 +108,10 @@ def two_spheres(symmetric: bool, contact_method=KDTREE):
     return p.finalize(), dict(vap=VAP_FIXED, contact_method=contact_method), 0.005, 1000
 
 
-def critical_2d_spheres(contact_method=KDTREE):
-    """test/test_sphere.cpp:423-484: 18 disks from std::minstd_rand0(123), dt 0.01, 20 steps."""
-    n = 3
-    g = MinstdRand0(123)
+def critical_2d_spheres(contact_method=KDTREE, n=3, seed=123):
+    """test/test_sphere.cpp:423-484: 18 disks from std::minstd_rand0(123), dt 0.01, 20 steps
+    (n = 2, seed 0: the 8 disks of test/test_friction.cpp:55-112)."""
+    g = MinstdRand0(seed)
     p = Particles(2)
     for i in range(n):
         for j in range(n):
@@ -470,3 +470,20 @@ def periodic_spheres_3d(problem=NOFRICTION):
     if problem == FRICTION:
         kw["mu"] = 0.3
     return p.finalize(), kw, 0.01, 100
+
+
+def two_spheres_friction(contact_method=KDTREE):
+    """test/test_friction.cpp:17-53: two disks (r 0.1) pushed into each other off-centre by
+    vap_fixed at (0.25, 0) and (-0.25, 0), Friction mu 0.5, default solver, dt 0.005; the
+    reference's snapshot is the state after 999 steps."""
+    p = Particles(2)
+    p.add_sphere((-0.2, -0.05), 0.1, Property(mass=1.0, moment_inertia=0.1, desired_velocity=(0.25, 0.0)))
+    p.add_sphere((0.2, 0.05), 0.1, Property(mass=1.0, moment_inertia=0.1, desired_velocity=(-0.25, 0.0)))
+    return p.finalize(), dict(problem=FRICTION, vap=VAP_FIXED, contact_method=contact_method, mu=0.5), 0.005, 999
+
+
+def critical_2d_spheres_friction(contact_method=KDTREE):
+    """test/test_friction.cpp:55-112: the critical 2D disks (n = 2, std::minstd_rand0(0)),
+    Friction mu 0.5, vap_fixed, dt 0.01; the reference's snapshot is the state after 99 steps."""
+    pa, _, dt, _ = critical_2d_spheres(contact_method, n=2, seed=0)
+    return pa, dict(problem=FRICTION, vap=VAP_FIXED, contact_method=contact_method, mu=0.5), dt, 99

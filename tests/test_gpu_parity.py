@@ -465,3 +465,14 @@ def test_periodic_spheres_3d_match_oracle(problem):
     assert across > 0
     assert rel_err(g.particles.pos, o.pa.pos) <= 1e-9
     assert np.all(g.particles.pos[1:, 0] >= 0.0) and np.all(g.particles.pos[1:, 0] <= 2.0)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("name", ["two_spheres_asymmetrical_friction", "2d_case_spheres_friction"])
+def test_friction_goldens_on_gpu(golden, name, precision):
+    """test/test_friction.cpp:17-112 on the GPU (the Friction rows of the 6-dof kernel), FP64
+    and mixed, against the reference's snapshots (tol 1e-6)."""
+    from test_oracle_golden import compare_positions
+    pa, kw, dt, total = S.two_spheres_friction() if name.startswith("two") else S.critical_2d_spheres_friction()
+    g = gpu_solver(pa, precision=precision, **kw).run(dt, total)
+    compare_positions(g.particles, golden[name]["objects"], 2, 1e-6)

@@ -356,3 +356,22 @@ def test_periodic_obstacle_near_bound_fails():
     s = orc.OracleSolver(pa, **kw)
     with pytest.raises(RuntimeError):
         s.run(dt, 1)
+
+
+def compare_positions(state, gold_objs, dim, tol):
+    """Older snapshots hold no properties: positions and quaternions (test/utils.cpp:14-75)."""
+    worst = 0.0
+    for k, o in enumerate(gold_objs):
+        worst = max(worst, max(abs(state.pos[k, d] - o["position"][d]) for d in range(dim)))
+        worst = max(worst, max(abs(state.q[k, d] - o["quaternion"][d]) for d in range(4)))
+    assert worst <= tol, f"max abs deviation {worst:.3e} > {tol}"
+    return worst
+
+
+@pytest.mark.parametrize("method", [S.KDTREE, S.BRUTE_FORCE])
+@pytest.mark.parametrize("name", ["two_spheres_asymmetrical_friction", "2d_case_spheres_friction"])
+def test_friction_goldens(golden, name, method):
+    """test/test_friction.cpp:17-112 against their snapshots (tol 1e-6)."""
+    scene = S.two_spheres_friction(method) if name.startswith("two") else S.critical_2d_spheres_friction(method)
+    s = run_oracle(scene)
+    compare_positions(s.pa, golden[name]["objects"], 2, 1e-6)
