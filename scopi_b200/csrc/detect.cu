@@ -1217,6 +1217,7 @@ void launch_append_links(int C, int W, const int* links, Contacts& c, Sizes* siz
 void launch_ghost_flags(const Bodies& b, const PeriodicBox& box, double dmax, int dim, GhostBodies& g, int* total,
                         int* scan_work, cudaStream_t s) {
     const long long m = (long long)dim * (b.n - b.nin);
+    cudaMemsetAsync(total, 0, sizeof(int), s);  // an empty scan (no active body) leaves it alone
     k_ghost_flags<<<blocks_for(m + 1), kThreads, 0, s>>>(b, box, dmax, dim, g.flag);
     LAUNCHED(1);
     scan_exclusive(g.flag, g.rank, nullptr, (int)m, m, total, scan_work, s, &g_detect_launches);
