@@ -389,3 +389,12 @@ def test_worm_container_like_reference(tmp_path):
     subprocess.run([GXX, "-std=c++17", "-Wall", "-Werror", *INC, src, "-o", exe], check=True)
     r = subprocess.run([exe], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_box_domain_api(tmp_path):
+    """BoxDomain<dim> (box.hpp): corners, periodic axes and accessors, without a GPU."""
+    exe = str(tmp_path / "box")
+    src = os.path.join(ROOT, "tests", "cpp", "box_domain.cpp")
+    subprocess.run([GXX, "-std=c++17", "-Wall", "-Werror", *INC, src, "-o", exe], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
