@@ -71,3 +71,49 @@ def test_solver_raises_without_library(tmp_path):
             _abi.load(str(tmp_path / "missing.so"))
         finally:
             _abi._lib = saved
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """The ctypes mirrors of scopi_gpu_params / _particles / _stats have the C layout (size and
+    the offsets of the fields added last), checked against the header compiled by gcc."""
+    import ctypes as C
+    import subprocess
+    from scopi_b200 import _abi
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "scopi_gpu.h"\n'
+                   'int main(void) { printf("%zu %zu %zu %zu %zu %zu %zu\\n", sizeof(scopi_gpu_params), '
+                   'offsetof(scopi_gpu_params, fixed_point_tol), offsetof(scopi_gpu_params, box_lower), '
+                   'offsetof(scopi_gpu_params, periodic), sizeof(scopi_gpu_particles), '
+                   'offsetof(scopi_gpu_particles, worm), sizeof(scopi_gpu_stats)); return 0; }\n')
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    want = [C.sizeof(_abi.Params), _abi.Params.fixed_point_tol.offset, _abi.Params.box_lower.offset,
+            _abi.Params.periodic.offset, C.sizeof(_abi.ParticlesC), _abi.ParticlesC.worm.offset, C.sizeof(_abi.Stats)]
+    assert got == want
+
+
+def test_default_params_have_no_box(lib):
+    import ctypes as C
+    from scopi_b200 import _abi
+    from scopi_b200.solver import _set_param
+    p = _abi.Params()
+    lib.scopi_gpu_default_params(C.byref(p), 3)
+    assert list(p.periodic) == [0, 0, 0] and list(p.box_lower) == [0.0] * 3
+    assert (p.fixed_point_tol, p.fixed_point_max_iter) == (1e-6, 1000)
+    _set_param(p, "box_upper", (4.0, 2.0))
+    _set_param(p, "periodic", (1, 0))
+    assert list(p.box_upper) == [4.0, 2.0, 0.0] and list(p.periodic) == [1, 0, 0]
+
+
+def test_worm_indices_in_the_container():
+    from scopi_b200.container import Particles, Property
+    p = Particles(2)
+    p.add_sphere((0.0, 5.0), 0.5, Property())
+    p.add_worm([(1.0, 0.0), (3.0, 0.0), (5.0, 0.0)], 1.0, Property(desired_velocity=(1.0, 0.0)))
+    p.add_worm([(1.0, 3.0), (3.0, 3.0)], 1.0, Property())
+    pa = p.finalize()
+    assert pa.worm.dtype.name == "int32" and pa.worm.tolist() == [-1, 0, 0, 0, 1, 1]
+    assert pa.radius.tolist() == [0.5, 1.0, 1.0, 1.0, 1.0, 1.0]
+    assert pa.vd[1:4, 0].tolist() == [1.0, 1.0, 1.0]
+    assert pa.copy().worm.tolist() == pa.worm.tolist()
