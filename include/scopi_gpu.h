@@ -103,6 +103,12 @@ typedef struct scopi_gpu_params {
                                      beyond a bound is wrapped (utils.hpp:229-257, base.hpp:118-137,
                                      solver.hpp:482-522).  Scenes of spheres (planes and segments as
                                      static obstacles away from the periodic lower bounds) */
+    int32_t barrier_timeout_us;   /* limit of every wait on a grid barrier inside a persistent APGD
+                                     launch, in microseconds (0: 20 s).  A block that waits longer
+                                     sets an error word and every block returns; the step then
+                                     fails with SCOPI_GPU_ETIMEOUT and the handle stays usable.
+                                     Infrastructure of this library: the reference solves on the
+                                     host and has no device waits. */
 } scopi_gpu_params;
 
 /* First APGD step of every solve.  REFERENCE: alpha as given (apgd.hpp:120, the
@@ -250,13 +256,24 @@ int32_t scopi_gpu_batch_set_block_threads(scopi_gpu_handle* h, int32_t threads);
    n.(d n + dt A U)), inv_mass (n_active, 1/m), inc_ptr/inc_idx (per active body, its
    contacts sorted by index, entry = contact | (1u<<31) when the body is the contact's j).
    Outputs: lambda (n_contacts), u (n_active*3, M^-1 B^T lambda; may be NULL).
+   The lists are checked on the device before the solve reads them (one read-back):
+   inc_ptr must start at 0, never decrease and end at most at 2 * n_contacts, every
+   inc_idx entry must name a contact < n_contacts and ci/cj must be < nb_inactive +
+   n_active; otherwise SCOPI_GPU_EINVAL with the reason in scopi_gpu_last_error(NULL).
    Returns SCOPI_GPU_OK, SCOPI_GPU_ENOCONV (max_ite reached) or an error; the call
-   synchronises `stream` (a cudaStream_t, NULL = legacy default stream). */
+   synchronises `stream` (a cudaStream_t, NULL = legacy default stream) before it returns. */
 int32_t scopi_gpu_apgd_noalloc(int32_t dim, int64_t n_active, int64_t nb_inactive, int64_t n_contacts,
                                const int32_t* ci, const int32_t* cj, const double* normal, const double* c,
                                const double* inv_mass, const int32_t* inc_ptr, const int32_t* inc_idx, double dt,
                                double alpha, double tolerance, int64_t max_ite, int32_t dynamic_descent,
                                double* lambda, double* u, int64_t* iterations, void* stream);
+
+/* Test of the barrier limit (no counterpart in the reference): block 0 of the next persistent
+   APGD launch of this handle does not count its first grid-barrier arrival, so that barrier
+   never completes; every block gives up after barrier_timeout_us and the step returns
+   SCOPI_GPU_ETIMEOUT.  One shot: later launches are not affected.  Single-scene handles
+   only (a batch's launch has no grid barrier: SCOPI_GPU_EINVAL). */
+int32_t scopi_gpu_test_barrier_stall(scopi_gpu_handle* h);
 
 /* The handle's CUDA stream (a cudaStream_t), so callers can order their own work and
    time the engine with CUDA events recorded on the stream its kernels run on.

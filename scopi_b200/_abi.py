@@ -23,7 +23,7 @@ EXPORTED = [
     "scopi_gpu_get_lambda", "scopi_gpu_get_stats", "scopi_gpu_amat", "scopi_gpu_atmat",
     "scopi_gpu_last_error", "scopi_gpu_kernel_launches", "scopi_gpu_get_stream", "scopi_gpu_apgd_noalloc",
     "scopi_gpu_batch_create", "scopi_gpu_batch_get_scene", "scopi_gpu_batch_get_scene_stats",
-    "scopi_gpu_batch_block_threads", "scopi_gpu_batch_set_block_threads",
+    "scopi_gpu_batch_block_threads", "scopi_gpu_batch_set_block_threads", "scopi_gpu_test_barrier_stall",
 ]
 
 
@@ -36,6 +36,7 @@ class Params(C.Structure):
         ("mixed_violation_tol", C.c_double), ("mixed_max_corrections", C.c_int32), ("device", C.c_int32),
         ("initial_step", C.c_int32), ("fixed_point_tol", C.c_double), ("fixed_point_max_iter", C.c_int64),
         ("box_lower", C.c_double * 3), ("box_upper", C.c_double * 3), ("periodic", C.c_int32 * 3),
+        ("barrier_timeout_us", C.c_int32),
     ]
 
 
@@ -113,6 +114,8 @@ def load(path: str = LIB_PATH):
     L.scopi_gpu_batch_block_threads.restype = C.c_int32
     L.scopi_gpu_batch_set_block_threads.argtypes = [H, C.c_int32]
     L.scopi_gpu_batch_set_block_threads.restype = C.c_int32
+    L.scopi_gpu_test_barrier_stall.argtypes = [H]
+    L.scopi_gpu_test_barrier_stall.restype = C.c_int32
     for name in ("scopi_gpu_create", "scopi_gpu_destroy", "scopi_gpu_set_particles", "scopi_gpu_get_particles",
                  "scopi_gpu_run", "scopi_gpu_detect", "scopi_gpu_get_contacts", "scopi_gpu_get_lambda",
                  "scopi_gpu_get_stats", "scopi_gpu_amat", "scopi_gpu_atmat"):

@@ -30,46 +30,8 @@ namespace {
 
 constexpr int kApgdThreads = 256;
 constexpr int kPartials = 9;  // s1..s8 and the FP32 curvature term
-constexpr unsigned long long kBarrierTimeoutNs = 20ull * 1000ull * 1000ull * 1000ull;
-
-__device__ __forceinline__ unsigned long long global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-// bar[0] = arrivals, bar[1] = generation, bar[2] = error flag
-__device__ bool grid_barrier(unsigned int* bar, unsigned int nblocks) {
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile unsigned int* vgen = bar + 1;
-        volatile unsigned int* verr = bar + 2;
-        const unsigned int gen = *vgen;
-        __threadfence();
-        const unsigned int arrived = atomicAdd(bar, 1u);
-        if (arrived == nblocks - 1) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            const unsigned long long t0 = global_ns();
-            unsigned int it = 0;
-            while (*vgen == gen) {
-                if (*verr) break;
-                if (((++it) & 1023u) == 0 && global_ns() - t0 > kBarrierTimeoutNs) {
-                    atomicExch(bar + 2, 1u);
-                    break;
-                }
-                __nanosleep(20);
-            }
-        }
-        __threadfence();
-        s_ok = (*verr == 0u);
-    }
-    __syncthreads();
-    return s_ok != 0;
-}
+// bounded grid barrier with a runtime limit (bar[3]) shared with the torque-free kernel
+using apgdc::grid_barrier;
 
 template <typename T>
 struct Vec6 {
@@ -237,6 +199,7 @@ struct ApgdArgs {
     long long max_ite;
     int dynamic;
     int curvature_start;
+    int stall;  // block 0 skips its first barrier arrival (test of the barrier limit)
 };
 
 template <typename T, int DIM, int PROB>
@@ -521,6 +484,7 @@ __global__ void __launch_bounds__(kApgdThreads) k_apgd(ApgdArgs<T> A) {
     int conv = 0, err = 0;
     int parity = 0;
     double last_step = 0.0;
+    bool withhold = A.stall != 0 && blockIdx.x == 0;
     if (A.curvature_start) {
         // initial step from the curvature along the first projected-gradient direction d of
         // the cold start (stored in the candidate buffers, which the first iteration
@@ -565,7 +529,8 @@ __global__ void __launch_bounds__(kApgdThreads) k_apgd(ApgdArgs<T> A) {
                 }
             }
         }
-        bool ok = grid_barrier(A.bar, nb);
+        bool ok = grid_barrier(A.bar, nb, withhold);
+        withhold = false;
         if (ok) particle_pass<T, DIM, PROB>(A, dbuf, ub[jn], ub[jl], ub[jp], (T)0, false, false, s);
         block_sum(s);
         double* part = A.partials;
@@ -591,7 +556,9 @@ __global__ void __launch_bounds__(kApgdThreads) k_apgd(ApgdArgs<T> A) {
         if (err) break;
         double s[kPartials] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
         contact_pass<T, DIM, PROB>(A, C, lamb[il], lamb[ip], lamb[in_], ub[jl], ub[jp], (T)beta, use_prev, bt, alpha, s);
-        if (!grid_barrier(A.bar, nb)) { err = 1; break; }
+        const bool wh = withhold;
+        withhold = false;
+        if (!grid_barrier(A.bar, nb, wh)) { err = 1; break; }
         particle_pass<T, DIM, PROB>(A, lamb[in_], ub[jn], ub[jl], ub[jp], (T)beta, use_prev, sizeof(T) == 4, s);
         block_sum(s);
         double* part = A.partials + (size_t)parity * nb * kPartials;
@@ -981,6 +948,7 @@ cudaError_t launch_apgd_invm(const Bodies& b, const StepParams& p, const ApgdSet
     A.dt2 = st.dt * st.dt;
     A.mu = st.mu;
     A.curvature_start = st.curvature_start;
+    A.stall = st.stall;
     A.max_ite = st.max_ite;
     A.dynamic = st.dynamic;
 #define LA(D, P) \

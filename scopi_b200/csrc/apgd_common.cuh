@@ -17,11 +17,20 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
-// Grid-wide barrier for a cooperative launch.  bar[0] = arrivals, bar[1] = generation,
-// bar[2] = error flag.  A block that waits longer than kBarrierTimeoutNs sets the flag and
-// returns false; every waiting block sees the flag and returns false too, so the kernel
-// ends with an error status instead of hanging.
-__device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int nblocks) {
+// Barrier words of a persistent launch (the host writes all four before the launch):
+// bar[0] = arrivals, bar[1] = generation, bar[2] = error flag, bar[3] = wait limit in
+// microseconds (0: kBarrierTimeoutNs).
+__device__ __forceinline__ unsigned long long barrier_limit_ns(const unsigned int* bar) {
+    const unsigned int us = *(volatile const unsigned int*)(bar + 3);
+    return us ? (unsigned long long)us * 1000ull : kBarrierTimeoutNs;
+}
+
+// Grid-wide barrier for a cooperative launch.  A block that waits longer than the limit
+// sets the error flag and returns false; every waiting block sees the flag and returns
+// false too, so the kernel ends with an error status instead of hanging.  withhold: this
+// block does not count itself (used once, to test that path: the barrier then never
+// completes and every block gives up after the limit).
+__device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int nblocks, bool withhold = false) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -29,17 +38,17 @@ __device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int nbl
         volatile unsigned int* verr = bar + 2;
         const unsigned int gen = *vgen;
         __threadfence();
-        const unsigned int arrived = atomicAdd(bar, 1u);
-        if (arrived == nblocks - 1) {
+        const unsigned int arrived = withhold ? 0u : atomicAdd(bar, 1u);
+        if (!withhold && arrived == nblocks - 1) {
             atomicExch(bar, 0u);
             __threadfence();
             atomicAdd(bar + 1, 1u);
         } else {
-            const unsigned long long t0 = global_ns();
+            const unsigned long long t0 = global_ns(), limit = barrier_limit_ns(bar);
             unsigned int it = 0;
             while (*vgen == gen) {
                 if (*verr) break;
-                if (((++it) & 1023u) == 0 && global_ns() - t0 > kBarrierTimeoutNs) {
+                if (((++it) & 1023u) == 0 && global_ns() - t0 > limit) {
                     atomicExch(bar + 2, 1u);
                     break;
                 }
@@ -57,7 +66,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int nbl
 // it).  bar[0] counts arrivals and only grows: it is a multiple of nblocks between
 // barriers (the host zeroes it before the launch), so an arrival's target is the next
 // multiple.  One atomic per block, then acquire loads.  A thread that waits longer than
-// kBarrierTimeoutNs sets the error flag bar[2]; every waiter sees the flag and returns
+// the limit (bar[3]) sets the error flag bar[2]; every waiter sees the flag and returns
 // false, so the kernel ends with an error status instead of hanging.  Blocks must not mix
 // it with grid_barrier after their first call (grid_barrier resets bar[0]).
 __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
@@ -67,13 +76,16 @@ __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
 }
 // Split form: grid_arrive publishes this block's writes and returns the arrival target;
 // the block may do independent work before grid_wait.
-__device__ __forceinline__ unsigned int grid_arrive(unsigned int* bar, unsigned int nblocks) {
+// withhold: compute the target without counting this block (the timeout test: the
+// barrier never completes and every waiter gives up after the limit).
+__device__ __forceinline__ unsigned int grid_arrive(unsigned int* bar, unsigned int nblocks, bool withhold = false) {
     __threadfence();
-    const unsigned int old = atomicAdd(bar, 1u);
+    const unsigned int old = withhold ? ld_acquire_u32(bar) : atomicAdd(bar, 1u);
     return (old / nblocks + 1u) * nblocks;
 }
 __device__ __forceinline__ bool grid_wait(unsigned int* bar, unsigned int target) {
     volatile unsigned int* verr = bar + 2;
+    const unsigned long long limit = barrier_limit_ns(bar);
     unsigned int it = 0;
     unsigned long long t0 = 0;
     for (;;) {
@@ -83,7 +95,7 @@ __device__ __forceinline__ bool grid_wait(unsigned int* bar, unsigned int target
             const unsigned long long t = global_ns();
             if (t0 == 0) {
                 t0 = t;
-            } else if (t - t0 > kBarrierTimeoutNs) {
+            } else if (t - t0 > limit) {
                 atomicExch(bar + 2, 1u);
                 return false;
             }

@@ -102,6 +102,7 @@ struct SphArgs {
     long long max_ite;
     int dynamic;
     int curvature_start;
+    int stall;  // block 0 skips its first barrier arrival (test of the barrier limit)
 };
 
 template <typename T>
@@ -245,6 +246,7 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
         cp_commit();
     };
     bool geom_issued = false;
+    bool withhold = A.stall != 0 && blockIdx.x == 0;
     if (A.curvature_start) {
         // initial step from the curvature along the first descent direction d (stored in
         // the candidate buffer, which the first contact pass overwrites); partial-sum
@@ -267,7 +269,8 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
         }
         block_sum<2>(a2);
         if (threadIdx.x == 0) A.partials[(size_t)1 * nb * 8 + blockIdx.x * 8] = a2[0];
-        bool ok = grid_barrier(A.bar, nb);
+        bool ok = grid_barrier(A.bar, nb, withhold);
+        withhold = false;
         double wm[2] = {0.0, 0.0};
         if (ok) GRID_STRIDE(p, A.na) {
             T w0 = 0, w1 = 0, w2 = 0;
@@ -393,8 +396,9 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
             unsigned int target = 0;
             if (tid == 0) {
                 for (int k = 0; k < 8; ++k) part[blockIdx.x * 8 + k] = s[k];
-                target = grid_arrive(A.bar, nb);
+                target = grid_arrive(A.bar, nb, withhold);
             }
+            withhold = false;
             // every thread is past its contact loop: the particle pass's first stages fill
             // the shared memory while the barrier waits (u(l) copied whatever beta is)
             {
@@ -616,9 +620,11 @@ __device__ __forceinline__ float idx_bits<float>(int c) { return __int_as_float(
 template <>
 __device__ __forceinline__ double idx_bits<double>(int c) { return __longlong_as_double((long long)c); }
 
+// cap: the records `inc` holds; a list longer than that is cut (the no-allocation entry
+// point rejects such lists before this runs; the engine sizes `inc` for every list)
 template <typename T>
-__global__ void k_pack_inc(int na, const int* ptr, const int* idx, const double* bn, V4<T>* inc) {
-    const int tot = ptr[na];
+__global__ void k_pack_inc(int na, const int* ptr, const int* idx, const double* bn, V4<T>* inc, long long cap) {
+    const long long tot = ptr[na] < cap ? (long long)ptr[na] : cap;
     GRID_STRIDE(k, tot) {
         const unsigned e = (unsigned)idx[k];
         const int c = (int)(e & 0x7fffffffu);
@@ -767,6 +773,7 @@ cudaError_t launch_apgd_sph(int nin, int na, int dim, int problem, const ApgdSet
     A.max_ite = st.max_ite;
     A.dynamic = st.dynamic;
     A.curvature_start = st.curvature_start;
+    A.stall = st.stall;
 #define LA(D, P) \
     if (dim == D && problem == P) return launch_t<T, D, P>(A, nblocks, s);
     LA(2, 0) LA(2, 2) LA(3, 0) LA(3, 2)
@@ -794,7 +801,7 @@ template <typename T>
 void launch_pack_inc(int na, const int* ptr, const int* idx, const double* bn, V4<T>* inc, long long inc_cap,
                      cudaStream_t s) {
     if (na <= 0) return;
-    k_pack_inc<T><<<blocks(inc_cap), 256, 0, s>>>(na, ptr, idx, bn, inc);
+    k_pack_inc<T><<<blocks(inc_cap), 256, 0, s>>>(na, ptr, idx, bn, inc, inc_cap);
     g_sph_launches += 1;
 }
 template void launch_pack_inc<double>(int, const int*, const int*, const double*, dvec4*, long long, cudaStream_t);
@@ -857,7 +864,8 @@ constexpr size_t kOffPart = align_up(kOffU + sizeof(dvec4) * 4 * kNoAllocMaxBodi
 constexpr size_t kOffBar = align_up(kOffPart + sizeof(double) * 4 * kNoAllocMaxBlocks * 8);
 constexpr size_t kOffRes = align_up(kOffBar + 4 * sizeof(unsigned int));
 constexpr size_t kOffSizes = align_up(kOffRes + sizeof(ApgdResult));
-constexpr size_t kNoAllocBytes = align_up(kOffSizes + sizeof(Sizes));
+constexpr size_t kOffFlag = align_up(kOffSizes + sizeof(Sizes));
+constexpr size_t kNoAllocBytes = align_up(kOffFlag + sizeof(unsigned int));
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
@@ -880,6 +888,31 @@ cudaError_t noalloc_scratch(unsigned char** out) {
     }
     *out = g_noalloc_dev[dev];
     return cudaSuccess;
+}
+
+// The caller's contact list and incidence lists, checked before the solve reads them so that
+// no index leaves its array: bit 1 inc_ptr does not start at 0 or decreases, bit 2
+// inc_ptr[na] > 2 C (more records than the fixed array holds), bit 4 a record names a
+// contact >= C, bit 8 a contact names a body outside [0, nb_inactive + n_active).
+constexpr unsigned kBadPtr = 1u, kBadTotal = 2u, kBadRecord = 4u, kBadBody = 8u;
+__global__ void k_noalloc_check(int na, int nbody, int C, const int* ci, const int* cj, const int* ptr, const int* idx,
+                                unsigned* flag) {
+    const int tot = ptr[na];
+    const bool tot_ok = tot >= 0 && tot <= 2 * C;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (ptr[0] != 0) atomicOr(flag, kBadPtr);
+        if (!tot_ok) atomicOr(flag, kBadTotal);
+    }
+    GRID_STRIDE(p, na) {
+        if (ptr[p] > ptr[p + 1]) atomicOr(flag, kBadPtr);
+    }
+    if (tot_ok) GRID_STRIDE(k, tot) {
+            if ((long long)((unsigned)idx[k] & 0x7fffffffu) >= (long long)C) atomicOr(flag, kBadRecord);
+        }
+    GRID_STRIDE(c, C) {
+        const int a = ci[c], b = cj[c];
+        if (a < 0 || a >= nbody || b < 0 || b >= nbody) atomicOr(flag, kBadBody);
+    }
 }
 
 __global__ void k_noalloc_prepare(Sizes* sizes, int C, int na, const double* inv_mass, double* invm) {
@@ -935,6 +968,10 @@ extern "C" int32_t scopi_gpu_apgd_noalloc(int32_t dim, int64_t n_active, int64_t
                          "8192 active bodies)");
         return SCOPI_GPU_EINVAL;
     }
+    if (nb_inactive > 0x7fffffffLL - n_active) {
+        set_global_error("scopi_gpu_apgd_noalloc: nb_inactive + n_active must fit in a 32-bit index");
+        return SCOPI_GPU_EINVAL;
+    }
     if (n_contacts > 0 && (!ci || !cj || !normal || !c || !inv_mass || !inc_ptr || !inc_idx || !lambda)) {
         set_global_error("scopi_gpu_apgd_noalloc: null array");
         return SCOPI_GPU_EINVAL;
@@ -972,12 +1009,51 @@ extern "C" int32_t scopi_gpu_apgd_noalloc(int32_t dim, int64_t n_active, int64_t
     unsigned int* bar = reinterpret_cast<unsigned int*>(base + kOffBar);
     ApgdResult* res = reinterpret_cast<ApgdResult*>(base + kOffRes);
     Sizes* sizes = reinterpret_cast<Sizes*>(base + kOffSizes);
+    unsigned* flag = reinterpret_cast<unsigned*>(base + kOffFlag);
+    // the caller's lists are checked first (one read-back): nothing below indexes with them
+    // before they are known to stay inside their arrays
+    e = cudaMemsetAsync(flag, 0, sizeof(unsigned), s);
+    if (e != cudaSuccess) {
+        set_global_error2("scopi_gpu_apgd_noalloc: cudaMemsetAsync: ", cudaGetErrorString(e));
+        return SCOPI_GPU_ECUDA;
+    }
+    k_noalloc_check<<<blocks(std::max(C, na + 1)), 256, 0, s>>>(na, (int)(nb_inactive + n_active), C, ci, cj,
+                                                                inc_ptr, inc_idx, flag);
+    unsigned host_flag = 0;
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&host_flag, flag, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        set_global_error2("scopi_gpu_apgd_noalloc: input check: ", cudaGetErrorString(e));
+        return SCOPI_GPU_ECUDA;
+    }
+    if (host_flag) {
+        set_global_error((host_flag & kBadTotal)
+                             ? "scopi_gpu_apgd_noalloc: inc_ptr[n_active] exceeds 2 * n_contacts"
+                             : (host_flag & kBadPtr)
+                                   ? "scopi_gpu_apgd_noalloc: inc_ptr must start at 0 and never decrease"
+                                   : (host_flag & kBadRecord)
+                                         ? "scopi_gpu_apgd_noalloc: inc_idx names a contact >= n_contacts"
+                                         : "scopi_gpu_apgd_noalloc: ci/cj must be < nb_inactive + n_active");
+        return SCOPI_GPU_EINVAL;
+    }
     // the array keeps the previous call's contents: clear what the solve reads before writing
-    cudaMemsetAsync(lam, 0, 2 * sizeof(double) * kNoAllocMaxContacts, s);     // lambda, lambda_prev
-    cudaMemsetAsync(ub, 0, sizeof(dvec4) * kNoAllocMaxBodies, s);             // u(lambda)
-    cudaMemsetAsync(ub + 2 * kNoAllocMaxBodies, 0, sizeof(dvec4) * kNoAllocMaxBodies, s);  // u(y)
-    cudaMemsetAsync(bar, 0, 4 * sizeof(unsigned int), s);
-    cudaMemsetAsync(res, 0, sizeof(ApgdResult), s);
+    // (lambda and lambda_prev, u(lambda), u(y), the barrier words, the result)
+    struct Clear {
+        void* p;
+        size_t n;
+    } clears[] = {{lam, 2 * sizeof(double) * kNoAllocMaxContacts},
+                  {ub, sizeof(dvec4) * kNoAllocMaxBodies},
+                  {ub + 2 * kNoAllocMaxBodies, sizeof(dvec4) * kNoAllocMaxBodies},
+                  {bar, 4 * sizeof(unsigned int)},
+                  {res, sizeof(ApgdResult)}};
+    for (const Clear& cl : clears) {
+        e = cudaMemsetAsync(cl.p, 0, cl.n, s);
+        if (e != cudaSuccess) {
+            set_global_error2("scopi_gpu_apgd_noalloc: cudaMemsetAsync: ", cudaGetErrorString(e));
+            return SCOPI_GPU_ECUDA;
+        }
+    }
     k_noalloc_prepare<<<blocks(na), 256, 0, s>>>(sizes, C, na, inv_mass, invm);
     launch_pack_cij(ci, cj, cij, sizes, C, s);
     k_noalloc_pack_nc<<<blocks(C), 256, 0, s>>>(normal, c, nc, C);
@@ -1009,6 +1085,7 @@ extern "C" int32_t scopi_gpu_apgd_noalloc(int32_t dim, int64_t n_active, int64_t
     A.max_ite = max_ite;
     A.dynamic = dynamic_descent ? 1 : 0;
     A.curvature_start = 0;
+    A.stall = 0;
     int maxb = apgd_sph_max_blocks(kNoFriction, dim, false);
     if (maxb > kNoAllocMaxBlocks) maxb = kNoAllocMaxBlocks;
     const int thr = SphOcc<double>::threads;

@@ -164,6 +164,7 @@ struct ApgdSettings {
     double dt;
     double mu;
     int curvature_start;      // first step from the curvature estimate instead of alpha
+    int stall;                // test of the barrier limit: block 0 skips its first arrival
 };
 
 struct ApgdResult {           // written by block 0 of the persistent kernel

@@ -116,6 +116,8 @@ struct scopi_gpu_handle {
     Sizes* h_sizes = nullptr;          // pinned
     ApgdResult* h_result = nullptr;    // pinned
     unsigned long long* h_viol = nullptr;
+    unsigned int* h_bar = nullptr;     // pinned: the four barrier words written before a launch
+    bool stall_next = false;           // scopi_gpu_test_barrier_stall: withhold one arrival once
     int max_blocks64 = 0, max_blocks32 = 0, max_sph64 = 0, max_sph32 = 0;
     // FrictionFixedPoint: P.problem holds FRICTION (the kernels' problem), this flag the loop
     // (ViscousFriction keeps its own problem code and runs the same loop)
@@ -467,6 +469,10 @@ struct scopi_gpu_handle {
         cudaMemset(d_sizes_cur, 0, sizeof(Sizes));
         cudaMemset(d_sizes_old, 0, sizeof(Sizes));
         cudaMemset(d_barrier, 0, 4 * sizeof(unsigned int));
+        if ((e = cudaMallocHost(&h_bar, 4 * sizeof(unsigned int))) != cudaSuccess)
+            return cuda_fail(e, "cudaMallocHost");
+        h_bar[0] = h_bar[1] = h_bar[2] = 0u;
+        h_bar[3] = P.barrier_timeout_us > 0 ? (unsigned int)P.barrier_timeout_us : 0u;
         if ((e = cudaMallocHost(&h_sizes, sizeof(Sizes))) != cudaSuccess) return cuda_fail(e, "cudaMallocHost");
         if ((e = cudaMallocHost(&h_result, sizeof(ApgdResult))) != cudaSuccess) return cuda_fail(e, "cudaMallocHost");
         if ((e = cudaMallocHost(&h_viol, sizeof(unsigned long long))) != cudaSuccess)
@@ -725,12 +731,20 @@ struct scopi_gpu_handle {
         return (int)std::min<long long>(b, maxb);
     }
 
+    // The barrier words of the next persistent launch: arrivals, generation and error flag
+    // zero, the wait limit (us, 0 = the default); and the one-shot stall of the timeout test.
+    cudaError_t reset_barrier(ApgdSettings& st) {
+        st.stall = stall_next ? 1 : 0;
+        stall_next = false;
+        return cudaMemcpyAsync(d_barrier, h_bar, 4 * sizeof(unsigned int), cudaMemcpyHostToDevice, stream);
+    }
+
     template <typename T>
     int run_apgd(SolveBuffers<T>& sb, const T* invm, int maxb, double dt, double tol, long long max_ite, long long M,
                  double alpha0 = 0.0) {
         Bodies b = bodies();
         StepParams sp = step_params(dt);
-        ApgdSettings st;
+        ApgdSettings st{};
         st.alpha = alpha0 > 0.0 ? alpha0 : P.alpha;
         st.tol = tol;
         st.max_ite = max_ite;
@@ -743,9 +757,10 @@ struct scopi_gpu_handle {
         cudaMemsetAsync(sb.lam[1], 0, M * sizeof(T), stream);
         cudaMemsetAsync(sb.u[0], 0, 6 * (size_t)na * sizeof(T), stream);
         cudaMemsetAsync(sb.u[1], 0, 6 * (size_t)na * sizeof(T), stream);
-        cudaMemsetAsync(d_barrier, 0, 4 * sizeof(unsigned int), stream);
+        cudaError_t e = reset_barrier(st);
+        if (e != cudaSuccess) return cuda_fail(e, "APGD barrier words");
         const int nb = nblocks_for(maxb, std::max<long long>(h_sizes->C, na));
-        cudaError_t e = launch_apgd_invm<T>(b, sp, st, cur, as, sb, invm, d_sizes_cur, nb, stream);
+        e = launch_apgd_invm<T>(b, sp, st, cur, as, sb, invm, d_sizes_cur, nb, stream);
         if (e != cudaSuccess) return cuda_fail(e, "APGD launch");
         cudaMemcpyAsync(h_result, d_result, sizeof(ApgdResult), cudaMemcpyDeviceToHost, stream);
         e = cudaStreamSynchronize(stream);
@@ -757,7 +772,7 @@ struct scopi_gpu_handle {
     template <typename T>
     int run_apgd_sph(SphSolve<T>& sb, int maxb, double dt, double tol, long long max_ite, long long M,
                      double alpha0 = 0.0) {
-        ApgdSettings st;
+        ApgdSettings st{};
         st.alpha = alpha0 > 0.0 ? alpha0 : P.alpha;
         st.tol = tol;
         st.max_ite = max_ite;
@@ -770,9 +785,10 @@ struct scopi_gpu_handle {
         cudaMemsetAsync(sb.lam[1], 0, M * sizeof(T), stream);
         cudaMemsetAsync(sb.u[0], 0, (size_t)na * sizeof(V4<T>), stream);
         cudaMemsetAsync(sb.u[2], 0, (size_t)na * sizeof(V4<T>), stream);
-        cudaMemsetAsync(d_barrier, 0, 4 * sizeof(unsigned int), stream);
+        cudaError_t e = reset_barrier(st);
+        if (e != cudaSuccess) return cuda_fail(e, "APGD barrier words");
         const int nb = nblocks_for(maxb, std::max<long long>(h_sizes->C, na), apgd_sph_threads(sizeof(T) == 4));
-        cudaError_t e = launch_apgd_sph<T>(nin, na, P.dim, P.problem, st, sb, d_sizes_cur, nb, stream);
+        e = launch_apgd_sph<T>(nin, na, P.dim, P.problem, st, sb, d_sizes_cur, nb, stream);
         if (e != cudaSuccess) return cuda_fail(e, "APGD launch");
         cudaMemcpyAsync(h_result, d_result, sizeof(ApgdResult), cudaMemcpyDeviceToHost, stream);
         e = cudaStreamSynchronize(stream);
@@ -1222,6 +1238,7 @@ int32_t scopi_gpu_destroy(scopi_gpu_handle* h) {
     if (h->h_sizes) cudaFreeHost(h->h_sizes);
     if (h->h_result) cudaFreeHost(h->h_result);
     if (h->h_viol) cudaFreeHost(h->h_viol);
+    if (h->h_bar) cudaFreeHost(h->h_bar);
     if (h->h_fp_part) cudaFreeHost(h->h_fp_part);
     if (h->h_gcount) cudaFreeHost(h->h_gcount);
     for (auto& x : h->ev)
@@ -1725,6 +1742,13 @@ int32_t scopi_gpu_batch_get_scene_stats(scopi_gpu_handle* h, int32_t scene, scop
 int32_t scopi_gpu_batch_block_threads(scopi_gpu_handle* h) {
     if (!h) return 0;
     return h->batch_threads ? h->batch_threads : h->batch_bt_used;
+}
+
+int32_t scopi_gpu_test_barrier_stall(scopi_gpu_handle* h) {
+    if (!h) return SCOPI_GPU_EINVAL;
+    if (h->batch) return h->fail(SCOPI_GPU_EINVAL, "a batch's APGD launch has no grid barrier");
+    h->stall_next = true;
+    return 0;
 }
 
 int32_t scopi_gpu_batch_set_block_threads(scopi_gpu_handle* h, int32_t threads) {
