@@ -246,10 +246,13 @@ def measured_peaks():
 
 
 # DRAM bytes (read + write) per FP32 APGD iteration per contact of k_apgd_sph on the
-# 1M-sphere workload, from one ncu capture of a whole launch (19 iterations, the curvature
-# pre-pass and one backtrack included): 6.274 GB / (19 x 3,001,248)
-# (profiles/apgd_sph_spheres_1m_ncu.md)
+# 1M-sphere workload, from one ncu capture of a whole launch at time step 2 (19 iterations,
+# the curvature pre-pass and one backtrack included): 6.274 GB / (19 x 3,001,248).  The
+# line's roofline.traffic scales it by the run's contacts and iterations per launch.
 TRAFFIC_FP32_PER_CONTACT_ITERATION = 110.0
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_apgd_sph<float,3,0> launch at "
+                  "time step 2 (110 B per FP32 contact-iteration), scaled by this run's contacts and FP32 "
+                  "iterations per launch")
 
 
 # ----------------------------------------------------------------------------- CPU legs
@@ -333,6 +336,8 @@ def main():
     ap.add_argument("--side", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-viscous", action="store_true")
+    ap.add_argument("--no-errors", action="store_true")
     ap.add_argument("--workload", default="spheres_1m", choices=["spheres_1m", "piles", "se_pile"],
                     help="spheres_1m: the headline line; piles: 256 pile scenes stepped as one batch; "
                          "se_pile: 50k superellipsoids with friction")
@@ -491,12 +496,42 @@ def se_pile(args, ranks):
     return 0
 
 
+def error_samples(pa, args, ranks):
+    """Error of the mixed form against FP64 on the same step: at 3 sampled steps k of the
+    timed window, the mixed trajectory's state before step k is solved once in FP64 and once
+    in the mixed form; errors in lambda, velocities and gaps (d + dt n.(v_i - v_j))."""
+    from scopi_b200 import FP64, MIXED, ScopiSolver
+    from scopi_b200.errors import solve_errors
+    kw, dt = solver_kwargs()
+    nin = pa.nb_inactive
+    steps = sorted({args.warmup + 1, args.warmup + max(1, args.steps // 2), args.warmup + args.steps})
+    walker = ScopiSolver(pa, precision=MIXED, mixed_violation_tol=1e-6, device=ranks.local, **kw)
+    done, out = 0, []
+    for k in steps:
+        if k - 1 > done:
+            walker.step(dt, k - 1 - done)
+            done = k - 1
+        state = walker.sync().copy()
+        recs = []
+        for prec in (FP64, MIXED):
+            s = ScopiSolver(state, precision=prec, mixed_violation_tol=1e-6, device=ranks.local, **kw).run(dt, 1)
+            recs.append({"contacts": s.current_contacts(), "lambda": s.lagrange_multiplier(),
+                         "v": s.particles.v.copy()})
+            s.close()
+        out.append({"step": k, **solve_errors(recs[0], recs[1], dt, nin)})
+    walker.close()
+    keys = ("lambda_rel", "lambda_max_abs", "v_rel", "v_max_abs", "gap_max_abs", "violation_ref", "violation_other")
+    return {"steps": steps, **{k + "_max": max(o[k] for o in out) for k in keys},
+            "definition": "same state, one FP64 and one mixed solve; gap = d + dt n.(v_i - v_j); rel = 2-norm",
+            "samples": out}
+
+
 def ours(args, ranks):
     import torch
     if not torch.cuda.is_available():
         print(json.dumps({"error": "no CUDA device"}))
         return 1
-    from scopi_b200 import FP64, MIXED, configs
+    from scopi_b200 import FP64, MIXED, VISCOUS, configs
     from scopi_b200.build import build
     build()
     pa = configs.spheres_1m(side=args.side)
@@ -515,6 +550,22 @@ def ours(args, ranks):
                          "iterations_per_step": statistics.mean(its),
                          "violation_max": max(p["violation"] for p in r["per_step"])}
     e2e_ms, h2d, d2h = time_e2e(pa, MIXED, args.steps, args.warmup, ranks)
+    # ViscousWithoutFriction on the same workload (gamma defaults 0 / -2 / 1e-6)
+    visc = None
+    if not args.no_viscous:
+        vm = time_path(pa, MIXED, args.steps, args.warmup, ranks, problem=VISCOUS)
+        vf = None if args.no_fp64 else time_path(pa, FP64, args.steps, args.warmup, ranks, problem=VISCOUS)
+        vm_val = ranks.world * args.steps * 1000.0 / ranks.max(vm["ms"])
+        visc = {"value": vm_val, "unit": UNIT, "problem": "ViscousWithoutFriction",
+                "violation_max": max(p["violation"] for p in vm["per_step"]),
+                "fp32_iterations_per_step": statistics.mean(p["fp32_iterations"] for p in vm["per_step"]),
+                "fp64": ({"value": ranks.world * args.steps * 1000.0 / ranks.max(vf["ms"]), "unit": UNIT,
+                          "violation_max": max(p["violation"] for p in vf["per_step"]),
+                          "iterations_per_step": statistics.mean(p["iterations"] for p in vf["per_step"])}
+                         if vf else None)}
+        if vf:
+            visc["mixed_over_fp64"] = vm_val / visc["fp64"]["value"]
+    errs = None if (args.no_fp64 or args.no_errors) else error_samples(pa, args, ranks)
 
     ms = ranks.max(mixed["ms"])
     value = args.gpus * args.steps * 1000.0 / ms if ranks.world > 1 else args.steps * 1000.0 / ms
@@ -530,10 +581,13 @@ def ours(args, ranks):
     C = statistics.mean(p["contacts"] for p in per)
     it32 = sum(p["fp32_iterations"] for p in per)
     ms_apgd = sum(p["ms_apgd_kernel"] for p in per)
-    b_iter32 = roofline_bytes_per_iter(C, n_active, 4)
-    b_iter32_tf = roofline_bytes_per_iter(C, n_active, 4, torque_free=True)
+    # headline bytes: what the torque-free iteration must move (normal only, translational
+    # slots); the full-row formula (9 values per contact, 6N slots, a third pass over B)
+    # counts six identically zero values per row and a pass the fused iteration never makes
+    b_iter32 = roofline_bytes_per_iter(C, n_active, 4, torque_free=True)
+    b_iter32_full = roofline_bytes_per_iter(C, n_active, 4)
     achieved = (it32 * b_iter32) / (ms_apgd * 1e-3) / 1e9 if ms_apgd > 0 else None
-    achieved_tf = (it32 * b_iter32_tf) / (ms_apgd * 1e-3) / 1e9 if ms_apgd > 0 else None
+    achieved_full = (it32 * b_iter32_full) / (ms_apgd * 1e-3) / 1e9 if ms_apgd > 0 else None
     peak, peak_kind = measured_peaks()
     # DRAM bytes of one APGD launch (one whole solve): ncu dram__bytes_read.sum +
     # dram__bytes_write.sum per FP32 iteration per contact, times this run's contacts and
@@ -545,11 +599,12 @@ def ours(args, ranks):
         p64 = f64["per_step"]
         it64 = sum(p["iterations"] for p in p64)
         ms64 = sum(p["ms_apgd_kernel"] for p in p64)
-        a64 = (it64 * roofline_bytes_per_iter(C, n_active, 8)) / (ms64 * 1e-3) / 1e9 if ms64 > 0 else None
-        a64_tf = ((it64 * roofline_bytes_per_iter(C, n_active, 8, torque_free=True)) / (ms64 * 1e-3) / 1e9
-                  if ms64 > 0 else None)
+        a64 = ((it64 * roofline_bytes_per_iter(C, n_active, 8, torque_free=True)) / (ms64 * 1e-3) / 1e9
+               if ms64 > 0 else None)
+        a64_full = (it64 * roofline_bytes_per_iter(C, n_active, 8)) / (ms64 * 1e-3) / 1e9 if ms64 > 0 else None
         f64_roof = {"achieved": a64, "peak": peak, "unit": "GB/s", "frac": (a64 / peak) if a64 else None,
-                    "achieved_streamed": a64_tf, "frac_streamed": (a64_tf / peak) if a64_tf else None,
+                    "achieved_formula_full_rows": a64_full,
+                    "frac_formula_full_rows": (a64_full / peak) if a64_full else None,
                     "iterations_per_step": it64 / len(p64), "ms_apgd_per_step": ms64 / len(p64),
                     "violation_max": max(p["violation"] for p in p64)}
 
@@ -584,13 +639,17 @@ def ours(args, ranks):
                      "peak_source": f"{peak_kind} hbm_gbs",
                      "kernel": "k_apgd_sph<float,3,NoFriction> (persistent, torque-free rows)",
                      "bytes_per_iteration": b_iter32,
-                     "achieved_streamed": achieved_tf,
-                     "frac_streamed": (achieved_tf / peak) if achieved_tf else None,
-                     "bytes_per_iteration_streamed": b_iter32_tf,
+                     "bytes_definition": "3C(3s+8) + 6Cs + 4(3N)s: normal-only rows, translational slots",
+                     "achieved_formula_full_rows": achieved_full,
+                     "frac_formula_full_rows": (achieved_full / peak) if achieved_full else None,
+                     "bytes_per_iteration_formula_full_rows": b_iter32_full,
+                     "traffic_source": TRAFFIC_SOURCE,
                      "traffic_per_iteration": (traffic / (it32 / len(per))) if traffic else None,
                      "iterations_per_step": it32 / len(per),
                      "ms_apgd_per_step": ms_apgd / len(per)},
         "cpu_baseline": cpu,
+        "viscous": visc,
+        "error_vs_fp64": errs,
         "clocks": mixed["clocks"],
         "gpu_launches": mixed["launches"],
         "solver": {"contacts": C, "violation_max": max(p["violation"] for p in per),

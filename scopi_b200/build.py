@@ -47,14 +47,18 @@ def build(verbose: bool = False, force: bool = False, extra: list | None = None)
     if not force and not needs_build():
         return OUT
     os.makedirs(BUILD, exist_ok=True)
-    objs = []
+    objs, procs = [], []
+    # the translation units are independent: compile them side by side
     for src, flags in SOURCES.items():
         obj = os.path.join(BUILD, src.replace(".cu", ".o"))
         cmd = [nvcc(), *ARCH, *COMMON, *flags, *(extra or []), "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
+        procs.append((cmd, subprocess.Popen(cmd)))
         objs.append(obj)
+    failed = [cmd for cmd, pr in procs if pr.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
     cmd = [nvcc(), *ARCH, "-shared", "-o", OUT, *objs, "-lcudart"]
     if verbose:
         print(" ".join(cmd), flush=True)
