@@ -201,6 +201,14 @@ int32_t scopi_gpu_get_stats(scopi_gpu_handle* h, scopi_gpu_stats* out);
 int32_t scopi_gpu_amat(scopi_gpu_handle* h, const double* u, double* out);
 int32_t scopi_gpu_atmat(scopi_gpu_handle* h, const double* f, double* out);
 
+/* The contact list AMatrix / ATMatrix are built on (AMatrix(contacts, particles),
+   matrix/velocities.hpp:54-66): replaces the handle's current contact list (the one
+   scopi_gpu_get_contacts returns and scopi_gpu_amat / scopi_gpu_atmat use) with n records;
+   nij/pi/pj are n*3.  Indices must be < the container's size (else SCOPI_GPU_EINVAL).
+   Single-scene handles; the next step detects its own contacts again. */
+int32_t scopi_gpu_set_contacts(scopi_gpu_handle* h, int64_t n, const int64_t* ci, const int64_t* cj,
+                               const double* dij, const double* nij, const double* pi, const double* pj);
+
 /* Message of the last failing call on this handle (or of the last failing create). */
 const char* scopi_gpu_last_error(scopi_gpu_handle* h);
 

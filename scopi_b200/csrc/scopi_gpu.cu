@@ -1525,6 +1525,44 @@ int32_t scopi_gpu_amat(scopi_gpu_handle* h, const double* u, double* out) {
     return 0;
 }
 
+int32_t scopi_gpu_set_contacts(scopi_gpu_handle* h, int64_t n, const int64_t* ci, const int64_t* cj,
+                               const double* dij, const double* nij, const double* pi, const double* pj) {
+    if (!h) return SCOPI_GPU_EINVAL;
+    if (h->batch) return h->fail(SCOPI_GPU_EINVAL, "set_contacts: single-scene handles only");
+    if (h->n == 0) return h->fail(SCOPI_GPU_EINVAL, "set_contacts: no particles");
+    if (n < 0 || n > 0x7fffffffLL || (n > 0 && (!ci || !cj || !dij || !nij || !pi || !pj)))
+        return h->fail(SCOPI_GPU_EINVAL, "set_contacts: null array or count out of range");
+    std::vector<int> i32(n), j32(n);
+    for (int64_t k = 0; k < n; ++k) {
+        if (ci[k] < 0 || ci[k] >= h->n || cj[k] < 0 || cj[k] >= h->n)
+            return h->fail(SCOPI_GPU_EINVAL, "set_contacts: body index out of range");
+        i32[k] = (int)ci[k];
+        j32[k] = (int)cj[k];
+    }
+    cudaSetDevice(h->dev);
+    if (n > h->c_cap) {
+        int rc = h->alloc_contacts(std::max<long long>((long long)(1.3 * (double)n) + 1024, 2 * h->c_cap));
+        if (rc) return rc;
+    }
+    cudaError_t e = cudaSuccess;
+    if (n > 0) {
+        e = cudaMemcpy(h->old.ci, i32.data(), n * sizeof(int), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(h->old.cj, j32.data(), n * sizeof(int), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(h->old.dij, dij, n * sizeof(double), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(h->old.nij, nij, 3 * n * sizeof(double), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(h->old.pi, pi, 3 * n * sizeof(double), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(h->old.pj, pj, 3 * n * sizeof(double), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemset(h->old.gamma, 0, n * sizeof(double));
+    }
+    Sizes s{};
+    s.C = (int)n;
+    if (e == cudaSuccess) e = cudaMemcpy(h->d_sizes_old, &s, sizeof(Sizes), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return h->cuda_fail(e, "set_contacts");
+    h->has_old = true;
+    h->last_lambda = nullptr;
+    return 0;
+}
+
 int32_t scopi_gpu_atmat(scopi_gpu_handle* h, const double* f, double* out) {
     if (!h || !f || !out) return SCOPI_GPU_EINVAL;
     cudaSetDevice(h->dev);

@@ -8,8 +8,11 @@
 //   quaternion(), mult_quaternion, normalize  src/quaternion.cpp:6-120
 //   NoFriction / Friction / Viscous           include/scopi/contact/property.hpp:14-36
 //   contact_property<...>                     include/scopi/contact/property.hpp:41-128
-//   ContactsParams<contact_kdtree/brute>      include/scopi/contact/contact_kdtree.hpp:203-238,
-//                                             include/scopi/contact/contact_brute_force.hpp:470-495
+//   ContactsParams<contact_kdtree/brute>      include/scopi/contact/contact_kdtree.hpp:27-61,
+//                                             include/scopi/contact/contact_brute_force.hpp:25-50
+//   contact_kdtree / contact_brute_force      include/scopi/contact/base.hpp:20-90 (run)
+//   neighbor<dim, problem_t>                  include/scopi/contact/neighbor.hpp:24-55
+//   AMatrix / ATMatrix                        include/scopi/matrix/velocities.hpp:53-254
 //   apgd_params / OptimGradient<apgd>         include/scopi/solvers/apgd.hpp:105-124,
 //                                             include/scopi/solvers/OptimGradient.hpp:56-349
 //   vap_fixed / vap_fpd                       include/scopi/vap/vap_fixed.hpp, vap_fpd.hpp
@@ -939,13 +942,144 @@ scopi_container<dim> from_json(const std::filesystem::path& path) {
 }
 
 // ------------------------------------------------------------------ contacts record
+namespace type {
+// a contact vector read as v[k] or v(k), as the reference's fixed-size tensors allow
+template <std::size_t dim>
+struct contact_vec : std::array<double, dim> {
+    double& operator()(std::size_t k) { return (*this)[k]; }
+    double operator()(std::size_t k) const { return (*this)[k]; }
+};
+}  // namespace type
+
+// neighbor<dim, problem_t> (contact/neighbor.hpp:24-55)
 template <std::size_t dim, class problem_t>
 struct neighbor {
     std::size_t i, j;
     double dij;
-    type::position_t<dim> nij, pi, pj;
+    type::contact_vec<dim> nij, pi, pj;
     contact_property<problem_t> property;
 };
+
+// ------------------------------------------------------------------ contact methods
+template <class D>
+struct ContactsParams;
+template <class problem_t>
+class contact_kdtree;
+template <class problem_t>
+class contact_brute_force;
+
+template <class problem_t>
+struct ContactsParams<contact_kdtree<problem_t>> {  // contact_kdtree.hpp:27-61
+    void init_options() {}
+    double dmax{2.};
+    double kd_tree_radius{17.};
+};
+template <class problem_t>
+struct ContactsParams<contact_brute_force<problem_t>> {  // contact_brute_force.hpp:25-50
+    void init_options() {}
+    double dmax{2.};
+};
+
+namespace detail {
+// contact_base::run (contact/base.hpp:71-84) through the C ABI: a handle with the method's
+// parameters detects the container's contacts (periodic copies of `box` included) and
+// returns them sorted by (i, j)
+template <std::size_t dim, class problem_t>
+std::vector<neighbor<dim, problem_t>> detect_contacts(int32_t method, double dmax, double kd_radius,
+                                                      const BoxDomain<dim>& box, scopi_container<dim>& particles);
+}  // namespace detail
+
+// contact_kdtree<problem_t> / contact_brute_force<problem_t> (contact_kdtree.hpp:70-268,
+// contact_brute_force.hpp:59-136): callable as in the reference,
+//     ContactsParams<contact_kdtree<NoFriction>> params; contact_kdtree cont(params);
+//     auto contacts = cont.run(particles);
+// the search is the GPU cell list of this library (same contact set as the kd-tree and the
+// brute force: every pair with dij < dmax, kd-tree candidates within the kd radius).
+template <class problem_t>
+class contact_kdtree {
+  public:
+    static constexpr int32_t code = SCOPI_GPU_KDTREE;
+    using params_t = ContactsParams<contact_kdtree<problem_t>>;
+    contact_kdtree() = default;
+    explicit contact_kdtree(const params_t& params) : m_params(params) {}
+    void init_options() { m_params.init_options(); }
+    params_t& get_params() { return m_params; }
+    contact_property<problem_t>& default_contact_property() { return m_property; }
+    template <std::size_t dim>
+    std::vector<neighbor<dim, problem_t>> run(const BoxDomain<dim>& box, scopi_container<dim>& particles) {
+        return detail::detect_contacts<dim, problem_t>(code, m_params.dmax, m_params.kd_tree_radius, box, particles);
+    }
+    template <std::size_t dim>
+    std::vector<neighbor<dim, problem_t>> run(scopi_container<dim>& particles) {
+        return run(BoxDomain<dim>(), particles);
+    }
+
+  private:
+    params_t m_params;
+    contact_property<problem_t> m_property;
+};
+
+template <class problem_t>
+class contact_brute_force {
+  public:
+    static constexpr int32_t code = SCOPI_GPU_BRUTE_FORCE;
+    using params_t = ContactsParams<contact_brute_force<problem_t>>;
+    contact_brute_force() = default;
+    explicit contact_brute_force(const params_t& params) : m_params(params) {}
+    void init_options() { m_params.init_options(); }
+    params_t& get_params() { return m_params; }
+    contact_property<problem_t>& default_contact_property() { return m_property; }
+    template <std::size_t dim>
+    std::vector<neighbor<dim, problem_t>> run(const BoxDomain<dim>& box, scopi_container<dim>& particles) {
+        return detail::detect_contacts<dim, problem_t>(code, m_params.dmax, 0.0, box, particles);
+    }
+    template <std::size_t dim>
+    std::vector<neighbor<dim, problem_t>> run(scopi_container<dim>& particles) {
+        return run(BoxDomain<dim>(), particles);
+    }
+
+  private:
+    params_t m_params;
+    contact_property<problem_t> m_property;
+};
+
+namespace detail {
+inline void check_abi(int32_t rc, scopi_gpu_handle* h, const char* what);
+
+// a handle holding the container (and, for the matrices, a given contact list)
+template <std::size_t dim>
+scopi_gpu_handle* open_handle(int32_t problem, int32_t method, double dmax, double kd_radius,
+                              const BoxDomain<dim>& box, scopi_container<dim>& particles) {
+    scopi_gpu_params p;
+    scopi_gpu_default_params(&p, (int32_t)dim);
+    p.problem = problem;
+    p.contact_method = method;
+    p.dmax = dmax;
+    if (method == SCOPI_GPU_KDTREE) p.kd_tree_radius = kd_radius;
+    for (std::size_t d = 0; d < dim; ++d) {
+        p.box_lower[d] = box.lower_bound(d);
+        p.box_upper[d] = box.upper_bound(d);
+        p.periodic[d] = box.is_periodic(d) ? 1 : 0;
+    }
+    scopi_gpu_handle* h = nullptr;
+    check_abi(scopi_gpu_create(&p, &h), nullptr, "create");
+    scopi_gpu_particles abi = particles.abi();
+    const int32_t rc = scopi_gpu_set_particles(h, &abi);
+    if (rc < 0) {
+        const std::string msg = scopi_gpu_last_error(h);
+        scopi_gpu_destroy(h);
+        throw std::runtime_error("scopi_gpu_set_particles: " + msg);
+    }
+    return h;
+}
+
+struct handle_guard {
+    scopi_gpu_handle* h;
+    ~handle_guard() {
+        if (h) scopi_gpu_destroy(h);
+    }
+};
+}  // namespace detail
 
 // ------------------------------------------------------------------ GPU policies
 namespace gpu {
@@ -980,26 +1114,13 @@ struct OptimGradient {
     params_t& get_params() { return m_params; }
 };
 
+// the contact methods above, under the GPU policy names
 template <class D>
-struct ContactsParams;
-
+using ContactsParams = scopi::ContactsParams<D>;
 template <class problem_t>
-struct contact_kdtree {
-    static constexpr int32_t code = SCOPI_GPU_KDTREE;
-};
+using contact_kdtree = scopi::contact_kdtree<problem_t>;
 template <class problem_t>
-struct contact_brute_force {
-    static constexpr int32_t code = SCOPI_GPU_BRUTE_FORCE;
-};
-template <class problem_t>
-struct ContactsParams<contact_kdtree<problem_t>> {  // contact_kdtree.hpp:203-238
-    double dmax{2.};
-    double kd_tree_radius{17.};
-};
-template <class problem_t>
-struct ContactsParams<contact_brute_force<problem_t>> {  // contact_brute_force.hpp:470-495
-    double dmax{2.};
-};
+using contact_brute_force = scopi::contact_brute_force<problem_t>;
 
 struct VapParams {};
 struct vap_fixed {
@@ -1017,12 +1138,6 @@ using apgd_params = gpu::apgd_params;
 using apgd = gpu::apgd<gpu::fp64>;
 template <class Method>
 using OptimGradient = gpu::OptimGradient<Method>;
-template <class problem_t>
-using contact_kdtree = gpu::contact_kdtree<problem_t>;
-template <class problem_t>
-using contact_brute_force = gpu::contact_brute_force<problem_t>;
-template <class D>
-using ContactsParams = gpu::ContactsParams<D>;
 using vap_fixed = gpu::vap_fixed;
 using vap_fpd = gpu::vap_fpd;
 
@@ -1278,6 +1393,113 @@ class ScopiSolver {
     ScopiParams m_params;
     std::vector<neighbor<dim, problem_t>> m_contacts;
     scopi_gpu_handle* m_h = nullptr;
+};
+
+// ------------------------------------------------------------------ contact methods, matrices
+namespace detail {
+inline void check_abi(int32_t rc, scopi_gpu_handle* h, const char* what) {
+    if (rc < 0) throw gpu_error(std::string("scopi_gpu_") + what + ": " + scopi_gpu_last_error(h));
+}
+
+template <std::size_t dim, class problem_t>
+std::vector<neighbor<dim, problem_t>> detect_contacts(int32_t method, double dmax, double kd_radius,
+                                                      const BoxDomain<dim>& box, scopi_container<dim>& particles) {
+    handle_guard g{open_handle<dim>(problem_code<problem_t>(), method, dmax, kd_radius, box, particles)};
+    int64_t n = 0;
+    check_abi(scopi_gpu_detect(g.h, &n), g.h, "detect");
+    std::vector<int64_t> ci(n), cj(n);
+    std::vector<double> d(n), nij(3 * n), pi(3 * n), pj(3 * n);
+    check_abi(scopi_gpu_get_contacts(g.h, n, &n, ci.data(), cj.data(), d.data(), nij.data(), pi.data(), pj.data(),
+                                     nullptr),
+              g.h, "get_contacts");
+    std::vector<neighbor<dim, problem_t>> out((std::size_t)n);
+    for (int64_t k = 0; k < n; ++k) {
+        auto& c = out[(std::size_t)k];
+        c.i = (std::size_t)ci[k];
+        c.j = (std::size_t)cj[k];
+        c.dij = d[k];
+        for (std::size_t x = 0; x < dim; ++x) {
+            c.nij[x] = nij[3 * k + x];
+            c.pi[x] = pi[3 * k + x];
+            c.pj[x] = pj[3 * k + x];
+        }
+    }
+    return out;
+}
+
+// a handle on the container with `contacts` as its contact list
+template <class Contacts_t, std::size_t dim>
+scopi_gpu_handle* jacobian_handle(const Contacts_t& contacts, const scopi_container<dim>& particles) {
+    auto& parts = const_cast<scopi_container<dim>&>(particles);  // read only: uploaded, not written
+    scopi_gpu_handle* h = open_handle<dim>(SCOPI_GPU_NOFRICTION, SCOPI_GPU_BRUTE_FORCE, 2.0, 0.0, BoxDomain<dim>(), parts);
+    const std::size_t n = contacts.size();
+    std::vector<int64_t> ci(n), cj(n);
+    std::vector<double> d(n), nij(3 * n, 0.0), pi(3 * n, 0.0), pj(3 * n, 0.0);
+    for (std::size_t k = 0; k < n; ++k) {
+        const auto& c = contacts[k];
+        ci[k] = (int64_t)c.i;
+        cj[k] = (int64_t)c.j;
+        d[k] = c.dij;
+        for (std::size_t x = 0; x < dim; ++x) {
+            nij[3 * k + x] = c.nij[x];
+            pi[3 * k + x] = c.pi[x];
+            pj[3 * k + x] = c.pj[x];
+        }
+    }
+    const int32_t rc = scopi_gpu_set_contacts(h, (int64_t)n, ci.data(), cj.data(), d.data(), nij.data(), pi.data(),
+                                              pj.data());
+    if (rc < 0) {
+        const std::string msg = scopi_gpu_last_error(h);
+        scopi_gpu_destroy(h);
+        throw gpu_error("scopi_gpu_set_contacts: " + msg);
+    }
+    return h;
+}
+}  // namespace detail
+
+// AMatrix (matrix/velocities.hpp:53-144): per contact (v_i - (p_i - x_i) x R_i w_i) -
+// (v_j - (p_j - x_j) x R_j w_j) on the active bodies; u holds 6 values per active body
+// (velocity, then rotation), the result 3 per contact.  Applied on the GPU.
+template <class Contacts_t, class Particles_t>
+class AMatrix {
+  public:
+    static constexpr std::size_t dim = Particles_t::dim_;
+    AMatrix(const Contacts_t& contacts, const Particles_t& particles) : m_contacts(contacts), m_particles(particles) {}
+    template <class Vec>
+    const std::vector<double>& mat_mult(const Vec& u) const {
+        if (std::size(u) != 6 * m_particles.nb_active()) throw gpu_error("AMatrix::mat_mult: u must hold 6 values per active body");
+        detail::handle_guard g{detail::jacobian_handle(m_contacts, m_particles)};
+        m_work.assign(3 * m_contacts.size(), 0.0);
+        if (!m_contacts.empty()) detail::check_abi(scopi_gpu_amat(g.h, std::data(u), m_work.data()), g.h, "amat");
+        return m_work;
+    }
+
+  private:
+    const Contacts_t& m_contacts;
+    const Particles_t& m_particles;
+    mutable std::vector<double> m_work;
+};
+
+// ATMatrix (matrix/velocities.hpp:153-254): the adjoint, forces (3 per contact) to 6 values
+// per active body.  Applied on the GPU.
+template <class Contacts_t, class Particles_t>
+class ATMatrix {
+  public:
+    static constexpr std::size_t dim = Particles_t::dim_;
+    ATMatrix(const Contacts_t& contacts, const Particles_t& particles) : m_contacts(contacts), m_particles(particles) {}
+    template <class Vec>
+    const std::vector<double>& mat_mult(const Vec& f) const {
+        if (std::size(f) != 3 * m_contacts.size()) throw gpu_error("ATMatrix::mat_mult: f must hold 3 values per contact");
+        detail::handle_guard g{detail::jacobian_handle(m_contacts, m_particles)};
+        m_work.assign(6 * m_particles.nb_active(), 0.0);
+        if (!m_contacts.empty()) detail::check_abi(scopi_gpu_atmat(g.h, std::data(f), m_work.data()), g.h, "atmat");
+        return m_work;
+    }
+
+  private:
+    const Contacts_t& m_contacts;
+    const Particles_t& m_particles;
+    mutable std::vector<double> m_work;
 };
 
 }  // namespace scopi

@@ -398,3 +398,28 @@ def test_box_domain_api(tmp_path):
     subprocess.run([GXX, "-std=c++17", "-Wall", "-Werror", *INC, src, "-o", exe], check=True)
     r = subprocess.run([exe], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+CM_SRC = os.path.join(ROOT, "tests", "cpp", "contacts_matrices_dropin.cpp")
+
+
+def test_contacts_matrices_header_compiles():
+    subprocess.run([GXX, "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", *INC, CM_SRC], check=True)
+
+
+@pytest.mark.gpu
+def test_cpp_contact_methods_and_matrices(tmp_path):
+    """contact_kdtree(params).run(particles), contact_brute_force, AMatrix / ATMatrix as the
+    reference's test_contacts_kdtree.cpp, test_contacts_brute_force.cpp and test_matrices.cpp
+    use them."""
+    from scopi_b200 import build
+    build.build()
+    out = str(tmp_path / "contacts_matrices")
+    lib = os.path.join(ROOT, "scopi_b200")
+    subprocess.run([GXX, "-O2", "-std=c++17", *INC, CM_SRC, "-L", lib, "-lscopi_gpu", f"-Wl,-rpath,{lib}", "-o", out],
+                   check=True)
+    r = subprocess.run([out], capture_output=True, text=True, cwd=tmp_path)
+    assert r.returncode == 0, r.stdout + r.stderr
+    res = json.loads(r.stdout)
+    assert res["failures"] == 0
+    assert abs(res["adjoint_difference"]) <= 1e-12
