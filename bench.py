@@ -208,7 +208,7 @@ def time_e2e(pa, precision, steps, warmup, ranks):
 
     keep = []
     host = pa.copy()
-    for k in ("shape", "pos", "q", "v", "omega", "vd", "omega_d", "f", "m", "j", "radius", "length"):
+    for k in ("shape", "worm", "pos", "q", "v", "omega", "vd", "omega_d", "f", "m", "j", "radius", "length"):
         arr, t = pinned(getattr(host, k))
         keep.append(t)
         setattr(host, k, arr)
@@ -230,7 +230,7 @@ def time_e2e(pa, precision, steps, warmup, ranks):
     ranks.barrier()
     ms = e0.elapsed_time(e1)
     n = host.n
-    h2d = 4 * n + 8 * n * (3 + 4 + 3 + 3 + 3 + 3 + 3 + 1 + 3 + 1 + 1)
+    h2d = 4 * n + 4 * n + 8 * n * (3 + 4 + 3 + 3 + 3 + 3 + 3 + 1 + 3 + 1 + 1)  # shape, worm, 11 FP64 fields
     d2h = 8 * n * (3 + 4 + 3 + 3)
     s.close()
     return ms, h2d, d2h
@@ -298,7 +298,7 @@ def reference_arm(args, ranks):
     from scopi_b200 import configs
     threads = os.cpu_count() or 1
     pa = configs.spheres_1m()
-    iters = REF_APGD_ITERATIONS_DEFAULT
+    iters, iters_src = reference_iterations(args.warmup + 1, args.warmup + args.steps)
     samples = []
     for k in range(args.warmup + args.steps):
         r = cpu_sample(pa, iters, threads)
@@ -310,11 +310,12 @@ def reference_arm(args, ranks):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD + ": 1,000,000 spheres, NoFriction, vap_fixed, dmax 0.0018, dt 1e-3, tol 1e-6"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "extrapolated": True,
+                         "cpu_model": cpu_model(),
                          "sample": (f"oracle (C++ restatement of the reference path, OpenMP on the loops the reference "
                                     f"parallelises, serial APGD) on the full 1M-sphere step, APGD capped at 1 and 3 "
-                                    f"iterations; steps/s = 1/(t_outside_apgd + t_per_iteration * {iters}), "
-                                    f"{iters} = FP64 APGD iterations per step of this workload measured on B200")},
+                                    f"iterations; steps/s = 1/(t_outside_apgd + t_per_iteration * {iters:.1f}), "
+                                    f"{iters:.1f} = mean FP64 APGD iterations per step of the timed steps ({iters_src})")},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "samples": samples,
     }
@@ -322,9 +323,24 @@ def reference_arm(args, ranks):
     return 0
 
 
-# mean FP64 APGD iterations per step of spheres_1m measured on B200 with the FP64 path
-# (the reference's algorithm and tolerance): 505 and 489 on the first two steps
+# FP64 APGD iterations of every step of the 100-step spheres_1m run, measured on B200 with
+# the FP64 path (the reference's iterate rule, cold start and tolerance); the file holds
+# the command that measured them.  The CPU legs take the mean over the steps they stand for.
+ITERATIONS_FILE = os.path.join(ROOT, "scopi_b200", "data", "spheres_1m_fp64_iterations.json")
 REF_APGD_ITERATIONS_DEFAULT = 497
+
+
+def reference_iterations(first, last):
+    """Mean FP64 iterations per step over steps first..last (1-based) and where it came from."""
+    try:
+        with open(ITERATIONS_FILE) as fh:
+            d = json.load(fh)
+        its = d["iterations"][first - 1:last]
+        if its:
+            return statistics.mean(its), f"measured per step on B200 ({d['command']}), steps {first}..{last}"
+    except (OSError, KeyError, ValueError):
+        pass
+    return REF_APGD_ITERATIONS_DEFAULT, "constant (first two steps measured on B200)"
 
 
 def main():
@@ -731,10 +747,12 @@ def ours(args, ranks):
 
     cpu = None
     if not args.no_cpu_baseline and ranks.rank == 0 and args.side == 100:
-        iters = (f64_roof["iterations_per_step"] if f64_roof else REF_APGD_ITERATIONS_DEFAULT)
+        iters = (f64_roof["iterations_per_step"] if f64_roof else
+                 reference_iterations(args.warmup + 1, args.warmup + args.steps)[0])
         threads = os.cpu_count() or 1
         r = cpu_sample(pa, iters, threads)
-        cpu = {"value": r["value"], "unit": UNIT, "cores": threads, "kind": "port",
+        cpu = {"value": r["value"], "unit": UNIT, "cores": threads, "kind": "port", "extrapolated": True,
+               "cpu_model": cpu_model(),
                "sample": (f"oracle on the full 1M-sphere step, APGD capped at 1 and 3 iterations "
                           f"({r['wall_s']:.1f} s wall); steps/s = 1/(t_outside_apgd "
                           f"{r['t_outside_apgd_s']:.2f} s + t_per_iteration {r['t_per_iteration_s']:.3f} s * "

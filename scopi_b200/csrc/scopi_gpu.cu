@@ -117,6 +117,8 @@ struct scopi_gpu_handle {
     ApgdResult* h_result = nullptr;    // pinned
     unsigned long long* h_viol = nullptr;
     unsigned int* h_bar = nullptr;     // pinned: the four barrier words written before a launch
+    int* d_census = nullptr;           // shape census of an upload (k_shape_census)
+    int* h_census = nullptr;           // pinned copy
     bool stall_next = false;           // scopi_gpu_test_barrier_stall: withhold one arrival once
     int max_blocks64 = 0, max_blocks32 = 0, max_sph64 = 0, max_sph32 = 0;
     // FrictionFixedPoint: P.problem holds FRICTION (the kernels' problem), this flag the loop
@@ -471,6 +473,8 @@ struct scopi_gpu_handle {
         cudaMemset(d_barrier, 0, 4 * sizeof(unsigned int));
         if ((e = cudaMallocHost(&h_bar, 4 * sizeof(unsigned int))) != cudaSuccess)
             return cuda_fail(e, "cudaMallocHost");
+        if ((e = alloc(fixed_mem, d_census, 4)) != cudaSuccess) return cuda_fail(e, "alloc");
+        if ((e = cudaMallocHost(&h_census, 4 * sizeof(int))) != cudaSuccess) return cuda_fail(e, "cudaMallocHost");
         h_bar[0] = h_bar[1] = h_bar[2] = 0u;
         h_bar[3] = P.barrier_timeout_us > 0 ? (unsigned int)P.barrier_timeout_us : 0u;
         if ((e = cudaMallocHost(&h_sizes, sizeof(Sizes))) != cudaSuccess) return cuda_fail(e, "cudaMallocHost");
@@ -1242,6 +1246,7 @@ int32_t scopi_gpu_destroy(scopi_gpu_handle* h) {
     if (h->h_result) cudaFreeHost(h->h_result);
     if (h->h_viol) cudaFreeHost(h->h_viol);
     if (h->h_bar) cudaFreeHost(h->h_bar);
+    if (h->h_census) cudaFreeHost(h->h_census);
     if (h->h_fp_part) cudaFreeHost(h->h_fp_part);
     if (h->h_gcount) cudaFreeHost(h->h_gcount);
     for (auto& x : h->ev)
@@ -1294,6 +1299,42 @@ static void launch_inverse_mass(int n, int nin, int dim, const double* m, const 
     k_inverse_mass<<<blocks, 256, 0, s>>>(n, nin, dim, m, j, im64, im32, imt64, imt32);
 }
 
+// Census of an uploaded container, on the device (the host would spend ~3 ns per body on it):
+// out[0] active superellipsoids, out[1] active spheres, out[2] bodies with a worm index, and
+// out[3] the container's rule violations: bit 1 unknown shape, bit 2 an active body that is
+// neither a sphere nor a superellipsoid, bit 4 a superellipsoid obstacle, bit 8 a segment in 3D.
+__global__ void k_shape_census(const int* shape, const int* worm, int n, int nin, int dim, int* out) {
+    int se = 0, sph = 0, wm = 0, bad = 0;
+    GRID_STRIDE(i, n) {
+        const int sh = shape[i];
+        if (sh < 0 || sh > 3) {
+            bad |= 1;
+        } else {
+            if (i >= nin && sh != SCOPI_GPU_SPHERE && sh != SCOPI_GPU_SUPERELLIPSOID) bad |= 2;
+            if (i < nin && sh == SCOPI_GPU_SUPERELLIPSOID) bad |= 4;
+            if (sh == SCOPI_GPU_SEGMENT && dim != 2) bad |= 8;
+        }
+        if (i >= nin) {
+            if (sh == SCOPI_GPU_SUPERELLIPSOID) ++se;
+            else if (sh == SCOPI_GPU_SPHERE) ++sph;
+        }
+        if (worm && worm[i] >= 0) ++wm;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        se += __shfl_down_sync(0xffffffffu, se, o);
+        sph += __shfl_down_sync(0xffffffffu, sph, o);
+        wm += __shfl_down_sync(0xffffffffu, wm, o);
+        bad |= __shfl_down_sync(0xffffffffu, bad, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (se) atomicAdd(out, se);
+        if (sph) atomicAdd(out + 1, sph);
+        if (wm) atomicAdd(out + 2, wm);
+        if (bad) atomicOr(out + 3, bad);
+    }
+}
+
 static int32_t upload_particles(scopi_gpu_handle* h, const scopi_gpu_particles* p, long long obs_cap) {
     if (!h || !p || p->n < 0 || p->nb_inactive < 0 || p->nb_inactive > p->n || p->n >= (1LL << 30))
         return h ? h->fail(SCOPI_GPU_EINVAL, "invalid particle container") : SCOPI_GPU_EINVAL;
@@ -1303,48 +1344,8 @@ static int32_t upload_particles(scopi_gpu_handle* h, const scopi_gpu_particles* 
     const int n = (int)p->n, nin = (int)p->nb_inactive;
     if ((long long)nin * (n - nin) >= (1LL << 31) && obs_cap < 0)
         return h->fail(SCOPI_GPU_EUNSUPPORTED, "obstacles x active bodies must stay below 2^31");
-    int n_se = 0, n_sph = 0;
-    for (int i = 0; i < n; ++i) {
-        const int s = p->shape[i];
-        if (s < 0 || s > 3) return h->fail(SCOPI_GPU_EINVAL, "unknown shape");
-        if (i >= nin && s != SCOPI_GPU_SPHERE && s != SCOPI_GPU_SUPERELLIPSOID)
-            return h->fail(SCOPI_GPU_EUNSUPPORTED, "active bodies must be spheres or superellipsoids");
-        if (i < nin && s == SCOPI_GPU_SUPERELLIPSOID)
-            return h->fail(SCOPI_GPU_EUNSUPPORTED, "superellipsoid obstacles are not supported");
-        if (s == SCOPI_GPU_SEGMENT && h->P.dim != 2) return h->fail(SCOPI_GPU_EUNSUPPORTED, "segments are 2D only");
-        if (i >= nin) (s == SCOPI_GPU_SUPERELLIPSOID ? n_se : n_sph)++;
-    }
-    if (n_se > 0) {
-        if (h->P.dim == 2 && nin > 0)
-            return h->fail(SCOPI_GPU_EUNSUPPORTED, "2D superellipsoids: scenes without obstacles");
-        if (n_sph > 0) return h->fail(SCOPI_GPU_EUNSUPPORTED, "spheres and superellipsoids cannot be mixed");
-        if (!p->axes || !p->squareness) return h->fail(SCOPI_GPU_EINVAL, "superellipsoid axes / squareness missing");
-        if (h->P.problem == SCOPI_GPU_VISCOUS || h->P.problem == SCOPI_GPU_VISCOUS_FRICTION)
-            return h->fail(SCOPI_GPU_EUNSUPPORTED, "superellipsoids: NoFriction and Friction problems");
-        if (h->batch) return h->fail(SCOPI_GPU_EUNSUPPORTED, "batches hold sphere scenes");
-        const bool d3 = h->P.dim == 3;  // 2D: (rx, ry) and e
-        for (int i = nin; i < n; ++i) {
-            const double* r = p->axes + 3 * (size_t)i;
-            const double* q = p->squareness + 2 * (size_t)i;
-            if (!(r[0] > 0 && r[1] > 0 && (!d3 || r[2] > 0)) || !(q[0] > 0 && q[0] < 2 && (!d3 || (q[1] > 0 && q[1] < 2))))
-                return h->fail(SCOPI_GPU_EINVAL, "superellipsoid: semi-axes > 0 and squareness in (0, 2)");
-        }
-    }
-    // worms: a link per pair of consecutive active spheres with the same worm index
-    std::vector<int> links;
-    if (p->worm) {
-        for (int i = 0; i < n; ++i) {
-            if (p->worm[i] < 0) continue;
-            if (i < nin || p->shape[i] != SCOPI_GPU_SPHERE)
-                return h->fail(SCOPI_GPU_EINVAL, "worms are runs of active spheres");
-            if (i + 1 < n && p->worm[i + 1] == p->worm[i]) links.push_back(i);
-        }
-        if (!links.empty() && (h->batch || h->P.problem != SCOPI_GPU_NOFRICTION))
-            return h->fail(SCOPI_GPU_EUNSUPPORTED, "worms: single scenes with the NoFriction problem");
-    }
     if (h->periodic) {
-        if (n_se > 0 || !links.empty() || h->batch)
-            return h->fail(SCOPI_GPU_EUNSUPPORTED, "periodic box: single scenes of spheres, no worms");
+        if (h->batch) return h->fail(SCOPI_GPU_EUNSUPPORTED, "periodic box: single scenes of spheres, no worms");
         if ((long long)nin * (n - nin) * (1 + h->P.dim) >= (1LL << 31))
             return h->fail(SCOPI_GPU_EUNSUPPORTED, "obstacles x active bodies and copies must stay below 2^31");
         for (int i = 0; i < nin; ++i) {
@@ -1359,10 +1360,9 @@ static int32_t upload_particles(scopi_gpu_handle* h, const scopi_gpu_particles* 
                                    "periodic box: an obstacle lies within dmax of a periodic lower bound");
         }
     }
-    h->has_se = n_se > 0;
     cudaSetDevice(h->dev);
-    cudaStreamSynchronize(h->stream);
     if (n != h->n || nin != h->nin || h->batch) {
+        cudaStreamSynchronize(h->stream);  // the buffers in use are released
         int rc = h->alloc_bodies(n, nin, obs_cap);
         if (rc) return rc;
         if (h->c_cap == 0) {
@@ -1374,9 +1374,16 @@ static int32_t upload_particles(scopi_gpu_handle* h, const scopi_gpu_particles* 
     }
     cudaStream_t s = h->stream;
     auto up = [&](void* dst, const void* src, size_t bytes) { cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s); };
-    h->n_links = (int)links.size();
-    if (!links.empty()) cudaMemcpy(h->d_links, links.data(), links.size() * sizeof(int), cudaMemcpyHostToDevice);
+    // shapes (and worm indices, staged in the link buffer) first, then their census on the
+    // device while the other fields copy; a container the census refuses leaves the handle
+    // without particles until the next valid upload
     up(h->d_shape, p->shape, n * sizeof(int));
+    if (p->worm) up(h->d_links, p->worm, n * sizeof(int));
+    cudaMemsetAsync(h->d_census, 0, 4 * sizeof(int), s);
+    if (n > 0)
+        k_shape_census<<<(int)std::min<long long>((n + 255) / 256, 8LL * kSMs), 256, 0, s>>>(
+            h->d_shape, p->worm ? h->d_links : nullptr, n, nin, h->P.dim, h->d_census);
+    cudaMemcpyAsync(h->h_census, h->d_census, 4 * sizeof(int), cudaMemcpyDeviceToHost, s);
     up(h->d_pos, p->pos, 3 * (size_t)n * sizeof(double));
     up(h->d_q, p->q, 4 * (size_t)n * sizeof(double));
     up(h->d_v, p->v, 3 * (size_t)n * sizeof(double));
@@ -1388,14 +1395,57 @@ static int32_t upload_particles(scopi_gpu_handle* h, const scopi_gpu_particles* 
     up(h->d_j, p->j, 3 * (size_t)n * sizeof(double));
     up(h->d_radius, p->radius, (size_t)n * sizeof(double));
     up(h->d_length, p->length, (size_t)n * sizeof(double));
-    // semi-axes and squareness are read for superellipsoid scenes only
-    if (n_se > 0) {
-        up(h->d_axes, p->axes, 3 * (size_t)n * sizeof(double));
-        up(h->d_sq, p->squareness, 2 * (size_t)n * sizeof(double));
-    }
     launch_inverse_mass(n, nin, h->P.dim, h->d_m, h->d_j, h->d_invm64, h->d_invm32, h->d_imt64, h->d_imt32, s);
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return h->cuda_fail(e, "set_particles");
+    const int n_se = h->h_census[0], n_sph = h->h_census[1], n_worm = h->h_census[2], bad = h->h_census[3];
+    auto refuse = [&](int code, const char* msg) {
+        h->n = h->nin = h->na = 0;  // the device holds a container that was not accepted
+        return h->fail(code, msg);
+    };
+    if (bad & 1) return refuse(SCOPI_GPU_EINVAL, "unknown shape");
+    if (bad & 2) return refuse(SCOPI_GPU_EUNSUPPORTED, "active bodies must be spheres or superellipsoids");
+    if (bad & 4) return refuse(SCOPI_GPU_EUNSUPPORTED, "superellipsoid obstacles are not supported");
+    if (bad & 8) return refuse(SCOPI_GPU_EUNSUPPORTED, "segments are 2D only");
+    if (n_se > 0) {
+        if (h->P.dim == 2 && nin > 0) return refuse(SCOPI_GPU_EUNSUPPORTED, "2D superellipsoids: scenes without obstacles");
+        if (n_sph > 0) return refuse(SCOPI_GPU_EUNSUPPORTED, "spheres and superellipsoids cannot be mixed");
+        if (!p->axes || !p->squareness) return refuse(SCOPI_GPU_EINVAL, "superellipsoid axes / squareness missing");
+        if (h->P.problem == SCOPI_GPU_VISCOUS || h->P.problem == SCOPI_GPU_VISCOUS_FRICTION)
+            return refuse(SCOPI_GPU_EUNSUPPORTED, "superellipsoids: NoFriction and Friction problems");
+        if (h->batch) return refuse(SCOPI_GPU_EUNSUPPORTED, "batches hold sphere scenes");
+        if (h->periodic) return refuse(SCOPI_GPU_EUNSUPPORTED, "periodic box: single scenes of spheres, no worms");
+        const bool d3 = h->P.dim == 3;  // 2D: (rx, ry) and e
+        for (int i = nin; i < n; ++i) {
+            const double* r = p->axes + 3 * (size_t)i;
+            const double* q = p->squareness + 2 * (size_t)i;
+            if (!(r[0] > 0 && r[1] > 0 && (!d3 || r[2] > 0)) || !(q[0] > 0 && q[0] < 2 && (!d3 || (q[1] > 0 && q[1] < 2))))
+                return refuse(SCOPI_GPU_EINVAL, "superellipsoid: semi-axes > 0 and squareness in (0, 2)");
+        }
+        // semi-axes and squareness are read for superellipsoid scenes only
+        up(h->d_axes, p->axes, 3 * (size_t)n * sizeof(double));
+        up(h->d_sq, p->squareness, 2 * (size_t)n * sizeof(double));
+    }
+    // worms: a link per pair of consecutive active spheres with the same worm index
+    std::vector<int> links;
+    if (n_worm > 0) {
+        for (int i = 0; i < n; ++i) {
+            if (p->worm[i] < 0) continue;
+            if (i < nin || p->shape[i] != SCOPI_GPU_SPHERE) return refuse(SCOPI_GPU_EINVAL, "worms are runs of active spheres");
+            if (i + 1 < n && p->worm[i + 1] == p->worm[i]) links.push_back(i);
+        }
+        if (!links.empty() && (h->batch || h->P.problem != SCOPI_GPU_NOFRICTION))
+            return refuse(SCOPI_GPU_EUNSUPPORTED, "worms: single scenes with the NoFriction problem");
+        if (!links.empty() && h->periodic)
+            return refuse(SCOPI_GPU_EUNSUPPORTED, "periodic box: single scenes of spheres, no worms");
+    }
+    h->has_se = n_se > 0;
+    h->n_links = (int)links.size();
+    if (!links.empty()) up(h->d_links, links.data(), links.size() * sizeof(int));
+    if (n_se > 0 || !links.empty()) {
+        e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return h->cuda_fail(e, "set_particles");
+    }
     return 0;
 }
 
