@@ -153,6 +153,9 @@ struct scopi_gpu_handle {
     bool friction_rows() const { return P.problem == SCOPI_GPU_FRICTION || P.problem == SCOPI_GPU_VISCOUS_FRICTION; }
     bool viscous_friction() const { return P.problem == SCOPI_GPU_VISCOUS_FRICTION; }
     bool fp_loop() const { return fixed_point || viscous_friction(); }
+    // the viscous problems carry each contact's gamma from the previous list by (i, j)
+    // (transfer, solver.hpp:241-258); the others never read it (it stays at its default)
+    bool carries_gamma() const { return P.problem == SCOPI_GPU_VISCOUS || viscous_friction(); }
     bool mixed() const { return P.precision == SCOPI_GPU_MIXED; }
     // Normal-only problems: every pair type of the hot path (sphere-sphere, sphere-plane,
     // sphere-segment) has its lever arm along the normal, so the rotational Jacobian terms
@@ -630,7 +633,8 @@ struct scopi_gpu_handle {
         }
         launch_geometry(eb, sp, ext, d_sizes_cur, c_cap, nullptr, nullptr, c_cap, stream);
         launch_periodic_remap(n, P.dim, box, gb, ext, cur, pw, d_sizes_cur, c_cap, d_gcount + 1, dw.scan_work, stream);
-        launch_transfer(sp, cur, d_sizes_cur, old, has_old ? &d_sizes_old->C : nullptr, c_cap, stream);
+        launch_transfer(sp, cur, d_sizes_cur, old, (has_old && carries_gamma()) ? &d_sizes_old->C : nullptr, c_cap,
+                        stream);
         if (assemble) {
             launch_assemble(b, sp, cur, as, d_sizes_cur, c_cap, dw.scan_work, dw.tmp_total + 2, stream);
             launch_incidence(b, sp, cur, as, inc, d_sizes_cur, c_cap, dw.scan_work, dw.tmp_total + 2, stream,
@@ -671,7 +675,8 @@ struct scopi_gpu_handle {
         // the step's list is the contact method's plus the worm links (compute_contacts,
         // solver.hpp:358-367); detection alone (assemble == false) is the contact method's
         if (assemble && n_links > 0) launch_append_links(h_sizes->C, n_links, d_links, cur, d_sizes_cur, stream);
-        launch_geometry(b, sp, cur, d_sizes_cur, c_cap, has_old ? &old : nullptr, has_old ? &d_sizes_old->C : nullptr,
+        const bool tr = has_old && carries_gamma();
+        launch_geometry(b, sp, cur, d_sizes_cur, c_cap, tr ? &old : nullptr, tr ? &d_sizes_old->C : nullptr,
                         c_cap, stream);
         if (has_se) {
             // the search kept bounding-sphere candidates: the pairs that can touch (gap along
