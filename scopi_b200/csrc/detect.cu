@@ -490,6 +490,124 @@ __global__ void k_pair_search(Bodies B, StepParams p, const Grid* grid, const in
     }
 }
 
+// Offset o of the half stencil: o = 0 the own cell, then the (dz, dy, dx) > (0, 0, 0) in
+// lexicographic order (13 in 3D, 4 in 2D).
+template <int DIM>
+__device__ __forceinline__ void half_stencil(int o, int& dx, int& dy, int& dz) {
+    dx = dy = dz = 0;
+    if (o == 0) return;
+    const int q = o - 1;
+    if (DIM == 3) {
+        if (q == 0) {
+            dx = 1;
+        } else if (q < 4) {
+            dy = 1;
+            dx = q - 2;
+        } else {
+            dz = 1;
+            dy = (q - 4) / 3 - 1;
+            dx = (q - 4) % 3 - 1;
+        }
+    } else {
+        if (q == 0) {
+            dx = 1;
+        } else {
+            dy = 1;
+            dx = q - 2;
+        }
+    }
+}
+
+// The same pairs as k_pair_search, one warp per cell: the candidate pairs of the cell with
+// itself (a < b by slot) and with its half-stencil neighbours are numbered, the warp's lanes
+// take them 32 at a time (so the uneven cell counts do not idle lanes), and each is tested and
+// emitted exactly as k_pair_search does (lower index first, atomic row slot).
+constexpr int kSearchWarps = 8;
+template <int DIM>
+__global__ void __launch_bounds__(32 * kSearchWarps) k_pair_search_cells(Bodies B, StepParams p, const Grid* grid,
+                                                                        const int* cell_start, const int* cell_body,
+                                                                        const double4* cell_pr, int* row_count,
+                                                                        int* row_tmp) {
+    constexpr int nst = DIM == 3 ? 14 : 5;
+    __shared__ int s_pref[kSearchWarps][16], s_beg[kSearchWarps][16], s_cnt[kSearchWarps][16];
+    const Grid g = *grid;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const long long nwarps = (long long)gridDim.x * kSearchWarps;
+    for (long long cid = (long long)blockIdx.x * kSearchWarps + w; cid < g.ncell; cid += nwarps) {
+        const int h0 = cell_start[cid], nh = cell_start[cid + 1] - h0;
+        if (nh == 0) continue;  // the whole warp
+        int cc[3];
+        cell_coords(g, (int)cid, cc);
+        int cnt = 0, beg = 0, ncb = 0;
+        if (lane < nst) {
+            if (lane == 0) {
+                beg = h0;
+                ncb = nh;
+                cnt = nh * (nh - 1) / 2;
+            } else {
+                int dx, dy, dz;
+                half_stencil<DIM>(lane, dx, dy, dz);
+                const int x = cc[0] + dx, y = cc[1] + dy, z = cc[2] + dz;
+                if (x >= 0 && x < g.nc[0] && y >= 0 && y < g.nc[1] && z < g.nc[2]) {
+                    const int c2 = (z * g.nc[1] + y) * g.nc[0] + x;
+                    beg = cell_start[c2];
+                    ncb = cell_start[c2 + 1] - beg;
+                    cnt = nh * ncb;
+                }
+            }
+        }
+        int incl = cnt;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += v;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        if (lane < 16) {
+            s_pref[w][lane] = incl - cnt;
+            s_beg[w][lane] = beg;
+            s_cnt[w][lane] = ncb;
+        }
+        __syncwarp();
+        for (int t = lane; t < total; t += 32) {
+            int lo = 0, hi = nst - 1;  // the last offset whose pairs start at or before t
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (s_pref[w][mid] <= t)
+                    lo = mid;
+                else
+                    hi = mid - 1;
+            }
+            int l = t - s_pref[w][lo];
+            int sa, sb;
+            if (lo == 0) {
+                int i = 0;
+                while (l >= nh - 1 - i) {
+                    l -= nh - 1 - i;
+                    ++i;
+                }
+                sa = h0 + i;
+                sb = h0 + i + 1 + l;
+            } else {
+                const int n2 = s_cnt[w][lo];
+                const int ia = l / n2;
+                sa = h0 + ia;
+                sb = s_beg[w][lo] + (l - ia * n2);
+            }
+            const int a = cell_body[sa], b = cell_body[sb];
+            if (B.scene && B.scene[a] != B.scene[b]) continue;
+            const double4 A = cell_pr[sa], Bb = cell_pr[sb];
+            const bool a_lo = a < b;
+            if (!pair_in_contact<DIM>(p, a_lo ? A : Bb, a_lo ? Bb : A)) continue;
+            const int lo_b = a_lo ? a : b, hi_b = a_lo ? b : a;
+            const int r = lo_b - B.nin;
+            const int slot = atomicAdd(&row_count[r], 1);
+            if (slot < kRowCap) row_tmp[(long long)r * kRowCap + slot] = hi_b;
+        }
+        __syncwarp();  // the tables are rewritten for the next cell
+    }
+}
+
 // Rows in place: (ci, cj) of row r at c_obs + row_ptr[r]; a row whose partners did not fit
 // its scratch is enumerated again over the full stencil by its thread.
 template <int DIM>
@@ -1119,12 +1237,14 @@ void launch_detect(const Bodies& b, const StepParams& p, DetectWork& w, Contacts
         k_cell_scatter<<<blocks_for(na), kThreads, 0, s>>>(b, w.cell_of, w.cell_start, w.cell_fill, w.cell_body,
                                                            w.cell_pr);
         cudaMemsetAsync(w.row_count, 0, (na + 1) * sizeof(int), s);
+        // one warp per cell over the cell capacity (the kernel stops at the grid's cell count)
+        const int sb = blocks_for(w.cell_cap, kSearchWarps);
         if (p.dim == 3)
-            k_pair_search<3><<<blocks_for(na, 128), 128, 0, s>>>(b, p, w.grid, w.cell_of, w.cell_start, w.cell_body,
-                                                                 w.cell_pr, w.row_count, w.row_tmp);
+            k_pair_search_cells<3><<<sb, 32 * kSearchWarps, 0, s>>>(b, p, w.grid, w.cell_start, w.cell_body, w.cell_pr,
+                                                                   w.row_count, w.row_tmp);
         else
-            k_pair_search<2><<<blocks_for(na, 128), 128, 0, s>>>(b, p, w.grid, w.cell_of, w.cell_start, w.cell_body,
-                                                                 w.cell_pr, w.row_count, w.row_tmp);
+            k_pair_search_cells<2><<<sb, 32 * kSearchWarps, 0, s>>>(b, p, w.grid, w.cell_start, w.cell_body, w.cell_pr,
+                                                                   w.row_count, w.row_tmp);
         LAUNCHED(3);
     }
     // obstacle rows come first in (i, j) order
