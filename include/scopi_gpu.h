@@ -201,6 +201,14 @@ int32_t scopi_gpu_get_stats(scopi_gpu_handle* h, scopi_gpu_stats* out);
 int32_t scopi_gpu_amat(scopi_gpu_handle* h, const double* u, double* out);
 int32_t scopi_gpu_atmat(scopi_gpu_handle* h, const double* f, double* out);
 
+/* Start angles (a1, b1, a2, b2) of the 3D superellipsoid-superellipsoid closest-point solves
+   of the last detection (closest_points.hpp:604-668), 4 per row of the candidate list: the
+   pairs that passed the bounding-sphere and support-gap tests, in (i, j) order, before the
+   dij < dmax filter; *n = the rows of that list.  Obstacle rows (first, solved in closed
+   form) hold no start.  For checking each pair's solve against another implementation from
+   the same start; no counterpart in the reference. */
+int32_t scopi_gpu_get_se_starts(scopi_gpu_handle* h, int64_t cap, int64_t* n, double* u);
+
 /* The contact list AMatrix / ATMatrix are built on (AMatrix(contacts, particles),
    matrix/velocities.hpp:54-66): replaces the handle's current contact list (the one
    scopi_gpu_get_contacts returns and scopi_gpu_amat / scopi_gpu_atmat use) with n records;

@@ -91,6 +91,10 @@ def lib():
         L.orc_se_plane_residual.argtypes = [P, P, P, P]
         L.orc_se_se_hybrid.restype = C.c_int
         L.orc_se_se_hybrid.argtypes = [P, P, P, C.POINTER(C.c_int)]
+        L.orc_se_se_from.restype = C.c_int
+        L.orc_se_se_from.argtypes = [P, P, P, P]
+        L.orc_se_se_start.restype = None
+        L.orc_se_se_start.argtypes = [P, P, P]
         L.orc_se2_se2.restype = C.c_int
         L.orc_se2_se2.argtypes = [P, P, P]
         L.orc_se2_hybrid.restype = C.c_int
@@ -276,6 +280,25 @@ def hybrid_solve2(s1, s2, u0):
     a, b = np.ascontiguousarray(s1, float), np.ascontiguousarray(s2, float)
     info = lib().orc_se2_hybrid(_dp(a), _dp(b), _dp(u), C.byref(nfev))
     return {"u": u, "info": info, "nfev": nfev.value}
+
+
+def se_se_from(s1, s2, u0):
+    """closest_points(superellipsoid<3>, superellipsoid<3>) with the solve started from u0."""
+    out = np.zeros(15)
+    a, b = np.ascontiguousarray(s1, float), np.ascontiguousarray(s2, float)
+    uu = np.ascontiguousarray(u0, float)
+    info = lib().orc_se_se_from(_dp(a), _dp(b), _dp(uu), _dp(out))
+    r = _unpack(out)
+    r["info"] = info
+    return r
+
+
+def se_se_start(s1, s2):
+    """Start (a1, b1, a2, b2) of the SE-SE solve: the first minimum of the start criterion."""
+    u = np.zeros(4)
+    a, b = np.ascontiguousarray(s1, float), np.ascontiguousarray(s2, float)
+    lib().orc_se_se_start(_dp(a), _dp(b), _dp(u))
+    return u
 
 
 def hybrid_solve(s1, s2, u0):

@@ -1282,6 +1282,16 @@ int orc_se_plane(const double* s, const double* plane, double* out) {
     return o.info;
 }
 
+int orc_se_se_from(const double* s1, const double* s2, const double* u0, double* out) {
+    const orc_se::PairOut o = orc_se::se_se(se_from(s1), se_from(s2), u0);
+    write_pair(o, out);
+    return o.info;
+}
+
+void orc_se_se_start(const double* s1, const double* s2, double* u0) {
+    orc_se::sese_start(se_from(s1), se_from(s2), u0);
+}
+
 int orc_se_se_hybrid(const double* s1, const double* s2, double* u, int* nfev) {
     const orc_se::SE a = se_from(s1), b = se_from(s2);
     const orc_se::HybrResult h = orc_se::hybrj<4>([&](const double* x, double* F) { orc_se::sese_F(a, b, x, F); },

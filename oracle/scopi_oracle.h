@@ -127,6 +127,10 @@ int orc_se_se(const double* s1, const double* s2, double* out);
 int orc_se_plane(const double* s, const double* plane, double* out);
 /* The hybrid method alone from the start u (in/out); returns info, *nfev its function count. */
 int orc_se_se_hybrid(const double* s1, const double* s2, double* u, int* nfev);
+/* start of the SE-SE solve: the grid argmin of closest_points.hpp:604-668 (angles a1, b1, a2, b2) */
+void orc_se_se_start(const double* s1, const double* s2, double* u0);
+/* the SE-SE closest points with the solve started from u0 instead of the grid argmin */
+int orc_se_se_from(const double* s1, const double* s2, const double* u0, double* out);
 /* F and the analytic Jacobian (column-major) of the SE-SE system at u, for cross-checks;
    the SE-plane residual (with the body's side as its sign) at u = (a, b, plane coords). */
 void orc_se_plane_residual(const double* s, const double* plane, const double* u, double* F);

@@ -600,10 +600,14 @@ inline void sese_start(const SE& s1, const SE& s2, double* u0) {
     u0[3] = U2[bj][1];
 }
 
-// closest_points(superellipsoid<3>, superellipsoid<3>), closest_points.hpp:263-733
-inline PairOut se_se(const SE& s1, const SE& s2) {
+// closest_points(superellipsoid<3>, superellipsoid<3>), closest_points.hpp:263-733; from a
+// given start u0 when it is not null (to compare a solve with another one's from its start)
+inline PairOut se_se(const SE& s1, const SE& s2, const double* u0 = nullptr) {
     double u[4];
-    sese_start(s1, s2, u);
+    if (u0)
+        for (int k = 0; k < 4; ++k) u[k] = u0[k];
+    else
+        sese_start(s1, s2, u);
     const HybrResult h = hybrj<4>([&](const double* x, double* F) { sese_F(s1, s2, x, F); },
                                   [&](const double* x, double* J) { sese_J(s1, s2, x, J); }, u);
     PairOut o;

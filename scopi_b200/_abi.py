@@ -24,7 +24,7 @@ EXPORTED = [
     "scopi_gpu_last_error", "scopi_gpu_kernel_launches", "scopi_gpu_get_stream", "scopi_gpu_apgd_noalloc",
     "scopi_gpu_batch_create", "scopi_gpu_batch_get_scene", "scopi_gpu_batch_get_scene_stats",
     "scopi_gpu_batch_block_threads", "scopi_gpu_batch_set_block_threads", "scopi_gpu_test_barrier_stall",
-    "scopi_gpu_set_contacts",
+    "scopi_gpu_set_contacts", "scopi_gpu_get_se_starts",
 ]
 
 
@@ -115,6 +115,8 @@ def load(path: str = LIB_PATH):
     L.scopi_gpu_batch_block_threads.restype = C.c_int32
     L.scopi_gpu_batch_set_block_threads.argtypes = [H, C.c_int32]
     L.scopi_gpu_batch_set_block_threads.restype = C.c_int32
+    L.scopi_gpu_get_se_starts.argtypes = [H, C.c_int64, I64, D]
+    L.scopi_gpu_get_se_starts.restype = C.c_int32
     L.scopi_gpu_set_contacts.argtypes = [H, C.c_int64, I64, I64, D, D, D, D]
     L.scopi_gpu_set_contacts.restype = C.c_int32
     L.scopi_gpu_test_barrier_stall.argtypes = [H]

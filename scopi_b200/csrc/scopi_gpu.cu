@@ -117,6 +117,7 @@ struct scopi_gpu_handle {
     ApgdResult* h_result = nullptr;    // pinned
     unsigned long long* h_viol = nullptr;
     unsigned int* h_bar = nullptr;     // pinned: the four barrier words written before a launch
+    int* h_se_cand = nullptr;          // pinned: superellipsoid candidate pairs of the last detection
     int* d_census = nullptr;           // shape census of an upload (k_shape_census)
     int* h_census = nullptr;           // pinned copy
     bool stall_next = false;           // scopi_gpu_test_barrier_stall: withhold one arrival once
@@ -477,6 +478,8 @@ struct scopi_gpu_handle {
         if ((e = cudaMallocHost(&h_bar, 4 * sizeof(unsigned int))) != cudaSuccess)
             return cuda_fail(e, "cudaMallocHost");
         if ((e = alloc(fixed_mem, d_census, 4)) != cudaSuccess) return cuda_fail(e, "alloc");
+        if ((e = cudaMallocHost(&h_se_cand, sizeof(int))) != cudaSuccess) return cuda_fail(e, "cudaMallocHost");
+        *h_se_cand = 0;
         if ((e = cudaMallocHost(&h_census, 4 * sizeof(int))) != cudaSuccess) return cuda_fail(e, "cudaMallocHost");
         h_bar[0] = h_bar[1] = h_bar[2] = 0u;
         h_bar[3] = P.barrier_timeout_us > 0 ? (unsigned int)P.barrier_timeout_us : 0u;
@@ -687,6 +690,7 @@ struct scopi_gpu_handle {
                                 dw.tmp_total + 2, stream);
             std::swap(cur, old);
             launch_se_pairs(P.dim, b, cur, d_sizes_cur, d_se_u, dw.tmp_total + 3, 3 * kSMs, stream);
+            cudaMemcpyAsync(h_se_cand, &d_sizes_cur->C, sizeof(int), cudaMemcpyDeviceToHost, stream);
             launch_se_filter(cur, old, d_sizes_cur, P.dmax, c_cap, d_se_keep, d_se_pos, dw.scan_work,
                              dw.tmp_total + 2, stream);
             std::swap(cur, old);
@@ -1252,6 +1256,7 @@ int32_t scopi_gpu_destroy(scopi_gpu_handle* h) {
     if (h->h_viol) cudaFreeHost(h->h_viol);
     if (h->h_bar) cudaFreeHost(h->h_bar);
     if (h->h_census) cudaFreeHost(h->h_census);
+    if (h->h_se_cand) cudaFreeHost(h->h_se_cand);
     if (h->h_fp_part) cudaFreeHost(h->h_fp_part);
     if (h->h_gcount) cudaFreeHost(h->h_gcount);
     for (auto& x : h->ev)
@@ -1580,6 +1585,21 @@ int32_t scopi_gpu_amat(scopi_gpu_handle* h, const double* u, double* out) {
     cudaFree(dout);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return h->cuda_fail(e, "amat");
+    return 0;
+}
+
+int32_t scopi_gpu_get_se_starts(scopi_gpu_handle* h, int64_t cap, int64_t* n, double* u) {
+    if (!h) return SCOPI_GPU_EINVAL;
+    cudaSetDevice(h->dev);
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return h->cuda_fail(e, "get_se_starts");
+    const long long cand = h->has_se ? *h->h_se_cand : 0;
+    if (n) *n = cand;
+    const long long k = std::min<long long>(cand, cap);
+    if (k > 0 && u) {
+        e = cudaMemcpy(u, h->d_se_u, 4 * k * sizeof(double), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return h->cuda_fail(e, "get_se_starts");
+    }
     return 0;
 }
 
