@@ -93,6 +93,8 @@ def lib():
         L.orc_se_se_hybrid.argtypes = [P, P, P, C.POINTER(C.c_int)]
         L.orc_se_se_from.restype = C.c_int
         L.orc_se_se_from.argtypes = [P, P, P, P]
+        L.orc_se_se_start_value.restype = C.c_double
+        L.orc_se_se_start_value.argtypes = [P, P, P]
         L.orc_se_se_start.restype = None
         L.orc_se_se_start.argtypes = [P, P, P]
         L.orc_se2_se2.restype = C.c_int
@@ -291,6 +293,13 @@ def se_se_from(s1, s2, u0):
     r = _unpack(out)
     r["info"] = info
     return r
+
+
+def se_se_start_value(s1, s2, u):
+    """The start criterion |p1 - p2| + 2 (1 + n1.n2) of the SE-SE solve at angles u."""
+    a, b = np.ascontiguousarray(s1, float), np.ascontiguousarray(s2, float)
+    uu = np.ascontiguousarray(u, float)
+    return float(lib().orc_se_se_start_value(_dp(a), _dp(b), _dp(uu)))
 
 
 def se_se_start(s1, s2):

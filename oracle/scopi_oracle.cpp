@@ -1288,6 +1288,14 @@ int orc_se_se_from(const double* s1, const double* s2, const double* u0, double*
     return o.info;
 }
 
+double orc_se_se_start_value(const double* s1, const double* s2, const double* u) {
+    const orc_se::SE a = se_from(s1), b = se_from(s2);
+    const orc_se::V3 p1 = orc_se::point(a, u[0], u[1]), n1 = orc_se::normal(a, u[0], u[1]);
+    const orc_se::V3 p2 = orc_se::point(b, u[2], u[3]), n2 = orc_se::normal(b, u[2], u[3]);
+    const orc_se::V3 df = {p1[0] - p2[0], p1[1] - p2[1], p1[2] - p2[2]};
+    return orc_se::norm(df) + 2 * (1 + orc_se::dot(n1, n2));
+}
+
 void orc_se_se_start(const double* s1, const double* s2, double* u0) {
     orc_se::sese_start(se_from(s1), se_from(s2), u0);
 }

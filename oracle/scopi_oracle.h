@@ -129,6 +129,8 @@ int orc_se_plane(const double* s, const double* plane, double* out);
 int orc_se_se_hybrid(const double* s1, const double* s2, double* u, int* nfev);
 /* start of the SE-SE solve: the grid argmin of closest_points.hpp:604-668 (angles a1, b1, a2, b2) */
 void orc_se_se_start(const double* s1, const double* s2, double* u0);
+/* the start criterion |p1 - p2| + 2 (1 + n1.n2) at angles u (closest_points.hpp:654-660) */
+double orc_se_se_start_value(const double* s1, const double* s2, const double* u);
 /* the SE-SE closest points with the solve started from u0 instead of the grid argmin */
 int orc_se_se_from(const double* s1, const double* s2, const double* u0, double* out);
 /* F and the analytic Jacobian (column-major) of the SE-SE system at u, for cross-checks;

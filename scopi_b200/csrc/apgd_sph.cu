@@ -167,13 +167,26 @@ struct SphState {
 // and the gathers that depend on a staged record (u(y) of the contact's bodies) are issued
 // one trip ahead.  The incidence records stay on plain loads: a body's records share L1
 // lines, which an L1-bypassing copy would fetch again from L2 for every record.
+// Launch shape per precision: threads per block, contact-pass stages GC (the u(y) gathers
+// of trip k + GD are issued during trip k: an L2 round trip is about one trip long),
+// particle-pass stages GP.
+template <typename T>
+struct SphShape;
+template <>
+struct SphShape<float> {
+    static constexpr int threads = 768, GC = 5, GD = 2, GP = 4;
+};
+template <>
+struct SphShape<double> {
+    static constexpr int threads = 512, GC = 4, GD = 2, GP = 4;
+};
 template <typename T>
 struct SphOcc {
-    static constexpr int threads = sizeof(T) == 4 ? 1024 : 512;
-    static constexpr int GS = 4;  // pipeline stages
-    static constexpr size_t contact_bytes = (size_t)GS * threads * (sizeof(int2) + sizeof(V4<T>) + 2 * sizeof(T));
+    static constexpr int threads = SphShape<T>::threads;
+    static constexpr int GC = SphShape<T>::GC, GD = SphShape<T>::GD, GP = SphShape<T>::GP;
+    static constexpr size_t contact_bytes = (size_t)GC * threads * (sizeof(int2) + sizeof(V4<T>) + 2 * sizeof(T));
     static constexpr size_t particle_bytes =
-        (size_t)GS * threads * ((sizeof(T) == 4 ? 2 : 1) * sizeof(V4<T>) + sizeof(T) + 2 * sizeof(int));
+        (size_t)GP * threads * ((sizeof(T) == 4 ? 2 : 1) * sizeof(V4<T>) + sizeof(T) + 2 * sizeof(int));
     static constexpr size_t smem = contact_bytes > particle_bytes ? contact_bytes : particle_bytes;
 };
 
@@ -181,19 +194,20 @@ template <typename T, int DIM, int PROB>
 __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A) {
     __shared__ SphState S;
     extern __shared__ __align__(32) unsigned char sph_dyn[];
-    constexpr int GS = SphOcc<T>::GS;
+    constexpr int GC = SphOcc<T>::GC, GD = SphOcc<T>::GD, GP = SphOcc<T>::GP;
+    static_assert(GD >= 1 && GD <= GC - 2, "the gathered records must be in the prologue's stages");
     const int NT = blockDim.x, tid = threadIdx.x;
-    // contact-pass stages [GS][NT] of each field
+    // contact-pass stages [GC][NT] of each field
     V4<T>* s_nc = reinterpret_cast<V4<T>*>(sph_dyn);
-    int2* s_ij = reinterpret_cast<int2*>(s_nc + GS * NT);
-    T* s_l = reinterpret_cast<T*>(s_ij + GS * NT);
-    T* s_lp = s_l + GS * NT;
-    // particle-pass stages (same memory)
+    int2* s_ij = reinterpret_cast<int2*>(s_nc + GC * NT);
+    T* s_l = reinterpret_cast<T*>(s_ij + GC * NT);
+    T* s_lp = s_l + GC * NT;
+    // particle-pass stages [GP][NT] (same memory)
     V4<T>* s_ul = reinterpret_cast<V4<T>*>(sph_dyn);
-    V4<T>* s_uy = s_ul + GS * NT;  // FP32 only
-    T* s_im = reinterpret_cast<T*>(s_ul + (sizeof(T) == 4 ? 2 : 1) * GS * NT);
-    int* s_p0 = reinterpret_cast<int*>(s_im + GS * NT);
-    int* s_p1 = s_p0 + GS * NT;
+    V4<T>* s_uy = s_ul + GP * NT;  // FP32 only
+    T* s_im = reinterpret_cast<T*>(s_ul + (sizeof(T) == 4 ? 2 : 1) * GP * NT);
+    int* s_p0 = reinterpret_cast<int*>(s_im + GP * NT);
+    int* s_p1 = s_p0 + GP * NT;
     if (threadIdx.x == 0) {
         S.alpha = A.alpha;
         S.lipsch = 1.0 / A.alpha;
@@ -225,8 +239,8 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
     // First stages of each pass are issued before the grid barrier that precedes the pass
     // when they do not depend on it: a contact's geometry (n, c), (ci, cj), and a body's
     // inc_ptr, 1/m, u(l), u(y).  Uncommitted copies join the next commit group.
-    auto issue_geom = [&](long long k) {
-        const int sl = (int)(k % GS) * NT + tid;
+    auto issue_geom = [&](int k) {
+        const int sl = (k % GC) * NT + tid;
         const long long c = base + k * S_;
         const bool on = k < ntrip_c && c < C;
         const long long cc = on ? c : 0;
@@ -234,7 +248,7 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
         cp8(s_ij + sl, A.cij + cc, on);
     };
     auto issue_body = [&](long long k, const V4<T>* uL, const V4<T>* uY, bool with_ul) {
-        const int sl = (int)(k % GS) * NT + tid;
+        const int sl = (int)(k % GP) * NT + tid;
         const long long p = base + k * S_;
         const bool on = k < ntrip_p && p < A.na;
         const long long pp = on ? p : 0;
@@ -325,25 +339,25 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
         {
             double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
             // ---- contact pass: g = dt^2 n.(u_i(y) - u_j(y)) + c, l+ = P(y - alpha g)
-            const long long ntrip = ntrip_c;
-            auto issue_lam = [&](long long k) {
-                const int sl = (int)(k % GS) * NT + tid;
-                const long long c = base + k * S_;
+            const int ntrip = (int)ntrip_c;
+            auto issue_lam = [&](int k) {
+                const int sl = (k % GC) * NT + tid;
+                const long long c = base + (long long)k * S_;
                 const bool on = k < ntrip && c < C;
                 const long long cc = on ? c : 0;
                 cp_val(s_l + sl, lam + cc, on);
                 cp_val(s_lp + sl, lprev + cc, on && use_prev);
             };
-            auto issue = [&](long long k) {
+            auto issue = [&](int k) {
                 issue_geom(k);
                 issue_lam(k);
                 cp_commit();
             };
             // u(y) of the contact's two bodies (written by other blocks: L2 loads)
-            auto gather = [&](long long k, T* g) {
-                const int sl = (int)(k % GS) * NT + tid;
+            auto gather = [&](int k, T* g) {
+                const int sl = (k % GC) * NT + tid;
                 const int2 ij = s_ij[sl];
-                const bool on = k < ntrip && base + k * S_ < C;
+                const bool on = k < ntrip && base + (long long)k * S_ < C;
                 V4<T> ui, uj;
                 ui.x = ui.y = ui.z = uj.x = uj.y = uj.z = (T)0;
                 if (on && ij.x >= A.nin) ui = ld4cg(uY + (ij.x - A.nin));
@@ -351,35 +365,36 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
                 g[0] = ui.x; g[1] = ui.y; g[2] = ui.z;
                 g[3] = uj.x; g[4] = uj.y; g[5] = uj.z;
             };
-            // prologue: the geometry of stages 0..GS-2 in one group (issued before the
+            // prologue: the geometry of stages 0..GC-2 in one group (issued before the
             // last barrier when geom_issued), then their multipliers one group per stage
             if (!geom_issued)
 #pragma unroll 1
-                for (int k = 0; k < GS - 1; ++k) issue_geom(k);
+                for (int k = 0; k < GC - 1; ++k) issue_geom(k);
             cp_commit();
             geom_issued = false;
 #pragma unroll 1
-            for (int k = 0; k < GS - 1; ++k) {
+            for (int k = 0; k < GC - 1; ++k) {
                 issue_lam(k);
                 cp_commit();
             }
-            cp_wait<GS - 2>();
-            // trip k computes with the gathers issued during trip k-1
-            T gc[6], gn[6];
-            gather(0, gc);
-#pragma unroll 1
-            for (long long k = 0; k < ntrip; ++k) {
-                issue(k + GS - 1);
-                cp_wait<GS - 2>();  // stage k+1 has landed
-                gather(k + 1, gn);
-                const long long c = base + k * S_;
-                if (c < C) {
-                    const int sl = (int)(k % GS) * NT + tid;
+            cp_wait<GC - 2>();
+            // trip k: commit stage k + GC - 1, wait for stage k + GD, gather trip k + GD's
+            // u(y), then compute trip k with the u(y) gathered GD trips ago.  Three register
+            // sets in rotation (the loop unrolled by three) so that no gather is forced to
+            // complete before its own trip.
+            static_assert(GD == 2, "three gather sets in rotation");
+            auto trip = [&](int k, const T* g, T* fill) {
+                issue(k + GC - 1);
+                cp_wait<GC - 1 - GD>();  // stages up to k + GD have landed
+                gather(k + GD, fill);
+                const long long c = base + (long long)k * S_;
+                if (k < ntrip && c < C) {
+                    const int sl = (k % GC) * NT + tid;
                     const V4<T> nc = s_nc[sl];
                     // bodies below nin (obstacles) gathered as zeros: same sum as skipping them
                     T qy = 0;
-                    qy += nc.x * gc[0] + nc.y * gc[1] + (DIM == 3 ? nc.z * gc[2] : (T)0);
-                    qy -= nc.x * gc[3] + nc.y * gc[4] + (DIM == 3 ? nc.z * gc[5] : (T)0);
+                    qy += nc.x * g[0] + nc.y * g[1] + (DIM == 3 ? nc.z * g[2] : (T)0);
+                    qy -= nc.x * g[3] + nc.y * g[4] + (DIM == 3 ? nc.z * g[5] : (T)0);
                     qy *= (T)A.dt2;
                     mult_update_v<T>(A, c, qy, nc.w, s_l[sl], s_lp[sl], lnew, beta, use_prev, bt, alpha, s);
                     if (PROB == kViscous) {
@@ -387,8 +402,15 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
                         if (sv >= 0) mult_update<T>(A, sv, -qy, -nc.w, lam, lprev, lnew, beta, use_prev, bt, alpha, s);
                     }
                 }
-#pragma unroll
-                for (int q = 0; q < 6; ++q) gc[q] = gn[q];
+            };
+            T g0[6], g1[6], g2[6];
+            gather(0, g0);
+            gather(1, g1);
+#pragma unroll 1
+            for (int k = 0; k < ntrip; k += 3) {
+                trip(k, g0, g2);
+                trip(k + 1, g1, g0);
+                trip(k + 2, g2, g1);
             }
             cp_wait<0>();
             // block partials to thread 0, grid barrier and grid sum in warp 0 only
@@ -404,7 +426,7 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
             {
                 const V4<T>* uL0 = pick4(S.jL, A.u0, A.u1, A.u2, A.u3);
 #pragma unroll 1
-                for (int k = 0; k < GS - 1; ++k) issue_body(k, uL0, uY, true);
+                for (int k = 0; k < GP - 1; ++k) issue_body(k, uL0, uY, true);
             }
             if (tid < 32) {
                 bool ok = true;
@@ -445,14 +467,14 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
             // are issued in batches so several loads are in flight per thread
             constexpr int KB = 4;
             const long long ntrip = ntrip_p;
-            // stages 0..GS-2 were issued before the barrier
+            // stages 0..GP-2 were issued before the barrier
 #pragma unroll 1
             for (long long kt = 0; kt < ntrip; ++kt) {
-                issue_body(kt + GS - 1, uL, uY, bn_ != (T)0);
-                cp_wait<GS - 1>();  // stage kt has landed
+                issue_body(kt + GP - 1, uL, uY, bn_ != (T)0);
+                cp_wait<GP - 1>();  // stage kt has landed
                 const long long p = base + kt * S_;
                 if (p >= A.na) continue;
-                const int sl = (int)(kt % GS) * NT + tid;
+                const int sl = (int)(kt % GP) * NT + tid;
                 T w0 = 0, w1 = 0, w2 = 0;
                 const int k0 = s_p0[sl], k1 = s_p1[sl];
                 for (int kb = k0; kb < k1; kb += KB) {
@@ -515,7 +537,7 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
             }
             // the next iteration's first contact geometry, while the barrier waits
 #pragma unroll 1
-            for (int k = 0; k < GS - 1; ++k) issue_geom(k);
+            for (int k = 0; k < GC - 1; ++k) issue_geom(k);
             geom_issued = true;
             bool ok = true;
             double t6[2];

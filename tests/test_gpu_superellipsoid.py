@@ -5,8 +5,8 @@ The reference's superellipsoid-superellipsoid solve (hybrd1 on a poorly scaled s
 last equation has a double root) converges (MINPACK info 1) for most pairs and stops on
 slow progress (info 4) for the others, some of them away from the root: there the result
 depends on the last bits of the arithmetic, so the GPU (CUDA's pow/sin/cos) and the oracle
-(glibc) agree to ~1e-12 on converged pairs and only approximately on the others.  The tests
-hold converged pairs to 1e-9 and bound the rest."""
+(glibc) agree to ~1e-12 on converged pairs; on the others the agreement is bounded by that
+pair's own sensitivity to the last bit of its inputs, measured on the oracle."""
 import math
 
 import numpy as np
@@ -43,24 +43,65 @@ def pair_scene(rng):
     return p.finalize(), [orc.se_record(*b) for b in bodies]
 
 
+def _gpu_start(solver):
+    """Start angles of the GPU's solve of the scene's single pair (scopi_gpu_get_se_starts)."""
+    import ctypes as C
+    from scopi_b200 import _abi
+    n = C.c_int64(0)
+    u = np.zeros(4)
+    assert _abi.load().scopi_gpu_get_se_starts(solver._h, 1, C.byref(n), u.ctypes.data_as(C.POINTER(C.c_double))) == 0
+    assert n.value == 1
+    return u
+
+
+def _one_ulp_sensitivity(s1, s2, u0, d0):
+    """How far the oracle's gap moves, solving from u0, when one centre coordinate of either
+    body moves by one ulp: the last-bit sensitivity of that pair's solve."""
+    worst = 0.0
+    for body in (0, 1):
+        for idx in range(3):
+            for direction in (np.inf, -np.inf):
+                t = (s1 if body == 0 else s2).copy()
+                t[idx] = np.nextafter(t[idx], direction)
+                r = orc.se_se_from(t, s2, u0) if body == 0 else orc.se_se_from(s1, t, u0)
+                worst = max(worst, abs(r["dij"] - d0))
+    return worst
+
+
 def test_superellipsoid_pairs_match_the_oracle():
+    """80 random pairs.  Start: the GPU's start is a minimum of the start criterion equal to
+    the oracle's to rounding (which of two equal minima comes first is decided by the last
+    bits: a surface point has the two angle representations (a, b) and (pi - a, b + pi)).
+    Solve: where MINPACK converges the closest points agree to 1e-9.  Where it stops on
+    slow progress (info != 1), the GPU's gap is compared with the oracle's solve from the
+    GPU's start and must lie within ten times that solve's own 1-ulp sensitivity (the
+    oracle's gap change under a 1-ulp move of one input coordinate), and within 5e-5 of the
+    oracle's own solve."""
     rng = np.random.default_rng(11)
-    agree, converged, worst_other = 0, 0, 0.0
-    for _ in range(80):
+    converged, slow = 0, 0
+    for k in range(80):
         pa, (s1, s2) = pair_scene(rng)
-        ref = orc.se_se(s1, s2)
-        c = gpu_solver(pa, dmax=0.05).detect()
+        g = gpu_solver(pa, dmax=0.05)
+        c = g.detect()
         assert list(c["i"]) == [0] and list(c["j"]) == [1]
-        if ref["info"] == 1:
+        u_gpu = _gpu_start(g)
+        g.close()
+        u_or = orc.se_se_start(s1, s2)
+        v_gpu, v_or = orc.se_se_start_value(s1, s2, u_gpu), orc.se_se_start_value(s1, s2, u_or)
+        assert abs(v_gpu - v_or) <= 1e-9 * abs(v_or), (k, v_gpu, v_or)
+        ref = orc.se_se(s1, s2)
+        same = orc.se_se_from(s1, s2, u_gpu)
+        d = c["dij"][0]
+        if ref["info"] == 1 and same["info"] == 1:
             converged += 1
-            if (abs(c["dij"][0] - ref["dij"]) <= 1e-9 and np.allclose(c["pi"][0], ref["pi"], atol=1e-9)
-                    and np.allclose(c["pj"][0], ref["pj"], atol=1e-9)):
-                agree += 1
+            assert abs(d - ref["dij"]) <= 1e-9, (k, d, ref["dij"])
+            assert np.allclose(c["pi"][0], ref["pi"], atol=1e-9) and np.allclose(c["pj"][0], ref["pj"], atol=1e-9), k
         else:
-            worst_other = max(worst_other, abs(c["dij"][0] - ref["dij"]))
-    assert converged >= 15
-    assert agree >= converged - 1, (agree, converged)
-    assert worst_other <= 5e-3
+            slow += 1
+            sens = _one_ulp_sensitivity(s1, s2, u_gpu, same["dij"])
+            assert abs(d - same["dij"]) <= max(1e-9, 10 * sens), (k, d, same["dij"], sens)
+            assert abs(d - ref["dij"]) <= 5e-5, (k, d, ref["dij"])
+    assert converged >= 15 and slow >= 30, (converged, slow)
 
 
 def test_superellipsoid_on_a_plane_matches_the_oracle():
@@ -91,15 +132,17 @@ def pile_kw(pa):
                 problem=FRICTION, kd_tree_radius=configs.se_kd_radius(pa, st["dmax"])), st
 
 
-def test_superellipsoid_pile_contact_set_matches_the_oracle():
-    pa = configs.se_pile(count=64, side=4, seed=3)
+@pytest.mark.parametrize("count,side,seed", [(64, 4, 3), (125, 5, 7), (216, 6, 9)])
+def test_superellipsoid_pile_contact_set_matches_the_oracle(count, side, seed):
+    """The same contact pairs as the oracle, in the same order, and gaps within the bound of
+    the slow-progress pairs."""
+    pa = configs.se_pile(count=count, side=side, seed=seed)
     kw, st = pile_kw(pa)
     g = gpu_solver(pa, **kw).detect()
     o = oracle_solver(pa, **kw).detect()
-    gs = set(zip(g["i"].tolist(), g["j"].tolist()))
-    os_ = set(zip(o["i"].tolist(), o["j"].tolist()))
-    assert len(os_) > 0
-    assert len(gs ^ os_) <= max(1, len(os_) // 50), (sorted(gs - os_), sorted(os_ - gs))
+    assert len(o["i"]) > 0
+    assert np.array_equal(g["i"], o["i"]) and np.array_equal(g["j"], o["j"])
+    assert np.max(np.abs(g["dij"] - o["dij"])) <= 5e-5
 
 
 def test_superellipsoid_pile_steps_like_the_oracle():
