@@ -74,7 +74,8 @@ def test_superellipsoid_pairs_match_the_oracle():
     last bits: a surface point has the two angle representations (a, b) and (pi - a, b + pi),
     whose criterion values differ by the rounding of pi - a, amplified near the poles where
     |cos a| is small; the widest such gap seen is 3e-8 relative).
-    Solve: where MINPACK converges the closest points agree to 1e-9.  Where it stops on
+    Solve: where MINPACK converges from that start the closest points agree to 1e-9 with the
+    oracle's solve from the same start, and to 1e-7 with the oracle's own.  Where it stops on
     slow progress (info != 1), the GPU's gap is compared with the oracle's solve from the
     GPU's start and must lie within ten times that solve's own 1-ulp sensitivity (the
     oracle's gap change under a 1-ulp move of one input coordinate), and within 5e-5 of the
@@ -94,10 +95,16 @@ def test_superellipsoid_pairs_match_the_oracle():
         ref = orc.se_se(s1, s2)
         same = orc.se_se_from(s1, s2, u_gpu)
         d = c["dij"][0]
-        if ref["info"] == 1 and same["info"] == 1:
+        if same["info"] == 1:
+            # converged from the same start: the same iterates to rounding; from the oracle's
+            # own start (possibly the other representation) the double root of F3 leaves the
+            # converged point defined only to ~1e-8
             converged += 1
-            assert abs(d - ref["dij"]) <= 1e-9, (k, d, ref["dij"])
-            assert np.allclose(c["pi"][0], ref["pi"], atol=1e-9) and np.allclose(c["pj"][0], ref["pj"], atol=1e-9), k
+            assert abs(d - same["dij"]) <= 1e-9, (k, d, same["dij"])
+            assert np.allclose(c["pi"][0], same["pi"], atol=1e-9) and np.allclose(c["pj"][0], same["pj"], atol=1e-9), k
+            if ref["info"] == 1:
+                assert abs(d - ref["dij"]) <= 1e-7, (k, d, ref["dij"])
+                assert np.allclose(c["pi"][0], ref["pi"], atol=1e-7) and np.allclose(c["pj"][0], ref["pj"], atol=1e-7), k
         else:
             slow += 1
             sens = _one_ulp_sensitivity(s1, s2, u_gpu, same["dij"])
@@ -148,19 +155,23 @@ def test_superellipsoid_pile_contact_set_matches_the_oracle(count, side, seed):
 
 
 def test_superellipsoid_pile_steps_like_the_oracle():
-    """FP64 with friction, a few steps of the pile: the same contacts as the oracle every
-    step; positions within 2e-5 relative.  Not 1e-9: the pairs where MINPACK stops on slow
-    progress have normals that differ by up to ~1e-2 between the two arithmetics."""
+    """FP64 with friction, the 27-body pile falling onto its floor for 100 steps (contacts from
+    the first step): the same contact pairs as the oracle every step, positions within 1e-9.
+    (At step 114 a slow-progress solve of a touching pair reports a penetration of about a
+    millimetre in both engines, which the solve turns into a kick of several m/s; from there
+    the pile is chaotic and the two runs separate.)"""
     pa = configs.se_pile(count=27, side=3, seed=4)
     kw, st = pile_kw(pa)
     g = gpu_solver(pa, **kw)
     o = oracle_solver(pa, **kw)
-    for k in range(4):
+    for k in range(100):
         g.run(st["dt"], 1)
         o.run(st["dt"], 1)
         gc, oc = g.current_contacts(), o.contacts()
+        assert len(oc["i"]) > 0
         assert np.array_equal(gc["i"], oc["i"]) and np.array_equal(gc["j"], oc["j"]), k
-    assert rel_err(g.particles.pos, o.pa.pos) <= 2e-5
+    assert rel_err(g.particles.pos, o.pa.pos) <= 1e-9
+    assert rel_err(g.particles.v, o.pa.v) <= 1e-6
     assert g.stats()["converged"] == 1
 
 
