@@ -426,7 +426,8 @@ def piles(args, ranks):
         ranks.barrier()
         out = {"ms": ranks.max(e0.elapsed_time(e1)), "launches": b.kernel_launches() - l0, "clocks": clocks,
                "violation_max": viol, "longest_scene_iterations_mean": statistics.mean(iters),
-               "contacts_mean": statistics.mean(contacts), "converged_all": conv, "block_threads": b.block_threads()}
+               "contacts_mean": statistics.mean(contacts), "converged_all": conv, "block_threads": b.block_threads(),
+               "tile": b.tile()}
         b.close()
         return out
 
@@ -458,7 +459,7 @@ def piles(args, ranks):
                   "block_threads": f64["block_threads"]} if f64 else None),
         "ablation": abl or None,
         "solver": {k: mixed[k] for k in ("violation_max", "longest_scene_iterations_mean", "contacts_mean",
-                                        "converged_all", "block_threads")},
+                                        "converged_all", "block_threads", "tile")},
         "clocks": mixed["clocks"], "gpu_launches": mixed["launches"],
     }
     if ranks.rank == 0:

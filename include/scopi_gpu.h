@@ -228,8 +228,9 @@ int64_t scopi_gpu_kernel_launches(scopi_gpu_handle* h);
    handle; scopi_gpu_run(h, dt, k, 0) then advances every scene k steps, one CUDA graph
    replay per step: contact detection keeps scenes apart, and one persistent launch solves
    all scenes (one CTA per scene, each iterating until its own stopping test holds; the
-   mixed precision form corrects each scene in FP64 inside the same launch).  The block
-   size of that launch is chosen on the first step by timing 256, 512 and 1024 threads.
+   mixed precision form corrects each scene in FP64 inside the same launch).  The launch
+   shape (threads per scene and tile) is chosen on the first step with a non-trivial solve
+   by timing each shape on that step's problem.
    NoFriction only.  scopi_gpu_get_stats reports the worst scene (iterations, violation). */
 typedef struct scopi_gpu_scene_stats {
     int64_t contacts;
@@ -253,6 +254,11 @@ int32_t scopi_gpu_batch_block_threads(scopi_gpu_handle* h);
 /* pin the block size per scene (256, 512 or 1024) instead of autotuning it on the first
    step; 0 restores autotuning.  Only before the first step (else SCOPI_GPU_EINVAL). */
 int32_t scopi_gpu_batch_set_block_threads(scopi_gpu_handle* h, int32_t threads);
+/* the tile of the batched solve (contacts / incidence records each thread keeps in flight),
+   autotuned with the block size: 256 x 4 or 2, 512 x 1 or 2, 1024 x 1 or 2 */
+int32_t scopi_gpu_batch_tile(scopi_gpu_handle* h);
+/* pin both (0, 0 restores autotuning); only before the first step */
+int32_t scopi_gpu_batch_set_shape(scopi_gpu_handle* h, int32_t threads, int32_t tile);
 
 /* APGD solve of one normal-contact QP (NoFriction, FP64, torque-free rows: sphere, plane
    and segment contacts) on caller-provided DEVICE arrays, allocating no device memory.

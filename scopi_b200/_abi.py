@@ -24,7 +24,7 @@ EXPORTED = [
     "scopi_gpu_last_error", "scopi_gpu_kernel_launches", "scopi_gpu_get_stream", "scopi_gpu_apgd_noalloc",
     "scopi_gpu_batch_create", "scopi_gpu_batch_get_scene", "scopi_gpu_batch_get_scene_stats",
     "scopi_gpu_batch_block_threads", "scopi_gpu_batch_set_block_threads", "scopi_gpu_test_barrier_stall",
-    "scopi_gpu_set_contacts", "scopi_gpu_get_se_starts",
+    "scopi_gpu_set_contacts", "scopi_gpu_get_se_starts", "scopi_gpu_batch_tile", "scopi_gpu_batch_set_shape",
 ]
 
 
@@ -119,6 +119,10 @@ def load(path: str = LIB_PATH):
     L.scopi_gpu_get_se_starts.restype = C.c_int32
     L.scopi_gpu_set_contacts.argtypes = [H, C.c_int64, I64, I64, D, D, D, D]
     L.scopi_gpu_set_contacts.restype = C.c_int32
+    L.scopi_gpu_batch_tile.argtypes = [H]
+    L.scopi_gpu_batch_tile.restype = C.c_int32
+    L.scopi_gpu_batch_set_shape.argtypes = [H, C.c_int32, C.c_int32]
+    L.scopi_gpu_batch_set_shape.restype = C.c_int32
     L.scopi_gpu_test_barrier_stall.argtypes = [H]
     L.scopi_gpu_test_barrier_stall.restype = C.c_int32
     for name in ("scopi_gpu_create", "scopi_gpu_destroy", "scopi_gpu_set_particles", "scopi_gpu_get_particles",

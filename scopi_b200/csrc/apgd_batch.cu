@@ -380,13 +380,13 @@ __device__ double residual_scene(const BatchArgs<T>& A, int o0, int n0, int a0, 
 // Two CTAs per SM at 256 and 512 threads (all 256 scenes of the benchmark batch resident
 // at once on 148 SMs), one at 1024; loads in flight per thread chosen to fit the registers.
 template <int BT>
-struct BatchKB {
-    static constexpr int value = BT <= 256 ? 4 : 1;
-    static constexpr int min_blocks = BT <= 512 ? 2 : 1;
+struct BatchMinBlocks {
+    static constexpr int value = BT <= 512 ? 2 : 1;
 };
 
-template <typename T, int DIM, int BT>
-__global__ void __launch_bounds__(BT, BatchKB<BT>::min_blocks) k_apgd_batch(BatchArgs<T> A) {
+// KB (the tile): independent contacts / incidence records each thread keeps in flight
+template <typename T, int DIM, int BT, int KB>
+__global__ void __launch_bounds__(BT, BatchMinBlocks<BT>::value) k_apgd_batch(BatchArgs<T> A) {
     if (A.sizes->overflow) return;  // the step is redone after the buffers grow
     __shared__ BState S;
     const int scene = A.order[blockIdx.x];
@@ -397,7 +397,7 @@ __global__ void __launch_bounds__(BT, BatchKB<BT>::min_blocks) k_apgd_batch(Batc
     int corr = 0, conv = 1;
     double viol = 0.0;
     if (nct > 0) {
-        solve_scene<T, DIM, BatchKB<BT>::value>(A, S, o0, n0, a0, nct, p0, p1, nullptr, A.alpha);
+        solve_scene<T, DIM, KB>(A, S, o0, n0, a0, nct, p0, p1, nullptr, A.alpha);
         iters += S.ite;
         nbt += S.nbt;
         nrs += S.nrs;
@@ -420,7 +420,7 @@ __global__ void __launch_bounds__(BT, BatchKB<BT>::min_blocks) k_apgd_batch(Batc
                 // the correction starts from the step size the previous solve ended with
                 const double a_next = 1.0 / S.lgood;
                 __syncthreads();
-                solve_scene<T, DIM, BatchKB<BT>::value>(A, S, o0, n0, a0, nct, p0, p1, A.lam64, a_next);
+                solve_scene<T, DIM, KB>(A, S, o0, n0, a0, nct, p0, p1, A.lam64, a_next);
                 iters += S.ite;
                 f32 += S.ite;
                 nbt += S.nbt;
@@ -473,9 +473,9 @@ __global__ void k_batch_ranges(int n_scenes, int nin, const int* sc_obs0, const 
     }
 }
 
-template <typename T, int DIM, int BT>
+template <typename T, int DIM, int BT, int KB>
 cudaError_t launch_bt(BatchArgs<T>& A, int n_scenes, cudaStream_t s) {
-    k_apgd_batch<T, DIM, BT><<<n_scenes, BT, 0, s>>>(A);
+    k_apgd_batch<T, DIM, BT, KB><<<n_scenes, BT, 0, s>>>(A);
     g_batch_launches += 1;
     return cudaGetLastError();
 }
@@ -490,8 +490,14 @@ void launch_batch_ranges(int n_scenes, int nin, const int* sc_obs0, const int* s
     g_batch_launches += 1;
 }
 
+bool batch_shape_valid(int block_threads, int tile) {
+    return (block_threads == 256 && (tile == 2 || tile == 4)) || ((block_threads == 512 || block_threads == 1024) &&
+                                                                  (tile == 1 || tile == 2));
+}
+
 template <typename T>
-cudaError_t launch_apgd_batch(int dim, int block_threads, const BatchSolve<T>& b, int n_scenes, cudaStream_t s) {
+cudaError_t launch_apgd_batch(int dim, int block_threads, int tile, const BatchSolve<T>& b, int n_scenes,
+                              cudaStream_t s) {
     BatchArgs<T> A;
     A.nin = b.nin;
     A.order = b.order;
@@ -522,13 +528,14 @@ cudaError_t launch_apgd_batch(int dim, int block_threads, const BatchSolve<T>& b
     A.dynamic = b.dynamic;
     A.max_corrections = b.max_corrections;
     A.curvature_start = b.curvature_start;
-#define LB(D, B) \
-    if (dim == D && block_threads == B) return launch_bt<T, D, B>(A, n_scenes, s);
-    LB(2, 256) LB(2, 512) LB(2, 1024) LB(3, 256) LB(3, 512) LB(3, 1024)
+#define LB(D, B, K) \
+    if (dim == D && block_threads == B && tile == K) return launch_bt<T, D, B, K>(A, n_scenes, s);
+    LB(2, 256, 4) LB(2, 256, 2) LB(2, 512, 1) LB(2, 512, 2) LB(2, 1024, 1) LB(2, 1024, 2)
+    LB(3, 256, 4) LB(3, 256, 2) LB(3, 512, 1) LB(3, 512, 2) LB(3, 1024, 1) LB(3, 1024, 2)
 #undef LB
     return cudaErrorInvalidValue;
 }
-template cudaError_t launch_apgd_batch<double>(int, int, const BatchSolve<double>&, int, cudaStream_t);
-template cudaError_t launch_apgd_batch<float>(int, int, const BatchSolve<float>&, int, cudaStream_t);
+template cudaError_t launch_apgd_batch<double>(int, int, int, const BatchSolve<double>&, int, cudaStream_t);
+template cudaError_t launch_apgd_batch<float>(int, int, int, const BatchSolve<float>&, int, cudaStream_t);
 
 }  // namespace scopi_gpu

@@ -327,8 +327,11 @@ long long apgd_batch_launches();
 void launch_batch_ranges(int n_scenes, int nin, const int* sc_obs0, const int* sc_obs1, const int* sc_p0,
                          const int* sc_p1, const int* obs_off, const int* obs_pos, const int* row_ptr,
                          const Sizes* sizes, int* o0, int* o1, int* a0, int* a1, cudaStream_t s);
-// one CTA per scene (block_threads = 256, 512 or 1024)
+// one CTA per scene: block_threads 256 (tile 2 or 4), 512 or 1024 (tile 1 or 2); the tile is
+// the number of independent contacts / incidence records a thread keeps in flight
+bool batch_shape_valid(int block_threads, int tile);
 template <typename T>
-cudaError_t launch_apgd_batch(int dim, int block_threads, const BatchSolve<T>& b, int n_scenes, cudaStream_t s);
+cudaError_t launch_apgd_batch(int dim, int block_threads, int tile, const BatchSolve<T>& b, int n_scenes,
+                              cudaStream_t s);
 
 }  // namespace scopi_gpu

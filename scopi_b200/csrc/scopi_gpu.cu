@@ -22,6 +22,8 @@ thread_local char g_global_error[512] = "";
 // batched scenes: threads per scene until the autotuner has run, and the longest scene
 // solve (APGD iterations) of the step whose problem it is tuned on
 constexpr int kBatchDefaultThreads = 512;
+// the tile a block size runs with unless the autotuner chose both
+inline int batch_default_tile(int threads) { return threads <= 256 ? 4 : 1; }
 constexpr long long kBatchTuneIterations = 64;
 
 struct DevMem {
@@ -211,13 +213,15 @@ struct scopi_gpu_handle {
     std::vector<BatchSceneStats> h_bstats;
     double* d_obs_snap = nullptr;  // obstacle pos (3) and q (4) before the step, restored on overflow
     int batch_threads = 0;         // block size chosen by the autotuner or pinned (0 = not yet)
+    int batch_tile = 0;            // contacts in flight per thread chosen with it
     int batch_bt_used = 0;         // block size of the last step
-    float batch_tune_ms[3] = {0, 0, 0};
+    int batch_tile_used = 0;
+    float batch_tune_ms[6] = {0, 0, 0, 0, 0, 0};
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     double graph_dt = 0.0;
     long long graph_cap = -1;
-    int graph_bt = 0;
+    int graph_bt = 0, graph_tile = 0;
     long long graph_kernels = 0;   // kernels one replay of `graph_exec` launches
     long long replayed = 0;        // kernels launched by graph replays so far
     long long cell_cap_hint = 0;   // cell-list capacity wanted by the batch layout
@@ -231,7 +235,7 @@ struct scopi_gpu_handle {
 
     // Every kernel of one batch step, enqueued on `stream` with no host synchronisation
     // (captured once into a CUDA graph and replayed every step).
-    void enqueue_batch_step(double dt, int bt) {
+    void enqueue_batch_step(double dt, int bt, int tile) {
         Bodies b = bodies();
         StepParams sp = step_params(dt);
         if (nin > 0) {
@@ -255,11 +259,11 @@ struct scopi_gpu_handle {
         }
         launch_batch_ranges(n_scenes, nin, d_sc_obs0, d_sc_obs1, d_sc_p0, d_sc_p1, d_obs_off, dw.obs_pos, dw.row_ptr,
                             d_sizes_cur, d_sc_o0, d_sc_o1, d_sc_a0, d_sc_a1, stream);
-        enqueue_batch_solve(dt, bt);
+        enqueue_batch_solve(dt, bt, tile);
         launch_update(b, sp, reinterpret_cast<const double*>(d_usfin), 4, 0, d_sizes_cur, stream);
     }
 
-    void enqueue_batch_solve(double dt, int bt) {
+    void enqueue_batch_solve(double dt, int bt, int tile) {
         auto fill = [&](auto& bs) {
             bs.nin = nin;
             bs.order = d_order;
@@ -294,7 +298,7 @@ struct scopi_gpu_handle {
             bs.inc = d_incv32;
             for (int k = 0; k < 3; ++k) bs.lam[k] = d_lam32[k];
             for (int k = 0; k < 4; ++k) bs.u[k] = d_us32[k];
-            launch_apgd_batch<float>(P.dim, bt, bs, n_scenes, stream);
+            launch_apgd_batch<float>(P.dim, bt, tile, bs, n_scenes, stream);
         } else {
             BatchSolve<double> bs{};
             fill(bs);
@@ -302,7 +306,7 @@ struct scopi_gpu_handle {
             bs.inc = d_incv64;
             for (int k = 0; k < 3; ++k) bs.lam[k] = d_lam64[k];
             for (int k = 0; k < 4; ++k) bs.u[k] = d_us64[k];
-            launch_apgd_batch<double>(P.dim, bt, bs, n_scenes, stream);
+            launch_apgd_batch<double>(P.dim, bt, tile, bs, n_scenes, stream);
         }
     }
 
@@ -350,21 +354,23 @@ struct scopi_gpu_handle {
     }
 
     // One time step of every scene: one CUDA graph replay (captured on the first step and
-    // again whenever dt, the contact capacity or the block size changes).  Autotuning: the
+    // again whenever dt, the contact capacity or the launch shape changes).  Autotuning: the
     // steps run with 512 threads per scene until the first step whose longest scene solve
     // takes >= 64 iterations (the first steps of a falling pile converge in one); that
-    // step's contact problem is then re-solved with 256, 512 and 1024 threads per scene
-    // and the fastest is kept for the rest of the run.
+    // step's contact problem is then re-solved with each shape (threads per scene x the tile,
+    // the contacts each thread keeps in flight: 256 x 4 / 2, 512 x 1 / 2, 1024 x 1 / 2) and the
+    // fastest is kept for the rest of the run.
     int step_batch(double dt) {
         for (int attempt = 0; attempt < 4; ++attempt) {
             const int bt = batch_threads ? batch_threads : kBatchDefaultThreads;
+            const int tile = batch_tile ? batch_tile : batch_default_tile(bt);
             cudaEventRecord(ev[0], stream);
-            if (!graph_exec || graph_dt != dt || graph_cap != c_cap || graph_bt != bt) {
+            if (!graph_exec || graph_dt != dt || graph_cap != c_cap || graph_bt != bt || graph_tile != tile) {
                 drop_graph();
                 cudaError_t e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
                 if (e != cudaSuccess) return cuda_fail(e, "cudaStreamBeginCapture");
                 const long long l0 = launches();
-                enqueue_batch_step(dt, bt);
+                enqueue_batch_step(dt, bt, tile);
                 graph_kernels = launches() - l0;
                 replayed -= graph_kernels;  // the capture itself launched nothing
                 e = cudaStreamEndCapture(stream, &graph);
@@ -374,6 +380,7 @@ struct scopi_gpu_handle {
                 graph_dt = dt;
                 graph_cap = c_cap;
                 graph_bt = bt;
+                graph_tile = tile;
                 cudaEventRecord(ev[0], stream);
             }
             cudaError_t e = cudaGraphLaunch(graph_exec, stream);
@@ -391,6 +398,7 @@ struct scopi_gpu_handle {
             collect_batch_stats();
             finish_batch_step_timing();
             batch_bt_used = bt;
+            batch_tile_used = tile;
             if (!batch_threads && stats.iterations >= kBatchTuneIterations) return autotune_batch(dt);
             return 0;
         }
@@ -400,12 +408,12 @@ struct scopi_gpu_handle {
     // timing only: re-solve the last step's contact problem (its packed records are still in
     // place; the update already used the step's own solve) with each block size
     int autotune_batch(double dt) {
-        const int cand[3] = {256, 512, 1024};
+        const int cand[6][2] = {{256, 4}, {256, 2}, {512, 1}, {512, 2}, {1024, 1}, {1024, 2}};
         float best = 1e30f;
-        int best_bt = kBatchDefaultThreads;
-        for (int k = 0; k < 3; ++k) {
+        int best_bt = kBatchDefaultThreads, best_tile = batch_default_tile(kBatchDefaultThreads);
+        for (int k = 0; k < 6; ++k) {
             cudaEventRecord(ev_a[0], stream);
-            enqueue_batch_solve(dt, cand[k]);
+            enqueue_batch_solve(dt, cand[k][0], cand[k][1]);
             cudaEventRecord(ev_a[1], stream);
             cudaError_t e = cudaEventSynchronize(ev_a[1]);
             if (e != cudaSuccess) return cuda_fail(e, "batch autotune");
@@ -414,10 +422,12 @@ struct scopi_gpu_handle {
             batch_tune_ms[k] = ms;
             if (ms < best) {
                 best = ms;
-                best_bt = cand[k];
+                best_bt = cand[k][0];
+                best_tile = cand[k][1];
             }
         }
         batch_threads = best_bt;
+        batch_tile = best_tile;
         return 0;
     }
 
@@ -1858,6 +1868,21 @@ int32_t scopi_gpu_batch_get_scene_stats(scopi_gpu_handle* h, int32_t scene, scop
 int32_t scopi_gpu_batch_block_threads(scopi_gpu_handle* h) {
     if (!h) return 0;
     return h->batch_threads ? h->batch_threads : h->batch_bt_used;
+}
+
+int32_t scopi_gpu_batch_tile(scopi_gpu_handle* h) {
+    if (!h) return 0;
+    return h->batch_tile ? h->batch_tile : h->batch_tile_used;
+}
+
+int32_t scopi_gpu_batch_set_shape(scopi_gpu_handle* h, int32_t threads, int32_t tile) {
+    if (!h || !h->batch) return SCOPI_GPU_EINVAL;
+    if (h->stats.steps > 0) return h->fail(SCOPI_GPU_EINVAL, "the launch shape is fixed once the batch has stepped");
+    if (!(threads == 0 && tile == 0) && !scopi_gpu::batch_shape_valid(threads, tile))
+        return h->fail(SCOPI_GPU_EINVAL, "launch shape must be 256 x 2|4, 512 x 1|2 or 1024 x 1|2 (0, 0 = autotune)");
+    h->batch_threads = threads;
+    h->batch_tile = tile;
+    return 0;
 }
 
 int32_t scopi_gpu_test_barrier_stall(scopi_gpu_handle* h) {

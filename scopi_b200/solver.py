@@ -230,7 +230,7 @@ class ScopiBatch:
     """
 
     def __init__(self, scenes, vap=VAP_FPD, contact_method=KDTREE, precision=FP64, device=0, block_threads=0,
-                 **overrides):
+                 tile=0, **overrides):
         self._lib = _abi.load()
         p = _abi.Params()
         self._lib.scopi_gpu_default_params(C.byref(p), scenes[0].dim)
@@ -250,7 +250,10 @@ class ScopiBatch:
         if rc < 0:
             raise ScopiGPUError(f"scopi_gpu_batch_create failed ({rc}): {self._lib.scopi_gpu_last_error(None).decode()}")
         self._h = h
-        if block_threads:
+        if block_threads and tile:
+            self._check(self._lib.scopi_gpu_batch_set_shape(h, int(block_threads), int(tile)),
+                        "scopi_gpu_batch_set_shape")
+        elif block_threads:
             self._check(self._lib.scopi_gpu_batch_set_block_threads(h, int(block_threads)),
                         "scopi_gpu_batch_set_block_threads")
 
@@ -285,6 +288,10 @@ class ScopiBatch:
 
     def block_threads(self) -> int:
         return int(self._lib.scopi_gpu_batch_block_threads(self._h))
+
+    def tile(self) -> int:
+        """Contacts each thread of the batched solve keeps in flight (autotuned with block_threads)."""
+        return int(self._lib.scopi_gpu_batch_tile(self._h))
 
     def stream_handle(self) -> int:
         return int(self._lib.scopi_gpu_get_stream(self._h) or 0)

@@ -103,11 +103,25 @@ def test_batch_block_sizes_agree_and_are_deterministic():
         assert rel_err(a, c) <= 1e-9
 
 
+@pytest.mark.parametrize("threads,tile", [(256, 2), (512, 2), (1024, 2), (512, 1)])
+def test_batch_tiles_agree_with_the_default_shape(threads, tile):
+    """Every launch shape the autotuner may pick (threads per scene x contacts in flight per
+    thread) solves the same problems: positions within 1e-9 of the default 256 x 4 shape."""
+    scenes = small_piles(5, 100, 1500, seed=10)
+    ref = ScopiBatch(scenes, vap=ST["vap"], precision=FP64, block_threads=256, tile=4, **KW).run(ST["dt"], 4)
+    b = ScopiBatch(scenes, vap=ST["vap"], precision=FP64, block_threads=threads, tile=tile, **KW).run(ST["dt"], 4)
+    assert b.block_threads() == threads and b.tile() == tile
+    for s in range(len(scenes)):
+        assert rel_err(b.scene(s).pos, ref.scene(s).pos) <= 1e-9, s
+    with pytest.raises(ScopiGPUError):
+        ScopiBatch(scenes, vap=ST["vap"], block_threads=256, tile=1, **KW)
+
+
 def test_batch_autotune_graph_replay_and_launch_count():
     scenes = small_piles(8, 100, 1500, seed=11)
     b = ScopiBatch(scenes, vap=ST["vap"], precision=MIXED, **KW)
     b.run(ST["dt"], 1)
-    assert b.block_threads() in (256, 512, 1024)
+    assert b.block_threads() in (256, 512, 1024) and b.tile() in (1, 2, 4)
     b.run(ST["dt"], 1)  # captures the graph, replays it once
     l1 = b.kernel_launches()
     b.run(ST["dt"], 1)
