@@ -494,11 +494,9 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
             V4<T>* uYN = pick4(S.jYN, A.u0, A.u1, A.u2, A.u3);
             const T bn_ = (T)S.beta_n;
             double sw = 0.0, sq = 0.0;
-            // one body per thread.  Its records in batches of KB: the contact indices first
-            // (one word of each record), then all the l+ gathers they name, then the normals
-            // (the same L1 lines as the indices): one L2 round trip per batch, and a batch
-            // covers the records of most bodies
-            constexpr int KB = 8;
+            // one body per thread; its incidence records, then the l+ gathers they index,
+            // are issued in batches so several loads are in flight per thread
+            constexpr int KB = 4;
             const long long ntrip = ntrip_p;
             // stages 0..GP-2 were issued before the barrier
 #pragma unroll 1
@@ -511,13 +509,22 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
                 T w0 = 0, w1 = 0, w2 = 0;
                 const int k0 = s_p0[sl], k1 = s_p1[sl];
                 for (int kb = k0; kb < k1; kb += KB) {
+                    T ex[KB], ey[KB], ez[KB], mu[KB];
                     int ci[KB];
-                    T mu[KB];
-#pragma unroll
-                    for (int q = 0; q < KB; ++q) ci[q] = kb + q < k1 ? idx_of(reinterpret_cast<const T*>(A.inc + kb + q)[3]) : -1;
 #pragma unroll
                     for (int q = 0; q < KB; ++q) {
-                        mu[q] = (T)0;
+                        ex[q] = ey[q] = ez[q] = mu[q] = (T)0;
+                        ci[q] = -1;
+                        if (kb + q < k1) {
+                            const V4<T> e = ld4(A.inc + kb + q);
+                            ex[q] = e.x;
+                            ey[q] = e.y;
+                            ez[q] = e.z;
+                            ci[q] = idx_of(e.w);
+                        }
+                    }
+#pragma unroll
+                    for (int q = 0; q < KB; ++q)
                         if (ci[q] >= 0) {
                             mu[q] = __ldcg(lnew + ci[q]);
                             if (PROB == kViscous) {
@@ -525,15 +532,12 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
                                 if (sv >= 0) mu[q] -= __ldcg(lnew + sv);
                             }
                         }
-                    }
 #pragma unroll
-                    for (int q = 0; q < KB; ++q)
-                        if (ci[q] >= 0) {
-                            const V4<T> e = ld4(A.inc + kb + q);
-                            w0 += mu[q] * e.x;
-                            w1 += mu[q] * e.y;
-                            if (DIM == 3) w2 += mu[q] * e.z;
-                        }
+                    for (int q = 0; q < KB; ++q) {
+                        w0 += mu[q] * ex[q];
+                        w1 += mu[q] * ey[q];
+                        if (DIM == 3) w2 += mu[q] * ez[q];
+                    }
                 }
                 const T im = s_im[sl];
                 const T n0 = im * w0, n1 = im * w1, n2 = im * w2;

@@ -389,6 +389,10 @@ __device__ __forceinline__ bool pair_in_contact(const StepParams& p, const doubl
     // superellipsoids (w = bounding radius): the pairs whose bounding spheres come within
     // dmax go to the exact solve of se.cu, which decides
     if (p.se_mode) return true;
+    // clearly inside: |x_i - x_j| < (r_i + r_j + dmax)(1 - 5e-10), a margin far above the
+    // rounding of the reference's dij (~1e-16 of the coordinates), so its dij < dmax holds;
+    // only the pairs in the thin shell around the threshold need the exact formula
+    if (s2 < lim * lim * (1.0 - 1e-9)) return true;
     PairGeom pg;
     sphere_sphere(DIM, xl, L.w, xh, H.w, pg);
     return pg.dij < p.dmax;
@@ -530,6 +534,7 @@ __global__ void __launch_bounds__(32 * kSearchWarps, 4) k_pair_search_cells(Bodi
                                                                         int* row_tmp) {
     constexpr int nst = DIM == 3 ? 14 : 5;
     __shared__ int s_pref[kSearchWarps][16], s_beg[kSearchWarps][16], s_cnt[kSearchWarps][16];
+    __shared__ unsigned s_inv[kSearchWarps][16];  // ceil(2^32 / count): l / count = umulhi(l, inv)
     const Grid g = *grid;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const long long nwarps = (long long)gridDim.x * kSearchWarps;
@@ -567,21 +572,18 @@ __global__ void __launch_bounds__(32 * kSearchWarps, 4) k_pair_search_cells(Bodi
             s_pref[w][lane] = incl - cnt;
             s_beg[w][lane] = beg;
             s_cnt[w][lane] = ncb;
+            // exact quotient for l < 2^16 and counts < 2^16 (l < nh * count here)
+            s_inv[w][lane] = ncb > 0 ? (unsigned)((0x100000000ULL + (unsigned long long)ncb - 1) / ncb) : 0u;
         }
         __syncwarp();
         // two pairs per lane and round: their loads, tests and row-slot atomics overlap
         // (an atomic's returned slot is a round trip to L2 before the store can go)
+        // a lane's pair numbers t only grow: its stencil offset advances with them
+        int o_cur = 0;
         auto locate = [&](int t, int& sa, int& sb) {
-            int lo = 0, hi = nst - 1;  // the last offset whose pairs start at or before t
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (s_pref[w][mid] <= t)
-                    lo = mid;
-                else
-                    hi = mid - 1;
-            }
-            int l = t - s_pref[w][lo];
-            if (lo == 0) {
+            while (o_cur < nst - 1 && s_pref[w][o_cur + 1] <= t) ++o_cur;
+            int l = t - s_pref[w][o_cur];
+            if (o_cur == 0) {
                 int i = 0;
                 while (l >= nh - 1 - i) {
                     l -= nh - 1 - i;
@@ -590,10 +592,9 @@ __global__ void __launch_bounds__(32 * kSearchWarps, 4) k_pair_search_cells(Bodi
                 sa = h0 + i;
                 sb = h0 + i + 1 + l;
             } else {
-                const int n2 = s_cnt[w][lo];
-                const int ia = l / n2;
+                const int ia = (int)__umulhi((unsigned)l, s_inv[w][o_cur]);
                 sa = h0 + ia;
-                sb = s_beg[w][lo] + (l - ia * n2);
+                sb = s_beg[w][o_cur] + (l - ia * s_cnt[w][o_cur]);
             }
         };
         for (int t0 = lane; t0 < total; t0 += 64) {
