@@ -534,7 +534,7 @@ __global__ void __launch_bounds__(32 * kSearchWarps, 4) k_pair_search_cells(Bodi
                                                                         int* row_tmp) {
     constexpr int nst = DIM == 3 ? 14 : 5;
     __shared__ int s_pref[kSearchWarps][16], s_beg[kSearchWarps][16], s_cnt[kSearchWarps][16];
-    __shared__ unsigned s_inv[kSearchWarps][16];  // ceil(2^32 / count): l / count = umulhi(l, inv)
+    __shared__ unsigned s_inv[kSearchWarps][16];  // ceil(2^32 / count) for counts >= 2: l / count = umulhi(l, inv)
     const Grid g = *grid;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const long long nwarps = (long long)gridDim.x * kSearchWarps;
@@ -572,8 +572,9 @@ __global__ void __launch_bounds__(32 * kSearchWarps, 4) k_pair_search_cells(Bodi
             s_pref[w][lane] = incl - cnt;
             s_beg[w][lane] = beg;
             s_cnt[w][lane] = ncb;
-            // exact quotient for l < 2^16 and counts < 2^16 (l < nh * count here)
-            s_inv[w][lane] = ncb > 0 ? (unsigned)((0x100000000ULL + (unsigned long long)ncb - 1) / ncb) : 0u;
+            // exact quotient for l < 2^16 and 2 <= counts < 2^16 (l < nh * count here); a count
+            // of 1 (whose reciprocal 2^32 does not fit) is taken apart in locate
+            s_inv[w][lane] = ncb > 1 ? (unsigned)((0x100000000ULL + (unsigned long long)ncb - 1) / ncb) : 0u;
         }
         __syncwarp();
         // two pairs per lane and round: their loads, tests and row-slot atomics overlap
@@ -592,9 +593,10 @@ __global__ void __launch_bounds__(32 * kSearchWarps, 4) k_pair_search_cells(Bodi
                 sa = h0 + i;
                 sb = h0 + i + 1 + l;
             } else {
-                const int ia = (int)__umulhi((unsigned)l, s_inv[w][o_cur]);
+                const int n2 = s_cnt[w][o_cur];
+                const int ia = n2 == 1 ? l : (int)__umulhi((unsigned)l, s_inv[w][o_cur]);
                 sa = h0 + ia;
-                sb = s_beg[w][o_cur] + (l - ia * s_cnt[w][o_cur]);
+                sb = s_beg[w][o_cur] + (l - ia * n2);
             }
         };
         for (int t0 = lane; t0 < total; t0 += 64) {
