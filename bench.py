@@ -442,6 +442,14 @@ def piles(args, ranks):
                          "violation_max": r["violation_max"],
                          "longest_scene_iterations_mean": r["longest_scene_iterations_mean"]}
     value = ranks.world * args.steps * 1000.0 / mixed["ms"]
+    # the FP64 leg with the reference's first step stops its landing solves at violations
+    # above 1e-6 (the reference's stopping rule); the FP64 leg that meets the bar is the one
+    # with the curvature first step
+    equal = None
+    if abl.get("fp64_curvature_start"):
+        fc = abl["fp64_curvature_start"]
+        equal = {"fp64_leg": "fp64_curvature_start", "fp64_violation_max": fc["violation_max"],
+                 "mixed_violation_max": mixed["violation_max"], "mixed_over_fp64": value / fc["value"]}
     line = {
         "metric": "time steps/s of 256 independent 2D pile scenes (one batch, violation <= 1e-6)",
         "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -458,6 +466,7 @@ def piles(args, ranks):
                   "longest_scene_iterations_mean": f64["longest_scene_iterations_mean"],
                   "block_threads": f64["block_threads"]} if f64 else None),
         "ablation": abl or None,
+        "at_equal_violation": equal,
         "solver": {k: mixed[k] for k in ("violation_max", "longest_scene_iterations_mean", "contacts_mean",
                                         "converged_all", "block_threads", "tile")},
         "clocks": mixed["clocks"], "gpu_launches": mixed["launches"],

@@ -76,11 +76,18 @@ __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
 }
 // Split form: grid_arrive publishes this block's writes and returns the arrival target;
 // the block may do independent work before grid_wait.
-// withhold: compute the target without counting this block (the timeout test: the
-// barrier never completes and every waiter gives up after the limit).
+__device__ __forceinline__ unsigned int atom_add_release_u32(unsigned int* p, unsigned int v) {
+    unsigned int old;
+    asm volatile("atom.release.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+// The arrival is a release at GPU scope: it orders before it every write this thread has
+// observed, which after the block barrier that precedes the call are all the block's
+// writes (release is cumulative), so no separate fence is needed.  withhold: compute the
+// target without counting this block (the timeout test: the barrier never completes and
+// every waiter gives up after the limit).
 __device__ __forceinline__ unsigned int grid_arrive(unsigned int* bar, unsigned int nblocks, bool withhold = false) {
-    __threadfence();
-    const unsigned int old = withhold ? ld_acquire_u32(bar) : atomicAdd(bar, 1u);
+    const unsigned int old = withhold ? ld_acquire_u32(bar) : atom_add_release_u32(bar, 1u);
     return (old / nblocks + 1u) * nblocks;
 }
 __device__ __forceinline__ bool grid_wait(unsigned int* bar, unsigned int target) {
@@ -102,7 +109,8 @@ __device__ __forceinline__ bool grid_wait(unsigned int* bar, unsigned int target
         }
         if (it > 32) __nanosleep(32);
     }
-    __threadfence();
+    // the acquire load that saw the target orders the reads after it (the block barrier that
+    // follows extends that to the other threads of the block)
     return *verr == 0u;
 }
 __device__ __forceinline__ bool grid_arrive_wait(unsigned int* bar, unsigned int nblocks) {

@@ -451,6 +451,7 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
                 bool ok = true;
                 if (tid == 0) ok = grid_wait(A.bar, target);
                 ok = __shfl_sync(0xffffffffu, ok, 0) != 0;
+                __syncwarp();  // the lanes' partial loads come after lane 0's acquire
                 double t[8] = {0, 0, 0, 0, 0, 0, 0, 0};
                 {
                     double tt[NS];
@@ -582,6 +583,7 @@ __global__ void __launch_bounds__(SphOcc<T>::threads, 1) k_apgd_sph(SphArgs<T> A
             if (tid < 32) {
                 if (tid == 0) ok = grid_wait(A.bar, target2);
                 ok = __shfl_sync(0xffffffffu, ok, 0) != 0;
+                __syncwarp();
                 if (NQ == 1) {
                     t6[0] = 0.0;
                     warp_grid_sum<1>(part2 + 1, nb, 8, t6 + 1);
