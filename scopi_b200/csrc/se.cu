@@ -555,10 +555,39 @@ __global__ void __launch_bounds__(kSeThreads, 3) k_se_start(Bodies B, Contacts c
 }
 
 // --------------------------------------------------------------- F and Jacobian
+// One evaluation's point, normal (and derivatives) of both bodies, computed by a quad of four
+// lanes that hold the same pair: the sixteen signed powers (8 per body, pw_arg / pw_exp) are
+// split four per lane, power m on lane m & 3, and exchanged by shuffles inside the quad, so
+// every lane assembles exactly what local() gives.  The lanes of a quad run the same hybrid
+// method on the same data, so they reach every shuffle together.
+__device__ __forceinline__ void local_pair_quad(const Body& s1, const Body& s2, const double* u, Local& L1, Local& L2,
+                                                bool deriv) {
+    const int ql = threadIdx.x & 3;
+    const unsigned qmask = 0xFu << (threadIdx.x & 28);
+    double sa[2], ca[2], sb[2], cb[2];
+    sincos(u[0], &sa[0], &ca[0]);
+    sincos(u[1], &sb[0], &cb[0]);
+    sincos(u[2], &sa[1], &ca[1]);
+    sincos(u[3], &sb[1], &cb[1]);
+    Pw mine[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int bd = j >> 1, w = ql + 4 * (j & 1);  // power m = ql + 4 j: body m >> 3, index m & 7
+        mine[j] = pw(pw_arg(w, sa[bd], ca[bd], sb[bd], cb[bd]), pw_exp(bd ? s2 : s1, w), deriv);
+    }
+    Pw P[16];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+        P[m].v = __shfl_sync(qmask, mine[m >> 2].v, m & 3, 4);
+        P[m].d = deriv ? __shfl_sync(qmask, mine[m >> 2].d, m & 3, 4) : 0.0;
+    }
+    assemble_local(s1, sa[0], ca[0], sb[0], cb[0], P, L1, deriv);
+    assemble_local(s2, sa[1], ca[1], sb[1], cb[1], P + 8, L2, deriv);
+}
+
 __device__ void sese_F(const Body& s1, const Body& s2, const double* u, double* F) {
     Local L1, L2;
-    local(s1, u[0], u[1], L1, false);
-    local(s2, u[2], u[3], L2, false);
+    local_pair_quad(s1, s2, u, L1, L2, false);
     double p1[3], p2[3], n1[3], n2[3];
     mv(s1.R, L1.p, p1);
     mv(s2.R, L2.p, p2);
@@ -572,8 +601,7 @@ __device__ void sese_F(const Body& s1, const Body& s2, const double* u, double* 
 
 __device__ void sese_J(const Body& s1, const Body& s2, const double* u, double* J) {  // column-major
     Local L1, L2;
-    local(s1, u[0], u[1], L1);
-    local(s2, u[2], u[3], L2);
+    local_pair_quad(s1, s2, u, L1, L2, true);
     double p1[3], p2[3], n1[3], n2[3];
     mv(s1.R, L1.p, p1);
     mv(s2.R, L2.p, p2);
@@ -603,24 +631,32 @@ __device__ void sese_J(const Body& s1, const Body& s2, const double* u, double* 
     }
 }
 
-// the hybrid method from the start, one row per thread, and the row's closest points; the
-// rows are handed out by a counter so that a lane takes the next row when its solve ends
-// (the evaluations per solve vary from a few to maxfev).  (One warp per row, with the 32
-// powers of an evaluation spread over the lanes, measured 5x slower: the hybrid method's
-// own scalar work, then done 32 times, outweighs the powers.)  Two 128-thread blocks per SM
-// (255 registers): the hybrid method's arrays then stay in L1 (three blocks at 168 registers
-// spilled 2.4 KB per thread and measured 20 % slower per step of the 50k pile).
+// The hybrid method from the start and the row's closest points, one row per quad of lanes
+// (the evaluations' powers split over the quad: local_pair_quad), rows handed out by a
+// counter so that a quad takes the next row when its solve ends.  The evaluations per solve
+// vary from a few to maxfev (1000), and the kernel's time is set by the slowest rows while
+// the other lanes idle (ncu at 8000 bodies, one lane per row: 2.7 % of the warp slots
+// active over a 111 ms launch): the quad shortens those rows.  (One warp per row, with the
+// powers spread over 32 lanes, was measured 5x slower: the hybrid method's own scalar work,
+// then done 32 times, outweighs the powers.)  Two 128-thread blocks per SM (255 registers):
+// the hybrid method's arrays stay in L1.
 __global__ void __launch_bounds__(128, 2) k_se_solve(Bodies B, Contacts c, const Sizes* sizes, const double* u0,
                                                     int* next) {
     const int C = sizes->C, C_obs = sizes->C_obs;
+    const int ql = threadIdx.x & 3;
+    const unsigned qmask = 0xFu << (threadIdx.x & 28);
     for (;;) {
-        const int k = C_obs + atomicAdd(next, 1);
+        int row = 0;
+        if (ql == 0) row = atomicAdd(next, 1);
+        row = __shfl_sync(qmask, row, 0, 4);
+        const int k = C_obs + row;
         if (k >= C) break;
         const Body s1 = load(B, c.ci[k]), s2 = load(B, c.cj[k]);
         double u[4];
         for (int q = 0; q < 4; ++q) u[q] = u0[4 * (long long)k + q];
         hybrj<4>([&](const double* x, double* F) { sese_F(s1, s2, x, F); },
               [&](const double* x, double* J) { sese_J(s1, s2, x, J); }, u);
+        if (ql != 0) continue;
         double pi_[3], pj_[3], nij[3];
         point(s1, u[0], u[1], pi_);
         point(s2, u[2], u[3], pj_);

@@ -99,15 +99,21 @@ __device__ __forceinline__ Pw pw(double t, double k, bool deriv) {
     r.d = deriv ? k * pow(at, k - 1) : 0.0;
     return r;
 }
-// deriv = false: point and normal only (the residual); true: also their angle derivatives
-__device__ __forceinline__ void local(const Body& s, double a, double b, Local& L, bool deriv = true) {
-    const double rx = s.r[0], ry = s.r[1], rz = s.r[2];
-    double sa, ca, sb, cb;
-    sincos(a, &sa, &ca);
-    sincos(b, &sb, &cb);
+// The eight signed powers of one body at angles (a, b), in the order C(a), S(a), C(b), S(b)
+// with exponents n, n, e, e, then the same with 2 - n, 2 - e: power w is the one of
+// sin/cos selected by w & 3 (0 cos a, 1 sin a, 2 cos b, 3 sin b) with exponent pw_exp(s, w).
+__device__ __forceinline__ double pw_exp(const Body& s, int w) {
     const double n2 = 2 - s.n, e2 = 2 - s.e;
-    const Pw Ca = pw(ca, s.n, deriv), Sa = pw(sa, s.n, deriv), Cb = pw(cb, s.e, deriv), Sb = pw(sb, s.e, deriv);
-    const Pw Ca2 = pw(ca, n2, deriv), Sa2 = pw(sa, n2, deriv), Cb2 = pw(cb, e2, deriv), Sb2 = pw(sb, e2, deriv);
+    return (w & 2) ? ((w & 4) ? e2 : s.e) : ((w & 4) ? n2 : s.n);
+}
+__device__ __forceinline__ double pw_arg(int w, double sa, double ca, double sb, double cb) {
+    return (w & 3) == 0 ? ca : ((w & 3) == 1 ? sa : ((w & 3) == 2 ? cb : sb));
+}
+// point, unnormalised normal and (deriv) their angle derivatives from the eight powers
+__device__ __forceinline__ void assemble_local(const Body& s, double sa, double ca, double sb, double cb, const Pw* P,
+                                               Local& L, bool deriv) {
+    const double rx = s.r[0], ry = s.r[1], rz = s.r[2];
+    const Pw &Ca = P[0], &Sa = P[1], &Cb = P[2], &Sb = P[3], &Ca2 = P[4], &Sa2 = P[5], &Cb2 = P[6], &Sb2 = P[7];
     L.p[0] = rx * Ca.v * Cb.v;
     L.p[1] = ry * Ca.v * Sb.v;
     L.p[2] = rz * Sa.v;
@@ -130,6 +136,16 @@ __device__ __forceinline__ void local(const Body& s, double a, double b, Local& 
     L.Nb[0] = ry * rz * Ca2.v * dCb2;
     L.Nb[1] = rx * rz * Ca2.v * dSb2;
     L.Nb[2] = 0.0;
+}
+// deriv = false: point and normal only (the residual); true: also their angle derivatives
+__device__ __forceinline__ void local(const Body& s, double a, double b, Local& L, bool deriv = true) {
+    double sa, ca, sb, cb;
+    sincos(a, &sa, &ca);
+    sincos(b, &sb, &cb);
+    Pw P[8];
+#pragma unroll
+    for (int w = 0; w < 8; ++w) P[w] = pw(pw_arg(w, sa, ca, sb, cb), pw_exp(s, w), deriv);
+    assemble_local(s, sa, ca, sb, cb, P, L, deriv);
 }
 
 // ---- 2D superellipsoids (superellipsoid.hpp:282-289, 303-312): p(b) = (rx C(b,e), ry S(b,e)),
