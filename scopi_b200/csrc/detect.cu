@@ -810,6 +810,7 @@ __global__ void k_assemble(Bodies B, StepParams p, Contacts c, Assembly a, const
             const double vz = DIM == 2 ? 0.0 : v[2];
             const double vv[3] = {v[0], v[1], vz};
             for (int d = 0; d < 3; ++d) AU[d] += (s == 0 ? 1.0 : -1.0) * (vv[d] - cr[d]);
+            if (p.torque_free) continue;  // no lever-arm rows: the torque-free kernels do not read them
             double rn[3];
             cross_dim(DIM, r, n, rn);
             const double sg = (s == 0) ? 1.0 : -1.0;
@@ -847,11 +848,12 @@ __global__ void k_assemble(Bodies B, StepParams p, Contacts c, Assembly a, const
             for (int d = 0; d < DIM; ++d) cc += Cv[d] * n[d];
             a.cvec[k] = cc;
         }
-        for (int d = 0; d < 3; ++d) {
-            a.bn[3 * (long long)k + d] = n[d];
-            a.bai[3 * (long long)k + d] = arow[0][d];
-            a.baj[3 * (long long)k + d] = arow[1][d];
-        }
+        for (int d = 0; d < 3; ++d) a.bn[3 * (long long)k + d] = n[d];
+        if (!p.torque_free)
+            for (int d = 0; d < 3; ++d) {
+                a.bai[3 * (long long)k + d] = arow[0][d];
+                a.baj[3 * (long long)k + d] = arow[1][d];
+            }
         if (p.problem == kViscous) a.vflag[k] = (c.gamma[k] < -p.gamma_tol) ? 1 : 0;
     }
 }

@@ -24,6 +24,8 @@ struct StepParams {
     double kd_radius;
     double dt;
     double gamma0, gamma_min, gamma_tol, mu;
+    int torque_free;      // every row is normal-only with lever arms along n: the assembly
+                          // writes no lever-arm rows (only the 6-dof kernels read them)
 };
 
 // partners per contact row kept by the one-pass pair search; a row with more is

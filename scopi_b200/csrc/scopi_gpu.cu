@@ -454,6 +454,7 @@ struct scopi_gpu_handle {
         s.gamma_min = P.gamma_min;
         s.gamma_tol = P.gamma_tol;
         s.mu = P.mu;
+        s.torque_free = sphere_mode() ? 1 : 0;
         return s;
     }
 
