@@ -435,65 +435,6 @@ __device__ __forceinline__ void for_each_pair_of(const Bodies& B, const StepPara
     }
 }
 
-// One pass over the half stencil: body k (cell-sorted slot) meets the bodies after it in its
-// own cell and those of the 13 (3D) / 4 (2D) neighbour cells that follow its cell in
-// (z, y, x) order, so every unordered pair of neighbouring cells is visited once.  A pair in
-// contact is counted in the row of its lower index (atomic slot) and its partner kept in
-// that row's scratch while the row has room; the row sort makes the order deterministic.
-template <int DIM>
-__global__ void k_pair_search(Bodies B, StepParams p, const Grid* grid, const int* cell_of, const int* cell_start,
-                              const int* cell_body, const double4* cell_pr, int* row_count, int* row_tmp) {
-    const Grid g = *grid;
-    constexpr int nst = DIM == 3 ? 14 : 5;
-    GRID_STRIDE(k, B.n - B.nin) {
-        const int a = cell_body[k];
-        const double4 A = cell_pr[k];
-        int cc[3];
-        cell_coords(g, cell_of[a - B.nin], cc);
-        for (int o = 0; o < nst; ++o) {
-            // o = 0: own cell; then the offsets with (dz, dy, dx) > (0, 0, 0) lexicographically
-            int dx = 0, dy = 0, dz = 0;
-            if (o > 0) {
-                const int q = o - 1;
-                if (DIM == 3) {
-                    if (q == 0) {
-                        dx = 1;
-                    } else if (q < 4) {
-                        dy = 1;
-                        dx = q - 2;
-                    } else {
-                        dz = 1;
-                        dy = (q - 4) / 3 - 1;
-                        dx = (q - 4) % 3 - 1;
-                    }
-                } else {
-                    if (q == 0) {
-                        dx = 1;
-                    } else {
-                        dy = 1;
-                        dx = q - 2;
-                    }
-                }
-            }
-            const int x = cc[0] + dx, y = cc[1] + dy, z = cc[2] + dz;
-            if (x < 0 || x >= g.nc[0] || y < 0 || y >= g.nc[1] || z >= g.nc[2]) continue;
-            const int cid = (z * g.nc[1] + y) * g.nc[0] + x;
-            const int t1 = cell_start[cid + 1];
-            for (int t = o == 0 ? (int)k + 1 : cell_start[cid]; t < t1; ++t) {
-                const int b = cell_body[t];
-                if (B.scene && B.scene[a] != B.scene[b]) continue;
-                const double4 Bb = cell_pr[t];
-                const bool a_lo = a < b;
-                if (!pair_in_contact<DIM>(p, a_lo ? A : Bb, a_lo ? Bb : A)) continue;
-                const int lo = a_lo ? a : b, hi = a_lo ? b : a;
-                const int r = lo - B.nin;
-                const int slot = atomicAdd(&row_count[r], 1);
-                if (slot < kRowCap) row_tmp[(long long)r * kRowCap + slot] = hi;
-            }
-        }
-    }
-}
-
 // Offset o of the half stencil: o = 0 the own cell, then the (dz, dy, dx) > (0, 0, 0) in
 // lexicographic order (13 in 3D, 4 in 2D).
 template <int DIM>
@@ -522,10 +463,14 @@ __device__ __forceinline__ void half_stencil(int o, int& dx, int& dy, int& dz) {
     }
 }
 
-// The same pairs as k_pair_search, one warp per cell: the candidate pairs of the cell with
-// itself (a < b by slot) and with its half-stencil neighbours are numbered, the warp's lanes
-// take them 32 at a time (so the uneven cell counts do not idle lanes), and each is tested and
-// emitted exactly as k_pair_search does (lower index first, atomic row slot).
+// The pair search over the half stencil, one warp per cell: a body meets the bodies after it
+// in its own cell and those of the 13 (3D) / 4 (2D) neighbour cells that follow its cell in
+// (z, y, x) order, so every unordered pair of neighbouring cells is visited once.  The
+// candidate pairs of the cell with itself (a < b by slot) and with its half-stencil neighbours
+// are numbered, and the warp's lanes take them 32 at a time (so the uneven cell counts do not
+// idle lanes).  A pair in contact is tested with the lower index first, counted in the row of
+// its lower index (atomic slot) and its partner kept in that row's scratch while the row has
+// room; the row sort makes the order deterministic.
 constexpr int kSearchWarps = 8;
 template <int DIM>
 __global__ void __launch_bounds__(32 * kSearchWarps, 4) k_pair_search_cells(Bodies B, StepParams p, const Grid* grid,
