@@ -102,6 +102,12 @@ def lib():
         L.orc_se2_hybrid.restype = C.c_int
         L.orc_se2_hybrid.argtypes = [P, P, P, C.POINTER(C.c_int)]
         L.orc_se2_system.argtypes = [P, P, P, P, P]
+        L.orc_sphere_se.restype = C.c_int
+        L.orc_sphere_se.argtypes = [C.c_int, P, P, C.c_int, C.c_int, P]
+        L.orc_se2_plane.restype = C.c_int
+        L.orc_se2_plane.argtypes = [P, P, P]
+        L.orc_lu_solve4.restype = C.c_int
+        L.orc_lu_solve4.argtypes = [P, P, P]
         _lib = L
     return _lib
 
@@ -317,3 +323,45 @@ def hybrid_solve(s1, s2, u0):
     a, b = np.ascontiguousarray(s1, float), np.ascontiguousarray(s2, float)
     info = lib().orc_se_se_hybrid(_dp(a), _dp(b), _dp(u), C.byref(nfev))
     return {"u": u, "info": info, "nfev": nfev.value}
+
+
+def sphere_record(c, q, r):
+    """Sphere record {c[3], q[4] (w, x, y, z), radius} of the sphere-superellipsoid entry point."""
+    return np.concatenate([np.asarray(c, float).ravel()[:3], np.asarray(q, float).ravel()[:4], [float(r)]])
+
+
+def sphere_se(dim, se, sph, reference_labels=True, se_is_i=True):
+    """closest_points(sphere, superellipsoid) (closest_points.hpp:944-1302 in 3D, 1316-1463 in
+    2D) on a superellipsoid record and a sphere record.  reference_labels: the reference's own
+    result (pi on the superellipsoid, nij the sphere's unit normal); else the pair labelled by
+    body (superellipsoid = body i when se_is_i).  'newton' is the Newton method's return:
+    iterations, -1 at the iteration cap, -2 on a singular Jacobian."""
+    out = np.zeros(16)
+    a, b = np.ascontiguousarray(se, float), np.ascontiguousarray(sph, float)
+    info = lib().orc_sphere_se(int(dim), _dp(a), _dp(b), int(bool(reference_labels)), int(bool(se_is_i)), _dp(out))
+    r = _unpack(out)
+    r["newton"] = info
+    if dim == 2:
+        r["u"] = r["u"][:2]
+    return r
+
+
+def se2_plane(s, plane_c, plane_angle):
+    """closest_points(superellipsoid<2>, plane<2>) in closed form; the plane is (centre, angle)."""
+    out = np.zeros(15)
+    a = np.ascontiguousarray(s, float)
+    q = [np.cos(plane_angle / 2), 0.0, 0.0, np.sin(plane_angle / 2)]
+    p = np.ascontiguousarray(np.concatenate([[plane_c[0], plane_c[1], 0.0], q]))
+    lib().orc_se2_plane(_dp(a), _dp(p), _dp(out))
+    r = _unpack(out)
+    r["u"] = r["u"][:2]
+    return r
+
+
+def lu_solve4(A, b):
+    """x with A x = b by the Newton method's solve (column-major inside); None on a zero pivot."""
+    a = np.ascontiguousarray(np.asarray(A, float).T.ravel())
+    bb = np.ascontiguousarray(np.asarray(b, float).ravel())
+    x = np.zeros(4)
+    rc = lib().orc_lu_solve4(_dp(a), _dp(bb), _dp(x))
+    return None if rc else x

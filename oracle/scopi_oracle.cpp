@@ -259,6 +259,24 @@ struct orc_solver {
             if (!(lim > 0.0) || s2 > lim * lim * (1.0 + 1e-9)) return false;
             if (orc_se::support_gap(se_of(a), se_of(b), 2) > p.dmax + 1e-9 * lim) return false;
             c = from_pair(orc_se::se2_se2(se_of(a), se_of(b)));
+        } else if ((sa == ORC_SPHERE && sb == ORC_SUPERELLIPSOID) || (sa == ORC_SUPERELLIPSOID && sb == ORC_SPHERE)) {
+            // closest_points(sphere, superellipsoid) and its mirror (closest_points.hpp:944-1302,
+            // 1316-1463): the same bounding-sphere and line-of-centres bounds as the pairs of
+            // two superellipsoids, then the reference's Newton solve, labelled by body
+            const int64_t e = sa == ORC_SUPERELLIPSOID ? a : b, sp = sa == ORC_SPHERE ? a : b;
+            double s2 = 0.0;
+            for (int k = 0; k < dim; ++k) s2 += (pos[a][k] - pos[b][k]) * (pos[a][k] - pos[b][k]);
+            const double lim = radius[a] + radius[b] + p.dmax;
+            if (!(lim > 0.0) || s2 > lim * lim * (1.0 + 1e-9)) return false;
+            const orc_se::SE E = se_of(e), S = sphere_of(sp);
+            if (orc_se::support_gap(E, S, dim) > p.dmax + 1e-9 * lim) return false;
+            c = from_pair(e == a ? orc_se::sphere_se_pair(E, S, true, dim) : orc_se::sphere_se_pair(S, E, false, dim));
+        } else if (dim == 2 && sa == ORC_SUPERELLIPSOID && sb == ORC_PLANE) {
+            c = from_pair(orc_se::se2_plane(se_of(a), plane_of(b)));
+        } else if (dim == 2 && sa == ORC_PLANE && sb == ORC_SUPERELLIPSOID) {  // closest_points.hpp:1951-1958
+            c = from_pair(orc_se::se2_plane(se_of(b), plane_of(a)));
+            for (auto& x : c.nij) x *= -1.;
+            std::swap(c.pi, c.pj);
         } else if (dim == 3 && sa == ORC_SUPERELLIPSOID && sb == ORC_PLANE) {
             c = from_pair(orc_se::se_plane(se_of(a), plane_of(b)));
         } else if (dim == 3 && sa == ORC_PLANE && sb == ORC_SUPERELLIPSOID) {  // closest_points.hpp:1761-1768
@@ -1118,6 +1136,7 @@ struct orc_solver {
         s.n = se_par[b][4];
         return s;
     }
+    orc_se::SE sphere_of(int64_t b) const { return orc_se::as_se(pos[b], rotation3(q[b]), radius[b]); }
     orc_se::Plane plane_of(int64_t b) const {
         orc_se::Plane p;
         p.c = pos[b];
@@ -1342,6 +1361,34 @@ void orc_se2_system(const double* s1, const double* s2, const double* u, double*
     const orc_se::SE a = se_from(s1), b = se_from(s2);
     orc_se::se2_F(a, b, u, F);
     orc_se::se2_J(a, b, u, J);
+}
+
+// sph = (centre[3], quaternion[4], radius); out as orc_se_se plus out[15] = the method's return
+int orc_sphere_se(int dim, const double* se, const double* sph, int reference_labels, int se_is_i, double* out) {
+    const orc_se::SE E = se_from(se);
+    const orc_se::SE S = orc_se::as_se({sph[0], sph[1], sph[2]}, rotation3({sph[3], sph[4], sph[5], sph[6]}), sph[7]);
+    const orc_se::PairOut o = reference_labels ? orc_se::sphere_se_newton(E, S, dim)
+                              : (se_is_i ? orc_se::sphere_se_pair(E, S, true, dim) : orc_se::sphere_se_pair(S, E, false, dim));
+    write_pair(o, out);
+    out[15] = o.info;
+    return o.info;
+}
+
+int orc_se2_plane(const double* s, const double* plane, double* out) {
+    orc_se::Plane p;
+    p.c = {plane[0], plane[1], plane[2]};
+    p.R = rotation3({plane[3], plane[4], plane[5], plane[6]});
+    const orc_se::PairOut o = orc_se::se2_plane(se_from(s), p);
+    write_pair(o, out);
+    return o.info;
+}
+
+// A x = b for a column-major 4 x 4 A (the Newton method's solve); 0, or -2 on a zero pivot
+int orc_lu_solve4(const double* A, const double* b, double* x) {
+    double a[16];
+    std::memcpy(a, A, sizeof(a));
+    std::memcpy(x, b, 4 * sizeof(double));
+    return orc_se::lu_solve<4>(a, x) ? 0 : -2;
 }
 
 }  // extern "C"

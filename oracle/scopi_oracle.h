@@ -142,6 +142,17 @@ void orc_se_se_system(const double* s1, const double* s2, const double* u, doubl
 int orc_se2_se2(const double* s1, const double* s2, double* out);
 int orc_se2_hybrid(const double* s1, const double* s2, double* u, int* nfev);
 void orc_se2_system(const double* s1, const double* s2, const double* u, double* F, double* J);
+// closest_points(sphere, superellipsoid) (closest_points.hpp:944-1302, 1316-1463): sph =
+// (centre[3], quaternion[4], radius); reference_labels = 1 gives the reference's own result
+// (pi on the superellipsoid, nij the sphere's normal, the Newton method alone), 0 the engine's
+// pair (the Newton method, the hybrid method where it fails) labelled by body with the
+// superellipsoid as body i when se_is_i; out as orc_se_se, out[15] = the solve's status (the
+// Newton method's iterations, -1 at its cap, -2 singular; 100 + the hybrid method's info)
+int orc_sphere_se(int dim, const double* se, const double* sph, int reference_labels, int se_is_i, double* out);
+// closest_points(superellipsoid<2>, plane<2>) in closed form; out as orc_se_se
+int orc_se2_plane(const double* s, const double* plane, double* out);
+// the Newton method's linear solve (dgesv restated) for a column-major 4 x 4 system
+int orc_lu_solve4(const double* A, const double* b, double* x);
 /* A.u and A^T.f on the current contact list (3C and 6*na long vectors). */
 int orc_amat(const orc_solver* s, const double* u, double* out);
 int orc_atmat(const orc_solver* s, const double* f, double* out);

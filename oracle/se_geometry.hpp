@@ -873,4 +873,337 @@ inline PairOut se2_se2(const SE& s1, const SE& s2) {
     return o;
 }
 
+// ------------------------------------------------------------------ damped Newton
+// newton_method (utils.hpp:81-118) in n unknowns: d = solve(J(u), -F(u)); return when
+// |d| < xtol (tested before the residual) or |F(u)| < ftol; otherwise a backtracking line
+// search t = 1, 0.99, 0.98, ... while |F(u + t d)| > |F(u)| and t > 0.01, then u += t d; at
+// most itermax steps (then -1).  The reference solves with LAPACK's dgesv (through
+// xt::linalg::solve); the solve here restates the published reference-LAPACK algorithm for a
+// small dense matrix: dgetf2 (column pivot = the first entry of largest |a| on or below the
+// diagonal, multipliers scaled by the pivot's reciprocal when |pivot| >= the safe minimum,
+// rank-1 update of the trailing block) and dgetrs (the row interchanges, then the unit lower
+// and the upper triangular solves).  An optimised LAPACK orders these operations its own way,
+// so the last bits of d are not pinned.  A zero pivot (the reference's solve throws there)
+// ends the method with -2.  Norms are sqrt(sum of squares).
+constexpr double kSafeMin = 2.2250738585072014e-308;  // dlamch('S')
+
+template <int N>
+inline bool lu_solve(double* A, double* b) {  // A column-major N x N (overwritten), b (in: rhs, out: x)
+    int piv[N];
+    for (int j = 0; j < N; ++j) {
+        int p = j;
+        double big = std::abs(A[j + N * j]);
+        for (int i = j + 1; i < N; ++i)
+            if (std::abs(A[i + N * j]) > big) {
+                big = std::abs(A[i + N * j]);
+                p = i;
+            }
+        piv[j] = p;
+        if (A[p + N * j] == 0.0) return false;
+        if (p != j)
+            for (int k = 0; k < N; ++k) std::swap(A[j + N * k], A[p + N * k]);
+        const double pv = A[j + N * j];
+        if (std::abs(pv) >= kSafeMin) {
+            const double r = 1.0 / pv;
+            for (int i = j + 1; i < N; ++i) A[i + N * j] *= r;
+        } else {
+            for (int i = j + 1; i < N; ++i) A[i + N * j] /= pv;
+        }
+        for (int k = j + 1; k < N; ++k) {
+            const double t = -A[j + N * k];
+            for (int i = j + 1; i < N; ++i) A[i + N * k] += A[i + N * j] * t;
+        }
+    }
+    for (int j = 0; j < N; ++j)
+        if (piv[j] != j) std::swap(b[j], b[piv[j]]);
+    for (int k = 0; k < N; ++k)
+        if (b[k] != 0.0)
+            for (int i = k + 1; i < N; ++i) b[i] -= b[k] * A[i + N * k];
+    for (int k = N - 1; k >= 0; --k)
+        if (b[k] != 0.0) {
+            b[k] /= A[k + N * k];
+            for (int i = 0; i < k; ++i) b[i] -= b[k] * A[i + N * k];
+        }
+    return true;
+}
+
+template <int N>
+inline double norm_n(const double* x) {
+    double s = 0.0;
+    for (int k = 0; k < N; ++k) s += x[k] * x[k];
+    return std::sqrt(s);
+}
+
+// returns the iterations taken (>= 0), -1 after itermax steps, -2 on a zero pivot
+template <int N, typename Fun, typename Jac>
+inline int newton(Fun&& fun, Jac&& jac, double* u, int itermax = 200, double ftol = 1.0e-10, double xtol = 1.0e-7) {
+    for (int cc = 0; cc < itermax; ++cc) {
+        double F[N], J[N * N], d[N];
+        fun(u, F);
+        jac(u, J);
+        for (int k = 0; k < N; ++k) d[k] = -F[k];
+        if (!lu_solve<N>(J, d)) return -2;
+        if (norm_n<N>(d) < xtol) return cc;
+        const double ferr = norm_n<N>(F);
+        if (ferr < ftol) return cc;
+        double t = 1;
+        for (;;) {
+            double x[N], Ft[N];
+            for (int k = 0; k < N; ++k) x[k] = u[k] + t * d[k];
+            fun(x, Ft);
+            if (!(norm_n<N>(Ft) > ferr && t > 0.01)) break;
+            t -= 0.01;
+        }
+        for (int k = 0; k < N; ++k) u[k] += t * d[k];
+    }
+    return -1;
+}
+
+// linspace(start, stop, num) with its endpoint (xtensor): start + k (stop - start)/(num - 1),
+// the last value stop itself
+inline double linspace_at(double start, double stop, int num, int k) {
+    if (k == num - 1) return stop;
+    return start + k * ((stop - start) / (num - 1));
+}
+
+// ------------------------------------------------------- sphere - superellipsoid
+// A sphere of radius r is the superellipsoid with semi-axes (r, r, r) and squareness (1, 1):
+// its parametrisation is then exactly sphere::point (sphere.hpp:195-211), since
+// sign(t)|t|^1 = t.  Its unit normal is sphere::normal (sphere.hpp:213-234).
+inline SE as_se(const V3& c, const M3& R, double r) {
+    SE s;
+    s.c = c;
+    s.R = R;
+    s.r[0] = s.r[1] = s.r[2] = r;
+    s.e = s.n = 1.0;
+    return s;
+}
+inline V3 sphere_normal(const SE& sph, double a, double b) {  // sphere.hpp:225-234
+    const V3 n = {std::cos(a) * std::cos(b), std::cos(a) * std::sin(b), std::sin(a)};
+    V3 w = mv(sph.R, n);
+    const double l = norm(w);
+    for (auto& x : w) x /= l;
+    return w;
+}
+
+// closest_points(sphere<3>, superellipsoid<3>), closest_points.hpp:944-1282: unknowns
+// u = (a1, b1, a2, b2), the superellipsoid's angles then the sphere's;
+//   F = [ (p2 - p1) x n1 ; n1.n2 + |n1||n2| ],  n1 = sign(cos a1) N1(a1, b1),  n2 = sign(cos a2) N2(a2, b2)
+// with N the unnormalised outward normals of superellipsoid::normal (the reference's
+// expressions carry the factor sign(cos a) on both normals, :1013-1037).  The Jacobian is the
+// chain rule on the parametrisation's derivatives.
+inline void sphse_F(const SE& s1, const SE& s2, const double* u, double* F) {
+    const Local L1 = local(s1, u[0], u[1]), L2 = local(s2, u[2], u[3]);
+    const double k1 = sgn(std::cos(u[0])), k2 = sgn(std::cos(u[2]));
+    const V3 p1 = mv(s1.R, L1.p), p2 = mv(s2.R, L2.p);
+    const V3 d = {p2[0] + s2.c[0] - p1[0] - s1.c[0], p2[1] + s2.c[1] - p1[1] - s1.c[1],
+                  p2[2] + s2.c[2] - p1[2] - s1.c[2]};
+    V3 n1 = mv(s1.R, L1.N), n2 = mv(s2.R, L2.N);
+    for (int c = 0; c < 3; ++c) {
+        n1[c] *= k1;
+        n2[c] *= k2;
+    }
+    const V3 x = cross(d, n1);
+    F[0] = x[0];
+    F[1] = x[1];
+    F[2] = x[2];
+    F[3] = dot(n1, n2) + norm(n1) * norm(n2);
+}
+inline void sphse_J(const SE& s1, const SE& s2, const double* u, double* J) {  // column-major 4x4
+    const Local L1 = local(s1, u[0], u[1]), L2 = local(s2, u[2], u[3]);
+    const double k1 = sgn(std::cos(u[0])), k2 = sgn(std::cos(u[2]));
+    const V3 p1 = mv(s1.R, L1.p), p2 = mv(s2.R, L2.p);
+    const V3 d = {p2[0] + s2.c[0] - p1[0] - s1.c[0], p2[1] + s2.c[1] - p1[1] - s1.c[1],
+                  p2[2] + s2.c[2] - p1[2] - s1.c[2]};
+    V3 n1 = mv(s1.R, L1.N), n2 = mv(s2.R, L2.N);
+    const V3 z = {0, 0, 0};
+    V3 dd[4], dn1[4], dn2[4];
+    const V3 pa1 = mv(s1.R, L1.pa), pb1 = mv(s1.R, L1.pb);
+    dd[0] = {-pa1[0], -pa1[1], -pa1[2]};
+    dd[1] = {-pb1[0], -pb1[1], -pb1[2]};
+    dd[2] = mv(s2.R, L2.pa);
+    dd[3] = mv(s2.R, L2.pb);
+    dn1[0] = mv(s1.R, L1.Na);
+    dn1[1] = mv(s1.R, L1.Nb);
+    dn1[2] = dn1[3] = z;
+    dn2[0] = dn2[1] = z;
+    dn2[2] = mv(s2.R, L2.Na);
+    dn2[3] = mv(s2.R, L2.Nb);
+    for (int c = 0; c < 3; ++c) {
+        n1[c] *= k1;
+        n2[c] *= k2;
+        for (int q = 0; q < 4; ++q) {
+            dn1[q][c] *= k1;
+            dn2[q][c] *= k2;
+        }
+    }
+    const double l1 = norm(n1), l2 = norm(n2);
+    for (int q = 0; q < 4; ++q) {
+        const V3 a = cross(dd[q], n1), b = cross(d, dn1[q]);
+        J[0 + 4 * q] = a[0] + b[0];
+        J[1 + 4 * q] = a[1] + b[1];
+        J[2 + 4 * q] = a[2] + b[2];
+        J[3 + 4 * q] = dot(dn1[q], n2) + dot(n1, dn2[q]) + dot(n1, dn1[q]) / l1 * l2 + l1 * dot(n2, dn2[q]) / l2;
+    }
+}
+// start (closest_points.hpp:1262-1274): ten angle pairs per body, (ainit(k), binit(k)) with
+// ainit = linspace(-pi/2, pi/2, 10), binit = linspace(-pi, pi, 10); the first minimum of
+// |p1 - p2| over the 10 x 10 pairs in row-major order
+inline void sphse_start(const SE& s1, const SE& s2, double* u0) {
+    const double pi = 4 * std::atan(1);
+    constexpr int num = 10;
+    double A[num], Bv[num];
+    for (int k = 0; k < num; ++k) {
+        A[k] = linspace_at(-pi / 2, pi / 2, num, k);
+        Bv[k] = linspace_at(-pi, pi, num, k);
+    }
+    V3 P1[num], P2[num];
+    for (int k = 0; k < num; ++k) {
+        P1[k] = point(s1, A[k], Bv[k]);
+        P2[k] = point(s2, A[k], Bv[k]);
+    }
+    double best = INFINITY;
+    int bi = 0, bj = 0;
+    for (int i = 0; i < num; ++i)
+        for (int j = 0; j < num; ++j) {
+            const V3 df = {P1[i][0] - P2[j][0], P1[i][1] - P2[j][1], P1[i][2] - P2[j][2]};
+            const double v = norm(df);
+            if (v < best) {
+                best = v;
+                bi = i;
+                bj = j;
+            }
+        }
+    u0[0] = A[bi];
+    u0[1] = Bv[bi];
+    u0[2] = A[bj];
+    u0[3] = Bv[bj];
+}
+// 2D start (closest_points.hpp:1425-1436): binit = {-pi, -pi/2, 0.001, pi/2} on both bodies,
+// the first minimum of |p1 - p2| over the 4 x 4 pairs in row-major order
+inline void sphse2_start(const SE& s1, const SE& s2, double* u0) {
+    const double pi = 4 * std::atan(1);
+    const double binit[4] = {-pi, -pi / 2, 0.001, pi / 2};
+    double best = INFINITY;
+    u0[0] = u0[1] = binit[0];
+    for (int i = 0; i < 4; ++i) {
+        const V3 P1 = point2(s1, binit[i]);
+        for (int j = 0; j < 4; ++j) {
+            const V3 P2 = point2(s2, binit[j]);
+            const double dx = P1[0] - P2[0], dy = P1[1] - P2[1];
+            const double v = std::sqrt(dx * dx + dy * dy);
+            if (v < best) {
+                best = v;
+                u0[0] = binit[i];
+                u0[1] = binit[j];
+            }
+        }
+    }
+}
+
+// closest_points(sphere, superellipsoid) in the reference's result convention
+// (closest_points.hpp:1275-1280 in 3D, 1437-1441 in 2D): pi on the superellipsoid, pj on the
+// sphere, nij = the sphere's unit normal at pj, dij = (pi - pj).nij; info = the Newton
+// method's return.  2D: u = (b1, b2) and F = [ (p2 - p1) x n1 ; n1.n2 + |n1||n2| ] with
+// n2 = the rotated r (cos b2, sin b2): se2_F / se2_J with the sphere as the superellipsoid
+// (r, r), e = 1 (the 2D expressions carry no sign factors).
+inline PairOut sphere_se_newton(const SE& se, const SE& sph, int dim) {
+    PairOut o;
+    double u[4] = {0, 0, 0, 0};
+    if (dim == 3) {
+        sphse_start(se, sph, u);
+        o.info = newton<4>([&](const double* x, double* F) { sphse_F(se, sph, x, F); },
+                           [&](const double* x, double* J) { sphse_J(se, sph, x, J); }, u);
+        o.pi = point(se, u[0], u[1]);
+        o.pj = point(sph, u[2], u[3]);
+        o.nij = sphere_normal(sph, u[2], u[3]);
+    } else {
+        sphse2_start(se, sph, u);
+        o.info = newton<2>([&](const double* x, double* F) { se2_F(se, sph, x, F); },
+                           [&](const double* x, double* J) { se2_J(se, sph, x, J); }, u);
+        o.pi = point2(se, u[0]);
+        o.pj = point2(sph, u[1]);
+        o.nij = normal2(sph, u[1]);  // sphere::normal(b): the rotated r (cos b, sin b), normalised
+    }
+    for (int k = 0; k < 4; ++k) o.u[k] = u[k];
+    const V3 df = {o.pi[0] - o.pj[0], o.pi[1] - o.pj[1], o.pi[2] - o.pj[2]};
+    o.dij = dot(df, o.nij);
+    return o;
+}
+
+// The engine's acceptance test.  F = 0 of the reference's system also holds at pairs that are
+// not the closest points: the farther point of the sphere (the factors sign(cos a) let the
+// two normals be parallel instead of opposite) or the far side of the superellipsoid, and
+// its start (ten samples per body along a diagonal of the angle square) often leads the
+// Newton method there, or to no convergence in 200 steps (the reference then keeps the last
+// iterate; on a singular Jacobian its solve throws).  For a convex body (squareness in
+// (0, 2)) a surface point p whose outward unit normal points at the sphere's centre c,
+// c - p = t N(p) with t > 0, is the point nearest c, and the sphere's nearest point then lies
+// on the segment from c to p.  The Newton result is kept when it converged and both hold to
+// within cos >= 1 - 1e-6; otherwise the pair is solved as the pair of superellipsoids it is
+// (the sphere with semi-axes (r, r, r) and squareness 1: se_se / se2_se2).
+inline bool sphere_se_valid(const SE& se, const SE& sph, int dim, const PairOut& o) {
+    if (o.info < 0) return false;
+    const double cos_tol = 1.0 - 1e-6;
+    const V3 w = {o.pi[0] - sph.c[0], o.pi[1] - sph.c[1], dim == 3 ? o.pi[2] - sph.c[2] : 0.0};
+    const double L = norm(w);
+    if (!(L > 0)) return false;
+    const V3 nu = {w[0] / L, w[1] / L, w[2] / L};
+    const V3 N = dim == 3 ? normal(se, o.u[0], o.u[1]) : normal2(se, o.u[0]);
+    return -dot(N, nu) >= cos_tol && dot(o.nij, nu) >= cos_tol;
+}
+
+// The engine's pair of (body i, body j), one of them a sphere (as_se) and the other a
+// superellipsoid, labelled as every other closest_points function labels its pair: pi on
+// body i, pj on body j, nij the outward normal of j at pj, pointing toward i (so that
+// dij + dt nij.(v_i - v_j) is the first-order gap).  The reference's sphere-superellipsoid
+// functions give, for (sphere i, superellipsoid j), the points and normal of the pair (j, i)
+// (closest_points.hpp:1275-1280), and for (superellipsoid i, sphere j) that result swapped
+// and negated (:1295-1302); with either labelling the contact row would push the bodies
+// together.  Here the Newton result R (pi on the superellipsoid, nij the sphere's normal) is
+// labelled by body when sphere_se_valid accepts it (info = its iterations); otherwise the
+// superellipsoid-pair solve of (i, j) gives the pair (info = 100 + the hybrid method's info).
+inline PairOut sphere_se_pair(const SE& bi, const SE& bj, bool i_is_se, int dim) {
+    const SE& se = i_is_se ? bi : bj;
+    const SE& sph = i_is_se ? bj : bi;
+    PairOut o = sphere_se_newton(se, sph, dim);
+    if (sphere_se_valid(se, sph, dim, o)) {
+        if (!i_is_se) {
+            std::swap(o.pi, o.pj);
+            for (auto& x : o.nij) x = -x;
+        }
+        return o;
+    }
+    o = dim == 3 ? se_se(bi, bj) : se2_se2(bi, bj);
+    o.info += 100;
+    return o;
+}
+
+// closest_points(superellipsoid<2>, plane<2>), closest_points.hpp:1783-1949, in closed form as
+// in 3D (se_plane): its system's second equation receives the signed centre-plane distance
+// where it needs the side (:1787, :1845), so its Newton has no root to find for bodies nearer
+// to the plane than one length unit; the solution of the intended system is the body point
+// whose outward normal is opposite to the plane normal oriented toward the body.  The plane
+// normal is column 0 of the plane's rotation (plane.hpp:143-147); u[1] = the plane coordinate
+// of pj along column 1.
+inline PairOut se2_plane(const SE& s, const Plane& P) {
+    const double np[2] = {P.R[0][0], P.R[1][0]};
+    const double rel[2] = {s.c[0] - P.c[0], s.c[1] - P.c[1]};
+    const double sg = rel[0] * np[0] + rel[1] * np[1] < 0 ? -1.0 : 1.0;
+    const double m0 = -sg * (s.R[0][0] * np[0] + s.R[1][0] * np[1]);
+    const double m1 = -sg * (s.R[0][1] * np[0] + s.R[1][1] * np[1]);
+    const double b = support_angle2(s, m0, m1);
+    PairOut o;
+    o.info = 0;
+    o.pi = point2(s, b);
+    const double h = (o.pi[0] - P.c[0]) * np[0] + (o.pi[1] - P.c[1]) * np[1];
+    o.pj = {o.pi[0] - h * np[0], o.pi[1] - h * np[1], 0.0};
+    o.nij = {sg * np[0], sg * np[1], 0.0};
+    o.dij = (o.pi[0] - o.pj[0]) * o.nij[0] + (o.pi[1] - o.pj[1]) * o.nij[1];
+    o.u[0] = b;
+    o.u[1] = P.R[0][1] * (o.pj[0] - P.c[0]) + P.R[1][1] * (o.pj[1] - P.c[1]);
+    o.u[2] = o.u[3] = 0.0;
+    return o;
+}
+
 }  // namespace orc_se

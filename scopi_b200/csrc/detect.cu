@@ -10,6 +10,7 @@
 
 #include "kernels.cuh"
 #include "se_geom.cuh"
+#include "se_newton.cuh"
 
 namespace scopi_gpu {
 
@@ -174,7 +175,10 @@ __device__ __forceinline__ void flip(PairGeom& g) {
     }
 }
 
-// closest_points_dispatcher restricted to the pairs of the hot path (a < b).
+// closest_points_dispatcher restricted to the pairs of the hot path (a < b).  SE = the scene
+// holds superellipsoids: their obstacle cases (plane-superellipsoid) compile into those
+// instantiations only, so the sphere scenes' kernels carry none of their code.
+template <bool SE>
 __device__ __forceinline__ bool exact_pair(const Bodies& B, int dim, int a, int b, PairGeom& g) {
     const int sa = B.shape[a], sb = B.shape[b];
     const double* xa = B.pos + 3 * (long long)a;
@@ -191,15 +195,32 @@ __device__ __forceinline__ bool exact_pair(const Bodies& B, int dim, int a, int 
         flip(g);
     } else if (sa == kSphere && sb == kSegment && dim == 2) {
         sphere_segment(xa, B.radius[a], xb, B.q + 4 * (long long)b, B.length[b], g);
-    } else if (sa == kPlane && sb == kSuperellipsoid && dim == 3) {  // closest_points.hpp:1761-1768
-        const se::Body s = se::load(B, b);
-        se::body_plane(s, xa, B.q + 4 * (long long)a, g.pi, g.pj, g.nij, g.dij);
-        flip(g);
-    } else if (sa == kSuperellipsoid && sb == kPlane && dim == 3) {
-        const se::Body s = se::load(B, a);
-        se::body_plane(s, xb, B.q + 4 * (long long)b, g.pi, g.pj, g.nij, g.dij);
     } else {
-        return false;  // superellipsoid pairs: se.cu
+        if constexpr (SE) {
+            if (sa == kPlane && sb == kSuperellipsoid && dim == 3) {  // closest_points.hpp:1761-1768
+                const se::Body s = se::load(B, b);
+                se::body_plane(s, xa, B.q + 4 * (long long)a, g.pi, g.pj, g.nij, g.dij);
+                flip(g);
+                return true;
+            }
+            if (sa == kSuperellipsoid && sb == kPlane && dim == 3) {
+                const se::Body s = se::load(B, a);
+                se::body_plane(s, xb, B.q + 4 * (long long)b, g.pi, g.pj, g.nij, g.dij);
+                return true;
+            }
+            if (sa == kPlane && sb == kSuperellipsoid && dim == 2) {  // closest_points.hpp:1951-1958
+                const se::Body2 s = se::load2(B, b);
+                se::body_plane2(s, xa, B.q + 4 * (long long)a, g.pi, g.pj, g.nij, g.dij);
+                flip(g);
+                return true;
+            }
+            if (sa == kSuperellipsoid && sb == kPlane && dim == 2) {
+                const se::Body2 s = se::load2(B, a);
+                se::body_plane2(s, xb, B.q + 4 * (long long)b, g.pi, g.pj, g.nij, g.dij);
+                return true;
+            }
+        }
+        return false;  // superellipsoid pairs: se.cu; sphere-superellipsoid: k_geometry
     }
     return true;
 }
@@ -645,13 +666,13 @@ __device__ __forceinline__ void obs_pair(const Bodies& B, long long k, int& o, i
     b = B.nin + B.obs_a0[o] + (int)(k - B.obs_off[o]);
 }
 
-template <int DIM>
+template <int DIM, bool SE>
 __global__ void k_obs_flags(Bodies B, StepParams p, long long nobs, int* flag) {
     GRID_STRIDE(k, nobs) {
         int o, b;
         obs_pair(B, k, o, b);
         PairGeom g;
-        flag[k] = (exact_pair(B, DIM, o, b, g) && g.dij < p.dmax) ? 1 : 0;
+        flag[k] = (exact_pair<SE>(B, DIM, o, b, g) && g.dij < p.dmax) ? 1 : 0;
     }
 }
 
@@ -684,15 +705,52 @@ __global__ void k_set_cobs(const int* totals, Sizes* sizes) {
 // closest points of the listed pairs; viscous gamma carried over from the previous list
 // by (i, j) (transfer, include/scopi/solver.hpp:241-258); the last n_links rows are worm
 // links, whose normal and distance are negated (add_contact.hpp:17-18).
-template <int DIM>
-__global__ void k_geometry(Bodies B, StepParams p, Contacts c, const Sizes* sizes, Contacts old_c, const int* old_C) {
+// SE (scenes with superellipsoids): a sphere-superellipsoid row takes the reference's Newton
+// solve (se_newton.cuh), labelled by body (pi on body i, pj on body j, nij the outward
+// normal of j pointing toward i, as every other pair: the reference's own functions give the
+// points and normal of the pair (j, i) for (sphere, superellipsoid) and that result swapped
+// and negated for (superellipsoid, sphere), closest_points.hpp:1275-1280, 1295-1302, with
+// which the contact row would push the bodies together); need_se[k] = 1 leaves the row to
+// launch_se_pairs (pairs of superellipsoids, and the sphere rows whose solve was refused).
+template <int DIM, bool SE>
+__global__ void k_geometry(Bodies B, StepParams p, Contacts c, const Sizes* sizes, Contacts old_c, const int* old_C,
+                           int* need_se) {
     const int C = sizes->C;
     const int first_link = C - sizes->n_links;
     const int oC = old_C ? *old_C : 0;
     GRID_STRIDE(k, C) {
         const int a = c.ci[k], b = c.cj[k];
         PairGeom g;
-        if (!exact_pair(B, DIM, a, b, g)) {
+        bool known = exact_pair<SE>(B, DIM, a, b, g);
+        if constexpr (SE) {
+            const int sa = B.shape[a], sb = B.shape[b];
+            int need = 0;
+            if (sa == kSuperellipsoid && sb == kSuperellipsoid) {
+                need = 1;
+            } else if ((sa == kSphere && sb == kSuperellipsoid) || (sa == kSuperellipsoid && sb == kSphere)) {
+                const bool i_se = sa == kSuperellipsoid;
+                const int e = i_se ? a : b, sph = i_se ? b : a;
+                se::SphSeOut o;
+                if (DIM == 3)
+                    o = se::sphere_se3(se::load(B, e), se::sphere_as_body(B, sph));
+                else
+                    o = se::sphere_se2(se::load2(B, e), se::load_any2(B, sph));
+                if (o.valid) {
+                    const double sg = i_se ? 1.0 : -1.0;
+                    for (int d = 0; d < 3; ++d) {
+                        g.pi[d] = i_se ? o.pi[d] : o.pj[d];
+                        g.pj[d] = i_se ? o.pj[d] : o.pi[d];
+                        g.nij[d] = sg * o.nij[d];
+                    }
+                    g.dij = o.dij;
+                    known = true;
+                } else {
+                    need = 1;
+                }
+            }
+            if (need_se) need_se[k] = need;
+        }
+        if (!known) {
             g.dij = 0.0;
             for (int d = 0; d < 3; ++d) g.nij[d] = g.pi[d] = g.pj[d] = 0.0;
         }
@@ -1215,10 +1273,18 @@ void launch_detect(const Bodies& b, const StepParams& p, DetectWork& w, Contacts
     // obstacle rows come first in (i, j) order
     const long long nobs = w.obs_cap;  // nin * na, or the sum of the per-obstacle ranges of a batch
     if (nobs > 0) {
-        if (p.dim == 3)
-            k_obs_flags<3><<<blocks_for(nobs), kThreads, 0, s>>>(b, p, nobs, w.obs_flag);
-        else
-            k_obs_flags<2><<<blocks_for(nobs), kThreads, 0, s>>>(b, p, nobs, w.obs_flag);
+        const bool se = b.axes != nullptr;
+        if (p.dim == 3) {
+            if (se)
+                k_obs_flags<3, true><<<blocks_for(nobs), kThreads, 0, s>>>(b, p, nobs, w.obs_flag);
+            else
+                k_obs_flags<3, false><<<blocks_for(nobs), kThreads, 0, s>>>(b, p, nobs, w.obs_flag);
+        } else {
+            if (se)
+                k_obs_flags<2, true><<<blocks_for(nobs), kThreads, 0, s>>>(b, p, nobs, w.obs_flag);
+            else
+                k_obs_flags<2, false><<<blocks_for(nobs), kThreads, 0, s>>>(b, p, nobs, w.obs_flag);
+        }
         scan_exclusive(w.obs_flag, w.obs_pos, nullptr, (int)nobs, nobs, w.tmp_total + 0, w.scan_work, s,
                        &g_detect_launches);
         LAUNCHED(1);
@@ -1250,13 +1316,22 @@ void launch_detect(const Bodies& b, const StepParams& p, DetectWork& w, Contacts
 }
 
 void launch_geometry(const Bodies& b, const StepParams& p, Contacts& c, const Sizes* sizes, long long c_cap,
-                     const Contacts* old_c, const int* old_C, long long, cudaStream_t s) {
+                     const Contacts* old_c, const int* old_C, long long, cudaStream_t s, int* need_se) {
     Contacts oc{};
     if (old_c) oc = *old_c;
-    if (p.dim == 3)
-        k_geometry<3><<<blocks_for(c_cap), kThreads, 0, s>>>(b, p, c, sizes, oc, old_c ? old_C : nullptr);
-    else
-        k_geometry<2><<<blocks_for(c_cap), kThreads, 0, s>>>(b, p, c, sizes, oc, old_c ? old_C : nullptr);
+    const int* oC = old_c ? old_C : nullptr;
+    const int blocks = blocks_for(c_cap);
+    if (b.axes) {
+        if (p.dim == 3)
+            k_geometry<3, true><<<blocks, kThreads, 0, s>>>(b, p, c, sizes, oc, oC, need_se);
+        else
+            k_geometry<2, true><<<blocks, kThreads, 0, s>>>(b, p, c, sizes, oc, oC, need_se);
+    } else {
+        if (p.dim == 3)
+            k_geometry<3, false><<<blocks, kThreads, 0, s>>>(b, p, c, sizes, oc, oC, nullptr);
+        else
+            k_geometry<2, false><<<blocks, kThreads, 0, s>>>(b, p, c, sizes, oc, oC, nullptr);
+    }
     LAUNCHED(1);
 }
 

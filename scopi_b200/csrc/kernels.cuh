@@ -77,8 +77,12 @@ void launch_vap(const Bodies& b, const StepParams& p, cudaStream_t s, const Size
 void launch_detect(const Bodies& b, const StepParams& p, DetectWork& w, Contacts& out, Sizes* sizes, long long c_cap,
                    cudaStream_t s);
 // Closest points of the listed pairs + viscous gamma transfer from the previous list.
+// Scenes with superellipsoids (b.axes set) also solve the sphere-superellipsoid rows and set
+// need_se[k] = 1 on the rows left to launch_se_pairs (pairs of superellipsoids and the
+// sphere-superellipsoid rows whose Newton solve was refused), 0 on the others.
 void launch_geometry(const Bodies& b, const StepParams& p, Contacts& c, const Sizes* sizes, long long c_cap,
-                     const Contacts* old_c, const int* old_C, long long old_cap, cudaStream_t s);
+                     const Contacts* old_c, const int* old_C, long long old_cap, cudaStream_t s,
+                     int* need_se = nullptr);
 void launch_assemble(const Bodies& b, const StepParams& p, const Contacts& c, Assembly& a, Sizes* sizes,
                      long long c_cap, int* scan_work, int* tmp_total, cudaStream_t s);
 // with_coef: also the 6 FP64 coefficients per incidence (inc.coef) that the 6-dof
@@ -146,9 +150,10 @@ void launch_atmat(const Bodies& b, const StepParams& p, const Contacts& c, const
 
 // ----------------------------------------------------------------- se.cu
 long long se_launches();
-// closest points of the superellipsoid rows [C_obs, C) of c; u0: 4 doubles per row (scratch)
-void launch_se_pairs(int dim, const Bodies& b, Contacts& c, const Sizes* sizes, double* u0, int* counter, int grid,
-                     cudaStream_t s);
+// closest points of the rows k in [C_obs, C) of c with need[k] set (launch_geometry); u0: 4
+// doubles per row (scratch)
+void launch_se_pairs(int dim, const Bodies& b, Contacts& c, const Sizes* sizes, const int* need, double* u0,
+                     int* counter, int grid, cudaStream_t s);
 // candidate rows of src whose bodies are not provably farther apart than dmax (obstacle
 // rows all kept), compacted into dst
 void launch_se_prefilter(int dim, const Bodies& b, const Contacts& src, Contacts& dst, Sizes* sizes, double dmax,

@@ -690,17 +690,20 @@ struct scopi_gpu_handle {
         // solver.hpp:358-367); detection alone (assemble == false) is the contact method's
         if (assemble && n_links > 0) launch_append_links(h_sizes->C, n_links, d_links, cur, d_sizes_cur, stream);
         const bool tr = has_old && carries_gamma();
-        launch_geometry(b, sp, cur, d_sizes_cur, c_cap, tr ? &old : nullptr, tr ? &d_sizes_old->C : nullptr,
-                        c_cap, stream);
-        if (has_se) {
+        if (!has_se) {
+            launch_geometry(b, sp, cur, d_sizes_cur, c_cap, tr ? &old : nullptr, tr ? &d_sizes_old->C : nullptr,
+                            c_cap, stream);
+        } else {
             // the search kept bounding-sphere candidates: the pairs that can touch (gap along
-            // the line of centres <= dmax), their closest points, then the rows with
-            // dij < dmax (no viscous gamma to carry here); each filter compacts into the other
-            // list, which becomes the current one
+            // the line of centres <= dmax), the closest points of the spheres' rows, those of
+            // the rows flagged in d_se_keep (pairs of superellipsoids, sphere rows whose Newton
+            // solve was refused), then the rows with dij < dmax (no viscous gamma to carry
+            // here); each filter compacts into the other list, which becomes the current one
             launch_se_prefilter(P.dim, b, cur, old, d_sizes_cur, P.dmax, c_cap, d_se_keep, d_se_pos, dw.scan_work,
                                 dw.tmp_total + 2, stream);
             std::swap(cur, old);
-            launch_se_pairs(P.dim, b, cur, d_sizes_cur, d_se_u, dw.tmp_total + 3, 3 * kSMs, stream);
+            launch_geometry(b, sp, cur, d_sizes_cur, c_cap, nullptr, nullptr, c_cap, stream, d_se_keep);
+            launch_se_pairs(P.dim, b, cur, d_sizes_cur, d_se_keep, d_se_u, dw.tmp_total + 3, 3 * kSMs, stream);
             cudaMemcpyAsync(h_se_cand, &d_sizes_cur->C, sizeof(int), cudaMemcpyDeviceToHost, stream);
             launch_se_filter(cur, old, d_sizes_cur, P.dmax, c_cap, d_se_keep, d_se_pos, dw.scan_work,
                              dw.tmp_total + 2, stream);
@@ -1323,7 +1326,8 @@ static void launch_inverse_mass(int n, int nin, int dim, const double* m, const 
 // Census of an uploaded container, on the device (the host would spend ~3 ns per body on it):
 // out[0] active superellipsoids, out[1] active spheres, out[2] bodies with a worm index, and
 // out[3] the container's rule violations: bit 1 unknown shape, bit 2 an active body that is
-// neither a sphere nor a superellipsoid, bit 4 a superellipsoid obstacle, bit 8 a segment in 3D.
+// neither a sphere nor a superellipsoid, bit 4 a superellipsoid obstacle, bit 8 a segment in 3D,
+// bit 16 an obstacle that is not a plane (refused with superellipsoids only).
 __global__ void k_shape_census(const int* shape, const int* worm, int n, int nin, int dim, int* out) {
     int se = 0, sph = 0, wm = 0, bad = 0;
     GRID_STRIDE(i, n) {
@@ -1334,6 +1338,7 @@ __global__ void k_shape_census(const int* shape, const int* worm, int n, int nin
             if (i >= nin && sh != SCOPI_GPU_SPHERE && sh != SCOPI_GPU_SUPERELLIPSOID) bad |= 2;
             if (i < nin && sh == SCOPI_GPU_SUPERELLIPSOID) bad |= 4;
             if (sh == SCOPI_GPU_SEGMENT && dim != 2) bad |= 8;
+            if (i < nin && sh != SCOPI_GPU_PLANE) bad |= 16;
         }
         if (i >= nin) {
             if (sh == SCOPI_GPU_SUPERELLIPSOID) ++se;
@@ -1419,7 +1424,7 @@ static int32_t upload_particles(scopi_gpu_handle* h, const scopi_gpu_particles* 
     launch_inverse_mass(n, nin, h->P.dim, h->d_m, h->d_j, h->d_invm64, h->d_invm32, h->d_imt64, h->d_imt32, s);
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return h->cuda_fail(e, "set_particles");
-    const int n_se = h->h_census[0], n_sph = h->h_census[1], n_worm = h->h_census[2], bad = h->h_census[3];
+    const int n_se = h->h_census[0], n_worm = h->h_census[2], bad = h->h_census[3];
     auto refuse = [&](int code, const char* msg) {
         h->n = h->nin = h->na = 0;  // the device holds a container that was not accepted
         return h->fail(code, msg);
@@ -1429,8 +1434,10 @@ static int32_t upload_particles(scopi_gpu_handle* h, const scopi_gpu_particles* 
     if (bad & 4) return refuse(SCOPI_GPU_EUNSUPPORTED, "superellipsoid obstacles are not supported");
     if (bad & 8) return refuse(SCOPI_GPU_EUNSUPPORTED, "segments are 2D only");
     if (n_se > 0) {
-        if (h->P.dim == 2 && nin > 0) return refuse(SCOPI_GPU_EUNSUPPORTED, "2D superellipsoids: scenes without obstacles");
-        if (n_sph > 0) return refuse(SCOPI_GPU_EUNSUPPORTED, "spheres and superellipsoids cannot be mixed");
+        // obstacles of superellipsoid scenes are planes: the reference leaves
+        // superellipsoid-segment pairs unimplemented (closest_points.hpp:919-931)
+        if (bad & 16) return refuse(SCOPI_GPU_EUNSUPPORTED, "superellipsoid scenes: plane obstacles only");
+        if (n_worm > 0) return refuse(SCOPI_GPU_EUNSUPPORTED, "worms: scenes of spheres");
         if (!p->axes || !p->squareness) return refuse(SCOPI_GPU_EINVAL, "superellipsoid axes / squareness missing");
         if (h->P.problem == SCOPI_GPU_VISCOUS || h->P.problem == SCOPI_GPU_VISCOUS_FRICTION)
             return refuse(SCOPI_GPU_EUNSUPPORTED, "superellipsoids: NoFriction and Friction problems");
@@ -1438,6 +1445,7 @@ static int32_t upload_particles(scopi_gpu_handle* h, const scopi_gpu_particles* 
         if (h->periodic) return refuse(SCOPI_GPU_EUNSUPPORTED, "periodic box: single scenes of spheres, no worms");
         const bool d3 = h->P.dim == 3;  // 2D: (rx, ry) and e
         for (int i = nin; i < n; ++i) {
+            if (p->shape[i] != SCOPI_GPU_SUPERELLIPSOID) continue;
             const double* r = p->axes + 3 * (size_t)i;
             const double* q = p->squareness + 2 * (size_t)i;
             if (!(r[0] > 0 && r[1] > 0 && (!d3 || r[2] > 0)) || !(q[0] > 0 && q[0] < 2 && (!d3 || (q[1] > 0 && q[1] < 2))))

@@ -55,6 +55,23 @@ __device__ __forceinline__ Body load(const Bodies& B, int b) {
     return s;
 }
 
+// A sphere of radius r is the superellipsoid with semi-axes (r, r, r) and squareness (1, 1):
+// its parametrisation is then exactly sphere::point (sphere.hpp:195-211), since
+// sign(t)|t|^1 = t.  load_any reads either shape as a Body (shape code 0 = sphere).
+__device__ __forceinline__ Body sphere_as_body(const Bodies& B, int b) {
+    Body s;
+    for (int k = 0; k < 3; ++k) {
+        s.c[k] = B.pos[3 * (long long)b + k];
+        s.r[k] = B.radius[b];
+    }
+    s.e = s.n = 1.0;
+    rot(B.q + 4 * (long long)b, s.R);
+    return s;
+}
+__device__ __forceinline__ Body load_any(const Bodies& B, int b) {
+    return B.shape[b] == 0 ? sphere_as_body(B, b) : load(B, b);
+}
+
 __device__ __forceinline__ void mv(const double* R, const double* x, double* y) {
     y[0] = R[0] * x[0] + R[1] * x[1] + R[2] * x[2];
     y[1] = R[3] * x[0] + R[4] * x[1] + R[5] * x[2];
@@ -171,6 +188,14 @@ __device__ __forceinline__ Body2 load2(const Bodies& B, int b) {
     s.e = B.sq[2 * (long long)b];
     return s;
 }
+__device__ __forceinline__ Body2 load_any2(const Bodies& B, int b) {
+    Body2 s = load2(B, b);
+    if (B.shape[b] == 0) {  // sphere: semi-axes (r, r), squareness 1
+        s.r[0] = s.r[1] = B.radius[b];
+        s.e = 1.0;
+    }
+    return s;
+}
 __device__ __forceinline__ void mv2(const double* R, const double* x, double* y) {
     y[0] = R[0] * x[0] + R[1] * x[1];
     y[1] = R[2] * x[0] + R[3] * x[1];
@@ -255,6 +280,30 @@ __device__ __forceinline__ void body_plane(const Body& s, const double* pc, cons
     }
     const double df[3] = {pi[0] - pj[0], pi[1] - pj[1], pi[2] - pj[2]};
     dij = dot3(df, nij);
+}
+
+// closest_points(superellipsoid<2>, plane<2>) (closest_points.hpp:1783-1949) in closed form, as
+// body_plane in 3D: the body point whose outward normal is opposite to the plane normal
+// (column 0 of the plane's rotation, plane.hpp:143-147) oriented toward the body, and its
+// projection on the plane; pi on the body, pj on the plane, nij = the oriented normal.
+__device__ __forceinline__ double support_angle2(const Body2& s, double m0, double m1);
+__device__ __forceinline__ void body_plane2(const Body2& s, const double* pc, const double* pq, double* pi, double* pj,
+                                            double* nij, double& dij) {
+    double P[9];
+    rot(pq, P);
+    const double np[2] = {P[0], P[3]};
+    const double rel[2] = {s.c[0] - pc[0], s.c[1] - pc[1]};
+    const double sg = rel[0] * np[0] + rel[1] * np[1] < 0 ? -1.0 : 1.0;
+    // body-frame direction of the wanted outward normal: -sg R^T np
+    const double m0 = -sg * (s.R[0] * np[0] + s.R[2] * np[1]), m1 = -sg * (s.R[1] * np[0] + s.R[3] * np[1]);
+    point2(s, support_angle2(s, m0, m1), pi);
+    const double h = (pi[0] - pc[0]) * np[0] + (pi[1] - pc[1]) * np[1];
+    pj[0] = pi[0] - h * np[0];
+    pj[1] = pi[1] - h * np[1];
+    nij[0] = sg * np[0];
+    nij[1] = sg * np[1];
+    pi[2] = pj[2] = nij[2] = 0.0;
+    dij = (pi[0] - pj[0]) * nij[0] + (pi[1] - pj[1]) * nij[1];
 }
 
 // ---- separation bound.  For convex bodies (squareness in (0, 2)) the distance is at least
