@@ -247,11 +247,11 @@ def measured_peaks():
 
 # DRAM bytes (read + write) per FP32 APGD iteration per contact of k_apgd_sph on the
 # 1M-sphere workload, from one ncu capture of a whole launch at time step 2 (19 iterations,
-# the curvature pre-pass and one backtrack included): 6.274 GB / (19 x 3,001,248).  The
+# the curvature pre-pass and one backtrack included): 5.930 GB / (19 x 3,000,279).  The
 # line's roofline.traffic scales it by the run's contacts and iterations per launch.
-TRAFFIC_FP32_PER_CONTACT_ITERATION = 110.0
+TRAFFIC_FP32_PER_CONTACT_ITERATION = 104.0
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_apgd_sph<float,3,0> launch at "
-                  "time step 2 (110 B per FP32 contact-iteration), scaled by this run's contacts and FP32 "
+                  "time step 2 (104 B per FP32 contact-iteration), scaled by this run's contacts and FP32 "
                   "iterations per launch")
 
 

@@ -377,12 +377,15 @@ __global__ void k_cell_assign(Bodies B, int dim, const Grid* grid, int* cell_of,
     }
 }
 
+// the first body placed in a cell also appends the cell to the occupied list (the search
+// visits only those; its result does not depend on their order: rows are sorted after)
 __global__ void k_cell_scatter(Bodies B, const int* cell_of, const int* cell_start, int* cell_fill, int* cell_body,
-                               double4* cell_pr) {
+                               double4* cell_pr, int* occ, int* n_occ) {
     GRID_STRIDE(k, B.n - B.nin) {
         const long long b = B.nin + k;
         const int c = cell_of[k];
         const int slot = atomicAdd(&cell_fill[c], 1);
+        if (occ && slot == 0) occ[atomicAdd(n_occ, 1)] = c;
         const int at = cell_start[c] + slot;
         cell_body[at] = (int)b;
         cell_pr[at] = make_double4(B.pos[3 * b], B.pos[3 * b + 1], B.pos[3 * b + 2], B.radius[b]);
@@ -484,9 +487,46 @@ __device__ __forceinline__ void half_stencil(int o, int& dx, int& dy, int& dz) {
     }
 }
 
-// The pair search over the half stencil, one warp per cell: a body meets the bodies after it
-// in its own cell and those of the 13 (3D) / 4 (2D) neighbour cells that follow its cell in
-// (z, y, x) order, so every unordered pair of neighbouring cells is visited once.  The
+// The pair search of 2D scenes, one thread per body: body k (cell-sorted slot) meets the
+// bodies after it in its own cell and those of the 4 neighbour cells of the half stencil.
+// With the few bodies per cell of 2D scenes (and the many empty cells of a batch's layout)
+// this beats a warp per occupied cell: 0.047 against 0.218 ms per step on the 256 pile
+// scenes.  Pairs are tested and emitted as k_pair_search_cells does.
+template <int DIM>
+__global__ void k_pair_search(Bodies B, StepParams p, const Grid* grid, const int* cell_of, const int* cell_start,
+                              const int* cell_body, const double4* cell_pr, int* row_count, int* row_tmp) {
+    const Grid g = *grid;
+    constexpr int nst = DIM == 3 ? 14 : 5;
+    GRID_STRIDE(k, B.n - B.nin) {
+        const int a = cell_body[k];
+        const double4 A = cell_pr[k];
+        int cc[3];
+        cell_coords(g, cell_of[a - B.nin], cc);
+        for (int o = 0; o < nst; ++o) {
+            int dx, dy, dz;
+            half_stencil<DIM>(o, dx, dy, dz);
+            const int x = cc[0] + dx, y = cc[1] + dy, z = cc[2] + dz;
+            if (x < 0 || x >= g.nc[0] || y < 0 || y >= g.nc[1] || z >= g.nc[2]) continue;
+            const int cid = (z * g.nc[1] + y) * g.nc[0] + x;
+            const int t1 = cell_start[cid + 1];
+            for (int t = o == 0 ? (int)k + 1 : cell_start[cid]; t < t1; ++t) {
+                const int b = cell_body[t];
+                if (B.scene && B.scene[a] != B.scene[b]) continue;
+                const double4 Bb = cell_pr[t];
+                const bool a_lo = a < b;
+                if (!pair_in_contact<DIM>(p, a_lo ? A : Bb, a_lo ? Bb : A)) continue;
+                const int lo = a_lo ? a : b, hi = a_lo ? b : a;
+                const int r = lo - B.nin;
+                const int slot = atomicAdd(&row_count[r], 1);
+                if (slot < kRowCap) row_tmp[(long long)r * kRowCap + slot] = hi;
+            }
+        }
+    }
+}
+
+// The pair search of 3D scenes over the half stencil, one warp per occupied cell: a body meets
+// the bodies after it in its own cell and those of the 13 neighbour cells that follow its cell
+// in (z, y, x) order, so every unordered pair of neighbouring cells is visited once.  The
 // candidate pairs of the cell with itself (a < b by slot) and with its half-stencil neighbours
 // are numbered, and the warp's lanes take them 32 at a time (so the uneven cell counts do not
 // idle lanes).  A pair in contact is tested with the lower index first, counted in the row of
@@ -496,7 +536,8 @@ constexpr int kSearchWarps = 8;
 template <int DIM>
 __global__ void __launch_bounds__(32 * kSearchWarps, 4) k_pair_search_cells(Bodies B, StepParams p, const Grid* grid,
                                                                         const int* cell_start, const int* cell_body,
-                                                                        const double4* cell_pr, int* row_count,
+                                                                        const double4* cell_pr, const int* occ,
+                                                                        const int* n_occ, int* row_count,
                                                                         int* row_tmp) {
     constexpr int nst = DIM == 3 ? 14 : 5;
     __shared__ int s_pref[kSearchWarps][16], s_beg[kSearchWarps][16], s_cnt[kSearchWarps][16];
@@ -504,7 +545,9 @@ __global__ void __launch_bounds__(32 * kSearchWarps, 4) k_pair_search_cells(Bodi
     const Grid g = *grid;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const long long nwarps = (long long)gridDim.x * kSearchWarps;
-    for (long long cid = (long long)blockIdx.x * kSearchWarps + w; cid < g.ncell; cid += nwarps) {
+    const long long nocc = *n_occ;
+    for (long long t = (long long)blockIdx.x * kSearchWarps + w; t < nocc; t += nwarps) {
+        const int cid = occ[t];
         const int h0 = cell_start[cid], nh = cell_start[cid + 1] - h0;
         if (nh == 0) continue;  // the whole warp
         int cc[3];
@@ -1257,17 +1300,17 @@ void launch_detect(const Bodies& b, const StepParams& p, DetectWork& w, Contacts
         k_cell_assign<<<blocks_for(na), kThreads, 0, s>>>(b, p.dim, w.grid, w.cell_of, w.cell_count);
         scan_exclusive(w.cell_count, w.cell_start, &w.grid->ncell1, 0, w.cell_cap + 1, w.tmp_total + 3, w.scan_work, s,
                        &g_detect_launches);
+        const bool by_cell = p.dim == 3;  // 3D: a warp per occupied cell; 2D: a thread per body
+        cudaMemsetAsync(w.n_occ, 0, sizeof(int), s);
         k_cell_scatter<<<blocks_for(na), kThreads, 0, s>>>(b, w.cell_of, w.cell_start, w.cell_fill, w.cell_body,
-                                                           w.cell_pr);
+                                                           w.cell_pr, by_cell ? w.occ : nullptr, w.n_occ);
         cudaMemsetAsync(w.row_count, 0, (na + 1) * sizeof(int), s);
-        // one warp per cell over the cell capacity (the kernel stops at the grid's cell count)
-        const int sb = blocks_for(w.cell_cap, kSearchWarps);
-        if (p.dim == 3)
-            k_pair_search_cells<3><<<sb, 32 * kSearchWarps, 0, s>>>(b, p, w.grid, w.cell_start, w.cell_body, w.cell_pr,
-                                                                   w.row_count, w.row_tmp);
+        if (by_cell)
+            k_pair_search_cells<3><<<blocks_for(na, kSearchWarps), 32 * kSearchWarps, 0, s>>>(
+                b, p, w.grid, w.cell_start, w.cell_body, w.cell_pr, w.occ, w.n_occ, w.row_count, w.row_tmp);
         else
-            k_pair_search_cells<2><<<sb, 32 * kSearchWarps, 0, s>>>(b, p, w.grid, w.cell_start, w.cell_body, w.cell_pr,
-                                                                   w.row_count, w.row_tmp);
+            k_pair_search<2><<<blocks_for(na), kThreads, 0, s>>>(b, p, w.grid, w.cell_of, w.cell_start, w.cell_body,
+                                                                w.cell_pr, w.row_count, w.row_tmp);
         LAUNCHED(3);
     }
     // obstacle rows come first in (i, j) order

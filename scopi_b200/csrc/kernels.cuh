@@ -41,6 +41,8 @@ struct DetectWork {
     int* cell_of;             // na
     int* cell_body;           // na (body index, sorted by cell)
     double4* cell_pr;         // na (x, y, z, r) sorted by cell
+    int* occ;                 // na: the occupied cells, in the order their first body was placed
+    int* n_occ;               // 1: their count
     int* row_count;           // na + 1
     int* row_ptr;             // na + 1
     int* row_tmp;             // na * kRowCap: partners found by the search pass, unordered

@@ -545,6 +545,7 @@ struct scopi_gpu_handle {
         dw.obs_cap = obs_cap >= 0 ? obs_cap : (long long)nin * naw;
         A(dw.grid, 1) A(dw.bbox_partial, 8 * 4 * kSMs) A(dw.cell_count, dw.cell_cap + 1) A(dw.cell_start, dw.cell_cap + 1)
         A(dw.cell_fill, dw.cell_cap) A(dw.cell_of, naw + 1) A(dw.cell_body, naw + 1) A(dw.cell_pr, naw + 1)
+        A(dw.occ, naw + 1) A(dw.n_occ, 1)
         A(dw.row_count, naw + 1) A(dw.row_ptr, naw + 1) A(dw.row_tmp, (size_t)naw * kRowCap + 1) A(dw.obs_flag, dw.obs_cap + 1) A(dw.obs_pos, dw.obs_cap + 1)
         A(dw.tmp_total, 4)
         if (periodic) {
