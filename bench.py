@@ -397,7 +397,8 @@ def piles(args, ranks):
     kw = dict(dmax=st["dmax"], tolerance=st["tolerance"], max_ite=st["max_ite"])
     n_disks = sum(s.n - s.nb_inactive for s in scenes)
 
-    def run(precision, sampler=None, **extra):
+    def run(precision, sampler=None, steps=None, **extra):
+        steps = steps or args.steps
         b = ScopiBatch(scenes, vap=st["vap"], precision=precision, device=ranks.local, mixed_violation_tol=1e-6,
                        **kw, **extra)
         b.run(st["dt"], args.warmup)
@@ -412,7 +413,7 @@ def piles(args, ranks):
             sampler.start()
         viol, iters, contacts, conv = 0.0, [], [], True
         e0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             b.run(st["dt"], 1)
             s = b.stats()
             viol = max(viol, s["violation"])
@@ -441,6 +442,17 @@ def piles(args, ranks):
             abl[name] = {"value": ranks.world * args.steps * 1000.0 / r["ms"], "unit": UNIT,
                          "violation_max": r["violation_max"],
                          "longest_scene_iterations_mean": r["longest_scene_iterations_mean"]}
+    # the same scenes with friction (mu 0.3; FP64, the 6-dof rows solved per scene), the first
+    # 200 steps after the warm-up
+    fr = None
+    if not args.no_fp64:
+        from scopi_b200 import FRICTION
+        fsteps = min(args.steps, 200)
+        r = run(FP64, steps=fsteps, problem=FRICTION, mu=0.3)
+        fr = {"value": ranks.world * fsteps * 1000.0 / r["ms"], "unit": UNIT, "problem": "Friction, mu 0.3",
+              "precision": "fp64", "steps": fsteps, "violation_max": r["violation_max"],
+              "longest_scene_iterations_mean": r["longest_scene_iterations_mean"],
+              "contacts_mean": r["contacts_mean"], "converged_all": r["converged_all"]}
     value = ranks.world * args.steps * 1000.0 / mixed["ms"]
     # the FP64 leg with the reference's first step stops its landing solves at violations
     # above 1e-6 (the reference's stopping rule); the FP64 leg that meets the bar is the one
@@ -467,6 +479,7 @@ def piles(args, ranks):
                   "block_threads": f64["block_threads"]} if f64 else None),
         "ablation": abl or None,
         "at_equal_violation": equal,
+        "friction": fr,
         "solver": {k: mixed[k] for k in ("violation_max", "longest_scene_iterations_mean", "contacts_mean",
                                         "converged_all", "block_threads", "tile")},
         "clocks": mixed["clocks"], "gpu_launches": mixed["launches"],

@@ -254,10 +254,12 @@ __device__ __forceinline__ void contact_scalar(const ApgdArgs<T>& A, long long m
     s[7] += (double)lp * (double)lp;
 }
 
+// Contact c's share of the contact pass (its rows of l+ and its terms of the partial sums).
 template <typename T, int DIM, int PROB>
-__device__ void contact_pass(const ApgdArgs<T>& A, int C, const T* lam, const T* lprev, T* lnew, const T* ul,
-                             const T* up, T beta, bool use_prev, bool bt, double alpha, double* s) {
-    GRID_STRIDE(c, C) {
+__device__ __forceinline__ void contact_one(const ApgdArgs<T>& A, long long c, const T* lam, const T* lprev, T* lnew,
+                                            const T* ul, const T* up, T beta, bool use_prev, bool bt, double alpha,
+                                            double* s) {
+    {
         const int i = A.ci[c], j = A.cj[c];
         if (PROB != kFriction && PROB != kViscousFriction) {
             T qy = 0;
@@ -392,12 +394,19 @@ __device__ void contact_pass(const ApgdArgs<T>& A, int C, const T* lam, const T*
     }
 }
 
-// curv (FP32 iterations): s[8] += (u(l+) - u(y))^T M (u(l+) - u(y)), the curvature d^T Q d / dt^2
-// along d = l+ - y of the curvature-form backtracking test
 template <typename T, int DIM, int PROB>
-__device__ void particle_pass(const ApgdArgs<T>& A, const T* lnew, T* unew, const T* ul, const T* up, T beta,
-                              bool use_prev, bool curv, double* s) {
-    GRID_STRIDE(p, A.na) {
+__device__ void contact_pass(const ApgdArgs<T>& A, int C, const T* lam, const T* lprev, T* lnew, const T* ul,
+                             const T* up, T beta, bool use_prev, bool bt, double alpha, double* s) {
+    GRID_STRIDE(c, C) contact_one<T, DIM, PROB>(A, c, lam, lprev, lnew, ul, up, beta, use_prev, bt, alpha, s);
+}
+
+// Body p's share of the particle pass.  curv (FP32 iterations): s[8] += (u(l+) - u(y))^T M
+// (u(l+) - u(y)), the curvature d^T Q d / dt^2 along d = l+ - y of the curvature-form
+// backtracking test.
+template <typename T, int DIM, int PROB>
+__device__ __forceinline__ void particle_one(const ApgdArgs<T>& A, long long p, const T* lnew, T* unew, const T* ul,
+                                             const T* up, T beta, bool use_prev, bool curv, double* s) {
+    {
         T w[6] = {0, 0, 0, 0, 0, 0};
         const int k0 = A.inc_ptr[p], k1 = A.inc_ptr[p + 1];
         for (int k = k0; k < k1; ++k) {
@@ -462,6 +471,12 @@ __device__ void particle_pass(const ApgdArgs<T>& A, const T* lnew, T* unew, cons
             s[8] += q;
         }
     }
+}
+
+template <typename T, int DIM, int PROB>
+__device__ void particle_pass(const ApgdArgs<T>& A, const T* lnew, T* unew, const T* ul, const T* up, T beta,
+                              bool use_prev, bool curv, double* s) {
+    GRID_STRIDE(p, A.na) particle_one<T, DIM, PROB>(A, p, lnew, unew, ul, up, beta, use_prev, curv, s);
 }
 
 template <typename T, int DIM, int PROB>
@@ -629,6 +644,190 @@ __global__ void __launch_bounds__(kApgdThreads) k_apgd(ApgdArgs<T> A) {
         A.result->error = err;
         A.result->last_step = last_step;
         A.result->lipsch = lgood;
+    }
+}
+
+// ------------------------------------------------- batched scenes, 6-dof rows (FP64)
+// One CTA per scene (scenes taken largest first): the iteration of k_apgd on the scene's
+// contacts (its obstacle rows [o0, o1), then its active rows [a0, a1)) and bodies [p0, p1),
+// with block barriers and block sums in place of the grid ones, so every scene iterates
+// until its own stopping test holds.  At the end the CTA copies its scene's multipliers and
+// u = M^-1 B^T l to fixed outputs (which rotating buffer holds them differs per scene) and
+// writes the scene's statistics with the violation max(0, -gap) of its final state.
+constexpr int kBatch6Threads = 256;
+
+__device__ __forceinline__ double block_max(double v) {
+    __shared__ double sh[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    double m = 0.0;
+    for (int w = 0; w < nw; ++w) m = fmax(m, sh[w]);
+    __syncthreads();
+    return m;
+}
+
+template <int DIM, int PROB>
+__global__ void __launch_bounds__(kBatch6Threads) k_apgd_batch6(ApgdArgs<double> A, Batch6Scenes S) {
+    using T = double;
+    constexpr int R = PROB == kFriction ? 3 : 1;  // multipliers per contact
+    T* lamb[3] = {A.lam0, A.lam1, A.lam2};
+    T* ub[3] = {A.u0, A.u1, A.u2};
+    for (int q = blockIdx.x; q < S.n_scenes; q += gridDim.x) {
+        const int sc = S.order[q];
+        const int o0 = S.sc_o0[sc], n0 = S.sc_o1[sc] - o0, a0 = S.sc_a0[sc];
+        const int nc = n0 + (S.sc_a1[sc] - a0);
+        const int p0 = S.sc_p0[sc], p1 = S.sc_p1[sc];
+        auto contact_at = [&](int k) -> long long { return k < n0 ? (long long)o0 + k : (long long)a0 + (k - n0); };
+        int il = 0, ip = 1, in_ = 2, jl = 0, jp = 1, jn = 2;
+        double alpha = A.alpha, lipsch = 1.0 / alpha, lgood = lipsch, theta = 1.0, beta = 0.0;
+        bool use_prev = false, bt = false;
+        double Fy = 0.0, last_step = 0.0;
+        long long ite = 0, nbt = 0, nrs = 0;
+        int conv = nc == 0 ? 1 : 0, err = 0;
+        if (nc > 0 && A.curvature_start) {
+            // L = 1.5 dt^2 |B^T d|^2_{M^-1} / |d|^2 along the first projected-gradient direction
+            T* dbuf = lamb[in_];
+            double s[kPartials] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            for (int k = threadIdx.x; k < nc; k += blockDim.x) {
+                const long long c = contact_at(k);
+                if (PROB == kFriction) {
+                    double z[3], n[3];
+                    for (int d = 0; d < 3; ++d) {
+                        n[d] = A.bn[3 * c + d];
+                        z[d] = -A.cvec[3 * c + d];
+                    }
+                    if (DIM == 2) z[2] = 0.0;
+                    cone_project<DIM>(z, n, A.mu);
+                    for (int d = 0; d < 3; ++d) {
+                        dbuf[3 * c + d] = z[d];
+                        s[1] += z[d] * z[d];
+                    }
+                } else {
+                    const T v = apgdc::first_descent<T>(A.cvec[c], nullptr, c);
+                    dbuf[c] = v;
+                    s[1] += v * v;
+                }
+            }
+            __syncthreads();
+            for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x)
+                particle_one<T, DIM, PROB>(A, p, dbuf, ub[jn], ub[jl], ub[jp], (T)0, false, false, s);
+            apgdc::block_sum<kPartials>(s);
+            double l;
+            if (apgdc::initial_lipschitz(s[1], s[6], A.dt2, l)) {
+                lipsch = l;
+                alpha = 1.0 / l;
+                lgood = l;
+            }
+        }
+        while (!conv) {
+            double s[kPartials] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            for (int k = threadIdx.x; k < nc; k += blockDim.x)
+                contact_one<T, DIM, PROB>(A, contact_at(k), lamb[il], lamb[ip], lamb[in_], ub[jl], ub[jp], (T)beta,
+                                          use_prev, bt, alpha, s);
+            __syncthreads();
+            for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x)
+                particle_one<T, DIM, PROB>(A, p, lamb[in_], ub[jn], ub[jl], ub[jp], (T)beta, use_prev, false, s);
+            apgdc::block_sum<kPartials>(s);
+            const double* t = s;
+            if (!bt) Fy = t[3];
+            const double F_lp = 0.5 * A.dt2 * t[6] + t[2];
+            if (A.dynamic && t[1] == 0.0) {
+                while (isfinite(lipsch)) {  // l+ == y bit for bit (as in k_apgd)
+                    lipsch *= 2;
+                    ++nbt;
+                }
+                alpha = 1. / lipsch;
+            } else if (A.dynamic && apgdc::sufficient_decrease_fails<T>(F_lp, Fy, t[0], t[1], A.dt2 * t[8], lipsch)) {
+                lipsch *= 2;
+                alpha = 1. / lipsch;
+                bt = true;
+                ++nbt;
+                if (nbt > 4000) {
+                    err = 2;
+                    break;
+                }
+                continue;
+            }
+            ++ite;
+            bt = false;
+            if (isfinite(lipsch)) lgood = lipsch;
+            last_step = sqrt(t[4]);
+            int tmp = ip;
+            ip = il;
+            il = in_;
+            in_ = tmp;
+            tmp = jp;
+            jp = jl;
+            jl = jn;
+            jn = tmp;
+            if (last_step < A.tol) {
+                conv = 1;
+                break;
+            }
+            const double theta1 = 0.5 * (theta * sqrt(4 + theta * theta) - theta * theta);
+            beta = theta * (1 - theta) / (theta * theta + theta1);
+            theta = theta1;
+            if (A.dynamic) {
+                if (t[5] > 0) {  // restart, apgd.hpp:200-206
+                    beta = 0.0;
+                    theta = 1.;
+                    ++nrs;
+                }
+                lipsch *= 0.97;
+                alpha = 1. / lipsch;
+            }
+            use_prev = (beta != 0.0);
+            if (ite >= A.max_ite) break;
+        }
+        // the scene's outputs and its violation max(0, -n.(dt^2 A u + C)) over its contacts
+        double vmax = 0.0;
+        for (int k = threadIdx.x; k < nc; k += blockDim.x) {
+            const long long c = contact_at(k);
+            for (int r = 0; r < R; ++r) S.lam_out[R * c + r] = lamb[il][R * c + r];
+            const int bi[2] = {A.ci[c], A.cj[c]};
+            double q3[3] = {0, 0, 0};
+            for (int side = 0; side < 2; ++side) {
+                if (bi[side] < A.nin) continue;
+                const T* uu = ub[jl] + 6 * (long long)(bi[side] - A.nin);
+                const double sg = side == 0 ? 1.0 : -1.0;
+                if (PROB == kFriction) {
+                    const T* P = A.bP + 18 * c + 9 * side;
+                    for (int d = 0; d < 3; ++d) {
+                        const double vd = (DIM == 2 && d == 2) ? 0.0 : uu[d];
+                        q3[d] += sg * (vd + P[d] * uu[3] + P[3 + d] * uu[4] + P[6 + d] * uu[5]);
+                    }
+                } else {
+                    const T* a = (side == 0 ? A.bai : A.baj) + 3 * c;
+                    for (int d = 0; d < DIM; ++d) q3[0] += sg * A.bn[3 * c + d] * uu[d];
+                    q3[0] += DIM == 3 ? a[0] * uu[3] + a[1] * uu[4] + a[2] * uu[5] : a[2] * uu[5];
+                }
+            }
+            double gap = 0.0;
+            if (PROB == kFriction) {
+                for (int d = 0; d < DIM; ++d) gap += (A.dt2 * q3[d] + A.cvec[3 * c + d]) * A.bn[3 * c + d];
+            } else {
+                gap = A.dt2 * q3[0] + A.cvec[c];
+            }
+            vmax = fmax(vmax, -gap);
+        }
+        for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x)
+            for (int d = 0; d < 6; ++d) S.u_out[6 * (long long)p + d] = ub[jl][6 * (long long)p + d];
+        vmax = block_max(vmax);
+        if (threadIdx.x == 0) {
+            BatchSceneStats& st = S.stats[sc];
+            st.contacts = nc;
+            st.iterations = ite;
+            st.fp32_iterations = 0;
+            st.backtracks = nbt;
+            st.restarts = nrs;
+            st.corrections = 0;
+            st.converged = conv && !err;
+            st.violation = vmax;
+        }
+        __syncthreads();
     }
 }
 
@@ -896,6 +1095,53 @@ int max_blocks_t() {
 }
 
 }  // namespace
+
+cudaError_t launch_apgd_batch6(const Bodies& b, const StepParams& p, const ApgdSettings& st, const Contacts& c,
+                               const Assembly& a, SolveBuffers<double>& sb, const double* invm,
+                               const Batch6Scenes& S, cudaStream_t s) {
+    ApgdArgs<double> A{};
+    A.nin = b.nin;
+    A.na = b.n - b.nin;
+    A.ci = c.ci;
+    A.cj = c.cj;
+    A.slot = a.slot;
+    A.mode = a.vflag;
+    A.bn = sb.bn;
+    A.bai = sb.bai;
+    A.baj = sb.baj;
+    A.bP = sb.bP;
+    A.cvec = sb.cvec;
+    A.shift = nullptr;
+    A.inc_ptr = sb.inc_ptr;
+    A.inc_idx = sb.inc_idx;
+    A.inc_coef = sb.inc_coef;
+    A.invm = invm;
+    A.lam0 = sb.lam[0];
+    A.lam1 = sb.lam[1];
+    A.lam2 = sb.lam[2];
+    A.u0 = sb.u[0];
+    A.u1 = sb.u[1];
+    A.u2 = sb.u[2];
+    A.g = sb.g;
+    A.alpha = st.alpha;
+    A.tol = st.tol;
+    A.dt2 = st.dt * st.dt;
+    A.mu = st.mu;
+    A.curvature_start = st.curvature_start;
+    A.max_ite = st.max_ite;
+    A.dynamic = st.dynamic;
+    const int grid = std::max(1, S.n_scenes);
+    if (p.problem == kFriction) {
+        if (p.dim == 3)
+            k_apgd_batch6<3, kFriction><<<grid, kBatch6Threads, 0, s>>>(A, S);
+        else
+            k_apgd_batch6<2, kFriction><<<grid, kBatch6Threads, 0, s>>>(A, S);
+    } else {
+        return cudaErrorInvalidValue;
+    }
+    g_apgd_launches += 1;
+    return cudaGetLastError();
+}
 
 int apgd_max_blocks(int problem, int dim, bool fp32) {
 #define MB(T, D, P) \

@@ -332,6 +332,21 @@ struct BatchSolve {
     int curvature_start;
 };
 
+// Batched scenes of a 6-dof problem (Friction), FP64: one CTA per scene over the scene
+// ranges of launch_batch_ranges; the multipliers (3 per contact) and u (6 per active body)
+// of every scene end in lam_out / u_out, its statistics in stats[scene].
+struct Batch6Scenes {
+    int n_scenes;
+    const int* order;
+    const int *sc_p0, *sc_p1, *sc_o0, *sc_o1, *sc_a0, *sc_a1;
+    BatchSceneStats* stats;
+    double* lam_out;
+    double* u_out;
+};
+cudaError_t launch_apgd_batch6(const Bodies& b, const StepParams& p, const ApgdSettings& st, const Contacts& c,
+                               const Assembly& a, SolveBuffers<double>& sb, const double* invm,
+                               const Batch6Scenes& S, cudaStream_t s);
+
 long long apgd_batch_launches();
 void launch_batch_ranges(int n_scenes, int nin, const int* sc_obs0, const int* sc_obs1, const int* sc_p0,
                          const int* sc_p1, const int* obs_off, const int* obs_pos, const int* row_ptr,

@@ -250,6 +250,14 @@ struct scopi_gpu_handle {
         launch_geometry(b, sp, cur, d_sizes_cur, c_cap, nullptr, nullptr, c_cap, stream);
         launch_assemble(b, sp, cur, as, d_sizes_cur, c_cap, dw.scan_work, dw.tmp_total + 2, stream);
         launch_incidence(b, sp, cur, as, inc, d_sizes_cur, c_cap, dw.scan_work, dw.tmp_total + 2, stream, false);
+        if (friction_rows()) {
+            // Friction scenes: the 6-dof rows (three per contact) solved per scene in FP64
+            launch_batch_ranges(n_scenes, nin, d_sc_obs0, d_sc_obs1, d_sc_p0, d_sc_p1, d_obs_off, dw.obs_pos,
+                                dw.row_ptr, d_sizes_cur, d_sc_o0, d_sc_o1, d_sc_a0, d_sc_a1, stream);
+            enqueue_batch_solve6(dt);
+            launch_update(b, sp, d_ufin, 6, 1, d_sizes_cur, stream);
+            return;
+        }
         launch_pack_cij(cur.ci, cur.cj, d_cij, d_sizes_cur, c_cap, stream);
         launch_pack_nc<double>(as.bn, as.cvec, d_nc64, d_sizes_cur, c_cap, stream);
         launch_pack_inc<double>(na, inc.ptr, inc.idx, as.bn, d_incv64, 2 * c_cap, stream);
@@ -261,6 +269,51 @@ struct scopi_gpu_handle {
                             d_sizes_cur, d_sc_o0, d_sc_o1, d_sc_a0, d_sc_a1, stream);
         enqueue_batch_solve(dt, bt, tile);
         launch_update(b, sp, reinterpret_cast<const double*>(d_usfin), 4, 0, d_sizes_cur, stream);
+    }
+
+    void enqueue_batch_solve6(double dt) {
+        Bodies b = bodies();
+        StepParams sp = step_params(dt);
+        ApgdSettings st{};
+        st.alpha = P.alpha;
+        st.tol = P.tolerance;
+        st.max_ite = P.max_ite;
+        st.dynamic = P.dynamic_descent;
+        st.dt = dt;
+        st.mu = P.mu;
+        st.curvature_start = curvature_start();
+        const long long M = (long long)mult_per_contact() * c_cap;
+        cudaMemsetAsync(d_lam64[0], 0, M * sizeof(double), stream);
+        cudaMemsetAsync(d_lam64[1], 0, M * sizeof(double), stream);
+        cudaMemsetAsync(d_u64[0], 0, 6 * (size_t)na * sizeof(double), stream);
+        cudaMemsetAsync(d_u64[1], 0, 6 * (size_t)na * sizeof(double), stream);
+        SolveBuffers<double> sb{};
+        sb.bn = as.bn;
+        sb.bai = as.bai;
+        sb.baj = as.baj;
+        sb.bP = as.bP;
+        sb.cvec = as.cvec;
+        sb.inc_ptr = inc.ptr;
+        sb.inc_idx = inc.idx;
+        sb.inc_coef = inc.coef;
+        for (int k = 0; k < 3; ++k) {
+            sb.lam[k] = d_lam64[k];
+            sb.u[k] = d_u64[k];
+        }
+        sb.g = d_g64;
+        Batch6Scenes S{};
+        S.n_scenes = n_scenes;
+        S.order = d_order;
+        S.sc_p0 = d_sc_p0;
+        S.sc_p1 = d_sc_p1;
+        S.sc_o0 = d_sc_o0;
+        S.sc_o1 = d_sc_o1;
+        S.sc_a0 = d_sc_a0;
+        S.sc_a1 = d_sc_a1;
+        S.stats = d_bstats;
+        S.lam_out = d_lamacc;
+        S.u_out = d_ufin;
+        launch_apgd_batch6(b, sp, st, cur, as, sb, d_invm64, S, stream);
     }
 
     void enqueue_batch_solve(double dt, int bt, int tile) {
@@ -399,7 +452,8 @@ struct scopi_gpu_handle {
             finish_batch_step_timing();
             batch_bt_used = bt;
             batch_tile_used = tile;
-            if (!batch_threads && stats.iterations >= kBatchTuneIterations) return autotune_batch(dt);
+            if (!batch_threads && !friction_rows() && stats.iterations >= kBatchTuneIterations)
+                return autotune_batch(dt);
             return 0;
         }
         return fail(SCOPI_GPU_ENOMEM, "contact capacity could not be grown");
@@ -1693,8 +1747,12 @@ int32_t scopi_gpu_batch_create(const scopi_gpu_params* p, int32_t n_scenes, cons
         return SCOPI_GPU_EINVAL;
     }
     *out = nullptr;
-    if (p->problem != SCOPI_GPU_NOFRICTION) {
-        scopi_gpu::set_global_error("scopi_gpu_batch_create: batches solve NoFriction scenes");
+    if (p->problem != SCOPI_GPU_NOFRICTION && p->problem != SCOPI_GPU_FRICTION) {
+        scopi_gpu::set_global_error("scopi_gpu_batch_create: batches solve NoFriction and Friction scenes");
+        return SCOPI_GPU_EUNSUPPORTED;
+    }
+    if (p->problem == SCOPI_GPU_FRICTION && p->precision != SCOPI_GPU_FP64) {
+        scopi_gpu::set_global_error("scopi_gpu_batch_create: Friction batches run in FP64");
         return SCOPI_GPU_EUNSUPPORTED;
     }
     long long ntot = 0, nin_tot = 0;

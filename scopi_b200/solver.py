@@ -225,16 +225,17 @@ class ScopiBatch:
     ``scenes`` is a list of ``ParticleArrays`` (each obstacles first).  ``run(dt, k)`` advances
     every scene k steps (one CUDA graph replay per step, one persistent launch solving every
     scene); ``scene(s)`` returns scene s's particles and ``scene_stats(s)`` its solver
-    statistics of the last step.  NoFriction only.  ``block_threads`` pins the threads per
-    scene (256, 512 or 1024); 0 lets the first step autotune it.
+    statistics of the last step.  ``problem``: NOFRICTION (FP64 or MIXED) or FRICTION (FP64,
+    ``mu`` in the overrides).  ``block_threads`` pins the threads per scene of the NoFriction
+    solve (256, 512 or 1024); 0 lets the first step autotune it.
     """
 
     def __init__(self, scenes, vap=VAP_FPD, contact_method=KDTREE, precision=FP64, device=0, block_threads=0,
-                 tile=0, **overrides):
+                 tile=0, problem=NOFRICTION, **overrides):
         self._lib = _abi.load()
         p = _abi.Params()
         self._lib.scopi_gpu_default_params(C.byref(p), scenes[0].dim)
-        p.problem, p.vap, p.contact_method, p.precision, p.device = NOFRICTION, vap, contact_method, precision, device
+        p.problem, p.vap, p.contact_method, p.precision, p.device = problem, vap, contact_method, precision, device
         for k, v in overrides.items():
             _set_param(p, k, v)
         self._params = p

@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 from gpu_helpers import oracle_solver, rel_err
-from scopi_b200 import FP64, MIXED, ScopiBatch, ScopiGPUError, ScopiSolver, configs
+from scopi_b200 import FP64, FRICTION, MIXED, ScopiBatch, ScopiGPUError, ScopiSolver, configs
 from scopi_b200.container import Particles, Property
 
 pytestmark = pytest.mark.gpu
@@ -170,3 +170,53 @@ def test_batch_mixed_keeps_violation_target_through_landing():
         b.run(ST["dt"], 1)
         worst = max(worst, b.stats()["violation"])
     assert worst <= 1e-6
+
+
+# ---- Friction scenes (LagrangeMultiplier<Friction>, lagrange_multiplier.hpp:208-273): the
+# 6-dof rows solved per scene in FP64, one CTA per scene (k_apgd_batch6)
+FKW = dict(KW, mu=0.3)
+
+
+def test_batch_friction_matches_oracle_per_scene():
+    scenes = small_piles(4)
+    steps = 8
+    b = ScopiBatch(scenes, vap=ST["vap"], precision=FP64, problem=FRICTION, **FKW)
+    oracles = [oracle_solver(s, vap=ST["vap"], problem=FRICTION, **FKW) for s in scenes]
+    for k in range(steps):
+        b.run(ST["dt"], 1)
+        for s, o in enumerate(oracles):
+            o.run(ST["dt"], 1)
+            assert b.scene_stats(s)["contacts"] == len(o.contacts()["i"]), f"scene {s} step {k}"
+    iters = 0
+    for s, o in enumerate(oracles):
+        g = b.scene(s)
+        st = b.scene_stats(s)
+        print(s, "positions", rel_err(g.pos, o.pa.pos), "velocities", rel_err(g.v, o.pa.v),
+              "omega", rel_err(g.omega, o.pa.omega), st)
+        assert rel_err(g.pos, o.pa.pos) <= 1e-9, s
+        assert rel_err(g.v, o.pa.v) <= 1e-7, s
+        assert rel_err(g.omega, o.pa.omega) <= 1e-6, s
+        assert st["converged"] == 1
+        iters = max(iters, st["iterations"])
+    assert iters > 10
+    b.close()
+
+
+def test_batch_friction_matches_single_scene_gpu():
+    scenes = small_piles(5, 100, 800, seed=9) + [lone_disk()]
+    steps = 5
+    b = ScopiBatch(scenes, vap=ST["vap"], precision=FP64, problem=FRICTION, **FKW).run(ST["dt"], steps)
+    for s, pa in enumerate(scenes):
+        one = ScopiSolver(pa, vap=ST["vap"], precision=FP64, problem=FRICTION, **FKW).run(ST["dt"], steps)
+        g = b.scene(s)
+        assert b.scene_stats(s)["contacts"] == one.stats()["contacts"], s
+        assert rel_err(g.pos, one.particles.pos) <= 1e-9, s
+        assert rel_err(g.v, one.particles.v) <= 1e-7, s
+        assert b.scene_stats(s)["violation"] <= 1e-5, (s, b.scene_stats(s))
+        one.close()
+    b.close()
+
+
+def test_batch_friction_refuses_mixed_precision():
+    with pytest.raises(ScopiGPUError):
+        ScopiBatch(small_piles(2), vap=ST["vap"], precision=MIXED, problem=FRICTION, **FKW)
