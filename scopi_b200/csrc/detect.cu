@@ -490,7 +490,7 @@ __device__ __forceinline__ void half_stencil(int o, int& dx, int& dy, int& dz) {
 // The pair search of 2D scenes, one thread per body: body k (cell-sorted slot) meets the
 // bodies after it in its own cell and those of the 4 neighbour cells of the half stencil.
 // With the few bodies per cell of 2D scenes (and the many empty cells of a batch's layout)
-// this beats a warp per occupied cell: 0.047 against 0.218 ms per step on the 256 pile
+// this beats a warp per occupied cell: 0.038 against 0.218 ms per step on the 256 pile
 // scenes.  Pairs are tested and emitted as k_pair_search_cells does.
 template <int DIM>
 __global__ void k_pair_search(Bodies B, StepParams p, const Grid* grid, const int* cell_of, const int* cell_start,
