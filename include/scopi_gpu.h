@@ -253,11 +253,13 @@ int32_t scopi_gpu_batch_get_scene(scopi_gpu_handle* h, int32_t scene, scopi_gpu_
 int32_t scopi_gpu_batch_get_scene_stats(scopi_gpu_handle* h, int32_t scene, scopi_gpu_scene_stats* out);
 /* block size chosen by the autotuner (0 before the first step) */
 int32_t scopi_gpu_batch_block_threads(scopi_gpu_handle* h);
-/* pin the block size per scene (256, 512 or 1024) instead of autotuning it on the first
-   step; 0 restores autotuning.  Only before the first step (else SCOPI_GPU_EINVAL). */
+/* pin the threads per scene (256, 512 or 1024: one CTA per scene; 2048: the scenes with at
+   least half the largest scene's bodies take a cluster of two 1024-thread CTAs, the others
+   one each) instead of autotuning it on the first step; 0 restores autotuning.  Only before
+   the first step (else SCOPI_GPU_EINVAL). */
 int32_t scopi_gpu_batch_set_block_threads(scopi_gpu_handle* h, int32_t threads);
 /* the tile of the batched solve (contacts / incidence records each thread keeps in flight),
-   autotuned with the block size: 256 x 4 or 2, 512 x 1 or 2, 1024 x 1 or 2 */
+   autotuned with the threads per scene: 256 x 4 or 2, 512, 1024 and 2048 x 1 or 2 */
 int32_t scopi_gpu_batch_tile(scopi_gpu_handle* h);
 /* pin both (0, 0 restores autotuning); only before the first step */
 int32_t scopi_gpu_batch_set_shape(scopi_gpu_handle* h, int32_t threads, int32_t tile);

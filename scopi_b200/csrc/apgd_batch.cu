@@ -9,6 +9,10 @@
 // and reruns the FP32 solve on the correction until the violation target holds.
 // The contacts of scene s are two contiguous ranges of the global (i, j)-sorted list:
 // the rows of its obstacles and the rows of its active bodies.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+
 #include "apgd_common.cuh"
 
 namespace scopi_gpu {
@@ -37,6 +41,8 @@ __device__ __forceinline__ int bidx(double w) { return (int)__double_as_longlong
 template <typename T>
 struct BatchArgs {
     int nin;
+    int n_scenes;
+    int n_big;                        // paired layout: the n_big largest scenes take two CTAs each
     const int* order;                 // scene order (largest first)
     const int* sc_p0;                 // per scene: active bodies [p0, p1) (active index)
     const int* sc_p1;
@@ -79,13 +85,53 @@ __device__ __forceinline__ T* lam_buf(const BatchArgs<T>& A, int k) {
 // contact k of scene (obstacle rows first, then active rows)
 __device__ __forceinline__ int scene_contact(int k, int o0, int n0, int a0) { return k < n0 ? o0 + k : a0 + (k - n0); }
 
+// The threads that solve one scene: one CTA (CS = 1), or a cluster of CS CTAs on CS SMs,
+// which spreads a large scene's passes over the load/store bandwidth of CS SMs (one SM
+// streams the ~1 MB per iteration of a 5000-disk scene at ~60 GB/s).  sync() orders the
+// scene's global memory at cluster scope (barrier.cluster arrive.release / wait.acquire);
+// reduce<NP>(v, slot) sums v over the scene's threads, the CTAs' partial sums added in rank
+// order, into thread 0 of every CTA, so that every CTA takes the same decisions.  `slot`
+// alternates between consecutive reductions: a CTA's partials are read through distributed
+// shared memory by the others before it can overwrite that slot.
+template <int CS>
+struct Grp {
+    int rank;
+    __device__ __forceinline__ int tid() const { return rank * (int)blockDim.x + (int)threadIdx.x; }
+    __device__ __forceinline__ int size() const { return CS * (int)blockDim.x; }
+    __device__ __forceinline__ void sync() const {
+        if (CS == 1)
+            __syncthreads();
+        else
+            asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+    }
+    template <int NP>
+    __device__ __forceinline__ void reduce(double* v, int slot) const {
+        block_reduce_t0<NP>(v);
+        if (CS == 1) return;
+        __shared__ double part[3][8];
+        if (threadIdx.x == 0)
+            for (int k = 0; k < NP; ++k) part[slot][k] = v[k];
+        sync();
+        if (threadIdx.x == 0) {
+            cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+            double t[NP];
+            for (int k = 0; k < NP; ++k) t[k] = 0.0;
+            for (int r = 0; r < CS; ++r) {
+                const double* rp = cl.map_shared_rank(&part[slot][0], r);
+                for (int k = 0; k < NP; ++k) t[k] += rp[k];
+            }
+            for (int k = 0; k < NP; ++k) v[k] = t[k];
+        }
+    }
+};
+
 // One APGD solve of the scene on the T data; `shift` (FP64 lambda so far) turns it into the
 // correction problem.  Returns in S the iteration counts; the result is lam[S.il], u[S.jL].
 // KB independent contacts / incidence records per thread are in flight: the passes are
 // bound by the latency of dependent L2 gathers, not by bandwidth.
-template <typename T, int DIM, int KB>
-__device__ void solve_scene(const BatchArgs<T>& A, BState& S, int o0, int n0, int a0, int nct, int p0, int p1,
-                            const double* shift, double alpha0) {
+template <typename T, int DIM, int KB, int CS>
+__device__ void solve_scene(const BatchArgs<T>& A, const Grp<CS>& G, BState& S, int o0, int n0, int a0, int nct,
+                            int p0, int p1, const double* shift, double alpha0) {
     if (threadIdx.x == 0) {
         S.alpha = alpha0;
         S.lipsch = 1.0 / alpha0;
@@ -106,30 +152,30 @@ __device__ void solve_scene(const BatchArgs<T>& A, BState& S, int o0, int n0, in
         S.conv = 0;
     }
     // cold start: lambda = lambda_prev = 0, u(lambda) = u(y) = 0 (apgd.hpp:152-159)
-    for (int k = threadIdx.x; k < nct; k += blockDim.x) {
+    const int tid = G.tid(), nt = G.size();
+    for (int k = tid; k < nct; k += nt) {
         const int c = scene_contact(k, o0, n0, a0);
         A.lam[0][c] = (T)0;
         A.lam[1][c] = (T)0;
     }
-    for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+    for (int p = p0 + tid; p < p1; p += nt) {
         bst4(A.u[0] + p, (T)0, (T)0, (T)0);
         bst4(A.u[2] + p, (T)0, (T)0, (T)0);
     }
-    __syncthreads();
-    const int nt = blockDim.x;
+    G.sync();
     if (A.curvature_start) {
         // initial step from the curvature along the first descent direction d (kept in the
         // candidate buffer, which the first contact pass overwrites)
         T* dbuf = A.lam[2];
         double r2[2] = {0.0, 0.0};
-        for (int k = threadIdx.x; k < nct; k += nt) {
+        for (int k = tid; k < nct; k += nt) {
             const int c = scene_contact(k, o0, n0, a0);
             const T d = first_descent<T>(bld4(A.nc + c).w, shift, c);
             dbuf[c] = d;
             r2[0] += (double)d * (double)d;
         }
-        __syncthreads();
-        for (int p = p0 + threadIdx.x; p < p1; p += nt) {
+        G.sync();
+        for (int p = p0 + tid; p < p1; p += nt) {
             T w0 = 0, w1 = 0, w2 = 0;
             for (int k = A.inc_ptr[p]; k < A.inc_ptr[p + 1]; ++k) {
                 const V4<T> e = bld4(A.inc + k);
@@ -140,7 +186,7 @@ __device__ void solve_scene(const BatchArgs<T>& A, BState& S, int o0, int n0, in
             }
             r2[1] += A.invm[4 * (long long)p] * ((double)w0 * w0 + (double)w1 * w1 + (double)w2 * w2);
         }
-        block_reduce_t0<2>(r2);
+        G.template reduce<2>(r2, 2);
         if (threadIdx.x == 0) {
             double l;
             if (initial_lipschitz(r2[0], r2[1], A.dt2, l)) {
@@ -160,7 +206,7 @@ __device__ void solve_scene(const BatchArgs<T>& A, BState& S, int o0, int n0, in
         T* lnew = A.lam[S.in_];
         const V4<T>* uY = A.u[S.jY];
         double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        for (int kb = threadIdx.x; kb < nct; kb += KB * nt) {
+        for (int kb = tid; kb < nct; kb += KB * nt) {
             int c[KB];
             int2 ij[KB];
             V4<T> n[KB];
@@ -217,7 +263,7 @@ __device__ void solve_scene(const BatchArgs<T>& A, BState& S, int o0, int n0, in
                 s[6] += (double)lp * (double)lp;
             }
         }
-        block_reduce_t0<8>(s);
+        G.template reduce<8>(s, 0);
         if (threadIdx.x == 0) {
             const double th = S.theta;
             S.theta1 = 0.5 * (th * sqrt(4 + th * th) - th * th);
@@ -236,7 +282,7 @@ __device__ void solve_scene(const BatchArgs<T>& A, BState& S, int o0, int n0, in
         V4<T>* uYN = A.u[S.jYN];
         const T bn_ = (T)S.beta_n;
         double sw = 0.0, sq = 0.0;
-        for (int p = p0 + threadIdx.x; p < p1; p += nt) {
+        for (int p = p0 + tid; p < p1; p += nt) {
             V4<T> ul, uy;
             if (bn_ != (T)0) ul = bld4(uL + p);
             if (sizeof(T) == 4) uy = bld4(uY + p);
@@ -275,7 +321,7 @@ __device__ void solve_scene(const BatchArgs<T>& A, BState& S, int o0, int n0, in
             }
         }
         double sw1[2] = {sw, sq};
-        block_reduce_t0<2>(sw1);
+        G.template reduce<2>(sw1, 1);
         if (threadIdx.x == 0) {
             const double F_lp = 0.5 * A.dt2 * sw1[0] + S.tk[2];
             bool accept = true;
@@ -330,10 +376,11 @@ __device__ void solve_scene(const BatchArgs<T>& A, BState& S, int o0, int n0, in
 
 // FP64 residual of the scene at lambda64: u = M^-1 B^T lambda (into ufin), g = dt^2 B u + c,
 // violation = max(0, -min g).  Writes g into nc[c].w (the next correction's linear term).
-template <typename T, int DIM>
-__device__ double residual_scene(const BatchArgs<T>& A, int o0, int n0, int a0, int nct, int p0, int p1,
-                                 bool write_linear_term) {
-    for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+template <typename T, int DIM, int CS>
+__device__ double residual_scene(const BatchArgs<T>& A, const Grp<CS>& G, int o0, int n0, int a0, int nct, int p0,
+                                 int p1, bool write_linear_term) {
+    const int tid = G.tid(), nt = G.size();
+    for (int p = p0 + tid; p < p1; p += nt) {
         double w0 = 0, w1 = 0, w2 = 0;
         for (int k = A.inc_ptr[p]; k < A.inc_ptr[p + 1]; ++k) {
             const dvec4 e = bld4(A.inc64 + k);
@@ -345,9 +392,9 @@ __device__ double residual_scene(const BatchArgs<T>& A, int o0, int n0, int a0, 
         const double im = A.invm[4 * (long long)p];
         bst4(A.ufin + p, im * w0, im * w1, im * w2);
     }
-    __syncthreads();
+    G.sync();
     double vmax[1] = {0.0};
-    for (int k = threadIdx.x; k < nct; k += blockDim.x) {
+    for (int k = tid; k < nct; k += nt) {
         const int c = scene_contact(k, o0, n0, a0);
         const int2 ij = A.cij[c];
         const dvec4 n = bld4(A.nc64 + c);
@@ -374,6 +421,16 @@ __device__ double residual_scene(const BatchArgs<T>& A, int o0, int n0, int a0, 
     double m = 0.0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, red[w]);
     __syncthreads();
+    if (CS > 1) {
+        // the max over the cluster's CTAs, read by every thread through distributed shared memory
+        __shared__ double cm;
+        if (threadIdx.x == 0) cm = m;
+        G.sync();
+        cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+        m = 0.0;
+        for (int r = 0; r < CS; ++r) m = fmax(m, *cl.map_shared_rank(&cm, r));
+        G.sync();  // no CTA overwrites cm before all have read it
+    }
     return m;
 }
 
@@ -385,11 +442,10 @@ struct BatchMinBlocks {
 };
 
 // KB (the tile): independent contacts / incidence records each thread keeps in flight
-template <typename T, int DIM, int BT, int KB>
-__global__ void __launch_bounds__(BT, BatchMinBlocks<BT>::value) k_apgd_batch(BatchArgs<T> A) {
-    if (A.sizes->overflow) return;  // the step is redone after the buffers grow
-    __shared__ BState S;
-    const int scene = A.order[blockIdx.x];
+// One scene's solve (main solve, FP64 residual, corrections) by the group G and its stats.
+template <typename T, int DIM, int KB, int CS>
+__device__ void batch_scene(const BatchArgs<T>& A, const Grp<CS>& G, BState& S, int scene) {
+    const int tid = G.tid(), nt = G.size();
     const int p0 = A.sc_p0[scene], p1 = A.sc_p1[scene];
     const int o0 = A.sc_o0[scene], o1 = A.sc_o1[scene], a0 = A.sc_a0[scene], a1 = A.sc_a1[scene];
     const int n0 = o1 - o0, nct = n0 + (a1 - a0);
@@ -397,7 +453,7 @@ __global__ void __launch_bounds__(BT, BatchMinBlocks<BT>::value) k_apgd_batch(Ba
     int corr = 0, conv = 1;
     double viol = 0.0;
     if (nct > 0) {
-        solve_scene<T, DIM, KB>(A, S, o0, n0, a0, nct, p0, p1, nullptr, A.alpha);
+        solve_scene<T, DIM, KB, CS>(A, G, S, o0, n0, a0, nct, p0, p1, nullptr, A.alpha);
         iters += S.ite;
         nbt += S.nbt;
         nrs += S.nrs;
@@ -405,22 +461,22 @@ __global__ void __launch_bounds__(BT, BatchMinBlocks<BT>::value) k_apgd_batch(Ba
         if (sizeof(T) == 4) f32 += S.ite;
         // lambda64 <- lambda (FP32 solves: projected onto R+ in FP64)
         const T* lres = A.lam[S.il];
-        for (int k = threadIdx.x; k < nct; k += blockDim.x) {
+        for (int k = tid; k < nct; k += nt) {
             const int c = scene_contact(k, o0, n0, a0);
             const double v = (double)lres[c];
             A.lam64[c] = v > 0.0 ? v : 0.0;
         }
-        __syncthreads();
+        G.sync();
         if (sizeof(T) == 8) {
-            viol = residual_scene<T, DIM>(A, o0, n0, a0, nct, p0, p1, false);
+            viol = residual_scene<T, DIM, CS>(A, G, o0, n0, a0, nct, p0, p1, false);
         } else {
             for (;;) {
-                viol = residual_scene<T, DIM>(A, o0, n0, a0, nct, p0, p1, true);
+                viol = residual_scene<T, DIM, CS>(A, G, o0, n0, a0, nct, p0, p1, true);
                 if (viol <= A.viol_tol || corr >= A.max_corrections) break;
                 // the correction starts from the step size the previous solve ended with
                 const double a_next = 1.0 / S.lgood;
-                __syncthreads();
-                solve_scene<T, DIM, KB>(A, S, o0, n0, a0, nct, p0, p1, A.lam64, a_next);
+                G.sync();
+                solve_scene<T, DIM, KB, CS>(A, G, S, o0, n0, a0, nct, p0, p1, A.lam64, a_next);
                 iters += S.ite;
                 f32 += S.ite;
                 nbt += S.nbt;
@@ -428,23 +484,23 @@ __global__ void __launch_bounds__(BT, BatchMinBlocks<BT>::value) k_apgd_batch(Ba
                 conv = conv && S.conv;
                 ++corr;
                 const T* dres = A.lam[S.il];
-                for (int k = threadIdx.x; k < nct; k += blockDim.x) {
+                for (int k = tid; k < nct; k += nt) {
                     const int c = scene_contact(k, o0, n0, a0);
                     const double v = A.lam64[c] + (double)dres[c];
                     A.lam64[c] = v > 0.0 ? v : 0.0;
                 }
-                __syncthreads();
+                G.sync();
             }
             // restore the linear term of the scene's packed records for the next step's reuse
-            for (int k = threadIdx.x; k < nct; k += blockDim.x) {
+            for (int k = tid; k < nct; k += nt) {
                 const int c = scene_contact(k, o0, n0, a0);
                 A.nc[c].w = (T)A.nc64[c].w;
             }
         }
     } else {
-        for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) bst4(A.ufin + p, 0.0, 0.0, 0.0);
+        for (int p = p0 + tid; p < p1; p += nt) bst4(A.ufin + p, 0.0, 0.0, 0.0);
     }
-    if (threadIdx.x == 0) {
+    if (G.rank == 0 && threadIdx.x == 0) {
         BatchSceneStats& st = A.stats[scene];
         st.contacts = nct;
         st.iterations = iters;
@@ -454,6 +510,38 @@ __global__ void __launch_bounds__(BT, BatchMinBlocks<BT>::value) k_apgd_batch(Ba
         st.corrections = corr;
         st.converged = conv;
         st.violation = viol;
+    }
+}
+
+// one CTA per scene, scenes largest first
+template <typename T, int DIM, int BT, int KB>
+__global__ void __launch_bounds__(BT, BatchMinBlocks<BT>::value) k_apgd_batch(BatchArgs<T> A) {
+    if (A.sizes->overflow) return;  // the step is redone after the buffers grow
+    __shared__ BState S;
+    Grp<1> G;
+    G.rank = 0;
+    batch_scene<T, DIM, KB, 1>(A, G, S, A.order[blockIdx.x]);
+}
+
+// Paired layout, launched as clusters of two CTAs: cluster q < n_big solves the q-th largest
+// scene with both CTAs (its passes on two SMs); every later cluster solves two of the other
+// scenes, one per CTA (those never meet a cluster barrier).
+template <typename T, int DIM, int BT, int KB>
+__global__ void __launch_bounds__(BT, BatchMinBlocks<BT>::value) k_apgd_batch_pairs(BatchArgs<T> A) {
+    if (A.sizes->overflow) return;  // all CTAs of a cluster alike
+    __shared__ BState S;
+    const int rank = (int)cooperative_groups::this_cluster().block_rank();
+    const int q = blockIdx.x / 2;
+    if (q < A.n_big) {
+        Grp<2> G;
+        G.rank = rank;
+        batch_scene<T, DIM, KB, 2>(A, G, S, A.order[q]);
+    } else {
+        const int j = A.n_big + 2 * (q - A.n_big) + rank;
+        if (j >= A.n_scenes) return;
+        Grp<1> G;
+        G.rank = 0;
+        batch_scene<T, DIM, KB, 1>(A, G, S, A.order[j]);
     }
 }
 
@@ -473,9 +561,27 @@ __global__ void k_batch_ranges(int n_scenes, int nin, const int* sc_obs0, const 
     }
 }
 
-template <typename T, int DIM, int BT, int KB>
+template <typename T, int DIM, int BT, int KB, int CS>
 cudaError_t launch_bt(BatchArgs<T>& A, int n_scenes, cudaStream_t s) {
-    k_apgd_batch<T, DIM, BT, KB><<<n_scenes, BT, 0, s>>>(A);
+    if (CS == 1) {
+        k_apgd_batch<T, DIM, BT, KB><<<n_scenes, BT, 0, s>>>(A);
+    } else {
+        // the n_big largest scenes on two CTAs each, the rest paired, every cluster two CTAs
+        const int clusters = A.n_big + (n_scenes - A.n_big + 1) / 2;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(2 * clusters, 1, 1);
+        cfg.blockDim = dim3(BT, 1, 1);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = s;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = 2;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, k_apgd_batch_pairs<T, DIM, BT, KB>, A);
+    }
     g_batch_launches += 1;
     return cudaGetLastError();
 }
@@ -490,9 +596,11 @@ void launch_batch_ranges(int n_scenes, int nin, const int* sc_obs0, const int* s
     g_batch_launches += 1;
 }
 
+// threads per scene: one CTA of 256, 512 or 1024 threads, or 2048 = a cluster of two
+// 1024-thread CTAs
 bool batch_shape_valid(int block_threads, int tile) {
-    return (block_threads == 256 && (tile == 2 || tile == 4)) || ((block_threads == 512 || block_threads == 1024) &&
-                                                                  (tile == 1 || tile == 2));
+    return (block_threads == 256 && (tile == 2 || tile == 4)) ||
+           ((block_threads == 512 || block_threads == 1024 || block_threads == 2048) && (tile == 1 || tile == 2));
 }
 
 template <typename T>
@@ -500,6 +608,8 @@ cudaError_t launch_apgd_batch(int dim, int block_threads, int tile, const BatchS
                               cudaStream_t s) {
     BatchArgs<T> A;
     A.nin = b.nin;
+    A.n_scenes = n_scenes;
+    A.n_big = std::min(std::max(b.n_big, 0), n_scenes);
     A.order = b.order;
     A.sc_p0 = b.sc_p0;
     A.sc_p1 = b.sc_p1;
@@ -528,10 +638,12 @@ cudaError_t launch_apgd_batch(int dim, int block_threads, int tile, const BatchS
     A.dynamic = b.dynamic;
     A.max_corrections = b.max_corrections;
     A.curvature_start = b.curvature_start;
-#define LB(D, B, K) \
-    if (dim == D && block_threads == B && tile == K) return launch_bt<T, D, B, K>(A, n_scenes, s);
-    LB(2, 256, 4) LB(2, 256, 2) LB(2, 512, 1) LB(2, 512, 2) LB(2, 1024, 1) LB(2, 1024, 2)
-    LB(3, 256, 4) LB(3, 256, 2) LB(3, 512, 1) LB(3, 512, 2) LB(3, 1024, 1) LB(3, 1024, 2)
+#define LB(D, B, K, C) \
+    if (dim == D && block_threads == B * C && tile == K) return launch_bt<T, D, B, K, C>(A, n_scenes, s);
+    LB(2, 256, 4, 1) LB(2, 256, 2, 1) LB(2, 512, 1, 1) LB(2, 512, 2, 1) LB(2, 1024, 1, 1) LB(2, 1024, 2, 1)
+    LB(2, 1024, 1, 2) LB(2, 1024, 2, 2)
+    LB(3, 256, 4, 1) LB(3, 256, 2, 1) LB(3, 512, 1, 1) LB(3, 512, 2, 1) LB(3, 1024, 1, 1) LB(3, 1024, 2, 1)
+    LB(3, 1024, 1, 2) LB(3, 1024, 2, 2)
 #undef LB
     return cudaErrorInvalidValue;
 }

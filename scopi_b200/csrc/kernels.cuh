@@ -310,6 +310,7 @@ struct BatchSceneStats {
 template <typename T>
 struct BatchSolve {
     int nin;
+    int n_big;  // 2048-thread shape: the scenes (largest first) that take two CTAs each
     const int* order;
     const int *sc_p0, *sc_p1, *sc_o0, *sc_o1, *sc_a0, *sc_a1;
     const int2* cij;

@@ -25,6 +25,8 @@ constexpr int kBatchDefaultThreads = 512;
 // the tile a block size runs with unless the autotuner chose both
 inline int batch_default_tile(int threads) { return threads <= 256 ? 4 : 1; }
 constexpr long long kBatchTuneIterations = 64;
+// launch shapes the autotuner times (threads per scene x tile; 2048 = a cluster of two CTAs)
+constexpr int kBatchShapes = 8;
 
 struct DevMem {
     std::vector<void*> ptrs;
@@ -216,7 +218,8 @@ struct scopi_gpu_handle {
     int batch_tile = 0;            // contacts in flight per thread chosen with it
     int batch_bt_used = 0;         // block size of the last step
     int batch_tile_used = 0;
-    float batch_tune_ms[6] = {0, 0, 0, 0, 0, 0};
+    float batch_tune_ms[kBatchShapes] = {};
+    int batch_n_big = 0;  // 2048-thread shape: scenes with at least half the largest scene's bodies
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     double graph_dt = 0.0;
@@ -319,6 +322,7 @@ struct scopi_gpu_handle {
     void enqueue_batch_solve(double dt, int bt, int tile) {
         auto fill = [&](auto& bs) {
             bs.nin = nin;
+            bs.n_big = batch_n_big;
             bs.order = d_order;
             bs.sc_p0 = d_sc_p0;
             bs.sc_p1 = d_sc_p1;
@@ -411,7 +415,8 @@ struct scopi_gpu_handle {
     // steps run with 512 threads per scene until the first step whose longest scene solve
     // takes >= 64 iterations (the first steps of a falling pile converge in one); that
     // step's contact problem is then re-solved with each shape (threads per scene x the tile,
-    // the contacts each thread keeps in flight: 256 x 4 / 2, 512 x 1 / 2, 1024 x 1 / 2) and the
+    // the contacts each thread keeps in flight: 256 x 4 / 2, 512, 1024 and 2048 x 1 / 2; 2048
+    // puts each of the largest scenes on a cluster of two CTAs) and the
     // fastest is kept for the rest of the run.
     int step_batch(double dt) {
         for (int attempt = 0; attempt < 4; ++attempt) {
@@ -462,10 +467,11 @@ struct scopi_gpu_handle {
     // timing only: re-solve the last step's contact problem (its packed records are still in
     // place; the update already used the step's own solve) with each block size
     int autotune_batch(double dt) {
-        const int cand[6][2] = {{256, 4}, {256, 2}, {512, 1}, {512, 2}, {1024, 1}, {1024, 2}};
+        const int cand[kBatchShapes][2] = {{256, 4},  {256, 2},  {512, 1},  {512, 2},
+                                           {1024, 1}, {1024, 2}, {2048, 1}, {2048, 2}};
         float best = 1e30f;
         int best_bt = kBatchDefaultThreads, best_tile = batch_default_tile(kBatchDefaultThreads);
-        for (int k = 0; k < 6; ++k) {
+        for (int k = 0; k < kBatchShapes; ++k) {
             cudaEventRecord(ev_a[0], stream);
             enqueue_batch_solve(dt, cand[k][0], cand[k][1]);
             cudaEventRecord(ev_a[1], stream);
@@ -1862,6 +1868,12 @@ int32_t scopi_gpu_batch_create(const scopi_gpu_params* p, int32_t n_scenes, cons
     for (int s = 0; s < n_scenes; ++s) order[s] = s;
     std::stable_sort(order.begin(), order.end(),
                      [&](int a, int b) { return (sc_p1[a] - sc_p0[a]) > (sc_p1[b] - sc_p0[b]); });
+    {
+        const int largest = n_scenes > 0 ? sc_p1[order[0]] - sc_p0[order[0]] : 0;
+        int nb = 0;
+        while (nb < n_scenes && 2 * (sc_p1[order[nb]] - sc_p0[order[nb]]) >= largest) ++nb;
+        h->batch_n_big = nb;
+    }
     scopi_gpu_particles cat{ntot, nin_tot, shape.data(), pos.data(), q.data(), v.data(), om.data(), vd.data(),
                             od.data(), f.data(), m.data(), jj.data(), rad.data(), len.data()};
     rc = upload_particles(h, &cat, obs_off[nin_tot]);
@@ -1964,7 +1976,7 @@ int32_t scopi_gpu_batch_set_block_threads(scopi_gpu_handle* h, int32_t threads) 
     if (!h || !h->batch) return SCOPI_GPU_EINVAL;
     if (h->stats.steps > 0) return h->fail(SCOPI_GPU_EINVAL, "the block size is fixed once the batch has stepped");
     if (threads != 0 && threads != 256 && threads != 512 && threads != 1024)
-        return h->fail(SCOPI_GPU_EINVAL, "block size must be 256, 512 or 1024 (0 = autotune)");
+        return h->fail(SCOPI_GPU_EINVAL, "threads per scene must be 256, 512, 1024 or 2048 (0 = autotune)");
     h->batch_threads = threads;
     return 0;
 }

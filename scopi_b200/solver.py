@@ -227,7 +227,8 @@ class ScopiBatch:
     scene); ``scene(s)`` returns scene s's particles and ``scene_stats(s)`` its solver
     statistics of the last step.  ``problem``: NOFRICTION (FP64 or MIXED) or FRICTION (FP64,
     ``mu`` in the overrides).  ``block_threads`` pins the threads per scene of the NoFriction
-    solve (256, 512 or 1024); 0 lets the first step autotune it.
+    solve (256, 512, 1024, or 2048: the largest scenes on two CTAs); 0 lets the first step
+    autotune it.
     """
 
     def __init__(self, scenes, vap=VAP_FPD, contact_method=KDTREE, precision=FP64, device=0, block_threads=0,

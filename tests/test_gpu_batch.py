@@ -103,10 +103,11 @@ def test_batch_block_sizes_agree_and_are_deterministic():
         assert rel_err(a, c) <= 1e-9
 
 
-@pytest.mark.parametrize("threads,tile", [(256, 2), (512, 2), (1024, 2), (512, 1)])
+@pytest.mark.parametrize("threads,tile", [(256, 2), (512, 2), (1024, 2), (512, 1), (2048, 1), (2048, 2)])
 def test_batch_tiles_agree_with_the_default_shape(threads, tile):
     """Every launch shape the autotuner may pick (threads per scene x contacts in flight per
-    thread) solves the same problems: positions within 1e-9 of the default 256 x 4 shape."""
+    thread; 2048 = a cluster of two CTAs per scene) solves the same problems: positions
+    within 1e-9 of the default 256 x 4 shape."""
     scenes = small_piles(5, 100, 1500, seed=10)
     ref = ScopiBatch(scenes, vap=ST["vap"], precision=FP64, block_threads=256, tile=4, **KW).run(ST["dt"], 4)
     b = ScopiBatch(scenes, vap=ST["vap"], precision=FP64, block_threads=threads, tile=tile, **KW).run(ST["dt"], 4)
@@ -121,7 +122,7 @@ def test_batch_autotune_graph_replay_and_launch_count():
     scenes = small_piles(8, 100, 1500, seed=11)
     b = ScopiBatch(scenes, vap=ST["vap"], precision=MIXED, **KW)
     b.run(ST["dt"], 1)
-    assert b.block_threads() in (256, 512, 1024) and b.tile() in (1, 2, 4)
+    assert b.block_threads() in (256, 512, 1024, 2048) and b.tile() in (1, 2, 4)
     b.run(ST["dt"], 1)  # captures the graph, replays it once
     l1 = b.kernel_launches()
     b.run(ST["dt"], 1)
@@ -135,20 +136,29 @@ def test_batch_autotune_graph_replay_and_launch_count():
         b._check(b._lib.scopi_gpu_batch_set_block_threads(b._h, 512), "set_block_threads")
 
 
-def test_batch_rejects_bad_block_size_and_friction():
+def test_batch_rejects_bad_block_size_and_viscous():
     scenes = small_piles(2)
     with pytest.raises(ScopiGPUError):
         ScopiBatch(scenes, block_threads=300, **KW)
     b = ScopiBatch(scenes, **KW)
     assert b._lib.scopi_gpu_batch_set_block_threads(b._h, 512) == 0
-    from scopi_b200 import _abi
-    import ctypes as C
-    p = _abi.Params()
-    b._lib.scopi_gpu_default_params(C.byref(p), 2)
-    p.problem = 1  # Friction
-    arr = (_abi.ParticlesC * 1)()
-    h = C.c_void_p()
-    assert b._lib.scopi_gpu_batch_create(C.byref(p), 0, arr, C.byref(h)) < 0
+    from scopi_b200 import VISCOUS
+    with pytest.raises(ScopiGPUError):
+        ScopiBatch(scenes, problem=VISCOUS, **KW)
+
+
+def test_batch_cluster_shape_mixed_meets_violation_target():
+    """The mixed form with two CTAs per scene (its FP64 residual and corrections included)
+    keeps every step's violation at or below 1e-6."""
+    scenes = small_piles(4, 200, 2000, seed=13)
+    b = ScopiBatch(scenes, vap=ST["vap"], precision=MIXED, block_threads=2048, tile=1, mixed_violation_tol=1e-6,
+                   **KW)
+    for _ in range(10):
+        b.run(ST["dt"], 1)
+        st = b.stats()
+        assert st["violation"] <= 1e-6 and st["converged"] == 1, st
+    assert b.block_threads() == 2048
+    b.close()
 
 
 def test_batch_autotune_waits_for_a_nontrivial_step():
