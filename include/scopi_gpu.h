@@ -231,8 +231,9 @@ int64_t scopi_gpu_kernel_launches(scopi_gpu_handle* h);
    mixed precision form corrects each scene in FP64 inside the same launch).  The launch
    shape (threads per scene and tile) is chosen on the first step with a non-trivial solve
    by timing each shape on that step's problem.
-   NoFriction (FP64 or MIXED) and Friction (FP64: the 6-dof rows, 256 threads per scene, no
-   autotuning); other problems return SCOPI_GPU_EUNSUPPORTED.  scopi_gpu_get_stats reports
+   NoFriction (FP64 or MIXED), Friction and ViscousWithoutFriction (FP64: the 6-dof rows, 256
+   threads per scene, no autotuning; Viscous scenes carry gamma from step to step); the
+   other problems return SCOPI_GPU_EUNSUPPORTED.  scopi_gpu_get_stats reports
    the worst scene (iterations, violation). */
 typedef struct scopi_gpu_scene_stats {
     int64_t contacts;

@@ -709,6 +709,14 @@ __global__ void __launch_bounds__(kBatch6Threads) k_apgd_batch6(ApgdArgs<double>
                     const T v = apgdc::first_descent<T>(A.cvec[c], nullptr, c);
                     dbuf[c] = v;
                     s[1] += v * v;
+                    if (PROB == kViscous) {
+                        const int sl = A.slot[c];
+                        if (sl >= 0) {
+                            const T v2 = apgdc::first_descent<T>(-A.cvec[c], nullptr, sl);
+                            dbuf[sl] = v2;
+                            s[1] += v2 * v2;
+                        }
+                    }
                 }
             }
             __syncthreads();
@@ -787,6 +795,10 @@ __global__ void __launch_bounds__(kBatch6Threads) k_apgd_batch6(ApgdArgs<double>
         for (int k = threadIdx.x; k < nc; k += blockDim.x) {
             const long long c = contact_at(k);
             for (int r = 0; r < R; ++r) S.lam_out[R * c + r] = lamb[il][R * c + r];
+            if (PROB == kViscous) {
+                const int sl = A.slot[c];
+                if (sl >= 0) S.lam_out[sl] = lamb[il][sl];
+            }
             const int bi[2] = {A.ci[c], A.cj[c]};
             double q3[3] = {0, 0, 0};
             for (int side = 0; side < 2; ++side) {
@@ -1136,6 +1148,11 @@ cudaError_t launch_apgd_batch6(const Bodies& b, const StepParams& p, const ApgdS
             k_apgd_batch6<3, kFriction><<<grid, kBatch6Threads, 0, s>>>(A, S);
         else
             k_apgd_batch6<2, kFriction><<<grid, kBatch6Threads, 0, s>>>(A, S);
+    } else if (p.problem == kViscous) {
+        if (p.dim == 3)
+            k_apgd_batch6<3, kViscous><<<grid, kBatch6Threads, 0, s>>>(A, S);
+        else
+            k_apgd_batch6<2, kViscous><<<grid, kBatch6Threads, 0, s>>>(A, S);
     } else {
         return cudaErrorInvalidValue;
     }

@@ -167,7 +167,11 @@ struct scopi_gpu_handle {
     // vanish and the translational kernels apply.
     // torque-free rows: every contact's lever arms are parallel to its normal (spheres,
     // planes, segments); superellipsoid contacts need the 6-dof rows
-    bool sphere_mode() const { return !friction_rows() && !has_se; }
+    // torque-free rows and the kernels for them (not for batches of Viscous scenes, which are
+    // solved with the 6-dof batched kernel)
+    bool sphere_mode() const { return !friction_rows() && !has_se && !batch_six(); }
+    // batches solved per scene by k_apgd_batch6 (FP64): Friction and Viscous scenes
+    bool batch_six() const { return batch && (friction_rows() || P.problem == SCOPI_GPU_VISCOUS); }
 
     Bodies bodies() const {
         Bodies b;
@@ -250,14 +254,27 @@ struct scopi_gpu_handle {
         cudaMemsetAsync(d_sizes_cur, 0, sizeof(Sizes), stream);
         launch_detect(b, sp, dw, cur, d_sizes_cur, c_cap, stream);
         launch_vap(b, sp, stream, d_sizes_cur);
-        launch_geometry(b, sp, cur, d_sizes_cur, c_cap, nullptr, nullptr, c_cap, stream);
+        // Viscous scenes carry gamma from the previous step's list by (i, j) (solver.hpp:241-258)
+        const bool visc = P.problem == SCOPI_GPU_VISCOUS;
+        launch_geometry(b, sp, cur, d_sizes_cur, c_cap, visc ? &old : nullptr, visc ? &d_sizes_old->C : nullptr, c_cap,
+                        stream);
         launch_assemble(b, sp, cur, as, d_sizes_cur, c_cap, dw.scan_work, dw.tmp_total + 2, stream);
-        launch_incidence(b, sp, cur, as, inc, d_sizes_cur, c_cap, dw.scan_work, dw.tmp_total + 2, stream, false);
-        if (friction_rows()) {
-            // Friction scenes: the 6-dof rows (three per contact) solved per scene in FP64
+        launch_incidence(b, sp, cur, as, inc, d_sizes_cur, c_cap, dw.scan_work, dw.tmp_total + 2, stream,
+                         batch_six());
+        if (batch_six()) {
+            // Friction (three multipliers per contact) and Viscous scenes (a second multiplier on
+            // the contacts with gamma < 0): the 6-dof rows solved per scene in FP64
             launch_batch_ranges(n_scenes, nin, d_sc_obs0, d_sc_obs1, d_sc_p0, d_sc_p1, d_obs_off, dw.obs_pos,
                                 dw.row_ptr, d_sizes_cur, d_sc_o0, d_sc_o1, d_sc_a0, d_sc_a1, stream);
             enqueue_batch_solve6(dt);
+            if (visc) {
+                launch_gamma_update(sp, cur, as, d_lamacc, d_sizes_cur, c_cap, stream);
+                // this step's list (pairs and gamma) is the next step's previous list
+                cudaMemcpyAsync(old.ci, cur.ci, c_cap * sizeof(int), cudaMemcpyDeviceToDevice, stream);
+                cudaMemcpyAsync(old.cj, cur.cj, c_cap * sizeof(int), cudaMemcpyDeviceToDevice, stream);
+                cudaMemcpyAsync(old.gamma, cur.gamma, c_cap * sizeof(double), cudaMemcpyDeviceToDevice, stream);
+                cudaMemcpyAsync(d_sizes_old, d_sizes_cur, sizeof(Sizes), cudaMemcpyDeviceToDevice, stream);
+            }
             launch_update(b, sp, d_ufin, 6, 1, d_sizes_cur, stream);
             return;
         }
@@ -457,7 +474,7 @@ struct scopi_gpu_handle {
             finish_batch_step_timing();
             batch_bt_used = bt;
             batch_tile_used = tile;
-            if (!batch_threads && !friction_rows() && stats.iterations >= kBatchTuneIterations)
+            if (!batch_threads && !batch_six() && stats.iterations >= kBatchTuneIterations)
                 return autotune_batch(dt);
             return 0;
         }
@@ -1753,12 +1770,12 @@ int32_t scopi_gpu_batch_create(const scopi_gpu_params* p, int32_t n_scenes, cons
         return SCOPI_GPU_EINVAL;
     }
     *out = nullptr;
-    if (p->problem != SCOPI_GPU_NOFRICTION && p->problem != SCOPI_GPU_FRICTION) {
-        scopi_gpu::set_global_error("scopi_gpu_batch_create: batches solve NoFriction and Friction scenes");
+    if (p->problem != SCOPI_GPU_NOFRICTION && p->problem != SCOPI_GPU_FRICTION && p->problem != SCOPI_GPU_VISCOUS) {
+        scopi_gpu::set_global_error("scopi_gpu_batch_create: batches solve NoFriction, Friction and Viscous scenes");
         return SCOPI_GPU_EUNSUPPORTED;
     }
-    if (p->problem == SCOPI_GPU_FRICTION && p->precision != SCOPI_GPU_FP64) {
-        scopi_gpu::set_global_error("scopi_gpu_batch_create: Friction batches run in FP64");
+    if (p->problem != SCOPI_GPU_NOFRICTION && p->precision != SCOPI_GPU_FP64) {
+        scopi_gpu::set_global_error("scopi_gpu_batch_create: Friction and Viscous batches run in FP64");
         return SCOPI_GPU_EUNSUPPORTED;
     }
     long long ntot = 0, nin_tot = 0;

@@ -225,8 +225,8 @@ class ScopiBatch:
     ``scenes`` is a list of ``ParticleArrays`` (each obstacles first).  ``run(dt, k)`` advances
     every scene k steps (one CUDA graph replay per step, one persistent launch solving every
     scene); ``scene(s)`` returns scene s's particles and ``scene_stats(s)`` its solver
-    statistics of the last step.  ``problem``: NOFRICTION (FP64 or MIXED) or FRICTION (FP64,
-    ``mu`` in the overrides).  ``block_threads`` pins the threads per scene of the NoFriction
+    statistics of the last step.  ``problem``: NOFRICTION (FP64 or MIXED), FRICTION (FP64,
+    ``mu`` in the overrides) or VISCOUS (FP64).  ``block_threads`` pins the threads per scene of the NoFriction
     solve (256, 512, 1024, or 2048: the largest scenes on two CTAs); 0 lets the first step
     autotune it.
     """

@@ -136,15 +136,15 @@ def test_batch_autotune_graph_replay_and_launch_count():
         b._check(b._lib.scopi_gpu_batch_set_block_threads(b._h, 512), "set_block_threads")
 
 
-def test_batch_rejects_bad_block_size_and_viscous():
+def test_batch_rejects_bad_block_size_and_viscous_friction():
     scenes = small_piles(2)
     with pytest.raises(ScopiGPUError):
         ScopiBatch(scenes, block_threads=300, **KW)
     b = ScopiBatch(scenes, **KW)
     assert b._lib.scopi_gpu_batch_set_block_threads(b._h, 512) == 0
-    from scopi_b200 import VISCOUS
+    from scopi_b200 import VISCOUS_FRICTION
     with pytest.raises(ScopiGPUError):
-        ScopiBatch(scenes, problem=VISCOUS, **KW)
+        ScopiBatch(scenes, problem=VISCOUS_FRICTION, **KW)
 
 
 def test_batch_cluster_shape_mixed_meets_violation_target():
@@ -230,3 +230,41 @@ def test_batch_friction_matches_single_scene_gpu():
 def test_batch_friction_refuses_mixed_precision():
     with pytest.raises(ScopiGPUError):
         ScopiBatch(small_piles(2), vap=ST["vap"], precision=MIXED, problem=FRICTION, **FKW)
+
+
+# ---- Viscous scenes (LagrangeMultiplier<Viscous>, lagrange_multiplier.hpp:116-206; gamma
+# carried by (i, j) from step to step, solver.hpp:241-258): FP64, one CTA per scene
+def test_batch_viscous_matches_oracle_per_scene():
+    from scopi_b200 import VISCOUS
+    scenes = small_piles(4)
+    steps = 10
+    b = ScopiBatch(scenes, vap=ST["vap"], precision=FP64, problem=VISCOUS, **KW)
+    oracles = [oracle_solver(s, vap=ST["vap"], problem=VISCOUS, **KW) for s in scenes]
+    for k in range(steps):
+        b.run(ST["dt"], 1)
+        for s, o in enumerate(oracles):
+            o.run(ST["dt"], 1)
+            assert b.scene_stats(s)["contacts"] == len(o.contacts()["i"]), f"scene {s} step {k}"
+    for s, o in enumerate(oracles):
+        g = b.scene(s)
+        st = b.scene_stats(s)
+        print(s, "positions", rel_err(g.pos, o.pa.pos), "velocities", rel_err(g.v, o.pa.v), st)
+        assert rel_err(g.pos, o.pa.pos) <= 1e-9, s
+        assert rel_err(g.v, o.pa.v) <= 1e-7, s
+        assert st["converged"] == 1
+    b.close()
+
+
+def test_batch_viscous_matches_single_scene_gpu():
+    from scopi_b200 import VISCOUS
+    scenes = small_piles(5, 100, 800, seed=14) + [lone_disk()]
+    steps = 8
+    b = ScopiBatch(scenes, vap=ST["vap"], precision=FP64, problem=VISCOUS, **KW).run(ST["dt"], steps)
+    for s, pa in enumerate(scenes):
+        one = ScopiSolver(pa, vap=ST["vap"], precision=FP64, problem=VISCOUS, **KW).run(ST["dt"], steps)
+        g = b.scene(s)
+        assert b.scene_stats(s)["contacts"] == one.stats()["contacts"], s
+        assert rel_err(g.pos, one.particles.pos) <= 1e-9, s
+        assert rel_err(g.v, one.particles.v) <= 1e-7, s
+        one.close()
+    b.close()
