@@ -274,8 +274,7 @@ int32_t scopi_gpu_batch_set_shape(scopi_gpu_handle* h, int32_t threads, int32_t 
    library (about 3.4 MB, held by every GPU that loads the library until exit), so:
      - limits: at most 16384 contacts and 8192 active bodies; larger sizes return
        SCOPI_GPU_EINVAL with a message in scopi_gpu_last_error(NULL);
-     - the first call on a device looks up that array's device address (make that first
-       call before any stream capture);
+     - the first call on a device looks up that array's device address;
      - all calls share the array: calls that overlap on the GPU (other streams or host
        threads) race; run them one after another.
    Inputs: ci, cj (n_contacts body indices, obstacles < nb_inactive), normal (n_contacts*3,
