@@ -192,8 +192,12 @@ def time_path(pa, precision, steps, warmup, ranks, sampler=None, solver=None, **
     return {"ms": ms, "per_step": per, "launches": launches, "clocks": clocks}
 
 
-def time_e2e(pa, precision, steps, warmup, ranks):
-    """Same steps through the C ABI with host buffers: upload, step, download every step."""
+def time_e2e(pa, precision, steps, warmup, ranks, full_upload=False):
+    """Same steps through the C ABI with host buffers: upload, step, download every step.
+
+    The upload is the state a step updates (pos, q, v, omega: scopi_gpu_set_state), or with
+    full_upload the whole container (scopi_gpu_set_particles: shapes, masses, forces and
+    desired velocities too, and the container's checks)."""
     import numpy as np
     import torch
 
@@ -221,8 +225,9 @@ def time_e2e(pa, precision, steps, warmup, ranks):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
+    upload = s.upload if full_upload else s.upload_state
     for _ in range(steps):
-        s.upload(host)
+        upload(host)
         s.step(dt, 1)
         s.download(host)
     e1.record(stream)
@@ -230,7 +235,10 @@ def time_e2e(pa, precision, steps, warmup, ranks):
     ranks.barrier()
     ms = e0.elapsed_time(e1)
     n = host.n
-    h2d = 4 * n + 4 * n + 8 * n * (3 + 4 + 3 + 3 + 3 + 3 + 3 + 1 + 3 + 1 + 1)  # shape, worm, 11 FP64 fields
+    if full_upload:
+        h2d = 4 * n + 4 * n + 8 * n * (3 + 4 + 3 + 3 + 3 + 3 + 3 + 1 + 3 + 1 + 1)  # shape, worm, 11 FP64 fields
+    else:
+        h2d = 8 * n * (3 + 4 + 3 + 3)  # pos, q, v, omega
     d2h = 8 * n * (3 + 4 + 3 + 3)
     s.close()
     return ms, h2d, d2h
@@ -710,6 +718,7 @@ def ours(args, ranks):
                          "iterations_per_step": statistics.mean(its),
                          "violation_max": max(p["violation"] for p in r["per_step"])}
     e2e_ms, h2d, d2h = time_e2e(pa, MIXED, args.steps, args.warmup, ranks)
+    e2e_full_ms, h2d_full, _ = time_e2e(pa, MIXED, args.steps, args.warmup, ranks, full_upload=True)
     # ViscousWithoutFriction on the same workload (gamma defaults 0 / -2 / 1e-6)
     visc = None
     if not args.no_viscous:
@@ -731,6 +740,7 @@ def ours(args, ranks):
     value = args.gpus * args.steps * 1000.0 / ms if ranks.world > 1 else args.steps * 1000.0 / ms
     e2e_ms = ranks.max(e2e_ms)
     e2e_val = (ranks.world * args.steps * 1000.0 / e2e_ms)
+    e2e_full_val = (ranks.world * args.steps * 1000.0 / ranks.max(e2e_full_ms))
     f64_val = None
     if f64:
         f64_ms = ranks.max(f64["ms"])
@@ -795,7 +805,12 @@ def ours(args, ranks):
         "fp64": {"value": f64_val, "unit": UNIT, "mixed_over_fp64": (value / f64_val) if f64_val else None,
                  "roofline": f64_roof},
         "ablation": abl or None,
-        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "upload": "scopi_gpu_set_state (pos, q, v, omega), step, scopi_gpu_get_particles",
+                "full_container": {"value": e2e_full_val, "unit": UNIT, "h2d_bytes_per_step": h2d_full,
+                                   "d2h_bytes_per_step": d2h,
+                                   "upload": "scopi_gpu_set_particles (all 13 fields), step, "
+                                             "scopi_gpu_get_particles"}},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                      "peak_source": f"{peak_kind} hbm_gbs",

@@ -180,6 +180,16 @@ int32_t scopi_gpu_destroy(scopi_gpu_handle* h);
 int32_t scopi_gpu_set_particles(scopi_gpu_handle* h, const scopi_gpu_particles* parts);
 int32_t scopi_gpu_get_particles(scopi_gpu_handle* h, scopi_gpu_particles* out);
 
+/* Write the fields a time step updates back into the container already on the device: the
+   writable pos()/q()/v()/omega() accessors of scopi_container (container.hpp:129,138,174,183)
+   used between two ScopiSolver::run calls.  parts->n and parts->nb_inactive must equal the
+   last set_particles' counts; pos, q, v and omega are copied where non-NULL, every other
+   field of parts is ignored (shapes, masses, forces and desired velocities stay those of the
+   last set_particles; change them with set_particles).  The previous contacts are kept, as
+   with set_particles.  The copies are enqueued on the handle's stream and the call returns
+   after they complete.  Batch handles and handles without particles return SCOPI_GPU_EINVAL. */
+int32_t scopi_gpu_set_state(scopi_gpu_handle* h, const scopi_gpu_particles* parts);
+
 /* ScopiSolver::run(dt, total_it, initial_iter), solver.hpp:267-303 (output disabled). */
 int32_t scopi_gpu_run(scopi_gpu_handle* h, double dt, int64_t total_it, int64_t initial_iter);
 

@@ -25,6 +25,7 @@ EXPORTED = [
     "scopi_gpu_batch_create", "scopi_gpu_batch_get_scene", "scopi_gpu_batch_get_scene_stats",
     "scopi_gpu_batch_block_threads", "scopi_gpu_batch_set_block_threads", "scopi_gpu_test_barrier_stall",
     "scopi_gpu_set_contacts", "scopi_gpu_get_se_starts", "scopi_gpu_batch_tile", "scopi_gpu_batch_set_shape",
+    "scopi_gpu_set_state",
 ]
 
 
@@ -88,6 +89,7 @@ def load(path: str = LIB_PATH):
     L.scopi_gpu_destroy.argtypes = [H]
     L.scopi_gpu_set_particles.argtypes = [H, C.POINTER(ParticlesC)]
     L.scopi_gpu_get_particles.argtypes = [H, C.POINTER(ParticlesC)]
+    L.scopi_gpu_set_state.argtypes = [H, C.POINTER(ParticlesC)]
     L.scopi_gpu_run.argtypes = [H, C.c_double, C.c_int64, C.c_int64]
     L.scopi_gpu_detect.argtypes = [H, I64]
     L.scopi_gpu_get_contacts.argtypes = [H, C.c_int64, I64, I64, I64, D, D, D, D, D]
@@ -126,6 +128,7 @@ def load(path: str = LIB_PATH):
     L.scopi_gpu_test_barrier_stall.argtypes = [H]
     L.scopi_gpu_test_barrier_stall.restype = C.c_int32
     for name in ("scopi_gpu_create", "scopi_gpu_destroy", "scopi_gpu_set_particles", "scopi_gpu_get_particles",
+                 "scopi_gpu_set_state",
                  "scopi_gpu_run", "scopi_gpu_detect", "scopi_gpu_get_contacts", "scopi_gpu_get_lambda",
                  "scopi_gpu_get_stats", "scopi_gpu_amat", "scopi_gpu_atmat"):
         getattr(L, name).restype = C.c_int32

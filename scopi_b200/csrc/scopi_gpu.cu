@@ -1556,6 +1556,28 @@ static int32_t upload_particles(scopi_gpu_handle* h, const scopi_gpu_particles* 
     return 0;
 }
 
+int32_t scopi_gpu_set_state(scopi_gpu_handle* h, const scopi_gpu_particles* p) {
+    if (!h || !p) return h ? h->fail(SCOPI_GPU_EINVAL, "set_state: null container") : SCOPI_GPU_EINVAL;
+    if (h->batch) return h->fail(SCOPI_GPU_EINVAL, "batch handles take their scenes at creation");
+    if (h->n == 0) return h->fail(SCOPI_GPU_EINVAL, "set_state: no particles (call set_particles first)");
+    if (p->n != h->n || p->nb_inactive != h->nin)
+        return h->fail(SCOPI_GPU_EINVAL, "set_state: n and nb_inactive must match the container on the device");
+    cudaSetDevice(h->dev);
+    cudaStream_t s = h->stream;
+    const size_t n = (size_t)h->n;
+    cudaError_t e = cudaSuccess;
+    auto up = [&](void* dst, const double* src, size_t count) {
+        if (src && e == cudaSuccess) e = cudaMemcpyAsync(dst, src, count * n * sizeof(double), cudaMemcpyHostToDevice, s);
+    };
+    up(h->d_pos, p->pos, 3);
+    up(h->d_q, p->q, 4);
+    up(h->d_v, p->v, 3);
+    up(h->d_omega, p->omega, 3);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return h->cuda_fail(e, "set_state");
+    return 0;
+}
+
 int32_t scopi_gpu_get_particles(scopi_gpu_handle* h, scopi_gpu_particles* o) {
     if (!h || !o) return SCOPI_GPU_EINVAL;
     cudaSetDevice(h->dev);

@@ -192,6 +192,14 @@ class ScopiSolver:
         s = self._struct(pa)
         self._check(self._lib.scopi_gpu_set_particles(self._h, C.byref(s)), "scopi_gpu_set_particles")
 
+    def upload_state(self, pa: ParticleArrays):
+        """Copy pos/q/v/omega from host arrays into the container on the device
+        (scopi_gpu_set_state); pa must hold as many bodies and obstacles as the device's
+        container, and its other fields are not read."""
+        self._ensure()
+        s = self._struct(pa)
+        self._check(self._lib.scopi_gpu_set_state(self._h, C.byref(s)), "scopi_gpu_set_state")
+
     def download(self, pa: ParticleArrays):
         """Copy pos/q/v/omega back into host arrays (scopi_gpu_get_particles)."""
         s = self._struct(pa)

@@ -63,6 +63,12 @@ def test_create_without_gpu_fails_cleanly(lib):
     assert b"CUDA" in lib.scopi_gpu_last_error(None)
 
 
+def test_set_state_without_handle_is_refused(lib):
+    # host-side argument checks only: no CUDA call is reached
+    from scopi_b200 import _abi
+    assert lib.scopi_gpu_set_state(None, None) == _abi.EINVAL
+
+
 def test_solver_raises_without_library(tmp_path):
     from scopi_b200 import _abi
     with pytest.raises(OSError):
