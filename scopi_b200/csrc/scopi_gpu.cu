@@ -1998,7 +1998,7 @@ int32_t scopi_gpu_batch_set_shape(scopi_gpu_handle* h, int32_t threads, int32_t 
     if (!h || !h->batch) return SCOPI_GPU_EINVAL;
     if (h->stats.steps > 0) return h->fail(SCOPI_GPU_EINVAL, "the launch shape is fixed once the batch has stepped");
     if (!(threads == 0 && tile == 0) && !scopi_gpu::batch_shape_valid(threads, tile))
-        return h->fail(SCOPI_GPU_EINVAL, "launch shape must be 256 x 2|4, 512 x 1|2 or 1024 x 1|2 (0, 0 = autotune)");
+        return h->fail(SCOPI_GPU_EINVAL, "launch shape must be 256 x 2|4, 512 x 1|2, 1024 x 1|2 or 2048 x 1|2 (0, 0 = autotune)");
     h->batch_threads = threads;
     h->batch_tile = tile;
     return 0;
@@ -2014,7 +2014,7 @@ int32_t scopi_gpu_test_barrier_stall(scopi_gpu_handle* h) {
 int32_t scopi_gpu_batch_set_block_threads(scopi_gpu_handle* h, int32_t threads) {
     if (!h || !h->batch) return SCOPI_GPU_EINVAL;
     if (h->stats.steps > 0) return h->fail(SCOPI_GPU_EINVAL, "the block size is fixed once the batch has stepped");
-    if (threads != 0 && threads != 256 && threads != 512 && threads != 1024)
+    if (threads != 0 && !scopi_gpu::batch_shape_valid(threads, batch_default_tile(threads)))
         return h->fail(SCOPI_GPU_EINVAL, "threads per scene must be 256, 512, 1024 or 2048 (0 = autotune)");
     h->batch_threads = threads;
     return 0;

@@ -142,6 +142,11 @@ def test_batch_rejects_bad_block_size_and_viscous_friction():
         ScopiBatch(scenes, block_threads=300, **KW)
     b = ScopiBatch(scenes, **KW)
     assert b._lib.scopi_gpu_batch_set_block_threads(b._h, 512) == 0
+    # 2048 = the cluster shape with its default tile
+    assert b._lib.scopi_gpu_batch_set_block_threads(b._h, 2048) == 0
+    assert b._lib.scopi_gpu_batch_set_block_threads(b._h, 4096) < 0
+    b.run(ST["dt"], 1)
+    assert b.block_threads() == 2048 and b.tile() == 1
     from scopi_b200 import VISCOUS_FRICTION
     with pytest.raises(ScopiGPUError):
         ScopiBatch(scenes, problem=VISCOUS_FRICTION, **KW)
